@@ -1,0 +1,122 @@
+/* rt_b200.h -- C ABI of the B200 flip-dynamics engine (librt_b200.so).
+ *
+ * This is the drop-in boundary for RandomTilings' per-model Tiler classes.
+ * Each entry point names the reference interface it replaces (paths are
+ * relative to the GPUTilings/RandomTilings source tree).  Plain pointers and
+ * sizes only; every function returns an rt_status (0 = success) and never
+ * throws or exits.  Tilings are host int32 arrays of N x N, row-major, in the
+ * reference's encodings:
+ *   domino        src/Domino/DominoTiler.h:17-37       (vertex edge bits)
+ *   lozenge       src/Lozenge/LozengeTiler.h:8-28       (vertex edge bits)
+ *   rect-triangle src/RectTriangle/RectTriangleTiler.h:16-27 (hex face digits)
+ *   tri-dimer     src/TriangleDimer/TriangleDimerTiler.h:13-67 (lozenge states)
+ * A handle (rt_tiler) is not thread-safe, like the reference classes, which
+ * own one command queue and one RNG buffer each.
+ */
+#ifndef RT_B200_H
+#define RT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    RT_OK = 0,
+    RT_E_INVAL = -1,     /* bad argument or tiling size */
+    RT_E_PARAMS = -2,    /* TinyMT parameter table missing, short or malformed */
+    RT_E_NOMEM = -3,     /* device or host allocation failed */
+    RT_E_CUDA = -4,      /* a CUDA call failed (rt_last_error has the text) */
+    RT_E_TIMEOUT = -5,   /* a bounded device wait gave up (kernel returned early) */
+    RT_E_NODEVICE = -6,  /* no usable sm_100 device */
+    RT_E_STATE = -7      /* call out of order (e.g. run before upload) */
+} rt_status;
+
+typedef enum { RT_DOMINO = 0, RT_LOZENGE = 1, RT_RECTTRI = 2, RT_TRIDIMER = 3 } rt_model;
+
+/* Which reference kernel file the flip follows. */
+typedef enum {
+    RT_KERNEL_DEFAULT = 0, /* dominokernel.cl / lozengekernel.cl / recttrianglekernel.cl / triangledimerkernel.cl */
+    RT_KERNEL_CFTP = 1,    /* domino only: dominokernelCFTP.cl (monotone heat bath) */
+    RT_KERNEL_QWEIGHT = 2  /* lozenge only: qlozengekernel.cl (volume weight q, int32 storage) */
+} rt_kernel;
+
+typedef enum {
+    RT_RNG_TINYMT = 0, /* bit-exact: per-work-item TinyMT streams + the reference's host colour order */
+    RT_RNG_PHILOX = 1  /* fast mode: Philox4x32-10 keyed by (chain, site, sweep, colour), cyclic colour sweeps */
+} rt_rng;
+
+typedef enum {
+    RT_QCMP_FLOAT32 = 0, /* q rounded to float before the compare (an fp32-only OpenCL device) */
+    RT_QCMP_DOUBLE = 1   /* q compared as the double literal of qlozengekernel.cl:3 */
+} rt_qcmp;
+
+typedef struct {
+    int32_t model;       /* rt_model */
+    int32_t kernel;      /* rt_kernel */
+    int32_t rng;         /* rt_rng */
+    int32_t qcmp;        /* rt_qcmp, q-weighted lozenge only */
+    double q;            /* volume weight, qlozengekernel.cl:3 (0.99) */
+    float weights[16];   /* rect-triangle face weights by digit, recttrianglekernel.cl:3-13 */
+    int32_t device;      /* CUDA device ordinal */
+    int32_t reserved;
+    void* stream;        /* cudaStream_t to run on; NULL = the handle creates its own */
+} rt_config;
+
+typedef struct rt_tiler rt_tiler;
+
+/* Fills *cfg with the reference defaults (q = 0.99, unit weights, TinyMT). */
+void rt_config_default(rt_config* cfg, int32_t model);
+
+/* Replaces the constructors DominoTiler(context, queue, devices, source, err)
+ * src/Domino/DominoTiler.h:61-67, LozengeTiler src/Lozenge/LozengeTiler.h:47-53,
+ * RectTriangleTiler src/RectTriangle/RectTriangleTiler.h:45-52 and
+ * TriangleDimerTiler src/TriangleDimer/TriangleDimerTiler.h:116-174.  The
+ * OpenCL objects become a device ordinal (+ optional stream) in *cfg. */
+rt_status rt_create(const rt_config* cfg, rt_tiler** out);
+rt_status rt_destroy(rt_tiler* h);
+
+/* Replaces LoadTinyMT(std::string params, int size), e.g.
+ * src/Domino/DominoTiler.cpp:109-111 -> src/TinyMT/file_reader.cpp:22-38.
+ * Reads `n` (mat1, mat2, tmat) triples from a tinymt32dc text table.  With no
+ * table loaded, every work item uses the TinyMT32J constants
+ * (src/TinyMT/tinymt32def.h:47-49). */
+rt_status rt_load_rng_params(rt_tiler* h, const char* path, int64_t n);
+/* Same, from memory: 3*n uint32 (mat1, mat2, tmat per id). */
+rt_status rt_set_rng_params(rt_tiler* h, const uint32_t* table, int64_t n);
+
+/* Replaces Walk(tiling&, long steps, long seed) src/Domino/DominoTiler.cpp:9-55,
+ * Walk(tiling&, int, long) src/Lozenge/LozengeTiler.cpp:18-88,
+ * src/RectTriangle/RectTriangleTiler.cpp:17-92,
+ * src/TriangleDimer/TriangleDimerTiler.cpp:86-483.  `tiling` (N*N int32,
+ * host) is updated in place; synchronous, like the reference. */
+rt_status rt_walk(rt_tiler* h, int32_t* tiling, int32_t n, int64_t steps, int64_t seed);
+
+/* Replaces DominoTiler::Walk(tiling&, vector<long> steps, vector<long> seeds)
+ * src/Domino/DominoTiler.cpp:58-107 (k epochs, TinyMT re-seeded each epoch). */
+rt_status rt_walk_epochs(rt_tiler* h, int32_t* tiling, int32_t n, const int64_t* steps, const int64_t* seeds,
+                         int32_t k);
+
+/* Split form of rt_walk, for callers that keep the lattice on the device
+ * (the reference re-uploads per Walk, DominoTiler.cpp:26-27,46-47):
+ * upload + split into colour arrays, run steps (asynchronous on the handle's
+ * stream), merge + download.  rt_walk == upload; run; download. */
+rt_status rt_upload(rt_tiler* h, const int32_t* tiling, int32_t n);
+rt_status rt_run(rt_tiler* h, int64_t steps, int64_t seed);
+rt_status rt_download(rt_tiler* h, int32_t* tiling);
+rt_status rt_synchronize(rt_tiler* h);
+/* The handle's cudaStream_t (as void*), for callers that time with events. */
+void* rt_stream(rt_tiler* h);
+/* Counters of the last run: phases executed and kernel launches issued. */
+rt_status rt_last_run_info(rt_tiler* h, int64_t* phases, int64_t* launches);
+
+/* Text of the last failure on this handle (or of the last rt_create). */
+const char* rt_last_error(rt_tiler* h);
+const char* rt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RT_B200_H */

@@ -1,0 +1,223 @@
+"""ctypes access to the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Two libraries, both built by oracle/Makefile:
+  _build/liboracle.so -- the C restatement (rt_oracle.c), always available;
+  _ref/libref.so      -- the reference's own sources compiled through the
+                         OpenCL shim; only where the reference tree was present
+                         at build time.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline load this.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libref.so")
+
+TINYMT32J = (0x8F7011EE, 0xFC78FF1F, 0x3793FDFF)
+
+_P, _I32, _I64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+
+
+def build_oracle() -> str:
+    """Builds the C restatement if it is missing (gcc only)."""
+    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < max(
+        os.path.getmtime(os.path.join(HERE, f)) for f in ("rt_oracle.c", "rt_oracle.h")
+    ):
+        subprocess.run(["make", "-C", HERE, "-s"], check=True)
+    return ORACLE_SO
+
+
+_orc = None
+_ref = None
+
+
+def oracle() -> ctypes.CDLL:
+    global _orc
+    if _orc is None:
+        lib = ctypes.CDLL(build_oracle())
+        lib.orc_domino_walk.argtypes = [_P, ctypes.c_int, _I64, _I64, _P, _I64, ctypes.c_int]
+        lib.orc_domino_walk_epochs.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, _P, _I64, ctypes.c_int]
+        lib.orc_lozenge_walk.argtypes = [_P, ctypes.c_int, _I64, _I64, _P, _I64, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_int]
+        lib.orc_recttri_walk.argtypes = [_P, ctypes.c_int, _I64, _I64, _P, _I64, _P]
+        lib.orc_tridimer_walk.argtypes = [_P, ctypes.c_int, _I64, _I64, _P, _I64]
+        lib.orc_mt19937_stream.argtypes = [_I64, _I64, _P]
+        lib.orc_minstd_raw_stream.argtypes = [_I64, _I64, _P]
+        lib.orc_minstd_uniform_stream.argtypes = [_I64, _I64, _P, ctypes.c_int, _P]
+        lib.orc_domino_colours.argtypes = [_I64, _I64, ctypes.c_int, _P]
+        lib.orc_lozenge_colours.argtypes = [_I64, _I64, _P]
+        lib.orc_tinymt_init.argtypes = [_P, ctypes.c_uint32]
+        lib.orc_tinymt_bits12.argtypes = [_P]
+        lib.orc_tinymt_bits12.restype = ctypes.c_uint32
+        _orc = lib
+    return _orc
+
+
+def have_ref() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        if not have_ref():
+            raise FileNotFoundError(REF_SO)
+        lib = ctypes.CDLL(REF_SO)
+        lib.ref_set_threads.argtypes = [ctypes.c_int]
+        lib.ref_write_params.argtypes = [ctypes.c_char_p, ctypes.c_long, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint]
+        lib.ref_tiler_create.restype = _P
+        lib.ref_tiler_create.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_long]
+        lib.ref_tiler_destroy.argtypes = [_P]
+        lib.ref_tiler_walk.argtypes = [_P, _P, ctypes.c_long, ctypes.c_long, ctypes.c_long]
+        lib.ref_tiler_walk_epochs.argtypes = [_P, _P, ctypes.c_long, _P, _P, ctypes.c_int]
+        lib.ref_build.restype = ctypes.c_long
+        lib.ref_build.argtypes = [ctypes.c_int, _P, ctypes.c_long, _P, ctypes.c_long, ctypes.c_int, ctypes.c_int, _P,
+                                  ctypes.c_long]
+        lib.ref_write.argtypes = [ctypes.c_int, _P, ctypes.c_long, _P, ctypes.c_long, ctypes.c_char_p]
+        _ref = lib
+    return _ref
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise RuntimeError(f"{what} failed with {rc}")
+
+
+def _tiling(t) -> tuple[np.ndarray, int]:
+    a = np.array(t, dtype=np.int32).reshape(-1).copy()
+    n = int(round(a.size ** 0.5))
+    assert n * n == a.size
+    return a, n
+
+
+def _table(params):
+    if params is None:
+        return None, 0, None
+    tab = np.ascontiguousarray(params, dtype=np.uint32).reshape(-1)
+    return tab.ctypes.data, tab.size // 3, tab
+
+
+# ---- the C restatement ----------------------------------------------------
+def domino_walk(t, steps, seed, cftp=False, params=None) -> np.ndarray:
+    a, n = _tiling(t)
+    p, np_, keep = _table(params)
+    _check(oracle().orc_domino_walk(a.ctypes.data, n, steps, seed, p, np_, int(cftp)), "orc_domino_walk")
+    return a
+
+
+def domino_walk_epochs(t, steps, seeds, cftp=True, params=None) -> np.ndarray:
+    a, n = _tiling(t)
+    st = np.ascontiguousarray(steps, dtype=np.int64)
+    se = np.ascontiguousarray(seeds, dtype=np.int64)
+    p, np_, keep = _table(params)
+    _check(oracle().orc_domino_walk_epochs(a.ctypes.data, n, st.ctypes.data, se.ctypes.data, st.size, p, np_,
+                                           int(cftp)), "orc_domino_walk_epochs")
+    return a
+
+
+def lozenge_walk(t, steps, seed, qweight=False, q=0.99, qcmp_double=False, params=None) -> np.ndarray:
+    a, n = _tiling(t)
+    p, np_, keep = _table(params)
+    _check(oracle().orc_lozenge_walk(a.ctypes.data, n, steps, seed, p, np_, int(qweight), q, int(qcmp_double)),
+           "orc_lozenge_walk")
+    return a
+
+
+def recttri_walk(t, steps, seed, weights=None, params=None) -> np.ndarray:
+    a, n = _tiling(t)
+    p, np_, keep = _table(params)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
+    _check(oracle().orc_recttri_walk(a.ctypes.data, n, steps, seed, p, np_, None if w is None else w.ctypes.data),
+           "orc_recttri_walk")
+    return a
+
+
+def tridimer_walk(t, steps, seed, params=None) -> np.ndarray:
+    a, n = _tiling(t)
+    p, np_, keep = _table(params)
+    _check(oracle().orc_tridimer_walk(a.ctypes.data, n, steps, seed, p, np_), "orc_tridimer_walk")
+    return a
+
+
+# ---- the reference's own code (oracle/_ref) --------------------------------
+REF_MODELS = {"domino": 0, "domino_cftp": 1, "lozenge": 2, "qlozenge": 3, "recttri": 4, "tridimer": 5}
+
+
+class RefTiler:
+    """One reference Tiler object (its LoadTinyMT already done)."""
+
+    def __init__(self, model: str, n_params: int, params=None, threads: int = 1):
+        lib = ref()
+        lib.ref_set_threads(threads)
+        fd, path = tempfile.mkstemp(prefix="tinymt_", suffix=".txt")
+        os.close(fd)
+        try:
+            if params is None:
+                lib.ref_write_params(path.encode(), n_params, *TINYMT32J)
+            else:
+                tab = np.asarray(params, dtype=np.uint32).reshape(-1, 3)
+                with open(path, "w") as f:
+                    f.write("# table\n")
+                    for i, (m1, m2, tm) in enumerate(tab[:n_params]):
+                        f.write(f"tinymt32,{i},127,{m1:08x},{m2:08x},{tm:08x},0\n")
+            self.h = lib.ref_tiler_create(REF_MODELS[model], path.encode(), n_params)
+        finally:
+            os.unlink(path)
+        if not self.h:
+            raise RuntimeError("ref_tiler_create failed")
+
+    def walk(self, t, steps, seed) -> np.ndarray:
+        a, n = _tiling(t)
+        _check(ref().ref_tiler_walk(self.h, a.ctypes.data, a.size, steps, seed), "ref_tiler_walk")
+        return a
+
+    def walk_epochs(self, t, steps, seeds) -> np.ndarray:
+        a, n = _tiling(t)
+        st = np.ascontiguousarray(steps, dtype=np.int64)
+        se = np.ascontiguousarray(seeds, dtype=np.int64)
+        _check(ref().ref_tiler_walk_epochs(self.h, a.ctypes.data, a.size, st.ctypes.data, se.ctypes.data, st.size),
+               "ref_tiler_walk_epochs")
+        return a
+
+    def close(self):
+        if self.h:
+            ref().ref_tiler_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+BUILD = {
+    "domino_rectangle": 0, "domino_aztec": 1, "domino_aztec_rectangle": 2, "domino_max": 3, "domino_min": 4,
+    "domino_vertices": 5, "domino_tiling_to_domain": 6, "domino_h2t": 7, "domino_t2h": 8,
+    "lozenge_almost_hex": 10, "lozenge_max": 11, "lozenge_min": 12, "lozenge_vertices": 13,
+    "lozenge_tiling_to_domain": 14, "lozenge_h2t": 15, "lozenge_t2h": 16,
+    "recttri_max_hex": 20, "recttri_min_hex": 21, "recttri_slope_hex": 22, "recttri_from_lozenge": 23,
+    "tridimer_ice_cream_cone": 30, "tridimer_test_butterfly": 31, "tridimer_triangle_flips": 32,
+    "tridimer_butterfly_flips": 33, "tridimer_vertices": 34, "tridimer_domain": 35, "tridimer_dimer_indicator": 36,
+}
+
+
+def ref_build(what: str, a=None, b=None, p0: int = 0, p1: int = 0) -> np.ndarray:
+    lib = ref()
+    A = None if a is None else np.ascontiguousarray(a, dtype=np.int32).reshape(-1)
+    B = None if b is None else np.ascontiguousarray(b, dtype=np.int32).reshape(-1)
+    args = (BUILD[what], None if A is None else A.ctypes.data, 0 if A is None else A.size,
+            None if B is None else B.ctypes.data, 0 if B is None else B.size, p0, p1)
+    n = lib.ref_build(*args, None, 0)
+    if n < 0:
+        raise RuntimeError(f"ref_build({what}) failed")
+    out = np.zeros(max(n, 1), dtype=np.int32)
+    lib.ref_build(*args, out.ctypes.data, n)
+    return out[:n]

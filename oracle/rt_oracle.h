@@ -1,0 +1,75 @@
+/* rt_oracle.h -- CPU restatement of RandomTilings' flip dynamics.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker the CUDA product is compared
+ * against: only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline /
+ * reference arm may load it.  The product library never links it.
+ *
+ * Parity of this restatement is pinned against the reference's own code
+ * (oracle/_ref/libref.so: the reference kernels and Tiler classes compiled unmodified
+ * through oracle/shim) by tests/test_oracle_pins.py and the golden fixtures in
+ * tests/golden/.
+ *
+ * Conventions shared by every walk:
+ *   - tilings are int32 N x N, row-major, exactly the reference's `tiling`;
+ *   - `params` is the TinyMT parameter table, 3 uint32 per work-item id
+ *     (mat1, mat2, tmat); NULL means the TinyMT32J constants for every id
+ *     (src/TinyMT/tinymt32def.h:47-49);
+ *   - return 0 on success, a negative ORC_E* code otherwise.
+ */
+#ifndef RT_ORACLE_H
+#define RT_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    ORC_OK = 0,
+    ORC_EINVAL = -1,   /* bad size / argument */
+    ORC_EPARAMS = -2,  /* parameter table too short */
+    ORC_ENOMEM = -3
+};
+
+/* q-lozenge acceptance arithmetic: qlozengekernel.cl:25 compares the double
+ * literal q against a float; an fp32-only device rounds q to float first. */
+enum { ORC_QCMP_FLOAT32 = 0, ORC_QCMP_DOUBLE = 1 };
+
+/* ---- generators (exposed for unit tests) ---- */
+typedef struct {
+    uint32_t s0, s1, s2, s3, mat1, mat2, tmat;
+} orc_tinymt;
+void orc_tinymt_init(orc_tinymt* st, uint32_t seed);
+uint32_t orc_tinymt_bits12(orc_tinymt* st);  /* raw float bits in [1,2) */
+float orc_tinymt_single01(orc_tinymt* st);
+
+/* std::mt19937 outputs; std::default_random_engine (minstd_rand0) with
+ * std::uniform_int_distribution<int>(0, hi) as libstdc++ implements it. */
+void orc_mt19937_stream(int64_t seed, int64_t n, uint32_t* out);
+void orc_minstd_raw_stream(int64_t seed, int64_t n, uint32_t* out);
+void orc_minstd_uniform_stream(int64_t seed, int64_t n, const int* his, int nhis, int* out);
+
+/* ---- walks ---- */
+int orc_domino_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
+                    int cftp_kernel);
+int orc_domino_walk_epochs(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k,
+                           const uint32_t* params, int64_t nparams, int cftp_kernel);
+/* qmode: 0 = uniform (lozengekernel.cl, char storage); 1 = q-weighted
+ * (qlozengekernel.cl, int storage) with comparison `qcmp`. */
+int orc_lozenge_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
+                     int qmode, double q, int qcmp);
+/* weights: 16 floats indexed by face digit (recttrianglekernel.cl:3-13);
+ * NULL = the reference's all-ones table. */
+int orc_recttri_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
+                     const float* weights);
+int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams);
+
+/* Colour schedules the host loops draw (one entry per step). */
+int orc_domino_colours(int64_t seed, int64_t steps, int single_walk, uint8_t* out);
+int orc_lozenge_colours(int64_t seed, int64_t steps, uint8_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RT_ORACLE_H */

@@ -1,0 +1,106 @@
+"""ctypes binding of include/rt_b200.h (librt_b200.so).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from . import _build
+
+RT_OK = 0
+RT_E_INVAL = -1
+RT_E_PARAMS = -2
+RT_E_NOMEM = -3
+RT_E_CUDA = -4
+RT_E_TIMEOUT = -5
+RT_E_NODEVICE = -6
+RT_E_STATE = -7
+
+RT_DOMINO, RT_LOZENGE, RT_RECTTRI, RT_TRIDIMER = 0, 1, 2, 3
+RT_KERNEL_DEFAULT, RT_KERNEL_CFTP, RT_KERNEL_QWEIGHT = 0, 1, 2
+RT_RNG_TINYMT, RT_RNG_PHILOX = 0, 1
+RT_QCMP_FLOAT32, RT_QCMP_DOUBLE = 0, 1
+
+_STATUS_NAMES = {
+    RT_OK: "RT_OK", RT_E_INVAL: "RT_E_INVAL", RT_E_PARAMS: "RT_E_PARAMS", RT_E_NOMEM: "RT_E_NOMEM",
+    RT_E_CUDA: "RT_E_CUDA", RT_E_TIMEOUT: "RT_E_TIMEOUT", RT_E_NODEVICE: "RT_E_NODEVICE",
+    RT_E_STATE: "RT_E_STATE",
+}
+
+
+class RtError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{_STATUS_NAMES.get(status, status)}: {message}")
+
+
+class RtConfig(ctypes.Structure):
+    _fields_ = [
+        ("model", ctypes.c_int32),
+        ("kernel", ctypes.c_int32),
+        ("rng", ctypes.c_int32),
+        ("qcmp", ctypes.c_int32),
+        ("q", ctypes.c_double),
+        ("weights", ctypes.c_float * 16),
+        ("device", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("stream", ctypes.c_void_p),
+    ]
+
+
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+
+# name -> (restype, argtypes); every symbol the header declares.
+SIGNATURES = {
+    "rt_config_default": (None, [ctypes.POINTER(RtConfig), _I32]),
+    "rt_create": (ctypes.c_int, [ctypes.POINTER(RtConfig), ctypes.POINTER(_P)]),
+    "rt_destroy": (ctypes.c_int, [_P]),
+    "rt_load_rng_params": (ctypes.c_int, [_P, ctypes.c_char_p, _I64]),
+    "rt_set_rng_params": (ctypes.c_int, [_P, _P, _I64]),
+    "rt_walk": (ctypes.c_int, [_P, _P, _I32, _I64, _I64]),
+    "rt_walk_epochs": (ctypes.c_int, [_P, _P, _I32, _P, _P, _I32]),
+    "rt_upload": (ctypes.c_int, [_P, _P, _I32]),
+    "rt_run": (ctypes.c_int, [_P, _I64, _I64]),
+    "rt_download": (ctypes.c_int, [_P, _P]),
+    "rt_synchronize": (ctypes.c_int, [_P]),
+    "rt_stream": (_P, [_P]),
+    "rt_last_run_info": (ctypes.c_int, [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
+    "rt_last_error": (ctypes.c_char_p, [_P]),
+    "rt_version": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True) -> ctypes.CDLL:
+    """Loads librt_b200.so (building it in-tree first if allowed)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise OSError(f"native library {path} is missing; run randomtilings_b200._build.build()")
+        _build.build()
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int, handle=None) -> None:
+    if status != RT_OK:
+        lib = load()
+        msg = lib.rt_last_error(handle)
+        raise RtError(status, msg.decode() if msg else "")

@@ -1,0 +1,509 @@
+// rt_capi.cu -- the C ABI (include/rt_b200.h): handles, schedules, transfers.
+//
+// The host side of a walk follows the reference's Walk methods: the colour
+// of every step comes from the same libstdc++ engines the reference uses on
+// its host (std::mt19937 for dominoes, DominoTiler.cpp:31-42;
+// std::default_random_engine + uniform_int_distribution<int>(0,2) for the
+// three-colour models, LozengeTiler.cpp:50-55, RectTriangleTiler.cpp:41-48),
+// drawn once per call into a phase list that the device walks in one launch.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "rt_internal.h"
+#include "rt_models.cuh"
+
+using namespace rtb;
+
+namespace {
+
+constexpr uint32_t kMat1 = 0x8f7011eeu;  // TinyMT32J, src/TinyMT/tinymt32def.h:47-49
+constexpr uint32_t kMat2 = 0xfc78ff1fu;
+constexpr uint32_t kTmat = 0x3793fdffu;
+
+thread_local std::string g_create_error;
+
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    bool reserve(size_t bytes) {
+        if (bytes <= cap) return true;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        if (cudaMallocHost(&p, bytes) != cudaSuccess) return false;
+        cap = bytes;
+        return true;
+    }
+    ~PinnedBuf() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    bool reserve(size_t bytes) {
+        if (bytes <= cap) return true;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return false;
+        cap = bytes;
+        return true;
+    }
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+// Integer threshold K with  (k * 2^-23 < x)  <=>  (k < K)  for k in [0, 2^23).
+uint32_t below_threshold(double x) {
+    const double s = std::ceil(x * 8388608.0);
+    if (s <= 0) return 0;
+    if (s >= 4294967295.0) return 0xffffffffu;
+    return (uint32_t)s;
+}
+// Largest K with  K <= x * 2^e  (clamped to [0, 2^32-1]).
+uint32_t floor_scaled(double x, int e) {
+    const double s = std::floor(std::ldexp(x, e));
+    if (s <= 0) return 0;
+    if (s >= 4294967295.0) return 0xffffffffu;
+    return (uint32_t)s;
+}
+
+}  // namespace
+
+struct rt_tiler {
+    rt_config cfg{};
+    int family = 0;
+    int ncol = 0;     // colour arrays
+    int kind = 0;     // split layout (0 domino, 1 lozenge, 2 rect-triangle)
+    int elem = 1;     // bytes per stored site
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+
+    std::vector<uint32_t> table;  // 3 per id
+    bool table_dirty = false;
+    DevBuf d_params;
+    int64_t d_params_n = 0;
+
+    int n = 0, rows = 0, cols = 0;
+    int nlat = 1;
+    DevBuf d_arr_block;  // all colour arrays of all lattices
+    void* d_arr[2][8] = {};
+    DevBuf d_tiling;
+    bool uploaded = false;
+
+    DevBuf d_phases, d_epoch_start, d_epoch_seed, d_flags, d_err;
+    PinnedBuf h_phases, h_epoch_start, h_epoch_seed, h_err;
+    cudaEvent_t ev_staged = nullptr;
+
+    WalkPlan plan;
+    int plan_rows = -1, plan_cols = -1;
+    int64_t last_phases = 0, last_launches = 0;
+    uint64_t timeout_ns = 5000000000ull;
+
+    rt_status fail(rt_status s, const std::string& msg) {
+        err = msg;
+        return s;
+    }
+    rt_status cuda_fail(cudaError_t e, const char* what) {
+        return fail(RT_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+};
+
+extern "C" {
+
+const char* rt_version(void) { return "randomtilings_b200 0.1 (sm_100a)"; }
+
+void rt_config_default(rt_config* cfg, int32_t model) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof *cfg);
+    cfg->model = model;
+    cfg->kernel = RT_KERNEL_DEFAULT;
+    cfg->rng = RT_RNG_TINYMT;
+    cfg->qcmp = RT_QCMP_FLOAT32;
+    cfg->q = 0.99;  // qlozengekernel.cl:3
+    cfg->weights[0] = 0.0f;  // recttrianglekernel.cl:13
+    for (int i = 1; i < 16; ++i) cfg->weights[i] = 1.0f;
+    cfg->device = 0;
+    cfg->stream = nullptr;
+}
+
+rt_status rt_create(const rt_config* cfg, rt_tiler** out) {
+    if (!cfg || !out) {
+        g_create_error = "null argument";
+        return RT_E_INVAL;
+    }
+    *out = nullptr;
+    int family = -1, ncol = 0, kind = 0, elem = 1;
+    switch (cfg->model) {
+        case RT_DOMINO:
+            if (cfg->kernel != RT_KERNEL_DEFAULT && cfg->kernel != RT_KERNEL_CFTP) break;
+            family = cfg->kernel == RT_KERNEL_CFTP ? FAM_DOMINO_HB : FAM_DOMINO;
+            ncol = 2, kind = 0, elem = 1;
+            break;
+        case RT_LOZENGE:
+            if (cfg->kernel == RT_KERNEL_DEFAULT) family = FAM_LOZENGE8, elem = 1;
+            else if (cfg->kernel == RT_KERNEL_QWEIGHT) family = FAM_QLOZENGE32, elem = 4;
+            ncol = 3, kind = 1;
+            break;
+        case RT_RECTTRI:
+            if (cfg->kernel != RT_KERNEL_DEFAULT) break;
+            family = FAM_RECTTRI, ncol = 3, kind = 2, elem = 4;
+            break;
+        default:
+            break;
+    }
+    if (family < 0) {
+        g_create_error = "unsupported model/kernel combination";
+        return RT_E_INVAL;
+    }
+    if (cfg->rng != RT_RNG_TINYMT) {
+        g_create_error = "rng mode not available for this model";
+        return RT_E_INVAL;
+    }
+    if (family == FAM_QLOZENGE32 && (!(cfg->q >= 0.0) || !std::isfinite(cfg->q))) {
+        g_create_error = "q must be a finite non-negative number";
+        return RT_E_INVAL;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) {
+        g_create_error = "no CUDA device with that ordinal";
+        return RT_E_NODEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || prop.major != 10) {
+        g_create_error = "device is not sm_100 (this library carries sm_100a code only)";
+        return RT_E_NODEVICE;
+    }
+    if (!prop.cooperativeLaunch) {
+        g_create_error = "device does not support cooperative launches";
+        return RT_E_NODEVICE;
+    }
+    cudaSetDevice(cfg->device);
+    rt_tiler* h = new rt_tiler();
+    h->cfg = *cfg;
+    h->family = family;
+    h->ncol = ncol;
+    h->kind = kind;
+    h->elem = elem;
+    if (cfg->stream) {
+        h->stream = static_cast<cudaStream_t>(cfg->stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete h;
+            g_create_error = "cudaStreamCreate failed";
+            return RT_E_CUDA;
+        }
+        h->own_stream = true;
+    }
+    if (cudaEventCreateWithFlags(&h->ev_staged, cudaEventDisableTiming) != cudaSuccess) {
+        if (h->own_stream) cudaStreamDestroy(h->stream);
+        delete h;
+        g_create_error = "cudaEventCreate failed";
+        return RT_E_CUDA;
+    }
+    if (const char* t = std::getenv("RT_WAIT_TIMEOUT_MS")) {
+        const long ms = std::atol(t);
+        if (ms > 0) h->timeout_ns = (uint64_t)ms * 1000000ull;
+    }
+    *out = h;
+    return RT_OK;
+}
+
+rt_status rt_destroy(rt_tiler* h) {
+    if (!h) return RT_E_INVAL;
+    cudaSetDevice(h->cfg.device);
+    cudaStreamSynchronize(h->stream);
+    if (h->ev_staged) cudaEventDestroy(h->ev_staged);
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return RT_OK;
+}
+
+const char* rt_last_error(rt_tiler* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+void* rt_stream(rt_tiler* h) { return h ? static_cast<void*>(h->stream) : nullptr; }
+
+rt_status rt_set_rng_params(rt_tiler* h, const uint32_t* table, int64_t n) {
+    if (!h || (!table && n > 0) || n < 0) return h ? h->fail(RT_E_INVAL, "bad parameter table") : RT_E_INVAL;
+    h->table.assign(table, table + 3 * n);
+    h->table_dirty = true;
+    return RT_OK;
+}
+
+// The layout src/TinyMT/file_reader.cpp:51-70,139-166 reads: lines starting
+// with '#' are skipped; mat1, mat2 and tmat are the hexadecimal fields after
+// the 3rd, 4th and 5th comma.
+rt_status rt_load_rng_params(rt_tiler* h, const char* path, int64_t n) {
+    if (!h || !path || n < 0) return h ? h->fail(RT_E_INVAL, "bad arguments") : RT_E_INVAL;
+    std::ifstream in(path);
+    if (!in) return h->fail(RT_E_PARAMS, std::string("cannot open parameter file ") + path);
+    std::vector<uint32_t> t;
+    t.reserve((size_t)(3 * n));
+    std::string line;
+    int64_t got = 0;
+    while (got < n && std::getline(in, line)) {
+        if (!line.empty() && line[0] == '#') continue;
+        size_t pos[5];
+        int commas = 0;
+        for (size_t i = 0; i < line.size() && commas < 5; ++i)
+            if (line[i] == ',') pos[commas++] = i;
+        if (commas < 5) return h->fail(RT_E_PARAMS, "parameter line " + std::to_string(got) + ": comma not found");
+        for (int f = 2; f < 5; ++f) t.push_back((uint32_t)std::strtoul(line.c_str() + pos[f] + 1, nullptr, 16));
+        ++got;
+    }
+    if (got < n) return h->fail(RT_E_PARAMS, "parameter file has " + std::to_string(got) + " entries, need " + std::to_string(n));
+    h->table.swap(t);
+    h->table_dirty = true;
+    return RT_OK;
+}
+
+static rt_status check_size(rt_tiler* h, int n) {
+    if (h->kind == 0 && (n < 6 || n % 2 != 0)) return h->fail(RT_E_INVAL, "domino tiling side must be even and >= 6");
+    if (h->kind != 0 && (n < 9 || n % 3 != 0))
+        return h->fail(RT_E_INVAL, "tiling side must be a multiple of 3 and >= 9");
+    return RT_OK;
+}
+
+static void grid_of(const rt_tiler* h, int n, int* rows, int* cols) {
+    if (h->kind == 0) {  // Rotate NDRange (N-2, N/2-2), DominoTiler.cpp:37
+        *rows = n - 2;
+        *cols = n / 2 - 2;
+    } else {  // (N, N/3), LozengeTiler.cpp:58, RectTriangleTiler.cpp:51
+        *rows = n;
+        *cols = n / 3;
+    }
+}
+
+rt_status rt_upload(rt_tiler* h, const int32_t* tiling, int32_t n) {
+    if (!h || !tiling) return h ? h->fail(RT_E_INVAL, "null tiling") : RT_E_INVAL;
+    rt_status s = check_size(h, n);
+    if (s != RT_OK) return s;
+    cudaSetDevice(h->cfg.device);
+    const size_t per_arr = (size_t)n * (size_t)(n / h->ncol) * (size_t)h->elem;
+    const size_t per_arr_al = (per_arr + 255) & ~(size_t)255;
+    if (!h->d_arr_block.reserve(per_arr_al * h->ncol * 2)) return h->fail(RT_E_NOMEM, "cudaMalloc lattice");
+    if (!h->d_tiling.reserve((size_t)n * n * 4)) return h->fail(RT_E_NOMEM, "cudaMalloc tiling");
+    for (int l = 0; l < 2; ++l)
+        for (int c = 0; c < 8; ++c)
+            h->d_arr[l][c] = c < h->ncol ? static_cast<char*>(h->d_arr_block.p) + (l * h->ncol + c) * per_arr_al : nullptr;
+    cudaError_t e = cudaMemcpyAsync(h->d_tiling.p, tiling, (size_t)n * n * 4, cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "upload");
+    s = launch_split(false, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0], h->stream,
+                     &h->err);
+    if (s != RT_OK) return s;
+    if (!h->d_err.reserve(sizeof(int)) || !h->h_err.reserve(sizeof(int))) return h->fail(RT_E_NOMEM, "error word");
+    e = cudaMemsetAsync(h->d_err.p, 0, sizeof(int), h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "memset");
+    h->n = n;
+    grid_of(h, n, &h->rows, &h->cols);
+    h->uploaded = true;
+    return RT_OK;
+}
+
+rt_status rt_download(rt_tiler* h, int32_t* tiling) {
+    if (!h || !tiling) return h ? h->fail(RT_E_INVAL, "null tiling") : RT_E_INVAL;
+    if (!h->uploaded) return h->fail(RT_E_STATE, "download before upload");
+    cudaSetDevice(h->cfg.device);
+    const int n = h->n;
+    rt_status s = launch_split(true, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0],
+                               h->stream, &h->err);
+    if (s != RT_OK) return s;
+    cudaError_t e = cudaMemcpyAsync(tiling, h->d_tiling.p, (size_t)n * n * 4, cudaMemcpyDeviceToHost, h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "download");
+    return rt_synchronize(h);
+}
+
+rt_status rt_synchronize(rt_tiler* h) {
+    if (!h) return RT_E_INVAL;
+    cudaSetDevice(h->cfg.device);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "stream synchronize");
+    if (h->uploaded) {
+        e = cudaMemcpy(h->h_err.p, h->d_err.p, sizeof(int), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return h->cuda_fail(e, "error word readback");
+        const int code = *static_cast<int*>(h->h_err.p);
+        if (code & ERR_TIMEOUT) return h->fail(RT_E_TIMEOUT, "a bounded wait between CTAs timed out; walk aborted");
+        if (code) return h->fail(RT_E_CUDA, "device error word " + std::to_string(code));
+    }
+    return RT_OK;
+}
+
+// Stages the TinyMT parameter table on the device (all ids the walk uses).
+static rt_status stage_params(rt_tiler* h, int64_t needed) {
+    if (h->table.empty()) return RT_OK;  // uniform TinyMT32J parameters
+    const int64_t have = (int64_t)h->table.size() / 3;
+    if (have < needed)
+        return h->fail(RT_E_PARAMS, "parameter table has " + std::to_string(have) + " entries, the walk needs " +
+                                         std::to_string(needed));
+    if (!h->table_dirty && h->d_params_n >= needed) return RT_OK;
+    std::vector<uint4> p((size_t)needed);
+    for (int64_t i = 0; i < needed; ++i) p[i] = make_uint4(h->table[3 * i], h->table[3 * i + 1], h->table[3 * i + 2], 0u);
+    if (!h->d_params.reserve((size_t)needed * sizeof(uint4))) return h->fail(RT_E_NOMEM, "cudaMalloc params");
+    cudaError_t e = cudaMemcpy(h->d_params.p, p.data(), (size_t)needed * sizeof(uint4), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return h->cuda_fail(e, "params upload");
+    h->d_params_n = needed;
+    h->table_dirty = false;
+    return RT_OK;
+}
+
+// Builds the phase list of `k` epochs and launches the walk.
+static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* seeds, int k, bool single_walk) {
+    if (!h->uploaded) return h->fail(RT_E_STATE, "run before upload");
+    cudaSetDevice(h->cfg.device);
+    int64_t total = 0;
+    for (int e = 0; e < k; ++e) {
+        if (steps[e] < 0) return h->fail(RT_E_INVAL, "negative step count");
+        total += steps[e];
+    }
+    h->last_phases = 0;
+    h->last_launches = 0;
+    if (total == 0) return RT_OK;
+    const int64_t nph = total + 1;  // + the final Update
+    // The staging buffers may still feed the previous run's copies.
+    cudaEventSynchronize(h->ev_staged);
+    if (!h->h_phases.reserve((size_t)nph * 4) || !h->d_phases.reserve((size_t)nph * 4) ||
+        !h->h_epoch_start.reserve((size_t)k * 8) || !h->d_epoch_start.reserve((size_t)k * 8) ||
+        !h->h_epoch_seed.reserve((size_t)k * 4) || !h->d_epoch_seed.reserve((size_t)k * 4))
+        return h->fail(RT_E_NOMEM, "schedule buffers");
+    uint32_t* ph = static_cast<uint32_t*>(h->h_phases.p);
+    int64_t* es = static_cast<int64_t*>(h->h_epoch_start.p);
+    uint32_t* sd = static_cast<uint32_t*>(h->h_epoch_seed.p);
+    int64_t at = 0;
+    uint32_t prev = NO_COLOUR;
+    for (int e = 0; e < k; ++e) {
+        es[e] = at;
+        if (h->kind == 0) {
+            std::mt19937 mt_rand(seeds[e]);
+            sd[e] = single_walk ? (uint32_t)mt_rand() : (uint32_t)seeds[e];  // DominoTiler.cpp:31-32 vs :81-82
+            for (int64_t s = 0; s < steps[e]; ++s) {
+                const uint32_t r = (uint32_t)(mt_rand() % 2);
+                ph[at++] = make_phase(OP_STEP, r, prev, true);
+                prev = r;
+            }
+        } else {
+            std::default_random_engine generator;
+            std::uniform_int_distribution<int> distribution(0, 2);
+            generator.seed(seeds[e]);
+            sd[e] = (uint32_t)seeds[e];  // Walk passes `seed` to InitTinyMT's uint argument
+            for (int64_t s = 0; s < steps[e]; ++s) {
+                const uint32_t r = (uint32_t)distribution(generator);
+                ph[at++] = make_phase(OP_STEP, r, prev, true);
+                prev = r;
+            }
+        }
+    }
+    ph[at++] = make_phase(OP_FINAL, prev, NO_COLOUR, false);
+
+    if (h->plan_rows != h->rows || h->plan_cols != h->cols) {
+        rt_status s = plan_walk(h->family, h->cfg.device, h->rows, h->cols, &h->plan, &h->err);
+        if (s != RT_OK) return s;
+        h->plan_rows = h->rows;
+        h->plan_cols = h->cols;
+    }
+    const int64_t ids = (int64_t)h->rows * h->cols;
+    rt_status s = stage_params(h, ids);
+    if (s != RT_OK) return s;
+    if (!h->d_flags.reserve((size_t)h->plan.ctas * sizeof(unsigned))) return h->fail(RT_E_NOMEM, "flags");
+
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(h->d_phases.p, ph, (size_t)nph * 4, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h->d_epoch_start.p, es, (size_t)k * 8, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h->d_epoch_seed.p, sd, (size_t)k * 4, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+        (e = cudaEventRecord(h->ev_staged, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->d_flags.p, 0, (size_t)h->plan.ctas * sizeof(unsigned), h->stream)) != cudaSuccess)
+        return h->cuda_fail(e, "schedule staging");
+
+    WalkArgs a;
+    std::memset(&a, 0, sizeof a);
+    for (int l = 0; l < 2; ++l)
+        for (int c = 0; c < 8; ++c) a.arr[l][c] = h->d_arr[l][c];
+    a.nlat = h->nlat;
+    a.n = h->n;
+    a.rows = h->rows;
+    a.cols = h->cols;
+    a.rng_kind = 0;
+    a.params = h->table.empty() ? nullptr : static_cast<const uint4*>(h->d_params.p);
+    a.mat1 = kMat1;
+    a.mat2 = kMat2;
+    a.tmat = kTmat;
+    a.phases = static_cast<const uint32_t*>(h->d_phases.p);
+    a.nphases = nph;
+    a.epoch_start = static_cast<const int64_t*>(h->d_epoch_start.p);
+    a.epoch_seed = static_cast<const uint32_t*>(h->d_epoch_seed.p);
+    a.nepochs = k;
+    switch (h->family) {
+        case FAM_DOMINO: a.thr[0] = below_threshold(0.8); break;       // dominokernel.cl:13
+        case FAM_DOMINO_HB: a.thr[0] = below_threshold(0.5); break;    // dominokernelCFTP.cl:22
+        case FAM_LOZENGE8:                                              // lozengekernel.cl:19-21
+            a.thr[0] = below_threshold(0.4);
+            a.thr[1] = below_threshold(0.8);
+            break;
+        case FAM_QLOZENGE32: {  // qlozengekernel.cl:18-26
+            if (h->cfg.qcmp == RT_QCMP_DOUBLE) {
+                a.thr[0] = floor_scaled(h->cfg.q, 22);
+                a.thr[1] = floor_scaled(1.0 / h->cfg.q, 24);
+            } else {
+                const float qf = (float)h->cfg.q;
+                const float inv = 1.0f / qf;
+                a.thr[0] = floor_scaled((double)qf, 22);
+                a.thr[1] = floor_scaled((double)inv, 24);
+            }
+            break;
+        }
+        default: break;
+    }
+    std::memcpy(a.weights, h->cfg.weights, sizeof a.weights);
+    a.flags = static_cast<unsigned*>(h->d_flags.p);
+    a.err = static_cast<int*>(h->d_err.p);
+    a.timeout_ns = h->timeout_ns;
+    s = launch_walk(h->plan, a, h->stream, &h->err);
+    if (s != RT_OK) return s;
+    h->last_phases = nph;
+    h->last_launches = 1;
+    return RT_OK;
+}
+
+rt_status rt_run(rt_tiler* h, int64_t steps, int64_t seed) {
+    if (!h) return RT_E_INVAL;
+    return run_schedule(h, &steps, &seed, 1, true);
+}
+
+rt_status rt_walk(rt_tiler* h, int32_t* tiling, int32_t n, int64_t steps, int64_t seed) {
+    if (!h) return RT_E_INVAL;
+    rt_status s = rt_upload(h, tiling, n);
+    if (s == RT_OK) s = run_schedule(h, &steps, &seed, 1, true);
+    if (s == RT_OK) s = rt_download(h, tiling);
+    return s;
+}
+
+rt_status rt_walk_epochs(rt_tiler* h, int32_t* tiling, int32_t n, const int64_t* steps, const int64_t* seeds,
+                         int32_t k) {
+    if (!h) return RT_E_INVAL;
+    if (h->kind != 0) return h->fail(RT_E_INVAL, "epoch walks exist for dominoes only (DominoTiler.h:76)");
+    if (k < 0 || (k > 0 && (!steps || !seeds))) return h->fail(RT_E_INVAL, "bad epoch arrays");
+    rt_status s = rt_upload(h, tiling, n);
+    if (s == RT_OK && k > 0) s = run_schedule(h, steps, seeds, k, false);
+    if (s == RT_OK) s = rt_download(h, tiling);
+    return s;
+}
+
+rt_status rt_last_run_info(rt_tiler* h, int64_t* phases, int64_t* launches) {
+    if (!h) return RT_E_INVAL;
+    if (phases) *phases = h->last_phases;
+    if (launches) *launches = h->last_launches;
+    return RT_OK;
+}
+
+}  // extern "C"

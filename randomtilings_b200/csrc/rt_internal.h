@@ -1,0 +1,36 @@
+// rt_internal.h -- declarations shared by the C-ABI layer and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/rt_b200.h"
+
+namespace rtb {
+
+struct WalkArgs;
+
+enum Family : int {
+    FAM_DOMINO = 0,      // dominokernel.cl, int8
+    FAM_DOMINO_HB = 1,   // dominokernelCFTP.cl, int8
+    FAM_LOZENGE8 = 2,    // lozengekernel.cl, int8
+    FAM_QLOZENGE32 = 3,  // qlozengekernel.cl, int32
+    FAM_RECTTRI = 4      // recttrianglekernel.cl, int32
+};
+
+struct WalkPlan {
+    int items = 0;
+    int block = 0;
+    int rows_per_cta = 0;
+    int ctas = 0;
+    const void* fn = nullptr;
+};
+
+rt_status plan_walk(int family, int device, int rows, int cols, WalkPlan* plan, std::string* err);
+rt_status launch_walk(const WalkPlan& plan, WalkArgs& args, cudaStream_t stream, std::string* err);
+// kind: 0 domino, 1 lozenge, 2 rect-triangle.
+rt_status launch_split(bool merge, int elem_bytes, int kind, int ncol, int n, int32_t* tiling, void* const* arr,
+                       cudaStream_t stream, std::string* err);
+
+}  // namespace rtb

@@ -1,0 +1,141 @@
+"""Python mirror of the reference's per-model Tiler classes over the C ABI.
+
+Method names and argument meanings follow the reference
+(src/Domino/DominoTiler.h, src/Lozenge/LozengeTiler.h,
+src/RectTriangle/RectTriangleTiler.h, src/TriangleDimer/TriangleDimerTiler.h):
+``LoadTinyMT(path, size)`` and ``Walk(tiling, steps, seed)`` mutate the
+caller's tiling in place.  The OpenCL (context, queue, devices, source)
+constructor arguments become a device ordinal plus kernel options.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi
+from ._capi import check
+
+
+def _as_tiling(t) -> tuple[np.ndarray, int]:
+    arr = np.ascontiguousarray(t, dtype=np.int32).reshape(-1)
+    n = int(round(arr.size ** 0.5))
+    if n * n != arr.size:
+        raise ValueError(f"tiling of {arr.size} entries is not square")
+    return arr, n
+
+
+def _writeback(dst, src: np.ndarray) -> None:
+    if isinstance(dst, np.ndarray):
+        if dst.dtype == np.int32 and dst.flags.c_contiguous:
+            if not np.shares_memory(dst, src):
+                dst.reshape(-1)[:] = src
+        else:
+            dst.reshape(-1)[:] = src
+    elif isinstance(dst, list):
+        dst[:] = src.tolist()
+    else:
+        raise TypeError("tiling must be a numpy array or a list")
+
+
+class _Tiler:
+    MODEL = -1
+
+    def __init__(self, device: int = 0, kernel: int = _capi.RT_KERNEL_DEFAULT, rng: int = _capi.RT_RNG_TINYMT,
+                 q: float = 0.99, qcmp: int = _capi.RT_QCMP_FLOAT32, weights=None, stream=None):
+        self._lib = _capi.load()
+        cfg = _capi.RtConfig()
+        self._lib.rt_config_default(ctypes.byref(cfg), self.MODEL)
+        cfg.kernel = kernel
+        cfg.rng = rng
+        cfg.q = q
+        cfg.qcmp = qcmp
+        cfg.device = device
+        if weights is not None:
+            for i, w in enumerate(weights):
+                cfg.weights[i] = float(w)
+        cfg.stream = stream
+        h = ctypes.c_void_p()
+        check(self._lib.rt_create(ctypes.byref(cfg), ctypes.byref(h)), None)
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.rt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, status: int) -> None:
+        check(status, self._h)
+
+    # -- reference methods -------------------------------------------------
+    def LoadTinyMT(self, params: str, size: int) -> None:
+        self._check(self._lib.rt_load_rng_params(self._h, params.encode(), int(size)))
+
+    def SetTinyMTTable(self, table) -> None:
+        tab = np.ascontiguousarray(table, dtype=np.uint32).reshape(-1)
+        self._check(self._lib.rt_set_rng_params(self._h, tab.ctypes.data, tab.size // 3))
+
+    def Walk(self, t, steps: int, seed: int) -> None:
+        arr, n = _as_tiling(t)
+        self._check(self._lib.rt_walk(self._h, arr.ctypes.data, n, int(steps), int(seed)))
+        _writeback(t, arr)
+
+    # -- device-resident form ---------------------------------------------
+    def upload(self, t) -> None:
+        arr, n = _as_tiling(t)
+        self._check(self._lib.rt_upload(self._h, arr.ctypes.data, n))
+        self._check(self._lib.rt_synchronize(self._h))
+
+    def run(self, steps: int, seed: int) -> None:
+        self._check(self._lib.rt_run(self._h, int(steps), int(seed)))
+
+    def download(self, out: np.ndarray) -> None:
+        self._check(self._lib.rt_download(self._h, out.ctypes.data))
+
+    def synchronize(self) -> None:
+        self._check(self._lib.rt_synchronize(self._h))
+
+    @property
+    def stream(self) -> int:
+        return self._lib.rt_stream(self._h) or 0
+
+    def last_run_info(self) -> tuple[int, int]:
+        ph, la = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self._lib.rt_last_run_info(self._h, ctypes.byref(ph), ctypes.byref(la)))
+        return ph.value, la.value
+
+
+class DominoTiler(_Tiler):
+    MODEL = _capi.RT_DOMINO
+
+    def Walk(self, t, steps, seed=None) -> None:  # noqa: N802 -- reference name
+        """Walk(t, steps, seed) or Walk(t, [steps...], [seeds...]) (DominoTiler.h:73,76)."""
+        if isinstance(steps, (list, tuple, np.ndarray)):
+            st = np.ascontiguousarray(steps, dtype=np.int64)
+            se = np.ascontiguousarray(seed, dtype=np.int64)
+            if st.size != se.size:
+                raise ValueError("steps and seeds must have the same length")
+            arr, n = _as_tiling(t)
+            self._check(self._lib.rt_walk_epochs(self._h, arr.ctypes.data, n, st.ctypes.data, se.ctypes.data,
+                                                 int(st.size)))
+            _writeback(t, arr)
+        else:
+            super().Walk(t, steps, seed)
+
+
+class LozengeTiler(_Tiler):
+    MODEL = _capi.RT_LOZENGE
+
+
+class RectTriangleTiler(_Tiler):
+    MODEL = _capi.RT_RECTTRI
+
+
+class TriangleDimerTiler(_Tiler):
+    MODEL = _capi.RT_TRIDIMER

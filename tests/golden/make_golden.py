@@ -1,0 +1,198 @@
+"""Regenerates the golden fixtures in this directory from the reference itself.
+
+Run from the repository root, on a machine that has the reference source tree
+(REF, default /root/reference) and has built oracle/_ref/libref.so
+(`make -C oracle ref`):
+
+    python tests/golden/make_golden.py
+
+Everything here comes out of the reference's own code (its Tiler classes and
+OpenCL kernels compiled for the CPU through oracle/shim): domains, extremal
+tilings, height functions, and walk results for fixed seeds.  The reference's
+deterministic example outputs (Examples/ExampleOuts) are checked against the
+same code and recorded by SHA-256.  The GPU tests read only the .npz/.json
+files written here; nothing reads the reference tree at test time.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
+sys.path.insert(0, ROOT)
+from oracle import pyoracle as po  # noqa: E402
+
+REF = os.environ.get("REF", "/root/reference")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def side(a) -> int:
+    return int(round(np.asarray(a).size ** 0.5))
+
+
+def builders() -> dict:
+    b = po.ref_build
+    out = {}
+    for n in (1, 2, 3, 5, 8, 13, 100):
+        d = b("domino_aztec", p0=n)
+        tmin, tmax = b("domino_min", d), b("domino_max", d)
+        out[f"domino/aztec{n}/domain"] = d
+        out[f"domino/aztec{n}/min"] = tmin
+        out[f"domino/aztec{n}/max"] = tmax
+        if n <= 13:
+            out[f"domino/aztec{n}/vertices"] = b("domino_vertices", d)
+            out[f"domino/aztec{n}/hmin"] = b("domino_t2h", tmin, d)
+            out[f"domino/aztec{n}/hmax"] = b("domino_t2h", tmax, d)
+            out[f"domino/aztec{n}/tiling_to_domain"] = b("domino_tiling_to_domain", tmin)
+    for (m, n) in ((2, 2), (4, 6), (5, 8), (7, 7)):
+        d = b("domino_rectangle", p0=m, p1=n)
+        out[f"domino/rect{m}x{n}/domain"] = d
+        out[f"domino/rect{m}x{n}/min"] = b("domino_min", d)
+        out[f"domino/rect{m}x{n}/max"] = b("domino_max", d)
+    for (n, rem) in ((4, (1,)), (6, (0, 2)), (7, (1, 3, 5))):
+        d = b("domino_aztec_rectangle", np.array(rem, dtype=np.int32), p0=n)
+        out[f"domino/aztecrect{n}_{'_'.join(map(str, rem))}/domain"] = d
+    for (n, m) in ((2, 0), (4, 0), (4, 1), (10, 2), (13, 5), (20, 0)):
+        d = b("lozenge_almost_hex", p0=n, p1=m)
+        tmin, tmax = b("lozenge_min", d), b("lozenge_max", d)
+        out[f"lozenge/hex{n}_{m}/domain"] = d
+        out[f"lozenge/hex{n}_{m}/min"] = tmin
+        out[f"lozenge/hex{n}_{m}/max"] = tmax
+        out[f"lozenge/hex{n}_{m}/vertices"] = b("lozenge_vertices", d)
+        out[f"lozenge/hex{n}_{m}/hmin"] = b("lozenge_t2h", tmin, d)
+        out[f"lozenge/hex{n}_{m}/hmax"] = b("lozenge_t2h", tmax, d)
+        out[f"lozenge/hex{n}_{m}/tiling_to_domain"] = b("lozenge_tiling_to_domain", tmin)
+        out[f"lozenge/hex{n}_{m}/recttri"] = b("recttri_from_lozenge", tmin, d)
+    for n in (1, 2, 3, 5, 6, 9, 20):
+        for kind in ("max_hex", "min_hex", "slope_hex"):
+            out[f"recttri/{kind}{n}"] = b(f"recttri_{kind}", p0=n)
+    for (n, m) in ((6, 0), (5, 0), (8, 2), (10, 3), (12, 0)):
+        t = b("tridimer_ice_cream_cone", p0=n, p1=m)
+        out[f"tridimer/cone{n}_{m}/tiling"] = t
+        out[f"tridimer/cone{n}_{m}/triangle_flips"] = b("tridimer_triangle_flips", t)
+        out[f"tridimer/cone{n}_{m}/butterfly_flips"] = b("tridimer_butterfly_flips", t)
+        out[f"tridimer/cone{n}_{m}/vertices"] = b("tridimer_vertices", t)
+        out[f"tridimer/cone{n}_{m}/domain"] = b("tridimer_domain", t)
+        for c in range(3):
+            out[f"tridimer/cone{n}_{m}/dimer{c}"] = b("tridimer_dimer_indicator", t, p0=c)
+    for k in range(3):
+        out[f"tridimer/butterfly{k}"] = b("tridimer_test_butterfly", p0=k)
+    return out
+
+
+def walks(start: dict) -> dict:
+    out = {}
+    cases = []
+    for n in (5, 13):
+        t = start[f"domino/aztec{n}/min"]
+        for cftp in (0, 1):
+            for seed in (42, 34893, -7):
+                cases.append(("domino_cftp" if cftp else "domino", f"domino{'_cftp' if cftp else ''}/aztec{n}/s{seed}",
+                              t, 300, seed))
+    for key in ("lozenge/hex4_1", "lozenge/hex10_2", "lozenge/hex13_5"):
+        t = start[f"{key}/min"]
+        for model in ("lozenge", "qlozenge"):
+            for seed in (42, 5):
+                cases.append((model, f"{model}/{key.split('/')[1]}/s{seed}", t, 700, seed))
+    for n in (2, 5, 9):
+        for kind in ("min_hex", "max_hex", "slope_hex"):
+            t = start[f"recttri/{kind}{n}"]
+            for seed in (42, 1234):
+                cases.append(("recttri", f"recttri/{kind}{n}/s{seed}", t, 500, seed))
+    for key in ("tridimer/cone6_0", "tridimer/cone8_2", "tridimer/cone10_3"):
+        t = start[f"{key}/tiling"]
+        for seed in (42, 7):
+            cases.append(("tridimer", f"tridimer/{key.split('/')[1]}/s{seed}", t, 400, seed))
+    for model, key, t, steps, seed in cases:
+        rt = po.RefTiler(model, side(t) ** 2)
+        out[f"{key}/start"] = t
+        out[f"{key}/steps"] = np.array([steps])
+        out[f"{key}/seed"] = np.array([seed])
+        out[f"{key}/end"] = rt.walk(t, steps, seed)
+        rt.close()
+    # multi-epoch CFTP walks (DominoTiler.cpp:58-107)
+    for n in (5, 13):
+        for which in ("min", "max"):
+            t = start[f"domino/aztec{n}/{which}"]
+            st, se = np.array([256, 128], dtype=np.int64), np.array([2718281, 345903], dtype=np.int64)
+            rt = po.RefTiler("domino_cftp", side(t) ** 2 // 2)
+            key = f"domino_epochs/aztec{n}/{which}"
+            out[f"{key}/start"] = t
+            out[f"{key}/steps"] = st
+            out[f"{key}/seeds"] = se
+            out[f"{key}/end"] = rt.walk_epochs(t, st, se)
+            rt.close()
+    return out
+
+
+def config0(start: dict) -> dict:
+    """Aztec diamond n=100 from the minimal tiling, seed 42."""
+    out = {}
+    t = start["domino/aztec100/min"]
+    d = start["domino/aztec100/domain"]
+    rt = po.RefTiler("domino", side(t) ** 2 // 2, threads=os.cpu_count() or 1)
+    for steps in (10000, 20000):
+        t0 = time.time()
+        end = rt.walk(t, steps, 42)
+        print(f"  cfg0 {steps} steps: {time.time() - t0:.1f}s", flush=True)
+        out[f"cfg0/s{steps}/end"] = end
+        out[f"cfg0/s{steps}/height"] = po.ref_build("domino_t2h", end, d)
+    rt.close()
+    return out
+
+
+def example_outputs() -> dict:
+    """SHA-256 of the deterministic Examples/ExampleOuts files, each checked
+    against the reference's code run here."""
+    ex = os.path.join(REF, "Examples", "ExampleOuts")
+    rec = {}
+    b = po.ref_build
+    for n, name in ((5, "MaxTiling"), (5, "MinTiling"), (5, "SlopeTiling")):
+        kind = {"MaxTiling": "max_hex", "MinTiling": "min_hex", "SlopeTiling": "slope_hex"}[name]
+        t = b(f"recttri_{kind}", p0=n)
+        got = np.loadtxt(os.path.join(ex, "RectTriangle", f"{name}.txt"), dtype=np.int64).reshape(-1)
+        assert (got == t).all(), name
+        for ext in ("txt", "svg"):
+            p = os.path.join(ex, "RectTriangle", f"{name}.{ext}")
+            rec[f"RectTriangle/{name}.{ext}"] = hashlib.sha256(open(p, "rb").read()).hexdigest()
+    t = b("tridimer_ice_cream_cone", p0=6, p1=0)
+    d = b("tridimer_domain", t)
+    assert (np.loadtxt(os.path.join(ex, "TriangleDimer", "DimerStart.txt"), dtype=np.int64).reshape(-1) == t).all()
+    # SaveMatrix writes sqrt(size) x sqrt(size) entries (common.cpp:169-171); the
+    # (M-1) x 2(M-1) domain is therefore saved truncated to its first k*k values.
+    saved = np.loadtxt(os.path.join(ex, "TriangleDimer", "Domain.txt"), dtype=np.int64).reshape(-1)
+    assert (saved == d[: saved.size]).all()
+    for f in ("DimerStart.txt", "Domain.txt", "Domain.svg", "DimerStart.svg", "TilingStart.svg"):
+        rec[f"TriangleDimer/{f}"] = hashlib.sha256(open(os.path.join(ex, "TriangleDimer", f), "rb").read()).hexdigest()
+    for f in ("domainAlmostHex.svg", "tilingStartAlmostHex.svg"):
+        rec[f"MinimalLozenge/{f}"] = hashlib.sha256(open(os.path.join(ex, "MinimalLozenge", f), "rb").read()).hexdigest()
+    rec["MinimalDomino/StartTiling.svg"] = hashlib.sha256(
+        open(os.path.join(ex, "MinimalDomino", "StartTiling.svg"), "rb").read()).hexdigest()
+    return rec
+
+
+def main() -> None:
+    if not po.have_ref():
+        sys.exit("oracle/_ref/libref.so is missing: run `make -C oracle ref` where the reference tree exists")
+    t0 = time.time()
+    start = builders()
+    print(f"builders: {len(start)} arrays", flush=True)
+    np.savez_compressed(os.path.join(OUT, "builders.npz"), **start)
+    w = walks(start)
+    print(f"walks: {len(w)} arrays", flush=True)
+    np.savez_compressed(os.path.join(OUT, "walks.npz"), **w)
+    c0 = config0(start)
+    np.savez_compressed(os.path.join(OUT, "config0.npz"), **c0)
+    if os.path.isdir(os.path.join(REF, "Examples")):
+        with open(os.path.join(OUT, "example_outputs.json"), "w") as f:
+            json.dump(example_outputs(), f, indent=1, sort_keys=True)
+    print(f"done in {time.time() - t0:.1f}s")
+
+
+if __name__ == "__main__":
+    main()
