@@ -1,0 +1,416 @@
+"""Benchmark of the bit-exact flip dynamics on the configs[1] workload.
+
+Workload: lozenge tilings of the a=b=c=500 hexagon (LozengeTiler::AlmostHexDomain
+(500, 0) -> MinTiling, 1008 x 1008 tiling, 338,688 flip attempts per colour
+step), started from the minimal tiling, 20,000 sweeps = 60,000 reference colour
+steps per walk, TinyMT streams seeded from 42.  One bench "step" is one such
+walk.  Uniform weights (int8 storage) are the headline; the q = 0.99 int32
+walk (float32 comparison) is reported beside it.
+
+  value : attempts/s with the lattice already resident on the device
+          (rt_upload outside the timed region; rt_run inside), CUDA events on
+          the library's stream, L2 flushed between walks;
+  e2e   : the same metric through rt_walk (the reference's Walk contract:
+          host int32 tiling in, host tiling out, H2D + split + walk + merge +
+          D2H every walk).
+
+`--impl reference` times the reference's own CPU code (its kernels and
+LozengeTiler::Walk built through oracle/shim: oracle/_ref) on the host cores,
+or the oracle's C restatement where oracle/_ref is absent.
+
+Multi-GPU: one walk is a single lattice, which this path does not split, so
+--gpus N runs N independent replicas (seeds 42 + rank), value = total
+attempts / max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "flip attempts/s & HBM GB/s vs peak; sweeps-to-0.5% height error, warm vs cold"
+HEX_SIDE = 500
+STEPS_PER_WALK = 60000  # reference colour steps = 20,000 sweeps of the three colours
+SEED = 42
+L2_FLUSH_BYTES = 256 << 20
+
+
+def workload_config() -> dict:
+    return {
+        "workload": "lozenge hexagon a=b=c=500 (1008x1008 tiling), minimal tiling start, "
+                    "20000 sweeps = 60000 colour steps per walk, TinyMT bit-exact mode",
+        "domain": "LozengeTiler::AlmostHexDomain(500,0)",
+        "tiling_side": 1008,
+        "attempts_per_step": 1008 * 336,
+        "steps_per_walk": STEPS_PER_WALK,
+        "seed": SEED,
+        "weights": "uniform (int8 lattice); q=0.99 int32 in `q_weighted`",
+        "l2": "flushed (256 MiB write) between timed walks",
+    }
+
+
+def peaks() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def start_tiling():
+    import randomtilings_b200 as rt
+
+    d = rt.LozengeTiler.AlmostHexDomain(HEX_SIDE, 0)
+    return rt.LozengeTiler.MinTiling(d)
+
+
+def algorithmic_bytes_per_step(n: int, elem: int) -> int:
+    """Lattice read + write of every colour-array site, plus the TinyMT state
+    (s0..s3 read + write, 32 B) of every attempt."""
+    sites = n * n
+    attempts = n * (n // 3)
+    return 2 * sites * elem + attempts * 32
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while timing."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        under_load = [x for x in sm if x > 500] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(under_load) if under_load else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(ngpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        return rank, world, local, dist
+    return 0, 1, 0, None
+
+
+def all_max(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def time_device_walks(tiler, steps: int, warmup: int, seed: int, flush) -> list[float]:
+    """Per-walk device milliseconds (events on the library's stream)."""
+    import torch
+
+    s = torch.cuda.ExternalStream(tiler.stream)
+    for w in range(warmup):
+        tiler.run(STEPS_PER_WALK, seed + 1000 + w)
+    tiler.synchronize()
+    out = []
+    for k in range(steps):
+        flush()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        tiler.run(STEPS_PER_WALK, seed + k)
+        e1.record(s)
+        tiler.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def time_e2e_walks(tiler_cls, kwargs, t0: np.ndarray, steps: int, warmup: int, seed: int, flush) -> list[float]:
+    """rt_walk with a host tiling: wall time per walk (the call is synchronous)."""
+    import torch
+
+    tl = tiler_cls(**kwargs)
+    host = np.array(t0, dtype=np.int32)
+    for w in range(warmup):
+        host[:] = t0
+        tl.Walk(host, STEPS_PER_WALK, seed + 1000 + w)
+    out = []
+    for k in range(steps):
+        host[:] = t0
+        flush()
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        tl.Walk(host, STEPS_PER_WALK, seed + k)
+        out.append((time.perf_counter() - a) * 1e3)
+    tl.close()
+    return out
+
+
+def run_b200(args) -> None:
+    import torch
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    import randomtilings_b200 as rt
+
+    rt.load(build_if_missing=False)
+    t0 = start_tiling()
+    n = int(round(t0.size ** 0.5))
+    attempts = n * (n // 3)
+    seed = SEED + rank
+    flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def flush():
+        flush_buf.fill_(1.0)
+
+    tl = rt.LozengeTiler(device=local)
+    tl.upload(t0)
+    tq = rt.LozengeTiler(device=local, kernel=2, q=0.99, qcmp=0)
+    tq.upload(t0)
+
+    barrier(dist)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        wall0 = time.perf_counter()
+        ms = time_device_walks(tl, args.steps, args.warmup, seed, flush)
+        wall = time.perf_counter() - wall0
+    torch.cuda.synchronize()
+    barrier(dist)
+    clocks = clk.summary()
+    ms_q = time_device_walks(tq, args.steps, args.warmup, seed, flush)
+    e2e_ms = time_e2e_walks(rt.LozengeTiler, {"device": local}, t0, args.steps, min(args.warmup, 3), seed, flush)
+    phases, launches = tl.last_run_info()
+
+    total_ms = all_max(dist, sum(ms))
+    total_q = all_max(dist, sum(ms_q))
+    total_e2e = all_max(dist, sum(e2e_ms))
+    work = attempts * STEPS_PER_WALK * args.steps * world
+    value = work / (total_ms / 1e3)
+    per_launch_ms = sum(ms) / len(ms)
+    algo = algorithmic_bytes_per_step(n, 1) * STEPS_PER_WALK
+    peak, peak_kind = peaks()
+    achieved = algo / (per_launch_ms / 1e3) / 1e9
+    algo_q = algorithmic_bytes_per_step(n, 4) * STEPS_PER_WALK
+    achieved_q = algo_q / (sum(ms_q) / len(ms_q) / 1e3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(t0, seconds=args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "attempts/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "int8",
+            "data": "synthetic (the reference's own domain builder; no dataset)",
+            "config": workload_config() | {"parallelism": f"replicas{world}"},
+            "impl": "b200",
+            "hbm_gbs_algorithmic": achieved,
+            "sweeps_per_s": value / attempts / 3,
+            "e2e": {
+                "value": attempts * STEPS_PER_WALK * args.steps * world / (total_e2e / 1e3),
+                "unit": "attempts/s",
+                "h2d_bytes_per_step": n * n * 4,
+                "d2h_bytes_per_step": n * n * 4,
+                "ms_per_step": total_e2e / args.steps,
+            },
+            "roofline": {
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": achieved / peak,
+                "peak_kind": peak_kind,
+                "traffic": args.traffic,
+                "kernel": "rtb::walk_kernel (one cooperative launch per walk)",
+                "algorithmic_bytes_per_launch": algo,
+                "launch_ms": per_launch_ms,
+            },
+            "q_weighted": {
+                "q": 0.99, "compare": "float32", "dtype": "int32",
+                "value": attempts * STEPS_PER_WALK * args.steps * world / (total_q / 1e3),
+                "unit": "attempts/s",
+                "ms_per_step": total_q / args.steps,
+                "hbm_gbs_algorithmic": achieved_q,
+                "frac": achieved_q / peak,
+            },
+            "gpu_launches": int(launches) * args.steps,
+            "phases_per_launch": int(phases),
+            "clocks": clocks,
+            "wall_s_timed_region": wall,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    tl.close()
+    tq.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(t0: np.ndarray, seconds: float = 15.0, threads: int | None = None) -> dict:
+    """The reference's own kernels + LozengeTiler::Walk on the host cores
+    (oracle/_ref), else the oracle's C restatement; a bounded sample of the
+    same walk (same domain, start and seed), timed with a wall clock."""
+    from oracle import pyoracle as po
+
+    n = int(round(t0.size ** 0.5))
+    attempts = n * (n // 3)
+    threads = threads or os.cpu_count() or 1
+    if po.have_ref():
+        rt = po.RefTiler("lozenge", attempts, threads=threads)
+        run = lambda s: rt.walk(t0, s, SEED)  # noqa: E731
+        kind, cores = "reference", threads
+    else:
+        run = lambda s: po.lozenge_walk(t0, s, SEED)  # noqa: E731
+        kind, cores = "port", 1
+    probe = 20
+    a = time.perf_counter()
+    run(probe)
+    dt = time.perf_counter() - a
+    steps = max(probe, int(probe * seconds / max(dt, 1e-6)))
+    a = time.perf_counter()
+    run(steps)
+    dt = time.perf_counter() - a
+    return {
+        "value": attempts * steps / dt,
+        "unit": "attempts/s",
+        "cores": cores,
+        "kind": kind,
+        "sample": f"hex a=b=c=500 walk, first {steps} colour steps (of 60000), seed {SEED}, {dt:.1f} s",
+    }
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import randomtilings_b200 as rt  # builders only (host C++)
+
+    t0 = start_tiling()
+    n = int(round(t0.size ** 0.5))
+    attempts = n * (n // 3)
+    per_step_s = max(1.0, args.cpu_seconds / max(args.steps, 1))
+    for _ in range(args.warmup):
+        cpu_baseline(t0, seconds=0.5)
+    vals = [cpu_baseline(t0, seconds=per_step_s) for _ in range(args.steps)]
+    value = statistics.median(v["value"] for v in vals)
+    ms_per_step = attempts * STEPS_PER_WALK / value * 1e3
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "attempts/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int8",
+        "data": "synthetic (the reference's own domain builder; no dataset)",
+        "config": workload_config() | {"parallelism": "cpu"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "attempts/s", "cores": vals[0]["cores"], "kind": vals[0]["kind"],
+                         "sample": vals[0]["sample"]},
+        "e2e": {"value": value, "unit": "attempts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    del rt
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    global STEPS_PER_WALK
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="dram bytes per walk launch from an ncu capture (reported in roofline.traffic)")
+    ap.add_argument("--walk-steps", type=int, default=STEPS_PER_WALK,
+                    help="colour steps per walk (default 60000 = 20000 sweeps; smaller only for profiling captures)")
+    args = ap.parse_args()
+    STEPS_PER_WALK = args.walk_steps
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

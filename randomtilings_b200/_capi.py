@@ -73,6 +73,32 @@ SIGNATURES = {
     "rt_version": (ctypes.c_char_p, []),
 }
 
+_PL = ctypes.POINTER(_I64)
+# include/rt_b200_host.h: every builder writes (out, cap) and reports *len.
+HOST_SIGNATURES = {
+    "rt_domino_rectangle": [_I32, _I32],
+    "rt_domino_aztec_rectangle": [_I32, _P, _I32],
+    "rt_domino_aztec": [_I32],
+    "rt_domino_domain_to_vertices": [_P, _I64],
+    "rt_domino_max_tiling": [_P, _I64],
+    "rt_domino_min_tiling": [_P, _I64],
+    "rt_domino_height_to_tiling": [_P, _I64, _P, _I64],
+    "rt_domino_tiling_to_height": [_P, _I64, _P, _I64],
+    "rt_domino_tiling_to_domain": [_P, _I64],
+    "rt_lozenge_almost_hex": [_I32, _I32],
+    "rt_lozenge_domain_to_vertices": [_P, _I64],
+    "rt_lozenge_max_tiling": [_P, _I64],
+    "rt_lozenge_min_tiling": [_P, _I64],
+    "rt_lozenge_height_to_tiling": [_P, _I64, _P, _I64],
+    "rt_lozenge_tiling_to_height": [_P, _I64, _P, _I64],
+    "rt_lozenge_tiling_to_domain": [_P, _I64],
+    "rt_recttri_max_hex": [_I32],
+    "rt_recttri_min_hex": [_I32],
+    "rt_recttri_from_lozenge": [_P, _I64, _P, _I64],
+}
+for _name, _args in HOST_SIGNATURES.items():
+    SIGNATURES[_name] = (ctypes.c_int, [*_args, _P, _I64, _PL])
+
 _lib = None
 
 

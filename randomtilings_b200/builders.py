@@ -1,0 +1,46 @@
+"""Domains, extremal tilings and height functions (host C++ in librt_b200.so).
+
+Thin numpy wrappers over include/rt_b200_host.h; the Tiler classes expose them
+under the reference's static-method names.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi
+
+
+def _arr(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x, dtype=np.int32).reshape(-1))
+
+
+def call(name: str, *args) -> np.ndarray:
+    """Calls a builder: array arguments become (pointer, length) pairs."""
+    lib = _capi.load()
+    fn = getattr(lib, name)
+    cargs, keep = [], []
+    for a in args:
+        if isinstance(a, (np.ndarray, list, tuple)):
+            arr = _arr(a)
+            keep.append(arr)
+            cargs += [arr.ctypes.data, arr.size]
+        else:
+            cargs.append(int(a))
+    n = ctypes.c_int64()
+    _capi.check(fn(*cargs, None, 0, ctypes.byref(n)))
+    out = np.zeros(max(n.value, 1), dtype=np.int32)
+    _capi.check(fn(*cargs, out.ctypes.data, out.size, ctypes.byref(n)))
+    return out[: n.value]
+
+
+def aztec_rectangle(order: int, remove) -> np.ndarray:
+    lib = _capi.load()
+    rem = _arr(remove)
+    n = ctypes.c_int64()
+    _capi.check(lib.rt_domino_aztec_rectangle(order, rem.ctypes.data, rem.size, None, 0, ctypes.byref(n)))
+    out = np.zeros(n.value, dtype=np.int32)
+    _capi.check(lib.rt_domino_aztec_rectangle(order, rem.ctypes.data, rem.size, out.ctypes.data, out.size,
+                                              ctypes.byref(n)))
+    return out

@@ -103,12 +103,13 @@ struct rt_tiler {
     DevBuf d_tiling;
     bool uploaded = false;
 
-    DevBuf d_phases, d_epoch_start, d_epoch_seed, d_flags, d_err;
+    DevBuf d_phases, d_epoch_start, d_epoch_seed, d_xbuf, d_err;
     PinnedBuf h_phases, h_epoch_start, h_epoch_seed, h_err;
     cudaEvent_t ev_staged = nullptr;
 
     WalkPlan plan;
-    int plan_rows = -1, plan_cols = -1;
+    int plan_rows = -1, plan_cols = -1, plan_nlat = -1;
+    bool plan_uniform = true;
     int64_t last_phases = 0, last_launches = 0;
     uint64_t timeout_ns = 5000000000ull;
 
@@ -406,23 +407,29 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     }
     ph[at++] = make_phase(OP_FINAL, prev, NO_COLOUR, false);
 
-    if (h->plan_rows != h->rows || h->plan_cols != h->cols) {
-        rt_status s = plan_walk(h->family, h->cfg.device, h->rows, h->cols, &h->plan, &h->err);
+    const int width = h->n / h->ncol;
+    const bool uniform = h->table.empty();
+    if (h->plan_rows != h->rows || h->plan_cols != h->cols || h->plan_nlat != h->nlat || h->plan_uniform != uniform) {
+        rt_status s =
+            plan_walk(h->family, h->cfg.device, h->nlat, h->rows, h->cols, width, uniform, &h->plan, &h->err);
         if (s != RT_OK) return s;
         h->plan_rows = h->rows;
         h->plan_cols = h->cols;
+        h->plan_nlat = h->nlat;
+        h->plan_uniform = uniform;
     }
     const int64_t ids = (int64_t)h->rows * h->cols;
     rt_status s = stage_params(h, ids);
     if (s != RT_OK) return s;
-    if (!h->d_flags.reserve((size_t)h->plan.ctas * sizeof(unsigned))) return h->fail(RT_E_NOMEM, "flags");
+    const size_t xbytes = (size_t)h->plan.ctas * 2 * 2 * h->nlat * h->plan.xwords * sizeof(unsigned long long);
+    if (!h->d_xbuf.reserve(xbytes)) return h->fail(RT_E_NOMEM, "halo exchange buffer");
 
     cudaError_t e;
     if ((e = cudaMemcpyAsync(h->d_phases.p, ph, (size_t)nph * 4, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
         (e = cudaMemcpyAsync(h->d_epoch_start.p, es, (size_t)k * 8, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
         (e = cudaMemcpyAsync(h->d_epoch_seed.p, sd, (size_t)k * 4, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
         (e = cudaEventRecord(h->ev_staged, h->stream)) != cudaSuccess ||
-        (e = cudaMemsetAsync(h->d_flags.p, 0, (size_t)h->plan.ctas * sizeof(unsigned), h->stream)) != cudaSuccess)
+        (e = cudaMemsetAsync(h->d_xbuf.p, 0, xbytes, h->stream)) != cudaSuccess)
         return h->cuda_fail(e, "schedule staging");
 
     WalkArgs a;
@@ -433,6 +440,8 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     a.n = h->n;
     a.rows = h->rows;
     a.cols = h->cols;
+    a.arows = h->n;
+    a.width = width;
     a.rng_kind = 0;
     a.params = h->table.empty() ? nullptr : static_cast<const uint4*>(h->d_params.p);
     a.mat1 = kMat1;
@@ -465,7 +474,7 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
         default: break;
     }
     std::memcpy(a.weights, h->cfg.weights, sizeof a.weights);
-    a.flags = static_cast<unsigned*>(h->d_flags.p);
+    a.xbuf = static_cast<unsigned long long*>(h->d_xbuf.p);
     a.err = static_cast<int*>(h->d_err.p);
     a.timeout_ns = h->timeout_ns;
     s = launch_walk(h->plan, a, h->stream, &h->err);

@@ -1,0 +1,608 @@
+// rt_host.cpp -- host-side domains, extremal tilings and height functions.
+//
+// These are the static helpers of the reference's Tiler classes, rewritten as
+// plain C++ behind the C ABI.  Domain / tiling encodings and the height
+// normalisation (h = 0 at the first boundary vertex in row-major order,
+// INT_MAX outside the domain) are the reference's, so results are
+// interchangeable with it.  Extremal tilings follow Thurston's construction:
+// boundary heights by a walk along the boundary, then the extremal height
+// function as a shortest-path flood that only moves in the height-increasing
+// (max) or -decreasing (min) direction, then the tiling from height
+// differences.  A domain that is not tileable is reported (RT_E_INVAL); the
+// reference prints a message and returns a partial result instead.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/rt_b200.h"
+#include "../../include/rt_b200_host.h"
+
+namespace {
+
+constexpr int32_t INF = INT_MAX;
+using Vec = std::vector<int32_t>;
+
+int isqrt_exact(int64_t n) {
+    if (n < 0) return -1;
+    int64_t r = (int64_t)std::llround(std::sqrt((double)n));
+    while (r * r > n) --r;
+    while ((r + 1) * (r + 1) <= n) ++r;
+    return r * r == n ? (int)r : -1;
+}
+
+rt_status emit(const Vec& v, int32_t* out, int64_t cap, int64_t* len) {
+    if (len) *len = (int64_t)v.size();
+    if (!out) return RT_OK;
+    if (cap < (int64_t)v.size()) return RT_E_INVAL;
+    std::copy(v.begin(), v.end(), out);
+    return RT_OK;
+}
+
+// Dijkstra with unit steps from all seeded vertices; `dir` = +1 grows heights
+// from the lowest (maximal height function), -1 shrinks them from the highest
+// (minimal one).  allowed(v, nb) says whether the move v -> nb is one that
+// changes the height by `dir`.
+template <class Neighbours, class Allowed>
+bool extremal_flood(Vec& hf, const Vec& verts, const std::vector<int>& seeds, int dir, Neighbours nbrs,
+                    Allowed allowed) {
+    std::map<int64_t, std::vector<int>> buckets;  // height -> vertices (processed lowest first for dir > 0)
+    for (int v : seeds) buckets[(int64_t)dir * hf[v]].push_back(v);
+    while (!buckets.empty()) {
+        auto it = buckets.begin();
+        std::vector<int> level;
+        level.swap(it->second);
+        buckets.erase(it);
+        for (size_t k = 0; k < level.size(); ++k) {
+            const int v = level[k];
+            int nb[8], cnt = nbrs(v, nb);
+            for (int e = 0; e < cnt; ++e) {
+                const int w = nb[e];
+                if (w < 0 || verts[w] == 0 || !allowed(v, e)) continue;
+                const int32_t h = hf[v] + dir;
+                if (verts[w] == 2) {
+                    // A boundary height may not exceed (max) / undercut (min) the flood.
+                    if (verts[v] != 2 && (int64_t)dir * hf[w] > (int64_t)dir * h) return false;
+                } else if (hf[w] == INF) {
+                    hf[w] = h;
+                    buckets[(int64_t)dir * h].push_back(w);
+                }
+            }
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Dominoes (src/Domino/DominoTiler.cpp).  Domain: M x M faces; tiling and
+// heights on the (M+1) x (M+1) vertices; vertex bits 1 up, 2 down, 8 towards
+// j+1, 4 towards j-1.
+// ---------------------------------------------------------------------------
+const int kDomDi[4] = {1, -1, 0, 0};
+const int kDomDj[4] = {0, 0, 1, -1};
+const int kDomBit[4] = {2, 1, 8, 4};
+
+int dom_face(const Vec& d, int m, int i, int j) { return (i >= 0 && j >= 0 && i < m && j < m) ? d[i * m + j] : 0; }
+
+// The two faces on either side of the edge from vertex (i, j) in direction nb.
+void dom_edge_faces(int i, int j, int nb, int f[4]) {
+    switch (nb) {
+        case 0: f[0] = i, f[1] = j - 1, f[2] = i, f[3] = j; break;
+        case 1: f[0] = i - 1, f[1] = j - 1, f[2] = i - 1, f[3] = j; break;
+        case 2: f[0] = i - 1, f[1] = j, f[2] = i, f[3] = j; break;
+        default: f[0] = i - 1, f[1] = j - 1, f[2] = i, f[3] = j - 1; break;
+    }
+}
+
+// Height change along an edge, checkerboard rule of DominoTiler.cpp:221-231.
+int dom_dh(int i, int j, int nb) { return (nb > 1 ? 1 : -1) * (((i + j) % 2 == 0) ? 1 : -1); }
+
+Vec dom_vertices(const Vec& d, int m) {
+    const int n = m + 1;
+    Vec v((size_t)n * n, 0);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            if (i == 0 || j == 0 || i == m || j == m) {
+                const int i0 = i - (i == m), i1 = i - 1 + (i == 0), j0 = j - (j == m), j1 = j - 1 + (j == 0);
+                if (dom_face(d, m, i0, j0) || dom_face(d, m, i1, j0) || dom_face(d, m, i0, j1) || dom_face(d, m, i1, j1))
+                    v[i * n + j] = 2;
+            } else {
+                const int s = (d[(i - 1) * m + j - 1] != 0) + (d[(i - 1) * m + j] != 0) + (d[i * m + j - 1] != 0) +
+                              (d[i * m + j] != 0);
+                v[i * n + j] = s == 4 ? 1 : s > 0 ? 2 : 0;
+            }
+        }
+    return v;
+}
+
+int first_boundary(const Vec& verts) {
+    for (size_t k = 0; k < verts.size(); ++k)
+        if (verts[k] == 2) return (int)k;
+    return -1;
+}
+
+Vec dom_height_to_tiling(const Vec& hf, const Vec& d, int n) {
+    const int m = n - 1;
+    Vec t((size_t)n * n, 0);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            if (hf[i * n + j] == INF) continue;
+            for (int nb = 0; nb < 4; ++nb) {
+                const int i2 = i + kDomDi[nb], j2 = j + kDomDj[nb];
+                if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n || hf[i2 * n + j2] == INF) continue;
+                int f[4];
+                dom_edge_faces(i, j, nb, f);
+                if (!dom_face(d, m, f[0], f[1]) && !dom_face(d, m, f[2], f[3])) continue;
+                const int64_t diff = (int64_t)hf[i2 * n + j2] - hf[i * n + j];
+                t[i * n + j] += kDomBit[nb] * (int32_t)std::llabs(diff / 2);
+            }
+        }
+    return t;
+}
+
+rt_status dom_extremal(const Vec& d, int dir, Vec* out) {
+    const int m = isqrt_exact((int64_t)d.size());
+    if (m < 1) return RT_E_INVAL;
+    const int n = m + 1;
+    const Vec verts = dom_vertices(d, m);
+    Vec hf((size_t)n * n, INF);
+    const int start = first_boundary(verts);
+    if (start < 0) return RT_E_INVAL;
+    hf[start] = 0;
+    // Boundary heights: walk along boundary edges (exactly one adjacent face in the domain).
+    std::deque<int> q{start};
+    std::vector<int> seeds{start};
+    while (!q.empty()) {
+        const int v = q.front();
+        q.pop_front();
+        const int i = v / n, j = v % n;
+        for (int nb = 0; nb < 4; ++nb) {
+            const int i2 = i + kDomDi[nb], j2 = j + kDomDj[nb];
+            if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n || verts[i2 * n + j2] != 2) continue;
+            int f[4];
+            dom_edge_faces(i, j, nb, f);
+            if ((dom_face(d, m, f[0], f[1]) != 0) == (dom_face(d, m, f[2], f[3]) != 0)) continue;
+            const int w = i2 * n + j2;
+            const int32_t h = hf[v] + dom_dh(i, j, nb);
+            if (hf[w] == INF) {
+                hf[w] = h;
+                q.push_back(w);
+                seeds.push_back(w);
+            } else if (hf[w] != h) {
+                return RT_E_INVAL;  // boundary heights inconsistent: not tileable
+            }
+        }
+    }
+    auto nbrs = [&](int v, int* out4) {
+        const int i = v / n, j = v % n;
+        for (int nb = 0; nb < 4; ++nb) {
+            const int i2 = i + kDomDi[nb], j2 = j + kDomDj[nb];
+            out4[nb] = (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n) ? -1 : i2 * n + j2;
+        }
+        return 4;
+    };
+    auto allowed = [&](int v, int nb) { return dom_dh(v / n, v % n, nb) == dir; };
+    if (!extremal_flood(hf, verts, seeds, dir, nbrs, allowed)) return RT_E_INVAL;
+    *out = dom_height_to_tiling(hf, d, n);
+    return RT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Lozenges (src/Lozenge/LozengeTiler.cpp).  Domain: M rows of 2M triangles;
+// tiling and heights on the (M+1) x (M+1) vertices of the triangular
+// lattice; six neighbours with height steps -1, +1, ... and bits 8, 2, 1, 4,
+// 16, 32 (LozengeTiler.cpp:12-16).
+// ---------------------------------------------------------------------------
+const int kLozDi[6] = {0, -1, -1, 0, 1, 1};
+const int kLozDj[6] = {1, 1, 0, -1, -1, 0};
+const int kLozDh[6] = {-1, 1, -1, 1, -1, 1};
+const int kLozBit[6] = {8, 2, 1, 4, 16, 32};
+// (row offset, offset from 2j) of the two triangles beside edge nb.
+const int kLozFace[6][4] = {{0, 0, -1, 1}, {-1, 1, -1, 0}, {-1, 0, -1, -1}, {-1, -1, 0, -2}, {0, -2, 0, -1}, {0, -1, 0, 0}};
+
+int loz_face(const Vec& d, int m, int r, int c) { return (r >= 0 && c >= 0 && r < m && c < 2 * m) ? d[r * 2 * m + c] : 0; }
+
+bool loz_edge_in(const Vec& d, int m, int i, int j, int nb, bool exclusive) {
+    const int a = loz_face(d, m, i + kLozFace[nb][0], 2 * j + kLozFace[nb][1]) != 0;
+    const int b = loz_face(d, m, i + kLozFace[nb][2], 2 * j + kLozFace[nb][3]) != 0;
+    return exclusive ? (a != b) : (a || b);
+}
+
+Vec loz_vertices(const Vec& d, int m) {
+    const int n = m + 1;
+    Vec v((size_t)n * n, 0);
+    for (int i = 1; i < m; ++i)
+        for (int j = 1; j < m; ++j) {
+            const int s = (d[i * 2 * m + 2 * j] != 0) + (d[i * 2 * m + 2 * j - 1] != 0) + (d[i * 2 * m + 2 * j - 2] != 0) +
+                          (d[(i - 1) * 2 * m + 2 * j] != 0) + (d[(i - 1) * 2 * m + 2 * j + 1] != 0) +
+                          (d[(i - 1) * 2 * m + 2 * j - 1] != 0);
+            v[i * n + j] = s == 6 ? 1 : s > 0 ? 2 : 0;
+        }
+    return v;
+}
+
+Vec loz_height_to_tiling(const Vec& hf, const Vec& d, int n) {
+    const int m = n - 1;
+    Vec t((size_t)n * n, 0);
+    for (int i = 1; i < n - 1; ++i)
+        for (int j = 1; j < n - 1; ++j)
+            for (int nb = 0; nb < 6; ++nb) {
+                if (!loz_edge_in(d, m, i, j, nb, false)) continue;
+                const int i2 = i + kLozDi[nb], j2 = j + kLozDj[nb];
+                if (std::llabs((int64_t)hf[i2 * n + j2] - hf[i * n + j]) == 2) t[i * n + j] += kLozBit[nb];
+            }
+    return t;
+}
+
+rt_status loz_extremal(const Vec& d, int dir, Vec* out) {
+    const int m = isqrt_exact((int64_t)d.size() / 2);
+    if (m < 2 || (int64_t)2 * m * m != (int64_t)d.size()) return RT_E_INVAL;
+    const int n = m + 1;
+    const Vec verts = loz_vertices(d, m);
+    Vec hf((size_t)n * n, INF);
+    const int start = first_boundary(verts);
+    if (start < 0) return RT_E_INVAL;
+    hf[start] = 0;
+    std::deque<int> q{start};
+    std::vector<int> seeds{start};
+    while (!q.empty()) {
+        const int v = q.front();
+        q.pop_front();
+        const int i = v / n, j = v % n;
+        for (int nb = 0; nb < 6; ++nb) {
+            const int i2 = i + kLozDi[nb], j2 = j + kLozDj[nb];
+            if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n || verts[i2 * n + j2] != 2) continue;
+            if (!loz_edge_in(d, m, i, j, nb, true)) continue;
+            const int w = i2 * n + j2;
+            const int32_t h = hf[v] + kLozDh[nb];
+            if (hf[w] == INF) {
+                hf[w] = h;
+                q.push_back(w);
+                seeds.push_back(w);
+            } else if (hf[w] != h) {
+                return RT_E_INVAL;
+            }
+        }
+    }
+    auto nbrs = [&](int v, int* out6) {
+        const int i = v / n, j = v % n;
+        for (int nb = 0; nb < 6; ++nb) {
+            const int i2 = i + kLozDi[nb], j2 = j + kLozDj[nb];
+            out6[nb] = (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n) ? -1 : i2 * n + j2;
+        }
+        return 6;
+    };
+    auto allowed = [&](int, int nb) { return kLozDh[nb] == dir; };
+    if (!extremal_flood(hf, verts, seeds, dir, nbrs, allowed)) return RT_E_INVAL;
+    for (size_t k = 0; k < hf.size(); ++k)
+        if (verts[k] == 0) hf[k] = INF;
+    *out = loz_height_to_tiling(hf, d, n);
+    return RT_OK;
+}
+
+// Change of coordinates of the rectangle-triangle hexagons
+// (RectTriangleTiler.cpp:446-456): row i moves down 3 and right N+3-i.
+Vec rt_shear(const Vec& g, int n, int m) {
+    const int m2 = m + 6 + (3 - m % 3) % 3;
+    Vec out((size_t)m2 * m2, 0);
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) {
+            const int j2 = j + n + 3 - i;
+            if (j2 >= 0 && j2 < m2) out[(size_t)(i + 3) * m2 + j2] = g[(size_t)i * m + j];
+        }
+    return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- dominoes ----------------------------------------------------------------
+rt_status rt_domino_rectangle(int32_t rows, int32_t cols, int32_t* out, int64_t cap, int64_t* len) {
+    if (rows < 0 || cols < 0) return RT_E_INVAL;
+    int dim = std::max(rows, cols) + 4;
+    if (dim % 2 == 0) ++dim;
+    Vec d((size_t)dim * dim, 0);
+    for (int i = 0; i < rows; ++i)
+        for (int j = 0; j < cols; ++j) d[(size_t)(i + 2) * dim + j + 2] = 1;
+    return emit(d, out, cap, len);
+}
+
+rt_status rt_domino_aztec_rectangle(int32_t order, const int32_t* remove, int32_t k, int32_t* out, int64_t cap,
+                                    int64_t* len) {
+    if (order < 1 || k < 0 || k >= 2 * order) return RT_E_INVAL;
+    const int n = order, m = 2 * n - k;
+    Vec d((size_t)m * m, 0);
+    for (int i = 0; i < m; ++i) {
+        int lo, hi;
+        if (i == 0 || i == m - 1) {
+            lo = (n - k) + (i == m - 1) * k - 1;
+            hi = lo + 1;
+        } else if (i < n - k) {
+            lo = n - k - i - 1, hi = n - k + i;
+        } else if (i > n - 1) {
+            lo = i - n + k, hi = 3 * n - k - i - 1;
+        } else {
+            lo = i - (n - k), hi = i + (n - k);
+        }
+        for (int j = std::max(lo, 0); j <= std::min(hi, m - 1); ++j) d[(size_t)i * m + j] = 1;
+    }
+    for (int r = 0; r < k; ++r) {
+        const int i0 = n - k + remove[r], j0 = remove[r];
+        if (i0 < 0 || j0 < 0 || i0 >= m || j0 >= m) return RT_E_INVAL;
+        d[(size_t)i0 * m + j0] = 0;
+    }
+    const int m2 = m + 4 + (1 - m % 2);  // odd side -> even tiling side (DominoTiler.cpp:183-184)
+    Vec d2((size_t)m2 * m2, 0);
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) d2[(size_t)(i + 2) * m2 + j + 2] = d[(size_t)i * m + j];
+    return emit(d2, out, cap, len);
+}
+
+rt_status rt_domino_aztec(int32_t order, int32_t* out, int64_t cap, int64_t* len) {
+    return rt_domino_aztec_rectangle(order, nullptr, 0, out, cap, len);
+}
+
+rt_status rt_domino_domain_to_vertices(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
+    const int m = isqrt_exact(dlen);
+    if (!d || m < 1) return RT_E_INVAL;
+    return emit(dom_vertices(Vec(d, d + dlen), m), out, cap, len);
+}
+
+rt_status rt_domino_max_tiling(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
+    if (!d) return RT_E_INVAL;
+    Vec t;
+    rt_status s = dom_extremal(Vec(d, d + dlen), +1, &t);
+    return s != RT_OK ? s : emit(t, out, cap, len);
+}
+
+rt_status rt_domino_min_tiling(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
+    if (!d) return RT_E_INVAL;
+    Vec t;
+    rt_status s = dom_extremal(Vec(d, d + dlen), -1, &t);
+    return s != RT_OK ? s : emit(t, out, cap, len);
+}
+
+rt_status rt_domino_height_to_tiling(const int32_t* h, int64_t hlen, const int32_t* d, int64_t dlen, int32_t* out,
+                                     int64_t cap, int64_t* len) {
+    const int n = isqrt_exact(hlen);
+    if (!h || !d || n < 2 || (int64_t)(n - 1) * (n - 1) != dlen) return RT_E_INVAL;
+    return emit(dom_height_to_tiling(Vec(h, h + hlen), Vec(d, d + dlen), n), out, cap, len);
+}
+
+rt_status rt_domino_tiling_to_height(const int32_t* t, int64_t tlen, const int32_t* d, int64_t dlen, int32_t* out,
+                                     int64_t cap, int64_t* len) {
+    const int n = isqrt_exact(tlen);
+    if (!t || !d || n < 2 || (int64_t)(n - 1) * (n - 1) != dlen) return RT_E_INVAL;
+    const int m = n - 1;
+    const Vec D(d, d + dlen);
+    const Vec verts = dom_vertices(D, m);
+    Vec hf((size_t)n * n, INF);
+    const int start = first_boundary(verts);
+    if (start >= 0) {
+        hf[start] = 0;
+        std::deque<int> q{start};
+        while (!q.empty()) {
+            const int v = q.front();
+            q.pop_front();
+            const int i = v / n, j = v % n;
+            for (int nb = 0; nb < 4; ++nb) {
+                if (t[v] & kDomBit[nb]) continue;  // a domino crosses this edge
+                const int i2 = i + kDomDi[nb], j2 = j + kDomDj[nb];
+                if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n) continue;
+                const int w = i2 * n + j2;
+                if (verts[w] == 0 || hf[w] != INF) continue;
+                int f[4];
+                dom_edge_faces(i, j, nb, f);
+                if (!dom_face(D, m, f[0], f[1]) && !dom_face(D, m, f[2], f[3])) continue;
+                hf[w] = hf[v] + dom_dh(i, j, nb);
+                q.push_back(w);
+            }
+        }
+    }
+    return emit(hf, out, cap, len);
+}
+
+rt_status rt_domino_tiling_to_domain(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len) {
+    const int n = isqrt_exact(tlen);
+    if (!t || n < 2) return RT_E_INVAL;
+    const int m = n - 1;
+    Vec d((size_t)m * m, 0);
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j)
+            if ((t[i * n + j] & (2 + 8)) || (t[(i + 1) * n + j + 1] & (1 + 4))) d[(size_t)i * m + j] = 1;
+    return emit(d, out, cap, len);
+}
+
+// ---- lozenges ------------------------------------------------------------------
+rt_status rt_lozenge_almost_hex(int32_t side, int32_t cut, int32_t* out, int64_t cap, int64_t* len) {
+    if (side < 1 || cut < 0 || cut > side) return RT_E_INVAL;
+    const int n = side;
+    const int rows = 2 * n, cols = 4 * n;
+    Vec d((size_t)rows * cols, 0);
+    for (int i = 0; i < rows; ++i)
+        for (int j = 0; j < cols; ++j)
+            d[(size_t)i * cols + j] = i < n ? (2 * i + j - 1 >= 2 * n - 2) : (2 * i + j <= 6 * n - 2);
+    for (int i = 0; i < cut; ++i)
+        for (int j = cols - 2 * cut; j < cols; ++j) d[(size_t)i * cols + j] = 0;
+    // 3 rows / 6 triangles of padding, then grow to a vertex side divisible by 3
+    // (LozengeTiler.cpp:370-388).
+    const int m2 = rows + 6;
+    const int k = (3 - (m2 + 1) % 3) % 3;
+    const int m3 = m2 + k;
+    Vec d3((size_t)m3 * 2 * m3, 0);
+    for (int i = 0; i < rows; ++i)
+        for (int j = 0; j < cols; ++j) d3[(size_t)(i + 3) * 2 * m3 + j + 6] = d[(size_t)i * cols + j];
+    return emit(d3, out, cap, len);
+}
+
+rt_status rt_lozenge_domain_to_vertices(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
+    const int m = isqrt_exact(dlen / 2);
+    if (!d || m < 2 || (int64_t)2 * m * m != dlen) return RT_E_INVAL;
+    return emit(loz_vertices(Vec(d, d + dlen), m), out, cap, len);
+}
+
+rt_status rt_lozenge_max_tiling(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
+    if (!d) return RT_E_INVAL;
+    Vec t;
+    rt_status s = loz_extremal(Vec(d, d + dlen), +1, &t);
+    return s != RT_OK ? s : emit(t, out, cap, len);
+}
+
+rt_status rt_lozenge_min_tiling(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
+    if (!d) return RT_E_INVAL;
+    Vec t;
+    rt_status s = loz_extremal(Vec(d, d + dlen), -1, &t);
+    return s != RT_OK ? s : emit(t, out, cap, len);
+}
+
+rt_status rt_lozenge_height_to_tiling(const int32_t* h, int64_t hlen, const int32_t* d, int64_t dlen, int32_t* out,
+                                      int64_t cap, int64_t* len) {
+    const int n = isqrt_exact(hlen);
+    if (!h || !d || n < 3 || (int64_t)2 * (n - 1) * (n - 1) != dlen) return RT_E_INVAL;
+    return emit(loz_height_to_tiling(Vec(h, h + hlen), Vec(d, d + dlen), n), out, cap, len);
+}
+
+rt_status rt_lozenge_tiling_to_height(const int32_t* t, int64_t tlen, const int32_t* d, int64_t dlen, int32_t* out,
+                                      int64_t cap, int64_t* len) {
+    const int n = isqrt_exact(tlen);
+    if (!t || !d || n < 3 || (int64_t)2 * (n - 1) * (n - 1) != dlen) return RT_E_INVAL;
+    const int m = n - 1;
+    const Vec D(d, d + dlen);
+    const Vec verts = loz_vertices(D, m);
+    Vec hf((size_t)n * n, INF);
+    const int start = first_boundary(verts);
+    if (start >= 0) {
+        hf[start] = 0;
+        std::deque<int> q{start};
+        while (!q.empty()) {
+            const int v = q.front();
+            q.pop_front();
+            const int i = v / n, j = v % n;
+            for (int nb = 0; nb < 6; ++nb) {
+                if (t[v] & kLozBit[nb]) continue;  // a lozenge covers this edge
+                const int i2 = i + kLozDi[nb], j2 = j + kLozDj[nb];
+                if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n) continue;
+                const int w = i2 * n + j2;
+                if (verts[w] == 0 || hf[w] != INF || !loz_edge_in(D, m, i, j, nb, false)) continue;
+                hf[w] = hf[v] + kLozDh[nb];
+                q.push_back(w);
+            }
+        }
+    }
+    return emit(hf, out, cap, len);
+}
+
+rt_status rt_lozenge_tiling_to_domain(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len) {
+    const int n = isqrt_exact(tlen);
+    if (!t || n < 3) return RT_E_INVAL;
+    const int m = n - 1;
+    Vec d((size_t)2 * m * m, 0);
+    auto set = [&](int r, int c) {
+        if (r >= 0 && r < m && c >= 0 && c < 2 * m) d[(size_t)r * 2 * m + c] = 1;
+    };
+    for (int i = 0; i < n - 1; ++i)
+        for (int j = 0; j < n - 1; ++j) {
+            const int v = t[i * n + j];
+            if (v & 1) set(i - 1, 2 * j), set(i - 1, 2 * j - 1);
+            if (v & 2) set(i - 1, 2 * j), set(i - 1, 2 * j + 1);
+            if (v & 8) set(i - 1, 2 * j + 1), set(i, 2 * j);
+        }
+    return emit(d, out, cap, len);
+}
+
+// ---- rectangle-triangle hexagons -------------------------------------------------
+rt_status rt_recttri_max_hex(int32_t side, int32_t* out, int64_t cap, int64_t* len) {
+    if (side < 1) return RT_E_INVAL;
+    const int n = side, m = 2 * n + 1;
+    Vec g((size_t)m * m, 0);
+    auto at = [&](int i, int j) -> int32_t& { return g[(size_t)i * m + j]; };
+    for (int i = 1; i < m - 1; ++i)
+        for (int j = 0; j < m; ++j) {
+            int32_t v;
+            if (j - i > n || i - j > n) v = 0;
+            else if (i < n && j < n) v = 0x333333;
+            else if (i < j && j > n) v = 0x111111;
+            else if (i > n && i > j) v = 0x222222;
+            else if (i == n && j < n) v = 0x333222;
+            else if (i < n && j == n) v = 0x331311;
+            else if (i == j && i > n) v = 0x211221;
+            else v = 0x331221;  // the centre, i == j == n
+            at(i, j) = v;
+        }
+    for (int i = 1; i < n; ++i) at(i, 0) = 0x003033, at(0, i) = 0x000333;
+    for (int i = n + 1; i < m - 1; ++i) at(i, m - 1) = 0x110100, at(m - 1, i) = 0x222000;
+    for (int i = 1; i < n; ++i) at(i, i + n) = 0x100110, at(i + n, i) = 0x022002;
+    at(0, 0) = 0x000033;
+    at(n, 0) = 0x003002;
+    at(0, n) = 0x000310;
+    at(m - 1, m - 1) = 0x210000;
+    at(n, m - 1) = 0x100100;
+    at(m - 1, n) = 0x022000;
+    return emit(rt_shear(g, n, m), out, cap, len);
+}
+
+rt_status rt_recttri_min_hex(int32_t side, int32_t* out, int64_t cap, int64_t* len) {
+    if (side < 1) return RT_E_INVAL;
+    const int n = side, m = 2 * n + 1;
+    Vec g((size_t)m * m, 0);
+    auto at = [&](int i, int j) -> int32_t& { return g[(size_t)i * m + j]; };
+    for (int i = 1; i < m - 1; ++i)
+        for (int j = 1; j < m - 1; ++j) {
+            int32_t v;
+            if (j - i > n || i - j > n) v = 0;
+            else if (i > n && j > n) v = 0x333333;
+            else if (i > j && j < n) v = 0x111111;
+            else if (i < n && i < j) v = 0x222222;
+            else if (i == n && j > n) v = 0x222333;
+            else if (i > n && j == n) v = 0x113133;
+            else if (i == j && i < n) v = 0x122112;
+            else v = 0x122133;  // the centre
+            at(i, j) = v;
+        }
+    for (int i = 1; i < n; ++i) at(i, 0) = 0x001011, at(0, i) = 0x000222;
+    for (int i = n + 1; i < m - 1; ++i) at(i, m - 1) = 0x330300, at(m - 1, i) = 0x333000;
+    for (int i = 1; i < n; ++i) at(i, i + n) = 0x200220, at(i + n, i) = 0x011001;
+    at(0, 0) = 0x000012;
+    at(m - 1, n) = 0x013000;
+    at(n, m - 1) = 0x200300;
+    at(0, n) = 0x000220;
+    at(n, 0) = 0x001001;
+    at(m - 1, m - 1) = 0x330000;
+    return emit(rt_shear(g, n, m), out, cap, len);
+}
+
+// LozengeToRectTriangle (RectTriangleTiler.cpp:523-565): each triangle of the
+// lozenge domain becomes a rect-triangle face digit (1, 2 or 3 by the lozenge
+// covering it) on its three corner vertices.
+rt_status rt_recttri_from_lozenge(const int32_t* tl, int64_t tlen, const int32_t* dl, int64_t dlen, int32_t* out,
+                                  int64_t cap, int64_t* len) {
+    const int n = isqrt_exact(tlen), m = isqrt_exact(dlen / 2);
+    if (!tl || !dl || n < 2 || m < 1 || (int64_t)2 * m * m != dlen || m + 1 > n) return RT_E_INVAL;
+    Vec t((size_t)n * n, 0);
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < 2 * m; ++j) {
+            if (dl[(size_t)i * 2 * m + j] != 1) continue;
+            const int c = j / 2;
+            if (j % 2 == 0) {  // downward-pointing face: corners (i, c), (i, c+1), (i+1, c)
+                const int v = tl[(size_t)i * n + c];
+                const int dgt = (v & 8) ? 1 : (v & 32) ? 3 : 2;
+                t[(size_t)i * n + c] += dgt;
+                t[(size_t)i * n + c + 1] += dgt << 8;
+                t[(size_t)(i + 1) * n + c] += dgt << 16;
+            } else {  // upward face: corners (i, c+1), (i+1, c), (i+1, c+1)
+                const int v = tl[(size_t)i * n + c + 1];
+                const int dgt = (v & 16) ? 2 : (v & 32) ? 3 : 1;
+                t[(size_t)i * n + c + 1] += dgt << 4;
+                t[(size_t)(i + 1) * n + c] += dgt << 12;
+                t[(size_t)(i + 1) * n + c + 1] += dgt << 20;
+            }
+        }
+    return emit(t, out, cap, len);
+}
+
+}  // extern "C"

@@ -24,10 +24,14 @@ struct WalkPlan {
     int block = 0;
     int rows_per_cta = 0;
     int ctas = 0;
+    size_t smem = 0;
+    int wpad = 0;    // shared-memory row stride (elements)
+    int xwords = 0;  // exchange words per halo row
     const void* fn = nullptr;
 };
 
-rt_status plan_walk(int family, int device, int rows, int cols, WalkPlan* plan, std::string* err);
+rt_status plan_walk(int family, int device, int nlat, int rows, int cols, int width, bool uniform, WalkPlan* plan,
+                    std::string* err);
 rt_status launch_walk(const WalkPlan& plan, WalkArgs& args, cudaStream_t stream, std::string* err);
 // kind: 0 domino, 1 lozenge, 2 rect-triangle.
 rt_status launch_split(bool merge, int elem_bytes, int kind, int ncol, int n, int32_t* tiling, void* const* arr,

@@ -1,7 +1,7 @@
 // rt_models.cuh -- per-model site rules of the persistent walk kernel.
 //
 // A model maps a position (r, c) of the Rotate NDRange to its colour-array
-// site, its TinyMT stream id, and applies one phase there:
+// site and stream id, and applies one phase there:
 //   OP_STEP  : if the previous phase flipped a different colour, first apply
 //              that colour's pending Update at this site (the reference runs
 //              Update right after every Rotate; when the same colour is
@@ -9,9 +9,14 @@
 //              second before anything reads it, so it is skipped), then flip
 //              the current colour with this position's draw;
 //   OP_FINAL : apply the last colour's Update (end of the walk).
-// Within one phase a site only reads the previously flipped colour at
-// neighbouring sites and writes the other colours, so positions are
-// independent and the kernel's result equals the reference's serial order.
+// Within one phase a site reads only the previously flipped colour at
+// neighbouring sites (and its own old values), and writes the other colours
+// at itself, so positions are independent and the result equals the
+// reference's serial order.
+//
+// The rules read and write the CTA's shared-memory copy of the lattice
+// through a Band view, indexed with the global (row, column) of the colour
+// arrays.
 #pragma once
 
 #include "rt_device.cuh"
@@ -19,10 +24,13 @@
 namespace rtb {
 
 struct WalkArgs {
-    void* arr[2][8];      // [lattice][colour] device arrays (2 lattices = coupled CFTP chains)
+    void* arr[2][8];      // [lattice][colour] global colour arrays (2 lattices = coupled CFTP chains)
     int nlat;             // 1 or 2
     int n;                // tiling side N
     int rows, cols;       // Rotate NDRange (position grid)
+    int arows, width;     // colour array shape
+    int wpad;             // shared-memory row stride (elements, multiple of 4)
+    int xwords;           // exchange words per row
     int rows_per_cta;
     int rng_kind;         // 0 TinyMT, 1 Philox
     const uint4* params;  // TinyMT (mat1, mat2, tmat, -) per stream id, or nullptr
@@ -36,119 +44,179 @@ struct WalkArgs {
     int nepochs;
     uint32_t thr[4];      // integer acceptance thresholds on the 23-bit draw
     float weights[16];    // rect-triangle face weights
-    unsigned* flags;      // per-CTA count of completed phases
+    unsigned long long* xbuf;  // tagged halo-row exchange slots
     int* err;
     uint64_t timeout_ns;
 };
 
 // ---------------------------------------------------------------------------
-// Domino (src/Domino/DominoTiler.cpp:9-107; dominokernel.cl, dominokernelCFTP.cl).
-// arr[0] = black ((i+j) even), arr[1] = white, int8, N x N/2.  Position
-// (r, c) of the (N-2) x (N/2-2) range is site (r+1, c+1), stream c + (N/2-2) r.
-// Reference colour r flips array 1-r and then refreshes array r from it.
+// Model interface.  Per phase every thread builds a small context once (the
+// decoded descriptor and the shared-memory planes it touches); per site the
+// model gets the site's offset `off` inside a colour plane of the band, its
+// global colour-array row i and column j, and the draw k.  Neighbours are
+// off +- 1 (columns) and off +- w (rows); w = band row stride.
 // ---------------------------------------------------------------------------
+
+// Domino (src/Domino/DominoTiler.cpp:9-107; dominokernel.cl, dominokernelCFTP.cl).
+// Colour 0 = black ((i+j) even), 1 = white, int8, N x N/2.  Position (r, c)
+// of the (N-2) x (N/2-2) range is site (r+1, c+1), stream c + (N/2-2) r.
+// Reference colour r flips array 1-r and then refreshes array r from it.
 template <bool HEAT_BATH>
 struct DominoRule {
+    using Elem = int8_t;
+    static constexpr int NCOL = 2;
+    static constexpr int ROFF = 1;
+    static constexpr int COFF = 1;
+    // Array the reference's colour r flips (DominoTiler.cpp:36-41).
+    __device__ static int flipped(int r) { return 1 - r; }
     __device__ static uint32_t stream_id(const WalkArgs& a, int r, int c) {
         return (uint32_t)c + (uint32_t)(a.n / 2 - 2) * (uint32_t)r;
     }
+    struct Ctx {
+        int8_t* dst;        // array written at the site
+        const int8_t* src;  // flipped array whose neighbours are read
+        int t;              // the reference's colour of the pending Update
+        bool step, upd;
+        int w;
+        uint32_t thr;
+    };
+    __device__ static Ctx ctx(const WalkArgs& a, int8_t* planes, int plane, uint32_t d) {
+        const int op = (int)ph_op(d), ca = (int)ph_a(d), cb = (int)ph_b(d);
+        Ctx x;
+        x.step = op == (int)OP_STEP;
+        x.w = a.wpad;
+        x.thr = a.thr[0];
+        if (x.step) {
+            x.upd = cb != (int)NO_COLOUR && cb != ca;
+            x.dst = planes + (1 - ca) * plane;
+            x.src = planes + ca * plane;
+            x.t = cb;
+        } else {
+            x.upd = true;
+            x.dst = planes + ca * plane;
+            x.src = planes + (1 - ca) * plane;
+            x.t = ca;
+        }
+        return x;
+    }
     // Edge bits of a site from its four neighbours in the flipped array:
     // 1 up, 2 down, 4 towards j-1, 8 towards j+1 (dominokernel.cl:22-31).
-    __device__ static int refreshed(const int8_t* f, int i, int j, int h, int t) {
-        const int up = ld_site(f + (i - 1) * h + j);
-        const int down = ld_site(f + (i + 1) * h + j);
-        const int west = ld_site(f + i * h + j - ((i + t + 1) & 1));
-        const int east = ld_site(f + i * h + j + ((i + t) & 1));
+    // The flipped array's neighbour towards j+1 shares the site's column in
+    // rows of parity (i+t) odd, towards j-1 in the others.
+    __device__ static int refreshed(const Ctx& x, int off, int i) {
+        const int p = (i + x.t) & 1;
+        const int up = x.src[off - x.w], down = x.src[off + x.w];
+        const int west = x.src[off - (1 - p)], east = x.src[off + p];
         return ((up & 2) >> 1) | ((down & 1) << 1) | ((west & 8) >> 1) | ((east & 4) << 1);
     }
-    // thr[0]: draws below it act (ceil(0.8 * 2^23), or 2^22 for the heat bath).
-    __device__ static int flip(int v, uint32_t k, const WalkArgs& a) {
-        if (HEAT_BATH) return k < a.thr[0] ? (v == 3 ? 12 : v) : (v == 12 ? 3 : v);
-        return k < a.thr[0] ? (v == 3 ? 12 : (v == 12 ? 3 : v)) : v;
+    // thr: draws below it act (ceil(0.8 * 2^23), or 2^22 for the heat bath).
+    __device__ static int flip(int v, uint32_t k, uint32_t thr) {
+        if (HEAT_BATH) return k < thr ? (v == 3 ? 12 : v) : (v == 12 ? 3 : v);
+        return k < thr ? (v == 3 ? 12 : (v == 12 ? 3 : v)) : v;
     }
-    __device__ static void apply(const WalkArgs& a, uint32_t d, int r, int c, uint32_t k) {
-        const int h = a.n / 2, i = r + 1, j = c + 1, at = i * h + j;
-        const uint32_t op = ph_op(d), ca = ph_a(d), cb = ph_b(d);
-        for (int l = 0; l < a.nlat; ++l) {
-            if (op == OP_STEP) {
-                int8_t* dst = static_cast<int8_t*>(a.arr[l][1 - ca]);
-                const bool upd = cb != NO_COLOUR && cb != ca;
-                const int v = upd ? refreshed(static_cast<const int8_t*>(a.arr[l][ca]), i, j, h, (int)cb)
-                                  : ld_site(dst + at);
-                const int nv = flip(v, k, a);
-                if (upd || nv != v) st_site(dst + at, nv);
-            } else {
-                st_site(static_cast<int8_t*>(a.arr[l][ca]) + at,
-                        refreshed(static_cast<const int8_t*>(a.arr[l][1 - ca]), i, j, h, (int)ca));
-            }
+    __device__ static void site(const WalkArgs&, const Ctx& x, int off, int i, int, uint32_t k) {
+        if (x.step) {
+            const int v = x.upd ? refreshed(x, off, i) : (int)x.dst[off];
+            x.dst[off] = (int8_t)flip(v, k, x.thr);
+        } else {
+            x.dst[off] = (int8_t)refreshed(x, off, i);
         }
     }
 };
 
-// ---------------------------------------------------------------------------
 // Shared skeleton of the three-colour models (lozenge, rect-triangle):
-// arrays arr[0..2] of N x N/3, position (r, c) = site (r, c), stream
-// c + (N/3) r; colour t's Update refreshes colours t+1 and t+2 (mod 3) at
-// interior sites 1 <= i <= N-2, 1 <= j <= N/3-2.
-// ---------------------------------------------------------------------------
+// arrays 0..2 of N x N/3, position (r, c) = site (r, c), stream c + (N/3) r;
+// colour t's Update refreshes colours t+1 and t+2 (mod 3) at interior sites
+// 1 <= i <= N-2, 1 <= j <= N/3-2.  `Rule::refresh` computes both refreshed
+// values from the flipped array; the diagonal neighbours' column shifts
+// depend on i mod 3 and are tabulated per phase (Rule::shift_table).
 template <class T, class Rule>
 struct ThreeColour {
+    using Elem = T;
+    static constexpr int NCOL = 3;
+    static constexpr int ROFF = 0;
+    static constexpr int COFF = 0;
+    __device__ static int flipped(int r) { return r; }
     __device__ static uint32_t stream_id(const WalkArgs& a, int r, int c) {
         return (uint32_t)c + (uint32_t)(a.n / 3) * (uint32_t)r;
     }
-    __device__ static void apply(const WalkArgs& a, uint32_t d, int r, int c, uint32_t k) {
-        const int m = a.n / 3, i = r, j = c;
-        const int at = i * m + j;
-        const bool interior = i >= 1 && i <= a.n - 2 && j >= 1 && j <= m - 2;
-        const uint32_t op = ph_op(d), ca = ph_a(d), cb = ph_b(d);
-        for (int l = 0; l < a.nlat; ++l) {
-            T* const* arr = reinterpret_cast<T* const*>(a.arr[l]);
-            if (op == OP_STEP) {
-                const bool upd = interior && cb != NO_COLOUR && cb != ca;
-                int v;
-                if (upd) {
-                    const int ia = (int)(cb + 1) % 3, ib = (int)(cb + 2) % 3;
-                    int na, nb;
-                    Rule::refresh(arr[cb], i, j, m, (int)cb, ld_site(arr[ia] + at), ld_site(arr[ib] + at), na, nb, a);
-                    if (ia == (int)ca) {
-                        v = na;
-                        st_site(arr[ib] + at, nb);
-                    } else {
-                        v = nb;
-                        st_site(arr[ia] + at, na);
-                    }
-                } else {
-                    v = ld_site(arr[ca] + at);
-                }
-                const int nv = Rule::flip(v, k, a);
-                if (upd || nv != v) st_site(arr[ca] + at, nv);
-            } else if (interior) {
-                const int ia = (int)(ca + 1) % 3, ib = (int)(ca + 2) % 3;
+    struct Ctx {
+        T* cur;      // colour flipped in this phase (STEP)
+        const T* f;  // colour whose Update is applied
+        T* pa;       // colour t+1
+        T* pb;       // colour t+2
+        bool step, upd, keep_a;
+        uint32_t shifts;
+        int w, imax, jmax;
+    };
+    __device__ static Ctx ctx(const WalkArgs& a, T* planes, int plane, uint32_t d) {
+        const int op = (int)ph_op(d), ca = (int)ph_a(d), cb = (int)ph_b(d);
+        Ctx x;
+        x.step = op == (int)OP_STEP;
+        x.w = a.wpad;
+        x.imax = a.n - 2;
+        x.jmax = a.n / 3 - 2;
+        const int t = x.step ? cb : ca;
+        x.upd = x.step ? (cb != (int)NO_COLOUR && cb != ca) : true;
+        x.cur = planes + (x.step ? ca : 0) * plane;
+        const int tt = x.upd ? t : 0;
+        x.f = planes + tt * plane;
+        x.pa = planes + ((tt + 1) % 3) * plane;
+        x.pb = planes + ((tt + 2) % 3) * plane;
+        x.keep_a = x.step && x.upd && (tt + 1) % 3 == ca;
+        x.shifts = Rule::shift_table(tt);
+        return x;
+    }
+    __device__ static void site(const WalkArgs& a, const Ctx& x, int off, int i, int j, uint32_t k) {
+        const bool interior = i >= 1 && i <= x.imax && j >= 1 && j <= x.jmax;
+        if (x.step) {
+            int v;
+            if (x.upd && interior) {
                 int na, nb;
-                Rule::refresh(arr[ca], i, j, m, (int)ca, ld_site(arr[ia] + at), ld_site(arr[ib] + at), na, nb, a);
-                st_site(arr[ia] + at, na);
-                st_site(arr[ib] + at, nb);
+                Rule::refresh(x.f, off, x.w, (x.shifts >> (3 * (i % 3))) & 7u, (int)x.pa[off], (int)x.pb[off], na, nb);
+                if (x.keep_a) {
+                    v = na;
+                    x.pb[off] = (T)nb;
+                } else {
+                    v = nb;
+                    x.pa[off] = (T)na;
+                }
+            } else {
+                v = (int)x.cur[off];
             }
+            x.cur[off] = (T)Rule::flip(v, k, a);
+        } else if (interior) {
+            int na, nb;
+            Rule::refresh(x.f, off, x.w, (x.shifts >> (3 * (i % 3))) & 7u, (int)x.pa[off], (int)x.pb[off], na, nb);
+            x.pa[off] = (T)na;
+            x.pb[off] = (T)nb;
         }
     }
 };
 
 // Lozenge (src/Lozenge/LozengeTiler.cpp:18-88; lozengekernel.cl, qlozengekernel.cl).
 // Flippable vertices: 25 = 1+8+16 (no cube) and 38 = 2+4+32 (cube).
-template <class T, bool QWEIGHT>
+template <bool QWEIGHT>
 struct LozengeRule {
     // UpdateTiles (lozengekernel.cl:36-54): colour t+1 refreshes bits {2,4,32},
-    // colour t+2 bits {1,8,16}; the column shift of the diagonal neighbours
-    // depends on i mod 3.
-    template <class P>
-    __device__ static void refresh(const P* f, int i, int j, int m, int t, int a_old, int b_old, int& na, int& nb,
-                                   const WalkArgs&) {
-        const int rr = i % 3;
-        const int sa = rr == (2 * t + 1) % 3, sw = rr == (2 * t + 2) % 3, se = rr == (2 * t) % 3;
-        na = (a_old & ~38) + ((ld_site(f + (i - 1) * m + j + sa) & 16) >> 3) + ((ld_site(f + i * m + j - sw) & 8) >> 1) +
-             ((ld_site(f + (i + 1) * m + j) & 1) << 5);
-        nb = (b_old & ~25) + ((ld_site(f + (i - 1) * m + j) & 32) >> 5) + ((ld_site(f + i * m + j + se) & 4) << 1) +
-             ((ld_site(f + (i + 1) * m + j - sa) & 2) << 3);
+    // colour t+2 bits {1,8,16}.  Per row class i mod 3: bit 0 = shift of the
+    // upper-right / lower-left reads, bit 1 = of the left read, bit 2 = of
+    // the right read.
+    __device__ static uint32_t shift_table(int t) {
+        uint32_t tab = 0;
+        for (int rr = 0; rr < 3; ++rr) {
+            const uint32_t sa = rr == (2 * t + 1) % 3, sw = rr == (2 * t + 2) % 3, se = rr == (2 * t) % 3;
+            tab |= (sa | (sw << 1) | (se << 2)) << (3 * rr);
+        }
+        return tab;
+    }
+    template <class T>
+    __device__ static void refresh(const T* f, int off, int w, uint32_t sh, int a_old, int b_old, int& na, int& nb) {
+        const int sa = sh & 1, sw = (sh >> 1) & 1, se = (sh >> 2) & 1;
+        na = (a_old & ~38) + (((int)f[off - w + sa] & 16) >> 3) + (((int)f[off - sw] & 8) >> 1) +
+             (((int)f[off + w] & 1) << 5);
+        nb = (b_old & ~25) + (((int)f[off - w] & 32) >> 5) + (((int)f[off + se] & 4) << 1) +
+             (((int)f[off + w - sa] & 2) << 3);
     }
     // Uniform (lozengekernel.cl:3-34): thr[0] = ceil(.4 * 2^23) adds a cube,
     // thr[1] = ceil(.8 * 2^23) removes one.
@@ -171,17 +239,25 @@ struct LozengeRule {
 // recttrianglekernel.cl).  A site holds six hex face digits.
 struct RectTriRule {
     __device__ static int digit(int x, int k) { return (int)(((unsigned)x >> (4 * k)) & 0xfu); }
-    // updateTiles1 / updateTiles2 (recttrianglekernel.cl:120-146).
-    template <class P>
-    __device__ static void refresh(const P* f, int i, int j, int m, int t, int, int, int& na, int& nb, const WalkArgs&) {
-        const int rr = i % 3;
-        const int s1 = rr == t, s2 = rr == (t + 1) % 3, s3 = rr == (t + 2) % 3;
-        const int up = ld_site(f + (i - 1) * m + j), side = ld_site(f + i * m + j + s1);
-        const int low = ld_site(f + (i + 1) * m + j - s2);
+    // updateTiles1 / updateTiles2 (recttrianglekernel.cl:120-146).  Per row
+    // class: bit 0 = shift of the side read of colour t+1 (s1), bit 1 = of
+    // the lower / upper-right reads (s2), bit 2 = of the side read of colour
+    // t+2 (s3).
+    __device__ static uint32_t shift_table(int t) {
+        uint32_t tab = 0;
+        for (int rr = 0; rr < 3; ++rr) {
+            const uint32_t s1 = rr == t, s2 = rr == (t + 1) % 3, s3 = rr == (t + 2) % 3;
+            tab |= (s1 | (s2 << 1) | (s3 << 2)) << (3 * rr);
+        }
+        return tab;
+    }
+    template <class T>
+    __device__ static void refresh(const T* f, int off, int w, uint32_t sh, int, int, int& na, int& nb) {
+        const int s1 = sh & 1, s2 = (sh >> 1) & 1, s3 = (sh >> 2) & 1;
+        const int up = f[off - w], side = f[off + s1], low = f[off + w - s2];
         na = (digit(up, 1) << 20) | (digit(up, 0) << 16) | (digit(side, 5) << 12) | (digit(low, 4) << 8) |
              (digit(low, 3) << 4) | digit(side, 2);
-        const int west = ld_site(f + i * m + j - s3), upr = ld_site(f + (i - 1) * m + j + s2);
-        const int down = ld_site(f + (i + 1) * m + j);
+        const int west = f[off - s3], upr = f[off - w + s2], down = f[off + w];
         nb = (digit(west, 3) << 20) | (digit(upr, 2) << 16) | (digit(upr, 1) << 12) | (digit(west, 0) << 8) |
              (digit(down, 5) << 4) | digit(down, 4);
     }

@@ -12,180 +12,333 @@
 
 namespace rtb {
 
-// Blocks until both neighbouring CTAs have completed `need` phases.  One
-// thread polls (acquire loads at gpu scope); the others wait at the barrier.
-// The wait is bounded: after a.timeout_ns of waiting, or when another CTA has
-// already raised an error, every CTA returns early and the host reports
-// RT_E_TIMEOUT.
-__device__ __forceinline__ bool wait_neighbours(const WalkArgs& a, int cta, unsigned need) {
-    __shared__ int s_abort;
-    if (threadIdx.x == 0) {
-        int abort_flag = 0;
-        uint64_t t0 = 0;
-        for (int side = 0; side < 2 && !abort_flag; ++side) {
-            const int nb = side == 0 ? cta - 1 : cta + 1;
-            if (nb < 0 || nb >= (int)gridDim.x) continue;
-            unsigned spins = 0;
-            while (ld_acquire(a.flags + nb) < need) {
-                if ((++spins & 15u) == 0u) {
-                    if (*(volatile int*)a.err) {
-                        abort_flag = 1;
-                        break;
-                    }
-                    const uint64_t now = global_ns();
-                    if (t0 == 0) {
-                        t0 = now;
-                    } else if (now - t0 > a.timeout_ns) {
-                        atomicOr(a.err, ERR_TIMEOUT);
-                        abort_flag = 1;
-                        break;
-                    }
-                    __nanosleep(64);
+// ---------------------------------------------------------------------------
+// Halo exchange.  After each flip phase a CTA publishes the first and last
+// row of its band (of the colour it just flipped) into a slot of global
+// memory; every 64-bit slot word carries 32 bits of lattice data and the
+// phase tag (phase + 1), so a neighbour knows the row is complete by polling
+// the words themselves -- no separate flag, no memory fence on the critical
+// path.  Slots are double-buffered by phase parity; a CTA enters phase p only
+// after both neighbours finished phase p-1, so a slot is never overwritten
+// before it was read.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long* slot(const WalkArgs& a, int cta, int side, int parity, int lat) {
+    return a.xbuf + ((((size_t)cta * 2 + side) * 2 + parity) * a.nlat + lat) * a.xwords;
+}
+
+template <class T>
+__device__ __forceinline__ uint32_t pack_word(const T* row, int w) {
+    if (sizeof(T) == 1) return reinterpret_cast<const uint32_t*>(row)[w];
+    return (uint32_t)row[w];
+}
+template <class T>
+__device__ __forceinline__ void unpack_word(T* row, int w, uint32_t v) {
+    if (sizeof(T) == 1)
+        reinterpret_cast<uint32_t*>(row)[w] = v;
+    else
+        row[w] = (T)v;
+}
+
+// Waits for one tagged word; returns false on timeout or when another CTA
+// already reported an error.
+__device__ __forceinline__ bool wait_word(const WalkArgs& a, const unsigned long long* p, uint32_t tag,
+                                          uint32_t* out, uint64_t& t0) {
+    unsigned spins = 0;
+    for (;;) {
+        const unsigned long long x = ld_relaxed64(p);
+        if ((uint32_t)(x >> 32) == tag) {
+            *out = (uint32_t)x;
+            return true;
+        }
+        if ((++spins & 63u) == 0u) {
+            if (*(volatile int*)a.err) return false;
+            const uint64_t now = global_ns();
+            if (t0 == 0) {
+                t0 = now;
+            } else if (now - t0 > a.timeout_ns) {
+                atomicOr(a.err, ERR_TIMEOUT);
+                return false;
+            }
+        }
+    }
+}
+
+// Shared memory of one CTA: the generator states of its positions (struct of
+// arrays s0[], s1[], s2[], s3[], so consecutive threads hit consecutive banks),
+// then the lattice band(s): for each lattice, NCOL colour planes of
+// (rows + 2 halo rows) x wpad elements.
+template <class Model, int BLOCK, bool UNIFORM>
+__global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ WalkArgs a) {
+    using T = typename Model::Elem;
+    constexpr int NC = Model::NCOL;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+
+    const int cta = blockIdx.x;
+    const int nct = gridDim.x;
+    const int tid = threadIdx.x;
+    const int r0 = cta * a.rows_per_cta;
+    const int r1 = min(a.rows, r0 + a.rows_per_cta);
+    const int a0 = r0 + Model::ROFF, a1 = r1 + Model::ROFF;  // owned colour-array rows
+    const int hr = a1 - a0 + 2;                                // + one halo row each side
+    const int W = a.wpad;
+    const int plane = hr * W;
+    const int cols = a.cols;
+    const int npos = max(0, r1 - r0) * cols;
+    const int spos = a.rows_per_cta * cols;  // state slots (same for every CTA)
+
+    uint32_t* s_st = reinterpret_cast<uint32_t*>(smem_raw);
+    T* lat = reinterpret_cast<T*>(smem_raw + (size_t)4 * spos * sizeof(uint32_t));
+    auto row_ptr = [&](int l, int c, int i) { return lat + ((size_t)l * NC + c) * plane + (size_t)(i - (a0 - 1)) * W; };
+
+    // Band + halo rows from the global colour arrays.
+    for (int l = 0; l < a.nlat; ++l)
+        for (int c = 0; c < NC; ++c) {
+            const T* g = static_cast<const T*>(a.arr[l][c]);
+            T* s = lat + ((size_t)l * NC + c) * plane;
+            for (int e = tid; e < plane; e += BLOCK) {
+                const int rr = a0 - 1 + e / W, j = e % W;
+                T v = (T)0;
+                if (rr >= 0 && rr < a.arows && j < a.width) v = g[(size_t)rr * a.width + j];
+                s[e] = v;
+            }
+        }
+
+    const TinyParams up{a.mat1, a.mat2, a.tmat};
+    auto params_of = [&](uint32_t sid) {
+        if (UNIFORM) return up;
+        const uint4 p = __ldg(a.params + sid);
+        return TinyParams{p.x, p.y, p.z};
+    };
+
+    // Positions in the band's first (last) row read the halo row that the CTA
+    // above (below) exchanges, so they are updated after the import ("edge"
+    // positions, spread over all threads); all other positions are updated
+    // before the wait, overlapping the neighbours' progress.
+    const bool has_top = cta > 0, has_bot = cta + 1 < nct;
+    const int q_lo = has_top ? min(cols, npos) : 0;
+    const int q_hi = has_bot ? max(q_lo, npos - cols) : npos;
+    const int top_n = has_top ? min(cols, npos) : 0;
+    const int bot_n = (has_bot && !(has_top && r1 - r0 == 1)) ? cols : 0;
+    const int n_edge = top_n + bot_n;
+    // Interior positions of this thread: q = q_lo + tid + m * BLOCK, walked
+    // with an incremental (row, column) instead of a division per site.
+    const int dr = BLOCK / cols, dc = BLOCK % cols;
+    const int q_first = q_lo + tid;
+    const int r_first = r0 + q_first / cols, c_first = q_first % cols;
+
+    int epoch = -1;
+    int64_t next_epoch = a.rng_kind == 0 && a.nepochs > 0 ? a.epoch_start[0] : INT64_MAX;
+    uint64_t t0 = 0;
+    uint32_t d = a.nphases > 0 ? __ldg(a.phases) : 0u;
+
+    __syncthreads();
+    for (int64_t ph = 0; ph < a.nphases; ++ph) {
+        const uint32_t d_next = ph + 1 < a.nphases ? __ldg(a.phases + ph + 1) : 0u;
+        if (ph == next_epoch) {
+            while (epoch + 1 < a.nepochs && a.epoch_start[epoch + 1] == ph) ++epoch;
+            next_epoch = epoch + 1 < a.nepochs ? a.epoch_start[epoch + 1] : INT64_MAX;
+            const uint32_t seed = a.epoch_seed[epoch];
+            for (int q = tid; q < npos; q += BLOCK) {
+                const uint32_t sid = Model::stream_id(a, r0 + q / cols, q % cols);
+                TinyState s;
+                tiny_seed(s, params_of(sid), seed + sid);
+                s_st[q] = s.s0;
+                s_st[spos + q] = s.s1;
+                s_st[2 * spos + q] = s.s2;
+                s_st[3 * spos + q] = s.s3;
+            }
+            __syncthreads();  // positions are drawn by other threads than the ones seeding them
+        }
+        const int op = (int)ph_op(d);
+        const bool draws = (d & PH_DRAWS) != 0u;
+        const typename Model::Ctx x0 = Model::ctx(a, lat, plane, d);
+        const typename Model::Ctx x1 = Model::ctx(a, lat + (size_t)NC * plane, plane, d);
+
+        auto site = [&](int q, int r, int c) {
+            uint32_t k = 0;
+            if (draws) {
+                if (a.rng_kind == 0) {
+                    const uint32_t sid = UNIFORM ? 0u : Model::stream_id(a, r, c);
+                    TinyState s{s_st[q], s_st[spos + q], s_st[2 * spos + q], s_st[3 * spos + q]};
+                    k = tiny_draw23(s, params_of(sid));
+                    s_st[q] = s.s0;
+                    s_st[spos + q] = s.s1;
+                    s_st[2 * spos + q] = s.s2;
+                    s_st[3 * spos + q] = s.s3;
+                } else {
+                    k = philox_first(Model::stream_id(a, r, c), (uint32_t)ph, (uint32_t)((uint64_t)ph >> 32), a.chain,
+                                     a.key0, a.key1) >> 9;
+                }
+            }
+            const int i = r + Model::ROFF, j = c + Model::COFF;
+            const int off = (r - r0 + 1) * W + j;
+            Model::site(a, x0, off, i, j, k);
+            if (a.nlat > 1) Model::site(a, x1, off, i, j, k);
+        };
+
+        {
+            int q = q_first, r = r_first, c = c_first;
+            while (q < q_hi) {
+                site(q, r, c);
+                q += BLOCK;
+                r += dr;
+                c += dc;
+                if (c >= cols) {
+                    c -= cols;
+                    ++r;
                 }
             }
         }
-        s_abort = abort_flag;
+        if (ph > 0) {
+            // Halo rows of the colour flipped in the previous phase.
+            const int pcol = Model::flipped(op == (int)OP_STEP ? (int)ph_b(d) : (int)ph_a(d));
+            const int par = (int)((ph - 1) & 1);
+            const uint32_t tag = (uint32_t)ph;
+            bool ok = true;
+            const int per_side = a.nlat * a.xwords;
+            for (int e = tid; e < 2 * per_side && ok; e += BLOCK) {
+                const int side = e / per_side;  // 0: row above (from cta-1), 1: row below (from cta+1)
+                const int rem = e % per_side;
+                const int l = rem / a.xwords, w = rem % a.xwords;
+                const int src = side == 0 ? cta - 1 : cta + 1;
+                if (src < 0 || src >= nct) continue;
+                uint32_t v;
+                ok = wait_word(a, slot(a, src, side == 0 ? 1 : 0, par, l) + w, tag, &v, t0);
+                if (ok) unpack_word<T>(row_ptr(l, pcol, side == 0 ? a0 - 1 : a1), w, v);
+            }
+            if (__syncthreads_or(!ok)) return;
+        }
+        for (int e = tid; e < n_edge; e += BLOCK) {
+            const bool top = e < top_n;
+            const int c = top ? e : e - top_n;
+            const int r = top ? r0 : r1 - 1;
+            site((r - r0) * cols + c, r, c);
+        }
+        __syncthreads();
+        if (op == (int)OP_STEP && ph + 1 < a.nphases) {
+            // Publish the band's first / last row of the colour just flipped.
+            const int col = Model::flipped((int)ph_a(d));
+            const int par = (int)(ph & 1);
+            const unsigned long long tag = (unsigned long long)(uint32_t)(ph + 1) << 32;
+            const int per_side = a.nlat * a.xwords;
+            for (int e = tid; e < 2 * per_side; e += BLOCK) {
+                const int side = e / per_side;  // 0: first row (read by cta-1), 1: last row (read by cta+1)
+                const int rem = e % per_side;
+                const int l = rem / a.xwords, w = rem % a.xwords;
+                const int dst = side == 0 ? cta - 1 : cta + 1;
+                if (dst < 0 || dst >= nct) continue;
+                const uint32_t v = pack_word<T>(row_ptr(l, col, side == 0 ? a0 : a1 - 1), w);
+                st_relaxed64(slot(a, cta, side, par, l) + w, tag | v);
+            }
+        }
+        d = d_next;
     }
+
+    // Owned rows back to the global colour arrays.
     __syncthreads();
-    return s_abort == 0;
-}
-
-__device__ __forceinline__ void publish(const WalkArgs& a, int cta, unsigned done) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        st_release(a.flags + cta, done);
-    }
-}
-
-template <class Model, int ITEMS, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) walk_kernel(const __grid_constant__ WalkArgs a) {
-    const int cta = blockIdx.x;
-    const int r0 = cta * a.rows_per_cta;
-    const int r1 = min(a.rows, r0 + a.rows_per_cta);
-    const int npos = max(0, r1 - r0) * a.cols;
-
-    int pr[ITEMS], pc[ITEMS];
-    uint32_t sid[ITEMS];
-    TinyState st[ITEMS];
-    TinyParams tp[ITEMS];
-#pragma unroll
-    for (int u = 0; u < ITEMS; ++u) {
-        const int q = (int)threadIdx.x + u * BLOCK;
-        pr[u] = q < npos ? r0 + q / a.cols : -1;
-        pc[u] = q < npos ? q % a.cols : 0;
-        sid[u] = pr[u] >= 0 ? Model::stream_id(a, pr[u], pc[u]) : 0u;
-        if (a.params != nullptr && pr[u] >= 0) {
-            const uint4 p = __ldg(a.params + sid[u]);
-            tp[u] = TinyParams{p.x, p.y, p.z};
-        } else {
-            tp[u] = TinyParams{a.mat1, a.mat2, a.tmat};
-        }
-        st[u] = TinyState{0u, 0u, 0u, 0u};
-    }
-
-    int epoch = -1;
-    for (int64_t ph = 0; ph < a.nphases; ++ph) {
-        if (a.rng_kind == 0) {
-            bool reseed = false;
-            while (epoch + 1 < a.nepochs && ph == a.epoch_start[epoch + 1]) {
-                ++epoch;
-                reseed = true;
-            }
-            if (reseed) {
-                const uint32_t seed = a.epoch_seed[epoch];
-#pragma unroll
-                for (int u = 0; u < ITEMS; ++u)
-                    if (pr[u] >= 0) tiny_seed(st[u], tp[u], seed + sid[u]);
+    for (int l = 0; l < a.nlat; ++l)
+        for (int c = 0; c < NC; ++c) {
+            T* g = static_cast<T*>(a.arr[l][c]);
+            for (int e = tid; e < (a1 - a0) * a.width; e += BLOCK) {
+                const int rr = a0 + e / a.width, j = e % a.width;
+                g[(size_t)rr * a.width + j] = row_ptr(l, c, rr)[j];
             }
         }
-        if (ph > 0 && !wait_neighbours(a, cta, (unsigned)ph)) return;
-        const uint32_t d = __ldg(a.phases + ph);
-        const bool draws = (d & PH_DRAWS) != 0u;
-#pragma unroll
-        for (int u = 0; u < ITEMS; ++u) {
-            if (pr[u] < 0) continue;
-            uint32_t k = 0;
-            if (draws) {
-                k = a.rng_kind == 0 ? tiny_draw23(st[u], tp[u])
-                                    : philox_first(sid[u], (uint32_t)ph, (uint32_t)((uint64_t)ph >> 32), a.chain,
-                                                   a.key0, a.key1) >> 9;
-            }
-            Model::apply(a, d, pr[u], pc[u], k);
-        }
-        publish(a, cta, (unsigned)(ph + 1));
-    }
 }
 
 // ---------------------------------------------------------------------------
-// Launch planning: the smallest per-thread item count whose CTA count fits
-// the cooperative co-residency limit.
+// Launch planning: the thinnest row bands whose CTAs are all co-resident
+// (cooperative launch) with their states and lattice band in shared memory.
 // ---------------------------------------------------------------------------
-constexpr int kBlock = 256;
+constexpr int kBlock = 1024;
 
 using KernelFn = void (*)(WalkArgs);
 
 template <class Model>
-static KernelFn pick_kernel(int items) {
-    switch (items) {
-        case 1: return walk_kernel<Model, 1, kBlock>;
-        case 2: return walk_kernel<Model, 2, kBlock>;
-        case 4: return walk_kernel<Model, 4, kBlock>;
-        default: return walk_kernel<Model, 8, kBlock>;
-    }
+static KernelFn pick_kernel(bool uniform) {
+    return uniform ? walk_kernel<Model, kBlock, true> : walk_kernel<Model, kBlock, false>;
 }
 
-static KernelFn kernel_for(int family, int items) {
+static KernelFn kernel_for(int family, bool uniform) {
     switch (family) {
-        case FAM_DOMINO: return pick_kernel<DominoRule<false>>(items);
-        case FAM_DOMINO_HB: return pick_kernel<DominoRule<true>>(items);
-        case FAM_LOZENGE8: return pick_kernel<ThreeColour<int8_t, LozengeRule<int8_t, false>>>(items);
-        case FAM_QLOZENGE32: return pick_kernel<ThreeColour<int32_t, LozengeRule<int32_t, true>>>(items);
-        case FAM_RECTTRI: return pick_kernel<ThreeColour<int32_t, RectTriRule>>(items);
+        case FAM_DOMINO: return pick_kernel<DominoRule<false>>(uniform);
+        case FAM_DOMINO_HB: return pick_kernel<DominoRule<true>>(uniform);
+        case FAM_LOZENGE8: return pick_kernel<ThreeColour<int8_t, LozengeRule<false>>>(uniform);
+        case FAM_QLOZENGE32: return pick_kernel<ThreeColour<int32_t, LozengeRule<true>>>(uniform);
+        case FAM_RECTTRI: return pick_kernel<ThreeColour<int32_t, RectTriRule>>(uniform);
         default: return nullptr;
     }
 }
 
-rt_status plan_walk(int family, int device, int rows, int cols, WalkPlan* plan, std::string* err) {
-    int sms = 0;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+static int family_ncol(int family) { return family <= FAM_DOMINO_HB ? 2 : 3; }
+static int family_elem(int family) { return family == FAM_QLOZENGE32 || family == FAM_RECTTRI ? 4 : 1; }
+
+size_t walk_smem_bytes(int family, int nlat, int rows_per_cta, int cols, int width) {
+    const int wpad = (width + 3) & ~3;
+    return (size_t)4 * 4 * rows_per_cta * cols +
+           (size_t)nlat * family_ncol(family) * (rows_per_cta + 2) * wpad * family_elem(family);
+}
+
+rt_status plan_walk(int family, int device, int nlat, int rows, int cols, int width, bool uniform, WalkPlan* plan,
+                    std::string* err) {
+    int sms = 0, smem_optin = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) {
         *err = "cudaDeviceGetAttribute failed";
         return RT_E_CUDA;
     }
-    static const int kItems[] = {1, 2, 4, 8};
-    for (int items : kItems) {
-        const int per_cta = kBlock * items;
-        if (cols > per_cta) continue;
-        const int rows_per_cta = std::max(1, per_cta / std::max(cols, 1));
-        const int ctas = (rows + rows_per_cta - 1) / rows_per_cta;
-        KernelFn fn = kernel_for(family, items);
-        if (!fn) {
-            *err = "unknown kernel family";
-            return RT_E_INVAL;
-        }
+    KernelFn fn = kernel_for(family, uniform);
+    if (!fn) {
+        *err = "unknown kernel family";
+        return RT_E_INVAL;
+    }
+    if (cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin) !=
+        cudaSuccess) {
+        *err = "cudaFuncSetAttribute failed";
+        return RT_E_CUDA;
+    }
+    const int wpad = (width + 3) & ~3;
+    for (int rpc = std::max(1, rows / (2 * sms)); rpc <= rows; ++rpc) {
+        const size_t smem = walk_smem_bytes(family, nlat, rpc, cols, width);
+        if (smem > (size_t)smem_optin) break;
+        const int ctas = (rows + rpc - 1) / rpc;
         int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, kBlock, 0) != cudaSuccess) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, kBlock, smem) != cudaSuccess) {
             *err = "cudaOccupancyMaxActiveBlocksPerMultiprocessor failed";
             return RT_E_CUDA;
         }
         if (ctas <= per_sm * sms) {
-            plan->items = items;
+            plan->items = (rpc * cols + kBlock - 1) / kBlock;
             plan->block = kBlock;
-            plan->rows_per_cta = rows_per_cta;
+            plan->rows_per_cta = rpc;
             plan->ctas = std::max(ctas, 1);
+            plan->smem = smem;
+            plan->wpad = wpad;
+            plan->xwords = family_elem(family) == 1 ? wpad / 4 : wpad;
             plan->fn = (const void*)fn;
             return RT_OK;
         }
     }
-    *err = "lattice too large for the register-resident walk (" + std::to_string(rows) + " x " + std::to_string(cols) +
-           " positions)";
+    *err = "lattice too large for the shared-memory-resident walk (" + std::to_string(rows) + " x " +
+           std::to_string(cols) + " positions)";
     return RT_E_INVAL;
 }
 
 rt_status launch_walk(const WalkPlan& plan, WalkArgs& args, cudaStream_t stream, std::string* err) {
     args.rows_per_cta = plan.rows_per_cta;
+    args.wpad = plan.wpad;
+    args.xwords = plan.xwords;
     void* kargs[] = {&args};
-    cudaError_t e = cudaLaunchCooperativeKernel(plan.fn, dim3(plan.ctas), dim3(plan.block), kargs, 0, stream);
+    cudaError_t e = cudaLaunchCooperativeKernel(plan.fn, dim3(plan.ctas), dim3(plan.block), kargs, plan.smem, stream);
     if (e != cudaSuccess) {
         *err = std::string("cooperative launch failed: ") + cudaGetErrorString(e);
         return RT_E_CUDA;

@@ -13,7 +13,7 @@ import ctypes
 
 import numpy as np
 
-from . import _capi
+from . import _capi, builders
 from ._capi import check
 
 
@@ -114,6 +114,17 @@ class _Tiler:
 class DominoTiler(_Tiler):
     MODEL = _capi.RT_DOMINO
 
+    # static helpers (src/Domino/DominoTiler.h:83-107)
+    Rectangle = staticmethod(lambda m, n: builders.call("rt_domino_rectangle", m, n))
+    AztecRectangle = staticmethod(lambda n, remove: builders.aztec_rectangle(n, remove))
+    AztecDiamond = staticmethod(lambda n: builders.call("rt_domino_aztec", n))
+    MaxTiling = staticmethod(lambda d: builders.call("rt_domino_max_tiling", d))
+    MinTiling = staticmethod(lambda d: builders.call("rt_domino_min_tiling", d))
+    DomainToVertices = staticmethod(lambda d: builders.call("rt_domino_domain_to_vertices", d))
+    TilingToDomain = staticmethod(lambda t: builders.call("rt_domino_tiling_to_domain", t))
+    HeightfuncToTiling = staticmethod(lambda h, d: builders.call("rt_domino_height_to_tiling", h, d))
+    TilingToHeightfunc = staticmethod(lambda t, d: builders.call("rt_domino_tiling_to_height", t, d))
+
     def Walk(self, t, steps, seed=None) -> None:  # noqa: N802 -- reference name
         """Walk(t, steps, seed) or Walk(t, [steps...], [seeds...]) (DominoTiler.h:73,76)."""
         if isinstance(steps, (list, tuple, np.ndarray)):
@@ -132,9 +143,23 @@ class DominoTiler(_Tiler):
 class LozengeTiler(_Tiler):
     MODEL = _capi.RT_LOZENGE
 
+    # static helpers (src/Lozenge/LozengeTiler.h:61-78)
+    AlmostHexDomain = staticmethod(lambda n, m: builders.call("rt_lozenge_almost_hex", n, m))
+    MaxTiling = staticmethod(lambda d: builders.call("rt_lozenge_max_tiling", d))
+    MinTiling = staticmethod(lambda d: builders.call("rt_lozenge_min_tiling", d))
+    DomainToVertices = staticmethod(lambda d: builders.call("rt_lozenge_domain_to_vertices", d))
+    TilingToDomain = staticmethod(lambda t: builders.call("rt_lozenge_tiling_to_domain", t))
+    HeightfuncToTiling = staticmethod(lambda h, d: builders.call("rt_lozenge_height_to_tiling", h, d))
+    TilingToHeightfunc = staticmethod(lambda t, d: builders.call("rt_lozenge_tiling_to_height", t, d))
+
 
 class RectTriangleTiler(_Tiler):
     MODEL = _capi.RT_RECTTRI
+
+    # static helpers (src/RectTriangle/RectTriangleTiler.h:60-66)
+    maxHex = staticmethod(lambda n: builders.call("rt_recttri_max_hex", n))
+    minHex = staticmethod(lambda n: builders.call("rt_recttri_min_hex", n))
+    LozengeToRectTriangle = staticmethod(lambda tl, dl: builders.call("rt_recttri_from_lozenge", tl, dl))
 
 
 class TriangleDimerTiler(_Tiler):
