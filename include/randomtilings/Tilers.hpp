@@ -1,0 +1,200 @@
+// Tilers.hpp -- header-only C++ layer with the reference's class and method
+// names over the C ABI of librt_b200.so.
+//
+// A caller of GPUTilings/RandomTilings keeps its code: `tiling`, `domain` and
+// `heightfunc` are std::vector<int> (src/common/common.h:43-45), Walk mutates
+// the tiling in place, builders return vectors by value.  The only change is
+// the constructor: the reference takes (cl::Context, cl::CommandQueue,
+// std::vector<cl::Device>, std::string kernelFile, cl_int&) and compiles an
+// OpenCL program; here it takes a device ordinal and the kernel variant.
+// Failures throw rt::Error (the reference throws cl::Error or exits).
+#pragma once
+
+#include <climits>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../rt_b200.h"
+#include "../rt_b200_host.h"
+
+namespace rt {
+
+typedef std::vector<int> domain;
+typedef std::vector<int> heightfunc;
+typedef std::vector<int> tiling;
+
+class Error : public std::runtime_error {
+public:
+    Error(rt_status s, const std::string& what) : std::runtime_error(what), status(s) {}
+    rt_status status;
+};
+
+namespace detail {
+inline void check(rt_status s, rt_tiler* h) {
+    if (s != RT_OK) throw Error(s, rt_last_error(h));
+}
+inline int side(const std::vector<int>& v) {
+    int n = 0;
+    while ((long long)(n + 1) * (n + 1) <= (long long)v.size()) ++n;
+    if ((long long)n * n != (long long)v.size()) throw Error(RT_E_INVAL, "array is not square");
+    return n;
+}
+// Calls a builder of rt_b200_host.h twice: size query, then fill.
+template <class F>
+std::vector<int> build(F f) {
+    int64_t len = 0;
+    check(f(nullptr, 0, &len), nullptr);
+    std::vector<int> out((size_t)len);
+    check(f(reinterpret_cast<int32_t*>(out.data()), len, &len), nullptr);
+    return out;
+}
+inline const int32_t* p(const std::vector<int>& v) { return reinterpret_cast<const int32_t*>(v.data()); }
+}  // namespace detail
+
+class TilerBase {
+protected:
+    rt_tiler* h_ = nullptr;
+    explicit TilerBase(int32_t model, int device, int32_t kernel) {
+        rt_config cfg;
+        rt_config_default(&cfg, model);
+        cfg.device = device;
+        cfg.kernel = kernel;
+        detail::check(rt_create(&cfg, &h_), nullptr);
+    }
+    explicit TilerBase(const rt_config& cfg) { detail::check(rt_create(&cfg, &h_), nullptr); }
+
+public:
+    TilerBase(const TilerBase&) = delete;
+    TilerBase& operator=(const TilerBase&) = delete;
+    ~TilerBase() {
+        if (h_) rt_destroy(h_);
+    }
+    // LoadTinyMT(std::string params, int size): the tinymt32dc parameter table.
+    void LoadTinyMT(const std::string& params, int size) {
+        detail::check(rt_load_rng_params(h_, params.c_str(), size), h_);
+    }
+    // Walk(tiling&, steps, seed).
+    void Walk(tiling& t, long steps, long seed) {
+        detail::check(rt_walk(h_, reinterpret_cast<int32_t*>(t.data()), detail::side(t), steps, seed), h_);
+    }
+    rt_tiler* handle() { return h_; }
+};
+
+// src/Domino/DominoTiler.h:43-115
+class DominoTiler : public TilerBase {
+public:
+    // cftp = true selects dominokernelCFTP.cl (monotone heat bath).
+    explicit DominoTiler(int device = 0, bool cftp = false)
+        : TilerBase(RT_DOMINO, device, cftp ? RT_KERNEL_CFTP : RT_KERNEL_DEFAULT) {}
+    explicit DominoTiler(const rt_config& cfg) : TilerBase(cfg) {}
+    using TilerBase::Walk;
+    // Walk(tiling&, vector<long> steps, vector<long> seeds): epochs, TinyMT re-seeded per epoch.
+    void Walk(tiling& t, const std::vector<long>& steps, const std::vector<long>& seeds) {
+        if (steps.size() != seeds.size()) throw Error(RT_E_INVAL, "steps and seeds differ in length");
+        std::vector<int64_t> st(steps.begin(), steps.end()), se(seeds.begin(), seeds.end());
+        detail::check(rt_walk_epochs(h_, reinterpret_cast<int32_t*>(t.data()), detail::side(t), st.data(), se.data(),
+                                     (int32_t)st.size()),
+                      h_);
+    }
+    static domain Rectangle(int M, int N) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) { return rt_domino_rectangle(M, N, o, c, l); });
+    }
+    static domain AztecRectangle(int N, const std::vector<int>& remove) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_domino_aztec_rectangle(N, detail::p(remove), (int32_t)remove.size(), o, c, l);
+        });
+    }
+    static domain AztecDiamond(int N) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) { return rt_domino_aztec(N, o, c, l); });
+    }
+    static tiling MaxTiling(const domain& d) {
+        return detail::build(
+            [&](int32_t* o, int64_t c, int64_t* l) { return rt_domino_max_tiling(detail::p(d), d.size(), o, c, l); });
+    }
+    static tiling MinTiling(const domain& d) {
+        return detail::build(
+            [&](int32_t* o, int64_t c, int64_t* l) { return rt_domino_min_tiling(detail::p(d), d.size(), o, c, l); });
+    }
+    static std::vector<int> DomainToVertices(const domain& d) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_domino_domain_to_vertices(detail::p(d), d.size(), o, c, l);
+        });
+    }
+    static domain TilingToDomain(const tiling& t) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_domino_tiling_to_domain(detail::p(t), t.size(), o, c, l);
+        });
+    }
+    static tiling HeightfuncToTiling(const heightfunc& hf, const domain& d) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_domino_height_to_tiling(detail::p(hf), hf.size(), detail::p(d), d.size(), o, c, l);
+        });
+    }
+    static heightfunc TilingToHeightfunc(const tiling& t, const domain& d) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_domino_tiling_to_height(detail::p(t), t.size(), detail::p(d), d.size(), o, c, l);
+        });
+    }
+};
+
+// src/Lozenge/LozengeTiler.h:35-79
+class LozengeTiler : public TilerBase {
+public:
+    // qweight = true selects qlozengekernel.cl (volume weight q, int32 storage).
+    explicit LozengeTiler(int device = 0, bool qweight = false)
+        : TilerBase(RT_LOZENGE, device, qweight ? RT_KERNEL_QWEIGHT : RT_KERNEL_DEFAULT) {}
+    explicit LozengeTiler(const rt_config& cfg) : TilerBase(cfg) {}
+    static domain AlmostHexDomain(int N, int M) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) { return rt_lozenge_almost_hex(N, M, o, c, l); });
+    }
+    static tiling MaxTiling(const domain& d) {
+        return detail::build(
+            [&](int32_t* o, int64_t c, int64_t* l) { return rt_lozenge_max_tiling(detail::p(d), d.size(), o, c, l); });
+    }
+    static tiling MinTiling(const domain& d) {
+        return detail::build(
+            [&](int32_t* o, int64_t c, int64_t* l) { return rt_lozenge_min_tiling(detail::p(d), d.size(), o, c, l); });
+    }
+    static std::vector<int> DomainToVertices(const domain& d) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_lozenge_domain_to_vertices(detail::p(d), d.size(), o, c, l);
+        });
+    }
+    static domain TilingToDomain(const tiling& t) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_lozenge_tiling_to_domain(detail::p(t), t.size(), o, c, l);
+        });
+    }
+    static tiling HeightfuncToTiling(const heightfunc& hf, const domain& d) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_lozenge_height_to_tiling(detail::p(hf), hf.size(), detail::p(d), d.size(), o, c, l);
+        });
+    }
+    static heightfunc TilingToHeightfunc(const tiling& t, const domain& d) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_lozenge_tiling_to_height(detail::p(t), t.size(), detail::p(d), d.size(), o, c, l);
+        });
+    }
+};
+
+// src/RectTriangle/RectTriangleTiler.h:30-73
+class RectTriangleTiler : public TilerBase {
+public:
+    explicit RectTriangleTiler(int device = 0) : TilerBase(RT_RECTTRI, device, RT_KERNEL_DEFAULT) {}
+    explicit RectTriangleTiler(const rt_config& cfg) : TilerBase(cfg) {}
+    static tiling maxHex(int N) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) { return rt_recttri_max_hex(N, o, c, l); });
+    }
+    static tiling minHex(int N) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) { return rt_recttri_min_hex(N, o, c, l); });
+    }
+    static tiling LozengeToRectTriangle(const tiling& tL, const domain& dL) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_recttri_from_lozenge(detail::p(tL), tL.size(), detail::p(dL), dL.size(), o, c, l);
+        });
+    }
+};
+
+}  // namespace rt

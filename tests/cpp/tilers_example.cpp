@@ -1,0 +1,44 @@
+// A reference-style caller of the C++ layer (include/randomtilings/Tilers.hpp):
+// the flow of the reference's MinimalLozengeEx / AztecDiamond examples with
+// the OpenCL set-up replaced by a device ordinal.  Used by the tests:
+//   tilers_example builders <out.txt>     host builders only (no GPU)
+//   tilers_example walk <out.txt>         + Walk on cuda:0
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+
+#include "randomtilings/Tilers.hpp"
+
+static void save(std::ofstream& f, const char* name, const std::vector<int>& v) {
+    f << name << " " << v.size();
+    for (int x : v) f << " " << x;
+    f << "\n";
+}
+
+int main(int argc, char** argv) {
+    if (argc < 3) return 2;
+    const bool walk = std::strcmp(argv[1], "walk") == 0;
+    std::ofstream f(argv[2]);
+    try {
+        rt::domain d = rt::LozengeTiler::AlmostHexDomain(10, 2);
+        rt::tiling t = rt::LozengeTiler::MaxTiling(d);
+        save(f, "lozenge_max", t);
+        save(f, "lozenge_hmax", rt::LozengeTiler::TilingToHeightfunc(t, d));
+        rt::domain a = rt::DominoTiler::AztecDiamond(12);
+        rt::tiling m = rt::DominoTiler::MinTiling(a);
+        save(f, "aztec_min", m);
+        if (walk) {
+            rt::LozengeTiler L(0);
+            L.Walk(t, 1000, 42);
+            save(f, "lozenge_walk", t);
+            rt::DominoTiler D(0, /*cftp=*/true);
+            std::vector<long> steps{256, 128}, seeds{2718281, 345903};
+            D.Walk(m, steps, seeds);
+            save(f, "aztec_epochs", m);
+        }
+    } catch (const rt::Error& e) {
+        std::fprintf(stderr, "rt::Error %d: %s\n", (int)e.status, e.what());
+        return 1;
+    }
+    return 0;
+}
