@@ -112,6 +112,22 @@ void* rt_stream(rt_tiler* h);
 /* Counters of the last run: phases executed and kernel launches issued. */
 rt_status rt_last_run_info(rt_tiler* h, int64_t* phases, int64_t* launches);
 
+/* No counterpart in the reference.  For callers that may not allocate GPU
+ * memory through the library -- programs that hand out all device memory
+ * from their own fixed pool, where a cudaMalloc/cudaFree inside a library
+ * would break their accounting and synchronise the device.  Same walk as
+ * rt_walk (TinyMT32J parameters, reference colour order), but `d_tiling` is
+ * the caller's DEVICE buffer (N*N int32, in and out) and no handle exists:
+ * every other byte the walk needs sits in one built-in device array of
+ * 16 MiB per GPU, kept until the process exits.  Walks that need more
+ * (tiling side x steps) are rejected with RT_E_INVAL.  The first call on a
+ * device looks the array up on that device; make it before any stream
+ * capture.  Calls share the array: calls that overlap on one GPU race.
+ * Synchronous on cfg->stream (NULL = the default stream).  A failure message
+ * goes to errbuf (errcap bytes) when errbuf is not NULL. */
+rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_tiling, int32_t n, int64_t steps, int64_t seed,
+                                 char* errbuf, size_t errcap);
+
 /* Text of the last failure on this handle (or of the last rt_create). */
 const char* rt_last_error(rt_tiler* h);
 const char* rt_version(void);

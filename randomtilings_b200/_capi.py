@@ -71,6 +71,8 @@ SIGNATURES = {
     "rt_last_run_info": (ctypes.c_int, [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
     "rt_last_error": (ctypes.c_char_p, [_P]),
     "rt_version": (ctypes.c_char_p, []),
+    "rt_walk_device_noalloc": (ctypes.c_int, [ctypes.POINTER(RtConfig), _P, _I32, _I64, _I64,
+                                              ctypes.POINTER(ctypes.c_char), ctypes.c_size_t]),
 }
 
 _PL = ctypes.POINTER(_I64)
