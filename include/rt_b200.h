@@ -99,6 +99,27 @@ rt_status rt_walk(rt_tiler* h, int32_t* tiling, int32_t n, int64_t steps, int64_
 rt_status rt_walk_epochs(rt_tiler* h, int32_t* tiling, int32_t n, const int64_t* steps, const int64_t* seeds,
                          int32_t k);
 
+/* Coupling from the past on the domino heat-bath chain (handle created with
+ * RT_KERNEL_CFTP).  Replaces the driver of Examples/AztecDiamondCftpEx.cpp:42-68
+ * over DominoTiler::Walk(tiling&, vector<long>, vector<long>)
+ * (src/Domino/DominoTiler.cpp:58-107): both chains (from tmax and tmin) run
+ * through the same epochs as two coupled lattices of one launch and are
+ * compared on the device.  Epoch seeds are successive std::mt19937(master_seed)
+ * outputs, newest epoch first.  schedule = RT_CFTP_REFERENCE prepends
+ * 2 * first_steps each trial (the example's +256 with first_steps = 128);
+ * RT_CFTP_DOUBLING doubles the total.  out_tiling (optional) receives the
+ * coalesced tiling. */
+typedef enum { RT_CFTP_DOUBLING = 0, RT_CFTP_REFERENCE = 1 } rt_cftp_schedule;
+typedef struct {
+    int64_t total_steps; /* colour steps from the past of the last trial */
+    int32_t trials;      /* trials run */
+    int32_t coalesced;   /* 1 if the chains met within max_trials */
+    double device_ms;    /* device time of the walks of all trials */
+} rt_cftp_stats;
+rt_status rt_cftp(rt_tiler* h, const int32_t* tmax, const int32_t* tmin, int32_t n, int64_t first_steps,
+                  int32_t schedule, int64_t master_seed, int32_t max_trials, int32_t* out_tiling,
+                  rt_cftp_stats* stats);
+
 /* Split form of rt_walk, for callers that keep the lattice on the device
  * (the reference re-uploads per Walk, DominoTiler.cpp:26-27,46-47):
  * upload + split into colour arrays, run steps (asynchronous on the handle's

@@ -69,6 +69,21 @@ rt_status rt_recttri_min_hex(int32_t side, int32_t* out, int64_t cap, int64_t* l
 rt_status rt_recttri_from_lozenge(const int32_t* tl, int64_t tlen, const int32_t* dl, int64_t dlen, int32_t* out,
                                   int64_t cap, int64_t* len);
 
+/* ---- triangular-lattice dimers (src/TriangleDimer/TriangleDimerTiler.h:182-195) ---- */
+/* TriangleDimerTiler::IceCreamCone(N, M), src/TriangleDimer/TriangleDimerTiler.cpp:485-581 */
+rt_status rt_tridimer_ice_cream_cone(int32_t side, int32_t cut, int32_t* out, int64_t cap, int64_t* len);
+/* TriangleDimerTiler::TestButterfly(type), :583-632 */
+rt_status rt_tridimer_test_butterfly(int32_t kind, int32_t* out, int64_t cap, int64_t* len);
+/* TriangleDimerTiler::TilingToTriangleFlips / TilingToButterflyFlips, :634-709 */
+rt_status rt_tridimer_triangle_flips(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len);
+rt_status rt_tridimer_butterfly_flips(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len);
+/* TriangleDimerTiler::TilingToVertices / TilingToDomain, :711-770 */
+rt_status rt_tridimer_vertices(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len);
+rt_status rt_tridimer_tiling_to_domain(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len);
+/* TriangleDimerTiler::DimerIndicator(t, c), :20-84 */
+rt_status rt_tridimer_dimer_indicator(const int32_t* t, int64_t tlen, int32_t orient, int32_t* out, int64_t cap,
+                                      int64_t* len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -122,6 +122,23 @@ def domino_walk_epochs(t, steps, seeds, cftp=True, params=None) -> np.ndarray:
     return a
 
 
+def cftp(tmax, tmin, first_steps: int, master_seed: int, schedule: str = "doubling", max_trials: int = 30):
+    """CFTP composed from the restated epoch walk, following
+    Examples/AztecDiamondCftpEx.cpp:42-68 (seeds: successive mt19937 outputs,
+    newest epoch first).  Returns (tiling, trials, total_steps, coalesced)."""
+    seeds_out = np.zeros(max_trials + 1, dtype=np.uint32)
+    oracle().orc_mt19937_stream(master_seed, max_trials + 1, seeds_out.ctypes.data)
+    steps, seeds = [first_steps], [int(seeds_out[0])]
+    for trial in range(max_trials):
+        top = domino_walk_epochs(tmax, steps, seeds, cftp=True)
+        bot = domino_walk_epochs(tmin, steps, seeds, cftp=True)
+        if np.array_equal(top, bot):
+            return top, trial + 1, sum(steps), True
+        steps.insert(0, 2 * steps[-1] if schedule == "reference" else sum(steps))
+        seeds.insert(0, int(seeds_out[trial + 1]))
+    return top, max_trials, sum(steps), False
+
+
 def lozenge_walk(t, steps, seed, qweight=False, q=0.99, qcmp_double=False, params=None) -> np.ndarray:
     a, n = _tiling(t)
     p, np_, keep = _table(params)

@@ -529,13 +529,474 @@ int orc_recttri_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint3
     return err;
 }
 
-/* Triangular-lattice dimers: not yet restated. */
+/* ------------------------------------------------------------------------ */
+/* Triangular-lattice dimers (bibone): src/TriangleDimer/TriangleDimerTiler */
+/* .cpp:86-483 and triangledimerkernel.cl.  Eight M x M int arrays (M =     */
+/* N/2): lozenge states H, L, R; triangle states U, D; butterfly states     */
+/* BH, BL, BR.  Each step flips one family (lozenge / triangle / butterfly) */
+/* of one orientation and class, then recomputes the dependent arrays by a  */
+/* fixed sequence of kernels; every kernel below is one NDRange (M, M),     */
+/* restated as a serial loop (each is race-free).                          */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int m;
+    int32_t *H, *L, *R, *U, *D, *BH, *BL, *BR;
+} td_state;
+
+#define TD(a, i, j) ((a)[(int64_t)(i) * st->m + (j)])
+#define TD_INTERIOR(i, j) ((i) >= 1 && (i) <= st->m - 2 && (j) >= 1 && (j) <= st->m - 2)
+
+static int dg(int32_t x, int k) { return (int)(((uint32_t)x >> (2 * k)) & 3u); } /* base-4 digit */
+static int cycle_up(int d) { return d == 0 ? 0 : d % 3 + 1; }          /* 1->2, 2->3, 3->1 */
+static int cycle_down(int d) { return d == 0 ? 0 : (d + 1) % 3 + 1; }  /* 1->3, 2->1, 3->2 */
+static int32_t bf_pack(int t1, int t4, int t16, int t64, int c) { return t1 + 4 * t4 + 16 * t16 + 64 * t64 + 256 * c; }
+
+/* RotateLozenges (triangledimerkernel.cl:4-22): every item draws; sites of
+ * orientation t and checkerboard class c toggle 5 <-> 10 when rd < .5. */
+static void td_rotate_lozenges(td_state* st, int32_t* A, int t, int c, orc_tinymt* rng) {
+    const int m = st->m;
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) {
+            const float rd = orc_tinymt_single01(&rng[(int64_t)j + (int64_t)m * i]);
+            const int cls = ((1 - (t & 1)) * i + ((1 + t) / 2) * j) % 2;
+            if ((double)rd < 0.5 && cls == c) {
+                int32_t* v = &TD(A, i, j);
+                if (*v == 5) *v = 10;
+                else if (*v == 10) *v = 5;
+            }
+        }
+}
+
+/* UpdateLozengesFlipped (:24-33): sites of the other class of the same
+ * orientation, from their four neighbours of the flipped class. */
+static void td_lozenges_flipped(td_state* st, int32_t* A, int t, int c) {
+    const int dj = t & 1, di = (2 - t) / 2;
+    for (int i = 1; i <= st->m - 2; ++i)
+        for (int j = 1; j <= st->m - 2; ++j) {
+            const int cls = ((1 - (t & 1)) * i + ((1 + t) / 2) * j) % 2;
+            if (cls == c) continue;
+            TD(A, i, j) = ((TD(A, i - 1, j + dj) >> 2) & 1) | (((TD(A, i - di, j + 1) >> 3) & 1) << 1) |
+                          ((TD(A, i + 1, j - dj) & 1) << 2) | (((TD(A, i + di, j - 1) >> 1) & 1) << 3);
+        }
+}
+
+/* UpdateLozenges0/1/2 (:35-78): the two other orientations take the bits they
+ * share with the flipped one. */
+static void td_lozenges_other(td_state* st, int t) {
+    for (int i = 1; i <= st->m - 2; ++i)
+        for (int j = 1; j <= st->m - 2; ++j) {
+            if (t == 0) {
+                const int32_t* f = st->H;
+                TD(st->L, i, j) = (TD(st->L, i, j) & ~10) | ((TD(f, i + 1, j) & 1) << 1) | ((TD(f, i + 1, j - 1) & 1) << 3);
+                TD(st->R, i, j) = (TD(st->R, i, j) & ~10) | (TD(f, i + 1, j) & 2) | (TD(f, i, j) & 8);
+            } else if (t == 1) {
+                const int32_t* f = st->L;
+                TD(st->R, i, j) = (TD(st->R, i, j) & ~5) | (TD(f, i, j) & 1) | ((TD(f, i + 1, j) & 1) << 2);
+                TD(st->H, i, j) = (TD(st->H, i, j) & ~5) | ((TD(f, i - 1, j) & 2) >> 1) | ((TD(f, i, j) & 2) << 1);
+            } else {
+                const int32_t* f = st->R;
+                TD(st->H, i, j) = (TD(st->H, i, j) & ~10) | (TD(f, i - 1, j) & 2) | ((TD(f, i, j - 1) & 2) << 2);
+                TD(st->L, i, j) = (TD(st->L, i, j) & ~5) | (TD(f, i, j) & 1) | (TD(f, i, j - 1) & 4);
+            }
+        }
+}
+
+/* UpdateTriangleUFromLozenges (:96-116). */
+static void td_up_from_lozenges(td_state* st) {
+    for (int i = 1; i <= st->m - 2; ++i)
+        for (int j = 1; j <= st->m - 2; ++j) {
+            const int32_t l0 = TD(st->L, i, j), l1 = TD(st->L, i, j + 1), h0 = TD(st->H, i, j), h1 = TD(st->H, i + 1, j);
+            const int a = ((l0 & 1) ? 1 : 0) + ((h0 & 8) ? 2 : 0) + ((h1 & 1) ? 3 : 0);
+            const int b = ((l1 & 1) ? 1 : 0) + ((h1 & 2) ? 2 : 0) + ((l1 & 2) ? 3 : 0);
+            const int c = ((l1 & 4) ? 1 : 0) + ((h1 & 8) ? 2 : 0) + ((h1 & 4) ? 3 : 0);
+            TD(st->U, i, j) = a + 4 * b + 16 * c;
+        }
+}
+
+/* UpdateButterflys{H,L,R}FromLozenge (:118-189). */
+static void td_butterfly_from_lozenges(td_state* st, int which) {
+    for (int i = 1; i <= st->m - 2; ++i)
+        for (int j = 1; j <= st->m - 2; ++j) {
+            int t1, t4, t16, t64, c;
+            if (which == 0) {
+                const int32_t h = TD(st->H, i, j), ru = TD(st->R, i - 1, j), lu = TD(st->L, i - 1, j + 1);
+                const int32_t r = TD(st->R, i, j), l = TD(st->L, i, j);
+                c = (lu >> 2) & 1;
+                t1 = ((ru >> 3) & 1) + 2 * (ru & 1) + 3 * (h & 1);
+                t4 = (lu & 1) + (lu & 2) + 3 * ((h >> 1) & 1);
+                t16 = ((r >> 1) & 1) + ((r >> 1) & 2) + 3 * ((h >> 2) & 1);
+                t64 = ((l >> 2) & 1) + ((l >> 2) & 2) + 3 * ((h >> 3) & 1);
+                TD(st->BH, i, j) = bf_pack(t1, t4, t16, t64, c);
+            } else if (which == 1) {
+                const int32_t l = TD(st->L, i, j), h = TD(st->H, i, j), r = TD(st->R, i, j);
+                const int32_t hd = TD(st->H, i + 1, j - 1), rw = TD(st->R, i, j - 1);
+                c = (r >> 3) & 1;
+                t1 = (h & 1) + (h & 2) + 3 * (l & 1);
+                t4 = ((r >> 1) & 1) + ((r >> 1) & 2) + 3 * ((l >> 1) & 1);
+                t16 = ((hd >> 2) & 1) + ((hd >> 2) & 2) + 3 * ((l >> 2) & 1);
+                t64 = ((rw >> 3) & 1) + 2 * (rw & 1) + 3 * ((l >> 3) & 1);
+                TD(st->BL, i, j) = bf_pack(t1, t4, t16, t64, c);
+            } else {
+                const int32_t r = TD(st->R, i, j), h = TD(st->H, i, j), le = TD(st->L, i, j + 1);
+                const int32_t hd = TD(st->H, i + 1, j), l = TD(st->L, i, j);
+                c = (le >> 3) & 1;
+                t1 = (h & 1) + (h & 2) + 3 * (r & 1);
+                t4 = (le & 1) + (le & 2) + 3 * ((r >> 1) & 1);
+                t16 = ((hd >> 2) & 1) + ((hd >> 2) & 2) + 3 * ((r >> 2) & 1);
+                t64 = ((l >> 2) & 1) + ((l >> 2) & 2) + 3 * ((r >> 3) & 1);
+                TD(st->BR, i, j) = bf_pack(t1, t4, t16, t64, c);
+            }
+        }
+}
+
+/* RotateTriangles (:191-211): class ((j-i) mod 3) == c toggles 45 <-> 54. */
+static void td_rotate_triangles(td_state* st, int32_t* A, int c, orc_tinymt* rng) {
+    const int m = st->m;
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) {
+            const float rd = orc_tinymt_single01(&rng[(int64_t)j + (int64_t)m * i]);
+            if ((double)rd < 0.5 && ((j - i) % 3 + 3) % 3 == c) {
+                int32_t* v = &TD(A, i, j);
+                if (*v == 45) *v = 54;
+                else if (*v == 54) *v = 45;
+            }
+        }
+}
+
+/* UpdateTrianglesFlipped0/1 (:213-253): same-kind triangles of the other two
+ * classes, one base-4 digit from each of three flipped-class neighbours. */
+static void td_triangles_flipped(td_state* st, int32_t* A, int up, int c) {
+    for (int i = 1; i <= st->m - 2; ++i)
+        for (int j = 1; j <= st->m - 2; ++j) {
+            const int cls = ((j - i) % 3 + 3) % 3;
+            if (cls == c) continue;
+            const int p = cls == (c + 1) % 3;
+            int32_t v;
+            if (up)
+                v = p ? dg(TD(A, i, j - 1), 1) + 4 * dg(TD(A, i - 1, j + 1), 2) + 16 * dg(TD(A, i + 1, j), 0)
+                      : dg(TD(A, i - 1, j), 2) + 4 * dg(TD(A, i, j + 1), 0) + 16 * dg(TD(A, i + 1, j - 1), 1);
+            else
+                v = p ? dg(TD(A, i, j - 1), 1) + 4 * dg(TD(A, i + 1, j), 2) + 16 * dg(TD(A, i - 1, j + 1), 0)
+                      : dg(TD(A, i + 1, j - 1), 2) + 4 * dg(TD(A, i, j + 1), 0) + 16 * dg(TD(A, i - 1, j), 1);
+            TD(A, i, j) = v;
+        }
+}
+
+/* UpdateTriangles (:255-275): down from up (t=0) or up from down (t=1). */
+static int td_tri_digit(int32_t v) {
+    return ((v & 48) == 16 ? 1 : 0) + ((v & 3) == 3 ? 2 : 0) + ((v & 12) == 8 ? 3 : 0);
+}
+static void td_triangles_other(td_state* st, const int32_t* A, int32_t* B, int t) {
+    const int p = t == 0 ? -1 : 1;
+    for (int i = 1; i <= st->m - 2; ++i)
+        for (int j = 1; j <= st->m - 2; ++j)
+            TD(B, i, j) = td_tri_digit(TD(A, i, j - 1 + t)) + 4 * td_tri_digit(TD(A, i, j + t)) +
+                          16 * td_tri_digit(TD(A, i + p, j));
+}
+
+/* UpdateLozenge{H,L,R}FromTriangles (:277-329). */
+static void td_lozenges_from_triangles(td_state* st) {
+    for (int i = 1; i <= st->m - 2; ++i)
+        for (int j = 1; j <= st->m - 2; ++j) {
+            const int32_t d = TD(st->D, i, j);
+            const int32_t uh = TD(st->U, i - 1, j), ul = TD(st->U, i, j - 1), ur = TD(st->U, i, j);
+            TD(st->H, i, j) = ((d & 48) == 32) + 2 * ((d & 48) == 48) + 4 * ((uh & 48) == 48) + 8 * ((uh & 48) == 32);
+            TD(st->L, i, j) = ((ul & 12) == 4) + 2 * ((ul & 12) == 12) + 4 * ((d & 3) == 1) + 8 * ((d & 3) == 2);
+            TD(st->R, i, j) = ((ur & 3) == 1) + 2 * ((d & 12) == 12) + 4 * ((d & 12) == 4) + 8 * ((ur & 3) == 2);
+        }
+}
+
+/* RotateButterflys (:331-353): slice (b1 i + b2 j) mod 3 == p1; within it the
+ * sites of parity p2 toggle 170 <-> 85 when rd < .5. */
+static void td_rotate_butterflies(td_state* st, int32_t* A, int t, int p1, int p2, orc_tinymt* rng) {
+    const int m = st->m;
+    const int b1 = 1 - (t & 1), b2 = (1 + t) / 2, b3 = t & 1;
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) {
+            const float rd = orc_tinymt_single01(&rng[(int64_t)j + (int64_t)m * i]);
+            if ((double)rd < 0.5 && (b1 * i + b2 * j) % 3 == p1 && ((b1 * j + b3 * i) & 1) == p2) {
+                int32_t* v = &TD(A, i, j);
+                if (*v == 170) *v = 85;
+                else if (*v == 85) *v = 170;
+            }
+        }
+}
+
+/* The three-pass butterfly update after a butterfly flip
+ * (UpdateButterflysFlipped{H,L,R}{1,21,22,23}, :356-652).  For orientation
+ * t the slice index and the positions of the neighbours differ; `nb` gives
+ * the neighbour cells of each pass. */
+static int td_slice(int t, int i, int j) { return t == 0 ? i % 3 : t == 1 ? j % 3 : (i + j) % 3; }
+static int td_par(int t, int i, int j) { return t == 1 ? (i & 1) : (j & 1); }
+
+static void td_butterfly_same_slice(td_state* st, int32_t* B, int t, int p1, int p2) {
+    for (int i = 1; i <= st->m - 2; ++i)
+        for (int j = 1; j <= st->m - 2; ++j) {
+            if (td_slice(t, i, j) != p1 || td_par(t, i, j) == p2) continue;
+            const int c = (TD(B, i, j) >> 8) & 1;
+            int t1, t4, t16, t64;
+            if (t == 2) {
+                const int32_t lo = TD(B, i + 1, j - 1), hi = TD(B, i - 1, j + 1);
+                t1 = cycle_down(dg(hi, 3));
+                t4 = cycle_up(dg(hi, 2));
+                t16 = cycle_down(dg(lo, 1));
+                t64 = cycle_up(dg(lo, 0));
+            } else {
+                const int32_t a = t == 0 ? TD(B, i, j - 1) : TD(B, i - 1, j);
+                const int32_t b = t == 0 ? TD(B, i, j + 1) : TD(B, i + 1, j);
+                t1 = cycle_up(dg(a, 1));
+                t4 = cycle_down(dg(b, 0));
+                t16 = cycle_up(dg(b, 3));
+                t64 = cycle_down(dg(a, 2));
+            }
+            TD(B, i, j) = bf_pack(t1, t4, t16, t64, c);
+        }
+}
+
+/* Pass 21 (first half of the adjacent slice) for H and L; R's first pass
+ * touches the slice p1+2 as well.  H: slice p1+1, neighbours above;
+ * L: slice p1+2, neighbours to the right; R: slice p1+2. */
+static void td_butterfly_pass21(td_state* st, int32_t* B, int t, int p1) {
+    const int want = t == 0 ? (p1 + 1) % 3 : (p1 + 2) % 3;
+    for (int i = 1; i <= st->m - 2; ++i)
+        for (int j = 1; j <= st->m - 2; ++j) {
+            if (td_slice(t, i, j) != want) continue;
+            const int32_t f = TD(B, i, j);
+            int t1, t4, t16, t64, c;
+            if (t == 2) {
+                const int32_t e = TD(B, i, j + 1), s = TD(B, i + 1, j);
+                c = dg(s, 0) == 1;
+                t1 = dg(f, 0);
+                t4 = dg(f, 1) == 2 ? 2 : (dg(e, 0) == 3) + 3 * (dg(e, 3) == 3);
+                t16 = dg(f, 2) == 1 ? 1 : 3 * (dg(s, 0) == 3) + 2 * (dg(s, 3) == 3);
+                t64 = dg(f, 3);
+            } else {
+                const int32_t a = t == 0 ? TD(B, i - 1, j) : TD(B, i - 1, j + 1);
+                const int32_t b = t == 0 ? TD(B, i - 1, j + 1) : TD(B, i, j + 1);
+                c = dg(a, 2) == 2;
+                t1 = dg(f, 0) == 2 ? 2 : (dg(a, 3) == 3) + 3 * (dg(a, 2) == 3);
+                t4 = dg(f, 1) == 1 ? 1 : 3 * (dg(b, 3) == 3) + 2 * (dg(b, 2) == 3);
+                t16 = dg(f, 2);
+                t64 = dg(f, 3);
+            }
+            TD(B, i, j) = bf_pack(t1, t4, t16, t64, c);
+        }
+}
+
+/* Pass 22: the other adjacent slice (H: p1+2, L and R: p1+1). */
+static void td_butterfly_pass22(td_state* st, int32_t* B, int t, int p1) {
+    const int want = t == 0 ? (p1 + 2) % 3 : (p1 + 1) % 3;
+    for (int i = 1; i <= st->m - 2; ++i)
+        for (int j = 1; j <= st->m - 2; ++j) {
+            if (td_slice(t, i, j) != want) continue;
+            const int32_t f = TD(B, i, j);
+            int t1, t4, t16, t64, c;
+            if (t == 2) {
+                const int32_t n1 = TD(B, i - 1, j), n2 = TD(B, i, j + 1), n3 = TD(B, i + 1, j), n4 = TD(B, i, j - 1);
+                c = dg(n1, 2) == 1;
+                t1 = dg(f, 0) == 1 ? 1 : 3 * (dg(n1, 2) == 3) + 2 * (dg(n1, 1) == 3);
+                t4 = (n2 & 256) ? 2 : (dg(f, 1) != 2) * dg(f, 1);
+                t16 = (n3 & 256) ? 1 : (dg(f, 2) != 1) * dg(f, 2);
+                t64 = dg(f, 3) == 2 ? 2 : (dg(n4, 2) == 3) + 3 * (dg(n4, 1) == 3);
+            } else {
+                const int32_t n1 = t == 0 ? TD(B, i - 1, j) : TD(B, i - 1, j + 1);
+                const int32_t n2 = t == 0 ? TD(B, i - 1, j + 1) : TD(B, i, j + 1);
+                const int32_t n3 = t == 0 ? TD(B, i + 1, j) : TD(B, i + 1, j - 1);
+                const int32_t n4 = t == 0 ? TD(B, i + 1, j - 1) : TD(B, i, j - 1);
+                c = dg(n3, 0) == 2;
+                t1 = (n1 & 256) ? 2 : (dg(f, 0) != 2) * dg(f, 0);
+                t4 = (n2 & 256) ? 1 : (dg(f, 1) != 1) * dg(f, 1);
+                t16 = dg(f, 2) == 2 ? 2 : 3 * (dg(n3, 0) == 3) + (dg(n3, 1) == 3);
+                t64 = dg(f, 3) == 1 ? 1 : 2 * (dg(n4, 0) == 3) + 3 * (dg(n4, 1) == 3);
+            }
+            TD(B, i, j) = bf_pack(t1, t4, t16, t64, c);
+        }
+}
+
+/* Pass 23: finishes the slice of pass 21. */
+static void td_butterfly_pass23(td_state* st, int32_t* B, int t, int p1) {
+    const int want = t == 0 ? (p1 + 1) % 3 : (p1 + 2) % 3;
+    for (int i = 1; i <= st->m - 2; ++i)
+        for (int j = 1; j <= st->m - 2; ++j) {
+            if (td_slice(t, i, j) != want) continue;
+            const int32_t f = TD(B, i, j);
+            const int c = (f >> 8) & 1;
+            int t1 = dg(f, 0), t4 = dg(f, 1), t16 = dg(f, 2), t64 = dg(f, 3);
+            if (t == 2) {
+                const int32_t n1 = TD(B, i - 1, j), n4 = TD(B, i, j - 1);
+                t1 = (n1 & 256) ? 1 : (dg(f, 0) != 1) * dg(f, 0);
+                t64 = (n4 & 256) ? 2 : (dg(f, 3) != 2) * dg(f, 3);
+            } else {
+                const int32_t n3 = t == 0 ? TD(B, i + 1, j) : TD(B, i + 1, j - 1);
+                const int32_t n4 = t == 0 ? TD(B, i + 1, j - 1) : TD(B, i, j - 1);
+                t16 = (n3 & 256) ? 2 : (dg(f, 2) != 2) * dg(f, 2);
+                t64 = (n4 & 256) ? 1 : (dg(f, 3) != 1) * dg(f, 3);
+            }
+            TD(B, i, j) = bf_pack(t1, t4, t16, t64, c);
+        }
+}
+
+/* UpdateLozengeFromButterflys{H,L,R} (:655-746). */
+static void td_lozenges_from_butterfly(td_state* st, int t) {
+    for (int i = 1; i <= st->m - 2; ++i)
+        for (int j = 1; j <= st->m - 2; ++j) {
+            const int32_t b = t == 0 ? TD(st->BH, i, j) : t == 1 ? TD(st->BL, i, j) : TD(st->BR, i, j);
+            const int d0 = dg(b, 0), d1 = dg(b, 1), d2 = dg(b, 2), d3 = dg(b, 3), c = (b >> 8) & 1;
+            const int32_t own = (d0 == 3) + 2 * (d1 == 3) + 4 * (d2 == 3) + 8 * (d3 == 3);
+            if (t == 0) {
+                TD(st->H, i, j) = own;
+                TD(st->L, i, j) = c + 2 * (d2 == 3) + 4 * (d3 == 1) + 8 * (d3 == 2);
+                TD(st->R, i, j) = c + 2 * (d2 == 1) + 4 * (d2 == 2) + 8 * (d3 == 3);
+            } else if (t == 1) {
+                TD(st->L, i, j) = own;
+                TD(st->R, i, j) = (d0 == 3) + 2 * (d1 == 1) + 4 * (d1 == 2) + 8 * c;
+                TD(st->H, i, j) = (d0 == 1) + 2 * (d0 == 2) + 4 * (d1 == 3) + 8 * c;
+            } else {
+                TD(st->R, i, j) = own;
+                TD(st->H, i, j) = (d0 == 1) + 2 * (d0 == 2) + 4 * c + 8 * (d3 == 3);
+                TD(st->L, i, j) = (d0 == 3) + 2 * c + 4 * (d3 == 1) + 8 * (d3 == 2);
+            }
+        }
+}
+
+/* TilingToTriangleFlips / TilingToButterflyFlips (TriangleDimerTiler.cpp:634-709):
+ * the derived arrays the host builds before a walk. */
+static void td_derive(const int32_t* t, int n, int32_t* tri, int32_t* bfl) {
+#define T(i, j) t[(int64_t)(i) * n + (j)]
+    for (int64_t k = 0; k < (int64_t)(n / 2) * n; ++k) tri[k] = 0;
+    for (int64_t k = 0; k < (int64_t)n * n; ++k) bfl[k] = 0;
+    for (int i = 1; i < n / 2 - 1; ++i)
+        for (int j = 1; j < n - 1; ++j) {
+            const int32_t a = T(2 * i + 1, j), b = T(2 * i + 1, j + 1);
+            int32_t v;
+            if (j % 2 == 0) {
+                const int32_t c = T(2 * i, j + 1);
+                v = (((a >> 2) & 1) + ((a >> 2) & 2) + 3 * ((b >> 3) & 1)) +
+                    4 * (((b >> 2) & 1) + (a & 2) + 3 * ((b >> 1) & 1)) +
+                    16 * (2 * (c & 1) + (a & 1) + 3 * ((c >> 1) & 1));
+            } else {
+                const int32_t c = T(2 * i + 2, j);
+                v = ((a & 1) + ((a >> 2) & 2) + 3 * ((b >> 3) & 1)) + 4 * ((b & 1) + (a & 2) + 3 * ((b >> 1) & 1)) +
+                    16 * (((c >> 2) & 2) + 3 * ((c >> 2) & 1) + ((a >> 2) & 1));
+            }
+            tri[(int64_t)i * n + j] = v;
+        }
+    for (int i = 2; i < n - 2; ++i)
+        for (int j = 2; j < n - 2; ++j) {
+            int f1, f4, f16, f64, c;
+            const int32_t x = T(i, j);
+            if (i % 2 == 0) {
+                if (j % 2 == 0) continue;
+                const int32_t u = T(i - 1, j), ue = T(i - 1, j + 1), d = T(i + 1, j), dw = T(i + 1, j - 1);
+                f1 = ((u >> 3) & 1) + 2 * (u & 1) + 3 * (x & 1);
+                f4 = (ue & 1) + (ue & 2) + 3 * ((x >> 1) & 1);
+                f16 = ((d >> 1) & 1) + ((d >> 1) & 2) + 3 * ((x >> 2) & 1);
+                f64 = ((dw >> 2) & 1) + ((dw >> 2) & 2) + 3 * ((x >> 3) & 1);
+                c = (ue >> 2) & 1;
+            } else if (j % 2 == 0) {
+                const int32_t ue = T(i - 1, j + 1), e = T(i, j + 1), dw = T(i + 1, j - 1), w = T(i, j - 1);
+                f1 = (ue & 1) + (ue & 2) + 3 * (x & 1);
+                f4 = ((e >> 1) & 1) + ((e >> 1) & 2) + 3 * ((x >> 1) & 1);
+                f16 = ((dw >> 2) & 1) + ((dw >> 2) & 2) + 3 * ((x >> 2) & 1);
+                f64 = ((w >> 3) & 1) + 2 * (w & 1) + 3 * ((x >> 3) & 1);
+                c = (e >> 3) & 1;
+            } else {
+                const int32_t u = T(i - 1, j), e = T(i, j + 1), d = T(i + 1, j), w = T(i, j - 1);
+                f1 = (u & 1) + (u & 2) + 3 * (x & 1);
+                f4 = (e & 1) + (e & 2) + 3 * ((x >> 1) & 1);
+                f16 = ((d >> 2) & 1) + ((d >> 2) & 2) + 3 * ((x >> 2) & 1);
+                f64 = ((w >> 2) & 1) + ((w >> 2) & 2) + 3 * ((x >> 3) & 1);
+                c = (e >> 3) & 1;
+            }
+            bfl[(int64_t)i * n + j] = f1 + 4 * f4 + 16 * f16 + 64 * f64 + 256 * c;
+        }
+#undef T
+}
+
 int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams) {
-    (void)t;
-    (void)n;
-    (void)steps;
-    (void)seed;
-    (void)params;
-    (void)nparams;
-    return ORC_EINVAL;
+    if (n < 8 || n % 2) return ORC_EINVAL;
+    const int m = n / 2;
+    const size_t mm = (size_t)m * m;
+    int32_t* buf = (int32_t*)calloc(8 * mm, sizeof(int32_t));
+    int32_t* tri = (int32_t*)calloc((size_t)(n / 2) * n, sizeof(int32_t));
+    int32_t* bfl = (int32_t*)calloc((size_t)n * n, sizeof(int32_t));
+    if (!buf || !tri || !bfl) {
+        free(buf);
+        free(tri);
+        free(bfl);
+        return ORC_ENOMEM;
+    }
+    td_state S = {m, buf, buf + mm, buf + 2 * mm, buf + 3 * mm, buf + 4 * mm, buf + 5 * mm, buf + 6 * mm, buf + 7 * mm};
+    td_state* st = &S;
+    td_derive(t, n, tri, bfl);
+    /* Split (TriangleDimerTiler.cpp:107-133). */
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            const int64_t at = (int64_t)(i / 2) * m + j / 2;
+            if (i % 2 == 0) {
+                if (j % 2 == 1) S.H[at] = t[(int64_t)i * n + j], S.BH[at] = bfl[(int64_t)i * n + j];
+            } else if (j % 2 == 0) {
+                S.L[at] = t[(int64_t)i * n + j], S.BL[at] = bfl[(int64_t)i * n + j];
+            } else {
+                S.R[at] = t[(int64_t)i * n + j], S.BR[at] = bfl[(int64_t)i * n + j];
+            }
+        }
+    for (int i = 0; i < n / 2; ++i)
+        for (int j = 0; j < n; ++j) (j % 2 == 0 ? S.D : S.U)[(int64_t)i * m + j / 2] = tri[(int64_t)i * n + j];
+    int err;
+    orc_tinymt* rng = tmt_streams((int64_t)mm, (uint32_t)(uint64_t)seed, params, nparams, &err);
+    if (rng) {
+        minstd g;
+        minstd_seed(&g, seed);
+        int32_t* lz[3] = {S.H, S.L, S.R};
+        int32_t* bf[3] = {S.BH, S.BL, S.BR};
+        for (int64_t s = 0; s < steps; ++s) {
+            const int kind = uniform_int(&g, 2), r1 = uniform_int(&g, 2), r2 = uniform_int(&g, 1);
+            if (kind == 0) { /* lozenge flips, TriangleDimerTiler.cpp:243-278 */
+                td_rotate_lozenges(st, lz[r1], r1, r2, rng);
+                td_lozenges_flipped(st, lz[r1], r1, r2);
+                td_lozenges_other(st, r1);
+                td_up_from_lozenges(st);
+                td_triangles_other(st, S.U, S.D, 0);
+                for (int w = 0; w < 3; ++w) td_butterfly_from_lozenges(st, w);
+            } else if (kind == 1) { /* triangle flips, :279-305 */
+                int32_t* A = r2 == 1 ? S.D : S.U;
+                td_rotate_triangles(st, A, r1, rng);
+                td_triangles_flipped(st, A, r2 == 0, r1);
+                if (r2 == 1)
+                    td_triangles_other(st, S.D, S.U, 1);
+                else
+                    td_triangles_other(st, S.U, S.D, 0);
+                td_lozenges_from_triangles(st);
+                for (int w = 0; w < 3; ++w) td_butterfly_from_lozenges(st, w);
+            } else { /* butterfly flips, :306-347 */
+                const int p1 = uniform_int(&g, 2), p2 = uniform_int(&g, 1);
+                td_rotate_butterflies(st, bf[r1], r1, p1, p2, rng);
+                td_butterfly_same_slice(st, bf[r1], r1, p1, p2);
+                td_butterfly_pass21(st, bf[r1], r1, p1);
+                td_butterfly_pass22(st, bf[r1], r1, p1);
+                td_butterfly_pass23(st, bf[r1], r1, p1);
+                td_lozenges_from_butterfly(st, r1);
+                for (int w = 0; w < 3; ++w)
+                    if (w != r1) td_butterfly_from_lozenges(st, w);
+                td_up_from_lozenges(st);
+                td_triangles_other(st, S.U, S.D, 0);
+            }
+        }
+        free(rng);
+        /* Only the lozenge states go back into the tiling (:362-376). */
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                const int64_t at = (int64_t)(i / 2) * m + j / 2;
+                if (i % 2 == 0) {
+                    if (j % 2 == 1) t[(int64_t)i * n + j] = S.H[at];
+                } else {
+                    t[(int64_t)i * n + j] = j % 2 == 0 ? S.L[at] : S.R[at];
+                }
+            }
+    }
+    free(buf);
+    free(tri);
+    free(bfl);
+    return err;
 }

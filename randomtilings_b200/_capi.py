@@ -50,6 +50,17 @@ class RtConfig(ctypes.Structure):
     ]
 
 
+class RtCftpStats(ctypes.Structure):
+    _fields_ = [
+        ("total_steps", ctypes.c_int64),
+        ("trials", ctypes.c_int32),
+        ("coalesced", ctypes.c_int32),
+        ("device_ms", ctypes.c_double),
+    ]
+
+
+RT_CFTP_DOUBLING, RT_CFTP_REFERENCE = 0, 1
+
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
 _I64 = ctypes.c_int64
@@ -63,6 +74,7 @@ SIGNATURES = {
     "rt_set_rng_params": (ctypes.c_int, [_P, _P, _I64]),
     "rt_walk": (ctypes.c_int, [_P, _P, _I32, _I64, _I64]),
     "rt_walk_epochs": (ctypes.c_int, [_P, _P, _I32, _P, _P, _I32]),
+    "rt_cftp": (ctypes.c_int, [_P, _P, _P, _I32, _I64, _I32, _I64, _I32, _P, ctypes.POINTER(RtCftpStats)]),
     "rt_upload": (ctypes.c_int, [_P, _P, _I32]),
     "rt_run": (ctypes.c_int, [_P, _I64, _I64]),
     "rt_download": (ctypes.c_int, [_P, _P]),
@@ -97,6 +109,13 @@ HOST_SIGNATURES = {
     "rt_recttri_max_hex": [_I32],
     "rt_recttri_min_hex": [_I32],
     "rt_recttri_from_lozenge": [_P, _I64, _P, _I64],
+    "rt_tridimer_ice_cream_cone": [_I32, _I32],
+    "rt_tridimer_test_butterfly": [_I32],
+    "rt_tridimer_triangle_flips": [_P, _I64],
+    "rt_tridimer_butterfly_flips": [_P, _I64],
+    "rt_tridimer_vertices": [_P, _I64],
+    "rt_tridimer_tiling_to_domain": [_P, _I64],
+    "rt_tridimer_dimer_indicator": [_P, _I64, _I32],
 }
 for _name, _args in HOST_SIGNATURES.items():
     SIGNATURES[_name] = (ctypes.c_int, [*_args, _P, _I64, _PL])

@@ -19,6 +19,7 @@
 
 #include "rt_internal.h"
 #include "rt_models.cuh"
+#include "rt_tridimer.cuh"
 
 using namespace rtb;
 
@@ -97,10 +98,14 @@ struct rt_tiler {
     int64_t d_params_n = 0;
 
     int n = 0, rows = 0, cols = 0;
+    int arows = 0, width = 0;  // shape of one colour array
     int nlat = 1;
     DevBuf d_arr_block;  // all colour arrays of all lattices
     void* d_arr[2][8] = {};
-    DevBuf d_tiling;
+    DevBuf d_tiling, d_tiling2;
+    size_t per_arr_al = 0;  // bytes of one colour array (256-aligned)
+    DevBuf d_count;
+    PinnedBuf h_count;
     bool uploaded = false;
 
     DevBuf d_phases, d_epoch_start, d_epoch_seed, d_xbuf, d_err;
@@ -161,6 +166,10 @@ rt_status rt_create(const rt_config* cfg, rt_tiler** out) {
         case RT_RECTTRI:
             if (cfg->kernel != RT_KERNEL_DEFAULT) break;
             family = FAM_RECTTRI, ncol = 3, kind = 2, elem = 4;
+            break;
+        case RT_TRIDIMER:
+            if (cfg->kernel != RT_KERNEL_DEFAULT) break;
+            family = FAM_TRIDIMER, ncol = 8, kind = 3, elem = 4;
             break;
         default:
             break;
@@ -272,7 +281,9 @@ rt_status rt_load_rng_params(rt_tiler* h, const char* path, int64_t n) {
 
 static rt_status check_size(rt_tiler* h, int n) {
     if (h->kind == 0 && (n < 6 || n % 2 != 0)) return h->fail(RT_E_INVAL, "domino tiling side must be even and >= 6");
-    if (h->kind != 0 && (n < 9 || n % 3 != 0))
+    if (h->kind == 3 && (n < 8 || n % 2 != 0))
+        return h->fail(RT_E_INVAL, "triangle-dimer tiling side must be even and >= 8");
+    if ((h->kind == 1 || h->kind == 2) && (n < 9 || n % 3 != 0))
         return h->fail(RT_E_INVAL, "tiling side must be a multiple of 3 and >= 9");
     return RT_OK;
 }
@@ -281,9 +292,24 @@ static void grid_of(const rt_tiler* h, int n, int* rows, int* cols) {
     if (h->kind == 0) {  // Rotate NDRange (N-2, N/2-2), DominoTiler.cpp:37
         *rows = n - 2;
         *cols = n / 2 - 2;
+    } else if (h->kind == 3) {  // (M, M), TriangleDimerTiler.cpp:246
+        *rows = n / 2;
+        *cols = n / 2;
     } else {  // (N, N/3), LozengeTiler.cpp:58, RectTriangleTiler.cpp:51
         *rows = n;
         *cols = n / 3;
+    }
+}
+
+// Shape of one colour array: domino N x N/2, three-colour N x N/3,
+// triangle-dimer N/2 x N/2.
+static void array_shape(const rt_tiler* h, int n, int* arows, int* width) {
+    if (h->kind == 3) {
+        *arows = n / 2;
+        *width = n / 2;
+    } else {
+        *arows = n;
+        *width = n / h->ncol;
     }
 }
 
@@ -292,22 +318,41 @@ rt_status rt_upload(rt_tiler* h, const int32_t* tiling, int32_t n) {
     rt_status s = check_size(h, n);
     if (s != RT_OK) return s;
     cudaSetDevice(h->cfg.device);
-    const size_t per_arr = (size_t)n * (size_t)(n / h->ncol) * (size_t)h->elem;
+    int arows, width;
+    array_shape(h, n, &arows, &width);
+    const size_t per_arr = (size_t)arows * (size_t)width * (size_t)h->elem;
     const size_t per_arr_al = (per_arr + 255) & ~(size_t)255;
+    h->per_arr_al = per_arr_al;
     if (!h->d_arr_block.reserve(per_arr_al * h->ncol * 2)) return h->fail(RT_E_NOMEM, "cudaMalloc lattice");
     if (!h->d_tiling.reserve((size_t)n * n * 4)) return h->fail(RT_E_NOMEM, "cudaMalloc tiling");
     for (int l = 0; l < 2; ++l)
         for (int c = 0; c < 8; ++c)
             h->d_arr[l][c] = c < h->ncol ? static_cast<char*>(h->d_arr_block.p) + (l * h->ncol + c) * per_arr_al : nullptr;
-    cudaError_t e = cudaMemcpyAsync(h->d_tiling.p, tiling, (size_t)n * n * 4, cudaMemcpyHostToDevice, h->stream);
+    // Alignment padding between the colour arrays is compared by the CFTP
+    // coalescence test, so it must hold the same bytes in both lattices.
+    cudaError_t e = cudaMemsetAsync(h->d_arr_block.p, 0, per_arr_al * h->ncol * 2, h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "memset lattice");
+    e = cudaMemcpyAsync(h->d_tiling.p, tiling, (size_t)n * n * 4, cudaMemcpyHostToDevice, h->stream);
     if (e != cudaSuccess) return h->cuda_fail(e, "upload");
-    s = launch_split(false, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0], h->stream,
-                     &h->err);
-    if (s != RT_OK) return s;
+    if (h->kind == 3) {
+        // The eight triangle-dimer arrays are derived on the host
+        // (TriangleDimerTiler.cpp:90-133) and copied up as they are.
+        std::vector<int32_t> arrays((size_t)8 * arows * width);
+        td_split_host(tiling, n, arrays.data());
+        for (int c = 0; c < 8 && e == cudaSuccess; ++c)
+            e = cudaMemcpy(h->d_arr[0][c], arrays.data() + (size_t)c * arows * width, per_arr, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return h->cuda_fail(e, "upload of the triangle-dimer arrays");
+    } else {
+        s = launch_split(false, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0],
+                         h->stream, &h->err);
+        if (s != RT_OK) return s;
+    }
     if (!h->d_err.reserve(sizeof(int)) || !h->h_err.reserve(sizeof(int))) return h->fail(RT_E_NOMEM, "error word");
     e = cudaMemsetAsync(h->d_err.p, 0, sizeof(int), h->stream);
     if (e != cudaSuccess) return h->cuda_fail(e, "memset");
     h->n = n;
+    h->arows = arows;
+    h->width = width;
     grid_of(h, n, &h->rows, &h->cols);
     h->uploaded = true;
     return RT_OK;
@@ -371,10 +416,12 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     h->last_phases = 0;
     h->last_launches = 0;
     if (total == 0) return RT_OK;
-    const int64_t nph = total + 1;  // + the final Update
+    // At most 7 phases per triangle-dimer step; one per step + the final
+    // Update for the colour models.
+    const int64_t cap_ph = h->kind == 3 ? 7 * total : total + 1;
     // The staging buffers may still feed the previous run's copies.
     cudaEventSynchronize(h->ev_staged);
-    if (!h->h_phases.reserve((size_t)nph * 4) || !h->d_phases.reserve((size_t)nph * 4) ||
+    if (!h->h_phases.reserve((size_t)cap_ph * 4) || !h->d_phases.reserve((size_t)cap_ph * 4) ||
         !h->h_epoch_start.reserve((size_t)k * 8) || !h->d_epoch_start.reserve((size_t)k * 8) ||
         !h->h_epoch_seed.reserve((size_t)k * 4) || !h->d_epoch_seed.reserve((size_t)k * 4))
         return h->fail(RT_E_NOMEM, "schedule buffers");
@@ -393,6 +440,40 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
                 ph[at++] = make_phase(OP_STEP, r, prev, true);
                 prev = r;
             }
+        } else if (h->kind == 3) {
+            // TriangleDimerTiler.cpp:230-348: per step the flip family, the
+            // orientation / class and the kind (or parity), and for butterflies
+            // the slice and parity, all from one default_random_engine.
+            std::default_random_engine generator;
+            std::uniform_int_distribution<int> d1(0, 2), d2(0, 1);
+            generator.seed(seeds[e]);
+            sd[e] = (uint32_t)seeds[e];
+            for (int64_t s = 0; s < steps[e]; ++s) {
+                const uint32_t kind = (uint32_t)d1(generator), r1 = (uint32_t)d1(generator),
+                               r2 = (uint32_t)d2(generator);
+                if (kind == 0) {  // lozenge flips, :243-278
+                    ph[at++] = make_phase(TD_ROT_LOZ, r1, r2, true);
+                    ph[at++] = make_phase(TD_LOZ_FLIPPED, r1, r2, false);
+                    ph[at++] = make_phase(TD_LOZ_OTHER, r1, 0, false);
+                    ph[at++] = make_phase(TD_UP_FROM_LOZ, 0, 0, false);
+                    ph[at++] = make_phase(TD_TRI_OTHER, 0, 7, false);
+                } else if (kind == 1) {  // triangle flips, :279-305
+                    ph[at++] = make_phase(TD_ROT_TRI, r2, r1, true);
+                    ph[at++] = make_phase(TD_TRI_FLIPPED, r2, r1, false);
+                    ph[at++] = make_phase(TD_TRI_OTHER, r2, 0, false);
+                    ph[at++] = make_phase(TD_LOZ_FROM_TRI, 0, 0, false);
+                    ph[at++] = make_phase(TD_BFLY_FROM_LOZ, 0, 7, false);
+                } else {  // butterfly flips, :306-347
+                    const uint32_t p1 = (uint32_t)d1(generator), p2 = (uint32_t)d2(generator);
+                    ph[at++] = make_phase(TD_ROT_BFLY, r1, p1 | (p2 << 2), true);
+                    ph[at++] = make_phase(TD_BFLY_SAME, r1, p1 | (p2 << 2), false);
+                    ph[at++] = make_phase(TD_BFLY_21, r1, p1, false);
+                    ph[at++] = make_phase(TD_BFLY_22, r1, p1, false);
+                    ph[at++] = make_phase(TD_BFLY_23_LOZ, r1, p1, false);
+                    ph[at++] = make_phase(TD_BFLY_FROM_LOZ, 1, 7u & ~(1u << r1), false);
+                    ph[at++] = make_phase(TD_TRI_OTHER, 0, 0, false);
+                }
+            }
         } else {
             std::default_random_engine generator;
             std::uniform_int_distribution<int> distribution(0, 2);
@@ -405,9 +486,10 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
             }
         }
     }
-    ph[at++] = make_phase(OP_FINAL, prev, NO_COLOUR, false);
+    if (h->kind != 3) ph[at++] = make_phase(OP_FINAL, prev, NO_COLOUR, false);
+    const int64_t nph = at;
 
-    const int width = h->n / h->ncol;
+    const int width = h->width;
     const bool uniform = h->table.empty();
     if (h->plan_rows != h->rows || h->plan_cols != h->cols || h->plan_nlat != h->nlat || h->plan_uniform != uniform) {
         rt_status s =
@@ -421,7 +503,8 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     const int64_t ids = (int64_t)h->rows * h->cols;
     rt_status s = stage_params(h, ids);
     if (s != RT_OK) return s;
-    const size_t xbytes = (size_t)h->plan.ctas * 2 * 2 * h->nlat * h->plan.xwords * sizeof(unsigned long long);
+    const size_t xbytes =
+        (size_t)h->plan.ctas * 2 * 2 * h->nlat * h->plan.xslots * h->plan.xwords * sizeof(unsigned long long);
     if (!h->d_xbuf.reserve(xbytes)) return h->fail(RT_E_NOMEM, "halo exchange buffer");
 
     cudaError_t e;
@@ -440,7 +523,7 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     a.n = h->n;
     a.rows = h->rows;
     a.cols = h->cols;
-    a.arows = h->n;
+    a.arows = h->arows;
     a.width = width;
     a.rng_kind = 0;
     a.params = h->table.empty() ? nullptr : static_cast<const uint4*>(h->d_params.p);
@@ -512,6 +595,90 @@ rt_status rt_last_run_info(rt_tiler* h, int64_t* phases, int64_t* launches) {
     if (!h) return RT_E_INVAL;
     if (phases) *phases = h->last_phases;
     if (launches) *launches = h->last_launches;
+    return RT_OK;
+}
+
+// Coupling from the past on the domino heat-bath chain: the reference's
+// Examples/AztecDiamondCftpEx.cpp:42-68 built on DominoTiler::Walk(tiling&,
+// vector<long>, vector<long>) (DominoTiler.cpp:58-107).  Each trial runs the
+// chains from the maximal and the minimal tiling through the same epochs
+// (same seeds, so the same draws) -- here as two coupled lattices of one
+// launch -- and compares them on the device.  Epoch seeds are successive
+// outputs of std::mt19937(master_seed), the newest epoch first, exactly as
+// the example draws them.
+rt_status rt_cftp(rt_tiler* h, const int32_t* tmax, const int32_t* tmin, int32_t n, int64_t first_steps,
+                  int32_t schedule, int64_t master_seed, int32_t max_trials, int32_t* out_tiling,
+                  rt_cftp_stats* stats) {
+    if (!h) return RT_E_INVAL;
+    if (h->family != FAM_DOMINO_HB)
+        return h->fail(RT_E_INVAL, "CFTP needs the monotone heat-bath kernel (RT_KERNEL_CFTP, dominokernelCFTP.cl)");
+    if (!tmax || !tmin || first_steps <= 0 || max_trials <= 0 ||
+        (schedule != RT_CFTP_DOUBLING && schedule != RT_CFTP_REFERENCE))
+        return h->fail(RT_E_INVAL, "bad CFTP arguments");
+    rt_status s = rt_upload(h, tmax, n);
+    if (s != RT_OK) return s;
+    const size_t tb = (size_t)n * n * 4;
+    if (!h->d_tiling2.reserve(tb) || !h->d_count.reserve(8) || !h->h_count.reserve(8))
+        return h->fail(RT_E_NOMEM, "CFTP buffers");
+    cudaError_t e = cudaMemcpyAsync(h->d_tiling2.p, tmin, tb, cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "upload of the minimal tiling");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::mt19937 mt(master_seed);
+    std::vector<int64_t> steps{first_steps}, seeds{(int64_t)mt()};
+    rt_cftp_stats st{};
+    double ms_total = 0;
+    h->nlat = 2;
+    for (int trial = 0; trial < max_trials; ++trial) {
+        // Restart both chains at the far end of the current schedule.
+        s = launch_split(false, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0],
+                         h->stream, &h->err);
+        if (s == RT_OK)
+            s = launch_split(false, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling2.p), h->d_arr[1],
+                             h->stream, &h->err);
+        if (s != RT_OK) break;
+        cudaEventRecord(e0, h->stream);
+        s = run_schedule(h, steps.data(), seeds.data(), (int)steps.size(), false);
+        if (s != RT_OK) break;
+        cudaEventRecord(e1, h->stream);
+        s = launch_count_diff(h->d_arr[0][0], h->d_arr[1][0], h->per_arr_al * h->ncol,
+                              static_cast<unsigned long long*>(h->d_count.p), h->stream, &h->err);
+        if (s != RT_OK) break;
+        e = cudaMemcpyAsync(h->h_count.p, h->d_count.p, 8, cudaMemcpyDeviceToHost, h->stream);
+        if (e != cudaSuccess) {
+            s = h->cuda_fail(e, "coalescence readback");
+            break;
+        }
+        s = rt_synchronize(h);
+        if (s != RT_OK) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms_total += ms;
+        st.trials = trial + 1;
+        st.total_steps = 0;
+        for (int64_t x : steps) st.total_steps += x;
+        if (*static_cast<unsigned long long*>(h->h_count.p) == 0) {
+            st.coalesced = 1;
+            break;
+        }
+        // Extend further into the past: the reference example prepends
+        // 2 * steps[last] (Examples/AztecDiamondCftpEx.cpp:67); the doubling
+        // schedule prepends the current total.
+        const int64_t add = schedule == RT_CFTP_REFERENCE ? 2 * steps.back() : st.total_steps;
+        steps.insert(steps.begin(), add);
+        seeds.insert(seeds.begin(), (int64_t)mt());
+    }
+    h->nlat = 1;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    st.device_ms = ms_total;
+    if (stats) *stats = st;
+    if (s != RT_OK) return s;
+    if (out_tiling) {
+        s = rt_download(h, out_tiling);  // lattice 0 = the chain started from the maximal tiling
+        if (s != RT_OK) return s;
+    }
     return RT_OK;
 }
 

@@ -605,4 +605,224 @@ rt_status rt_recttri_from_lozenge(const int32_t* tl, int64_t tlen, const int32_t
     return emit(t, out, cap, len);
 }
 
+// ---- dimers on the triangular lattice -------------------------------------------
+// Tile state encoding of src/TriangleDimer/TriangleDimerTiler.h:13-67: the
+// N x N "tiling" holds, at (even i, odd j) / (odd i, even j) / (odd i, odd j),
+// the 4-bit lozenge states of the H / L / R edges of the triangular lattice.
+
+// Tile states from edge indicator arrays h, l, r of eSize x eSize
+// (IceCreamCone / TestButterfly, TriangleDimerTiler.cpp:281-296, :365-380).
+static Vec td_tiles_from_edges(const Vec& h, const Vec& l, const Vec& r, int e) {
+    const int ts = 2 * e;
+    Vec t((size_t)ts * ts, 0);
+    auto H = [&](int i, int j) { return h[(size_t)i * e + j]; };
+    auto L = [&](int i, int j) { return l[(size_t)i * e + j]; };
+    auto R = [&](int i, int j) { return r[(size_t)i * e + j]; };
+    for (int i = 3; i < ts - 1; ++i)
+        for (int j = 3; j < ts - 1; ++j) {
+            int32_t v;
+            if (i % 2 == 0) {
+                if (j % 2 == 0) continue;
+                v = R(i / 2 - 1, j / 2) + 2 * L(i / 2 - 1, j / 2 + 1) + 4 * R(i / 2, j / 2) + 8 * L(i / 2, j / 2);
+            } else if (j % 2 == 0) {
+                v = H(i / 2, j / 2) + 2 * R(i / 2, j / 2) + 4 * H(i / 2 + 1, j / 2 - 1) + 8 * R(i / 2, j / 2 - 1);
+            } else {
+                v = H(i / 2, j / 2) + 2 * L(i / 2, j / 2 + 1) + 4 * H(i / 2 + 1, j / 2) + 8 * L(i / 2, j / 2);
+            }
+            t[(size_t)i * ts + j] = v;
+        }
+    return t;
+}
+
+rt_status rt_tridimer_ice_cream_cone(int32_t side, int32_t cut, int32_t* out, int64_t cap, int64_t* len) {
+    // A downward equilateral triangle of side N with a triangle of side M cut
+    // from its top-left corner, as a dimer cover built row by row
+    // (TriangleDimerTiler.cpp:236-332).  Parities the reference only warns
+    // about are accepted (its construction then covers a slightly different
+    // domain); cut > side - 1 is rejected.
+    if (side < 1 || cut < 0 || cut > side - 1) return RT_E_INVAL;
+    const int n = side, m = cut, e = n + 4;
+    const int k = ((n + 1) * (n + 2) / 2) % 2;
+    Vec h((size_t)e * e, 0), l((size_t)e * e, 0), r((size_t)e * e, 0);
+    for (int i = 2; i < e - 2; ++i)
+        for (int j = 2; j < e - i; ++j) {
+            const size_t at = (size_t)i * e + j;
+            if (i < m + 2) {
+                if ((i + j) % 2 == m % 2 && m != 0 && j > m + 3 - i) h[at] = 1;
+                if ((n - m) % 2 == 0 && i % 2 == 0 && j == e - i - 1) r[at] = 1;
+            } else {
+                if (j % 2 == 0) h[at] = 1;
+                if (i % 4 == (3 + n % 2 + 2 * k) % 4 && j == e - i - 1) h[at] = 0, l[at] = 1;
+                if (i % 4 == (2 + n % 2 + 2 * k) % 4 && j == e - i - 1) r[at] = 1;
+            }
+        }
+    return emit(td_tiles_from_edges(h, l, r, e), out, cap, len);
+}
+
+rt_status rt_tridimer_test_butterfly(int32_t kind, int32_t* out, int64_t cap, int64_t* len) {
+    // One butterfly of orientation H (0), L (1) or R (2) (TriangleDimerTiler.cpp:334-383).
+    if (kind < 0 || kind > 2) return RT_E_INVAL;
+    const int e = 8;
+    Vec h((size_t)e * e, 0), l((size_t)e * e, 0), r((size_t)e * e, 0);
+    if (kind == 0) h[2 * e + 3] = h[4 * e + 3] = r[2 * e + 4] = r[3 * e + 2] = 1;
+    if (kind == 1) r[2 * e + 3] = r[4 * e + 2] = l[3 * e + 2] = l[3 * e + 4] = 1;
+    if (kind == 2) l[2 * e + 4] = l[4 * e + 3] = r[3 * e + 2] = r[3 * e + 4] = 1;
+    return emit(td_tiles_from_edges(h, l, r, e), out, cap, len);
+}
+
+}  // extern "C"
+
+namespace rtb {
+// Triangle-flip states ((N/2) x N) and butterfly-flip states (N x N) of a
+// tiling (TilingToTriangleFlips / TilingToButterflyFlips,
+// TriangleDimerTiler.cpp:385-460).
+void td_derived_states(const int32_t* t, int n, int32_t* tri, int32_t* bfl) {
+    auto T = [&](int i, int j) { return t[(size_t)i * n + j]; };
+    std::fill(tri, tri + (size_t)(n / 2) * n, 0);
+    std::fill(bfl, bfl + (size_t)n * n, 0);
+    auto b = [](int32_t x, int k) { return (x >> k) & 1; };
+    for (int i = 1; i < n / 2 - 1; ++i)
+        for (int j = 1; j < n - 1; ++j) {
+            const int32_t a = T(2 * i + 1, j), c = T(2 * i + 1, j + 1);
+            int d0, d1, d2;
+            if (j % 2 == 0) {  // down triangle
+                const int32_t u = T(2 * i, j + 1);
+                d0 = b(a, 2) + 2 * b(a, 3) + 3 * b(c, 3);
+                d1 = b(c, 2) + 2 * b(a, 1) + 3 * b(c, 1);
+                d2 = 2 * b(u, 0) + b(a, 0) + 3 * b(u, 1);
+            } else {  // up triangle
+                const int32_t w = T(2 * i + 2, j);
+                d0 = b(a, 0) + 2 * b(a, 3) + 3 * b(c, 3);
+                d1 = b(c, 0) + 2 * b(a, 1) + 3 * b(c, 1);
+                d2 = 2 * b(w, 3) + 3 * b(w, 2) + b(a, 2);
+            }
+            tri[(size_t)i * n + j] = d0 + 4 * d1 + 16 * d2;
+        }
+    for (int i = 2; i < n - 2; ++i)
+        for (int j = 2; j < n - 2; ++j) {
+            const int32_t x = T(i, j);
+            int f1, f4, f16, f64, c;
+            if (i % 2 == 0) {
+                if (j % 2 == 0) continue;
+                const int32_t u = T(i - 1, j), ue = T(i - 1, j + 1), d = T(i + 1, j), dw = T(i + 1, j - 1);
+                f1 = b(u, 3) + 2 * b(u, 0) + 3 * b(x, 0);
+                f4 = b(ue, 0) + 2 * b(ue, 1) + 3 * b(x, 1);
+                f16 = b(d, 1) + 2 * b(d, 2) + 3 * b(x, 2);
+                f64 = b(dw, 2) + 2 * b(dw, 3) + 3 * b(x, 3);
+                c = b(ue, 2);
+            } else if (j % 2 == 0) {
+                const int32_t ue = T(i - 1, j + 1), e = T(i, j + 1), dw = T(i + 1, j - 1), w = T(i, j - 1);
+                f1 = b(ue, 0) + 2 * b(ue, 1) + 3 * b(x, 0);
+                f4 = b(e, 1) + 2 * b(e, 2) + 3 * b(x, 1);
+                f16 = b(dw, 2) + 2 * b(dw, 3) + 3 * b(x, 2);
+                f64 = b(w, 3) + 2 * b(w, 0) + 3 * b(x, 3);
+                c = b(e, 3);
+            } else {
+                const int32_t u = T(i - 1, j), e = T(i, j + 1), d = T(i + 1, j), w = T(i, j - 1);
+                f1 = b(u, 0) + 2 * b(u, 1) + 3 * b(x, 0);
+                f4 = b(e, 0) + 2 * b(e, 1) + 3 * b(x, 1);
+                f16 = b(d, 2) + 2 * b(d, 3) + 3 * b(x, 2);
+                f64 = b(w, 2) + 2 * b(w, 3) + 3 * b(x, 3);
+                c = b(e, 3);
+            }
+            bfl[(size_t)i * n + j] = f1 + 4 * f4 + 16 * f16 + 64 * f64 + 256 * c;
+        }
+}
+
+// The eight M x M arrays the walk runs on (TriangleDimerTiler.cpp:107-133),
+// in the order H, L, R, U, D, BH, BL, BR.
+void td_split_host(const int32_t* t, int n, int32_t* arrays) {
+    const int m = n / 2;
+    const size_t mm = (size_t)m * m;
+    Vec tri((size_t)(n / 2) * n), bfl((size_t)n * n);
+    td_derived_states(t, n, tri.data(), bfl.data());
+    std::fill(arrays, arrays + 8 * mm, 0);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            const size_t at = (size_t)(i / 2) * m + j / 2;
+            const size_t src = (size_t)i * n + j;
+            if (i % 2 == 0) {
+                if (j % 2 == 1) arrays[0 * mm + at] = t[src], arrays[5 * mm + at] = bfl[src];
+            } else if (j % 2 == 0) {
+                arrays[1 * mm + at] = t[src], arrays[6 * mm + at] = bfl[src];
+            } else {
+                arrays[2 * mm + at] = t[src], arrays[7 * mm + at] = bfl[src];
+            }
+        }
+    for (int i = 0; i < n / 2; ++i)
+        for (int j = 0; j < n; ++j) arrays[(j % 2 == 0 ? 4 : 3) * mm + (size_t)i * m + j / 2] = tri[(size_t)i * n + j];
+}
+}  // namespace rtb
+
+extern "C" {
+
+rt_status rt_tridimer_triangle_flips(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len) {
+    const int n = isqrt_exact(tlen);
+    if (!t || n < 2 || n % 2) return RT_E_INVAL;
+    Vec tri((size_t)(n / 2) * n), bfl((size_t)n * n);
+    rtb::td_derived_states(t, n, tri.data(), bfl.data());
+    return emit(tri, out, cap, len);
+}
+
+rt_status rt_tridimer_butterfly_flips(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len) {
+    const int n = isqrt_exact(tlen);
+    if (!t || n < 2 || n % 2) return RT_E_INVAL;
+    Vec tri((size_t)(n / 2) * n), bfl((size_t)n * n);
+    rtb::td_derived_states(t, n, tri.data(), bfl.data());
+    return emit(bfl, out, cap, len);
+}
+
+// Vertices covered by a dimer ((N/2+1)^2, TilingToVertices :711-737).
+static Vec td_vertices(const int32_t* t, int n) {
+    const int m = n / 2 + 1;
+    Vec v((size_t)m * m, 0);
+    for (int i = 2; i < m - 2; ++i)
+        for (int j = 2; j < m - 2; ++j) {
+            const int32_t a = t[(size_t)2 * (i - 1) * n + 2 * j + 1], b = t[(size_t)2 * (i + 1) * n + 2 * j - 1];
+            const int32_t c = t[(size_t)(2 * i - 1) * n + 2 * j], d = t[(size_t)(2 * i - 1) * n + 2 * j + 1];
+            v[(size_t)i * m + j] = ((a & 12) || (b & 3) || (c & 4) || (d & 4)) ? 1 : 0;
+        }
+    return v;
+}
+
+rt_status rt_tridimer_vertices(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len) {
+    const int n = isqrt_exact(tlen);
+    if (!t || n < 8 || n % 2) return RT_E_INVAL;
+    return emit(td_vertices(t, n), out, cap, len);
+}
+
+// Triangles whose three corners are covered (TilingToDomain :739-770).
+rt_status rt_tridimer_tiling_to_domain(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len) {
+    const int n = isqrt_exact(tlen);
+    if (!t || n < 8 || n % 2) return RT_E_INVAL;
+    const int m = n / 2 + 1;
+    const Vec v = td_vertices(t, n);
+    Vec d((size_t)(m - 1) * 2 * (m - 1), 0);
+    auto V = [&](int i, int j) { return v[(size_t)i * m + j] == 1; };
+    for (int i = 0; i < m - 1; ++i)
+        for (int j = 0; j < 2 * (m - 1); ++j) {
+            const bool in = j % 2 == 0 ? (V(i, j / 2) && V(i, j / 2 + 1) && V(i + 1, j / 2))
+                                       : (V(i, j / 2 + 1) && V(i + 1, j / 2) && V(i + 1, j / 2 + 1));
+            d[(size_t)i * 2 * (m - 1) + j] = in;
+        }
+    return emit(d, out, cap, len);
+}
+
+// 0/1 indicator of dimers of one orientation (DimerIndicator :20-84; the
+// reference reads orientations 1 and 2 from the (even, odd) cells and 0 from
+// the (odd, odd) cells, bits 8, 4 and 1 respectively).
+rt_status rt_tridimer_dimer_indicator(const int32_t* t, int64_t tlen, int32_t orient, int32_t* out, int64_t cap,
+                                      int64_t* len) {
+    const int n = isqrt_exact(tlen);
+    if (!t || n < 2 || n % 2 || orient < 0 || orient > 2) return RT_E_INVAL;
+    const int m = n / 2;
+    Vec dd((size_t)m * m, 0);
+    const int bit = orient == 1 ? 8 : orient == 2 ? 4 : 1;
+    const int ri = orient == 0 ? 1 : 0;
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j)
+            dd[(size_t)i * m + j] = (t[(size_t)(2 * i + ri) * n + 2 * j + 1] & bit) == bit;
+    return emit(dd, out, cap, len);
+}
+
 }  // extern "C"

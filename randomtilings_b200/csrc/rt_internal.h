@@ -16,7 +16,8 @@ enum Family : int {
     FAM_DOMINO_HB = 1,   // dominokernelCFTP.cl, int8
     FAM_LOZENGE8 = 2,    // lozengekernel.cl, int8
     FAM_QLOZENGE32 = 3,  // qlozengekernel.cl, int32
-    FAM_RECTTRI = 4      // recttrianglekernel.cl, int32
+    FAM_RECTTRI = 4,     // recttrianglekernel.cl, int32
+    FAM_TRIDIMER = 5     // triangledimerkernel.cl, 8 int32 arrays
 };
 
 struct WalkPlan {
@@ -27,14 +28,23 @@ struct WalkPlan {
     size_t smem = 0;
     int wpad = 0;    // shared-memory row stride (elements)
     int xwords = 0;  // exchange words per halo row
+    int xslots = 1;  // arrays exchanged per phase
     const void* fn = nullptr;
 };
 
 rt_status plan_walk(int family, int device, int nlat, int rows, int cols, int width, bool uniform, WalkPlan* plan,
                     std::string* err);
 rt_status launch_walk(const WalkPlan& plan, WalkArgs& args, cudaStream_t stream, std::string* err);
-// kind: 0 domino, 1 lozenge, 2 rect-triangle.
+// kind: 0 domino, 1 lozenge, 2 rect-triangle, 3 triangle-dimer (merge only).
 rt_status launch_split(bool merge, int elem_bytes, int kind, int ncol, int n, int32_t* tiling, void* const* arr,
                        cudaStream_t stream, std::string* err);
+
+// Host split of a triangle-dimer tiling into its eight M x M arrays
+// (H, L, R, U, D, BH, BL, BR), rt_host.cpp.
+void td_split_host(const int32_t* t, int n, int32_t* arrays);
+
+// Counts differing 32-bit words of a and b (bytes must be a multiple of 4).
+rt_status launch_count_diff(const void* a, const void* b, size_t bytes, unsigned long long* d_count,
+                            cudaStream_t stream, std::string* err);
 
 }  // namespace rtb

@@ -31,6 +31,7 @@ struct WalkArgs {
     int arows, width;     // colour array shape
     int wpad;             // shared-memory row stride (elements, multiple of 4)
     int xwords;           // exchange words per row
+    int xslots;           // exchanged arrays per phase (slots per side)
     int rows_per_cta;
     int rng_kind;         // 0 TinyMT, 1 Philox
     const uint4* params;  // TinyMT (mat1, mat2, tmat, -) per stream id, or nullptr
@@ -80,7 +81,8 @@ struct DominoRule {
         int w;
         uint32_t thr;
     };
-    __device__ static Ctx ctx(const WalkArgs& a, int8_t* planes, int plane, uint32_t d) {
+    __device__ static uint32_t written(uint32_t d) { return ph_op(d) == OP_STEP ? 1u << flipped((int)ph_a(d)) : 0u; }
+    __device__ static Ctx ctx(const WalkArgs& a, int8_t* planes, int plane, uint32_t d, int) {
         const int op = (int)ph_op(d), ca = (int)ph_a(d), cb = (int)ph_b(d);
         Ctx x;
         x.step = op == (int)OP_STEP;
@@ -149,7 +151,8 @@ struct ThreeColour {
         uint32_t shifts;
         int w, imax, jmax;
     };
-    __device__ static Ctx ctx(const WalkArgs& a, T* planes, int plane, uint32_t d) {
+    __device__ static uint32_t written(uint32_t d) { return ph_op(d) == OP_STEP ? 1u << flipped((int)ph_a(d)) : 0u; }
+    __device__ static Ctx ctx(const WalkArgs& a, T* planes, int plane, uint32_t d, int) {
         const int op = (int)ph_op(d), ca = (int)ph_a(d), cb = (int)ph_b(d);
         Ctx x;
         x.step = op == (int)OP_STEP;

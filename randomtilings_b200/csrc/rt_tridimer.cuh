@@ -1,0 +1,352 @@
+// rt_tridimer.cuh -- dimers on the triangular lattice (the reference's
+// TriangleDimerTiler, src/TriangleDimer/TriangleDimerTiler.cpp:86-483 and
+// triangledimerkernel.cl) as a phase program of the persistent walk kernel.
+//
+// Eight M x M int32 arrays (M = N/2), in band order:
+//   0 H, 1 L, 2 R   lozenge states (one per edge orientation)
+//   3 U, 4 D        up / down triangle states (three base-4 digits)
+//   5 BH, 6 BL, 7 BR butterfly states (four base-4 digits + centre bit)
+// The reference launches one kernel per array update; here each phase is
+// one of those updates (or several that read only arrays finished in earlier
+// phases and write different arrays), applied at every site, and a phase
+// exchanges the halo rows of every array it wrote.  Position (i, j) of the
+// (M, M) NDRange owns stream j + M i (src/TinyMT/tinymt.clh:24-30).
+#pragma once
+
+#include "rt_models.cuh"
+
+namespace rtb {
+
+enum : uint32_t {
+    TD_ROT_LOZ = 16,        // a = orientation t, b = class c           (RotateLozenges)            [draws]
+    TD_LOZ_FLIPPED = 17,    // a = t, b = c                             (UpdateLozengesFlipped)
+    TD_LOZ_OTHER = 18,      // a = t                                    (UpdateLozenges0/1/2)
+    TD_UP_FROM_LOZ = 19,    //                                          (UpdateTriangleUFromLozenges)
+    TD_TRI_OTHER = 20,      // a = 0: D from U, 1: U from D; b = butterflies refreshed from lozenges
+    TD_ROT_TRI = 21,        // a = 1: down, 0: up; b = class c          (RotateTriangles)           [draws]
+    TD_TRI_FLIPPED = 22,    // a = 1: down, 0: up; b = c                (UpdateTrianglesFlipped1/0)
+    TD_LOZ_FROM_TRI = 23,   //                                          (UpdateLozenge{H,L,R}FromTriangles)
+    TD_BFLY_FROM_LOZ = 24,  // b = butterfly mask; a = 1: also U from lozenges
+    TD_ROT_BFLY = 25,       // a = t, b = p1 | p2 << 2                  (RotateButterflys)          [draws]
+    TD_BFLY_SAME = 26,      // a = t, b = p1 | p2 << 2                  (UpdateButterflysFlipped?1)
+    TD_BFLY_21 = 27,        // a = t, b = p1
+    TD_BFLY_22 = 28,        // a = t, b = p1
+    TD_BFLY_23_LOZ = 29     // a = t, b = p1: pass 23, then the lozenges from that butterfly array
+};
+
+struct TriDimerRule {
+    using Elem = int32_t;
+    static constexpr int NCOL = 8;
+    static constexpr int ROFF = 0;
+    static constexpr int COFF = 0;
+    __device__ static uint32_t stream_id(const WalkArgs& a, int r, int c) {
+        return (uint32_t)c + (uint32_t)(a.n / 2) * (uint32_t)r;
+    }
+    // Arrays a phase writes (bit k = array k); their halo rows are exchanged.
+    __device__ static uint32_t written(uint32_t d) {
+        const uint32_t op = ph_op(d), a = ph_a(d), b = ph_b(d);
+        switch (op) {
+            case TD_ROT_LOZ:
+            case TD_LOZ_FLIPPED: return 1u << a;
+            case TD_LOZ_OTHER: return 7u & ~(1u << a);
+            case TD_UP_FROM_LOZ: return 1u << 3;
+            case TD_TRI_OTHER: return (a == 0 ? 1u << 4 : 1u << 3) | (b << 5);
+            case TD_ROT_TRI:
+            case TD_TRI_FLIPPED: return a == 1 ? 1u << 4 : 1u << 3;
+            case TD_LOZ_FROM_TRI: return 7u;
+            case TD_BFLY_FROM_LOZ: return (b << 5) | (a ? 1u << 3 : 0u);
+            case TD_ROT_BFLY:
+            case TD_BFLY_SAME:
+            case TD_BFLY_21:
+            case TD_BFLY_22: return 1u << (5 + a);
+            case TD_BFLY_23_LOZ: return (1u << (5 + a)) | 7u;
+            default: return 0u;
+        }
+    }
+    struct Ctx {
+        int32_t* base;
+        int plane, w, m, row0;
+        uint32_t op, a, b;
+    };
+    __device__ static Ctx ctx(const WalkArgs& ar, int32_t* planes, int plane, uint32_t d, int row0) {
+        Ctx x;
+        x.row0 = row0;
+        x.base = planes;
+        x.plane = plane;
+        x.w = ar.wpad;
+        x.m = ar.n / 2;
+        x.op = ph_op(d);
+        x.a = ph_a(d);
+        x.b = ph_b(d);
+        return x;
+    }
+
+    // ---- helpers ------------------------------------------------------------
+    __device__ static int dg(int32_t x, int k) { return (int)(((uint32_t)x >> (2 * k)) & 3u); }
+    __device__ static int cyc_up(int v) { return v == 0 ? 0 : v % 3 + 1; }          // 1->2, 2->3, 3->1
+    __device__ static int cyc_dn(int v) { return v == 0 ? 0 : (v + 1) % 3 + 1; }    // 1->3, 2->1, 3->2
+    __device__ static int32_t pack(int t1, int t4, int t16, int t64, int c) {
+        return t1 + 4 * t4 + 16 * t16 + 64 * t64 + 256 * c;
+    }
+    __device__ static int tri_digit(int32_t v) {
+        return ((v & 48) == 16 ? 1 : 0) + ((v & 3) == 3 ? 2 : 0) + ((v & 12) == 8 ? 3 : 0);
+    }
+
+    // Butterfly state of orientation `which` from the lozenge arrays
+    // (UpdateButterflys{H,L,R}FromLozenge, triangledimerkernel.cl:118-189).
+    template <class At>
+    __device__ static int32_t bfly_from_loz(At at, int which, int i, int j) {
+        int t1, t4, t16, t64, c;
+        if (which == 0) {
+            const int32_t h = at(0, i, j), ru = at(2, i - 1, j), lu = at(1, i - 1, j + 1), r = at(2, i, j), l = at(1, i, j);
+            c = (lu >> 2) & 1;
+            t1 = ((ru >> 3) & 1) + 2 * (ru & 1) + 3 * (h & 1);
+            t4 = (lu & 1) + (lu & 2) + 3 * ((h >> 1) & 1);
+            t16 = ((r >> 1) & 1) + ((r >> 1) & 2) + 3 * ((h >> 2) & 1);
+            t64 = ((l >> 2) & 1) + ((l >> 2) & 2) + 3 * ((h >> 3) & 1);
+        } else if (which == 1) {
+            const int32_t l = at(1, i, j), h = at(0, i, j), r = at(2, i, j), hd = at(0, i + 1, j - 1), rw = at(2, i, j - 1);
+            c = (r >> 3) & 1;
+            t1 = (h & 1) + (h & 2) + 3 * (l & 1);
+            t4 = ((r >> 1) & 1) + ((r >> 1) & 2) + 3 * ((l >> 1) & 1);
+            t16 = ((hd >> 2) & 1) + ((hd >> 2) & 2) + 3 * ((l >> 2) & 1);
+            t64 = ((rw >> 3) & 1) + 2 * (rw & 1) + 3 * ((l >> 3) & 1);
+        } else {
+            const int32_t r = at(2, i, j), h = at(0, i, j), le = at(1, i, j + 1), hd = at(0, i + 1, j), l = at(1, i, j);
+            c = (le >> 3) & 1;
+            t1 = (h & 1) + (h & 2) + 3 * (r & 1);
+            t4 = (le & 1) + (le & 2) + 3 * ((r >> 1) & 1);
+            t16 = ((hd >> 2) & 1) + ((hd >> 2) & 2) + 3 * ((r >> 2) & 1);
+            t64 = ((l >> 2) & 1) + ((l >> 2) & 2) + 3 * ((r >> 3) & 1);
+        }
+        return pack(t1, t4, t16, t64, c);
+    }
+
+    // Up-triangle state from the lozenges (UpdateTriangleUFromLozenges, :96-116).
+    template <class At>
+    __device__ static int32_t up_from_loz(At at, int i, int j) {
+        const int32_t l0 = at(1, i, j), l1 = at(1, i, j + 1), h0 = at(0, i, j), h1 = at(0, i + 1, j);
+        const int x = ((l0 & 1) ? 1 : 0) + ((h0 & 8) ? 2 : 0) + ((h1 & 1) ? 3 : 0);
+        const int y = ((l1 & 1) ? 1 : 0) + ((h1 & 2) ? 2 : 0) + ((l1 & 2) ? 3 : 0);
+        const int z = ((l1 & 4) ? 1 : 0) + ((h1 & 8) ? 2 : 0) + ((h1 & 4) ? 3 : 0);
+        return x + 4 * y + 16 * z;
+    }
+
+    __device__ static int slice(int t, int i, int j) { return t == 0 ? i % 3 : t == 1 ? j % 3 : (i + j) % 3; }
+    __device__ static int bpar(int t, int i, int j) { return t == 1 ? (i & 1) : (j & 1); }
+
+    __device__ static void site(const WalkArgs&, const Ctx& x, int, int i, int j, uint32_t k) {
+        auto at = [&](int arr, int ii, int jj) -> int32_t& {
+            return x.base[arr * x.plane + (ii - x.row0) * x.w + jj];
+        };
+        const bool interior = i >= 1 && i <= x.m - 2 && j >= 1 && j <= x.m - 2;
+        const int t = (int)x.a;
+        switch (x.op) {
+            case TD_ROT_LOZ: {  // :4-22
+                const int cls = ((1 - (t & 1)) * i + ((1 + t) / 2) * j) % 2;
+                if (k < (1u << 22) && cls == (int)x.b) {
+                    int32_t& v = at(t, i, j);
+                    v = v == 5 ? 10 : v == 10 ? 5 : v;
+                }
+                break;
+            }
+            case TD_LOZ_FLIPPED: {  // :24-33
+                const int cls = ((1 - (t & 1)) * i + ((1 + t) / 2) * j) % 2;
+                if (!interior || cls == (int)x.b) break;
+                const int dj = t & 1, di = (2 - t) / 2;
+                at(t, i, j) = ((at(t, i - 1, j + dj) >> 2) & 1) | (((at(t, i - di, j + 1) >> 3) & 1) << 1) |
+                              ((at(t, i + 1, j - dj) & 1) << 2) | (((at(t, i + di, j - 1) >> 1) & 1) << 3);
+                break;
+            }
+            case TD_LOZ_OTHER: {  // :35-78
+                if (!interior) break;
+                if (t == 0) {
+                    at(1, i, j) = (at(1, i, j) & ~10) | ((at(0, i + 1, j) & 1) << 1) | ((at(0, i + 1, j - 1) & 1) << 3);
+                    at(2, i, j) = (at(2, i, j) & ~10) | (at(0, i + 1, j) & 2) | (at(0, i, j) & 8);
+                } else if (t == 1) {
+                    at(2, i, j) = (at(2, i, j) & ~5) | (at(1, i, j) & 1) | ((at(1, i + 1, j) & 1) << 2);
+                    at(0, i, j) = (at(0, i, j) & ~5) | ((at(1, i - 1, j) & 2) >> 1) | ((at(1, i, j) & 2) << 1);
+                } else {
+                    at(0, i, j) = (at(0, i, j) & ~10) | (at(2, i - 1, j) & 2) | ((at(2, i, j - 1) & 2) << 2);
+                    at(1, i, j) = (at(1, i, j) & ~5) | (at(2, i, j) & 1) | (at(2, i, j - 1) & 4);
+                }
+                break;
+            }
+            case TD_UP_FROM_LOZ:
+                if (interior) at(3, i, j) = up_from_loz(at, i, j);
+                break;
+            case TD_TRI_OTHER: {  // :255-275, then :118-189 for the butterflies in b
+                if (!interior) break;
+                const int src = t == 0 ? 3 : 4, dst = t == 0 ? 4 : 3, p = t == 0 ? -1 : 1;
+                at(dst, i, j) = tri_digit(at(src, i, j - 1 + t)) + 4 * tri_digit(at(src, i, j + t)) +
+                                16 * tri_digit(at(src, i + p, j));
+                for (int w = 0; w < 3; ++w)
+                    if (x.b & (1u << w)) at(5 + w, i, j) = bfly_from_loz(at, w, i, j);
+                break;
+            }
+            case TD_ROT_TRI: {  // :191-211
+                if (k < (1u << 22) && ((j - i) % 3 + 3) % 3 == (int)x.b) {
+                    int32_t& v = at(t == 1 ? 4 : 3, i, j);
+                    v = v == 45 ? 54 : v == 54 ? 45 : v;
+                }
+                break;
+            }
+            case TD_TRI_FLIPPED: {  // :213-253
+                const int cls = ((j - i) % 3 + 3) % 3;
+                if (!interior || cls == (int)x.b) break;
+                const int p = cls == ((int)x.b + 1) % 3;
+                const int arr = t == 1 ? 4 : 3;
+                int32_t v;
+                if (t == 0)
+                    v = p ? dg(at(arr, i, j - 1), 1) + 4 * dg(at(arr, i - 1, j + 1), 2) + 16 * dg(at(arr, i + 1, j), 0)
+                          : dg(at(arr, i - 1, j), 2) + 4 * dg(at(arr, i, j + 1), 0) + 16 * dg(at(arr, i + 1, j - 1), 1);
+                else
+                    v = p ? dg(at(arr, i, j - 1), 1) + 4 * dg(at(arr, i + 1, j), 2) + 16 * dg(at(arr, i - 1, j + 1), 0)
+                          : dg(at(arr, i + 1, j - 1), 2) + 4 * dg(at(arr, i, j + 1), 0) + 16 * dg(at(arr, i - 1, j), 1);
+                at(arr, i, j) = v;
+                break;
+            }
+            case TD_LOZ_FROM_TRI: {  // :277-329
+                if (!interior) break;
+                const int32_t dd = at(4, i, j), uh = at(3, i - 1, j), ul = at(3, i, j - 1), ur = at(3, i, j);
+                at(0, i, j) = ((dd & 48) == 32) + 2 * ((dd & 48) == 48) + 4 * ((uh & 48) == 48) + 8 * ((uh & 48) == 32);
+                at(1, i, j) = ((ul & 12) == 4) + 2 * ((ul & 12) == 12) + 4 * ((dd & 3) == 1) + 8 * ((dd & 3) == 2);
+                at(2, i, j) = ((ur & 3) == 1) + 2 * ((dd & 12) == 12) + 4 * ((dd & 12) == 4) + 8 * ((ur & 3) == 2);
+                break;
+            }
+            case TD_BFLY_FROM_LOZ:
+                if (!interior) break;
+                for (int w = 0; w < 3; ++w)
+                    if (x.b & (1u << w)) at(5 + w, i, j) = bfly_from_loz(at, w, i, j);
+                if (x.a) at(3, i, j) = up_from_loz(at, i, j);
+                break;
+            case TD_ROT_BFLY: {  // :331-353
+                const int p1 = (int)(x.b & 3), p2 = (int)(x.b >> 2);
+                const int b1 = 1 - (t & 1), b2 = (1 + t) / 2, b3 = t & 1;
+                if (k < (1u << 22) && (b1 * i + b2 * j) % 3 == p1 && ((b1 * j + b3 * i) & 1) == p2) {
+                    int32_t& v = at(5 + t, i, j);
+                    v = v == 170 ? 85 : v == 85 ? 170 : v;
+                }
+                break;
+            }
+            case TD_BFLY_SAME: {  // UpdateButterflysFlipped{H,L,R}1
+                const int p1 = (int)(x.b & 3), p2 = (int)(x.b >> 2);
+                if (!interior || slice(t, i, j) != p1 || bpar(t, i, j) == p2) break;
+                const int arr = 5 + t;
+                const int c = (at(arr, i, j) >> 8) & 1;
+                int t1, t4, t16, t64;
+                if (t == 2) {
+                    const int32_t lo = at(arr, i + 1, j - 1), hi = at(arr, i - 1, j + 1);
+                    t1 = cyc_dn(dg(hi, 3));
+                    t4 = cyc_up(dg(hi, 2));
+                    t16 = cyc_dn(dg(lo, 1));
+                    t64 = cyc_up(dg(lo, 0));
+                } else {
+                    const int32_t u = t == 0 ? at(arr, i, j - 1) : at(arr, i - 1, j);
+                    const int32_t v = t == 0 ? at(arr, i, j + 1) : at(arr, i + 1, j);
+                    t1 = cyc_up(dg(u, 1));
+                    t4 = cyc_dn(dg(v, 0));
+                    t16 = cyc_up(dg(v, 3));
+                    t64 = cyc_dn(dg(u, 2));
+                }
+                at(arr, i, j) = pack(t1, t4, t16, t64, c);
+                break;
+            }
+            case TD_BFLY_21: {
+                const int p1 = (int)x.b;
+                const int want = t == 0 ? (p1 + 1) % 3 : (p1 + 2) % 3;
+                if (!interior || slice(t, i, j) != want) break;
+                const int arr = 5 + t;
+                const int32_t f = at(arr, i, j);
+                int t1, t4, t16, t64, c;
+                if (t == 2) {
+                    const int32_t e = at(arr, i, j + 1), s = at(arr, i + 1, j);
+                    c = dg(s, 0) == 1;
+                    t1 = dg(f, 0);
+                    t4 = dg(f, 1) == 2 ? 2 : (dg(e, 0) == 3) + 3 * (dg(e, 3) == 3);
+                    t16 = dg(f, 2) == 1 ? 1 : 3 * (dg(s, 0) == 3) + 2 * (dg(s, 3) == 3);
+                    t64 = dg(f, 3);
+                } else {
+                    const int32_t u = t == 0 ? at(arr, i - 1, j) : at(arr, i - 1, j + 1);
+                    const int32_t v = t == 0 ? at(arr, i - 1, j + 1) : at(arr, i, j + 1);
+                    c = dg(u, 2) == 2;
+                    t1 = dg(f, 0) == 2 ? 2 : (dg(u, 3) == 3) + 3 * (dg(u, 2) == 3);
+                    t4 = dg(f, 1) == 1 ? 1 : 3 * (dg(v, 3) == 3) + 2 * (dg(v, 2) == 3);
+                    t16 = dg(f, 2);
+                    t64 = dg(f, 3);
+                }
+                at(arr, i, j) = pack(t1, t4, t16, t64, c);
+                break;
+            }
+            case TD_BFLY_22: {
+                const int p1 = (int)x.b;
+                const int want = t == 0 ? (p1 + 2) % 3 : (p1 + 1) % 3;
+                if (!interior || slice(t, i, j) != want) break;
+                const int arr = 5 + t;
+                const int32_t f = at(arr, i, j);
+                int t1, t4, t16, t64, c;
+                if (t == 2) {
+                    const int32_t n1 = at(arr, i - 1, j), n2 = at(arr, i, j + 1), n3 = at(arr, i + 1, j), n4 = at(arr, i, j - 1);
+                    c = dg(n1, 2) == 1;
+                    t1 = dg(f, 0) == 1 ? 1 : 3 * (dg(n1, 2) == 3) + 2 * (dg(n1, 1) == 3);
+                    t4 = (n2 & 256) ? 2 : (dg(f, 1) != 2) * dg(f, 1);
+                    t16 = (n3 & 256) ? 1 : (dg(f, 2) != 1) * dg(f, 2);
+                    t64 = dg(f, 3) == 2 ? 2 : (dg(n4, 2) == 3) + 3 * (dg(n4, 1) == 3);
+                } else {
+                    const int32_t n1 = t == 0 ? at(arr, i - 1, j) : at(arr, i - 1, j + 1);
+                    const int32_t n2 = t == 0 ? at(arr, i - 1, j + 1) : at(arr, i, j + 1);
+                    const int32_t n3 = t == 0 ? at(arr, i + 1, j) : at(arr, i + 1, j - 1);
+                    const int32_t n4 = t == 0 ? at(arr, i + 1, j - 1) : at(arr, i, j - 1);
+                    c = dg(n3, 0) == 2;
+                    t1 = (n1 & 256) ? 2 : (dg(f, 0) != 2) * dg(f, 0);
+                    t4 = (n2 & 256) ? 1 : (dg(f, 1) != 1) * dg(f, 1);
+                    t16 = dg(f, 2) == 2 ? 2 : 3 * (dg(n3, 0) == 3) + (dg(n3, 1) == 3);
+                    t64 = dg(f, 3) == 1 ? 1 : 2 * (dg(n4, 0) == 3) + 3 * (dg(n4, 1) == 3);
+                }
+                at(arr, i, j) = pack(t1, t4, t16, t64, c);
+                break;
+            }
+            case TD_BFLY_23_LOZ: {
+                if (!interior) break;
+                const int p1 = (int)x.b;
+                const int want = t == 0 ? (p1 + 1) % 3 : (p1 + 2) % 3;
+                const int arr = 5 + t;
+                if (slice(t, i, j) == want) {
+                    const int32_t f = at(arr, i, j);
+                    int t1 = dg(f, 0), t4 = dg(f, 1), t16 = dg(f, 2), t64 = dg(f, 3);
+                    if (t == 2) {
+                        t1 = (at(arr, i - 1, j) & 256) ? 1 : (dg(f, 0) != 1) * dg(f, 0);
+                        t64 = (at(arr, i, j - 1) & 256) ? 2 : (dg(f, 3) != 2) * dg(f, 3);
+                    } else {
+                        const int32_t n3 = t == 0 ? at(arr, i + 1, j) : at(arr, i + 1, j - 1);
+                        const int32_t n4 = t == 0 ? at(arr, i + 1, j - 1) : at(arr, i, j - 1);
+                        t16 = (n3 & 256) ? 2 : (dg(f, 2) != 2) * dg(f, 2);
+                        t64 = (n4 & 256) ? 1 : (dg(f, 3) != 1) * dg(f, 3);
+                    }
+                    at(arr, i, j) = pack(t1, t4, t16, t64, (f >> 8) & 1);
+                }
+                // UpdateLozengeFromButterflys{H,L,R} (:655-746), own site only.
+                const int32_t bf = at(arr, i, j);
+                const int d0 = dg(bf, 0), d1 = dg(bf, 1), d2 = dg(bf, 2), d3 = dg(bf, 3), c = (bf >> 8) & 1;
+                const int32_t own = (d0 == 3) + 2 * (d1 == 3) + 4 * (d2 == 3) + 8 * (d3 == 3);
+                if (t == 0) {
+                    at(0, i, j) = own;
+                    at(1, i, j) = c + 2 * (d2 == 3) + 4 * (d3 == 1) + 8 * (d3 == 2);
+                    at(2, i, j) = c + 2 * (d2 == 1) + 4 * (d2 == 2) + 8 * (d3 == 3);
+                } else if (t == 1) {
+                    at(1, i, j) = own;
+                    at(2, i, j) = (d0 == 3) + 2 * (d1 == 1) + 4 * (d1 == 2) + 8 * c;
+                    at(0, i, j) = (d0 == 1) + 2 * (d0 == 2) + 4 * (d1 == 3) + 8 * c;
+                } else {
+                    at(2, i, j) = own;
+                    at(0, i, j) = (d0 == 1) + 2 * (d0 == 2) + 4 * c + 8 * (d3 == 3);
+                    at(1, i, j) = (d0 == 3) + 2 * c + 4 * (d3 == 1) + 8 * (d3 == 2);
+                }
+                break;
+            }
+            default: break;
+        }
+    }
+};
+
+}  // namespace rtb

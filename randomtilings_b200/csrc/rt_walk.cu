@@ -9,6 +9,7 @@
 
 #include "rt_internal.h"
 #include "rt_models.cuh"
+#include "rt_tridimer.cuh"
 
 namespace rtb {
 
@@ -31,8 +32,15 @@ __device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned lon
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-__device__ __forceinline__ unsigned long long* slot(const WalkArgs& a, int cta, int side, int parity, int lat) {
-    return a.xbuf + ((((size_t)cta * 2 + side) * 2 + parity) * a.nlat + lat) * a.xwords;
+__device__ __forceinline__ unsigned long long* slot(const WalkArgs& a, int cta, int side, int parity, int lat,
+                                                   int k) {
+    return a.xbuf + (((((size_t)cta * 2 + side) * 2 + parity) * a.nlat + lat) * a.xslots + k) * a.xwords;
+}
+
+// Index of the k-th set bit of mask (k < popc(mask)).
+__device__ __forceinline__ int nth_bit(uint32_t mask, int k) {
+    for (int i = 0; i < k; ++i) mask &= mask - 1;
+    return __ffs(mask) - 1;
 }
 
 template <class T>
@@ -139,6 +147,7 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
     int64_t next_epoch = a.rng_kind == 0 && a.nepochs > 0 ? a.epoch_start[0] : INT64_MAX;
     uint64_t t0 = 0;
     uint32_t d = a.nphases > 0 ? __ldg(a.phases) : 0u;
+    uint32_t d_prev = 0u;
 
     __syncthreads();
     for (int64_t ph = 0; ph < a.nphases; ++ph) {
@@ -158,10 +167,9 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
             }
             __syncthreads();  // positions are drawn by other threads than the ones seeding them
         }
-        const int op = (int)ph_op(d);
         const bool draws = (d & PH_DRAWS) != 0u;
-        const typename Model::Ctx x0 = Model::ctx(a, lat, plane, d);
-        const typename Model::Ctx x1 = Model::ctx(a, lat + (size_t)NC * plane, plane, d);
+        const typename Model::Ctx x0 = Model::ctx(a, lat, plane, d, a0 - 1);
+        const typename Model::Ctx x1 = Model::ctx(a, lat + (size_t)NC * plane, plane, d, a0 - 1);
 
         auto site = [&](int q, int r, int c) {
             uint32_t k = 0;
@@ -199,21 +207,22 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
             }
         }
         if (ph > 0) {
-            // Halo rows of the colour flipped in the previous phase.
-            const int pcol = Model::flipped(op == (int)OP_STEP ? (int)ph_b(d) : (int)ph_a(d));
+            // Halo rows of every array the neighbours wrote in the previous phase.
+            const uint32_t mask = Model::written(d_prev);
+            const int nx = __popc(mask);
             const int par = (int)((ph - 1) & 1);
             const uint32_t tag = (uint32_t)ph;
             bool ok = true;
-            const int per_side = a.nlat * a.xwords;
+            const int per_side = a.nlat * nx * a.xwords;
             for (int e = tid; e < 2 * per_side && ok; e += BLOCK) {
                 const int side = e / per_side;  // 0: row above (from cta-1), 1: row below (from cta+1)
                 const int rem = e % per_side;
-                const int l = rem / a.xwords, w = rem % a.xwords;
+                const int l = rem / (nx * a.xwords), kx = (rem / a.xwords) % nx, w = rem % a.xwords;
                 const int src = side == 0 ? cta - 1 : cta + 1;
                 if (src < 0 || src >= nct) continue;
                 uint32_t v;
-                ok = wait_word(a, slot(a, src, side == 0 ? 1 : 0, par, l) + w, tag, &v, t0);
-                if (ok) unpack_word<T>(row_ptr(l, pcol, side == 0 ? a0 - 1 : a1), w, v);
+                ok = wait_word(a, slot(a, src, side == 0 ? 1 : 0, par, l, kx) + w, tag, &v, t0);
+                if (ok) unpack_word<T>(row_ptr(l, nth_bit(mask, kx), side == 0 ? a0 - 1 : a1), w, v);
             }
             if (__syncthreads_or(!ok)) return;
         }
@@ -224,22 +233,24 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
             site((r - r0) * cols + c, r, c);
         }
         __syncthreads();
-        if (op == (int)OP_STEP && ph + 1 < a.nphases) {
-            // Publish the band's first / last row of the colour just flipped.
-            const int col = Model::flipped((int)ph_a(d));
+        if (ph + 1 < a.nphases) {
+            // Publish the band's first / last row of every array written in this phase.
+            const uint32_t mask = Model::written(d);
+            const int nx = __popc(mask);
             const int par = (int)(ph & 1);
             const unsigned long long tag = (unsigned long long)(uint32_t)(ph + 1) << 32;
-            const int per_side = a.nlat * a.xwords;
+            const int per_side = a.nlat * nx * a.xwords;
             for (int e = tid; e < 2 * per_side; e += BLOCK) {
                 const int side = e / per_side;  // 0: first row (read by cta-1), 1: last row (read by cta+1)
                 const int rem = e % per_side;
-                const int l = rem / a.xwords, w = rem % a.xwords;
+                const int l = rem / (nx * a.xwords), kx = (rem / a.xwords) % nx, w = rem % a.xwords;
                 const int dst = side == 0 ? cta - 1 : cta + 1;
                 if (dst < 0 || dst >= nct) continue;
-                const uint32_t v = pack_word<T>(row_ptr(l, col, side == 0 ? a0 : a1 - 1), w);
-                st_relaxed64(slot(a, cta, side, par, l) + w, tag | v);
+                const uint32_t v = pack_word<T>(row_ptr(l, nth_bit(mask, kx), side == 0 ? a0 : a1 - 1), w);
+                st_relaxed64(slot(a, cta, side, par, l, kx) + w, tag | v);
             }
         }
+        d_prev = d;
         d = d_next;
     }
 
@@ -275,12 +286,14 @@ static KernelFn kernel_for(int family, bool uniform) {
         case FAM_LOZENGE8: return pick_kernel<ThreeColour<int8_t, LozengeRule<false>>>(uniform);
         case FAM_QLOZENGE32: return pick_kernel<ThreeColour<int32_t, LozengeRule<true>>>(uniform);
         case FAM_RECTTRI: return pick_kernel<ThreeColour<int32_t, RectTriRule>>(uniform);
+        case FAM_TRIDIMER: return pick_kernel<TriDimerRule>(uniform);
         default: return nullptr;
     }
 }
 
-static int family_ncol(int family) { return family <= FAM_DOMINO_HB ? 2 : 3; }
-static int family_elem(int family) { return family == FAM_QLOZENGE32 || family == FAM_RECTTRI ? 4 : 1; }
+static int family_ncol(int family) { return family <= FAM_DOMINO_HB ? 2 : family == FAM_TRIDIMER ? 8 : 3; }
+static int family_elem(int family) { return family == FAM_LOZENGE8 || family <= FAM_DOMINO_HB ? 1 : 4; }
+static int family_xslots(int family) { return family == FAM_TRIDIMER ? 4 : 1; }
 
 size_t walk_smem_bytes(int family, int nlat, int rows_per_cta, int cols, int width) {
     const int wpad = (width + 3) & ~3;
@@ -324,6 +337,7 @@ rt_status plan_walk(int family, int device, int nlat, int rows, int cols, int wi
             plan->smem = smem;
             plan->wpad = wpad;
             plan->xwords = family_elem(family) == 1 ? wpad / 4 : wpad;
+            plan->xslots = family_xslots(family);
             plan->fn = (const void*)fn;
             return RT_OK;
         }
@@ -337,6 +351,7 @@ rt_status launch_walk(const WalkPlan& plan, WalkArgs& args, cudaStream_t stream,
     args.rows_per_cta = plan.rows_per_cta;
     args.wpad = plan.wpad;
     args.xwords = plan.xwords;
+    args.xslots = plan.xslots;
     void* kargs[] = {&args};
     cudaError_t e = cudaLaunchCooperativeKernel(plan.fn, dim3(plan.ctas), dim3(plan.block), kargs, plan.smem, stream);
     if (e != cudaSuccess) {
@@ -376,6 +391,18 @@ __global__ void merge_kernel(int32_t* __restrict__ t, int n, int ncol, int kind,
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)n * n) return;
     const int i = (int)(idx / n), j = (int)(idx % n);
+    if (kind == 3) {
+        // Triangle dimers: only the lozenge states go back (TriangleDimerTiler.cpp:362-376);
+        // (even, even) cells keep the caller's values.
+        const int m = n / 2;
+        const int64_t at = (int64_t)(i / 2) * m + j / 2;
+        if (i % 2 == 0) {
+            if (j % 2 == 1) t[idx] = (int32_t)a0[at];
+        } else {
+            t[idx] = (int32_t)(j % 2 == 0 ? a1[at] : a2[at]);
+        }
+        return;
+    }
     const int w = n / ncol;
     int c, col;
     if (kind == 0) {
@@ -413,6 +440,36 @@ rt_status launch_split(bool merge, int elem_bytes, int kind, int ncol, int n, in
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         *err = std::string("split/merge launch failed: ") + cudaGetErrorString(e);
+        return RT_E_CUDA;
+    }
+    return RT_OK;
+}
+
+// Number of differing 32-bit words between two equally sized arrays (CFTP
+// coalescence test of the coupled chains, done on the device so that only a
+// counter crosses to the host).
+__global__ void count_diff_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, size_t words,
+                                  unsigned long long* count) {
+    unsigned long long local = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += (size_t)gridDim.x * blockDim.x)
+        local += __ldg(a + i) != __ldg(b + i);
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
+}
+
+rt_status launch_count_diff(const void* a, const void* b, size_t bytes, unsigned long long* d_count,
+                            cudaStream_t stream, std::string* err) {
+    const size_t words = bytes / 4;
+    const int threads = 256;
+    const int blocks = (int)std::min<size_t>((words + threads - 1) / threads, 148 * 8);
+    cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof *d_count, stream);
+    if (e == cudaSuccess && blocks > 0) {
+        count_diff_kernel<<<blocks, threads, 0, stream>>>(static_cast<const uint32_t*>(a),
+                                                          static_cast<const uint32_t*>(b), words, d_count);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        *err = std::string("coalescence check failed: ") + cudaGetErrorString(e);
         return RT_E_CUDA;
     }
     return RT_OK;

@@ -139,6 +139,21 @@ class DominoTiler(_Tiler):
         else:
             super().Walk(t, steps, seed)
 
+    def CFTP(self, tmax, tmin, first_steps: int = 1024, schedule: int = _capi.RT_CFTP_DOUBLING,
+             master_seed: int = 345903, max_trials: int = 30):
+        """Coupling from the past (Examples/AztecDiamondCftpEx.cpp:42-68); the
+        handle must use kernel=RT_KERNEL_CFTP.  Returns (tiling, stats dict)."""
+        a, n = _as_tiling(tmax)
+        b, n2 = _as_tiling(tmin)
+        if n != n2:
+            raise ValueError("tmax and tmin differ in size")
+        out = np.zeros_like(a)
+        st = _capi.RtCftpStats()
+        self._check(self._lib.rt_cftp(self._h, a.ctypes.data, b.ctypes.data, n, int(first_steps), int(schedule),
+                                      int(master_seed), int(max_trials), out.ctypes.data, ctypes.byref(st)))
+        return out, {"total_steps": st.total_steps, "trials": st.trials, "coalesced": bool(st.coalesced),
+                     "device_ms": st.device_ms}
+
 
 class LozengeTiler(_Tiler):
     MODEL = _capi.RT_LOZENGE
@@ -164,3 +179,12 @@ class RectTriangleTiler(_Tiler):
 
 class TriangleDimerTiler(_Tiler):
     MODEL = _capi.RT_TRIDIMER
+
+    # static helpers (src/TriangleDimer/TriangleDimerTiler.h:182-195)
+    IceCreamCone = staticmethod(lambda n, m: builders.call("rt_tridimer_ice_cream_cone", n, m))
+    TestButterfly = staticmethod(lambda k: builders.call("rt_tridimer_test_butterfly", k))
+    TilingToTriangleFlips = staticmethod(lambda t: builders.call("rt_tridimer_triangle_flips", t))
+    TilingToButterflyFlips = staticmethod(lambda t: builders.call("rt_tridimer_butterfly_flips", t))
+    TilingToVertices = staticmethod(lambda t: builders.call("rt_tridimer_vertices", t))
+    TilingToDomain = staticmethod(lambda t: builders.call("rt_tridimer_tiling_to_domain", t))
+    DimerIndicator = staticmethod(lambda t, c: builders.call("rt_tridimer_dimer_indicator", t, c))

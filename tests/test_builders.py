@@ -81,3 +81,25 @@ def test_not_tileable_is_an_error():
     d = D.Rectangle(3, 3)  # odd area
     with pytest.raises(rt.RtError):
         D.MinTiling(d)
+
+
+T = rt.TriangleDimerTiler
+CONES = [(6, 0), (5, 0), (8, 2), (10, 3), (12, 0)]
+
+
+@pytest.mark.parametrize("n,m", CONES)
+def test_tridimer_cone_and_derived_states(n, m):
+    key = f"tridimer/cone{n}_{m}"
+    t = T.IceCreamCone(n, m)
+    assert np.array_equal(t, B[f"{key}/tiling"])
+    assert np.array_equal(T.TilingToTriangleFlips(t), B[f"{key}/triangle_flips"])
+    assert np.array_equal(T.TilingToButterflyFlips(t), B[f"{key}/butterfly_flips"])
+    assert np.array_equal(T.TilingToVertices(t), B[f"{key}/vertices"])
+    assert np.array_equal(T.TilingToDomain(t), B[f"{key}/domain"])
+    for c in range(3):
+        assert np.array_equal(T.DimerIndicator(t, c), B[f"{key}/dimer{c}"])
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_tridimer_test_butterfly(k):
+    assert np.array_equal(T.TestButterfly(k), B[f"tridimer/butterfly{k}"])

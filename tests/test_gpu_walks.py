@@ -145,3 +145,26 @@ def test_bad_sizes_are_rejected(rt):
     tl = rt.LozengeTiler()
     with pytest.raises(rt.RtError):
         tl.Walk(np.zeros(10 * 10, dtype=np.int32), 10, 1)
+
+
+@pytest.mark.parametrize("key", cases("walks", "tridimer/"))
+def test_tridimer_golden(rt, key):
+    g = golden("walks")
+    tl = rt.TriangleDimerTiler()
+    got = _walk(tl, g[f"{key}/start"], int(g[f"{key}/steps"][0]), int(g[f"{key}/seed"][0]))
+    assert np.array_equal(got, g[f"{key}/end"])
+
+
+@pytest.mark.parametrize("n,m,seed", [(12, 0, 1), (20, 0, 99), (25, 7, -8), (40, 10, 2024)])
+def test_tridimer_vs_restatement(rt, n, m, seed):
+    t = rt.TriangleDimerTiler.IceCreamCone(n, m)
+    tl = rt.TriangleDimerTiler()
+    got = _walk(tl, t, 3000, seed)
+    assert np.array_equal(got, po.tridimer_walk(t, 3000, seed))
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_tridimer_single_butterflies(rt, k):
+    t = rt.TriangleDimerTiler.TestButterfly(k)
+    got = _walk(rt.TriangleDimerTiler(), t, 500, 5)
+    assert np.array_equal(got, po.tridimer_walk(t, 500, 5))

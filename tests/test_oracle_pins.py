@@ -122,3 +122,34 @@ def test_reference_serial_equals_threaded():
     a = po.RefTiler("domino", t.size // 2, threads=1).walk(t, 500, 3)
     b = po.RefTiler("domino", t.size // 2, threads=4).walk(t, 500, 3)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("key", cases("walks", "tridimer/"))
+def test_tridimer_walk_matches_reference(key):
+    g = golden("walks")
+    got = po.tridimer_walk(g[f"{key}/start"], int(g[f"{key}/steps"][0]), int(g[f"{key}/seed"][0]))
+    assert np.array_equal(got, g[f"{key}/end"])
+
+
+@pytest.mark.skipif(not po.have_ref(), reason="oracle/_ref not built here")
+@pytest.mark.parametrize("n,m,seed", [(12, 0, 1), (16, 4, 12345), (25, 7, -8)])
+def test_tridimer_fresh_reference_runs(n, m, seed):
+    t = po.ref_build("tridimer_ice_cream_cone", p0=n, p1=m)
+    r = po.RefTiler("tridimer", t.size).walk(t, 2000, seed)
+    assert np.array_equal(po.tridimer_walk(t, 2000, seed), r)
+
+
+@pytest.mark.skipif(not po.have_ref(), reason="oracle/_ref not built here")
+def test_cftp_composition_matches_reference_epoch_walks():
+    """The oracle's CFTP (used by the GPU CFTP tests) against the same schedule
+    driven through the reference's own epoch Walk."""
+    b = golden("builders")
+    tmax, tmin = b["domino/aztec5/max"], b["domino/aztec5/min"]
+    got, trials, total, ok = po.cftp(tmax, tmin, 128, 345903, "reference")
+    seeds = np.zeros(trials, dtype=np.uint32)
+    po.oracle().orc_mt19937_stream(345903, trials, seeds.ctypes.data)
+    steps = [256] * (trials - 1) + [128]  # newest epoch first
+    sd = [int(s) for s in seeds[::-1]]
+    rt = po.RefTiler("domino_cftp", tmax.size // 2)
+    top, bot = rt.walk_epochs(tmax, steps, sd), rt.walk_epochs(tmin, steps, sd)
+    assert ok and np.array_equal(top, bot) and np.array_equal(top, got)
