@@ -18,6 +18,7 @@
 
 #include "../rt_b200.h"
 #include "../rt_b200_host.h"
+#include "../rt_b200_svg.h"
 
 namespace rt {
 
@@ -80,6 +81,13 @@ public:
         detail::check(rt_walk(h_, reinterpret_cast<int32_t*>(t.data()), detail::side(t), steps, seed), h_);
     }
     rt_tiler* handle() { return h_; }
+    // src/common/common.h:50-69
+    static void SaveMatrix(const std::vector<int>& a, const std::string& f) {
+        detail::check(rt_save_matrix(detail::p(a), a.size(), f.c_str()), nullptr);
+    }
+    static std::vector<int> LoadMatrix(const std::string& f) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) { return rt_load_matrix(f.c_str(), o, c, l); });
+    }
 };
 
 // src/Domino/DominoTiler.h:43-115
@@ -137,6 +145,21 @@ public:
             return rt_domino_tiling_to_height(detail::p(t), t.size(), detail::p(d), d.size(), o, c, l);
         });
     }
+    static void DomainToSVG(const domain& d, const std::string& f) {
+        detail::check(rt_domino_domain_svg(detail::p(d), d.size(), f.c_str()), nullptr);
+    }
+    static void TilingToSVG(const tiling& t, const std::string& f) {
+        detail::check(rt_domino_tiling_svg(detail::p(t), t.size(), f.c_str()), nullptr);
+    }
+    static void MayaToSVG(const tiling& t, const std::string& f) {
+        detail::check(rt_domino_maya_svg(detail::p(t), t.size(), f.c_str()), nullptr);
+    }
+    static void DimerToSVG(const tiling& t, const std::string& f) {
+        detail::check(rt_domino_dimer_svg(detail::p(t), t.size(), nullptr, 0, f.c_str()), nullptr);
+    }
+    static void DimerToSVG(const tiling& t, const domain& d, const std::string& f) {
+        detail::check(rt_domino_dimer_svg(detail::p(t), t.size(), detail::p(d), d.size(), f.c_str()), nullptr);
+    }
 };
 
 // src/Lozenge/LozengeTiler.h:35-79
@@ -177,6 +200,21 @@ public:
             return rt_lozenge_tiling_to_height(detail::p(t), t.size(), detail::p(d), d.size(), o, c, l);
         });
     }
+    static void DomainToSVG(const domain& d, const std::string& f) {
+        detail::check(rt_lozenge_domain_svg(detail::p(d), d.size(), f.c_str()), nullptr);
+    }
+    static void TilingToSVG(const tiling& t, const std::string& f) {
+        detail::check(rt_lozenge_tiling_svg(detail::p(t), t.size(), f.c_str()), nullptr);
+    }
+    static void DimerToSVG(const tiling& t, const std::string& f) {
+        detail::check(rt_lozenge_dimer_svg(detail::p(t), t.size(), nullptr, 0, f.c_str()), nullptr);
+    }
+    static void DimerToSVG(const tiling& t, const domain& d, const std::string& f) {
+        detail::check(rt_lozenge_dimer_svg(detail::p(t), t.size(), detail::p(d), d.size(), f.c_str()), nullptr);
+    }
+    static void PrintDomain(const domain& d, const std::string& f) {
+        detail::check(rt_lozenge_print_domain(detail::p(d), d.size(), f.c_str()), nullptr);
+    }
 };
 
 // src/RectTriangle/RectTriangleTiler.h:30-73
@@ -194,6 +232,59 @@ public:
         return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
             return rt_recttri_from_lozenge(detail::p(tL), tL.size(), detail::p(dL), dL.size(), o, c, l);
         });
+    }
+    static void TilingToSVG(const tiling& t, const std::string& f) {
+        detail::check(rt_recttri_tiling_svg(detail::p(t), t.size(), f.c_str()), nullptr);
+    }
+};
+
+// src/TriangleDimer/TriangleDimerTiler.h:72-202
+class TriangleDimerTiler : public TilerBase {
+public:
+    explicit TriangleDimerTiler(int device = 0) : TilerBase(RT_TRIDIMER, device, RT_KERNEL_DEFAULT) {}
+    explicit TriangleDimerTiler(const rt_config& cfg) : TilerBase(cfg) {}
+    static tiling IceCreamCone(int N, int M) {
+        return detail::build(
+            [&](int32_t* o, int64_t c, int64_t* l) { return rt_tridimer_ice_cream_cone(N, M, o, c, l); });
+    }
+    static tiling TestButterfly(int type) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) { return rt_tridimer_test_butterfly(type, o, c, l); });
+    }
+    static std::vector<int> TilingToTriangleFlips(const tiling& t) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_tridimer_triangle_flips(detail::p(t), t.size(), o, c, l);
+        });
+    }
+    static std::vector<int> TilingToButterflyFlips(const tiling& t) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_tridimer_butterfly_flips(detail::p(t), t.size(), o, c, l);
+        });
+    }
+    static std::vector<int> TilingToVertices(const tiling& t) {
+        return detail::build(
+            [&](int32_t* o, int64_t c, int64_t* l) { return rt_tridimer_vertices(detail::p(t), t.size(), o, c, l); });
+    }
+    static domain TilingToDomain(const tiling& t) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_tridimer_tiling_to_domain(detail::p(t), t.size(), o, c, l);
+        });
+    }
+    static std::vector<int> DimerIndicator(const tiling& t, int c0) {
+        return detail::build([&](int32_t* o, int64_t c, int64_t* l) {
+            return rt_tridimer_dimer_indicator(detail::p(t), t.size(), c0, o, c, l);
+        });
+    }
+    static void DomainToSVG(const domain& d, const std::string& f) {
+        detail::check(rt_tridimer_domain_svg(detail::p(d), d.size(), f.c_str()), nullptr);
+    }
+    static void TilingToSVG(const tiling& t, const std::string& f) {
+        detail::check(rt_tridimer_tiling_svg(detail::p(t), t.size(), f.c_str()), nullptr);
+    }
+    static void DimerToSVG(const tiling& t, const std::string& f) {
+        detail::check(rt_tridimer_dimer_svg(detail::p(t), t.size(), nullptr, 0, f.c_str()), nullptr);
+    }
+    static void DimerToSVG(const tiling& t, const domain& d, const std::string& f) {
+        detail::check(rt_tridimer_dimer_svg(detail::p(t), t.size(), detail::p(d), d.size(), f.c_str()), nullptr);
     }
 };
 

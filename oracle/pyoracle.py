@@ -238,3 +238,21 @@ def ref_build(what: str, a=None, b=None, p0: int = 0, p1: int = 0) -> np.ndarray
     out = np.zeros(max(n, 1), dtype=np.int32)
     lib.ref_build(*args, out.ctypes.data, n)
     return out[:n]
+
+
+REF_WRITE = {
+    "domino_domain": 0, "domino_tiling": 1, "domino_maya": 2, "domino_dimer": 3, "domino_dimer_d": 4,
+    "lozenge_domain": 10, "lozenge_tiling": 11, "lozenge_dimer": 12, "lozenge_dimer_d": 13, "lozenge_print_domain": 14,
+    "recttri_tiling": 20, "tridimer_domain": 30, "tridimer_tiling": 31, "tridimer_dimer": 32, "tridimer_dimer_d": 33,
+    "save_matrix": 40,
+}
+
+
+def ref_write(what: str, filename: str, a, b=None) -> None:
+    """One of the reference's SVG / text writers, run through oracle/_ref."""
+    A = np.ascontiguousarray(a, dtype=np.int32).reshape(-1)
+    B = None if b is None else np.ascontiguousarray(b, dtype=np.int32).reshape(-1)
+    rc = ref().ref_write(REF_WRITE[what], A.ctypes.data, A.size, None if B is None else B.ctypes.data,
+                         0 if B is None else B.size, str(filename).encode())
+    if rc != 0:
+        raise RuntimeError(f"ref_write({what}) failed")

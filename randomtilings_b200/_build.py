@@ -31,7 +31,8 @@ def sources() -> list[str]:
 
 def headers() -> list[str]:
     out = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    out.append(os.path.join(HERE, "..", "include", "rt_b200.h"))
+    inc = os.path.join(HERE, "..", "include")
+    out += [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
     return out
 
 

@@ -120,6 +120,25 @@ HOST_SIGNATURES = {
 for _name, _args in HOST_SIGNATURES.items():
     SIGNATURES[_name] = (ctypes.c_int, [*_args, _P, _I64, _PL])
 
+_S = ctypes.c_char_p
+# include/rt_b200_svg.h
+SIGNATURES.update({
+    "rt_domino_domain_svg": (ctypes.c_int, [_P, _I64, _S]),
+    "rt_domino_tiling_svg": (ctypes.c_int, [_P, _I64, _S]),
+    "rt_domino_maya_svg": (ctypes.c_int, [_P, _I64, _S]),
+    "rt_domino_dimer_svg": (ctypes.c_int, [_P, _I64, _P, _I64, _S]),
+    "rt_lozenge_domain_svg": (ctypes.c_int, [_P, _I64, _S]),
+    "rt_lozenge_tiling_svg": (ctypes.c_int, [_P, _I64, _S]),
+    "rt_lozenge_dimer_svg": (ctypes.c_int, [_P, _I64, _P, _I64, _S]),
+    "rt_lozenge_print_domain": (ctypes.c_int, [_P, _I64, _S]),
+    "rt_recttri_tiling_svg": (ctypes.c_int, [_P, _I64, _S]),
+    "rt_tridimer_domain_svg": (ctypes.c_int, [_P, _I64, _S]),
+    "rt_tridimer_tiling_svg": (ctypes.c_int, [_P, _I64, _S]),
+    "rt_tridimer_dimer_svg": (ctypes.c_int, [_P, _I64, _P, _I64, _S]),
+    "rt_save_matrix": (ctypes.c_int, [_P, _I64, _S]),
+    "rt_load_matrix": (ctypes.c_int, [_S, _P, _I64, _PL]),
+})
+
 _lib = None
 
 

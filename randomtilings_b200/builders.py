@@ -44,3 +44,30 @@ def aztec_rectangle(order: int, remove) -> np.ndarray:
     _capi.check(lib.rt_domino_aztec_rectangle(order, rem.ctypes.data, rem.size, out.ctypes.data, out.size,
                                               ctypes.byref(n)))
     return out
+
+
+def write(name: str, filename: str, *arrays) -> None:
+    """Calls an SVG / text writer of include/rt_b200_svg.h; None arrays pass NULL."""
+    lib = _capi.load()
+    cargs, keep = [], []
+    for a in arrays:
+        if a is None:
+            cargs += [None, 0]
+        else:
+            arr = _arr(a)
+            keep.append(arr)
+            cargs += [arr.ctypes.data, arr.size]
+    _capi.check(getattr(lib, name)(*cargs, str(filename).encode()))
+
+
+def save_matrix(a, filename: str) -> None:
+    write("rt_save_matrix", filename, a)
+
+
+def load_matrix(filename: str) -> np.ndarray:
+    lib = _capi.load()
+    n = ctypes.c_int64()
+    _capi.check(lib.rt_load_matrix(str(filename).encode(), None, 0, ctypes.byref(n)))
+    out = np.zeros(max(n.value, 1), dtype=np.int32)
+    _capi.check(lib.rt_load_matrix(str(filename).encode(), out.ctypes.data, out.size, ctypes.byref(n)))
+    return out[: n.value]

@@ -1,0 +1,513 @@
+// rt_svg.cpp -- SVG and text output of domains, tilings and dimer covers.
+//
+// The reference draws with std::ofstream and the stream's default number
+// formatting (6 significant digits); these writers produce the same bytes,
+// so pictures and matrices written by either side are interchangeable (the
+// tests compare SHA-256 digests with the reference's own output).  Each
+// writer cites the reference function whose format it keeps.
+#include <cmath>
+#include <cstdint>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/rt_b200.h"
+#include "../../include/rt_b200_host.h"
+#include "../../include/rt_b200_svg.h"
+
+namespace {
+
+using Vec = std::vector<int32_t>;
+const double kSqrt3 = 1.7320508075688772935274;  // common.h:41
+
+int side_of(int64_t len) {
+    int64_t r = (int64_t)std::llround(std::sqrt((double)len));
+    while (r * r > len) --r;
+    while ((r + 1) * (r + 1) <= len) ++r;
+    return (int)r;
+}
+
+const char* kSvgOpen = "<svg xmlns='http://www.w3.org/2000/svg' xmlns:xlink=\"http://www.w3.org/1999/xlink\" ";
+
+// <use xlink:href = "#id" x = "X" y = "Y"/>  (the spaced form) or without spaces.
+void use(std::ostream& o, const char* id, double x, double y, bool spaced) {
+    if (spaced)
+        o << "<use xlink:href = \"#" << id << "\" x = \"" << x << "\" y = \"" << y << "\"/>\n";
+    else
+        o << "<use xlink:href=\"#" << id << "\" x=\"" << x << "\" y=\"" << y << "\"/>\n";
+}
+
+// Header of the triangular-lattice pictures (viewBox 1.5 M, aspect 433.013:500).
+void tri_header(std::ostream& o, double m) {
+    o << kSvgOpen << "height=\"433.013\" width=\"500\" viewBox=\"0 0 " << 3 / 2.0 * m << " " << 3 / 2.0 * m
+      << "\" preserveAspectRatio=\"none\">\n";
+}
+
+rt_status finish(std::ofstream& f) {
+    f.close();
+    return f ? RT_OK : RT_E_INVAL;
+}
+
+// ---- rectangle-triangle face pictures (RectTriangleTiler.cpp:567-697) ----------
+double vx(int i, int j) { return 20 * (i * 1 / 2.0 + j); }
+double vy(int i, int) { return 20 * (i * kSqrt3 / 2.0); }
+
+std::string face_picture(int type, int i, int j) {
+    static const char* kFill[4] = {
+        "", "\" style=\"fill:midnightblue;stroke:midnightblue;stroke-width:.4\" />\n",
+        "\" style=\"fill:slategrey;stroke:slategrey;stroke-width:.4\" />\n",
+        "\" style=\"fill:lightsteelblue;stroke:lightsteelblue;stroke-width:.4\" />\n"};
+    const char* edge = " style=\"stroke:rgb(0,0,0);stroke-width:.5\" stroke-linecap = \"round\" />\n";
+    // Corners P, Q, R of the face and the midpoints p, q, r of the opposite
+    // sides; per face type: which corner polygons / edges / half-edges are drawn.
+    bool PQ = false, PR = false, QR = false, p = false, q = false, r = false;
+    int whole = 0, pPR = 0, pPQ = 0, rRQ = 0, rRP = 0, qQR = 0, qQP = 0;
+    switch (type) {
+        case 1: PR = QR = r = true, whole = 1; break;
+        case 2: QR = PQ = q = true, whole = 3; break;
+        case 3: PQ = PR = p = true, whole = 2; break;
+        case 4: r = true, whole = 2; break;
+        case 5: q = true, whole = 1; break;
+        case 6: p = true, whole = 3; break;
+        case 7: PQ = true, whole = 2; break;
+        case 8: PR = true, whole = 1; break;
+        case 9: QR = true, whole = 3; break;
+        case 10: rRP = 1, rRQ = 2, r = PR = true; break;
+        case 11: qQP = 1, qQR = 3, q = QR = true; break;
+        case 12: pPQ = 2, pPR = 3, p = PQ = true; break;
+        case 13: rRP = 2, rRQ = 1, r = QR = true; break;
+        case 14: qQP = 3, qQR = 1, q = PQ = true; break;
+        case 15: pPQ = 3, pPR = 2, p = PR = true; break;
+        default: break;
+    }
+    double Px, Py, Qx, Qy, Rx, Ry;
+    if (j % 2 == 1) {
+        Px = vx(i + 1, j / 2), Py = vy(i + 1, j / 2);
+        Qx = vx(i + 1, j / 2 + 1), Qy = vy(i + 1, j / 2 + 1);
+        Rx = vx(i, j / 2 + 1), Ry = vy(i, j / 2 + 2);
+    } else {
+        Px = vx(i, j / 2 + 1), Py = vy(i, j / 2 + 1);
+        Qx = vx(i, j / 2), Qy = vy(i, j / 2);
+        Rx = vx(i + 1, j / 2), Ry = vy(i + 1, j / 2);
+    }
+    const double px = (Rx + Qx) / 2, py = (Ry + Qy) / 2;
+    const double qx = (Px + Rx) / 2, qy = (Py + Ry) / 2;
+    const double rx = (Px + Qx) / 2, ry = (Py + Qy) / 2;
+    std::stringstream o;
+    auto poly = [&](double ax, double ay, double bx, double by, double cx, double cy, int colour) {
+        o << "<polygon points=\"" << ax << "," << ay << " " << bx << "," << by << " " << cx << "," << cy << " "
+          << kFill[colour];
+    };
+    auto line = [&](double ax, double ay, double bx, double by) {
+        o << "<line x1=\"" << ax << "\" y1=\"" << ay << "\" x2=\"" << bx << "\" y2=\"" << by << "\"" << edge;
+    };
+    if (whole > 0) poly(Px, Py, Qx, Qy, Rx, Ry, whole);
+    if (pPR > 0) poly(Px, Py, px, py, Rx, Ry, pPR);
+    if (pPQ > 0) poly(Px, Py, px, py, Qx, Qy, pPQ);
+    if (rRQ > 0) poly(Rx, Ry, rx, ry, Qx, Qy, rRQ);
+    if (rRP > 0) poly(Rx, Ry, rx, ry, Px, Py, rRP);
+    if (qQR > 0) poly(Qx, Qy, qx, qy, Rx, Ry, qQR);
+    if (qQP > 0) poly(Qx, Qy, qx, qy, Px, Py, qQP);
+    if (PQ) line(Px, Py, Qx, Qy);
+    if (PR) line(Px, Py, Rx, Ry);
+    if (QR) line(Rx, Ry, Qx, Qy);
+    if (p) line(Px, Py, px, py);
+    if (q) line(Qx, Qy, qx, qy);
+    if (r) line(Rx, Ry, rx, ry);
+    return o.str();
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- dominoes ------------------------------------------------------------------
+rt_status rt_domino_domain_svg(const int32_t* d, int64_t dlen, const char* filename) {
+    if (!d || !filename) return RT_E_INVAL;
+    const int m = side_of(dlen);
+    std::ofstream o(filename);
+    o << kSvgOpen << "height=\"500\" width=\"500\" viewBox=\"0 0 " << m << " " << m << "\">\n";
+    o << "<defs>\n";
+    o << "<g id=\"b\">  <polygon points = \"-.5,-.5 .5,-.5 .5,.5 -.5,.5\" fill=\"blue\"/> </g>\n";
+    o << "<g id=\"w\">  <polygon points = \"-.5,-.5 .5,-.5 .5,.5 -.5,.5\" fill=\"grey\"/> </g>\n";
+    o << "</defs>\n";
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j)
+            if (d[(size_t)i * m + j] == 1) use(o, (i + j) % 2 == 0 ? "b" : "w", j + .5, i + .5, true);
+    o << "</svg>";
+    return finish(o);
+}
+
+// Dominoes as rectangles anchored at the vertex whose up (1) / left-edge (4)
+// bit is set (DominoTiler::TilingToSVG, DominoTiler.cpp:613-640) or as pairs
+// of discs (MayaToSVG, :642-681).
+static rt_status domino_pairs_svg(const int32_t* t, int64_t tlen, const char* filename, bool maya) {
+    if (!t || !filename) return RT_E_INVAL;
+    const int n = side_of(tlen);
+    std::ofstream o(filename);
+    o << kSvgOpen << "height=\"500\" width=\"500\" viewBox=\"0 0 " << (n - 1) << " " << (n - 1) << "\">\n";
+    o << "<defs>\n";
+    if (!maya) {
+        const char* h = "<polygon points = \"-1,0 -1,-1 1,-1 1,0\" fill=\"white\" stroke=\"black\" stroke-width=\".05\"/>";
+        const char* v = "<polygon points = \"-1,-1 0,-1 0,1 -1,1\" fill=\"white\" stroke=\"black\" stroke-width=\".05\"/>";
+        o << "<g id=\"h1\">  " << h << " </g>\n";
+        o << "<g id=\"v1\">  " << v << " </g>\n";
+        o << "<g id=\"h2\">  " << h << " </g>\n";
+        o << "<g id=\"v2\">  " << v << " </g>\n";
+    } else {
+        auto disc = [&](const char* cx, const char* cy, const char* fill) {
+            o << "<circle cx=\"" << cx << "\" cy=\"" << cy << "\" r=\".4\" stroke=\"black\" stroke-width=\".02\" fill=\""
+              << fill << "\"/>";
+        };
+        const char* names[4] = {"h1", "h2", "v1", "v2"};
+        for (int g = 0; g < 4; ++g) {
+            const char* fill = g % 2 == 0 ? "black" : "white";
+            o << "<g id=\"" << names[g] << "\">";
+            if (g < 2) {
+                disc("-.5", "-.5", fill);
+                o << " ";
+                disc(".5", "-.5", fill);
+            } else {
+                disc("-.5", "-.5", fill);
+                o << " ";
+                disc("-.5", ".5", fill);
+            }
+            o << "</g>\n";
+        }
+    }
+    o << "</defs>\n";
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            const int32_t v = t[(size_t)i * n + j];
+            const bool odd = (i + j) % 2 == 1;
+            if ((v & 1) == 1) use(o, odd ? "h1" : "h2", j, i, true);
+            if ((v & 4) == 4) use(o, odd ? "v1" : "v2", j, i, true);
+        }
+    o << "</svg>";
+    return finish(o);
+}
+
+rt_status rt_domino_tiling_svg(const int32_t* t, int64_t tlen, const char* filename) {
+    return domino_pairs_svg(t, tlen, filename, false);
+}
+
+rt_status rt_domino_maya_svg(const int32_t* t, int64_t tlen, const char* filename) {
+    return domino_pairs_svg(t, tlen, filename, true);
+}
+
+// DominoTiler::DimerToSVG(t, d) (DominoTiler.cpp:538-611); d = NULL takes the
+// domain from the tiling (DimerToSVG(t), :533-536).
+rt_status rt_domino_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d, int64_t dlen, const char* filename) {
+    if (!t || !filename) return RT_E_INVAL;
+    const int n = side_of(tlen), m = n - 1;
+    Vec dom;
+    if (!d) {
+        dom.assign((size_t)m * m, 0);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j)
+                if ((t[(size_t)i * n + j] & (2 + 8)) || (t[(size_t)(i + 1) * n + j + 1] & (1 + 4))) dom[(size_t)i * m + j] = 1;
+        d = dom.data();
+        dlen = (int64_t)dom.size();
+    }
+    if (dlen < (int64_t)m * m) return RT_E_INVAL;
+    auto D = [&](int i, int j) { return d[(size_t)i * m + j]; };
+    std::ofstream o(filename);
+    o << kSvgOpen << "height=\"500\" width=\"500\" viewBox=\"0 0 " << m << " " << m << "\">\n";
+    o << "<defs>\n";
+    o << "<g id=\"hd\">  <polyline points= \"-.5,0 .5,0\" stroke=\"red\" stroke-width=\".05\"/> </g>\n";
+    o << "<g id=\"he\">  <polyline points= \"-.5,0 .5,0\" stroke=\"black\" stroke-width=\".01\"/> </g>\n";
+    o << "<g id=\"vd\">  <polyline points= \"0,-.5 0,.5\" stroke=\"red\" stroke-width=\".05\"/> </g>\n";
+    o << "<g id=\"ve\">  <polyline points= \"0,-.5 0,.5\" stroke=\"black\" stroke-width=\".01\"/> </g>\n";
+    o << "<g id=\"b\">  <circle cx=\"0\" cy=\"0\" r=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
+    o << "<g id=\"w\">  <circle cx=\"0\" cy=\"0\" r=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"white\" /> </g>\n";
+    o << "</defs>\n";
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            const double x = j, y = i;
+            const int32_t v = t[(size_t)i * n + j];
+            if ((v & 1) == 1) use(o, "hd", x, y - .5, false);
+            if ((v & 4) == 4) use(o, "vd", x - .5, y, false);
+        }
+    for (int i = 1; i < m; ++i)
+        for (int j = 1; j < m; ++j) {
+            if (D(i, j) != 1) continue;
+            const double x = j + .5, y = i + .5;
+            if ((i + j) % 2 == 1) {
+                if (D(i, j + 1) == 1) use(o, "he", x + .5, y, false);
+                if (D(i, j - 1) == 1) use(o, "he", x - .5, y, false);
+            }
+            if (D(i - 1, j) == 1) use(o, "ve", x, y - .5, false);
+            if (D(i + 1, j) == 1) use(o, "ve", x, y + .5, false);
+        }
+    for (int i = 1; i < m; ++i)
+        for (int j = 1; j < m; ++j)
+            if (D(i, j) == 1) use(o, (i + j) % 2 == 0 ? "b" : "w", j + .5, i + .5, true);
+    o << "</svg>";
+    return finish(o);
+}
+
+// ---- lozenges ----------------------------------------------------------------------
+// LozengeTiler::DomainToSVG (LozengeTiler.cpp:593-613).
+rt_status rt_lozenge_domain_svg(const int32_t* d, int64_t dlen, const char* filename) {
+    if (!d || !filename) return RT_E_INVAL;
+    const int m = side_of(dlen / 2);
+    std::ofstream o(filename);
+    tri_header(o, m);
+    o << "<defs>\n";
+    o << "<g id=\"w\">  <polygon points = \"0,1 .5,0 1,1\" fill=\"lightsteelblue\"/> </g>\n";
+    o << "<g id=\"b\">  <polygon points = \"0,0 1,0 .5,1\" fill=\"slategrey\"/> </g>\n";
+    o << "</defs>\n";
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < 2 * m; ++j)
+            if (d[(size_t)i * 2 * m + j] == 1) use(o, j % 2 == 0 ? "b" : "w", .5 * j + .5 * i, i, true);
+    o << "</svg>";
+    return finish(o);
+}
+
+// LozengeTiler::TilingToSVG (LozengeTiler.cpp:565-590).
+rt_status rt_lozenge_tiling_svg(const int32_t* t, int64_t tlen, const char* filename) {
+    if (!t || !filename) return RT_E_INVAL;
+    const int n = side_of(tlen), m = n - 1;
+    std::ofstream o(filename);
+    tri_header(o, m);
+    o << "<defs>\n";
+    o << "<g id=\"r\">  <polygon points = \"0,0 -1,0 -.5,-1 .5,-1\" fill=\"midnightblue\"/> </g>\n";
+    o << "<g id=\"g\">  <polygon points = \"0,0 1,0 .5,-1 -.5,-1\" fill=\"lightsteelblue\"/> </g>\n";
+    o << "<g id=\"b\">  <polygon points = \"0,0 .5,-1 1,0 .5,1\" fill=\"slategrey\"/> </g>\n";
+    o << "</defs>\n";
+    for (int i = 1; i < n - 1; ++i)
+        for (int j = 1; j < n - 1; ++j) {
+            const int32_t v = t[(size_t)i * n + j];
+            if ((v & 1) == 1) use(o, "r", j + .5 * i, i, true);
+            if ((v & 2) == 2) use(o, "g", j + .5 * i, i, true);
+            if ((v & 8) == 8) use(o, "b", j + .5 * i, i, true);
+        }
+    o << "</svg>";
+    return finish(o);
+}
+
+// LozengeTiler::DimerToSVG(t, d) (LozengeTiler.cpp:487-562); d = NULL takes
+// the domain from the tiling (TilingToDomain, :436-462).
+rt_status rt_lozenge_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d, int64_t dlen, const char* filename) {
+    if (!t || !filename) return RT_E_INVAL;
+    const int n = side_of(tlen), m = n - 1;
+    Vec dom;
+    if (!d) {
+        dom.assign((size_t)2 * m * m, 0);
+        auto set = [&](int r, int c) {
+            if (r >= 0 && r < m && c >= 0 && c < 2 * m) dom[(size_t)r * 2 * m + c] = 1;
+        };
+        for (int i = 0; i < n - 1; ++i)
+            for (int j = 0; j < n - 1; ++j) {
+                const int32_t v = t[(size_t)i * n + j];
+                if (v & 1) set(i - 1, 2 * j), set(i - 1, 2 * j - 1);
+                if (v & 2) set(i - 1, 2 * j), set(i - 1, 2 * j + 1);
+                if (v & 8) set(i - 1, 2 * j + 1), set(i, 2 * j);
+            }
+        d = dom.data();
+        dlen = (int64_t)dom.size();
+    }
+    if (dlen < (int64_t)2 * m * m + 2 * m) {  // the reference reads row N-1 (one past the domain)
+        Vec pad(d, d + dlen);
+        pad.resize((size_t)2 * m * (m + 2), 0);
+        dom.swap(pad);
+        d = dom.data();
+    }
+    auto D = [&](int i, int j) { return d[(size_t)i * m * 2 + j]; };
+    std::ofstream o(filename);
+    tri_header(o, m);
+    o << "<defs>\n";
+    o << "<g id=\"e1\">  <polyline points= \"-.5,-.33333333333 0,-.666666666666\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
+    o << "<g id=\"e2\">  <polyline points= \"0,-.666666666 .5,-.333333333333\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
+    o << "<g id=\"e8\">  <polyline points= \".5,-.333333333333 .5,.333333333333\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
+    o << "<g id=\"d1\">  <polyline points= \"-.5,-.33333333333 0,-.666666666666\" stroke=\"black\" stroke-width=\".025\"/> </g>\n";
+    o << "<g id=\"d2\">  <polyline points= \"0,-.666666666 .5,-.333333333333\" stroke=\"black\" stroke-width=\".025\"/> </g>\n";
+    o << "<g id=\"d8\">  <polyline points= \".5,-.333333333333 .5,.333333333333\" stroke=\"black\" stroke-width=\".025\"/> </g>\n";
+    o << "<g id=\"b\">  <ellipse cx=\".5\" cy=\".333333333333\" rx=\".1\" ry=\".11547\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
+    o << "<g id=\"w\">  <ellipse cx=\".5\" cy=\".666666666666\" rx=\".1\"  ry=\".11547\" stroke=\"black\" stroke-width=\".02\" fill=\"white\" /> </g>\n";
+    o << "</defs>\n";
+    for (int i = 1; i < n - 1; ++i)
+        for (int j = 1; j < n - 1; ++j) {
+            const int32_t v = t[(size_t)i * n + j];
+            if ((v & 1) == 1) use(o, "d1", j + .5 * i, i, true);
+            if ((v & 2) == 2) use(o, "d2", j + .5 * i, i, true);
+            if ((v & 8) == 8) use(o, "d8", j + .5 * i, i, true);
+        }
+    for (int i = 1; i < n - 1; ++i)
+        for (int j = 1; j < 2 * n - 1; ++j)
+            if (D(i, j) == 1 && j % 2 == 0) {
+                if (D(i, j - 1) == 1) use(o, "e1", .5 + .5 * j + .5 * i, i + 1, true);
+                if (D(i, j + 1) == 1) use(o, "e2", .5 + .5 * j + .5 * i, i + 1, true);
+                if (D(i + 1, j - 1) == 1) use(o, "e8", .5 + .5 * j + .5 * i, i + 1, true);
+            }
+    for (int i = 1; i < n - 1; ++i)
+        for (int j = 1; j < 2 * n - 1; ++j)
+            if (D(i, j) == 1) use(o, j % 2 == 0 ? "b" : "w", .5 * i + .5 * j, i, true);
+    o << "</svg>";
+    return finish(o);
+}
+
+// LozengeTiler::PrintDomain (LozengeTiler.cpp:391-403): the M x 2M domain as text.
+rt_status rt_lozenge_print_domain(const int32_t* d, int64_t dlen, const char* filename) {
+    if (!d || !filename) return RT_E_INVAL;
+    const int m = side_of(dlen / 2);
+    std::ofstream o(filename);
+    for (int i = 0; i < m; ++i) {
+        for (int j = 0; j < 2 * m; ++j) o << d[(size_t)i * 2 * m + j] << " ";
+        o << "\n";
+    }
+    return finish(o);
+}
+
+// ---- rectangle-triangle (RectTriangleTiler::TilingToSVG, :567-592) -------------------
+rt_status rt_recttri_tiling_svg(const int32_t* t, int64_t tlen, const char* filename) {
+    if (!t || !filename) return RT_E_INVAL;
+    const int n = side_of(tlen), m = n - 1;
+    const double W = kSqrt3 * 2 * (n + 1), H = 3 / 2.0 * (n + 1), s = 20;
+    std::ofstream o(filename);
+    o << "<svg xmlns='http://www.w3.org/2000/svg' height=\"" << s * H << "\" width=\"" << s * W << "\" >\n";
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) {
+            o << face_picture((t[(size_t)i * n + j + 1] & (0xf << 4)) >> 4, i, 2 * j + 1);
+            o << face_picture(t[(size_t)i * n + j] & 0xf, i, 2 * j);
+        }
+    o << "</svg>";
+    return finish(o);
+}
+
+// ---- triangular-lattice dimers (TriangleDimerTiler.cpp:772-902) ------------------------
+rt_status rt_tridimer_domain_svg(const int32_t* d, int64_t dlen, const char* filename) {
+    if (!d || !filename) return RT_E_INVAL;
+    const int m = side_of(dlen / 2);
+    std::ofstream o(filename);
+    tri_header(o, m);
+    o << "<defs>\n";
+    o << "<g id=\"w\">  <polygon points = \"0,1 .5,0 1,1\" fill=\"paleturquoise\"/> </g>\n";
+    o << "<g id=\"b\">  <polygon points = \"0,0 1,0 .5,1\" fill=\"deepskyblue\"/> </g>\n";
+    o << "</defs>\n";
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < 2 * m; ++j)
+            if (d[(size_t)i * m * 2 + j] == 1) use(o, j % 2 == 0 ? "b" : "w", .5 * j + .5 * i, i, true);
+    o << "</svg>";
+    return finish(o);
+}
+
+rt_status rt_tridimer_tiling_svg(const int32_t* t, int64_t tlen, const char* filename) {
+    if (!t || !filename) return RT_E_INVAL;
+    const int n = side_of(tlen), m = n / 2;
+    std::ofstream o(filename);
+    tri_header(o, m);
+    o << "<defs>\n";
+    o << "<g id=\"dR\">  <polygon points = \"1,-0.6666666667 0.5,-0.3333333333 0.5,0.3333333333 0,0.6666666667 0,1.333333333 0.5,1.666666667 1,1.333333333 1,0.6666666667 1.5,0.3333333333 1.5,-0.3333333333\" fill=\"midnightblue\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
+    o << "<g id=\"dL\">  <polygon points = \"0,-0.6666666667 0.5,-0.3333333333 0.5,0.3333333333 1,0.6666666667 1,1.333333333 0.5,1.666666667 0,1.333333333 0,0.6666666667 -0.5,0.3333333333 -0.5,-0.3333333333\" fill=\"lightsteelblue\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
+    o << "<g id=\"dH\">  <polygon points = \"0,-0.6666666667 0.5,-0.3333333333 1,-0.6666666667 1.5,-0.3333333333 1.5,0.3333333333 1,0.6666666667 0.5,0.3333333333 0,0.6666666667 -0.5,0.3333333333 -0.5,-0.3333333333\" fill=\"slategrey\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
+    o << "</defs>\n";
+    for (int i = 0; i < m - 1; ++i)
+        for (int j = 1; j < 2 * m - 1; j += 2) {
+            const double x = .5 * j + .5 * i;
+            if ((t[(size_t)2 * i * n + j] & 4) == 4) use(o, "dR", x, i, true);
+            if ((t[(size_t)2 * i * n + j] & 8) == 8) use(o, "dL", x, i, true);
+            if ((t[(size_t)(2 * i + 1) * n + j] & 1) == 1) use(o, "dH", x, i, true);
+        }
+    o << "</svg>";
+    return finish(o);
+}
+
+// TriangleDimerTiler::DimerToSVG(t, d) (:841-902); d = NULL takes the domain
+// from the tiling (TilingToDomain).
+rt_status rt_tridimer_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d, int64_t dlen, const char* filename) {
+    if (!t || !filename) return RT_E_INVAL;
+    const int n = side_of(tlen);
+    Vec dom;
+    if (!d) {
+        int64_t len = 0;
+        if (rt_tridimer_tiling_to_domain(t, tlen, nullptr, 0, &len) != RT_OK) return RT_E_INVAL;
+        dom.resize((size_t)len);
+        if (rt_tridimer_tiling_to_domain(t, tlen, dom.data(), len, &len) != RT_OK) return RT_E_INVAL;
+        d = dom.data();
+        dlen = len;
+    }
+    const int m = side_of(dlen / 2);
+    // The reference also reads one cell before the domain and one row past it.
+    Vec pad((size_t)2 * m * (m + 2) + 2, 0);
+    for (int64_t k = 0; k < dlen; ++k) pad[(size_t)k + 2 * m + 1] = d[k];
+    auto D = [&](int i, int j) { return pad[(size_t)(i * 2 * m + j) + 2 * m + 1]; };
+    std::ofstream o(filename);
+    tri_header(o, m);
+    o << "<defs>\n";
+    o << "<g id=\"dR\">  <polyline points= \".5,1 1,0\" stroke=\"darkblue\" stroke-width=\".05\"/> </g>\n";
+    o << "<g id=\"dL\">  <polyline points= \".5,1 0,0\" stroke=\"darkred\" stroke-width=\".05\"/> </g>\n";
+    o << "<g id=\"dH\">  <polyline points= \"1,0 0,0\" stroke=\"darkgreen\" stroke-width=\".05\"/> </g>\n";
+    o << "<g id=\"eR\">  <polyline points= \".5,1 1,0\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
+    o << "<g id=\"eL\">  <polyline points= \".5,1 0,0\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
+    o << "<g id=\"eH\">  <polyline points= \"1,0 0,0\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
+    o << "<g id=\"v1\">  <ellipse cx=\".5\" cy=\"0\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
+    o << "<g id=\"v2\">  <ellipse cx=\"1.5\" cy=\"0\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
+    o << "<g id=\"v3\">  <ellipse cx=\"1\" cy=\"1\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
+    o << "</defs>\n";
+    for (int i = 0; i < m - 1; ++i)
+        for (int j = 1; j < 2 * m - 1; j += 2) {
+            const double x = .5 * j + .5 * i;
+            const int32_t a = t[(size_t)2 * i * n + j], h = t[(size_t)(2 * i + 1) * n + j];
+            if ((a & 4) == 4) use(o, "dR", x, i, true);
+            else if (D(i, j - 1) == 1) use(o, "eR", x, i, true);
+            if ((a & 8) == 8) use(o, "dL", x, i, true);
+            else if (D(i, j - 1) == 1) use(o, "eL", x, i, true);
+            if ((h & 1) == 1) use(o, "dH", x, i, true);
+            else if (D(i, j - 1) == 1 || D(i - 1, j) == 1) use(o, "eH", x, i, true);
+            if ((a & 4) == 0 && D(i, j) == 1) use(o, "eR", x, i, true);
+            if ((a & 8) == 0 && D(i, j - 2) == 1 && j > 1) use(o, "eL", x, i, true);
+        }
+    for (int i = 0; i < m; ++i)
+        for (int j = 2; j < 2 * m; j += 2) {
+            const double x = .5 * j + .5 * i;
+            if (D(i, j) == 1 || D(i, j - 1) == 1) use(o, "v1", x, i, true);
+            if (D(i, j) == 1 || D(i, j + 1) == 1) use(o, "v2", x, i, true);
+            if (D(i, j) == 1 || D(i, j + 1) == 1 || D(i, j - 1) == 1) use(o, "v3", x, i, true);
+        }
+    o << "</svg>";
+    return finish(o);
+}
+
+// ---- text matrices (common.cpp:82-161) ---------------------------------------------------
+// SaveMatrix: sqrt(size) rows of sqrt(size) values, each followed by a space.
+rt_status rt_save_matrix(const int32_t* a, int64_t len, const char* filename) {
+    if (!a || !filename) return RT_E_INVAL;
+    const int n = side_of(len);
+    std::ofstream o(filename);
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < n; ++j) o << a[(size_t)i * n + j] << " ";
+        o << "\n";
+    }
+    return finish(o);
+}
+
+// LoadMatrix: every maximal run of decimal digits is one value (like the
+// reference, minus signs are not read).
+rt_status rt_load_matrix(const char* filename, int32_t* out, int64_t cap, int64_t* len) {
+    if (!filename) return RT_E_INVAL;
+    std::ifstream in(filename);
+    if (!in) return RT_E_INVAL;
+    std::vector<int32_t> v;
+    char c;
+    bool inside = false;
+    int64_t cur = 0;
+    while (in.get(c)) {
+        if (c >= '0' && c <= '9') {
+            cur = inside ? cur * 10 + (c - '0') : (c - '0');
+            inside = true;
+        } else if (inside) {
+            v.push_back((int32_t)cur);
+            inside = false;
+        }
+    }
+    if (inside) v.push_back((int32_t)cur);
+    if (len) *len = (int64_t)v.size();
+    if (!out) return RT_OK;
+    if (cap < (int64_t)v.size()) return RT_E_INVAL;
+    for (size_t k = 0; k < v.size(); ++k) out[k] = v[k];
+    return RT_OK;
+}
+
+}  // extern "C"

@@ -40,6 +40,9 @@ def _writeback(dst, src: np.ndarray) -> None:
 
 class _Tiler:
     MODEL = -1
+    # common helpers (src/common/common.h:50-69)
+    SaveMatrix = staticmethod(lambda a, f: builders.save_matrix(a, f))
+    LoadMatrix = staticmethod(lambda f: builders.load_matrix(f))
 
     def __init__(self, device: int = 0, kernel: int = _capi.RT_KERNEL_DEFAULT, rng: int = _capi.RT_RNG_TINYMT,
                  q: float = 0.99, qcmp: int = _capi.RT_QCMP_FLOAT32, weights=None, stream=None):
@@ -124,6 +127,14 @@ class DominoTiler(_Tiler):
     TilingToDomain = staticmethod(lambda t: builders.call("rt_domino_tiling_to_domain", t))
     HeightfuncToTiling = staticmethod(lambda h, d: builders.call("rt_domino_height_to_tiling", h, d))
     TilingToHeightfunc = staticmethod(lambda t, d: builders.call("rt_domino_tiling_to_height", t, d))
+    DomainToSVG = staticmethod(lambda d, f: builders.write("rt_domino_domain_svg", f, d))
+    TilingToSVG = staticmethod(lambda t, f: builders.write("rt_domino_tiling_svg", f, t))
+    MayaToSVG = staticmethod(lambda t, f: builders.write("rt_domino_maya_svg", f, t))
+
+    @staticmethod
+    def DimerToSVG(t, *args):  # DimerToSVG(t, filename) or DimerToSVG(t, d, filename)
+        d, f = (None, args[0]) if len(args) == 1 else args
+        builders.write("rt_domino_dimer_svg", f, t, d)
 
     def Walk(self, t, steps, seed=None) -> None:  # noqa: N802 -- reference name
         """Walk(t, steps, seed) or Walk(t, [steps...], [seeds...]) (DominoTiler.h:73,76)."""
@@ -166,6 +177,14 @@ class LozengeTiler(_Tiler):
     TilingToDomain = staticmethod(lambda t: builders.call("rt_lozenge_tiling_to_domain", t))
     HeightfuncToTiling = staticmethod(lambda h, d: builders.call("rt_lozenge_height_to_tiling", h, d))
     TilingToHeightfunc = staticmethod(lambda t, d: builders.call("rt_lozenge_tiling_to_height", t, d))
+    DomainToSVG = staticmethod(lambda d, f: builders.write("rt_lozenge_domain_svg", f, d))
+    TilingToSVG = staticmethod(lambda t, f: builders.write("rt_lozenge_tiling_svg", f, t))
+    PrintDomain = staticmethod(lambda d, f: builders.write("rt_lozenge_print_domain", f, d))
+
+    @staticmethod
+    def DimerToSVG(t, *args):
+        d, f = (None, args[0]) if len(args) == 1 else args
+        builders.write("rt_lozenge_dimer_svg", f, t, d)
 
 
 class RectTriangleTiler(_Tiler):
@@ -175,6 +194,7 @@ class RectTriangleTiler(_Tiler):
     maxHex = staticmethod(lambda n: builders.call("rt_recttri_max_hex", n))
     minHex = staticmethod(lambda n: builders.call("rt_recttri_min_hex", n))
     LozengeToRectTriangle = staticmethod(lambda tl, dl: builders.call("rt_recttri_from_lozenge", tl, dl))
+    TilingToSVG = staticmethod(lambda t, f: builders.write("rt_recttri_tiling_svg", f, t))
 
 
 class TriangleDimerTiler(_Tiler):
@@ -188,3 +208,10 @@ class TriangleDimerTiler(_Tiler):
     TilingToVertices = staticmethod(lambda t: builders.call("rt_tridimer_vertices", t))
     TilingToDomain = staticmethod(lambda t: builders.call("rt_tridimer_tiling_to_domain", t))
     DimerIndicator = staticmethod(lambda t, c: builders.call("rt_tridimer_dimer_indicator", t, c))
+    DomainToSVG = staticmethod(lambda d, f: builders.write("rt_tridimer_domain_svg", f, d))
+    TilingToSVG = staticmethod(lambda t, f: builders.write("rt_tridimer_tiling_svg", f, t))
+
+    @staticmethod
+    def DimerToSVG(t, *args):
+        d, f = (None, args[0]) if len(args) == 1 else args
+        builders.write("rt_tridimer_dimer_svg", f, t, d)

@@ -24,6 +24,9 @@ int main(int argc, char** argv) {
         rt::tiling t = rt::LozengeTiler::MaxTiling(d);
         save(f, "lozenge_max", t);
         save(f, "lozenge_hmax", rt::LozengeTiler::TilingToHeightfunc(t, d));
+        rt::tiling cone = rt::TriangleDimerTiler::IceCreamCone(10, 3);
+        save(f, "cone", cone);
+        if (argc > 3) rt::LozengeTiler::TilingToSVG(t, argv[3]);
         rt::domain a = rt::DominoTiler::AztecDiamond(12);
         rt::tiling m = rt::DominoTiler::MinTiling(a);
         save(f, "aztec_min", m);
@@ -35,6 +38,9 @@ int main(int argc, char** argv) {
             std::vector<long> steps{256, 128}, seeds{2718281, 345903};
             D.Walk(m, steps, seeds);
             save(f, "aztec_epochs", m);
+            rt::TriangleDimerTiler T(0);
+            T.Walk(cone, 800, 9);
+            save(f, "cone_walk", cone);
         }
     } catch (const rt::Error& e) {
         std::fprintf(stderr, "rt::Error %d: %s\n", (int)e.status, e.what());

@@ -176,6 +176,52 @@ def example_outputs() -> dict:
     return rec
 
 
+SVG_CASES = [
+    # (writer, builders.npz / walks.npz key of the first array, key of the second or None)
+    ("domino_domain", "b:domino/aztec5/domain", None),
+    ("domino_domain", "b:domino/rect5x8/domain", None),
+    ("domino_tiling", "b:domino/aztec5/min", None),
+    ("domino_tiling", "w:domino/aztec13/s42/end", None),
+    ("domino_maya", "b:domino/aztec8/max", None),
+    ("domino_dimer", "b:domino/aztec5/min", None),
+    ("domino_dimer", "w:domino_cftp/aztec13/s-7/end", None),
+    ("domino_dimer_d", "b:domino/aztec8/min", "b:domino/aztec8/domain"),
+    ("lozenge_domain", "b:lozenge/hex10_2/domain", None),
+    ("lozenge_tiling", "b:lozenge/hex10_2/max", None),
+    ("lozenge_tiling", "w:lozenge/hex13_5/s42/end", None),
+    ("lozenge_dimer", "b:lozenge/hex4_1/min", None),
+    ("lozenge_dimer", "w:qlozenge/hex10_2/s5/end", None),
+    ("lozenge_dimer_d", "b:lozenge/hex10_2/min", "b:lozenge/hex10_2/domain"),
+    ("lozenge_print_domain", "b:lozenge/hex4_1/domain", None),
+    ("recttri_tiling", "b:recttri/max_hex5", None),
+    ("recttri_tiling", "b:recttri/min_hex5", None),
+    ("recttri_tiling", "b:recttri/slope_hex5", None),
+    ("recttri_tiling", "w:recttri/slope_hex9/s42/end", None),
+    ("tridimer_domain", "b:tridimer/cone6_0/domain", None),
+    ("tridimer_tiling", "b:tridimer/cone6_0/tiling", None),
+    ("tridimer_tiling", "w:tridimer/cone10_3/s7/end", None),
+    ("tridimer_dimer", "b:tridimer/cone6_0/tiling", None),
+    ("tridimer_dimer", "w:tridimer/cone8_2/s42/end", None),
+    ("tridimer_dimer_d", "b:tridimer/cone10_3/tiling", "b:tridimer/cone10_3/domain"),
+    ("save_matrix", "b:recttri/max_hex5", None),
+    ("save_matrix", "b:tridimer/cone6_0/domain", None),
+]
+
+
+def svg_digests(b: dict, w: dict) -> dict:
+    """SHA-256 of the reference's writers on the cases above."""
+    import tempfile
+
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for k, (writer, ka, kb) in enumerate(SVG_CASES):
+            get = lambda key: (b if key[0] == "b" else w)[key[2:]]  # noqa: E731
+            path = os.path.join(tmp, f"{k}.out")
+            po.ref_write(writer, path, get(ka), None if kb is None else get(kb))
+            out[f"{k}:{writer}:{ka}:{kb}"] = hashlib.sha256(open(path, "rb").read()).hexdigest()
+    return out
+
+
 def main() -> None:
     if not po.have_ref():
         sys.exit("oracle/_ref/libref.so is missing: run `make -C oracle ref` where the reference tree exists")
@@ -188,6 +234,8 @@ def main() -> None:
     np.savez_compressed(os.path.join(OUT, "walks.npz"), **w)
     c0 = config0(start)
     np.savez_compressed(os.path.join(OUT, "config0.npz"), **c0)
+    with open(os.path.join(OUT, "svg_digests.json"), "w") as f:
+        json.dump(svg_digests(start, w), f, indent=1)
     if os.path.isdir(os.path.join(REF, "Examples")):
         with open(os.path.join(OUT, "example_outputs.json"), "w") as f:
             json.dump(example_outputs(), f, indent=1, sort_keys=True)

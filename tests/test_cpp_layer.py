@@ -36,8 +36,11 @@ def _read(path) -> dict:
 def test_cpp_layer_builders(tmp_path):
     exe = _build(tmp_path)
     out = str(tmp_path / "b.txt")
-    subprocess.run([exe, "builders", out], check=True)
+    svg = str(tmp_path / "t.svg")
+    subprocess.run([exe, "builders", out, svg], check=True)
     got, b = _read(out), golden("builders")
+    assert np.array_equal(got["cone"], b["tridimer/cone10_3/tiling"])
+    assert os.path.getsize(svg) > 1000
     assert np.array_equal(got["lozenge_max"], b["lozenge/hex10_2/max"])
     assert np.array_equal(got["lozenge_hmax"], b["lozenge/hex10_2/hmax"])
     d = b["domino/aztec13/domain"]
@@ -51,5 +54,6 @@ def test_cpp_layer_walks(tmp_path):
     subprocess.run([exe, "walk", out], check=True)
     got, b = _read(out), golden("builders")
     assert np.array_equal(got["lozenge_walk"], po.lozenge_walk(b["lozenge/hex10_2/max"], 1000, 42))
+    assert np.array_equal(got["cone_walk"], po.tridimer_walk(b["tridimer/cone10_3/tiling"], 800, 9))
     assert np.array_equal(got["aztec_epochs"],
                           po.domino_walk_epochs(got["aztec_min"], [256, 128], [2718281, 345903], cftp=True))
