@@ -81,6 +81,18 @@ public:
         detail::check(rt_walk(h_, reinterpret_cast<int32_t*>(t.data()), detail::side(t), steps, seed), h_);
     }
     rt_tiler* handle() { return h_; }
+    // Coupling from the past (Examples/AztecDiamondCftpEx.cpp:42-68) on a
+    // monotone kernel; returns the coalesced tiling, stats in *st.
+    tiling CFTP(const tiling& tmax, const tiling& tmin, long first_steps, long master_seed,
+                int32_t schedule = RT_CFTP_DOUBLING, int max_trials = 30, rt_cftp_stats* st = nullptr) {
+        if (tmax.size() != tmin.size()) throw Error(RT_E_INVAL, "tmax and tmin differ in size");
+        tiling out(tmax.size());
+        rt_cftp_stats local{};
+        detail::check(rt_cftp(h_, detail::p(tmax), detail::p(tmin), detail::side(tmax), first_steps, schedule,
+                              master_seed, max_trials, reinterpret_cast<int32_t*>(out.data()), st ? st : &local),
+                      h_);
+        return out;
+    }
     // src/common/common.h:50-69
     static void SaveMatrix(const std::vector<int>& a, const std::string& f) {
         detail::check(rt_save_matrix(detail::p(a), a.size(), f.c_str()), nullptr);

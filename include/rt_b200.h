@@ -99,8 +99,11 @@ rt_status rt_walk(rt_tiler* h, int32_t* tiling, int32_t n, int64_t steps, int64_
 rt_status rt_walk_epochs(rt_tiler* h, int32_t* tiling, int32_t n, const int64_t* steps, const int64_t* seeds,
                          int32_t k);
 
-/* Coupling from the past on the domino heat-bath chain (handle created with
- * RT_KERNEL_CFTP).  Replaces the driver of Examples/AztecDiamondCftpEx.cpp:42-68
+/* Coupling from the past on a monotone chain: the domino heat bath (handle
+ * created with RT_KERNEL_CFTP) or either lozenge kernel (epochs restart the
+ * colour engine and the draws from the epoch seed, as the domino epoch Walk
+ * does); in fast mode (RT_RNG_PHILOX) each epoch seed is that epoch's Philox
+ * key.  Replaces the driver of Examples/AztecDiamondCftpEx.cpp:42-68
  * over DominoTiler::Walk(tiling&, vector<long>, vector<long>)
  * (src/Domino/DominoTiler.cpp:58-107): both chains (from tmax and tmin) run
  * through the same epochs as two coupled lattices of one launch and are

@@ -53,6 +53,14 @@ def oracle() -> ctypes.CDLL:
         lib.orc_minstd_uniform_stream.argtypes = [_I64, _I64, _P, ctypes.c_int, _P]
         lib.orc_domino_colours.argtypes = [_I64, _I64, ctypes.c_int, _P]
         lib.orc_lozenge_colours.argtypes = [_I64, _I64, _P]
+        lib.orc_lozenge_walk_epochs.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, _P, _I64, ctypes.c_int,
+                                                ctypes.c_double, ctypes.c_int]
+        lib.orc_philox4x32_10.argtypes = [_P, _P, _P]
+        lib.orc_domino_walk_fast.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.c_int]
+        lib.orc_lozenge_walk_fast.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.c_int,
+                                              ctypes.c_double, ctypes.c_int]
+        lib.orc_recttri_walk_fast.argtypes = [_P, ctypes.c_int, _I64, _I64, ctypes.c_uint32, _P]
+        lib.orc_tridimer_walk_fast.argtypes = [_P, ctypes.c_int, _I64, _I64, ctypes.c_uint32]
         lib.orc_tinymt_init.argtypes = [_P, ctypes.c_uint32]
         lib.orc_tinymt_bits12.argtypes = [_P]
         lib.orc_tinymt_bits12.restype = ctypes.c_uint32
@@ -122,23 +130,6 @@ def domino_walk_epochs(t, steps, seeds, cftp=True, params=None) -> np.ndarray:
     return a
 
 
-def cftp(tmax, tmin, first_steps: int, master_seed: int, schedule: str = "doubling", max_trials: int = 30):
-    """CFTP composed from the restated epoch walk, following
-    Examples/AztecDiamondCftpEx.cpp:42-68 (seeds: successive mt19937 outputs,
-    newest epoch first).  Returns (tiling, trials, total_steps, coalesced)."""
-    seeds_out = np.zeros(max_trials + 1, dtype=np.uint32)
-    oracle().orc_mt19937_stream(master_seed, max_trials + 1, seeds_out.ctypes.data)
-    steps, seeds = [first_steps], [int(seeds_out[0])]
-    for trial in range(max_trials):
-        top = domino_walk_epochs(tmax, steps, seeds, cftp=True)
-        bot = domino_walk_epochs(tmin, steps, seeds, cftp=True)
-        if np.array_equal(top, bot):
-            return top, trial + 1, sum(steps), True
-        steps.insert(0, 2 * steps[-1] if schedule == "reference" else sum(steps))
-        seeds.insert(0, int(seeds_out[trial + 1]))
-    return top, max_trials, sum(steps), False
-
-
 def lozenge_walk(t, steps, seed, qweight=False, q=0.99, qcmp_double=False, params=None) -> np.ndarray:
     a, n = _tiling(t)
     p, np_, keep = _table(params)
@@ -161,6 +152,86 @@ def tridimer_walk(t, steps, seed, params=None) -> np.ndarray:
     p, np_, keep = _table(params)
     _check(oracle().orc_tridimer_walk(a.ctypes.data, n, steps, seed, p, np_), "orc_tridimer_walk")
     return a
+
+
+def lozenge_walk_epochs(t, steps, seeds, qweight=False, q=0.99, qcmp_double=False, params=None) -> np.ndarray:
+    a, n = _tiling(t)
+    st = np.ascontiguousarray(steps, dtype=np.int64)
+    se = np.ascontiguousarray(seeds, dtype=np.int64)
+    p, np_, keep = _table(params)
+    _check(oracle().orc_lozenge_walk_epochs(a.ctypes.data, n, st.ctypes.data, se.ctypes.data, st.size, p, np_,
+                                            int(qweight), q, int(qcmp_double)), "orc_lozenge_walk_epochs")
+    return a
+
+
+# ---- fast mode (counter-based draws, cyclic colours) ----------------------
+def philox4x32_10(ctr, key) -> list[int]:
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    oracle().orc_philox4x32_10(c.ctypes.data, k.ctypes.data, out.ctypes.data)
+    return [int(x) for x in out]
+
+
+def _epochs(steps, keys):
+    st = np.atleast_1d(np.ascontiguousarray(steps, dtype=np.int64))
+    ke = np.atleast_1d(np.ascontiguousarray(np.asarray(keys, dtype=np.uint64).astype(np.int64), dtype=np.int64))
+    assert st.size == ke.size
+    return st, ke
+
+
+def walk_fast(model: str, t, steps, keys, chain: int = 0, q: float = 0.99, qcmp_double: bool = False,
+              weights=None) -> np.ndarray:
+    """Fast-mode walk of `model` in {"domino", "domino_cftp", "lozenge",
+    "qlozenge", "recttri", "tridimer"}; steps / keys are one value or one
+    per epoch (epochs: dominoes and lozenges)."""
+    a, n = _tiling(t)
+    st, ke = _epochs(steps, keys)
+    lib = oracle()
+    if model in ("domino", "domino_cftp"):
+        rc = lib.orc_domino_walk_fast(a.ctypes.data, n, st.ctypes.data, ke.ctypes.data, st.size, chain,
+                                      int(model == "domino_cftp"))
+    elif model in ("lozenge", "qlozenge"):
+        rc = lib.orc_lozenge_walk_fast(a.ctypes.data, n, st.ctypes.data, ke.ctypes.data, st.size, chain,
+                                       int(model == "qlozenge"), q, int(qcmp_double))
+    elif model == "recttri":
+        assert st.size == 1
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
+        rc = lib.orc_recttri_walk_fast(a.ctypes.data, n, int(st[0]), int(ke[0]), chain,
+                                       None if w is None else w.ctypes.data)
+    elif model == "tridimer":
+        assert st.size == 1
+        rc = lib.orc_tridimer_walk_fast(a.ctypes.data, n, int(st[0]), int(ke[0]), chain)
+    else:
+        raise ValueError(model)
+    _check(rc, f"fast walk of {model}")
+    return a
+
+
+def cftp(tmax, tmin, first_steps: int, master_seed: int, schedule: str = "doubling", max_trials: int = 30,
+         model: str = "domino_cftp", fast: bool = False, **kw):
+    """CFTP composed from the restated epoch walks, following
+    Examples/AztecDiamondCftpEx.cpp:42-68 (seeds: successive mt19937 outputs,
+    newest epoch first; in fast mode each seed is its epoch's Philox key).
+    model: "domino_cftp", "lozenge" or "qlozenge" (kw: q, qcmp_double).
+    Returns (tiling, trials, total_steps, coalesced)."""
+    def run(t, steps, seeds):
+        if fast:
+            return walk_fast(model, t, steps, seeds, **kw)
+        if model == "domino_cftp":
+            return domino_walk_epochs(t, steps, seeds, cftp=True)
+        return lozenge_walk_epochs(t, steps, seeds, qweight=model == "qlozenge", **kw)
+
+    seeds_out = np.zeros(max_trials + 1, dtype=np.uint32)
+    oracle().orc_mt19937_stream(master_seed, max_trials + 1, seeds_out.ctypes.data)
+    steps, seeds = [first_steps], [int(seeds_out[0])]
+    for trial in range(max_trials):
+        top, bot = run(tmax, steps, seeds), run(tmin, steps, seeds)
+        if np.array_equal(top, bot):
+            return top, trial + 1, sum(steps), True
+        steps.insert(0, 2 * steps[-1] if schedule == "reference" else sum(steps))
+        seeds.insert(0, int(seeds_out[trial + 1]))
+    return top, max_trials, sum(steps), False
 
 
 # ---- the reference's own code (oracle/_ref) --------------------------------

@@ -103,6 +103,83 @@ static orc_tinymt* tmt_streams(int64_t count, uint32_t seed, const uint32_t* par
 }
 
 /* ------------------------------------------------------------------------ */
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as  */
+/* easy as 1, 2, 3", SC'11): ten rounds of two 32x32->64 multiplies by      */
+/* 0xD2511F53 / 0xCD9E8D57, key bumped by the Weyl constants 0x9E3779B9 /   */
+/* 0xBB67AE85 between rounds.  The fast mode's counter-based generator; it  */
+/* has no counterpart in the reference.                                     */
+/* ------------------------------------------------------------------------ */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3], k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0, n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        c0 = n0;
+        c1 = (uint32_t)p1;
+        c2 = n2;
+        c3 = (uint32_t)p0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0, out[1] = c1, out[2] = c2, out[3] = c3;
+}
+
+/* Where a Rotate's draws come from.  Bit-exact mode: the reference's TinyMT
+ * stream of work item c + cols * r.  Fast mode: position (r, c) of the Rotate
+ * range belongs to quad u = r * ceil(cols / 4) + c / 4 and takes word c mod 4
+ * of Philox4x32-10(counter = (u, step lo, step hi, chain), key), where `step`
+ * counts the drawing steps of the epoch from 0.  Either way the draw is
+ * k * 2^-23 with a 23-bit k (the top bits of the 32-bit word). */
+typedef struct {
+    int fast;
+    orc_tinymt* tmt;
+    int64_t cols;
+    uint32_t key[2], chain;
+    uint64_t step;
+    int64_t cached_u; /* quad whose words are in w[] (-1: none) */
+    uint32_t w[4];
+} orc_draws;
+
+static float orc_draw(orc_draws* d, int64_t r, int64_t c) {
+    if (!d->fast) return orc_tinymt_single01(&d->tmt[c + d->cols * r]);
+    const int64_t u = r * ((d->cols + 3) / 4) + c / 4;
+    if (u != d->cached_u) {
+        const uint32_t ctr[4] = {(uint32_t)u, (uint32_t)d->step, (uint32_t)(d->step >> 32), d->chain};
+        orc_philox4x32_10(ctr, d->key, d->w);
+        d->cached_u = u;
+    }
+    return (float)(d->w[c & 3] >> 9) * (1.0f / 8388608.0f);
+}
+
+/* Starts an epoch: TinyMT streams seeded with `seed` (bit-exact mode) or the
+ * Philox key `seed` (fast mode). */
+static int draws_begin(orc_draws* d, int fast, int64_t items, int64_t cols, uint64_t seed, uint32_t chain,
+                       const uint32_t* params, int64_t nparams) {
+    int err = ORC_OK;
+    memset(d, 0, sizeof *d);
+    d->fast = fast;
+    d->cols = cols;
+    d->chain = chain;
+    d->cached_u = -1;
+    if (fast) {
+        d->key[0] = (uint32_t)seed;
+        d->key[1] = (uint32_t)(seed >> 32);
+    } else {
+        d->tmt = tmt_streams(items, (uint32_t)seed, params, nparams, &err);
+    }
+    return err;
+}
+/* After every Rotate: the next step's counters. */
+static void draws_next(orc_draws* d) {
+    d->step++;
+    d->cached_u = -1;
+}
+static void draws_end(orc_draws* d) {
+    free(d->tmt);
+    d->tmt = NULL;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Host colour generators.                                                  */
 /* std::mt19937 (DominoTiler.cpp:31,35,81,85): the standard MT19937.        */
 /* std::default_random_engine is libstdc++'s minstd_rand0 (a = 16807,       */
@@ -208,12 +285,11 @@ int orc_lozenge_colours(int64_t seed, int64_t steps, uint8_t* out) {
  * dominokernelCFTP.cl:11-31 (heat bath: rd < .5 -> 12, else -> 3).
  * Work item (g0, g1) of the (N-2) x (N/2-2) range owns site (g0+1, g1+1) and
  * TinyMT stream g1 + (N/2-2) g0 (src/TinyMT/tinymt.clh:24-30). */
-static void domino_rotate(int8_t* a, int n, orc_tinymt* rng, int cftp) {
+static void domino_rotate(int8_t* a, int n, orc_draws* rng, int cftp) {
     const int h = n / 2, gw = h - 2;
     for (int g0 = 0; g0 < n - 2; ++g0)
         for (int g1 = 0; g1 < gw; ++g1) {
-            const int64_t id = (int64_t)g1 + (int64_t)gw * g0;
-            const float rd = orc_tinymt_single01(&rng[id]);
+            const float rd = orc_draw(rng, g0, g1);
             int8_t* v = &a[(g0 + 1) * h + (g1 + 1)];
             if (cftp) {
                 if ((double)rd < 0.5) {
@@ -257,7 +333,7 @@ static void domino_merge(int32_t* t, int n, const int8_t* b, const int8_t* w) {
 }
 
 static int domino_run(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k, int single_walk,
-                      const uint32_t* params, int64_t nparams, int cftp) {
+                      const uint32_t* params, int64_t nparams, int cftp, int fast, uint32_t chain) {
     if (n < 6 || n % 2) return ORC_EINVAL;
     const int h = n / 2;
     const int64_t items = (int64_t)(n - 2) * (h - 2);
@@ -274,20 +350,25 @@ static int domino_run(int32_t* t, int n, const int64_t* steps, const int64_t* se
         mt_state m;
         mt_seed(&m, seeds[e]);
         /* single Walk: TinyMT seed = first mt19937 output (DominoTiler.cpp:31-32);
-         * epoch Walk: TinyMT seed = seeds[k] itself (DominoTiler.cpp:81-82). */
-        const uint32_t tseed = single_walk ? mt_next(&m) : (uint32_t)(uint64_t)seeds[e];
-        orc_tinymt* rng = tmt_streams(items, tseed, params, nparams, &err);
-        if (!rng) break;
+         * epoch Walk: TinyMT seed = seeds[k] itself (DominoTiler.cpp:81-82).
+         * Fast mode: the Philox key is the seed and the colours alternate,
+         * black ((i+j) even) first. */
+        const uint64_t tseed = fast ? (uint64_t)seeds[e] : single_walk ? mt_next(&m) : (uint32_t)(uint64_t)seeds[e];
+        orc_draws rng;
+        err = draws_begin(&rng, fast, items, h - 2, tseed, chain, params, nparams);
+        if (err != ORC_OK) break;
         for (int64_t s = 0; s < steps[e]; ++s) {
-            if (mt_next(&m) % 2u == 1u) {
-                domino_rotate(b, n, rng, cftp);
+            const int black = fast ? (s & 1) == 0 : mt_next(&m) % 2u == 1u;
+            if (black) {
+                domino_rotate(b, n, &rng, cftp);
                 domino_update(w, b, n, 1);
             } else {
-                domino_rotate(w, n, rng, cftp);
+                domino_rotate(w, n, &rng, cftp);
                 domino_update(b, w, n, 0);
             }
+            draws_next(&rng);
         }
-        free(rng);
+        draws_end(&rng);
     }
     if (err == ORC_OK) domino_merge(t, n, b, w);
     free(b);
@@ -297,13 +378,19 @@ static int domino_run(int32_t* t, int n, const int64_t* steps, const int64_t* se
 
 int orc_domino_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
                     int cftp_kernel) {
-    return domino_run(t, n, &steps, &seed, 1, 1, params, nparams, cftp_kernel);
+    return domino_run(t, n, &steps, &seed, 1, 1, params, nparams, cftp_kernel, 0, 0);
 }
 
 int orc_domino_walk_epochs(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k,
                            const uint32_t* params, int64_t nparams, int cftp_kernel) {
     if (k < 0) return ORC_EINVAL;
-    return domino_run(t, n, steps, seeds, k, 0, params, nparams, cftp_kernel);
+    return domino_run(t, n, steps, seeds, k, 0, params, nparams, cftp_kernel, 0, 0);
+}
+
+int orc_domino_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
+                         int cftp_kernel) {
+    if (k < 0) return ORC_EINVAL;
+    return domino_run(t, n, steps, keys, k, 0, NULL, 0, cftp_kernel, 1, chain);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -316,13 +403,13 @@ int orc_domino_walk_epochs(int32_t* t, int n, const int64_t* steps, const int64_
 
 /* RotateTiles, lozengekernel.cl:3-34 (uniform) and qlozengekernel.cl:5-32
  * (q-weighted).  Work item (i, j) owns stream j + (N/3) i. */
-static void lozenge_rotate(void* arr, int isint, int n, orc_tinymt* rng, int qmode, double q, int qcmp) {
+static void lozenge_rotate(void* arr, int isint, int n, orc_draws* rng, int qmode, double q, int qcmp) {
     const int m = n / 3;
     const float qf = (float)q;
     const float qinvf = 1.0f / qf;
     for (int i = 0; i < n; ++i)
         for (int j = 0; j < m; ++j) {
-            const float rd = orc_tinymt_single01(&rng[(int64_t)j + (int64_t)m * i]);
+            const float rd = orc_draw(rng, i, j);
             const int64_t at = (int64_t)i * m + j;
             const int v = isint ? ((int32_t*)arr)[at] : ((int8_t*)arr)[at];
             int nv = v;
@@ -379,9 +466,12 @@ static void lozenge_update(const void* fv, void* av, void* bv, int isint, int n,
 #undef LZ
 }
 
-int orc_lozenge_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
-                     int qmode, double q, int qcmp) {
-    if (n < 3 || n % 3) return ORC_EINVAL;
+/* Epochs as the domino epoch Walk composes them (DominoTiler.cpp:58-107):
+ * epoch e restarts the colour engine and the draws from seeds[e].  The
+ * reference's single Walk (LozengeTiler.cpp:18-88) is the one-epoch case. */
+static int lozenge_run(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k, const uint32_t* params,
+                       int64_t nparams, int qmode, double q, int qcmp, int fast, uint32_t chain) {
+    if (n < 3 || n % 3 || k < 0) return ORC_EINVAL;
     const int m = n / 3;
     const int isint = qmode != 0; /* lozengekernel.cl stores char, qlozengekernel.cl int */
     const size_t es = isint ? 4 : 1;
@@ -400,26 +490,46 @@ int orc_lozenge_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint3
             else
                 ((int8_t*)arr[c])[at] = (int8_t)t[(int64_t)i * n + j];
         }
-    int err;
-    orc_tinymt* rng = tmt_streams((int64_t)n * m, (uint32_t)(uint64_t)seed, params, nparams, &err);
-    if (rng) {
+    int err = ORC_OK;
+    for (int e = 0; e < k && err == ORC_OK; ++e) {
+        orc_draws rng;
+        err = draws_begin(&rng, fast, (int64_t)n * m, m, fast ? (uint64_t)seeds[e] : (uint32_t)(uint64_t)seeds[e],
+                          chain, params, nparams);
+        if (err != ORC_OK) break;
         minstd g;
-        minstd_seed(&g, seed);
-        for (int64_t s = 0; s < steps; ++s) {
-            const int r = uniform_int(&g, 2);
-            lozenge_rotate(arr[r], isint, n, rng, qmode, q, qcmp);
+        minstd_seed(&g, seeds[e]);
+        for (int64_t s = 0; s < steps[e]; ++s) {
+            const int r = fast ? (int)(s % 3) : uniform_int(&g, 2);
+            lozenge_rotate(arr[r], isint, n, &rng, qmode, q, qcmp);
             lozenge_update(arr[r], arr[(r + 1) % 3], arr[(r + 2) % 3], isint, n, r);
+            draws_next(&rng);
         }
-        free(rng);
+        draws_end(&rng);
+    }
+    if (err == ORC_OK)
         for (int i = 0; i < n; ++i)
             for (int j = 0; j < n; ++j) {
                 const int c = ((j - i) % 3 + 3) % 3;
                 const int64_t at = (int64_t)i * m + j / 3;
                 t[(int64_t)i * n + j] = isint ? ((int32_t*)arr[c])[at] : ((int8_t*)arr[c])[at];
             }
-    }
     for (int c = 0; c < 3; ++c) free(arr[c]);
     return err;
+}
+
+int orc_lozenge_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
+                     int qmode, double q, int qcmp) {
+    return lozenge_run(t, n, &steps, &seed, 1, params, nparams, qmode, q, qcmp, 0, 0);
+}
+
+int orc_lozenge_walk_epochs(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k,
+                            const uint32_t* params, int64_t nparams, int qmode, double q, int qcmp) {
+    return lozenge_run(t, n, steps, seeds, k, params, nparams, qmode, q, qcmp, 0, 0);
+}
+
+int orc_lozenge_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
+                          int qmode, double q, int qcmp) {
+    return lozenge_run(t, n, steps, keys, k, NULL, 0, qmode, q, qcmp, 1, chain);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -465,11 +575,11 @@ static int32_t rt_propose(int32_t v, float rd, const float* w) {
     return ratio >= x ? nv : v;
 }
 
-static void rt_flip(int32_t* a, int n, orc_tinymt* rng, const float* w) {
+static void rt_flip(int32_t* a, int n, orc_draws* rng, const float* w) {
     const int m = n / 3;
     for (int i = 0; i < n; ++i)
         for (int j = 0; j < m; ++j) {
-            const float rd = orc_tinymt_single01(&rng[(int64_t)j + (int64_t)m * i]);
+            const float rd = orc_draw(rng, i, j);
             int32_t* v = &a[(int64_t)i * m + j];
             *v = rt_propose(*v, rd, w);
         }
@@ -498,8 +608,8 @@ static void rt_update(const int32_t* f, int32_t* a, int32_t* b, int n, int t) {
 #undef PUT
 }
 
-int orc_recttri_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
-                     const float* weights) {
+static int recttri_run(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
+                       const float* weights, int fast, uint32_t chain) {
     if (n < 3 || n % 3) return ORC_EINVAL;
     const float* w = weights ? weights : kRtDefaultWeights;
     const int m = n / 3;
@@ -511,22 +621,33 @@ int orc_recttri_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint3
     }
     for (int i = 0; i < n; ++i)
         for (int j = 0; j < n; ++j) arr[((i - j) % 3 + 3) % 3][(int64_t)i * m + j / 3] = t[(int64_t)i * n + j];
-    int err;
-    orc_tinymt* rng = tmt_streams((int64_t)n * m, (uint32_t)(uint64_t)seed, params, nparams, &err);
-    if (rng) {
+    orc_draws rng;
+    int err = draws_begin(&rng, fast, (int64_t)n * m, m, fast ? (uint64_t)seed : (uint32_t)(uint64_t)seed, chain,
+                          params, nparams);
+    if (err == ORC_OK) {
         minstd g;
         minstd_seed(&g, seed);
         for (int64_t s = 0; s < steps; ++s) {
-            const int r = uniform_int(&g, 2);
-            rt_flip(arr[r], n, rng, w);
+            const int r = fast ? (int)(s % 3) : uniform_int(&g, 2);
+            rt_flip(arr[r], n, &rng, w);
             rt_update(arr[r], arr[(r + 1) % 3], arr[(r + 2) % 3], n, r);
+            draws_next(&rng);
         }
-        free(rng);
+        draws_end(&rng);
         for (int i = 0; i < n; ++i)
             for (int j = 0; j < n; ++j) t[(int64_t)i * n + j] = arr[((i - j) % 3 + 3) % 3][(int64_t)i * m + j / 3];
     }
     for (int c = 0; c < 3; ++c) free(arr[c]);
     return err;
+}
+
+int orc_recttri_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
+                     const float* weights) {
+    return recttri_run(t, n, steps, seed, params, nparams, weights, 0, 0);
+}
+
+int orc_recttri_walk_fast(int32_t* t, int n, int64_t steps, int64_t key, uint32_t chain, const float* weights) {
+    return recttri_run(t, n, steps, key, NULL, 0, weights, 1, chain);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -553,11 +674,11 @@ static int32_t bf_pack(int t1, int t4, int t16, int t64, int c) { return t1 + 4 
 
 /* RotateLozenges (triangledimerkernel.cl:4-22): every item draws; sites of
  * orientation t and checkerboard class c toggle 5 <-> 10 when rd < .5. */
-static void td_rotate_lozenges(td_state* st, int32_t* A, int t, int c, orc_tinymt* rng) {
+static void td_rotate_lozenges(td_state* st, int32_t* A, int t, int c, orc_draws* rng) {
     const int m = st->m;
     for (int i = 0; i < m; ++i)
         for (int j = 0; j < m; ++j) {
-            const float rd = orc_tinymt_single01(&rng[(int64_t)j + (int64_t)m * i]);
+            const float rd = orc_draw(rng, i, j);
             const int cls = ((1 - (t & 1)) * i + ((1 + t) / 2) * j) % 2;
             if ((double)rd < 0.5 && cls == c) {
                 int32_t* v = &TD(A, i, j);
@@ -650,11 +771,11 @@ static void td_butterfly_from_lozenges(td_state* st, int which) {
 }
 
 /* RotateTriangles (:191-211): class ((j-i) mod 3) == c toggles 45 <-> 54. */
-static void td_rotate_triangles(td_state* st, int32_t* A, int c, orc_tinymt* rng) {
+static void td_rotate_triangles(td_state* st, int32_t* A, int c, orc_draws* rng) {
     const int m = st->m;
     for (int i = 0; i < m; ++i)
         for (int j = 0; j < m; ++j) {
-            const float rd = orc_tinymt_single01(&rng[(int64_t)j + (int64_t)m * i]);
+            const float rd = orc_draw(rng, i, j);
             if ((double)rd < 0.5 && ((j - i) % 3 + 3) % 3 == c) {
                 int32_t* v = &TD(A, i, j);
                 if (*v == 45) *v = 54;
@@ -708,12 +829,12 @@ static void td_lozenges_from_triangles(td_state* st) {
 
 /* RotateButterflys (:331-353): slice (b1 i + b2 j) mod 3 == p1; within it the
  * sites of parity p2 toggle 170 <-> 85 when rd < .5. */
-static void td_rotate_butterflies(td_state* st, int32_t* A, int t, int p1, int p2, orc_tinymt* rng) {
+static void td_rotate_butterflies(td_state* st, int32_t* A, int t, int p1, int p2, orc_draws* rng) {
     const int m = st->m;
     const int b1 = 1 - (t & 1), b2 = (1 + t) / 2, b3 = t & 1;
     for (int i = 0; i < m; ++i)
         for (int j = 0; j < m; ++j) {
-            const float rd = orc_tinymt_single01(&rng[(int64_t)j + (int64_t)m * i]);
+            const float rd = orc_draw(rng, i, j);
             if ((double)rd < 0.5 && (b1 * i + b2 * j) % 3 == p1 && ((b1 * j + b3 * i) & 1) == p2) {
                 int32_t* v = &TD(A, i, j);
                 if (*v == 170) *v = 85;
@@ -913,7 +1034,8 @@ static void td_derive(const int32_t* t, int n, int32_t* tri, int32_t* bfl) {
 #undef T
 }
 
-int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams) {
+static int tridimer_run(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
+                        int fast, uint32_t chain) {
     if (n < 8 || n % 2) return ORC_EINVAL;
     const int m = n / 2;
     const size_t mm = (size_t)m * m;
@@ -943,15 +1065,32 @@ int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint
         }
     for (int i = 0; i < n / 2; ++i)
         for (int j = 0; j < n; ++j) (j % 2 == 0 ? S.D : S.U)[(int64_t)i * m + j / 2] = tri[(int64_t)i * n + j];
-    int err;
-    orc_tinymt* rng = tmt_streams((int64_t)mm, (uint32_t)(uint64_t)seed, params, nparams, &err);
-    if (rng) {
+    orc_draws draws, *rng = &draws;
+    int err = draws_begin(rng, fast, (int64_t)mm, m, fast ? (uint64_t)seed : (uint32_t)(uint64_t)seed, chain, params,
+                          nparams);
+    if (err == ORC_OK) {
         minstd g;
         minstd_seed(&g, seed);
         int32_t* lz[3] = {S.H, S.L, S.R};
         int32_t* bf[3] = {S.BH, S.BL, S.BR};
         for (int64_t s = 0; s < steps; ++s) {
-            const int kind = uniform_int(&g, 2), r1 = uniform_int(&g, 2), r2 = uniform_int(&g, 1);
+            /* Fast mode: step s makes move s mod 30 of a fixed sweep over every
+             * flip class -- lozenges (orientation r1, class r2), triangles
+             * (kind r2, class r1), butterflies (orientation r1, slice p1,
+             * parity p2) -- instead of drawing the move. */
+            int kind, r1, r2, p1 = 0, p2 = 0;
+            if (fast) {
+                const int mv = (int)(s % 30);
+                if (mv < 6) {
+                    kind = 0, r1 = mv / 2, r2 = mv % 2;
+                } else if (mv < 12) {
+                    kind = 1, r2 = (mv - 6) / 3, r1 = (mv - 6) % 3;
+                } else {
+                    kind = 2, r1 = (mv - 12) / 6, p1 = ((mv - 12) / 2) % 3, p2 = (mv - 12) % 2;
+                }
+            } else {
+                kind = uniform_int(&g, 2), r1 = uniform_int(&g, 2), r2 = uniform_int(&g, 1);
+            }
             if (kind == 0) { /* lozenge flips, TriangleDimerTiler.cpp:243-278 */
                 td_rotate_lozenges(st, lz[r1], r1, r2, rng);
                 td_lozenges_flipped(st, lz[r1], r1, r2);
@@ -970,7 +1109,7 @@ int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint
                 td_lozenges_from_triangles(st);
                 for (int w = 0; w < 3; ++w) td_butterfly_from_lozenges(st, w);
             } else { /* butterfly flips, :306-347 */
-                const int p1 = uniform_int(&g, 2), p2 = uniform_int(&g, 1);
+                if (!fast) p1 = uniform_int(&g, 2), p2 = uniform_int(&g, 1);
                 td_rotate_butterflies(st, bf[r1], r1, p1, p2, rng);
                 td_butterfly_same_slice(st, bf[r1], r1, p1, p2);
                 td_butterfly_pass21(st, bf[r1], r1, p1);
@@ -982,8 +1121,9 @@ int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint
                 td_up_from_lozenges(st);
                 td_triangles_other(st, S.U, S.D, 0);
             }
+            draws_next(rng);
         }
-        free(rng);
+        draws_end(rng);
         /* Only the lozenge states go back into the tiling (:362-376). */
         for (int i = 0; i < n; ++i)
             for (int j = 0; j < n; ++j) {
@@ -999,4 +1139,12 @@ int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint
     free(tri);
     free(bfl);
     return err;
+}
+
+int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams) {
+    return tridimer_run(t, n, steps, seed, params, nparams, 0, 0);
+}
+
+int orc_tridimer_walk_fast(int32_t* t, int n, int64_t steps, int64_t key, uint32_t chain) {
+    return tridimer_run(t, n, steps, key, NULL, 0, 1, chain);
 }

@@ -65,6 +65,24 @@ int orc_recttri_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint3
                      const float* weights);
 int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams);
 
+/* Epoch walks of the lozenge models (each epoch restarts the colour engine
+ * and the TinyMT streams from seeds[e], as the domino epoch Walk does). */
+int orc_lozenge_walk_epochs(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k,
+                            const uint32_t* params, int64_t nparams, int qmode, double q, int qcmp);
+
+/* ---- fast mode (no reference counterpart) ----
+ * Counter-based draws: Philox4x32-10 keyed by the epoch key, counter =
+ * (position quad, step within the epoch, 0, chain); colours in a fixed
+ * cycle (dominoes: black, white; three-colour models: 0, 1, 2; triangle
+ * dimers: a 30-move sweep over every flip class). */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+int orc_domino_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
+                         int cftp_kernel);
+int orc_lozenge_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
+                          int qmode, double q, int qcmp);
+int orc_recttri_walk_fast(int32_t* t, int n, int64_t steps, int64_t key, uint32_t chain, const float* weights);
+int orc_tridimer_walk_fast(int32_t* t, int n, int64_t steps, int64_t key, uint32_t chain);
+
 /* Colour schedules the host loops draw (one entry per step). */
 int orc_domino_colours(int64_t seed, int64_t steps, int single_walk, uint8_t* out);
 int orc_lozenge_colours(int64_t seed, int64_t steps, uint8_t* out);

@@ -178,8 +178,8 @@ rt_status rt_create(const rt_config* cfg, rt_tiler** out) {
         g_create_error = "unsupported model/kernel combination";
         return RT_E_INVAL;
     }
-    if (cfg->rng != RT_RNG_TINYMT) {
-        g_create_error = "rng mode not available for this model";
+    if (cfg->rng != RT_RNG_TINYMT && cfg->rng != RT_RNG_PHILOX) {
+        g_create_error = "unknown rng mode";
         return RT_E_INVAL;
     }
     if (family == FAM_QLOZENGE32 && (!(cfg->q >= 0.0) || !std::isfinite(cfg->q))) {
@@ -404,10 +404,47 @@ static rt_status stage_params(rt_tiler* h, int64_t needed) {
     return RT_OK;
 }
 
+// Phases of one triangle-dimer step (TriangleDimerTiler.cpp:243-347): the
+// flip family `kind` (0 lozenges, 1 triangles, 2 butterflies), orientation /
+// class r1, kind or parity r2, and for butterflies the slice p1 and parity p2.
+static int64_t td_step_phases(uint32_t* ph, int64_t at, uint32_t kind, uint32_t r1, uint32_t r2, uint32_t p1,
+                              uint32_t p2) {
+    if (kind == 0) {  // lozenge flips, :243-278
+        ph[at++] = make_phase(TD_ROT_LOZ, r1, r2, true);
+        ph[at++] = make_phase(TD_LOZ_FLIPPED, r1, r2, false);
+        ph[at++] = make_phase(TD_LOZ_OTHER, r1, 0, false);
+        ph[at++] = make_phase(TD_UP_FROM_LOZ, 0, 0, false);
+        ph[at++] = make_phase(TD_TRI_OTHER, 0, 7, false);
+    } else if (kind == 1) {  // triangle flips, :279-305
+        ph[at++] = make_phase(TD_ROT_TRI, r2, r1, true);
+        ph[at++] = make_phase(TD_TRI_FLIPPED, r2, r1, false);
+        ph[at++] = make_phase(TD_TRI_OTHER, r2, 0, false);
+        ph[at++] = make_phase(TD_LOZ_FROM_TRI, 0, 0, false);
+        ph[at++] = make_phase(TD_BFLY_FROM_LOZ, 0, 7, false);
+    } else {  // butterfly flips, :306-347
+        ph[at++] = make_phase(TD_ROT_BFLY, r1, p1 | (p2 << 2), true);
+        ph[at++] = make_phase(TD_BFLY_SAME, r1, p1 | (p2 << 2), false);
+        ph[at++] = make_phase(TD_BFLY_21, r1, p1, false);
+        ph[at++] = make_phase(TD_BFLY_22, r1, p1, false);
+        ph[at++] = make_phase(TD_BFLY_23_LOZ, r1, p1, false);
+        ph[at++] = make_phase(TD_BFLY_FROM_LOZ, 1, 7u & ~(1u << r1), false);
+        ph[at++] = make_phase(TD_TRI_OTHER, 0, 0, false);
+    }
+    return at;
+}
+
 // Builds the phase list of `k` epochs and launches the walk.
+//
+// Bit-exact mode draws the colours as the reference's host loops do.  Fast
+// mode (RT_RNG_PHILOX) has no host generator: step s of an epoch flips
+// colour s mod NCOL in a fixed cycle (dominoes: the black array, then the
+// white; lozenges and rectangle-triangles: 0, 1, 2; triangle dimers: move
+// s mod 30 of a sweep over every flip class), and each epoch's seed is its
+// 64-bit Philox key.
 static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* seeds, int k, bool single_walk) {
     if (!h->uploaded) return h->fail(RT_E_STATE, "run before upload");
     cudaSetDevice(h->cfg.device);
+    const bool fast = h->cfg.rng == RT_RNG_PHILOX;
     int64_t total = 0;
     for (int e = 0; e < k; ++e) {
         if (steps[e] < 0) return h->fail(RT_E_INVAL, "negative step count");
@@ -423,16 +460,34 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     cudaEventSynchronize(h->ev_staged);
     if (!h->h_phases.reserve((size_t)cap_ph * 4) || !h->d_phases.reserve((size_t)cap_ph * 4) ||
         !h->h_epoch_start.reserve((size_t)k * 8) || !h->d_epoch_start.reserve((size_t)k * 8) ||
-        !h->h_epoch_seed.reserve((size_t)k * 4) || !h->d_epoch_seed.reserve((size_t)k * 4))
+        !h->h_epoch_seed.reserve((size_t)k * 8) || !h->d_epoch_seed.reserve((size_t)k * 8))
         return h->fail(RT_E_NOMEM, "schedule buffers");
     uint32_t* ph = static_cast<uint32_t*>(h->h_phases.p);
     int64_t* es = static_cast<int64_t*>(h->h_epoch_start.p);
-    uint32_t* sd = static_cast<uint32_t*>(h->h_epoch_seed.p);
+    uint64_t* sd = static_cast<uint64_t*>(h->h_epoch_seed.p);
     int64_t at = 0;
     uint32_t prev = NO_COLOUR;
     for (int e = 0; e < k; ++e) {
         es[e] = at;
-        if (h->kind == 0) {
+        if (fast) {
+            sd[e] = (uint64_t)seeds[e];
+            for (int64_t s = 0; s < steps[e]; ++s) {
+                if (h->kind == 3) {
+                    const uint32_t mv = (uint32_t)(s % 30);
+                    if (mv < 6)
+                        at = td_step_phases(ph, at, 0, mv / 2, mv % 2, 0, 0);
+                    else if (mv < 12)
+                        at = td_step_phases(ph, at, 1, (mv - 6) % 3, (mv - 6) / 3, 0, 0);
+                    else
+                        at = td_step_phases(ph, at, 2, (mv - 12) / 6, 0, ((mv - 12) / 2) % 3, (mv - 12) % 2);
+                } else {
+                    // Domino colour r flips array 1 - r: black (array 0) on even steps.
+                    const uint32_t r = h->kind == 0 ? (uint32_t)(1 - (s & 1)) : (uint32_t)(s % 3);
+                    ph[at++] = make_phase(OP_STEP, r, prev, true);
+                    prev = r;
+                }
+            }
+        } else if (h->kind == 0) {
             std::mt19937 mt_rand(seeds[e]);
             sd[e] = single_walk ? (uint32_t)mt_rand() : (uint32_t)seeds[e];  // DominoTiler.cpp:31-32 vs :81-82
             for (int64_t s = 0; s < steps[e]; ++s) {
@@ -451,28 +506,12 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
             for (int64_t s = 0; s < steps[e]; ++s) {
                 const uint32_t kind = (uint32_t)d1(generator), r1 = (uint32_t)d1(generator),
                                r2 = (uint32_t)d2(generator);
-                if (kind == 0) {  // lozenge flips, :243-278
-                    ph[at++] = make_phase(TD_ROT_LOZ, r1, r2, true);
-                    ph[at++] = make_phase(TD_LOZ_FLIPPED, r1, r2, false);
-                    ph[at++] = make_phase(TD_LOZ_OTHER, r1, 0, false);
-                    ph[at++] = make_phase(TD_UP_FROM_LOZ, 0, 0, false);
-                    ph[at++] = make_phase(TD_TRI_OTHER, 0, 7, false);
-                } else if (kind == 1) {  // triangle flips, :279-305
-                    ph[at++] = make_phase(TD_ROT_TRI, r2, r1, true);
-                    ph[at++] = make_phase(TD_TRI_FLIPPED, r2, r1, false);
-                    ph[at++] = make_phase(TD_TRI_OTHER, r2, 0, false);
-                    ph[at++] = make_phase(TD_LOZ_FROM_TRI, 0, 0, false);
-                    ph[at++] = make_phase(TD_BFLY_FROM_LOZ, 0, 7, false);
-                } else {  // butterfly flips, :306-347
-                    const uint32_t p1 = (uint32_t)d1(generator), p2 = (uint32_t)d2(generator);
-                    ph[at++] = make_phase(TD_ROT_BFLY, r1, p1 | (p2 << 2), true);
-                    ph[at++] = make_phase(TD_BFLY_SAME, r1, p1 | (p2 << 2), false);
-                    ph[at++] = make_phase(TD_BFLY_21, r1, p1, false);
-                    ph[at++] = make_phase(TD_BFLY_22, r1, p1, false);
-                    ph[at++] = make_phase(TD_BFLY_23_LOZ, r1, p1, false);
-                    ph[at++] = make_phase(TD_BFLY_FROM_LOZ, 1, 7u & ~(1u << r1), false);
-                    ph[at++] = make_phase(TD_TRI_OTHER, 0, 0, false);
+                uint32_t p1 = 0, p2 = 0;
+                if (kind == 2) {
+                    p1 = (uint32_t)d1(generator);
+                    p2 = (uint32_t)d2(generator);
                 }
+                at = td_step_phases(ph, at, kind, r1, r2, p1, p2);
             }
         } else {
             std::default_random_engine generator;
@@ -490,10 +529,10 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     const int64_t nph = at;
 
     const int width = h->width;
-    const bool uniform = h->table.empty();
+    const bool uniform = fast || h->table.empty();
     if (h->plan_rows != h->rows || h->plan_cols != h->cols || h->plan_nlat != h->nlat || h->plan_uniform != uniform) {
-        rt_status s =
-            plan_walk(h->family, h->cfg.device, h->nlat, h->rows, h->cols, width, uniform, &h->plan, &h->err);
+        rt_status s = plan_walk(h->family, h->cfg.device, h->nlat, h->rows, h->cols, width, uniform, fast, &h->plan,
+                                &h->err);
         if (s != RT_OK) return s;
         h->plan_rows = h->rows;
         h->plan_cols = h->cols;
@@ -501,7 +540,7 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
         h->plan_uniform = uniform;
     }
     const int64_t ids = (int64_t)h->rows * h->cols;
-    rt_status s = stage_params(h, ids);
+    rt_status s = fast ? RT_OK : stage_params(h, ids);
     if (s != RT_OK) return s;
     const size_t xbytes =
         (size_t)h->plan.ctas * 2 * 2 * h->nlat * h->plan.xslots * h->plan.xwords * sizeof(unsigned long long);
@@ -510,7 +549,7 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     cudaError_t e;
     if ((e = cudaMemcpyAsync(h->d_phases.p, ph, (size_t)nph * 4, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
         (e = cudaMemcpyAsync(h->d_epoch_start.p, es, (size_t)k * 8, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(h->d_epoch_seed.p, sd, (size_t)k * 4, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h->d_epoch_seed.p, sd, (size_t)k * 8, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
         (e = cudaEventRecord(h->ev_staged, h->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->d_xbuf.p, 0, xbytes, h->stream)) != cudaSuccess)
         return h->cuda_fail(e, "schedule staging");
@@ -525,15 +564,16 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     a.cols = h->cols;
     a.arows = h->arows;
     a.width = width;
-    a.rng_kind = 0;
-    a.params = h->table.empty() ? nullptr : static_cast<const uint4*>(h->d_params.p);
+    a.rng_kind = fast ? 1 : 0;
+    a.chain = 0;
+    a.params = uniform ? nullptr : static_cast<const uint4*>(h->d_params.p);
     a.mat1 = kMat1;
     a.mat2 = kMat2;
     a.tmat = kTmat;
     a.phases = static_cast<const uint32_t*>(h->d_phases.p);
     a.nphases = nph;
     a.epoch_start = static_cast<const int64_t*>(h->d_epoch_start.p);
-    a.epoch_seed = static_cast<const uint32_t*>(h->d_epoch_seed.p);
+    a.epoch_seed = static_cast<const uint64_t*>(h->d_epoch_seed.p);
     a.nepochs = k;
     switch (h->family) {
         case FAM_DOMINO: a.thr[0] = below_threshold(0.8); break;       // dominokernel.cl:13
@@ -598,20 +638,27 @@ rt_status rt_last_run_info(rt_tiler* h, int64_t* phases, int64_t* launches) {
     return RT_OK;
 }
 
-// Coupling from the past on the domino heat-bath chain: the reference's
-// Examples/AztecDiamondCftpEx.cpp:42-68 built on DominoTiler::Walk(tiling&,
-// vector<long>, vector<long>) (DominoTiler.cpp:58-107).  Each trial runs the
-// chains from the maximal and the minimal tiling through the same epochs
-// (same seeds, so the same draws) -- here as two coupled lattices of one
-// launch -- and compares them on the device.  Epoch seeds are successive
-// outputs of std::mt19937(master_seed), the newest epoch first, exactly as
-// the example draws them.
+// Coupling from the past: the reference's Examples/AztecDiamondCftpEx.cpp:42-68
+// built on DominoTiler::Walk(tiling&, vector<long>, vector<long>)
+// (DominoTiler.cpp:58-107).  Each trial runs the chains from the maximal and
+// the minimal tiling through the same epochs (same seeds, so the same draws)
+// -- here as two coupled lattices of one launch -- and compares them on the
+// device.  Epoch seeds are successive outputs of std::mt19937(master_seed),
+// the newest epoch first, exactly as the example draws them.  Any kernel whose
+// update is monotone under shared draws qualifies: the domino heat bath
+// (dominokernelCFTP.cl) and both lozenge kernels (a draw either raises the
+// site, lowers it, or leaves it, whatever its state; lozengekernel.cl:19-31,
+// qlozengekernel.cl:18-29).  Lozenge epochs restart the colour engine and the
+// draws from the epoch seed as the domino epoch Walk does.  In fast mode the
+// epoch seeds are the epochs' Philox keys.
 rt_status rt_cftp(rt_tiler* h, const int32_t* tmax, const int32_t* tmin, int32_t n, int64_t first_steps,
                   int32_t schedule, int64_t master_seed, int32_t max_trials, int32_t* out_tiling,
                   rt_cftp_stats* stats) {
     if (!h) return RT_E_INVAL;
-    if (h->family != FAM_DOMINO_HB)
-        return h->fail(RT_E_INVAL, "CFTP needs the monotone heat-bath kernel (RT_KERNEL_CFTP, dominokernelCFTP.cl)");
+    if (h->family != FAM_DOMINO_HB && h->family != FAM_LOZENGE8 && h->family != FAM_QLOZENGE32)
+        return h->fail(RT_E_INVAL,
+                       "CFTP needs a monotone kernel: the domino heat bath (RT_KERNEL_CFTP, dominokernelCFTP.cl) "
+                       "or a lozenge kernel");
     if (!tmax || !tmin || first_steps <= 0 || max_trials <= 0 ||
         (schedule != RT_CFTP_DOUBLING && schedule != RT_CFTP_REFERENCE))
         return h->fail(RT_E_INVAL, "bad CFTP arguments");

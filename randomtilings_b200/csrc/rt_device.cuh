@@ -116,8 +116,9 @@ __host__ __device__ inline void philox_round(uint32_t& c0, uint32_t& c1, uint32_
     c3 = n3;
 }
 
-__host__ __device__ inline uint32_t philox_first(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
-                                                 uint32_t k1) {
+// All four output words of Philox4x32-10 for counter (c0..c3) and key (k0, k1).
+__host__ __device__ inline uint4 philox4(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                         uint32_t k1) {
 #ifdef __CUDA_ARCH__
 #pragma unroll
 #endif
@@ -126,7 +127,17 @@ __host__ __device__ inline uint32_t philox_first(uint32_t c0, uint32_t c1, uint3
         k0 += 0x9E3779B9u;
         k1 += 0xBB67AE85u;
     }
-    return c0;
+    return make_uint4(c0, c1, c2, c3);
+}
+
+// Fast-mode draws.  Positions of one row of the Rotate grid are taken in
+// quads of four consecutive columns; quad u = r * ceil(cols/4) + c/4 of step s
+// (counted within the epoch) of chain `chain` uses word (c mod 4) of
+// Philox4x32-10(counter = (u, s mod 2^32, s / 2^32, chain), key = epoch key),
+// and its top 23 bits are the draw k, so the integer acceptance thresholds of
+// the TinyMT mode apply unchanged.
+__host__ __device__ inline uint32_t quad_word(const uint4& w, int lane) {
+    return lane == 0 ? w.x : lane == 1 ? w.y : lane == 2 ? w.z : w.w;
 }
 
 // ---------------------------------------------------------------------------

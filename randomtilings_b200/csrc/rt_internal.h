@@ -32,8 +32,8 @@ struct WalkPlan {
     const void* fn = nullptr;
 };
 
-rt_status plan_walk(int family, int device, int nlat, int rows, int cols, int width, bool uniform, WalkPlan* plan,
-                    std::string* err);
+rt_status plan_walk(int family, int device, int nlat, int rows, int cols, int width, bool uniform, bool philox,
+                    WalkPlan* plan, std::string* err);
 rt_status launch_walk(const WalkPlan& plan, WalkArgs& args, cudaStream_t stream, std::string* err);
 // kind: 0 domino, 1 lozenge, 2 rect-triangle, 3 triangle-dimer (merge only).
 rt_status launch_split(bool merge, int elem_bytes, int kind, int ncol, int n, int32_t* tiling, void* const* arr,

@@ -33,15 +33,14 @@ struct WalkArgs {
     int xwords;           // exchange words per row
     int xslots;           // exchanged arrays per phase (slots per side)
     int rows_per_cta;
-    int rng_kind;         // 0 TinyMT, 1 Philox
+    int rng_kind;         // 0 TinyMT, 1 Philox (fast mode)
     const uint4* params;  // TinyMT (mat1, mat2, tmat, -) per stream id, or nullptr
     uint32_t mat1, mat2, tmat;
-    uint32_t key0, key1;  // Philox key (fast mode)
     uint32_t chain;       // Philox counter word 3 (fast mode)
     const uint32_t* phases;
     int64_t nphases;
-    const int64_t* epoch_start;  // first phase of each TinyMT epoch
-    const uint32_t* epoch_seed;  // TinyMT seed of each epoch
+    const int64_t* epoch_start;  // first phase of each epoch
+    const uint64_t* epoch_seed;  // per epoch: TinyMT seed (low 32 bits) or Philox key (fast mode)
     int nepochs;
     uint32_t thr[4];      // integer acceptance thresholds on the 23-bit draw
     float weights[16];    // rect-triangle face weights

@@ -140,7 +140,7 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
     }
     std::string perr;  // filled only on a failure path
     WalkPlan plan;
-    s = plan_walk(family, cfg->device, 1, rows, cols, width, true, &plan, &perr);
+    s = plan_walk(family, cfg->device, 1, rows, cols, width, true, false, &plan, &perr);
     if (s != RT_OK) {
         say(errbuf, errcap, "%s", perr.c_str());
         return s;
@@ -177,7 +177,7 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
         int64_t done = 0;
         int fill = 0;
         uint32_t prev = NO_COLOUR;
-        uint32_t tseed;
+        uint64_t tseed;
         std::mt19937 mt(seed);
         std::default_random_engine lcg;
         std::uniform_int_distribution<int> dist(0, 2);
@@ -208,7 +208,7 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
         const int64_t ep_start = 0;
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(base + off_ep, &ep_start, 8, cudaMemcpyHostToDevice, stream);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(base + off_ep + 8, &tseed, 4, cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(base + off_ep + 8, &tseed, 8, cudaMemcpyHostToDevice, stream);
         // The exchange slots and the error word must start at zero on every call.
         if (e == cudaSuccess) e = cudaMemsetAsync(base + off_x, 0, xbytes, stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(base + off_err, 0, sizeof(int), stream);
@@ -243,7 +243,7 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
         a.phases = reinterpret_cast<const uint32_t*>(base + off_ph);
         a.nphases = nph;
         a.epoch_start = reinterpret_cast<const int64_t*>(base + off_ep);
-        a.epoch_seed = reinterpret_cast<const uint32_t*>(base + off_ep + 8);
+        a.epoch_seed = reinterpret_cast<const uint64_t*>(base + off_ep + 8);
         a.nepochs = 1;
         switch (family) {
             case FAM_DOMINO: a.thr[0] = below(0.8); break;

@@ -80,11 +80,12 @@ __device__ __forceinline__ bool wait_word(const WalkArgs& a, const unsigned long
     }
 }
 
-// Shared memory of one CTA: the generator states of its positions (struct of
-// arrays s0[], s1[], s2[], s3[], so consecutive threads hit consecutive banks),
-// then the lattice band(s): for each lattice, NCOL colour planes of
-// (rows + 2 halo rows) x wpad elements.
-template <class Model, int BLOCK, bool UNIFORM>
+// Shared memory of one CTA: in bit-exact mode the generator states of its
+// positions (struct of arrays s0[], s1[], s2[], s3[], so consecutive threads
+// hit consecutive banks; the fast mode keeps no state), then the lattice
+// band(s): for each lattice, NCOL colour planes of (rows + 2 halo rows) x wpad
+// elements.
+template <class Model, int BLOCK, bool UNIFORM, bool PHILOX>
 __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ WalkArgs a) {
     using T = typename Model::Elem;
     constexpr int NC = Model::NCOL;
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
     const int plane = hr * W;
     const int cols = a.cols;
     const int npos = max(0, r1 - r0) * cols;
-    const int spos = a.rows_per_cta * cols;  // state slots (same for every CTA)
+    const int spos = PHILOX ? 0 : a.rows_per_cta * cols;  // state slots (same for every CTA)
 
     uint32_t* s_st = reinterpret_cast<uint32_t*>(smem_raw);
     T* lat = reinterpret_cast<T*>(smem_raw + (size_t)4 * spos * sizeof(uint32_t));
@@ -132,19 +133,30 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
     // positions, spread over all threads); all other positions are updated
     // before the wait, overlapping the neighbours' progress.
     const bool has_top = cta > 0, has_bot = cta + 1 < nct;
+    const bool bot_edge = has_bot && !(has_top && r1 - r0 == 1);  // last row is an edge row of its own
     const int q_lo = has_top ? min(cols, npos) : 0;
     const int q_hi = has_bot ? max(q_lo, npos - cols) : npos;
     const int top_n = has_top ? min(cols, npos) : 0;
-    const int bot_n = (has_bot && !(has_top && r1 - r0 == 1)) ? cols : 0;
+    const int bot_n = bot_edge ? cols : 0;
     const int n_edge = top_n + bot_n;
     // Interior positions of this thread: q = q_lo + tid + m * BLOCK, walked
     // with an incremental (row, column) instead of a division per site.
     const int dr = BLOCK / cols, dc = BLOCK % cols;
     const int q_first = q_lo + tid;
     const int r_first = r0 + q_first / cols, c_first = q_first % cols;
+    // Fast mode walks quads of four consecutive columns instead (one Philox
+    // call per quad): interior rows ri_lo..ri_hi-1, the same edge rows.
+    const int G = (cols + 3) >> 2;
+    const int ri_lo = r0 + (has_top ? 1 : 0);
+    const int ri_hi = max(ri_lo, r1 - (has_bot ? 1 : 0));
+    const int nq_in = (ri_hi - ri_lo) * G;
+    const int nq_edge = ((has_top ? 1 : 0) + (bot_edge ? 1 : 0)) * G;
+    const int dqr = BLOCK / G, dqc = BLOCK % G;
 
     int epoch = -1;
-    int64_t next_epoch = a.rng_kind == 0 && a.nepochs > 0 ? a.epoch_start[0] : INT64_MAX;
+    int64_t next_epoch = a.nepochs > 0 ? a.epoch_start[0] : INT64_MAX;
+    uint32_t key0 = 0, key1 = 0;  // fast mode: Philox key of the epoch
+    int64_t dstep = 0;            // fast mode: drawing steps since the epoch started
     uint64_t t0 = 0;
     uint32_t d = a.nphases > 0 ? __ldg(a.phases) : 0u;
     uint32_t d_prev = 0u;
@@ -155,45 +167,75 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
         if (ph == next_epoch) {
             while (epoch + 1 < a.nepochs && a.epoch_start[epoch + 1] == ph) ++epoch;
             next_epoch = epoch + 1 < a.nepochs ? a.epoch_start[epoch + 1] : INT64_MAX;
-            const uint32_t seed = a.epoch_seed[epoch];
-            for (int q = tid; q < npos; q += BLOCK) {
-                const uint32_t sid = Model::stream_id(a, r0 + q / cols, q % cols);
-                TinyState s;
-                tiny_seed(s, params_of(sid), seed + sid);
-                s_st[q] = s.s0;
-                s_st[spos + q] = s.s1;
-                s_st[2 * spos + q] = s.s2;
-                s_st[3 * spos + q] = s.s3;
+            const uint64_t eseed = a.epoch_seed[epoch];
+            if (PHILOX) {
+                key0 = (uint32_t)eseed;
+                key1 = (uint32_t)(eseed >> 32);
+                dstep = 0;
+            } else {
+                const uint32_t seed = (uint32_t)eseed;
+                for (int q = tid; q < npos; q += BLOCK) {
+                    const uint32_t sid = Model::stream_id(a, r0 + q / cols, q % cols);
+                    TinyState s;
+                    tiny_seed(s, params_of(sid), seed + sid);
+                    s_st[q] = s.s0;
+                    s_st[spos + q] = s.s1;
+                    s_st[2 * spos + q] = s.s2;
+                    s_st[3 * spos + q] = s.s3;
+                }
+                __syncthreads();  // positions are drawn by other threads than the ones seeding them
             }
-            __syncthreads();  // positions are drawn by other threads than the ones seeding them
         }
         const bool draws = (d & PH_DRAWS) != 0u;
         const typename Model::Ctx x0 = Model::ctx(a, lat, plane, d, a0 - 1);
         const typename Model::Ctx x1 = Model::ctx(a, lat + (size_t)NC * plane, plane, d, a0 - 1);
 
-        auto site = [&](int q, int r, int c) {
-            uint32_t k = 0;
-            if (draws) {
-                if (a.rng_kind == 0) {
-                    const uint32_t sid = UNIFORM ? 0u : Model::stream_id(a, r, c);
-                    TinyState s{s_st[q], s_st[spos + q], s_st[2 * spos + q], s_st[3 * spos + q]};
-                    k = tiny_draw23(s, params_of(sid));
-                    s_st[q] = s.s0;
-                    s_st[spos + q] = s.s1;
-                    s_st[2 * spos + q] = s.s2;
-                    s_st[3 * spos + q] = s.s3;
-                } else {
-                    k = philox_first(Model::stream_id(a, r, c), (uint32_t)ph, (uint32_t)((uint64_t)ph >> 32), a.chain,
-                                     a.key0, a.key1) >> 9;
-                }
-            }
+        auto site_k = [&](int r, int c, uint32_t k) {
             const int i = r + Model::ROFF, j = c + Model::COFF;
             const int off = (r - r0 + 1) * W + j;
             Model::site(a, x0, off, i, j, k);
             if (a.nlat > 1) Model::site(a, x1, off, i, j, k);
         };
+        // Bit-exact mode: one position, its TinyMT state in shared memory.
+        auto site = [&](int q, int r, int c) {
+            uint32_t k = 0;
+            if (draws) {
+                const uint32_t sid = UNIFORM ? 0u : Model::stream_id(a, r, c);
+                TinyState s{s_st[q], s_st[spos + q], s_st[2 * spos + q], s_st[3 * spos + q]};
+                k = tiny_draw23(s, params_of(sid));
+                s_st[q] = s.s0;
+                s_st[spos + q] = s.s1;
+                s_st[2 * spos + q] = s.s2;
+                s_st[3 * spos + q] = s.s3;
+            }
+            site_k(r, c, k);
+        };
+        // Fast mode: quad cq of row r, one Philox call for its four positions.
+        auto quad = [&](int r, int cq) {
+            uint4 w = make_uint4(0u, 0u, 0u, 0u);
+            if (draws)
+                w = philox4((uint32_t)(r * G + cq), (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32), a.chain, key0,
+                            key1);
+            const int c = cq * 4;
+            site_k(r, c, w.x >> 9);
+            if (c + 1 < cols) site_k(r, c + 1, w.y >> 9);
+            if (c + 2 < cols) site_k(r, c + 2, w.z >> 9);
+            if (c + 3 < cols) site_k(r, c + 3, w.w >> 9);
+        };
 
-        {
+        if (PHILOX) {
+            int u = tid, r = ri_lo + tid / G, cq = tid % G;
+            while (u < nq_in) {
+                quad(r, cq);
+                u += BLOCK;
+                r += dqr;
+                cq += dqc;
+                if (cq >= G) {
+                    cq -= G;
+                    ++r;
+                }
+            }
+        } else {
             int q = q_first, r = r_first, c = c_first;
             while (q < q_hi) {
                 site(q, r, c);
@@ -226,11 +268,18 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
             }
             if (__syncthreads_or(!ok)) return;
         }
-        for (int e = tid; e < n_edge; e += BLOCK) {
-            const bool top = e < top_n;
-            const int c = top ? e : e - top_n;
-            const int r = top ? r0 : r1 - 1;
-            site((r - r0) * cols + c, r, c);
+        if (PHILOX) {
+            for (int e = tid; e < nq_edge; e += BLOCK) {
+                const bool top = has_top && e < G;
+                quad(top ? r0 : r1 - 1, top ? e : e - (has_top ? G : 0));
+            }
+        } else {
+            for (int e = tid; e < n_edge; e += BLOCK) {
+                const bool top = e < top_n;
+                const int c = top ? e : e - top_n;
+                const int r = top ? r0 : r1 - 1;
+                site((r - r0) * cols + c, r, c);
+            }
         }
         __syncthreads();
         if (ph + 1 < a.nphases) {
@@ -250,6 +299,7 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
                 st_relaxed64(slot(a, cta, side, par, l, kx) + w, tag | v);
             }
         }
+        if (PHILOX && draws) ++dstep;
         d_prev = d;
         d = d_next;
     }
@@ -275,18 +325,19 @@ constexpr int kBlock = 1024;
 using KernelFn = void (*)(WalkArgs);
 
 template <class Model>
-static KernelFn pick_kernel(bool uniform) {
-    return uniform ? walk_kernel<Model, kBlock, true> : walk_kernel<Model, kBlock, false>;
+static KernelFn pick_kernel(bool uniform, bool philox) {
+    if (philox) return walk_kernel<Model, kBlock, true, true>;
+    return uniform ? walk_kernel<Model, kBlock, true, false> : walk_kernel<Model, kBlock, false, false>;
 }
 
-static KernelFn kernel_for(int family, bool uniform) {
+static KernelFn kernel_for(int family, bool uniform, bool philox) {
     switch (family) {
-        case FAM_DOMINO: return pick_kernel<DominoRule<false>>(uniform);
-        case FAM_DOMINO_HB: return pick_kernel<DominoRule<true>>(uniform);
-        case FAM_LOZENGE8: return pick_kernel<ThreeColour<int8_t, LozengeRule<false>>>(uniform);
-        case FAM_QLOZENGE32: return pick_kernel<ThreeColour<int32_t, LozengeRule<true>>>(uniform);
-        case FAM_RECTTRI: return pick_kernel<ThreeColour<int32_t, RectTriRule>>(uniform);
-        case FAM_TRIDIMER: return pick_kernel<TriDimerRule>(uniform);
+        case FAM_DOMINO: return pick_kernel<DominoRule<false>>(uniform, philox);
+        case FAM_DOMINO_HB: return pick_kernel<DominoRule<true>>(uniform, philox);
+        case FAM_LOZENGE8: return pick_kernel<ThreeColour<int8_t, LozengeRule<false>>>(uniform, philox);
+        case FAM_QLOZENGE32: return pick_kernel<ThreeColour<int32_t, LozengeRule<true>>>(uniform, philox);
+        case FAM_RECTTRI: return pick_kernel<ThreeColour<int32_t, RectTriRule>>(uniform, philox);
+        case FAM_TRIDIMER: return pick_kernel<TriDimerRule>(uniform, philox);
         default: return nullptr;
     }
 }
@@ -295,21 +346,21 @@ static int family_ncol(int family) { return family <= FAM_DOMINO_HB ? 2 : family
 static int family_elem(int family) { return family == FAM_LOZENGE8 || family <= FAM_DOMINO_HB ? 1 : 4; }
 static int family_xslots(int family) { return family == FAM_TRIDIMER ? 4 : 1; }
 
-size_t walk_smem_bytes(int family, int nlat, int rows_per_cta, int cols, int width) {
+size_t walk_smem_bytes(int family, int nlat, int rows_per_cta, int cols, int width, bool philox) {
     const int wpad = (width + 3) & ~3;
-    return (size_t)4 * 4 * rows_per_cta * cols +
+    return (philox ? (size_t)0 : (size_t)4 * 4 * rows_per_cta * cols) +
            (size_t)nlat * family_ncol(family) * (rows_per_cta + 2) * wpad * family_elem(family);
 }
 
-rt_status plan_walk(int family, int device, int nlat, int rows, int cols, int width, bool uniform, WalkPlan* plan,
-                    std::string* err) {
+rt_status plan_walk(int family, int device, int nlat, int rows, int cols, int width, bool uniform, bool philox,
+                    WalkPlan* plan, std::string* err) {
     int sms = 0, smem_optin = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
         cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) {
         *err = "cudaDeviceGetAttribute failed";
         return RT_E_CUDA;
     }
-    KernelFn fn = kernel_for(family, uniform);
+    KernelFn fn = kernel_for(family, uniform, philox);
     if (!fn) {
         *err = "unknown kernel family";
         return RT_E_INVAL;
@@ -321,7 +372,7 @@ rt_status plan_walk(int family, int device, int nlat, int rows, int cols, int wi
     }
     const int wpad = (width + 3) & ~3;
     for (int rpc = std::max(1, rows / (2 * sms)); rpc <= rows; ++rpc) {
-        const size_t smem = walk_smem_bytes(family, nlat, rpc, cols, width);
+        const size_t smem = walk_smem_bytes(family, nlat, rpc, cols, width, philox);
         if (smem > (size_t)smem_optin) break;
         const int ctas = (rows + rpc - 1) / rpc;
         int per_sm = 0;

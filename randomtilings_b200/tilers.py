@@ -89,6 +89,22 @@ class _Tiler:
         self._check(self._lib.rt_walk(self._h, arr.ctypes.data, n, int(steps), int(seed)))
         _writeback(t, arr)
 
+    def CFTP(self, tmax, tmin, first_steps: int = 1024, schedule: int = _capi.RT_CFTP_DOUBLING,
+             master_seed: int = 345903, max_trials: int = 30):
+        """Coupling from the past (Examples/AztecDiamondCftpEx.cpp:42-68) for a
+        monotone kernel: dominoes with kernel=RT_KERNEL_CFTP, or either lozenge
+        kernel.  Returns (tiling, stats dict)."""
+        a, n = _as_tiling(tmax)
+        b, n2 = _as_tiling(tmin)
+        if n != n2:
+            raise ValueError("tmax and tmin differ in size")
+        out = np.zeros_like(a)
+        st = _capi.RtCftpStats()
+        self._check(self._lib.rt_cftp(self._h, a.ctypes.data, b.ctypes.data, n, int(first_steps), int(schedule),
+                                      int(master_seed), int(max_trials), out.ctypes.data, ctypes.byref(st)))
+        return out, {"total_steps": st.total_steps, "trials": st.trials, "coalesced": bool(st.coalesced),
+                     "device_ms": st.device_ms}
+
     # -- device-resident form ---------------------------------------------
     def upload(self, t) -> None:
         arr, n = _as_tiling(t)
@@ -149,22 +165,6 @@ class DominoTiler(_Tiler):
             _writeback(t, arr)
         else:
             super().Walk(t, steps, seed)
-
-    def CFTP(self, tmax, tmin, first_steps: int = 1024, schedule: int = _capi.RT_CFTP_DOUBLING,
-             master_seed: int = 345903, max_trials: int = 30):
-        """Coupling from the past (Examples/AztecDiamondCftpEx.cpp:42-68); the
-        handle must use kernel=RT_KERNEL_CFTP.  Returns (tiling, stats dict)."""
-        a, n = _as_tiling(tmax)
-        b, n2 = _as_tiling(tmin)
-        if n != n2:
-            raise ValueError("tmax and tmin differ in size")
-        out = np.zeros_like(a)
-        st = _capi.RtCftpStats()
-        self._check(self._lib.rt_cftp(self._h, a.ctypes.data, b.ctypes.data, n, int(first_steps), int(schedule),
-                                      int(master_seed), int(max_trials), out.ctypes.data, ctypes.byref(st)))
-        return out, {"total_steps": st.total_steps, "trials": st.trials, "coalesced": bool(st.coalesced),
-                     "device_ms": st.device_ms}
-
 
 class LozengeTiler(_Tiler):
     MODEL = _capi.RT_LOZENGE
