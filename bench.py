@@ -75,12 +75,12 @@ def start_tiling():
     return rt.LozengeTiler.MinTiling(d)
 
 
-def algorithmic_bytes_per_step(n: int, elem: int) -> int:
+def algorithmic_bytes_per_step(n: int, elem: int, rng_state: bool = True) -> int:
     """Lattice read + write of every colour-array site, plus the TinyMT state
-    (s0..s3 read + write, 32 B) of every attempt."""
+    (s0..s3 read + write, 32 B) of every attempt (none in fast mode)."""
     sites = n * n
     attempts = n * (n // 3)
-    return 2 * sites * elem + attempts * 32
+    return 2 * sites * elem + (attempts * 32 if rng_state else 0)
 
 
 class ClockSampler:
@@ -229,6 +229,8 @@ def run_b200(args) -> None:
     tl.upload(t0)
     tq = rt.LozengeTiler(device=local, kernel=2, q=0.99, qcmp=0)
     tq.upload(t0)
+    tf = rt.LozengeTiler(device=local, rng=rt.RT_RNG_PHILOX)
+    tf.upload(t0)
 
     barrier(dist)
     torch.cuda.synchronize()
@@ -240,11 +242,13 @@ def run_b200(args) -> None:
     barrier(dist)
     clocks = clk.summary()
     ms_q = time_device_walks(tq, args.steps, args.warmup, seed, flush)
+    ms_f = time_device_walks(tf, args.steps, args.warmup, seed, flush)
     e2e_ms = time_e2e_walks(rt.LozengeTiler, {"device": local}, t0, args.steps, min(args.warmup, 3), seed, flush)
     phases, launches = tl.last_run_info()
 
     total_ms = all_max(dist, sum(ms))
     total_q = all_max(dist, sum(ms_q))
+    total_f = all_max(dist, sum(ms_f))
     total_e2e = all_max(dist, sum(e2e_ms))
     work = attempts * STEPS_PER_WALK * args.steps * world
     value = work / (total_ms / 1e3)
@@ -254,6 +258,8 @@ def run_b200(args) -> None:
     achieved = algo / (per_launch_ms / 1e3) / 1e9
     algo_q = algorithmic_bytes_per_step(n, 4) * STEPS_PER_WALK
     achieved_q = algo_q / (sum(ms_q) / len(ms_q) / 1e3) / 1e9
+    algo_f = algorithmic_bytes_per_step(n, 1, rng_state=False) * STEPS_PER_WALK
+    achieved_f = algo_f / (sum(ms_f) / len(ms_f) / 1e3) / 1e9
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -304,6 +310,14 @@ def run_b200(args) -> None:
                 "hbm_gbs_algorithmic": achieved_q,
                 "frac": achieved_q / peak,
             },
+            "fast_mode": {
+                "rng": "Philox4x32-10 keyed by (position quad, step, chain), cyclic colours", "dtype": "int8",
+                "value": attempts * STEPS_PER_WALK * args.steps * world / (total_f / 1e3),
+                "unit": "attempts/s",
+                "ms_per_step": total_f / args.steps,
+                "hbm_gbs_algorithmic": achieved_f,
+                "frac": achieved_f / peak,
+            },
             "gpu_launches": int(launches) * args.steps,
             "phases_per_launch": int(phases),
             "clocks": clocks,
@@ -314,6 +328,7 @@ def run_b200(args) -> None:
         print(json.dumps(line), flush=True)
     tl.close()
     tq.close()
+    tf.close()
     if dist is not None:
         dist.destroy_process_group()
 

@@ -125,15 +125,18 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
 }
 
 /* Where a Rotate's draws come from.  Bit-exact mode: the reference's TinyMT
- * stream of work item c + cols * r.  Fast mode: position (r, c) of the Rotate
- * range belongs to quad u = r * ceil(cols / 4) + c / 4 and takes word c mod 4
- * of Philox4x32-10(counter = (u, step lo, step hi, chain), key), where `step`
+ * stream of work item c + cols * r.  Fast mode: work item (r, c) acts on site
+ * (i, j) = (r + roff, c + coff) of its colour array (`width` sites per row);
+ * the site belongs to quad u = i * ceil(width / 4) + j / 4 -- the 32-bit word
+ * of four int8 sites that holds it -- and takes output word j mod 4 of
+ * Philox4x32-10(counter = (u, step lo, step hi, chain), key), where `step`
  * counts the drawing steps of the epoch from 0.  Either way the draw is
  * k * 2^-23 with a 23-bit k (the top bits of the 32-bit word). */
 typedef struct {
     int fast;
     orc_tinymt* tmt;
     int64_t cols;
+    int64_t roff, coff, width;
     uint32_t key[2], chain;
     uint64_t step;
     int64_t cached_u; /* quad whose words are in w[] (-1: none) */
@@ -142,23 +145,29 @@ typedef struct {
 
 static float orc_draw(orc_draws* d, int64_t r, int64_t c) {
     if (!d->fast) return orc_tinymt_single01(&d->tmt[c + d->cols * r]);
-    const int64_t u = r * ((d->cols + 3) / 4) + c / 4;
+    const int64_t i = r + d->roff, j = c + d->coff;
+    const int64_t u = i * ((d->width + 3) / 4) + j / 4;
     if (u != d->cached_u) {
         const uint32_t ctr[4] = {(uint32_t)u, (uint32_t)d->step, (uint32_t)(d->step >> 32), d->chain};
         orc_philox4x32_10(ctr, d->key, d->w);
         d->cached_u = u;
     }
-    return (float)(d->w[c & 3] >> 9) * (1.0f / 8388608.0f);
+    return (float)(d->w[j & 3] >> 9) * (1.0f / 8388608.0f);
 }
 
 /* Starts an epoch: TinyMT streams seeded with `seed` (bit-exact mode) or the
- * Philox key `seed` (fast mode). */
-static int draws_begin(orc_draws* d, int fast, int64_t items, int64_t cols, uint64_t seed, uint32_t chain,
-                       const uint32_t* params, int64_t nparams) {
+ * Philox key `seed` (fast mode).  Work item (r, c) of the Rotate range (cols
+ * items per row) acts on site (r + roff, c + coff) of a colour array `width`
+ * sites wide. */
+static int draws_begin(orc_draws* d, int fast, int64_t items, int64_t cols, int64_t roff, int64_t coff,
+                       int64_t width, uint64_t seed, uint32_t chain, const uint32_t* params, int64_t nparams) {
     int err = ORC_OK;
     memset(d, 0, sizeof *d);
     d->fast = fast;
     d->cols = cols;
+    d->roff = roff;
+    d->coff = coff;
+    d->width = width;
     d->chain = chain;
     d->cached_u = -1;
     if (fast) {
@@ -355,7 +364,7 @@ static int domino_run(int32_t* t, int n, const int64_t* steps, const int64_t* se
          * black ((i+j) even) first. */
         const uint64_t tseed = fast ? (uint64_t)seeds[e] : single_walk ? mt_next(&m) : (uint32_t)(uint64_t)seeds[e];
         orc_draws rng;
-        err = draws_begin(&rng, fast, items, h - 2, tseed, chain, params, nparams);
+        err = draws_begin(&rng, fast, items, h - 2, 1, 1, h, tseed, chain, params, nparams);
         if (err != ORC_OK) break;
         for (int64_t s = 0; s < steps[e]; ++s) {
             const int black = fast ? (s & 1) == 0 : mt_next(&m) % 2u == 1u;
@@ -493,8 +502,8 @@ static int lozenge_run(int32_t* t, int n, const int64_t* steps, const int64_t* s
     int err = ORC_OK;
     for (int e = 0; e < k && err == ORC_OK; ++e) {
         orc_draws rng;
-        err = draws_begin(&rng, fast, (int64_t)n * m, m, fast ? (uint64_t)seeds[e] : (uint32_t)(uint64_t)seeds[e],
-                          chain, params, nparams);
+        err = draws_begin(&rng, fast, (int64_t)n * m, m, 0, 0, m,
+                          fast ? (uint64_t)seeds[e] : (uint32_t)(uint64_t)seeds[e], chain, params, nparams);
         if (err != ORC_OK) break;
         minstd g;
         minstd_seed(&g, seeds[e]);
@@ -622,8 +631,8 @@ static int recttri_run(int32_t* t, int n, int64_t steps, int64_t seed, const uin
     for (int i = 0; i < n; ++i)
         for (int j = 0; j < n; ++j) arr[((i - j) % 3 + 3) % 3][(int64_t)i * m + j / 3] = t[(int64_t)i * n + j];
     orc_draws rng;
-    int err = draws_begin(&rng, fast, (int64_t)n * m, m, fast ? (uint64_t)seed : (uint32_t)(uint64_t)seed, chain,
-                          params, nparams);
+    int err = draws_begin(&rng, fast, (int64_t)n * m, m, 0, 0, m, fast ? (uint64_t)seed : (uint32_t)(uint64_t)seed,
+                          chain, params, nparams);
     if (err == ORC_OK) {
         minstd g;
         minstd_seed(&g, seed);
@@ -1066,8 +1075,8 @@ static int tridimer_run(int32_t* t, int n, int64_t steps, int64_t seed, const ui
     for (int i = 0; i < n / 2; ++i)
         for (int j = 0; j < n; ++j) (j % 2 == 0 ? S.D : S.U)[(int64_t)i * m + j / 2] = tri[(int64_t)i * n + j];
     orc_draws draws, *rng = &draws;
-    int err = draws_begin(rng, fast, (int64_t)mm, m, fast ? (uint64_t)seed : (uint32_t)(uint64_t)seed, chain, params,
-                          nparams);
+    int err = draws_begin(rng, fast, (int64_t)mm, m, 0, 0, m, fast ? (uint64_t)seed : (uint32_t)(uint64_t)seed, chain,
+                          params, nparams);
     if (err == ORC_OK) {
         minstd g;
         minstd_seed(&g, seed);

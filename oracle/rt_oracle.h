@@ -72,7 +72,9 @@ int orc_lozenge_walk_epochs(int32_t* t, int n, const int64_t* steps, const int64
 
 /* ---- fast mode (no reference counterpart) ----
  * Counter-based draws: Philox4x32-10 keyed by the epoch key, counter =
- * (position quad, step within the epoch, 0, chain); colours in a fixed
+ * (site word, step within the epoch, chain) -- the site word being the
+ * 32-bit word of four consecutive int8 sites of a colour-array row, index
+ * i * ceil(width / 4) + j / 4, lane j mod 4; colours in a fixed
  * cycle (dominoes: black, white; three-colour models: 0, 1, 2; triangle
  * dimers: a 30-move sweep over every flip class). */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);

@@ -4,7 +4,10 @@ The compute path is librt_b200.so (CUDA kernels behind the C ABI declared in
 include/rt_b200.h); this package only binds it.  Importing the package does
 not touch the GPU; creating a Tiler does.
 """
-from ._capi import RtError, load  # noqa: F401
+from ._capi import (RT_CFTP_DOUBLING, RT_CFTP_REFERENCE, RT_KERNEL_CFTP, RT_KERNEL_DEFAULT,  # noqa: F401
+                    RT_KERNEL_QWEIGHT, RT_QCMP_DOUBLE, RT_QCMP_FLOAT32, RT_RNG_PHILOX, RT_RNG_TINYMT, RtError, load)
 from .tilers import DominoTiler, LozengeTiler, RectTriangleTiler, TriangleDimerTiler  # noqa: F401
 
-__all__ = ["DominoTiler", "LozengeTiler", "RectTriangleTiler", "TriangleDimerTiler", "RtError", "load"]
+__all__ = ["DominoTiler", "LozengeTiler", "RectTriangleTiler", "TriangleDimerTiler", "RtError", "load",
+           "RT_KERNEL_DEFAULT", "RT_KERNEL_CFTP", "RT_KERNEL_QWEIGHT", "RT_RNG_TINYMT", "RT_RNG_PHILOX",
+           "RT_QCMP_FLOAT32", "RT_QCMP_DOUBLE", "RT_CFTP_DOUBLING", "RT_CFTP_REFERENCE"]

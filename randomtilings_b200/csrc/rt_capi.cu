@@ -8,6 +8,7 @@
 // drawn once per call into a phase list that the device walks in one launch.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -115,6 +116,8 @@ struct rt_tiler {
     WalkPlan plan;
     int plan_rows = -1, plan_cols = -1, plan_nlat = -1;
     bool plan_uniform = true;
+    int kernel_choice = 0;  // 0 auto, 1 generic walk kernel only, 2 word kernel only (RT_WALK_KERNEL)
+    int ctas_hint = 0;      // word kernel grid (RT_WALK_CTAS; 0 = one CTA per SM)
     int64_t last_phases = 0, last_launches = 0;
     uint64_t timeout_ns = 5000000000ull;
 
@@ -223,6 +226,11 @@ rt_status rt_create(const rt_config* cfg, rt_tiler** out) {
         g_create_error = "cudaEventCreate failed";
         return RT_E_CUDA;
     }
+    if (const char* kc = std::getenv("RT_WALK_KERNEL")) {
+        if (std::strcmp(kc, "generic") == 0) h->kernel_choice = 1;
+        if (std::strcmp(kc, "word") == 0) h->kernel_choice = 2;
+    }
+    if (const char* ct = std::getenv("RT_WALK_CTAS")) h->ctas_hint = std::max(0, std::atoi(ct));
     if (const char* t = std::getenv("RT_WAIT_TIMEOUT_MS")) {
         const long ms = std::atol(t);
         if (ms > 0) h->timeout_ns = (uint64_t)ms * 1000000ull;
@@ -531,8 +539,16 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     const int width = h->width;
     const bool uniform = fast || h->table.empty();
     if (h->plan_rows != h->rows || h->plan_cols != h->cols || h->plan_nlat != h->nlat || h->plan_uniform != uniform) {
-        rt_status s = plan_walk(h->family, h->cfg.device, h->nlat, h->rows, h->cols, width, uniform, fast, &h->plan,
-                                &h->err);
+        // The word kernel serves the int8 models with uniform generator
+        // parameters; everything else (and any band it cannot hold) runs on
+        // the generic walk kernel.
+        rt_status s = RT_E_INVAL;
+        if (h->kernel_choice != 1 && uniform && word_family(h->family))
+            s = plan_word_walk(h->family, h->cfg.device, h->nlat, h->rows, width, fast, h->ctas_hint, &h->plan,
+                               &h->err);
+        if (s != RT_OK && h->kernel_choice == 2) return s;
+        if (s != RT_OK)
+            s = plan_walk(h->family, h->cfg.device, h->nlat, h->rows, h->cols, width, uniform, fast, &h->plan, &h->err);
         if (s != RT_OK) return s;
         h->plan_rows = h->rows;
         h->plan_cols = h->cols;

@@ -130,9 +130,10 @@ __host__ __device__ inline uint4 philox4(uint32_t c0, uint32_t c1, uint32_t c2, 
     return make_uint4(c0, c1, c2, c3);
 }
 
-// Fast-mode draws.  Positions of one row of the Rotate grid are taken in
-// quads of four consecutive columns; quad u = r * ceil(cols/4) + c/4 of step s
-// (counted within the epoch) of chain `chain` uses word (c mod 4) of
+// Fast-mode draws.  The site (i, j) that a work item flips lies in the 32-bit
+// word u = i * ceil(width/4) + j/4 of four consecutive sites of its colour
+// array row (`width` sites per row); at step s (counted within the epoch) of
+// chain `chain` it uses output word (j mod 4) of
 // Philox4x32-10(counter = (u, s mod 2^32, s / 2^32, chain), key = epoch key),
 // and its top 23 bits are the draw k, so the integer acceptance thresholds of
 // the TinyMT mode apply unchanged.

@@ -35,6 +35,11 @@ struct WalkPlan {
 rt_status plan_walk(int family, int device, int nlat, int rows, int cols, int width, bool uniform, bool philox,
                     WalkPlan* plan, std::string* err);
 rt_status launch_walk(const WalkPlan& plan, WalkArgs& args, cudaStream_t stream, std::string* err);
+// Word-parallel kernel of the int8 models (rt_word.cu): uniform TinyMT32J
+// parameters or fast mode.  ctas_hint <= 0: one CTA per SM.
+bool word_family(int family);
+rt_status plan_word_walk(int family, int device, int nlat, int rows, int width, bool philox, int ctas_hint,
+                         WalkPlan* plan, std::string* err);
 // kind: 0 domino, 1 lozenge, 2 rect-triangle, 3 triangle-dimer (merge only).
 rt_status launch_split(bool merge, int elem_bytes, int kind, int ncol, int n, int32_t* tiling, void* const* arr,
                        cudaStream_t stream, std::string* err);

@@ -9,76 +9,10 @@
 
 #include "rt_internal.h"
 #include "rt_models.cuh"
+#include "rt_exchange.cuh"
 #include "rt_tridimer.cuh"
 
 namespace rtb {
-
-// ---------------------------------------------------------------------------
-// Halo exchange.  After each flip phase a CTA publishes the first and last
-// row of its band (of the colour it just flipped) into a slot of global
-// memory; every 64-bit slot word carries 32 bits of lattice data and the
-// phase tag (phase + 1), so a neighbour knows the row is complete by polling
-// the words themselves -- no separate flag, no memory fence on the critical
-// path.  Slots are double-buffered by phase parity; a CTA enters phase p only
-// after both neighbours finished phase p-1, so a slot is never overwritten
-// before it was read.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-__device__ __forceinline__ unsigned long long* slot(const WalkArgs& a, int cta, int side, int parity, int lat,
-                                                   int k) {
-    return a.xbuf + (((((size_t)cta * 2 + side) * 2 + parity) * a.nlat + lat) * a.xslots + k) * a.xwords;
-}
-
-// Index of the k-th set bit of mask (k < popc(mask)).
-__device__ __forceinline__ int nth_bit(uint32_t mask, int k) {
-    for (int i = 0; i < k; ++i) mask &= mask - 1;
-    return __ffs(mask) - 1;
-}
-
-template <class T>
-__device__ __forceinline__ uint32_t pack_word(const T* row, int w) {
-    if (sizeof(T) == 1) return reinterpret_cast<const uint32_t*>(row)[w];
-    return (uint32_t)row[w];
-}
-template <class T>
-__device__ __forceinline__ void unpack_word(T* row, int w, uint32_t v) {
-    if (sizeof(T) == 1)
-        reinterpret_cast<uint32_t*>(row)[w] = v;
-    else
-        row[w] = (T)v;
-}
-
-// Waits for one tagged word; returns false on timeout or when another CTA
-// already reported an error.
-__device__ __forceinline__ bool wait_word(const WalkArgs& a, const unsigned long long* p, uint32_t tag,
-                                          uint32_t* out, uint64_t& t0) {
-    unsigned spins = 0;
-    for (;;) {
-        const unsigned long long x = ld_relaxed64(p);
-        if ((uint32_t)(x >> 32) == tag) {
-            *out = (uint32_t)x;
-            return true;
-        }
-        if ((++spins & 63u) == 0u) {
-            if (*(volatile int*)a.err) return false;
-            const uint64_t now = global_ns();
-            if (t0 == 0) {
-                t0 = now;
-            } else if (now - t0 > a.timeout_ns) {
-                atomicOr(a.err, ERR_TIMEOUT);
-                return false;
-            }
-        }
-    }
-}
 
 // Shared memory of one CTA: in bit-exact mode the generator states of its
 // positions (struct of arrays s0[], s1[], s2[], s3[], so consecutive threads
@@ -144,9 +78,13 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
     const int dr = BLOCK / cols, dc = BLOCK % cols;
     const int q_first = q_lo + tid;
     const int r_first = r0 + q_first / cols, c_first = q_first % cols;
-    // Fast mode walks quads of four consecutive columns instead (one Philox
-    // call per quad): interior rows ri_lo..ri_hi-1, the same edge rows.
-    const int G = (cols + 3) >> 2;
+    // Fast mode walks quads instead -- the words of four consecutive sites of
+    // a colour-array row, one Philox call each: quads qlo..qlo+G-1 of every
+    // row cover the positions; interior rows ri_lo..ri_hi-1, the same edge
+    // rows.
+    const int Gw = (a.width + 3) >> 2;  // quads per colour-array row (counter)
+    const int qlo = Model::COFF >> 2;
+    const int G = ((Model::COFF + cols - 1) >> 2) - qlo + 1;
     const int ri_lo = r0 + (has_top ? 1 : 0);
     const int ri_hi = max(ri_lo, r1 - (has_bot ? 1 : 0));
     const int nq_in = (ri_hi - ri_lo) * G;
@@ -210,17 +148,19 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
             }
             site_k(r, c, k);
         };
-        // Fast mode: quad cq of row r, one Philox call for its four positions.
+        // Fast mode: quad qlo + cq of position row r, one Philox call for the
+        // (up to) four positions whose sites it holds.
         auto quad = [&](int r, int cq) {
+            const int q = qlo + cq;
             uint4 w = make_uint4(0u, 0u, 0u, 0u);
             if (draws)
-                w = philox4((uint32_t)(r * G + cq), (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32), a.chain, key0,
-                            key1);
-            const int c = cq * 4;
-            site_k(r, c, w.x >> 9);
-            if (c + 1 < cols) site_k(r, c + 1, w.y >> 9);
-            if (c + 2 < cols) site_k(r, c + 2, w.z >> 9);
-            if (c + 3 < cols) site_k(r, c + 3, w.w >> 9);
+                w = philox4((uint32_t)((r + Model::ROFF) * Gw + q), (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32),
+                            a.chain, key0, key1);
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int c = 4 * q + b - Model::COFF;
+                if (c >= 0 && c < cols) site_k(r, c, quad_word(w, b) >> 9);
+            }
         };
 
         if (PHILOX) {

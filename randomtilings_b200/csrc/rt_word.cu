@@ -1,0 +1,578 @@
+// rt_word.cu -- the word-parallel walk kernel of the int8 models.
+//
+// Dominoes (dominokernel.cl, dominokernelCFTP.cl) and uniform lozenges
+// (lozengekernel.cl) store one byte per site.  This kernel treats a 32-bit
+// word of four consecutive sites of a colour-array row as its unit of work:
+// the Update of a colour is a handful of masks and byte shifts on words of
+// the flipped colour (neighbours at j +- 1 are funnel shifts of two adjacent
+// words), the flip test is a per-byte compare, and each thread keeps the
+// TinyMT states of the four positions of each of its words in registers for
+// the whole walk (bit-exact mode) or draws them from one Philox call per word
+// (fast mode).  Schedule, bands, halo exchange and bounded waits are those of
+// the generic walk kernel (rt_walk.cu); only the per-site arithmetic differs,
+// and it produces the same bytes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+
+#include "rt_exchange.cuh"
+#include "rt_internal.h"
+#include "rt_models.cuh"
+
+namespace rtb {
+
+constexpr int kWordBlockMax = 512;
+
+// 0x01 in every byte of v equal to the same byte of pat (bytes < 0x80).
+__device__ __forceinline__ uint32_t eq_bytes(uint32_t v, uint32_t pat) {
+    const uint32_t x = v ^ pat;
+    return (~(x + 0x7f7f7f7fu) >> 7) & 0x01010101u;
+}
+
+// 0x01 in byte b iff k_b < thr.
+__device__ __forceinline__ uint32_t below4(const uint32_t (&k)[4], uint32_t thr) {
+    return (uint32_t)(k[0] < thr) | ((uint32_t)(k[1] < thr) << 8) | ((uint32_t)(k[2] < thr) << 16) |
+           ((uint32_t)(k[3] < thr) << 24);
+}
+
+__device__ __forceinline__ uint32_t lds(const unsigned char* p) { return *reinterpret_cast<const uint32_t*>(p); }
+__device__ __forceinline__ void sts(unsigned char* p, uint32_t v) { *reinterpret_cast<uint32_t*>(p) = v; }
+
+// Domino UpdateTiles (dominokernel.cl:22-31) for the four sites of a word:
+// edge bits 1 up, 2 down, 4 towards j-1, 8 towards j+1 from the flipped array
+// `src`; the neighbour towards j+1 shares the column in rows with
+// p = (i + t) odd, towards j-1 in the others.
+__device__ __forceinline__ uint32_t domino_refresh(const unsigned char* src, int off, int W, int p) {
+    const uint32_t up = lds(src + off - W), dn = lds(src + off + W);
+    const uint32_t l = lds(src + off - 4), c = lds(src + off), r = lds(src + off + 4);
+    const uint32_t west = p ? c : __funnelshift_l(l, c, 8);
+    const uint32_t east = p ? __funnelshift_r(c, r, 8) : c;
+    return ((up & 0x02020202u) >> 1) | ((dn & 0x01010101u) << 1) | ((west & 0x08080808u) >> 1) |
+           ((east & 0x04040404u) << 1);
+}
+
+// Lozenge UpdateTiles (lozengekernel.cl:36-54) for four sites: colour t+1
+// keeps all but bits {2,4,32} and takes them from f[i-1][j+sa], f[i][j-sw],
+// f[i+1][j]; colour t+2 keeps all but {1,8,16} and takes them from f[i-1][j],
+// f[i][j+se], f[i+1][j-sa].  The bit fields never overlap, so the reference's
+// sums are ORs.
+__device__ __forceinline__ void lozenge_refresh(const unsigned char* f, int off, int W, uint32_t sh, uint32_t a_old,
+                                                uint32_t b_old, uint32_t& na, uint32_t& nb) {
+    const uint32_t u0 = lds(f + off - W), u1 = lds(f + off - W + 4);
+    const uint32_t ml = lds(f + off - 4), m0 = lds(f + off), mr = lds(f + off + 4);
+    const uint32_t dl = lds(f + off + W - 4), d0 = lds(f + off + W);
+    const uint32_t sa = sh & 1u, sw = (sh >> 1) & 1u, se = (sh >> 2) & 1u;
+    const uint32_t fu_sa = sa ? __funnelshift_r(u0, u1, 8) : u0;
+    const uint32_t fw = sw ? __funnelshift_l(ml, m0, 8) : m0;
+    const uint32_t fe = se ? __funnelshift_r(m0, mr, 8) : m0;
+    const uint32_t fd_sa = sa ? __funnelshift_l(dl, d0, 8) : d0;
+    na = (a_old & 0xd9d9d9d9u) | ((fu_sa & 0x10101010u) >> 3) | ((fw & 0x08080808u) >> 1) |
+         ((d0 & 0x01010101u) << 5);
+    nb = (b_old & 0xe6e6e6e6u) | ((u0 & 0x20202020u) >> 5) | ((fe & 0x04040404u) << 1) |
+         ((fd_sa & 0x02020202u) << 3);
+}
+
+__device__ __forceinline__ uint32_t merge(uint32_t old, uint32_t nw, uint32_t mask) { return (old & ~mask) | (nw & mask); }
+
+// Fixed facts of one word of the band: its byte offset in a colour plane,
+// its colour-array row i, and two byte masks: `um` (0xff) marks the sites an
+// Update refreshes (1 <= i <= N-2, 1 <= j <= width-2), `vm` (0x01) the sites
+// that are Rotate positions.
+struct WordInfo {
+    int off;
+    int cls;  // lozenges: i mod 3; dominoes: i mod 2
+    uint32_t um;
+    uint32_t vm;
+};
+
+template <int FAM>
+struct WordModel {
+    static constexpr bool DOM = FAM != FAM_LOZENGE8;
+    static constexpr int NC = DOM ? 2 : 3;
+    static constexpr int ROFF = DOM ? 1 : 0;
+    static constexpr int COFF = DOM ? 1 : 0;
+    __device__ static uint32_t written(uint32_t d) {
+        if (ph_op(d) != OP_STEP) return 0u;
+        return 1u << (DOM ? 1 - (int)ph_a(d) : (int)ph_a(d));
+    }
+};
+
+// Per-phase decoded descriptor: which planes a word reads and writes.
+struct WordPhase {
+    bool step, upd, keep_a;
+    int par;                // dominoes: parity t of the pending Update
+    uint32_t shifts;        // lozenges: column shifts per row class (3 bits each)
+    unsigned char* dst;     // dominoes: array written; lozenges: colour flipped (STEP)
+    const unsigned char* src;  // flipped array whose neighbours are read (Update)
+    unsigned char* pa;      // lozenges: colours t+1, t+2 of the Update
+    unsigned char* pb;
+};
+
+__device__ __forceinline__ uint32_t lozenge_shift_table(int t) {
+    uint32_t tab = 0;
+#pragma unroll
+    for (int rr = 0; rr < 3; ++rr) {
+        const uint32_t sa = rr == (2 * t + 1) % 3, sw = rr == (2 * t + 2) % 3, se = rr == (2 * t) % 3;
+        tab |= (sa | (sw << 1) | (se << 2)) << (3 * rr);
+    }
+    return tab;
+}
+
+// One phase on one word of one lattice; `lo` is the byte offset of the
+// lattice's planes from those the phase descriptor points at.
+// m0 / m1: per-byte draw masks (0x01) -- dominoes: k < thr[0]; lozenges:
+// k < thr[0] (add a cube) and thr[0] <= k < thr[1] (remove one).
+template <int FAM>
+__device__ __forceinline__ void word_phase(const WordPhase& P, int lo, int W, const WordInfo& wi, uint32_t m0,
+                                           uint32_t m1) {
+    const int off = wi.off + lo;
+    if (FAM != FAM_LOZENGE8) {
+        uint32_t v = lds(P.dst + off);
+        if (P.upd) v = merge(v, domino_refresh(P.src, off, W, (wi.cls ^ P.par) & 1), wi.um);
+        if (P.step) {
+            const uint32_t e3 = eq_bytes(v, 0x03030303u), e12 = eq_bytes(v, 0x0c0c0c0cu);
+            uint32_t tog;
+            if (FAM == FAM_DOMINO_HB)  // dominokernelCFTP.cl:19-28: k < 2^22 -> 12, else -> 3
+                tog = (e3 & m0) | (e12 & ~m0);
+            else  // dominokernel.cl:11-17: k < thr toggles 3 <-> 12
+                tog = (e3 | e12) & m0;
+            v ^= (tog & wi.vm) * 15u;
+        }
+        sts(P.dst + off, v);
+    } else {
+        if (P.step) {
+            uint32_t v;
+            if (P.upd) {
+                const uint32_t ao = lds(P.pa + off), bo = lds(P.pb + off);
+                uint32_t na, nb;
+                lozenge_refresh(P.src, off, W, (P.shifts >> (3 * wi.cls)) & 7u, ao, bo, na, nb);
+                na = merge(ao, na, wi.um);
+                nb = merge(bo, nb, wi.um);
+                if (P.keep_a) {
+                    v = na;
+                    sts(P.pb + off, nb);
+                } else {
+                    v = nb;
+                    sts(P.pa + off, na);
+                }
+            } else {
+                v = lds(P.dst + off);
+            }
+            // lozengekernel.cl:19-31: k < thr0 turns 25 into 38, thr0 <= k < thr1 turns 38 into 25.
+            const uint32_t tog = (eq_bytes(v, 0x19191919u) & m0) | (eq_bytes(v, 0x26262626u) & m1);
+            v ^= (tog & wi.vm) * 63u;
+            sts(P.dst + off, v);
+        } else {
+            const uint32_t ao = lds(P.pa + off), bo = lds(P.pb + off);
+            uint32_t na, nb;
+            lozenge_refresh(P.src, off, W, (P.shifts >> (3 * wi.cls)) & 7u, ao, bo, na, nb);
+            sts(P.pa + off, merge(ao, na, wi.um));
+            sts(P.pb + off, merge(bo, nb, wi.um));
+        }
+    }
+}
+
+// 0x01 per byte of the bits set in mask, one bit per byte index.
+__device__ __forceinline__ uint32_t lane_bytes(uint32_t bits) {
+    return (bits & 1u) | ((bits & 2u) << 7) | ((bits & 4u) << 14) | ((bits & 8u) << 21);
+}
+
+// Shared memory: 16 bytes of slack, then for each lattice NC colour planes of
+// (band rows + 2 halo rows) x wpad bytes, then 16 bytes of slack (the funnel
+// shifts read one word beyond a row; those bytes only reach sites outside
+// the update / flip masks).
+template <int FAM, int MAXW, bool PHILOX, int LB>
+__global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ WalkArgs a) {
+    using M = WordModel<FAM>;
+    constexpr int NC = M::NC;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char* lat = smem_raw + 16;
+
+    const int BLOCK = blockDim.x;
+    const int cta = blockIdx.x, nct = gridDim.x, tid = threadIdx.x;
+    const int r0 = cta * a.rows_per_cta;
+    const int r1 = min(a.rows, r0 + a.rows_per_cta);
+    const int nrows = r1 - r0;
+    const int a0 = r0 + M::ROFF, a1 = r1 + M::ROFF;
+    const int W = a.wpad;
+    const int plane = (nrows + 2) * W;
+    const int Gw = W >> 2;  // words per row (the fast mode's counter stride too)
+    const int nwords = nrows * Gw;
+    const int N = a.n;
+
+    for (int l = 0; l < a.nlat; ++l)
+        for (int c = 0; c < NC; ++c) {
+            const int8_t* g = static_cast<const int8_t*>(a.arr[l][c]);
+            unsigned char* s = lat + (l * NC + c) * plane;
+            for (int e = tid; e < plane; e += BLOCK) {
+                const int rr = a0 - 1 + e / W, j = e % W;
+                int8_t v = 0;
+                if (rr >= 0 && rr < a.arows && j < a.width) v = g[(size_t)rr * a.width + j];
+                s[e] = (unsigned char)v;
+            }
+        }
+
+    const bool has_top = cta > 0, has_bot = cta + 1 < nct;
+    const bool bot_edge = has_bot && !(has_top && nrows == 1);
+    // Update mask of band row rr / word w: rows 1..N-2, columns 1..width-2;
+    // Rotate positions: columns COFF..COFF+cols-1 (all band rows).
+    auto info_at = [&](int rr, int w) {
+        WordInfo wi;
+        wi.off = (rr + 1) * W + 4 * w;
+        const int i = a0 + rr;
+        wi.cls = M::DOM ? (i & 1) : i % 3;
+        const int j0 = 4 * w;
+        uint32_t ub = 0, vb = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int j = j0 + b;
+            if (j >= 1 && j <= a.width - 2) ub |= 1u << b;
+            if (j >= M::COFF && j < M::COFF + a.cols) vb |= 1u << b;
+        }
+        if (!(i >= 1 && i <= N - 2)) ub = 0;
+        wi.um = lane_bytes(ub) * 0xffu;
+        wi.vm = lane_bytes(vb);
+        return wi;
+    };
+    auto is_edge = [&](int u) {
+        const int rr = u / Gw;
+        return (has_top && rr == 0) || (bot_edge && rr == nrows - 1);
+    };
+    // Lozenge column shifts for each colour t whose Update is applied.
+    uint32_t shift_tab[3] = {0u, 0u, 0u};
+    if (!M::DOM) {
+        shift_tab[0] = lozenge_shift_table(0);
+        shift_tab[1] = lozenge_shift_table(1);
+        shift_tab[2] = lozenge_shift_table(2);
+    }
+    // This thread's share of the halo exchange: words e = tid + x * BLOCK of
+    // [side][lattice][word] (one array per phase in these models).
+    const int per_side = a.nlat * a.xwords;
+
+    // The words u = tid + m * BLOCK (m < MAXW) of this thread, their facts
+    // and (bit-exact mode) their positions' TinyMT states, all in registers.
+    // MAXW = 0 (fast mode on large bands): words are walked at run time.
+    constexpr int NW = MAXW > 0 ? MAXW : 1;
+    WordInfo winfo[NW];
+    TinyState st[PHILOX ? 1 : NW][4];
+    uint32_t wflags = 0;  // bit 2m: word m exists, bit 2m+1: it is an edge word
+    if (MAXW > 0) {
+#pragma unroll
+        for (int m = 0; m < MAXW; ++m) {
+            const int u = tid + m * BLOCK;
+            if (u < nwords) {
+                winfo[m] = info_at(u / Gw, u % Gw);
+                wflags |= (1u << (2 * m)) | ((is_edge(u) ? 1u : 0u) << (2 * m + 1));
+            } else {
+                winfo[m] = WordInfo{0, 0, 0u, 0u};
+            }
+        }
+    }
+    const TinyParams tp{a.mat1, a.mat2, a.tmat};
+
+    int epoch = -1;
+    int64_t next_epoch = a.nepochs > 0 ? a.epoch_start[0] : INT64_MAX;
+    uint32_t key0 = 0, key1 = 0;
+    int64_t dstep = 0;
+    uint64_t t0 = 0;
+    uint32_t d = a.nphases > 0 ? __ldg(a.phases) : 0u;
+    uint32_t d_prev = 0u;
+
+    __syncthreads();
+    for (int64_t ph = 0; ph < a.nphases; ++ph) {
+        const uint32_t d_next = ph + 1 < a.nphases ? __ldg(a.phases + ph + 1) : 0u;
+        if (ph == next_epoch) {
+            while (epoch + 1 < a.nepochs && a.epoch_start[epoch + 1] == ph) ++epoch;
+            next_epoch = epoch + 1 < a.nepochs ? a.epoch_start[epoch + 1] : INT64_MAX;
+            const uint64_t eseed = a.epoch_seed[epoch];
+            if (PHILOX) {
+                key0 = (uint32_t)eseed;
+                key1 = (uint32_t)(eseed >> 32);
+                dstep = 0;
+            } else {
+#pragma unroll
+                for (int m = 0; m < NW; ++m) {
+                    if (!(wflags & (1u << (2 * m)))) continue;
+                    const int rpos = r0 + winfo[m].off / W - 1;  // position row
+                    const int jw = winfo[m].off % W;             // 4 * word
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        if (!(winfo[m].vm & (1u << (8 * b)))) continue;
+                        const uint32_t sid = (uint32_t)(jw + b - M::COFF) + (uint32_t)a.cols * (uint32_t)rpos;
+                        tiny_seed(st[m][b], tp, (uint32_t)eseed + sid);
+                    }
+                }
+            }
+        }
+        const bool draws = (d & PH_DRAWS) != 0u;
+        WordPhase P;
+        {
+            const int op = (int)ph_op(d), ca = (int)ph_a(d), cb = (int)ph_b(d);
+            P.step = op == (int)OP_STEP;
+            P.upd = P.step ? (cb != (int)NO_COLOUR && cb != ca) : true;
+            const int tt = P.step ? (P.upd ? cb : 0) : ca;
+            if (M::DOM) {
+                // Reference colour r flips array 1 - r, then refreshes array r from it.
+                const int flip_arr = P.step ? 1 - ca : ca;
+                P.dst = lat + flip_arr * plane;
+                P.src = lat + (1 - flip_arr) * plane;
+                P.par = tt & 1;
+                P.keep_a = false;
+                P.shifts = 0u;
+                P.pa = P.pb = nullptr;
+            } else {
+                const int t1 = tt == 2 ? 0 : tt + 1, t2 = tt == 0 ? 2 : tt - 1;
+                P.dst = lat + ca * plane;
+                P.src = lat + tt * plane;
+                P.pa = lat + t1 * plane;
+                P.pb = lat + t2 * plane;
+                P.keep_a = P.step && P.upd && t1 == ca;
+                P.shifts = tt == 0 ? shift_tab[0] : tt == 1 ? shift_tab[1] : shift_tab[2];
+                P.par = 0;
+            }
+        }
+        const int lat1 = NC * plane;  // second lattice (coupled CFTP chains)
+        auto apply = [&](const WordInfo& wi, const uint32_t (&k)[4]) {
+            uint32_t m0 = 0, m1 = 0;
+            if (draws) {
+                m0 = below4(k, a.thr[0]);
+                if (!M::DOM) m1 = below4(k, a.thr[1]) & ~m0;
+            }
+            word_phase<FAM>(P, 0, W, wi, m0, m1);
+            if (a.nlat > 1) word_phase<FAM>(P, lat1, W, wi, m0, m1);
+        };
+        // Word m of this thread (u = tid + m * BLOCK of the band).
+        auto own_word = [&](int m) {
+            uint32_t k[4] = {0u, 0u, 0u, 0u};
+            if (draws) {
+                if (PHILOX) {
+                    const int u = tid + m * BLOCK;
+                    const uint4 w4 = philox4((uint32_t)(a0 * Gw + u), (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32),
+                                             a.chain, key0, key1);
+                    k[0] = w4.x >> 9;
+                    k[1] = w4.y >> 9;
+                    k[2] = w4.z >> 9;
+                    k[3] = w4.w >> 9;
+                } else {
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        if (winfo[m].vm & (1u << (8 * b))) k[b] = tiny_draw23(st[PHILOX ? 0 : m][b], tp);
+                }
+            }
+            apply(winfo[m], k);
+        };
+        auto philox_word = [&](int rr, int w) {
+            const WordInfo wi = info_at(rr, w);
+            uint32_t k[4] = {0u, 0u, 0u, 0u};
+            if (draws) {
+                const uint4 w4 = philox4((uint32_t)((a0 + rr) * Gw + w), (uint32_t)dstep,
+                                         (uint32_t)((uint64_t)dstep >> 32), a.chain, key0, key1);
+                k[0] = w4.x >> 9;
+                k[1] = w4.y >> 9;
+                k[2] = w4.z >> 9;
+                k[3] = w4.w >> 9;
+            }
+            apply(wi, k);
+        };
+        // Fast mode: words u = lo + tid + x * BLOCK < hi, walked with an
+        // incremental (row, word) pair.
+        auto philox_range = [&](int lo, int hi) {
+            int u = lo + tid;
+            if (u >= hi) return;
+            int rr = u / Gw, w = u - rr * Gw;
+            const int drr = BLOCK / Gw, dw = BLOCK - drr * Gw;
+            for (; u < hi; u += BLOCK) {
+                philox_word(rr, w);
+                rr += drr;
+                w += dw;
+                if (w >= Gw) {
+                    w -= Gw;
+                    ++rr;
+                }
+            }
+        };
+
+        // Words away from the band's edge rows first, overlapping the neighbours' progress.
+        if (MAXW == 0) {
+            const int lo = has_top ? Gw : 0;
+            philox_range(lo, max(lo, nwords - (has_bot ? Gw : 0)));
+        } else {
+#pragma unroll
+            for (int m = 0; m < NW; ++m)
+                if ((wflags >> (2 * m) & 3u) == 1u) own_word(m);
+        }
+        if (ph > 0) {
+            // Halo rows of the array the neighbours flipped in the previous phase.
+            const uint32_t mask = M::written(d_prev);
+            bool ok = true;
+            if (mask) {
+                const int arr = __ffs(mask) - 1;
+                const int par = (int)((ph - 1) & 1);
+                const uint32_t tag = (uint32_t)ph;
+                for (int e = tid; e < 2 * per_side && ok; e += BLOCK) {
+                    const int side = e >= per_side;  // 0: row above (from cta-1), 1: row below (from cta+1)
+                    const int rem = e - side * per_side;
+                    const int l = rem >= a.xwords;
+                    const int w = rem - l * a.xwords;
+                    const int src = side == 0 ? cta - 1 : cta + 1;
+                    if (src < 0 || src >= nct) continue;
+                    uint32_t v;
+                    ok = wait_word(a, slot(a, src, 1 - side, par, l, 0) + w, tag, &v, t0);
+                    if (ok) sts(lat + (l * NC + arr) * plane + (side == 0 ? 0 : nrows + 1) * W + 4 * w, v);
+                }
+            }
+            if (__syncthreads_or(!ok)) return;
+        }
+        if (MAXW == 0) {
+            if (has_top) philox_range(0, Gw);
+            if (bot_edge) philox_range(nwords - Gw, nwords);
+        } else {
+#pragma unroll
+            for (int m = 0; m < NW; ++m)
+                if ((wflags >> (2 * m) & 3u) == 3u) own_word(m);
+        }
+        __syncthreads();
+        if (ph + 1 < a.nphases) {
+            // Publish the band's first / last row of the array flipped in this phase.
+            const uint32_t mask = M::written(d);
+            if (mask) {
+                const int arr = __ffs(mask) - 1;
+                const int par = (int)(ph & 1);
+                const unsigned long long tag = (unsigned long long)(uint32_t)(ph + 1) << 32;
+                for (int e = tid; e < 2 * per_side; e += BLOCK) {
+                    const int side = e >= per_side;  // 0: first row (read by cta-1), 1: last row (read by cta+1)
+                    const int rem = e - side * per_side;
+                    const int l = rem >= a.xwords;
+                    const int w = rem - l * a.xwords;
+                    const int dst = side == 0 ? cta - 1 : cta + 1;
+                    if (dst < 0 || dst >= nct) continue;
+                    const unsigned char* row = lat + (l * NC + arr) * plane + (side == 0 ? 1 : nrows) * W;
+                    st_relaxed64(slot(a, cta, side, par, l, 0) + w, tag | lds(row + 4 * w));
+                }
+            }
+        }
+        if (PHILOX && draws) ++dstep;
+        d_prev = d;
+        d = d_next;
+    }
+
+    __syncthreads();
+    for (int l = 0; l < a.nlat; ++l)
+        for (int c = 0; c < NC; ++c) {
+            int8_t* g = static_cast<int8_t*>(a.arr[l][c]);
+            const unsigned char* s = lat + (l * NC + c) * plane;
+            for (int e = tid; e < nrows * a.width; e += BLOCK) {
+                const int rr = e / a.width, j = e % a.width;
+                g[(size_t)(a0 + rr) * a.width + j] = (int8_t)s[(rr + 1) * W + j];
+            }
+        }
+}
+
+using KernelFn = void (*)(WalkArgs);
+
+template <int FAM>
+static KernelFn word_fn(int maxw, bool philox) {
+    if (philox) {
+        switch (maxw) {
+            case 0: return word_kernel<FAM, 0, true, 1024>;
+            case 1: return word_kernel<FAM, 1, true, 1024>;
+            case 2: return word_kernel<FAM, 2, true, 1024>;
+            case 4: return word_kernel<FAM, 4, true, 1024>;
+            default: return nullptr;
+        }
+    }
+    switch (maxw) {
+        case 1: return word_kernel<FAM, 1, false, 1024>;
+        case 2: return word_kernel<FAM, 2, false, 512>;
+        case 4: return word_kernel<FAM, 4, false, 512>;
+        default: return nullptr;
+    }
+}
+
+static KernelFn word_kernel_for(int family, int maxw, bool philox) {
+    switch (family) {
+        case FAM_DOMINO: return word_fn<FAM_DOMINO>(maxw, philox);
+        case FAM_DOMINO_HB: return word_fn<FAM_DOMINO_HB>(maxw, philox);
+        case FAM_LOZENGE8: return word_fn<FAM_LOZENGE8>(maxw, philox);
+        default: return nullptr;
+    }
+}
+
+bool word_family(int family) { return family == FAM_DOMINO || family == FAM_DOMINO_HB || family == FAM_LOZENGE8; }
+
+rt_status plan_word_walk(int family, int device, int nlat, int rows, int width, bool philox, int ctas_hint,
+                         WalkPlan* plan, std::string* err) {
+    if (!word_family(family)) {
+        *err = "no word kernel for this model";
+        return RT_E_INVAL;
+    }
+    int sms = 0, smem_optin = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) {
+        *err = "cudaDeviceGetAttribute failed";
+        return RT_E_CUDA;
+    }
+    const int nc = family == FAM_LOZENGE8 ? 3 : 2;
+    const int wpad = (width + 3) & ~3;
+    const int gw = wpad / 4;
+    int ctas = std::max(1, std::min(ctas_hint > 0 ? ctas_hint : sms, rows));
+    const int rpc = (rows + ctas - 1) / ctas;
+    ctas = (rows + rpc - 1) / rpc;
+    const int words = rpc * gw;
+    // One word per thread up to 1024 threads; bit-exact mode then keeps 2
+    // or 4 words' generator states per thread in registers (512 threads).
+    int maxw = 1, block = 0;
+    if (philox) {
+        // Fast mode keeps no generator state: up to 4 words' facts per thread
+        // in registers, beyond that words are walked at run time.
+        maxw = words <= 1024 ? 1 : words <= 2048 ? 2 : words <= 4096 ? 4 : 0;
+        block = maxw == 0 ? 1024 : std::min(1024, ((words + maxw - 1) / maxw + 31) / 32 * 32);
+    } else if (words <= 1024) {
+        block = (words + 31) / 32 * 32;
+    } else {
+        for (maxw = 2; maxw <= 4; maxw *= 2)
+            if ((words + maxw - 1) / maxw <= kWordBlockMax) break;
+        if (maxw > 4) {
+            *err = "band too wide for register-resident generator states";
+            return RT_E_INVAL;
+        }
+        block = ((words + maxw - 1) / maxw + 31) / 32 * 32;
+    }
+    const size_t smem = 32 + (size_t)nlat * nc * (rpc + 2) * wpad;
+    if (smem > (size_t)smem_optin) {
+        *err = "band does not fit in shared memory";
+        return RT_E_INVAL;
+    }
+    KernelFn fn = word_kernel_for(family, maxw, philox);
+    if (!fn) {
+        *err = "no word kernel for this configuration";
+        return RT_E_INVAL;
+    }
+    if (cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
+        *err = "cudaFuncSetAttribute failed";
+        return RT_E_CUDA;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, block, smem) != cudaSuccess) {
+        *err = "cudaOccupancyMaxActiveBlocksPerMultiprocessor failed";
+        return RT_E_CUDA;
+    }
+    if (per_sm < 1 || ctas > per_sm * sms) {
+        *err = "word-kernel grid cannot be co-resident";
+        return RT_E_INVAL;
+    }
+    plan->items = maxw;
+    plan->block = block;
+    plan->rows_per_cta = rpc;
+    plan->ctas = ctas;
+    plan->smem = smem;
+    plan->wpad = wpad;
+    plan->xwords = wpad / 4;
+    plan->xslots = 1;
+    plan->fn = (const void*)fn;
+    return RT_OK;
+}
+
+}  // namespace rtb
