@@ -61,7 +61,7 @@ typedef struct {
     double q;            /* volume weight, qlozengekernel.cl:3 (0.99) */
     float weights[16];   /* rect-triangle face weights by digit, recttrianglekernel.cl:3-13 */
     int32_t device;      /* CUDA device ordinal */
-    int32_t reserved;
+    uint32_t chain;      /* fast mode: Philox counter word 3 (a chain's index in a batch); 0 otherwise */
     void* stream;        /* cudaStream_t to run on; NULL = the handle creates its own */
 } rt_config;
 

@@ -47,6 +47,9 @@ rt_status rt_domino_tiling_to_domain(const int32_t* t, int64_t tlen, int32_t* ou
 /* ---- lozenges (src/Lozenge/LozengeTiler.h:61-78) ---- */
 /* LozengeTiler::AlmostHexDomain(N, M), src/Lozenge/LozengeTiler.cpp:344-389 */
 rt_status rt_lozenge_almost_hex(int32_t side, int32_t cut, int32_t* out, int64_t cap, int64_t* len);
+/* Hexagon with sides a, b, c, a, b, c (generalises AlmostHexDomain(N, 0),
+ * which is a = b = c = N).  No reference counterpart. */
+rt_status rt_lozenge_hexagon(int32_t a, int32_t b, int32_t c, int32_t* out, int64_t cap, int64_t* len);
 /* LozengeTiler::DomainToVertices, src/Lozenge/LozengeTiler.cpp:405-434 */
 rt_status rt_lozenge_domain_to_vertices(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len);
 /* LozengeTiler::MaxTiling / MinTiling, src/Lozenge/LozengeTiler.cpp:140-318 */

@@ -45,7 +45,7 @@ class RtConfig(ctypes.Structure):
         ("q", ctypes.c_double),
         ("weights", ctypes.c_float * 16),
         ("device", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("chain", ctypes.c_uint32),
         ("stream", ctypes.c_void_p),
     ]
 
@@ -60,6 +60,29 @@ class RtCftpStats(ctypes.Structure):
 
 
 RT_CFTP_DOUBLING, RT_CFTP_REFERENCE = 0, 1
+
+
+class RtChain(ctypes.Structure):
+    _fields_ = [
+        ("model", ctypes.c_int32),
+        ("kernel", ctypes.c_int32),
+        ("chain", ctypes.c_uint32),
+        ("reserved", ctypes.c_int32),
+        ("key", ctypes.c_int64),
+    ]
+
+
+class RtBatchInfo(ctypes.Structure):
+    _fields_ = [
+        ("chains", ctypes.c_int32),
+        ("cluster", ctypes.c_int32 * 6),
+        ("block", ctypes.c_int32 * 6),
+        ("clusters", ctypes.c_int32 * 6),
+        ("tune_ms", ctypes.c_double),
+        ("run_ms", ctypes.c_double),
+        ("attempts", ctypes.c_int64),
+        ("algorithmic_bytes", ctypes.c_int64),
+    ]
 
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
@@ -100,6 +123,7 @@ HOST_SIGNATURES = {
     "rt_domino_tiling_to_height": [_P, _I64, _P, _I64],
     "rt_domino_tiling_to_domain": [_P, _I64],
     "rt_lozenge_almost_hex": [_I32, _I32],
+    "rt_lozenge_hexagon": [_I32, _I32, _I32],
     "rt_lozenge_domain_to_vertices": [_P, _I64],
     "rt_lozenge_max_tiling": [_P, _I64],
     "rt_lozenge_min_tiling": [_P, _I64],
@@ -137,6 +161,19 @@ SIGNATURES.update({
     "rt_tridimer_dimer_svg": (ctypes.c_int, [_P, _I64, _P, _I64, _S]),
     "rt_save_matrix": (ctypes.c_int, [_P, _I64, _S]),
     "rt_load_matrix": (ctypes.c_int, [_S, _P, _I64, _PL]),
+})
+
+# include/rt_b200_batch.h
+SIGNATURES.update({
+    "rt_batch_create": (ctypes.c_int, [_I32, ctypes.POINTER(_P)]),
+    "rt_batch_destroy": (ctypes.c_int, [_P]),
+    "rt_batch_add": (ctypes.c_int, [_P, ctypes.POINTER(RtChain), _P, _I32, _PL]),
+    "rt_batch_set_tuning": (ctypes.c_int, [_P, _I32, _I32, _I32]),
+    "rt_batch_run": (ctypes.c_int, [_P, _I64]),
+    "rt_batch_download": (ctypes.c_int, [_P, _I64, _P]),
+    "rt_batch_get_info": (ctypes.c_int, [_P, ctypes.POINTER(RtBatchInfo)]),
+    "rt_batch_last_error": (ctypes.c_char_p, [_P]),
+    "rt_mixed_chain_spec": (ctypes.c_int, [_I64, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
 })
 
 _lib = None

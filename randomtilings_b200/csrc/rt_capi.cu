@@ -83,6 +83,89 @@ uint32_t floor_scaled(double x, int e) {
 
 }  // namespace
 
+namespace rtb {
+
+// Phases of one triangle-dimer step (TriangleDimerTiler.cpp:243-347): the
+// flip family `kind` (0 lozenges, 1 triangles, 2 butterflies), orientation /
+// class r1, kind or parity r2, and for butterflies the slice p1 and parity p2.
+int64_t td_step_phases(uint32_t* ph, int64_t at, uint32_t kind, uint32_t r1, uint32_t r2, uint32_t p1, uint32_t p2) {
+    if (kind == 0) {  // lozenge flips, :243-278
+        ph[at++] = make_phase(TD_ROT_LOZ, r1, r2, true);
+        ph[at++] = make_phase(TD_LOZ_FLIPPED, r1, r2, false);
+        ph[at++] = make_phase(TD_LOZ_OTHER, r1, 0, false);
+        ph[at++] = make_phase(TD_UP_FROM_LOZ, 0, 0, false);
+        ph[at++] = make_phase(TD_TRI_OTHER, 0, 7, false);
+    } else if (kind == 1) {  // triangle flips, :279-305
+        ph[at++] = make_phase(TD_ROT_TRI, r2, r1, true);
+        ph[at++] = make_phase(TD_TRI_FLIPPED, r2, r1, false);
+        ph[at++] = make_phase(TD_TRI_OTHER, r2, 0, false);
+        ph[at++] = make_phase(TD_LOZ_FROM_TRI, 0, 0, false);
+        ph[at++] = make_phase(TD_BFLY_FROM_LOZ, 0, 7, false);
+    } else {  // butterfly flips, :306-347
+        ph[at++] = make_phase(TD_ROT_BFLY, r1, p1 | (p2 << 2), true);
+        ph[at++] = make_phase(TD_BFLY_SAME, r1, p1 | (p2 << 2), false);
+        ph[at++] = make_phase(TD_BFLY_21, r1, p1, false);
+        ph[at++] = make_phase(TD_BFLY_22, r1, p1, false);
+        ph[at++] = make_phase(TD_BFLY_23_LOZ, r1, p1, false);
+        ph[at++] = make_phase(TD_BFLY_FROM_LOZ, 1, 7u & ~(1u << r1), false);
+        ph[at++] = make_phase(TD_TRI_OTHER, 0, 0, false);
+    }
+    return at;
+}
+
+// Fast-mode step s of an epoch: dominoes flip the black array (0) on even
+// steps and the white one on odd steps (reference colour r flips array
+// 1 - r); lozenges and rectangle-triangles flip colour s mod 3; triangle
+// dimers make move s mod 30 of a sweep over every flip class.
+int64_t fast_step_phases(int kind, int64_t s, uint32_t* ph, int64_t at, uint32_t* prev) {
+    if (kind == 3) {
+        const uint32_t mv = (uint32_t)(s % 30);
+        if (mv < 6) return td_step_phases(ph, at, 0, mv / 2, mv % 2, 0, 0);
+        if (mv < 12) return td_step_phases(ph, at, 1, (mv - 6) % 3, (mv - 6) / 3, 0, 0);
+        return td_step_phases(ph, at, 2, (mv - 12) / 6, 0, ((mv - 12) / 2) % 3, (mv - 12) % 2);
+    }
+    const uint32_t r = kind == 0 ? (uint32_t)(1 - (s & 1)) : (uint32_t)(s % 3);
+    ph[at++] = make_phase(OP_STEP, r, *prev, true);
+    *prev = r;
+    return at;
+}
+
+void fast_phases(int kind, int64_t steps, std::vector<uint32_t>& ph) {
+    const size_t base = ph.size();
+    ph.resize(base + (size_t)(kind == 3 ? 7 * steps : steps + 1));
+    int64_t at = (int64_t)base;
+    uint32_t prev = NO_COLOUR;
+    for (int64_t s = 0; s < steps; ++s) at = fast_step_phases(kind, s, ph.data(), at, &prev);
+    if (kind != 3 && steps > 0) ph[at++] = make_phase(OP_FINAL, prev, NO_COLOUR, false);
+    ph.resize((size_t)at);
+}
+
+void family_thresholds(int family, double q, int qcmp, uint32_t thr[4]) {
+    thr[0] = thr[1] = thr[2] = thr[3] = 0;
+    switch (family) {
+        case FAM_DOMINO: thr[0] = below_threshold(0.8); break;     // dominokernel.cl:13
+        case FAM_DOMINO_HB: thr[0] = below_threshold(0.5); break;  // dominokernelCFTP.cl:22
+        case FAM_LOZENGE8:                                          // lozengekernel.cl:19-21
+            thr[0] = below_threshold(0.4);
+            thr[1] = below_threshold(0.8);
+            break;
+        case FAM_QLOZENGE32:  // qlozengekernel.cl:18-26
+            if (qcmp == RT_QCMP_DOUBLE) {
+                thr[0] = floor_scaled(q, 22);
+                thr[1] = floor_scaled(1.0 / q, 24);
+            } else {
+                const float qf = (float)q;
+                const float inv = 1.0f / qf;
+                thr[0] = floor_scaled((double)qf, 22);
+                thr[1] = floor_scaled((double)inv, 24);
+            }
+            break;
+        default: break;
+    }
+}
+
+}  // namespace rtb
+
 struct rt_tiler {
     rt_config cfg{};
     int family = 0;
@@ -412,35 +495,6 @@ static rt_status stage_params(rt_tiler* h, int64_t needed) {
     return RT_OK;
 }
 
-// Phases of one triangle-dimer step (TriangleDimerTiler.cpp:243-347): the
-// flip family `kind` (0 lozenges, 1 triangles, 2 butterflies), orientation /
-// class r1, kind or parity r2, and for butterflies the slice p1 and parity p2.
-static int64_t td_step_phases(uint32_t* ph, int64_t at, uint32_t kind, uint32_t r1, uint32_t r2, uint32_t p1,
-                              uint32_t p2) {
-    if (kind == 0) {  // lozenge flips, :243-278
-        ph[at++] = make_phase(TD_ROT_LOZ, r1, r2, true);
-        ph[at++] = make_phase(TD_LOZ_FLIPPED, r1, r2, false);
-        ph[at++] = make_phase(TD_LOZ_OTHER, r1, 0, false);
-        ph[at++] = make_phase(TD_UP_FROM_LOZ, 0, 0, false);
-        ph[at++] = make_phase(TD_TRI_OTHER, 0, 7, false);
-    } else if (kind == 1) {  // triangle flips, :279-305
-        ph[at++] = make_phase(TD_ROT_TRI, r2, r1, true);
-        ph[at++] = make_phase(TD_TRI_FLIPPED, r2, r1, false);
-        ph[at++] = make_phase(TD_TRI_OTHER, r2, 0, false);
-        ph[at++] = make_phase(TD_LOZ_FROM_TRI, 0, 0, false);
-        ph[at++] = make_phase(TD_BFLY_FROM_LOZ, 0, 7, false);
-    } else {  // butterfly flips, :306-347
-        ph[at++] = make_phase(TD_ROT_BFLY, r1, p1 | (p2 << 2), true);
-        ph[at++] = make_phase(TD_BFLY_SAME, r1, p1 | (p2 << 2), false);
-        ph[at++] = make_phase(TD_BFLY_21, r1, p1, false);
-        ph[at++] = make_phase(TD_BFLY_22, r1, p1, false);
-        ph[at++] = make_phase(TD_BFLY_23_LOZ, r1, p1, false);
-        ph[at++] = make_phase(TD_BFLY_FROM_LOZ, 1, 7u & ~(1u << r1), false);
-        ph[at++] = make_phase(TD_TRI_OTHER, 0, 0, false);
-    }
-    return at;
-}
-
 // Builds the phase list of `k` epochs and launches the walk.
 //
 // Bit-exact mode draws the colours as the reference's host loops do.  Fast
@@ -479,22 +533,7 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
         es[e] = at;
         if (fast) {
             sd[e] = (uint64_t)seeds[e];
-            for (int64_t s = 0; s < steps[e]; ++s) {
-                if (h->kind == 3) {
-                    const uint32_t mv = (uint32_t)(s % 30);
-                    if (mv < 6)
-                        at = td_step_phases(ph, at, 0, mv / 2, mv % 2, 0, 0);
-                    else if (mv < 12)
-                        at = td_step_phases(ph, at, 1, (mv - 6) % 3, (mv - 6) / 3, 0, 0);
-                    else
-                        at = td_step_phases(ph, at, 2, (mv - 12) / 6, 0, ((mv - 12) / 2) % 3, (mv - 12) % 2);
-                } else {
-                    // Domino colour r flips array 1 - r: black (array 0) on even steps.
-                    const uint32_t r = h->kind == 0 ? (uint32_t)(1 - (s & 1)) : (uint32_t)(s % 3);
-                    ph[at++] = make_phase(OP_STEP, r, prev, true);
-                    prev = r;
-                }
-            }
+            for (int64_t s = 0; s < steps[e]; ++s) at = fast_step_phases(h->kind, s, ph, at, &prev);
         } else if (h->kind == 0) {
             std::mt19937 mt_rand(seeds[e]);
             sd[e] = single_walk ? (uint32_t)mt_rand() : (uint32_t)seeds[e];  // DominoTiler.cpp:31-32 vs :81-82
@@ -581,7 +620,7 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     a.arows = h->arows;
     a.width = width;
     a.rng_kind = fast ? 1 : 0;
-    a.chain = 0;
+    a.chain = h->cfg.chain;
     a.params = uniform ? nullptr : static_cast<const uint4*>(h->d_params.p);
     a.mat1 = kMat1;
     a.mat2 = kMat2;
@@ -591,27 +630,7 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     a.epoch_start = static_cast<const int64_t*>(h->d_epoch_start.p);
     a.epoch_seed = static_cast<const uint64_t*>(h->d_epoch_seed.p);
     a.nepochs = k;
-    switch (h->family) {
-        case FAM_DOMINO: a.thr[0] = below_threshold(0.8); break;       // dominokernel.cl:13
-        case FAM_DOMINO_HB: a.thr[0] = below_threshold(0.5); break;    // dominokernelCFTP.cl:22
-        case FAM_LOZENGE8:                                              // lozengekernel.cl:19-21
-            a.thr[0] = below_threshold(0.4);
-            a.thr[1] = below_threshold(0.8);
-            break;
-        case FAM_QLOZENGE32: {  // qlozengekernel.cl:18-26
-            if (h->cfg.qcmp == RT_QCMP_DOUBLE) {
-                a.thr[0] = floor_scaled(h->cfg.q, 22);
-                a.thr[1] = floor_scaled(1.0 / h->cfg.q, 24);
-            } else {
-                const float qf = (float)h->cfg.q;
-                const float inv = 1.0f / qf;
-                a.thr[0] = floor_scaled((double)qf, 22);
-                a.thr[1] = floor_scaled((double)inv, 24);
-            }
-            break;
-        }
-        default: break;
-    }
+    family_thresholds(h->family, h->cfg.q, h->cfg.qcmp, a.thr);
     std::memcpy(a.weights, h->cfg.weights, sizeof a.weights);
     a.xbuf = static_cast<unsigned long long*>(h->d_xbuf.p);
     a.err = static_cast<int*>(h->d_err.p);

@@ -17,6 +17,7 @@
 #include <deque>
 #include <map>
 #include <string>
+#include <random>
 #include <vector>
 
 #include "../../include/rt_b200.h"
@@ -440,6 +441,34 @@ rt_status rt_lozenge_almost_hex(int32_t side, int32_t cut, int32_t* out, int64_t
     return emit(d3, out, cap, len);
 }
 
+// Hexagon with sides a (top), b, c, a, b, c in the triangle-row encoding of
+// AlmostHexDomain (LozengeTiler.cpp:344-388), which it generalises (a = b =
+// c = N gives AlmostHexDomain(N, 0)): b + c rows of 2a + 2b triangles; row i
+// starts at column max(0, 2b - 1 - 2i) (the upper-left side slants for b
+// rows, the lower-left one is vertical for c rows) and ends at column
+// 2a + 2b - 1 for i < c, then 2a + 2b - 2 - 2(i - c) (the upper-right side
+// is vertical for c rows, the lower-right one slants for b rows).  The same
+// padding as AlmostHexDomain follows.  No reference counterpart.
+rt_status rt_lozenge_hexagon(int32_t a, int32_t b, int32_t c, int32_t* out, int64_t cap, int64_t* len) {
+    if (a < 1 || b < 1 || c < 1) return RT_E_INVAL;
+    const int rows = b + c, cols = 2 * a + 2 * b;
+    Vec d((size_t)rows * cols, 0);
+    for (int i = 0; i < rows; ++i) {
+        const int lo = std::max(0, 2 * b - 1 - 2 * i);
+        const int hi = i < c ? 2 * a + 2 * b - 1 : 2 * a + 2 * b - 2 - 2 * (i - c);
+        for (int j = lo; j <= hi && j < cols; ++j) d[(size_t)i * cols + j] = 1;
+    }
+    // 3 rows / 6 triangles of padding, then a square array of side m3
+    // (vertex side divisible by 3) as LozengeTiler.cpp:370-388 builds it.
+    const int m2 = std::max(rows + 6, (cols + 12 + 1) / 2);
+    const int k = (3 - (m2 + 1) % 3) % 3;
+    const int m3 = m2 + k;
+    Vec d3((size_t)m3 * 2 * m3, 0);
+    for (int i = 0; i < rows; ++i)
+        for (int j = 0; j < cols; ++j) d3[(size_t)(i + 3) * 2 * m3 + j + 6] = d[(size_t)i * cols + j];
+    return emit(d3, out, cap, len);
+}
+
 rt_status rt_lozenge_domain_to_vertices(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
     const int m = isqrt_exact(dlen / 2);
     if (!d || m < 2 || (int64_t)2 * m * m != dlen) return RT_E_INVAL;
@@ -826,3 +855,35 @@ rt_status rt_tridimer_dimer_indicator(const int32_t* t, int64_t tlen, int32_t or
 }
 
 }  // extern "C"
+
+extern "C" rt_status rt_mixed_chain_spec(int64_t seed, int32_t* model, int32_t* p) {
+    if (!model || !p || seed < 0) return RT_E_INVAL;
+    std::mt19937 mt((std::mt19937::result_type)seed);
+    p[0] = p[1] = p[2] = 0;
+    switch (seed % 4) {
+        case 0: {
+            std::uniform_int_distribution<int> n(16, 256);
+            *model = RT_DOMINO;
+            p[0] = n(mt);
+            break;
+        }
+        case 1: {
+            std::uniform_int_distribution<int> side(8, 128);
+            *model = RT_LOZENGE;
+            p[0] = side(mt);
+            p[1] = side(mt);
+            p[2] = side(mt);
+            break;
+        }
+        case 2:
+            *model = RT_TRIDIMER;
+            p[0] = 64;
+            p[1] = 1;
+            break;
+        default:
+            *model = RT_RECTTRI;
+            p[0] = 64;
+            break;
+    }
+    return RT_OK;
+}

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/rt_b200.h"
 
@@ -43,6 +44,15 @@ rt_status plan_word_walk(int family, int device, int nlat, int rows, int width, 
 // kind: 0 domino, 1 lozenge, 2 rect-triangle, 3 triangle-dimer (merge only).
 rt_status launch_split(bool merge, int elem_bytes, int kind, int ncol, int n, int32_t* tiling, void* const* arr,
                        cudaStream_t stream, std::string* err);
+
+// Fast-mode schedules (rt_capi.cu).  kind: 0 domino, 1 lozenge,
+// 2 rect-triangle, 3 triangle dimer.  fast_step_phases appends the phases of
+// step s of an epoch; fast_phases appends a whole walk of `steps` steps
+// (with the final Update of the colour models).
+int64_t fast_step_phases(int kind, int64_t s, uint32_t* ph, int64_t at, uint32_t* prev);
+void fast_phases(int kind, int64_t steps, std::vector<uint32_t>& ph);
+// Integer acceptance thresholds of a kernel family on the 23-bit draw.
+void family_thresholds(int family, double q, int qcmp, uint32_t thr[4]);
 
 // Host split of a triangle-dimer tiling into its eight M x M arrays
 // (H, L, R, U, D, BH, BL, BR), rt_host.cpp.

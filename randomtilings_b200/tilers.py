@@ -45,7 +45,7 @@ class _Tiler:
     LoadMatrix = staticmethod(lambda f: builders.load_matrix(f))
 
     def __init__(self, device: int = 0, kernel: int = _capi.RT_KERNEL_DEFAULT, rng: int = _capi.RT_RNG_TINYMT,
-                 q: float = 0.99, qcmp: int = _capi.RT_QCMP_FLOAT32, weights=None, stream=None):
+                 q: float = 0.99, qcmp: int = _capi.RT_QCMP_FLOAT32, weights=None, stream=None, chain: int = 0):
         self._lib = _capi.load()
         cfg = _capi.RtConfig()
         self._lib.rt_config_default(ctypes.byref(cfg), self.MODEL)
@@ -54,6 +54,7 @@ class _Tiler:
         cfg.q = q
         cfg.qcmp = qcmp
         cfg.device = device
+        cfg.chain = chain
         if weights is not None:
             for i, w in enumerate(weights):
                 cfg.weights[i] = float(w)
@@ -171,6 +172,7 @@ class LozengeTiler(_Tiler):
 
     # static helpers (src/Lozenge/LozengeTiler.h:61-78)
     AlmostHexDomain = staticmethod(lambda n, m: builders.call("rt_lozenge_almost_hex", n, m))
+    Hexagon = staticmethod(lambda a, b, c: builders.call("rt_lozenge_hexagon", a, b, c))  # no reference counterpart
     MaxTiling = staticmethod(lambda d: builders.call("rt_lozenge_max_tiling", d))
     MinTiling = staticmethod(lambda d: builders.call("rt_lozenge_min_tiling", d))
     DomainToVertices = staticmethod(lambda d: builders.call("rt_lozenge_domain_to_vertices", d))

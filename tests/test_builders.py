@@ -103,3 +103,37 @@ def test_tridimer_cone_and_derived_states(n, m):
 @pytest.mark.parametrize("k", [0, 1, 2])
 def test_tridimer_test_butterfly(k):
     assert np.array_equal(T.TestButterfly(k), B[f"tridimer/butterfly{k}"])
+
+
+def _macmahon(a: int, b: int, c: int) -> int:
+    from fractions import Fraction
+
+    p = Fraction(1)
+    for i in range(1, a + 1):
+        for j in range(1, b + 1):
+            for k in range(1, c + 1):
+                p *= Fraction(i + j + k - 1, i + j + k - 2)
+    return int(p)
+
+
+def test_lozenge_hexagon_generalises_almost_hex():
+    import randomtilings_b200 as rt
+
+    for n in (1, 2, 5, 13):
+        assert np.array_equal(rt.LozengeTiler.Hexagon(n, n, n), rt.LozengeTiler.AlmostHexDomain(n, 0))
+
+
+@pytest.mark.parametrize("a,b,c", [(1, 1, 1), (2, 1, 1), (1, 2, 1), (1, 1, 2), (2, 2, 1), (1, 2, 3), (3, 1, 2),
+                                   (2, 3, 2)])
+def test_lozenge_hexagon_tilings(a, b, c):
+    """Extremal tilings of the a x b x c hexagon tile exactly its domain, and
+    chains started there reach MacMahon's number of tilings."""
+    import randomtilings_b200 as rt
+    from oracle import pyoracle as po
+
+    d = rt.LozengeTiler.Hexagon(a, b, c)
+    tmin, tmax = rt.LozengeTiler.MinTiling(d), rt.LozengeTiler.MaxTiling(d)
+    assert np.array_equal(rt.LozengeTiler.TilingToDomain(tmin), d)
+    assert np.array_equal(rt.LozengeTiler.TilingToDomain(tmax), d)
+    seen = {po.walk_fast("lozenge", t0, 60, key).tobytes() for key in range(300) for t0 in (tmin, tmax)}
+    assert len(seen) == _macmahon(a, b, c)
