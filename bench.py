@@ -261,6 +261,8 @@ def run_b200(args) -> None:
     algo_f = algorithmic_bytes_per_step(n, 1, rng_state=False) * STEPS_PER_WALK
     achieved_f = algo_f / (sum(ms_f) / len(ms_f) / 1e3) / 1e9
 
+    batched = None if args.no_batch else measure_batch(args, rank, world, dist, peaks()[0])
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(t0, seconds=args.cpu_seconds)
@@ -318,6 +320,7 @@ def run_b200(args) -> None:
                 "hbm_gbs_algorithmic": achieved_f,
                 "frac": achieved_f / peak,
             },
+            "batched": batched,
             "gpu_launches": int(launches) * args.steps,
             "phases_per_launch": int(phases),
             "clocks": clocks,
@@ -331,6 +334,53 @@ def run_b200(args) -> None:
     tf.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+def measure_batch(args, rank: int, world: int, dist, peak: float) -> dict:
+    """The batched pattern: args.batch_chains chains of the mixed workload
+    (chain seed s: domain type s mod 4, sizes from std::mt19937(s)), minimal
+    tilings, args.batch_sweeps sweeps each in fast mode, as one graph of one
+    persistent cluster launch per kernel family.  Ranks take seeds round-robin
+    (no communication); value = all ranks' attempts / max device time."""
+    import randomtilings_b200 as rt
+    from randomtilings_b200 import workloads
+
+    bt = rt.Batch(device=int(os.environ.get("LOCAL_RANK", "0")))
+    kinds = {}
+    for seed in range(rank, args.batch_chains, world):
+        model, t = workloads.mixed_chain(seed)
+        bt.add(model, t, key=seed, chain=seed)
+        kinds[model] = kinds.get(model, 0) + 1
+    bt.run(2)  # autotuner (on a scratch copy) + graph build; then a short warm-up run
+    bt.run(2)
+    barrier(dist)
+    bt.run(args.batch_sweeps)
+    info = bt.info()
+    bt.close()
+    ms = all_max(dist, info["run_ms"])
+    total_attempts, total_bytes = float(info["attempts"]), float(info["algorithmic_bytes"])
+    if dist is not None:
+        import torch
+
+        x = torch.tensor([total_attempts, total_bytes], dtype=torch.float64, device="cuda")
+        dist.all_reduce(x)
+        total_attempts, total_bytes = float(x[0]), float(x[1])
+    achieved = total_bytes / world / (ms / 1e3) / 1e9  # per GPU
+    return {
+        "workload": f"{args.batch_chains} chains of the mixed workload (seed s: s mod 4 -> Aztec diamond n in "
+                    "[16,256] / hexagon a,b,c in [8,128] / triangle-dimer IceCreamCone(64,1) / rectangle-triangle "
+                    f"hexagon 64; sizes from std::mt19937(s)), minimal tilings, {args.batch_sweeps} sweeps, "
+                    "fast mode (Philox), one CUDA graph",
+        "chains_per_model_rank0": {str(k): v for k, v in sorted(kinds.items())},
+        "value": total_attempts / (ms / 1e3),
+        "unit": "attempts/s",
+        "ms": ms,
+        "hbm_gbs_algorithmic": achieved,
+        "frac": achieved / peak,
+        "plans_rank0": info["plans"],
+        "tune_ms_rank0": info["tune_ms"],
+        "graph_launches": 1,
+    }
 
 
 def cpu_baseline(t0: np.ndarray, seconds: float = 15.0, threads: int | None = None) -> dict:
@@ -415,6 +465,9 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--traffic", type=float, default=None,
                     help="dram bytes per walk launch from an ncu capture (reported in roofline.traffic)")
+    ap.add_argument("--batch-chains", type=int, default=4096)
+    ap.add_argument("--batch-sweeps", type=int, default=5000)
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--walk-steps", type=int, default=STEPS_PER_WALK,
                     help="colour steps per walk (default 60000 = 20000 sweeps; smaller only for profiling captures)")
     args = ap.parse_args()
