@@ -61,6 +61,7 @@ def oracle() -> ctypes.CDLL:
                                               ctypes.c_double, ctypes.c_int]
         lib.orc_recttri_walk_fast.argtypes = [_P, ctypes.c_int, _I64, _I64, ctypes.c_uint32, _P]
         lib.orc_tridimer_walk_fast.argtypes = [_P, ctypes.c_int, _I64, _I64, ctypes.c_uint32]
+        lib.orc_project_heights.argtypes = [ctypes.c_int, _P, _I64, _P, _P, _P, _P, ctypes.c_int, _P]
         lib.orc_tinymt_init.argtypes = [_P, ctypes.c_uint32]
         lib.orc_tinymt_bits12.argtypes = [_P]
         lib.orc_tinymt_bits12.restype = ctypes.c_uint32
@@ -232,6 +233,20 @@ def cftp(tmax, tmin, first_steps: int, master_seed: int, schedule: str = "doubli
         steps.insert(0, 2 * steps[-1] if schedule == "reference" else sum(steps))
         seeds.insert(0, int(seeds_out[trial + 1]))
     return top, max_trials, sum(steps), False
+
+
+def project_heights(model: str, domain, hmin, hmax, target) -> np.ndarray:
+    """The oracle's height projection; model "domino" or "lozenge"."""
+    d = np.ascontiguousarray(domain, dtype=np.int32).reshape(-1)
+    lo = np.ascontiguousarray(hmin, dtype=np.int32).reshape(-1)
+    hi = np.ascontiguousarray(hmax, dtype=np.int32).reshape(-1)
+    t = np.ascontiguousarray(target, dtype=np.float32).reshape(-1)
+    n = int(round(lo.size ** 0.5))
+    out = np.zeros(n * n, dtype=np.int32)
+    _check(oracle().orc_project_heights(0 if model == "domino" else 1, d.ctypes.data, d.size, lo.ctypes.data,
+                                        hi.ctypes.data, t.ctypes.data, out.ctypes.data, n, None),
+           "orc_project_heights")
+    return out
 
 
 # ---- the reference's own code (oracle/_ref) --------------------------------

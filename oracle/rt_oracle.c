@@ -11,6 +11,7 @@
  */
 #include "rt_oracle.h"
 
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -1156,4 +1157,122 @@ int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint
 
 int orc_tridimer_walk_fast(int32_t* t, int n, int64_t steps, int64_t key, uint32_t chain) {
     return tridimer_run(t, n, steps, key, NULL, 0, 1, chain);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Height-function projection (no reference counterpart; the checker of    */
+/* rt_project_heights).  Graph: DominoTiler::DomainToVertices               */
+/* (DominoTiler.cpp:479-500) / LozengeTiler::DomainToVertices               */
+/* (LozengeTiler.cpp:405-434) for the vertex kinds, and the edges           */
+/* TilingToHeightfunc walks (DominoTiler.cpp:204-206,423-458;               */
+/* LozengeTiler.cpp:12-16,95-138): neighbour inside and one of the two      */
+/* faces beside the edge in the domain.  Edge step s: dominoes              */
+/* (nb > 1 ? 1 : -1) * ((i+j) even ? 1 : -1), lozenges dh[nb].              */
+/* ------------------------------------------------------------------------ */
+static const int kPDomN[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+static const int kPDomF[4][2][2] = {{{0, -1}, {0, 0}}, {{-1, -1}, {-1, 0}}, {{-1, 0}, {0, 0}}, {{-1, -1}, {0, -1}}};
+static const int kPLozN[6][2] = {{0, 1}, {-1, 1}, {-1, 0}, {0, -1}, {1, -1}, {1, 0}};
+static const int kPLozS[6] = {-1, 1, -1, 1, -1, 1};
+static const int kPLozF[6][2][2] = {{{0, 0}, {-1, 1}}, {{-1, 1}, {-1, 0}}, {{-1, 0}, {-1, -1}},
+                                    {{-1, -1}, {0, -2}}, {{0, -2}, {0, -1}}, {{0, -1}, {0, 0}}};
+
+static int p_dface(const int32_t* d, int m, int i, int j) { return i >= 0 && j >= 0 && i < m && j < m ? d[i * m + j] != 0 : 0; }
+static int p_lface(const int32_t* d, int m, int r, int c) {
+    return r >= 0 && c >= 0 && r < m && c < 2 * m ? d[r * 2 * m + c] != 0 : 0;
+}
+
+int orc_project_heights(int model, const int32_t* d, int64_t dlen, const int32_t* hmin, const int32_t* hmax,
+                        const float* target, int32_t* out, int n, int64_t* passes_out) {
+    const int dom = model == 0;
+    const int m = n - 1;
+    if ((dom && (int64_t)m * m != dlen) || (!dom && (int64_t)2 * m * m != dlen) || m < 2) return ORC_EINVAL;
+    const int nb_count = dom ? 4 : 6, M = dom ? 4 : 3;
+    uint8_t* kind = (uint8_t*)calloc((size_t)n * n, 1);
+    uint8_t* edges = (uint8_t*)calloc((size_t)n * n, 1);
+    if (!kind || !edges) {
+        free(kind);
+        free(edges);
+        return ORC_ENOMEM;
+    }
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            int k = 0;
+            if (dom) {
+                if (i == 0 || j == 0 || i == m || j == m) {
+                    const int i0 = i - (i == m), i1 = i - 1 + (i == 0), j0 = j - (j == m), j1 = j - 1 + (j == 0);
+                    if (p_dface(d, m, i0, j0) || p_dface(d, m, i1, j0) || p_dface(d, m, i0, j1) || p_dface(d, m, i1, j1))
+                        k = 2;
+                } else {
+                    const int c = p_dface(d, m, i - 1, j - 1) + p_dface(d, m, i - 1, j) + p_dface(d, m, i, j - 1) +
+                                  p_dface(d, m, i, j);
+                    k = c == 4 ? 1 : c > 0 ? 2 : 0;
+                }
+            } else if (!(i == 0 || j == 0 || i == m || j == m)) {
+                const int c = p_lface(d, m, i, 2 * j) + p_lface(d, m, i, 2 * j - 1) + p_lface(d, m, i, 2 * j - 2) +
+                              p_lface(d, m, i - 1, 2 * j) + p_lface(d, m, i - 1, 2 * j + 1) + p_lface(d, m, i - 1, 2 * j - 1);
+                k = c == 6 ? 1 : c > 0 ? 2 : 0;
+            }
+            kind[i * n + j] = (uint8_t)k;
+        }
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            if (!kind[i * n + j]) continue;
+            for (int nb = 0; nb < nb_count; ++nb) {
+                const int i2 = i + (dom ? kPDomN[nb][0] : kPLozN[nb][0]), j2 = j + (dom ? kPDomN[nb][1] : kPLozN[nb][1]);
+                if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n || !kind[i2 * n + j2]) continue;
+                int in;
+                if (dom)
+                    in = p_dface(d, m, i + kPDomF[nb][0][0], j + kPDomF[nb][0][1]) ||
+                         p_dface(d, m, i + kPDomF[nb][1][0], j + kPDomF[nb][1][1]);
+                else
+                    in = p_lface(d, m, i + kPLozF[nb][0][0], 2 * j + kPLozF[nb][0][1]) ||
+                         p_lface(d, m, i + kPLozF[nb][1][0], 2 * j + kPLozF[nb][1][1]);
+                if (in) edges[i * n + j] |= (uint8_t)(1u << nb);
+            }
+        }
+    /* 1. residue rounding, clamped; boundary vertices fixed at h_min */
+    for (int64_t v = 0; v < (int64_t)n * n; ++v) {
+        if (!kind[v]) {
+            out[v] = INT32_MAX;
+        } else if (kind[v] == 2) {
+            out[v] = hmin[v];
+        } else {
+            const double q = floor(((double)target[v] - (double)hmin[v]) / (double)M + 0.5);
+            double g = (double)hmin[v] + (double)M * q;
+            if (g < (double)hmin[v]) g = (double)hmin[v];
+            if (g > (double)hmax[v]) g = (double)hmax[v];
+            out[v] = (int32_t)g;
+        }
+    }
+    /* 2. min-plus relaxation of the interior vertices, in place, until a pass changes nothing */
+    int64_t passes = 0;
+    int changed = 1;
+    while (changed) {
+        changed = 0;
+        ++passes;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                const int64_t v = (int64_t)i * n + j;
+                if (kind[v] != 1) continue;
+                int32_t best = out[v];
+                for (int nb = 0; nb < nb_count; ++nb) {
+                    if (!(edges[v] & (1u << nb))) continue;
+                    const int i2 = i + (dom ? kPDomN[nb][0] : kPLozN[nb][0]), j2 = j + (dom ? kPDomN[nb][1] : kPLozN[nb][1]);
+                    const int s = dom ? (nb > 1 ? 1 : -1) * (((i + j) % 2 == 0) ? 1 : -1) : kPLozS[nb];
+                    const int32_t cand = out[(int64_t)i2 * n + j2] + (s == -1 ? 1 : M - 1);
+                    if (cand < best) best = cand;
+                }
+                if (best < out[v]) {
+                    out[v] = best;
+                    changed = 1;
+                }
+            }
+    }
+    /* 3. back up to h_min */
+    for (int64_t v = 0; v < (int64_t)n * n; ++v)
+        if (kind[v] && out[v] < hmin[v]) out[v] = hmin[v];
+    if (passes_out) *passes_out = passes;
+    free(kind);
+    free(edges);
+    return ORC_OK;
 }

@@ -85,6 +85,12 @@ int orc_lozenge_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t
 int orc_recttri_walk_fast(int32_t* t, int n, int64_t steps, int64_t key, uint32_t chain, const float* weights);
 int orc_tridimer_walk_fast(int32_t* t, int n, int64_t steps, int64_t key, uint32_t chain);
 
+/* Exact projection of a real height surface onto a valid height function
+ * (the checker of rt_project_heights): model 0 dominoes, 1 lozenges; n the
+ * vertex side; hmin / hmax the extremal height functions. */
+int orc_project_heights(int model, const int32_t* d, int64_t dlen, const int32_t* hmin, const int32_t* hmax,
+                        const float* target, int32_t* out, int n, int64_t* passes);
+
 /* Colour schedules the host loops draw (one entry per step). */
 int orc_domino_colours(int64_t seed, int64_t steps, int single_walk, uint8_t* out);
 int orc_lozenge_colours(int64_t seed, int64_t steps, uint8_t* out);

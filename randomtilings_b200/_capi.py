@@ -176,6 +176,16 @@ SIGNATURES.update({
     "rt_mixed_chain_spec": (ctypes.c_int, [_I64, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
 })
 
+
+class RtProjectStats(ctypes.Structure):
+    _fields_ = [("passes", ctypes.c_int64), ("lowered", ctypes.c_int64), ("raised", ctypes.c_int64),
+                ("device_ms", ctypes.c_double)]
+
+
+# include/rt_b200_project.h
+SIGNATURES["rt_project_heights"] = (ctypes.c_int, [_I32, _P, _I64, _P, _P, _P, _P, _I64, _I32,
+                                                   ctypes.POINTER(RtProjectStats)])
+
 _lib = None
 
 

@@ -887,3 +887,65 @@ extern "C" rt_status rt_mixed_chain_spec(int64_t seed, int32_t* model, int32_t* 
     }
     return RT_OK;
 }
+
+namespace rtb {
+
+// The graph the height-function projection relaxes over (rt_project.cu):
+// vertex side *n, per vertex its kind (0 outside the domain, 1 interior,
+// 2 boundary -- as DomainToVertices marks them) and a bit per neighbour
+// direction whose edge touches the domain with both ends inside it.
+// Directions: dominoes (i+1, j), (i-1, j), (i, j+1), (i, j-1); lozenges
+// (i, j+1), (i-1, j+1), (i-1, j), (i, j-1), (i+1, j-1), (i+1, j).
+bool lipschitz_graph(int model, const int32_t* d, int64_t dlen, int* n_out, std::vector<uint8_t>* kind,
+                     std::vector<uint8_t>* edges) {
+    if (!d) return false;
+    if (model == RT_DOMINO) {
+        const int m = isqrt_exact(dlen);
+        if (m < 1) return false;
+        const int n = m + 1;
+        const Vec D(d, d + dlen);
+        const Vec verts = dom_vertices(D, m);
+        kind->assign((size_t)n * n, 0);
+        edges->assign((size_t)n * n, 0);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                const int v = i * n + j;
+                (*kind)[v] = (uint8_t)verts[v];
+                if (!verts[v]) continue;
+                for (int nb = 0; nb < 4; ++nb) {
+                    const int i2 = i + kDomDi[nb], j2 = j + kDomDj[nb];
+                    if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n || !verts[i2 * n + j2]) continue;
+                    int f[4];
+                    dom_edge_faces(i, j, nb, f);
+                    if (dom_face(D, m, f[0], f[1]) || dom_face(D, m, f[2], f[3])) (*edges)[v] |= (uint8_t)(1u << nb);
+                }
+            }
+        *n_out = n;
+        return true;
+    }
+    if (model == RT_LOZENGE) {
+        const int m = isqrt_exact(dlen / 2);
+        if (m < 2 || (int64_t)2 * m * m != dlen) return false;
+        const int n = m + 1;
+        const Vec D(d, d + dlen);
+        const Vec verts = loz_vertices(D, m);
+        kind->assign((size_t)n * n, 0);
+        edges->assign((size_t)n * n, 0);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                const int v = i * n + j;
+                (*kind)[v] = (uint8_t)verts[v];
+                if (!verts[v]) continue;
+                for (int nb = 0; nb < 6; ++nb) {
+                    const int i2 = i + kLozDi[nb], j2 = j + kLozDj[nb];
+                    if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n || !verts[i2 * n + j2]) continue;
+                    if (loz_edge_in(D, m, i, j, nb, false)) (*edges)[v] |= (uint8_t)(1u << nb);
+                }
+            }
+        *n_out = n;
+        return true;
+    }
+    return false;
+}
+
+}  // namespace rtb

@@ -54,6 +54,11 @@ void fast_phases(int kind, int64_t steps, std::vector<uint32_t>& ph);
 // Integer acceptance thresholds of a kernel family on the 23-bit draw.
 void family_thresholds(int family, double q, int qcmp, uint32_t thr[4]);
 
+// Vertex kinds and in-domain edge bits of a domino / lozenge domain
+// (rt_host.cpp), the graph of the height-function projection.
+bool lipschitz_graph(int model, const int32_t* d, int64_t dlen, int* n_out, std::vector<uint8_t>* kind,
+                     std::vector<uint8_t>* edges);
+
 // Host split of a triangle-dimer tiling into its eight M x M arrays
 // (H, L, R, U, D, BH, BL, BR), rt_host.cpp.
 void td_split_host(const int32_t* t, int n, int32_t* arrays);
