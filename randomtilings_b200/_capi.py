@@ -186,6 +186,21 @@ class RtProjectStats(ctypes.Structure):
 SIGNATURES["rt_project_heights"] = (ctypes.c_int, [_I32, _P, _I64, _P, _P, _P, _P, _I64, _I32,
                                                    ctypes.POINTER(RtProjectStats)])
 
+# include/rt_b200_mlp.h
+RT_MLP_IN, RT_MLP_WIDTH = 8, 128
+RT_MLP_PARAMS = 128 * 8 + 128 + 128 * 128 + 128 + 128 * 128 + 128 + 128 + 1
+SIGNATURES.update({
+    "rt_mlp_create": (ctypes.c_int, [_I32, ctypes.c_uint64, ctypes.POINTER(_P)]),
+    "rt_mlp_destroy": (ctypes.c_int, [_P]),
+    "rt_mlp_get_params": (ctypes.c_int, [_P, _P]),
+    "rt_mlp_set_params": (ctypes.c_int, [_P, _P]),
+    "rt_mlp_predict": (ctypes.c_int, [_P, _P, _I64, _P]),
+    "rt_mlp_loss_grad": (ctypes.c_int, [_P, _P, _P, _I64, ctypes.POINTER(ctypes.c_float), _P]),
+    "rt_mlp_set_data": (ctypes.c_int, [_P, _P, _P, _I64]),
+    "rt_mlp_train": (ctypes.c_int, [_P, _I64, _I32, ctypes.c_float, ctypes.c_uint64,
+                                    ctypes.POINTER(ctypes.c_float)]),
+})
+
 _lib = None
 
 

@@ -1,0 +1,559 @@
+// rt_mlp.cu -- training and inference kernels of the coordinate MLP
+// (include/rt_b200_mlp.h).
+//
+// Layers 1 and 2 (128 x 128) are tensor-core GEMMs: a CTA of four warps
+// computes a 64 x 64 tile of C = A * B with mma.sync m16n8k16 (BF16 inputs,
+// FP32 accumulators), A and B staged through shared memory 32 columns of K
+// at a time; each GEMM names its operands' layouts, so one kernel serves
+// the forward product X * W^T, the input gradient dZ * W and the weight
+// gradient dZ^T * X (the last split over K, reduced with FP32 atomics).
+// Epilogues fuse bias + GELU (forward) and the GELU derivative (backward).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/rt_b200_mlp.h"
+#include "rt_device.cuh"
+
+namespace rtb {
+namespace mlp {
+
+constexpr int IN = RT_MLP_IN;
+constexpr int H = RT_MLP_WIDTH;
+// Offsets into the FP32 parameter vector.
+constexpr int OW0 = 0, OB0 = OW0 + H * IN, OW1 = OB0 + H, OB1 = OW1 + H * H, OW2 = OB1 + H, OB2 = OW2 + H * H,
+              OW3 = OB2 + H, OB3 = OW3 + H, NPARAM = OB3 + 1;
+static_assert(NPARAM == RT_MLP_PARAMS, "parameter layout");
+
+// GELU, tanh form: 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))).
+__device__ __forceinline__ float gelu(float z) {
+    const float u = 0.7978845608f * (z + 0.044715f * z * z * z);
+    return 0.5f * z * (1.0f + tanhf(u));
+}
+__device__ __forceinline__ float gelu_grad(float z) {
+    const float u = 0.7978845608f * (z + 0.044715f * z * z * z);
+    const float t = tanhf(u);
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * 0.7978845608f * (1.0f + 3.0f * 0.044715f * z * z);
+}
+
+// ---------------------------------------------------------------------------
+// Operand access.  A matrix operand is (ptr, ld, trans): element (r, c) of
+// the logical matrix is ptr[r * ld + c], or ptr[c * ld + r] when trans.
+// ---------------------------------------------------------------------------
+struct Op {
+    const __nv_bfloat16* p;
+    int ld;
+    int trans;
+};
+__device__ __forceinline__ __nv_bfloat16 op_at(const Op& o, int r, int c) {
+    return o.trans ? o.p[(size_t)c * o.ld + r] : o.p[(size_t)r * o.ld + c];
+}
+
+__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+enum Epi : int {
+    EPI_FWD = 0,     // z = acc + bias[n]; out_f = z; out_h = bf16(gelu(z))
+    EPI_DGELU = 1,   // d = acc * gelu'(zin[m][n]); out_f = d; out_h = bf16(d)
+    EPI_ATOMIC = 2   // out_f[m][n] += acc (weight gradients, split over K)
+};
+
+struct GemmArgs {
+    Op A, B;        // C[M][N] = A[M][K] * B[K][N]
+    int M, N, K;
+    int ksplit;     // K range per blockIdx.z
+    int epi;
+    const float* bias;
+    const float* zin;   // EPI_DGELU: pre-activation [M][N]
+    float* out_f;       // [M][N]
+    __nv_bfloat16* out_h;  // [M][N] (EPI_FWD, EPI_DGELU)
+};
+
+constexpr int TM = 64, TN = 64, TK = 32, PAD = 8;
+
+__global__ void __launch_bounds__(128) gemm_bf16(const __grid_constant__ GemmArgs g) {
+    __shared__ __align__(16) __nv_bfloat16 sA[TM][TK + PAD];  // [m][k]
+    __shared__ __align__(16) __nv_bfloat16 sB[TN][TK + PAD];  // [n][k]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+    const int k_begin = blockIdx.z * g.ksplit, k_end = min(g.K, k_begin + g.ksplit);
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;  // warp tile 32 x 32
+    const int grp = lane >> 2, tig = lane & 3;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int x = 0; x < 4; ++x) acc[i][j][x] = 0.0f;
+
+    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+    for (int k0 = k_begin; k0 < k_end; k0 += TK) {
+        for (int e = tid; e < TM * TK; e += 128) {
+            const int r = e / TK, c = e % TK;
+            const int gm = m0 + r, gk = k0 + c;
+            sA[r][c] = (gm < g.M && gk < k_end) ? op_at(g.A, gm, gk) : zero;
+        }
+        for (int e = tid; e < TN * TK; e += 128) {
+            const int r = e / TK, c = e % TK;  // r = n, c = k
+            const int gn = n0 + r, gk = k0 + c;
+            sB[r][c] = (gn < g.N && gk < k_end) ? op_at(g.B, gk, gn) : zero;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < TK; kk += 16) {
+            uint32_t a[2][4], b[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int r = wm + 16 * i + grp;
+                a[i][0] = pack2(sA[r][kk + 2 * tig], sA[r][kk + 2 * tig + 1]);
+                a[i][1] = pack2(sA[r + 8][kk + 2 * tig], sA[r + 8][kk + 2 * tig + 1]);
+                a[i][2] = pack2(sA[r][kk + 2 * tig + 8], sA[r][kk + 2 * tig + 9]);
+                a[i][3] = pack2(sA[r + 8][kk + 2 * tig + 8], sA[r + 8][kk + 2 * tig + 9]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int nn = wn + 8 * j + grp;
+                b[j][0] = pack2(sB[nn][kk + 2 * tig], sB[nn][kk + 2 * tig + 1]);
+                b[j][1] = pack2(sB[nn][kk + 2 * tig + 8], sB[nn][kk + 2 * tig + 9]);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) mma16816(acc[i][j], a[i], b[j]);
+        }
+        __syncthreads();
+    }
+    // Accumulator (i, j, x): row wm + 16 i + grp + 8 (x >> 1), column wn + 8 j + 2 tig + (x & 1).
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int x = 0; x < 4; ++x) {
+                const int m = m0 + wm + 16 * i + grp + 8 * (x >> 1);
+                const int n = n0 + wn + 8 * j + 2 * tig + (x & 1);
+                if (m >= g.M || n >= g.N) continue;
+                const float v = acc[i][j][x];
+                const size_t at = (size_t)m * g.N + n;
+                if (g.epi == EPI_FWD) {
+                    const float z = v + g.bias[n];
+                    g.out_f[at] = z;
+                    g.out_h[at] = __float2bfloat16(gelu(z));
+                } else if (g.epi == EPI_DGELU) {
+                    const float d = v * gelu_grad(g.zin[at]);
+                    g.out_f[at] = d;
+                    g.out_h[at] = __float2bfloat16(d);
+                } else {
+                    atomicAdd(g.out_f + at, v);
+                }
+            }
+}
+
+// Layer 0 (IN -> H), FP32: z0 = x W0^T + b0, h1 = bf16(gelu(z0)).
+__global__ void layer0_fwd(const float* __restrict__ x, const float* __restrict__ P, int n, float* z0,
+                           __nv_bfloat16* h1) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)n * H) return;
+    const int r = (int)(e / H), o = (int)(e % H);
+    float z = P[OB0 + o];
+#pragma unroll
+    for (int k = 0; k < IN; ++k) z += P[OW0 + o * IN + k] * x[(size_t)r * IN + k];
+    z0[e] = z;
+    h1[e] = __float2bfloat16(gelu(z));
+}
+
+// Layer 3 (H -> 1), FP32, one warp per row: y = h3 . W3 + b3; with a target,
+// also dy = 2 (y - t) / n and the mean squared error (one atomic per block).
+__global__ void layer3_fwd(const __nv_bfloat16* __restrict__ h3, const float* __restrict__ P, int n, float* y,
+                           const float* __restrict__ target, float* dy, float* loss) {
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    __shared__ float part[32];
+    float err = 0.0f;
+    if (row < n) {
+        float s = 0.0f;
+        for (int k = lane; k < H; k += 32) s += __bfloat162float(h3[(size_t)row * H + k]) * P[OW3 + k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        const float v = s + P[OB3];
+        if (lane == 0) {
+            if (y) y[row] = v;
+            if (target) {
+                const float e = v - target[row];
+                dy[row] = 2.0f * e / (float)n;
+                err = e * e / (float)n;
+            }
+        }
+    }
+    if (!target) return;
+    if (lane == 0) part[threadIdx.x >> 5] = err;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
+        atomicAdd(loss, t);
+    }
+}
+
+// Backward of layer 3, elementwise: dz2 = dy W3 * gelu'(z2) (FP32 and BF16).
+__global__ void layer3_bwd(const float* __restrict__ z2, const float* __restrict__ dy, const float* __restrict__ P,
+                           int n, float* dz2, __nv_bfloat16* dz2h) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)n * H) return;
+    const int r = (int)(e / H), k = (int)(e % H);
+    const float g = dy[r] * P[OW3 + k] * gelu_grad(z2[e]);
+    dz2[e] = g;
+    dz2h[e] = __float2bfloat16(g);
+}
+
+// Output-layer weights: G[W3][k] = sum_r dy[r] h3[r][k] (block k < H), and
+// G[b3] = sum_r dy[r] (block H).
+__global__ void layer3_wgrad(const __nv_bfloat16* __restrict__ h3, const float* __restrict__ dy, int n, float* G) {
+    const int k = blockIdx.x;
+    float s = 0.0f;
+    for (int r = threadIdx.x; r < n; r += blockDim.x)
+        s += dy[r] * (k < H ? __bfloat162float(h3[(size_t)r * H + k]) : 1.0f);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ float part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
+        G[k < H ? OW3 + k : OB3] += t;
+    }
+}
+
+// Bias gradient: G[off + c] += sum_r d[r][c].
+__global__ void bias_grad(const float* __restrict__ d, int n, float* G, int off) {
+    const int c = blockIdx.x;
+    float s = 0.0f;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) s += d[(size_t)r * H + c];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ float part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
+        G[off + c] += t;
+    }
+}
+
+// Layer 0 weights: G[W0] += dz0^T x, G[b0] by bias_grad.
+__global__ void layer0_wgrad(const float* __restrict__ dz0, const float* __restrict__ x, int n, float* G) {
+    const int o = blockIdx.x, k = threadIdx.x & 7, part = threadIdx.x >> 3;  // 256 threads: 32 parts x 8 inputs
+    float s = 0.0f;
+    for (int r = part; r < n; r += 32) s += dz0[(size_t)r * H + o] * x[(size_t)r * IN + k];
+    __shared__ float red[32][IN];
+    red[part][k] = s;
+    __syncthreads();
+    if (part == 0) {
+        float t = 0.0f;
+        for (int p = 0; p < 32; ++p) t += red[p][k];
+        G[OW0 + o * IN + k] += t;
+    }
+}
+
+// BF16 copies of W1, W2 for the tensor-core GEMMs.
+__global__ void to_bf16(const float* __restrict__ P, __nv_bfloat16* w1, __nv_bfloat16* w2) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= H * H) return;
+    w1[e] = __float2bfloat16(P[OW1 + e]);
+    w2[e] = __float2bfloat16(P[OW2 + e]);
+}
+
+__global__ void adam(float* P, const float* __restrict__ G, float* m1, float* m2, int n, float lr, float b1t,
+                     float b2t) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const float g = G[e];
+    const float a = 0.9f * m1[e] + 0.1f * g;
+    const float b = 0.999f * m2[e] + 0.001f * g * g;
+    m1[e] = a;
+    m2[e] = b;
+    const float mh = a / (1.0f - b1t), vh = b / (1.0f - b2t);
+    P[e] -= lr * mh / (sqrtf(vh) + 1e-8f);
+}
+
+// Batch rows drawn with replacement: row = floor(u * rows) with u from
+// Philox keyed by (seed, step).
+__global__ void gather_batch(const float* __restrict__ X, const float* __restrict__ T, int64_t rows, int batch,
+                             uint64_t seed, int64_t step, float* xb, float* tb) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= batch) return;
+    const uint4 w = philox4((uint32_t)b, (uint32_t)step, (uint32_t)((uint64_t)step >> 32), 0x4d4c50u,
+                            (uint32_t)seed, (uint32_t)(seed >> 32));
+    const uint64_t r64 = (((uint64_t)w.x << 32) | w.y) % (uint64_t)rows;
+#pragma unroll
+    for (int k = 0; k < IN; ++k) xb[(size_t)b * IN + k] = X[r64 * IN + k];
+    tb[b] = T[r64];
+}
+
+}  // namespace mlp
+}  // namespace rtb
+
+using namespace rtb::mlp;
+
+struct rt_mlp {
+    int device = 0;
+    cudaStream_t s = nullptr;
+    float *P = nullptr, *G = nullptr, *M1 = nullptr, *M2 = nullptr;
+    __nv_bfloat16 *w1 = nullptr, *w2 = nullptr;
+    int64_t adam_t = 0;
+    // workspace for batches of up to `cap` rows
+    int64_t cap = 0;
+    float *x = nullptr, *t = nullptr, *y = nullptr, *dy = nullptr, *z0 = nullptr, *z1 = nullptr, *z2 = nullptr,
+          *d0 = nullptr, *d1 = nullptr, *d2 = nullptr, *loss = nullptr;
+    __nv_bfloat16 *h1 = nullptr, *h2 = nullptr, *h3 = nullptr, *d1h = nullptr, *d2h = nullptr;
+    float *X = nullptr, *T = nullptr;
+    int64_t rows = 0;
+};
+
+namespace {
+
+void free_ws(rt_mlp* m) {
+    void* ps[] = {m->x, m->t, m->y, m->dy, m->z0, m->z1, m->z2, m->d0, m->d1, m->d2, m->h1, m->h2, m->h3, m->d1h, m->d2h};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    m->x = m->t = m->y = m->dy = m->z0 = m->z1 = m->z2 = m->d0 = m->d1 = m->d2 = nullptr;
+    m->h1 = m->h2 = m->h3 = m->d1h = m->d2h = nullptr;
+    m->cap = 0;
+}
+
+bool reserve(rt_mlp* m, int64_t n) {
+    if (n <= m->cap) return true;
+    free_ws(m);
+    const size_t nh = (size_t)n * H;
+    bool ok = cudaMalloc(&m->x, (size_t)n * IN * 4) == cudaSuccess && cudaMalloc(&m->t, (size_t)n * 4) == cudaSuccess &&
+              cudaMalloc(&m->y, (size_t)n * 4) == cudaSuccess && cudaMalloc(&m->dy, (size_t)n * 4) == cudaSuccess &&
+              cudaMalloc(&m->z0, nh * 4) == cudaSuccess && cudaMalloc(&m->z1, nh * 4) == cudaSuccess &&
+              cudaMalloc(&m->z2, nh * 4) == cudaSuccess && cudaMalloc(&m->d0, nh * 4) == cudaSuccess &&
+              cudaMalloc(&m->d1, nh * 4) == cudaSuccess && cudaMalloc(&m->d2, nh * 4) == cudaSuccess &&
+              cudaMalloc(&m->h1, nh * 2) == cudaSuccess && cudaMalloc(&m->h2, nh * 2) == cudaSuccess &&
+              cudaMalloc(&m->h3, nh * 2) == cudaSuccess && cudaMalloc(&m->d1h, nh * 2) == cudaSuccess &&
+              cudaMalloc(&m->d2h, nh * 2) == cudaSuccess;
+    if (!ok) {
+        free_ws(m);
+        return false;
+    }
+    m->cap = n;
+    return true;
+}
+
+GemmArgs gemm(Op A, Op B, int M, int N, int K, int epi) {
+    GemmArgs g;
+    std::memset(&g, 0, sizeof g);
+    g.A = A;
+    g.B = B;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.ksplit = K;
+    g.epi = epi;
+    return g;
+}
+
+void launch_gemm(const GemmArgs& g, int splits, cudaStream_t s) {
+    dim3 grid((g.N + TN - 1) / TN, (g.M + TM - 1) / TM, splits);
+    gemm_bf16<<<grid, 128, 0, s>>>(g);
+}
+
+// Forward pass of the n rows in m->x; with `with_target`, also the loss and
+// dy.  Returns y in m->y.
+void forward(rt_mlp* m, int n, bool with_target) {
+    cudaStream_t s = m->s;
+    const int nh = n * H;
+    layer0_fwd<<<(nh + 255) / 256, 256, 0, s>>>(m->x, m->P, n, m->z0, m->h1);
+    // z1 = h1 W1^T + b1: A = h1 [n][H], B(k, o) = W1[o][k] -> (w1, H, trans)
+    GemmArgs g = gemm(Op{m->h1, H, 0}, Op{m->w1, H, 1}, n, H, H, EPI_FWD);
+    g.bias = m->P + OB1;
+    g.out_f = m->z1;
+    g.out_h = m->h2;
+    launch_gemm(g, 1, s);
+    g = gemm(Op{m->h2, H, 0}, Op{m->w2, H, 1}, n, H, H, EPI_FWD);
+    g.bias = m->P + OB2;
+    g.out_f = m->z2;
+    g.out_h = m->h3;
+    launch_gemm(g, 1, s);
+    if (with_target) cudaMemsetAsync(m->loss, 0, 4, s);
+    layer3_fwd<<<(n + 7) / 8, 256, 0, s>>>(m->h3, m->P, n, m->y, with_target ? m->t : nullptr, m->dy, m->loss);
+}
+
+// Gradient of the loss over the batch in m->x / m->t into m->G (zeroed here).
+void backward(rt_mlp* m, int n) {
+    cudaStream_t s = m->s;
+    const int nh = n * H;
+    cudaMemsetAsync(m->G, 0, NPARAM * 4, s);
+    layer3_wgrad<<<H + 1, 256, 0, s>>>(m->h3, m->dy, n, m->G);
+    layer3_bwd<<<(nh + 255) / 256, 256, 0, s>>>(m->z2, m->dy, m->P, n, m->d2, m->d2h);
+    const int splits = (n + 1023) / 1024;
+    const int ks = ((n + splits - 1) / splits + TK - 1) / TK * TK;
+    // dW2 = dz2^T h2: A(o, r) = dz2[r][o] -> (d2h, H, trans); B(r, k) = h2[r][k]
+    GemmArgs g = gemm(Op{m->d2h, H, 1}, Op{m->h2, H, 0}, H, H, n, EPI_ATOMIC);
+    g.ksplit = ks;
+    g.out_f = m->G + OW2;
+    launch_gemm(g, splits, s);
+    bias_grad<<<H, 256, 0, s>>>(m->d2, n, m->G, OB2);
+    // dz1 = (dz2 W2) * gelu'(z1): A = dz2 [n][H], B(o, k) = W2[o][k]
+    g = gemm(Op{m->d2h, H, 0}, Op{m->w2, H, 0}, n, H, H, EPI_DGELU);
+    g.zin = m->z1;
+    g.out_f = m->d1;
+    g.out_h = m->d1h;
+    launch_gemm(g, 1, s);
+    g = gemm(Op{m->d1h, H, 1}, Op{m->h1, H, 0}, H, H, n, EPI_ATOMIC);
+    g.ksplit = ks;
+    g.out_f = m->G + OW1;
+    launch_gemm(g, splits, s);
+    bias_grad<<<H, 256, 0, s>>>(m->d1, n, m->G, OB1);
+    g = gemm(Op{m->d1h, H, 0}, Op{m->w1, H, 0}, n, H, H, EPI_DGELU);
+    g.zin = m->z0;
+    g.out_f = m->d0;
+    g.out_h = m->h3;  // scratch: the BF16 copy of dz0 is not needed
+    launch_gemm(g, 1, s);
+    layer0_wgrad<<<H, 256, 0, s>>>(m->d0, m->x, n, m->G);
+    bias_grad<<<H, 256, 0, s>>>(m->d0, n, m->G, OB0);
+}
+
+rt_status sync(rt_mlp* m) { return cudaStreamSynchronize(m->s) == cudaSuccess ? RT_OK : RT_E_CUDA; }
+
+}  // namespace
+
+extern "C" {
+
+rt_status rt_mlp_create(int32_t device, uint64_t seed, rt_mlp** out) {
+    if (!out) return RT_E_INVAL;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return RT_E_NODEVICE;
+    rt_mlp* m = new rt_mlp();
+    m->device = device;
+    bool ok = cudaStreamCreateWithFlags(&m->s, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaMalloc(&m->P, NPARAM * 4) == cudaSuccess && cudaMalloc(&m->G, NPARAM * 4) == cudaSuccess &&
+              cudaMalloc(&m->M1, NPARAM * 4) == cudaSuccess && cudaMalloc(&m->M2, NPARAM * 4) == cudaSuccess &&
+              cudaMalloc(&m->w1, H * H * 2) == cudaSuccess && cudaMalloc(&m->w2, H * H * 2) == cudaSuccess &&
+              cudaMalloc(&m->loss, 4) == cudaSuccess;
+    if (!ok) {
+        rt_mlp_destroy(m);
+        return RT_E_NOMEM;
+    }
+    // Initialisation: weights uniform in +-1/sqrt(fan_in) from Philox(seed), biases 0.
+    std::vector<float> p(NPARAM, 0.0f);
+    auto fill = [&](int off, int count, int fan_in) {
+        const float a = 1.0f / std::sqrt((float)fan_in);
+        for (int i = 0; i < count; ++i) {
+            const uint4 w = rtb::philox4((uint32_t)(off + i), 0x494e4954u, 0, 0, (uint32_t)seed, (uint32_t)(seed >> 32));
+            p[off + i] = a * (2.0f * ((float)(w.x >> 8) * (1.0f / 16777216.0f)) - 1.0f);
+        }
+    };
+    fill(OW0, H * IN, IN);
+    fill(OW1, H * H, H);
+    fill(OW2, H * H, H);
+    fill(OW3, H, H);
+    *out = m;
+    return rt_mlp_set_params(m, p.data());
+}
+
+rt_status rt_mlp_destroy(rt_mlp* m) {
+    if (!m) return RT_E_INVAL;
+    cudaSetDevice(m->device);
+    if (m->s) cudaStreamSynchronize(m->s);
+    free_ws(m);
+    void* ps[] = {m->P, m->G, m->M1, m->M2, m->w1, m->w2, m->loss, m->X, m->T};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    if (m->s) cudaStreamDestroy(m->s);
+    delete m;
+    return RT_OK;
+}
+
+rt_status rt_mlp_get_params(rt_mlp* m, float* params) {
+    if (!m || !params) return RT_E_INVAL;
+    cudaSetDevice(m->device);
+    if (cudaMemcpyAsync(params, m->P, NPARAM * 4, cudaMemcpyDeviceToHost, m->s) != cudaSuccess) return RT_E_CUDA;
+    return sync(m);
+}
+
+rt_status rt_mlp_set_params(rt_mlp* m, const float* params) {
+    if (!m || !params) return RT_E_INVAL;
+    cudaSetDevice(m->device);
+    cudaMemcpyAsync(m->P, params, NPARAM * 4, cudaMemcpyHostToDevice, m->s);
+    cudaMemsetAsync(m->M1, 0, NPARAM * 4, m->s);
+    cudaMemsetAsync(m->M2, 0, NPARAM * 4, m->s);
+    m->adam_t = 0;
+    to_bf16<<<(H * H + 255) / 256, 256, 0, m->s>>>(m->P, m->w1, m->w2);
+    return sync(m);
+}
+
+rt_status rt_mlp_predict(rt_mlp* m, const float* x, int64_t n, float* y) {
+    if (!m || !x || !y || n < 0) return RT_E_INVAL;
+    cudaSetDevice(m->device);
+    const int64_t chunk = 1 << 18;
+    for (int64_t r0 = 0; r0 < n; r0 += chunk) {
+        const int rn = (int)std::min<int64_t>(chunk, n - r0);
+        if (!reserve(m, rn)) return RT_E_NOMEM;
+        cudaMemcpyAsync(m->x, x + r0 * IN, (size_t)rn * IN * 4, cudaMemcpyHostToDevice, m->s);
+        forward(m, rn, false);
+        cudaMemcpyAsync(y + r0, m->y, (size_t)rn * 4, cudaMemcpyDeviceToHost, m->s);
+        rt_status st = sync(m);
+        if (st != RT_OK) return st;
+    }
+    return RT_OK;
+}
+
+rt_status rt_mlp_loss_grad(rt_mlp* m, const float* x, const float* target, int64_t n, float* loss, float* grad) {
+    if (!m || !x || !target || n <= 0 || n > (1 << 22)) return RT_E_INVAL;
+    cudaSetDevice(m->device);
+    if (!reserve(m, n)) return RT_E_NOMEM;
+    cudaMemcpyAsync(m->x, x, (size_t)n * IN * 4, cudaMemcpyHostToDevice, m->s);
+    cudaMemcpyAsync(m->t, target, (size_t)n * 4, cudaMemcpyHostToDevice, m->s);
+    forward(m, (int)n, true);
+    backward(m, (int)n);
+    if (loss) cudaMemcpyAsync(loss, m->loss, 4, cudaMemcpyDeviceToHost, m->s);
+    if (grad) cudaMemcpyAsync(grad, m->G, NPARAM * 4, cudaMemcpyDeviceToHost, m->s);
+    return sync(m);
+}
+
+rt_status rt_mlp_set_data(rt_mlp* m, const float* x, const float* target, int64_t n) {
+    if (!m || !x || !target || n <= 0) return RT_E_INVAL;
+    cudaSetDevice(m->device);
+    if (m->X) cudaFree(m->X);
+    if (m->T) cudaFree(m->T);
+    m->X = m->T = nullptr;
+    if (cudaMalloc(&m->X, (size_t)n * IN * 4) != cudaSuccess || cudaMalloc(&m->T, (size_t)n * 4) != cudaSuccess)
+        return RT_E_NOMEM;
+    cudaMemcpyAsync(m->X, x, (size_t)n * IN * 4, cudaMemcpyHostToDevice, m->s);
+    cudaMemcpyAsync(m->T, target, (size_t)n * 4, cudaMemcpyHostToDevice, m->s);
+    m->rows = n;
+    return sync(m);
+}
+
+rt_status rt_mlp_train(rt_mlp* m, int64_t steps, int32_t batch, float lr, uint64_t seed, float* loss) {
+    if (!m || steps < 0 || batch <= 0 || batch > (1 << 22) || !m->X) return RT_E_INVAL;
+    cudaSetDevice(m->device);
+    if (!reserve(m, batch)) return RT_E_NOMEM;
+    for (int64_t k = 0; k < steps; ++k) {
+        gather_batch<<<(batch + 255) / 256, 256, 0, m->s>>>(m->X, m->T, m->rows, batch, seed, m->adam_t, m->x, m->t);
+        forward(m, batch, true);
+        backward(m, batch);
+        ++m->adam_t;
+        const float b1t = std::pow(0.9f, (float)m->adam_t), b2t = std::pow(0.999f, (float)m->adam_t);
+        adam<<<(NPARAM + 255) / 256, 256, 0, m->s>>>(m->P, m->G, m->M1, m->M2, NPARAM, lr, b1t, b2t);
+        to_bf16<<<(H * H + 255) / 256, 256, 0, m->s>>>(m->P, m->w1, m->w2);
+    }
+    if (loss) cudaMemcpyAsync(loss, m->loss, 4, cudaMemcpyDeviceToHost, m->s);
+    return sync(m);
+}
+
+}  // extern "C"
