@@ -201,6 +201,7 @@ struct rt_tiler {
     bool plan_uniform = true;
     int kernel_choice = 0;  // 0 auto, 1 generic walk kernel only, 2 word kernel only (RT_WALK_KERNEL)
     int ctas_hint = 0;      // word kernel grid (RT_WALK_CTAS; 0 = one CTA per SM)
+    int64_t drop_phase = -1;  // RT_TEST_DROP_PUBLISH: a phase whose rows CTA 0 withholds (bounded-wait tests)
     int64_t last_phases = 0, last_launches = 0;
     uint64_t timeout_ns = 5000000000ull;
 
@@ -314,6 +315,7 @@ rt_status rt_create(const rt_config* cfg, rt_tiler** out) {
         if (std::strcmp(kc, "word") == 0) h->kernel_choice = 2;
     }
     if (const char* ct = std::getenv("RT_WALK_CTAS")) h->ctas_hint = std::max(0, std::atoi(ct));
+    if (const char* dp = std::getenv("RT_TEST_DROP_PUBLISH")) h->drop_phase = std::atoll(dp);
     if (const char* t = std::getenv("RT_WAIT_TIMEOUT_MS")) {
         const long ms = std::atol(t);
         if (ms > 0) h->timeout_ns = (uint64_t)ms * 1000000ull;
@@ -635,6 +637,7 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     a.xbuf = static_cast<unsigned long long*>(h->d_xbuf.p);
     a.err = static_cast<int*>(h->d_err.p);
     a.timeout_ns = h->timeout_ns;
+    a.drop_phase = h->drop_phase;
     s = launch_walk(h->plan, a, h->stream, &h->err);
     if (s != RT_OK) return s;
     h->last_phases = nph;

@@ -48,11 +48,14 @@ __device__ __forceinline__ void unpack_word(T* row, int w, uint32_t v) {
         row[w] = (T)v;
 }
 
-// Waits for one tagged word; returns false on timeout or when another CTA
-// already reported an error.
+// Waits for one tagged word; returns false on timeout (a.timeout_ns from the
+// first check of this wait's clock) or when another CTA already reported an
+// error.  The clock starts at this wait, so a walk may run for any length of
+// time; only a single wait is bounded.
 __device__ __forceinline__ bool wait_word(const WalkArgs& a, const unsigned long long* p, uint32_t tag,
-                                          uint32_t* out, uint64_t& t0) {
+                                          uint32_t* out) {
     unsigned spins = 0;
+    uint64_t t0 = 0;
     for (;;) {
         const unsigned long long x = ld_relaxed64(p);
         if ((uint32_t)(x >> 32) == tag) {

@@ -47,6 +47,7 @@ struct WalkArgs {
     unsigned long long* xbuf;  // tagged halo-row exchange slots
     int* err;
     uint64_t timeout_ns;
+    int64_t drop_phase;   // tests of the bounded waits: CTA 0 does not publish this phase's rows (-1: none)
 };
 
 // ---------------------------------------------------------------------------

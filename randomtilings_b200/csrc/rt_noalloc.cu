@@ -265,6 +265,7 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
         a.xbuf = reinterpret_cast<unsigned long long*>(base + off_x);
         a.err = reinterpret_cast<int*>(base + off_err);
         a.timeout_ns = 5000000000ull;
+        a.drop_phase = -1;
         s = launch_walk(plan, a, stream, &perr);
         if (s != RT_OK) {
             say(errbuf, errcap, "%s", perr.c_str());

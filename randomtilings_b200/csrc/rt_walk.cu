@@ -95,7 +95,6 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
     int64_t next_epoch = a.nepochs > 0 ? a.epoch_start[0] : INT64_MAX;
     uint32_t key0 = 0, key1 = 0;  // fast mode: Philox key of the epoch
     int64_t dstep = 0;            // fast mode: drawing steps since the epoch started
-    uint64_t t0 = 0;
     uint32_t d = a.nphases > 0 ? __ldg(a.phases) : 0u;
     uint32_t d_prev = 0u;
 
@@ -203,7 +202,7 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
                 const int src = side == 0 ? cta - 1 : cta + 1;
                 if (src < 0 || src >= nct) continue;
                 uint32_t v;
-                ok = wait_word(a, slot(a, src, side == 0 ? 1 : 0, par, l, kx) + w, tag, &v, t0);
+                ok = wait_word(a, slot(a, src, side == 0 ? 1 : 0, par, l, kx) + w, tag, &v);
                 if (ok) unpack_word<T>(row_ptr(l, nth_bit(mask, kx), side == 0 ? a0 - 1 : a1), w, v);
             }
             if (__syncthreads_or(!ok)) return;
@@ -222,7 +221,7 @@ __global__ void __launch_bounds__(BLOCK, 1) walk_kernel(const __grid_constant__ 
             }
         }
         __syncthreads();
-        if (ph + 1 < a.nphases) {
+        if (ph + 1 < a.nphases && !(cta == 0 && ph == a.drop_phase)) {
             // Publish the band's first / last row of every array written in this phase.
             const uint32_t mask = Model::written(d);
             const int nx = __popc(mask);

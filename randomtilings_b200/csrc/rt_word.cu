@@ -122,7 +122,6 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
     int64_t next_epoch = a.nepochs > 0 ? a.epoch_start[0] : INT64_MAX;
     uint32_t key0 = 0, key1 = 0;
     int64_t dstep = 0;
-    uint64_t t0 = 0;
     uint32_t d = a.nphases > 0 ? __ldg(a.phases) : 0u;
     uint32_t d_prev = 0u;
 
@@ -240,7 +239,7 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
                     const int src = side == 0 ? cta - 1 : cta + 1;
                     if (src < 0 || src >= nct) continue;
                     uint32_t v;
-                    ok = wait_word(a, slot(a, src, 1 - side, par, l, 0) + w, tag, &v, t0);
+                    ok = wait_word(a, slot(a, src, 1 - side, par, l, 0) + w, tag, &v);
                     if (ok) sts(lat + (l * NC + arr) * plane + (side == 0 ? 0 : nrows + 1) * W + 4 * w, v);
                 }
             }
@@ -255,7 +254,7 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
                 if ((wflags >> (2 * m) & 3u) == 3u) own_word(m);
         }
         __syncthreads();
-        if (ph + 1 < a.nphases) {
+        if (ph + 1 < a.nphases && !(cta == 0 && ph == a.drop_phase)) {
             // Publish the band's first / last row of the array flipped in this phase.
             const uint32_t mask = M::written(d);
             if (mask) {
