@@ -45,7 +45,14 @@ typedef enum {
 
 typedef enum {
     RT_RNG_TINYMT = 0, /* bit-exact: per-work-item TinyMT streams + the reference's host colour order */
-    RT_RNG_PHILOX = 1  /* fast mode: Philox4x32-10 keyed by (chain, site, sweep, colour), cyclic colour sweeps */
+    RT_RNG_PHILOX = 1, /* fast mode: Philox4x32-10 keyed by (chain, site, sweep, colour), cyclic colour sweeps */
+    RT_RNG_PLANES = 2  /* bit-plane mode (dominoes; uniform lozenges): the lattice as bit planes, 32 sites per
+                          word, one Philox4x32-10 bit per site and colour step, cyclic colour sweeps.  Rules:
+                          domino heat bath (RT_KERNEL_CFTP): a rotatable site becomes 12 where its bit is 1,
+                          else 3; domino toggle (RT_KERNEL_DEFAULT): 3 <-> 12 where either of two bits is 1
+                          (probability 3/4 instead of dominokernel.cl's 0.8); lozenges: heat bath, 25 -> 38
+                          where the bit is 1, 38 -> 25 where it is 0.  Same equilibrium (uniform); the heat
+                          baths are monotone, so rt_cftp accepts them. */
 } rt_rng;
 
 typedef enum {
@@ -133,6 +140,12 @@ rt_status rt_download(rt_tiler* h, int32_t* tiling);
 rt_status rt_synchronize(rt_tiler* h);
 /* The handle's cudaStream_t (as void*), for callers that time with events. */
 void* rt_stream(rt_tiler* h);
+/* Device form of rt_download, for statistics computed on the device (no
+ * reference counterpart): merges the colour arrays into the handle's own
+ * N x N int32 device tiling (asynchronous on rt_stream(h)) and returns its
+ * address in *d_tiling; it stays valid until the next rt_upload / rt_walk
+ * or rt_destroy, and is overwritten by the next rt_download / rt_device_tiling. */
+rt_status rt_device_tiling(rt_tiler* h, int32_t** d_tiling);
 /* Counters of the last run: phases executed and kernel launches issued. */
 rt_status rt_last_run_info(rt_tiler* h, int64_t* phases, int64_t* launches);
 

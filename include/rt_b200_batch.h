@@ -29,7 +29,10 @@ typedef struct {
     int32_t model;    /* rt_model */
     int32_t kernel;   /* RT_KERNEL_DEFAULT; dominoes may use RT_KERNEL_CFTP (heat bath) */
     uint32_t chain;   /* Philox counter word 3 */
-    int32_t reserved; /* 0 */
+    float q;          /* lozenges: volume weight q in (0, 1]; 0 = uniform (q = 1).  A site adds a
+                         cube when its draw is below 0.4 q and removes one when its draw lies in
+                         [0.4, 0.8), so the chain's equilibrium weighs a tiling by q^volume and
+                         q = 1 is the uniform rule of lozengekernel.cl:19-21.  Other models: 0. */
     int64_t key;      /* Philox key (the chain's seed) */
 } rt_chain;
 
@@ -62,6 +65,10 @@ rt_status rt_batch_set_tuning(rt_batch* b, int32_t autotune, int32_t cluster, in
  * run of s1 + s2). */
 rt_status rt_batch_run(rt_batch* b, int64_t sweeps);
 rt_status rt_batch_download(rt_batch* b, int64_t index, int32_t* tiling);
+/* Device form of rt_batch_download: chain `index`'s N x N tiling into the
+ * caller's device buffer d_tiling (N*N int32), asynchronous on `stream`
+ * (cudaStream_t, NULL = the legacy default stream); allocates nothing. */
+rt_status rt_batch_device_tiling(rt_batch* b, int64_t index, int32_t* d_tiling, void* stream);
 rt_status rt_batch_get_info(rt_batch* b, rt_batch_info* info);
 const char* rt_batch_last_error(rt_batch* b);
 

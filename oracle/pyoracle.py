@@ -57,6 +57,8 @@ def oracle() -> ctypes.CDLL:
                                                 ctypes.c_double, ctypes.c_int]
         lib.orc_philox4x32_10.argtypes = [_P, _P, _P]
         lib.orc_domino_walk_fast.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.c_int]
+        lib.orc_domino_walk_planes.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.c_int]
+        lib.orc_lozenge_walk_planes.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32]
         lib.orc_lozenge_walk_fast.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.c_int,
                                               ctypes.c_double, ctypes.c_int]
         lib.orc_recttri_walk_fast.argtypes = [_P, ctypes.c_int, _I64, _I64, ctypes.c_uint32, _P]
@@ -184,17 +186,20 @@ def _epochs(steps, keys):
 def walk_fast(model: str, t, steps, keys, chain: int = 0, q: float = 0.99, qcmp_double: bool = False,
               weights=None) -> np.ndarray:
     """Fast-mode walk of `model` in {"domino", "domino_cftp", "lozenge",
-    "qlozenge", "recttri", "tridimer"}; steps / keys are one value or one
-    per epoch (epochs: dominoes and lozenges)."""
+    "qlozenge", "lozenge_q8", "recttri", "tridimer"}; steps / keys are one
+    value or one per epoch (epochs: dominoes and lozenges).  "lozenge_q8" is
+    the batched chains' volume-weighted int8 rule (add below 0.4 q, remove in
+    [0.4, 0.8))."""
     a, n = _tiling(t)
     st, ke = _epochs(steps, keys)
     lib = oracle()
     if model in ("domino", "domino_cftp"):
         rc = lib.orc_domino_walk_fast(a.ctypes.data, n, st.ctypes.data, ke.ctypes.data, st.size, chain,
                                       int(model == "domino_cftp"))
-    elif model in ("lozenge", "qlozenge"):
+    elif model in ("lozenge", "qlozenge", "lozenge_q8"):
+        qmode = {"lozenge": 0, "qlozenge": 1, "lozenge_q8": 2}[model]
         rc = lib.orc_lozenge_walk_fast(a.ctypes.data, n, st.ctypes.data, ke.ctypes.data, st.size, chain,
-                                       int(model == "qlozenge"), q, int(qcmp_double))
+                                       qmode, q, int(qcmp_double))
     elif model == "recttri":
         assert st.size == 1
         w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
@@ -209,14 +214,34 @@ def walk_fast(model: str, t, steps, keys, chain: int = 0, q: float = 0.99, qcmp_
     return a
 
 
+def walk_planes(model: str, t, steps, keys, chain: int = 0) -> np.ndarray:
+    """Bit-plane mode walk of `model` in {"domino" (two-bit toggle),
+    "domino_cftp" (heat bath), "lozenge" (heat bath)}; steps / keys are one
+    value or one per epoch."""
+    a, n = _tiling(t)
+    st, ke = _epochs(steps, keys)
+    lib = oracle()
+    if model in ("domino", "domino_cftp"):
+        rc = lib.orc_domino_walk_planes(a.ctypes.data, n, st.ctypes.data, ke.ctypes.data, st.size, chain,
+                                        int(model == "domino_cftp"))
+    elif model == "lozenge":
+        rc = lib.orc_lozenge_walk_planes(a.ctypes.data, n, st.ctypes.data, ke.ctypes.data, st.size, chain)
+    else:
+        raise ValueError(model)
+    _check(rc, f"bit-plane walk of {model}")
+    return a
+
+
 def cftp(tmax, tmin, first_steps: int, master_seed: int, schedule: str = "doubling", max_trials: int = 30,
-         model: str = "domino_cftp", fast: bool = False, **kw):
+         model: str = "domino_cftp", fast: bool = False, planes: bool = False, **kw):
     """CFTP composed from the restated epoch walks, following
     Examples/AztecDiamondCftpEx.cpp:42-68 (seeds: successive mt19937 outputs,
     newest epoch first; in fast mode each seed is its epoch's Philox key).
     model: "domino_cftp", "lozenge" or "qlozenge" (kw: q, qcmp_double).
     Returns (tiling, trials, total_steps, coalesced)."""
     def run(t, steps, seeds):
+        if planes:
+            return walk_planes(model, t, steps, seeds, **kw)
         if fast:
             return walk_fast(model, t, steps, seeds, **kw)
         if model == "domino_cftp":

@@ -156,6 +156,22 @@ static float orc_draw(orc_draws* d, int64_t r, int64_t c) {
     return (float)(d->w[j & 3] >> 9) * (1.0f / 8388608.0f);
 }
 
+/* Bit-plane mode (no reference counterpart): one random bit per site.  Site
+ * (i, j) of a colour array `width` sites wide lies in 32-bit word j / 32 of
+ * its row, and words come in fours: quad q = j / 128 of band row g = i -
+ * roff takes Philox4x32-10(counter = (g * ceil(ceil(width / 32) / 4) + q,
+ * step lo, step hi, chain), key) and word (j / 32) mod 4 of the output; the
+ * site's bit is bit j mod 32 of that word.  `second` selects the second bit
+ * of the domino toggle rule (counter word 0 with its top bit set). */
+static int plane_bit(const orc_draws* d, int64_t i, int64_t j, int second) {
+    const int64_t ww = (d->width + 31) / 32, qpr = (ww + 3) / 4;
+    const uint32_t c0 = (uint32_t)((i - d->roff) * qpr + (j / 32) / 4) | (second ? 0x80000000u : 0u);
+    const uint32_t ctr[4] = {c0, (uint32_t)d->step, (uint32_t)(d->step >> 32), d->chain};
+    uint32_t out[4];
+    orc_philox4x32_10(ctr, d->key, out);
+    return (int)((out[(j / 32) & 3] >> (j & 31)) & 1u);
+}
+
 /* Starts an epoch: TinyMT streams seeded with `seed` (bit-exact mode) or the
  * Philox key `seed` (fast mode).  Work item (r, c) of the Rotate range (cols
  * items per row) acts on site (r + roff, c + coff) of a colour array `width`
@@ -316,6 +332,22 @@ static void domino_rotate(int8_t* a, int n, orc_draws* rng, int cftp) {
         }
 }
 
+/* Bit-plane mode Rotate (no reference counterpart): heat bath -- a rotatable
+ * site (3 or 12) becomes 12 where its bit is 1, else 3; toggle -- 3 <-> 12
+ * where either of its two bits is 1. */
+static void domino_rotate_planes(int8_t* a, int n, const orc_draws* rng, int heat_bath) {
+    const int h = n / 2;
+    for (int i = 1; i <= n - 2; ++i)
+        for (int j = 1; j <= h - 2; ++j) {
+            int8_t* v = &a[i * h + j];
+            if (*v != 3 && *v != 12) continue;
+            if (heat_bath)
+                *v = plane_bit(rng, i, j, 0) ? 12 : 3;
+            else if (plane_bit(rng, i, j, 0) | plane_bit(rng, i, j, 1))
+                *v = (int8_t)(*v ^ 15);
+        }
+}
+
 /* UpdateTiles, dominokernel.cl:22-31: each interior site of the other colour
  * takes its four edge bits from its four neighbours in the flipped array.
  * For a row of parity i%2, the neighbour towards j-1 sits at array column
@@ -344,6 +376,8 @@ static void domino_merge(int32_t* t, int n, const int8_t* b, const int8_t* w) {
 
 static int domino_run(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k, int single_walk,
                       const uint32_t* params, int64_t nparams, int cftp, int fast, uint32_t chain) {
+    /* fast == 2: bit-plane mode (Philox bits, same colour cycle as fast mode) */
+    const int planes = fast == 2;
     if (n < 6 || n % 2) return ORC_EINVAL;
     const int h = n / 2;
     const int64_t items = (int64_t)(n - 2) * (h - 2);
@@ -370,10 +404,16 @@ static int domino_run(int32_t* t, int n, const int64_t* steps, const int64_t* se
         for (int64_t s = 0; s < steps[e]; ++s) {
             const int black = fast ? (s & 1) == 0 : mt_next(&m) % 2u == 1u;
             if (black) {
-                domino_rotate(b, n, &rng, cftp);
+                if (planes)
+                    domino_rotate_planes(b, n, &rng, cftp);
+                else
+                    domino_rotate(b, n, &rng, cftp);
                 domino_update(w, b, n, 1);
             } else {
-                domino_rotate(w, n, &rng, cftp);
+                if (planes)
+                    domino_rotate_planes(w, n, &rng, cftp);
+                else
+                    domino_rotate(w, n, &rng, cftp);
                 domino_update(b, w, n, 0);
             }
             draws_next(&rng);
@@ -403,6 +443,12 @@ int orc_domino_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t*
     return domino_run(t, n, steps, keys, k, 0, NULL, 0, cftp_kernel, 1, chain);
 }
 
+int orc_domino_walk_planes(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
+                           int heat_bath) {
+    if (k < 0) return ORC_EINVAL;
+    return domino_run(t, n, steps, keys, k, 0, NULL, 0, heat_bath, 2, chain);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Lozenge: src/Lozenge/LozengeTiler.cpp:18-88, lozengekernel.cl and        */
 /* qlozengekernel.cl.  Vertex bits (LozengeTiler.h:11-17): 1 and 2 the two  */
@@ -423,7 +469,14 @@ static void lozenge_rotate(void* arr, int isint, int n, orc_draws* rng, int qmod
             const int64_t at = (int64_t)i * m + j;
             const int v = isint ? ((int32_t*)arr)[at] : ((int8_t*)arr)[at];
             int nv = v;
-            if (!qmode) {
+            if (qmode == 2) {
+                /* volume weight q in the int8 fast rule of the batched chains: add below 0.4 q */
+                if ((double)rd < 0.4 * q) {
+                    if (v == 25) nv = 38;
+                } else if ((double)rd >= 0.4 && (double)rd < 0.8) {
+                    if (v == 38) nv = 25;
+                }
+            } else if (!qmode) {
                 if ((double)rd < 0.4) {
                     if (v == 25) nv = 38;
                 } else if ((double)rd < 0.8) {
@@ -450,6 +503,18 @@ static void lozenge_rotate(void* arr, int isint, int n, orc_draws* rng, int qmod
 /* UpdateTiles, lozengekernel.cl:36-54: after colour t flipped (array f), the
  * next colour (array a) refreshes bits {2,4,32} and the one after (array b)
  * bits {1,8,16} from f; the column shift of each neighbour depends on i mod 3. */
+/* Bit-plane mode Rotate (no reference counterpart): heat bath -- 25 -> 38
+ * (add a cube) where the site's bit is 1, 38 -> 25 where it is 0. */
+static void lozenge_rotate_planes(int8_t* a, int n, const orc_draws* rng) {
+    const int m = n / 3;
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < m; ++j) {
+            int8_t* v = &a[(int64_t)i * m + j];
+            if (*v == 25 && plane_bit(rng, i, j, 0)) *v = 38;
+            else if (*v == 38 && !plane_bit(rng, i, j, 0)) *v = 25;
+        }
+}
+
 static void lozenge_update(const void* fv, void* av, void* bv, int isint, int n, int t) {
     const int m = n / 3;
 #define LZ(arr, r, c) (isint ? ((const int32_t*)(arr))[(int64_t)(r)*m + (c)] : ((const int8_t*)(arr))[(int64_t)(r)*m + (c)])
@@ -483,7 +548,7 @@ static int lozenge_run(int32_t* t, int n, const int64_t* steps, const int64_t* s
                        int64_t nparams, int qmode, double q, int qcmp, int fast, uint32_t chain) {
     if (n < 3 || n % 3 || k < 0) return ORC_EINVAL;
     const int m = n / 3;
-    const int isint = qmode != 0; /* lozengekernel.cl stores char, qlozengekernel.cl int */
+    const int isint = qmode == 1; /* lozengekernel.cl stores char, qlozengekernel.cl int */
     const size_t es = isint ? 4 : 1;
     void* arr[3];
     for (int c = 0; c < 3; ++c) arr[c] = calloc((size_t)n * m, es);
@@ -510,7 +575,10 @@ static int lozenge_run(int32_t* t, int n, const int64_t* steps, const int64_t* s
         minstd_seed(&g, seeds[e]);
         for (int64_t s = 0; s < steps[e]; ++s) {
             const int r = fast ? (int)(s % 3) : uniform_int(&g, 2);
-            lozenge_rotate(arr[r], isint, n, &rng, qmode, q, qcmp);
+            if (fast == 2)
+                lozenge_rotate_planes((int8_t*)arr[r], n, &rng);
+            else
+                lozenge_rotate(arr[r], isint, n, &rng, qmode, q, qcmp);
             lozenge_update(arr[r], arr[(r + 1) % 3], arr[(r + 2) % 3], isint, n, r);
             draws_next(&rng);
         }
@@ -540,6 +608,10 @@ int orc_lozenge_walk_epochs(int32_t* t, int n, const int64_t* steps, const int64
 int orc_lozenge_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
                           int qmode, double q, int qcmp) {
     return lozenge_run(t, n, steps, keys, k, NULL, 0, qmode, q, qcmp, 1, chain);
+}
+
+int orc_lozenge_walk_planes(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain) {
+    return lozenge_run(t, n, steps, keys, k, NULL, 0, 0, 1.0, 0, 2, chain);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -56,7 +56,9 @@ int orc_domino_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32
 int orc_domino_walk_epochs(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k,
                            const uint32_t* params, int64_t nparams, int cftp_kernel);
 /* qmode: 0 = uniform (lozengekernel.cl, char storage); 1 = q-weighted
- * (qlozengekernel.cl, int storage) with comparison `qcmp`. */
+ * (qlozengekernel.cl, int storage) with comparison `qcmp`; 2 = the batched
+ * chains' volume weight on char storage (no reference counterpart): add a
+ * cube when rd < 0.4 q, remove one when 0.4 <= rd < 0.8 (double compare). */
 int orc_lozenge_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
                      int qmode, double q, int qcmp);
 /* weights: 16 floats indexed by face digit (recttrianglekernel.cl:3-13);
@@ -82,6 +84,12 @@ int orc_domino_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t*
                          int cftp_kernel);
 int orc_lozenge_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
                           int qmode, double q, int qcmp);
+/* Bit-plane mode (RT_RNG_PLANES): the same colour cycle as fast mode, one
+ * Philox bit per site and step (plane_bit in rt_oracle.c), heat-bath rules
+ * (dominoes: heat_bath = 1; heat_bath = 0 is the two-bit toggle). */
+int orc_domino_walk_planes(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
+                           int heat_bath);
+int orc_lozenge_walk_planes(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain);
 int orc_recttri_walk_fast(int32_t* t, int n, int64_t steps, int64_t key, uint32_t chain, const float* weights);
 int orc_tridimer_walk_fast(int32_t* t, int n, int64_t steps, int64_t key, uint32_t chain);
 

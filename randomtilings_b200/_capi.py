@@ -20,7 +20,7 @@ RT_E_STATE = -7
 
 RT_DOMINO, RT_LOZENGE, RT_RECTTRI, RT_TRIDIMER = 0, 1, 2, 3
 RT_KERNEL_DEFAULT, RT_KERNEL_CFTP, RT_KERNEL_QWEIGHT = 0, 1, 2
-RT_RNG_TINYMT, RT_RNG_PHILOX = 0, 1
+RT_RNG_TINYMT, RT_RNG_PHILOX, RT_RNG_PLANES = 0, 1, 2
 RT_QCMP_FLOAT32, RT_QCMP_DOUBLE = 0, 1
 
 _STATUS_NAMES = {
@@ -67,7 +67,7 @@ class RtChain(ctypes.Structure):
         ("model", ctypes.c_int32),
         ("kernel", ctypes.c_int32),
         ("chain", ctypes.c_uint32),
-        ("reserved", ctypes.c_int32),
+        ("q", ctypes.c_float),
         ("key", ctypes.c_int64),
     ]
 
@@ -103,6 +103,7 @@ SIGNATURES = {
     "rt_download": (ctypes.c_int, [_P, _P]),
     "rt_synchronize": (ctypes.c_int, [_P]),
     "rt_stream": (_P, [_P]),
+    "rt_device_tiling": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     "rt_last_run_info": (ctypes.c_int, [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
     "rt_last_error": (ctypes.c_char_p, [_P]),
     "rt_version": (ctypes.c_char_p, []),
@@ -171,6 +172,7 @@ SIGNATURES.update({
     "rt_batch_set_tuning": (ctypes.c_int, [_P, _I32, _I32, _I32]),
     "rt_batch_run": (ctypes.c_int, [_P, _I64]),
     "rt_batch_download": (ctypes.c_int, [_P, _I64, _P]),
+    "rt_batch_device_tiling": (ctypes.c_int, [_P, _I64, _P, _P]),
     "rt_batch_get_info": (ctypes.c_int, [_P, ctypes.POINTER(RtBatchInfo)]),
     "rt_batch_last_error": (ctypes.c_char_p, [_P]),
     "rt_mixed_chain_spec": (ctypes.c_int, [_I64, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
@@ -185,6 +187,17 @@ class RtProjectStats(ctypes.Structure):
 # include/rt_b200_project.h
 SIGNATURES["rt_project_heights"] = (ctypes.c_int, [_I32, _P, _I64, _P, _P, _P, _P, _I64, _I32,
                                                    ctypes.POINTER(RtProjectStats)])
+
+# include/rt_b200_height.h
+SIGNATURES.update({
+    "rt_hplan_create": (ctypes.c_int, [_I32, _P, _I64, _I32, ctypes.POINTER(_P)]),
+    "rt_hplan_destroy": (ctypes.c_int, [_P]),
+    "rt_hplan_info": (ctypes.c_int, [_P, ctypes.POINTER(_I32), ctypes.POINTER(_I64)]),
+    "rt_hplan_last_error": (ctypes.c_char_p, [_P]),
+    "rt_hplan_heights": (ctypes.c_int, [_P, _P, _P, _P]),
+    "rt_hplan_accumulate": (ctypes.c_int, [_P, _P, _P, _P]),
+    "rt_hplan_error": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(ctypes.c_double), _P]),
+})
 
 # include/rt_b200_mlp.h
 RT_MLP_IN, RT_MLP_WIDTH = 8, 128

@@ -49,10 +49,13 @@ class Batch:
         except Exception:
             pass
 
-    def add(self, model: int, tiling, key: int, chain: int | None = None, kernel: int = _capi.RT_KERNEL_DEFAULT) -> int:
+    def add(self, model: int, tiling, key: int, chain: int | None = None, kernel: int = _capi.RT_KERNEL_DEFAULT,
+            q: float = 0.0) -> int:
+        """q: lozenge volume weight in (0, 1] (0 = uniform), see rt_chain.q."""
         arr, n = _as_tiling(tiling)
         c = _capi.RtChain()
         c.model, c.kernel, c.key = model, kernel, int(np.int64(np.uint64(key & (2**64 - 1))))
+        c.q = float(q)
         c.chain = len(self._sizes) if chain is None else chain
         idx = ctypes.c_int64()
         self._check(self._lib.rt_batch_add(self._h, ctypes.byref(c), arr.ctypes.data, n, ctypes.byref(idx)))
@@ -70,6 +73,10 @@ class Batch:
         out = np.zeros(n * n, dtype=np.int32)
         self._check(self._lib.rt_batch_download(self._h, int(index), out.ctypes.data))
         return out
+
+    def device_tiling(self, index: int, d_tiling: int, stream: int = 0) -> None:
+        """Chain `index`'s tiling into the device buffer at d_tiling (N*N int32)."""
+        self._check(self._lib.rt_batch_device_tiling(self._h, int(index), d_tiling, stream or None))
 
     def info(self) -> dict:
         i = _capi.RtBatchInfo()

@@ -36,6 +36,8 @@ struct BatchChain {
     int n, rows, cols, arows, width, wpad;
     uint32_t chain, pad_;
     uint64_t key;
+    uint32_t thr[3];  // lozenges: add below thr[0]; remove in [thr[2], thr[1])
+    uint32_t pad2_;
 };
 
 struct BatchArgs {
@@ -142,8 +144,12 @@ __global__ void __launch_bounds__(1024, 1) batch_word_kernel(const __grid_consta
                     const uint4 w4 = philox4((uint32_t)((a0 + rr) * Gw + w), (uint32_t)dstep,
                                              (uint32_t)((uint64_t)dstep >> 32), ch.chain, key0, key1);
                     const uint32_t k[4] = {w4.x >> 9, w4.y >> 9, w4.z >> 9, w4.w >> 9};
-                    m0 = below4(k, b.thr[0]);
-                    if (!M::DOM) m1 = below4(k, b.thr[1]) & ~m0;
+                    if (M::DOM) {
+                        m0 = below4(k, b.thr[0]);
+                    } else {
+                        m0 = below4(k, ch.thr[0]);
+                        m1 = below4(k, ch.thr[1]) & ~below4(k, ch.thr[2]);
+                    }
                 }
                 word_phase<FAM>(P, 0, W, wi, m0, m1);
                 rr += drr;
@@ -320,6 +326,7 @@ constexpr int kFamilies = 6;
 
 struct Chain {
     int fam = 0, kind = 0, n = 0, ncol = 0, elem = 1;
+    uint32_t thr[3] = {0u, 0u, 0u};
     int rows = 0, cols = 0, arows = 0, width = 0;
     uint32_t chain = 0;
     uint64_t key = 0;
@@ -522,6 +529,7 @@ std::vector<BatchChain> records(rt_batch* b, int f, char* base) {
         x.wpad = (c.width + 3) & ~3;
         x.chain = c.chain;
         x.key = c.key;
+        for (int k = 0; k < 3; ++k) x.thr[k] = c.thr[k];
     }
     return r;
 }
@@ -735,6 +743,14 @@ rt_status rt_batch_add(rt_batch* b, const rt_chain* c, const int32_t* tiling, in
         ch.rows = n, ch.cols = n / 3, ch.arows = n, ch.width = n / 3;
     }
     ch.per_arr = ((size_t)ch.arows * ch.width * ch.elem + 255) & ~(size_t)255;
+    const double q = c->q == 0.0f ? 1.0 : (double)c->q;
+    if (!(q > 0.0 && q <= 1.0) || (ch.kind != 1 && q != 1.0))
+        return b->fail(RT_E_INVAL, "q must lie in (0, 1] (lozenges) or be 0");
+    if (ch.kind == 1) {
+        ch.thr[0] = below_threshold(0.4 * q);
+        ch.thr[1] = below_threshold(0.8);
+        ch.thr[2] = below_threshold(0.4);
+    }
     ch.chain = c->chain;
     ch.key = (uint64_t)c->key;
     ch.start.assign(tiling, tiling + (size_t)n * n);
@@ -866,6 +882,23 @@ rt_status rt_batch_download(rt_batch* b, int64_t index, int32_t* tiling) {
     cudaError_t ce = cudaMemcpyAsync(tiling, tmp.p, tb, cudaMemcpyDeviceToHost, b->stream);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(b->stream);
     if (ce != cudaSuccess) return b->fail(RT_E_CUDA, std::string("batch download: ") + cudaGetErrorString(ce));
+    return RT_OK;
+}
+
+rt_status rt_batch_device_tiling(rt_batch* b, int64_t index, int32_t* d_tiling, void* stream) {
+    if (!b || !d_tiling) return b ? b->fail(RT_E_INVAL, "null tiling") : RT_E_INVAL;
+    if (index < 0 || index >= (int64_t)b->chains.size()) return b->fail(RT_E_INVAL, "no chain with that index");
+    cudaSetDevice(b->device);
+    rt_status s = upload(b);
+    if (s != RT_OK) return s;
+    const Chain& c = b->chains[(size_t)index];
+    if (c.kind == 3) return b->fail(RT_E_INVAL, "device tilings of triangle-dimer chains are not merged on the device");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // The merge writes every cell of the colour models' tilings.
+    char* base = static_cast<char*>(b->fam[c.fam].data.p) + c.off;
+    void* arr[3] = {base, base + c.per_arr, c.ncol > 2 ? base + 2 * c.per_arr : nullptr};
+    std::string e;
+    if (launch_split(true, c.elem, c.kind, c.ncol, c.n, d_tiling, arr, st, &e) != RT_OK) return b->fail(RT_E_CUDA, e);
     return RT_OK;
 }
 

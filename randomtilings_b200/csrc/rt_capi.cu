@@ -66,13 +66,6 @@ struct DevBuf {
     }
 };
 
-// Integer threshold K with  (k * 2^-23 < x)  <=>  (k < K)  for k in [0, 2^23).
-uint32_t below_threshold(double x) {
-    const double s = std::ceil(x * 8388608.0);
-    if (s <= 0) return 0;
-    if (s >= 4294967295.0) return 0xffffffffu;
-    return (uint32_t)s;
-}
 // Largest K with  K <= x * 2^e  (clamped to [0, 2^32-1]).
 uint32_t floor_scaled(double x, int e) {
     const double s = std::floor(std::ldexp(x, e));
@@ -84,6 +77,13 @@ uint32_t floor_scaled(double x, int e) {
 }  // namespace
 
 namespace rtb {
+
+uint32_t below_threshold(double x) {
+    const double s = std::ceil(x * 8388608.0);
+    if (s <= 0) return 0;
+    if (s >= 4294967295.0) return 0xffffffffu;
+    return (uint32_t)s;
+}
 
 // Phases of one triangle-dimer step (TriangleDimerTiler.cpp:243-347): the
 // flip family `kind` (0 lozenges, 1 triangles, 2 butterflies), orientation /
@@ -201,6 +201,7 @@ struct rt_tiler {
     bool plan_uniform = true;
     int kernel_choice = 0;  // 0 auto, 1 generic walk kernel only, 2 word kernel only (RT_WALK_KERNEL)
     int ctas_hint = 0;      // word kernel grid (RT_WALK_CTAS; 0 = one CTA per SM)
+    int depth_hint = 0;     // bit-plane kernel: phases per halo exchange (RT_PLANE_DEPTH; 0 = up to 8)
     int64_t drop_phase = -1;  // RT_TEST_DROP_PUBLISH: a phase whose rows CTA 0 withholds (bounded-wait tests)
     int64_t last_phases = 0, last_launches = 0;
     uint64_t timeout_ns = 5000000000ull;
@@ -265,8 +266,12 @@ rt_status rt_create(const rt_config* cfg, rt_tiler** out) {
         g_create_error = "unsupported model/kernel combination";
         return RT_E_INVAL;
     }
-    if (cfg->rng != RT_RNG_TINYMT && cfg->rng != RT_RNG_PHILOX) {
+    if (cfg->rng != RT_RNG_TINYMT && cfg->rng != RT_RNG_PHILOX && cfg->rng != RT_RNG_PLANES) {
         g_create_error = "unknown rng mode";
+        return RT_E_INVAL;
+    }
+    if (cfg->rng == RT_RNG_PLANES && !word_family(family)) {
+        g_create_error = "bit-plane mode exists for dominoes and uniform lozenges";
         return RT_E_INVAL;
     }
     if (family == FAM_QLOZENGE32 && (!(cfg->q >= 0.0) || !std::isfinite(cfg->q))) {
@@ -315,6 +320,7 @@ rt_status rt_create(const rt_config* cfg, rt_tiler** out) {
         if (std::strcmp(kc, "word") == 0) h->kernel_choice = 2;
     }
     if (const char* ct = std::getenv("RT_WALK_CTAS")) h->ctas_hint = std::max(0, std::atoi(ct));
+    if (const char* dp = std::getenv("RT_PLANE_DEPTH")) h->depth_hint = std::max(0, std::atoi(dp));
     if (const char* dp = std::getenv("RT_TEST_DROP_PUBLISH")) h->drop_phase = std::atoll(dp);
     if (const char* t = std::getenv("RT_WAIT_TIMEOUT_MS")) {
         const long ms = std::atol(t);
@@ -464,6 +470,17 @@ rt_status rt_download(rt_tiler* h, int32_t* tiling) {
     return rt_synchronize(h);
 }
 
+rt_status rt_device_tiling(rt_tiler* h, int32_t** d_tiling) {
+    if (!h || !d_tiling) return h ? h->fail(RT_E_INVAL, "null pointer") : RT_E_INVAL;
+    if (!h->uploaded) return h->fail(RT_E_STATE, "device tiling before upload");
+    cudaSetDevice(h->cfg.device);
+    rt_status s = launch_split(true, h->elem, h->kind, h->ncol, h->n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0],
+                               h->stream, &h->err);
+    if (s != RT_OK) return s;
+    *d_tiling = static_cast<int32_t*>(h->d_tiling.p);
+    return RT_OK;
+}
+
 rt_status rt_synchronize(rt_tiler* h) {
     if (!h) return RT_E_INVAL;
     cudaSetDevice(h->cfg.device);
@@ -508,7 +525,8 @@ static rt_status stage_params(rt_tiler* h, int64_t needed) {
 static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* seeds, int k, bool single_walk) {
     if (!h->uploaded) return h->fail(RT_E_STATE, "run before upload");
     cudaSetDevice(h->cfg.device);
-    const bool fast = h->cfg.rng == RT_RNG_PHILOX;
+    const bool planes = h->cfg.rng == RT_RNG_PLANES;
+    const bool fast = h->cfg.rng == RT_RNG_PHILOX || planes;  // counter-based draws, cyclic colours
     int64_t total = 0;
     for (int e = 0; e < k; ++e) {
         if (steps[e] < 0) return h->fail(RT_E_INVAL, "negative step count");
@@ -582,9 +600,13 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     if (h->plan_rows != h->rows || h->plan_cols != h->cols || h->plan_nlat != h->nlat || h->plan_uniform != uniform) {
         // The word kernel serves the int8 models with uniform generator
         // parameters; everything else (and any band it cannot hold) runs on
-        // the generic walk kernel.
+        // the generic walk kernel.  Bit-plane mode has its own kernel.
         rt_status s = RT_E_INVAL;
-        if (h->kernel_choice != 1 && uniform && word_family(h->family))
+        if (planes) {
+            s = plan_plane_walk(h->family, h->cfg.device, h->nlat, h->rows, width, h->ctas_hint, h->depth_hint,
+                                &h->plan, &h->err);
+            if (s != RT_OK) return s;
+        } else if (h->kernel_choice != 1 && uniform && word_family(h->family))
             s = plan_word_walk(h->family, h->cfg.device, h->nlat, h->rows, width, fast, h->ctas_hint, &h->plan,
                                &h->err);
         if (s != RT_OK && h->kernel_choice == 2) return s;
@@ -697,6 +719,7 @@ rt_status rt_cftp(rt_tiler* h, const int32_t* tmax, const int32_t* tmin, int32_t
         return h->fail(RT_E_INVAL,
                        "CFTP needs a monotone kernel: the domino heat bath (RT_KERNEL_CFTP, dominokernelCFTP.cl) "
                        "or a lozenge kernel");
+    // (bit-plane mode: both admitted families use heat-bath rules, monotone under shared bits)
     if (!tmax || !tmin || first_steps <= 0 || max_trials <= 0 ||
         (schedule != RT_CFTP_DOUBLING && schedule != RT_CFTP_REFERENCE))
         return h->fail(RT_E_INVAL, "bad CFTP arguments");

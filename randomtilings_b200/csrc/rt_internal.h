@@ -30,6 +30,8 @@ struct WalkPlan {
     int wpad = 0;    // shared-memory row stride (elements)
     int xwords = 0;  // exchange words per halo row
     int xslots = 1;  // arrays exchanged per phase
+    int depth = 1;   // bit-plane kernel: phases per halo exchange
+    int pwords = 0;  // bit-plane kernel: words per row
     const void* fn = nullptr;
 };
 
@@ -41,6 +43,10 @@ rt_status launch_walk(const WalkPlan& plan, WalkArgs& args, cudaStream_t stream,
 bool word_family(int family);
 rt_status plan_word_walk(int family, int device, int nlat, int rows, int width, bool philox, int ctas_hint,
                          WalkPlan* plan, std::string* err);
+// Bit-plane kernel of the int8 models (rt_plane.cu, RT_RNG_PLANES).
+// ctas_hint / depth_hint <= 0: one CTA per SM / the largest depth up to 8.
+rt_status plan_plane_walk(int family, int device, int nlat, int rows, int width, int ctas_hint, int depth_hint,
+                          WalkPlan* plan, std::string* err);
 // kind: 0 domino, 1 lozenge, 2 rect-triangle, 3 triangle-dimer (merge only).
 rt_status launch_split(bool merge, int elem_bytes, int kind, int ncol, int n, int32_t* tiling, void* const* arr,
                        cudaStream_t stream, std::string* err);
@@ -51,6 +57,8 @@ rt_status launch_split(bool merge, int elem_bytes, int kind, int ncol, int n, in
 // (with the final Update of the colour models).
 int64_t fast_step_phases(int kind, int64_t s, uint32_t* ph, int64_t at, uint32_t* prev);
 void fast_phases(int kind, int64_t steps, std::vector<uint32_t>& ph);
+// Integer threshold K with (k * 2^-23 < x) <=> (k < K) for k in [0, 2^23).
+uint32_t below_threshold(double x);
 // Integer acceptance thresholds of a kernel family on the 23-bit draw.
 void family_thresholds(int family, double q, int qcmp, uint32_t thr[4]);
 

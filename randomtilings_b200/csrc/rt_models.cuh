@@ -48,6 +48,8 @@ struct WalkArgs {
     int* err;
     uint64_t timeout_ns;
     int64_t drop_phase;   // tests of the bounded waits: CTA 0 does not publish this phase's rows (-1: none)
+    int depth;            // bit-plane kernel: phases per halo exchange
+    int pwords;           // bit-plane kernel: 32-bit words per colour-array row
 };
 
 // ---------------------------------------------------------------------------

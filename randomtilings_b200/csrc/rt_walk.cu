@@ -342,6 +342,8 @@ rt_status launch_walk(const WalkPlan& plan, WalkArgs& args, cudaStream_t stream,
     args.wpad = plan.wpad;
     args.xwords = plan.xwords;
     args.xslots = plan.xslots;
+    args.depth = plan.depth;
+    args.pwords = plan.pwords;
     void* kargs[] = {&args};
     cudaError_t e = cudaLaunchCooperativeKernel(plan.fn, dim3(plan.ctas), dim3(plan.block), kargs, plan.smem, stream);
     if (e != cudaSuccess) {

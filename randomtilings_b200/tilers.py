@@ -121,6 +121,13 @@ class _Tiler:
     def synchronize(self) -> None:
         self._check(self._lib.rt_synchronize(self._h))
 
+    def device_tiling(self) -> int:
+        """Device address of the current tiling (N x N int32), merged on the
+        handle's stream (rt_device_tiling)."""
+        ptr = ctypes.c_void_p()
+        self._check(self._lib.rt_device_tiling(self._h, ctypes.byref(ptr)))
+        return ptr.value
+
     @property
     def stream(self) -> int:
         return self._lib.rt_stream(self._h) or 0

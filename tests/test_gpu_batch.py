@@ -127,3 +127,35 @@ def test_batch_rejects_unsupported_chains(rt):
         bt.add(rt.RT_LOZENGE, golden("builders")["lozenge/hex4_0/min"], 1, kernel=rt.RT_KERNEL_QWEIGHT)
     with pytest.raises(rt.RtError):
         bt.add(rt.RT_DOMINO, np.zeros(49, dtype=np.int32), 1)
+
+
+def test_volume_weighted_lozenge_chains_equal_the_oracle(rt):
+    """Per-chain volume weight q (rt_chain.q) on the int8 lozenge family:
+    each chain equals the oracle's replay of the same rule and draws, and q = 1
+    equals the uniform chain."""
+    tmin = rt.LozengeTiler.MinTiling(rt.LozengeTiler.Hexagon(11, 8, 14))
+    qs = [np.float32(0.985), np.float32(0.5), np.float32(1.0), np.float32(0.0)]
+    bt = rt.Batch()
+    for c, qv in enumerate(qs):
+        bt.add(rt.RT_LOZENGE, tmin, key=77, chain=c, q=float(qv))
+    bt.run(SWEEPS)
+    got = [bt.download(c) for c in range(len(qs))]
+    bt.close()
+    for c, qv in enumerate(qs):
+        q = 1.0 if qv == 0 else float(qv)
+        want = po.walk_fast("lozenge_q8", tmin, 3 * SWEEPS, 77, chain=c, q=q)
+        assert np.array_equal(got[c], want), c
+    assert np.array_equal(po.walk_fast("lozenge_q8", tmin, 3 * SWEEPS, 77, chain=3, q=1.0),
+                          po.walk_fast("lozenge", tmin, 3 * SWEEPS, 77, chain=3))
+    # q = 0.5 removes cubes twice as often as it adds them: the volume ends lower
+    assert not np.array_equal(got[1], got[2])
+
+
+def test_batch_rejects_bad_q(rt):
+    bt = rt.Batch()
+    t = rt.LozengeTiler.MinTiling(rt.LozengeTiler.Hexagon(4, 4, 4))
+    with pytest.raises(rt.RtError):
+        bt.add(rt.RT_LOZENGE, t, key=1, q=1.5)
+    with pytest.raises(rt.RtError):
+        bt.add(rt.RT_DOMINO, rt.DominoTiler.MinTiling(rt.DominoTiler.AztecDiamond(5)), key=1, q=0.9)
+    bt.close()
