@@ -231,6 +231,8 @@ def run_b200(args) -> None:
     tq.upload(t0)
     tf = rt.LozengeTiler(device=local, rng=rt.RT_RNG_PHILOX)
     tf.upload(t0)
+    tp = rt.LozengeTiler(device=local, rng=rt.RT_RNG_PLANES)
+    tp.upload(t0)
 
     barrier(dist)
     torch.cuda.synchronize()
@@ -243,12 +245,15 @@ def run_b200(args) -> None:
     clocks = clk.summary()
     ms_q = time_device_walks(tq, args.steps, args.warmup, seed, flush)
     ms_f = time_device_walks(tf, args.steps, args.warmup, seed, flush)
+    ms_p = time_device_walks(tp, args.steps, args.warmup, seed, flush)
+    aztec = measure_aztec2000(args, local, seed, flush)
     e2e_ms = time_e2e_walks(rt.LozengeTiler, {"device": local}, t0, args.steps, min(args.warmup, 3), seed, flush)
     phases, launches = tl.last_run_info()
 
     total_ms = all_max(dist, sum(ms))
     total_q = all_max(dist, sum(ms_q))
     total_f = all_max(dist, sum(ms_f))
+    total_p = all_max(dist, sum(ms_p))
     total_e2e = all_max(dist, sum(e2e_ms))
     work = attempts * STEPS_PER_WALK * args.steps * world
     value = work / (total_ms / 1e3)
@@ -320,6 +325,13 @@ def run_b200(args) -> None:
                 "hbm_gbs_algorithmic": achieved_f,
                 "frac": achieved_f / peak,
             },
+            "bit_planes": {
+                "rng": "one Philox4x32-10 bit per site, heat-bath rule, lattice as bit planes, cyclic colours",
+                "value": attempts * STEPS_PER_WALK * args.steps * world / (total_p / 1e3),
+                "unit": "attempts/s",
+                "ms_per_step": total_p / args.steps,
+            },
+            "aztec2000": aztec,
             "batched": batched,
             "gpu_launches": int(launches) * args.steps,
             "phases_per_launch": int(phases),
@@ -332,8 +344,71 @@ def run_b200(args) -> None:
     tl.close()
     tq.close()
     tf.close()
+    tp.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+def measure_aztec2000(args, device: int, seed: int, flush) -> dict:
+    """The large lattice of the warm-start evaluation (Aztec diamond of order
+    2000, 4006 x 4006 tiling, 8,016,008 attempts per colour step): fast mode and
+    bit-plane mode, 4,000 colour steps per walk."""
+    import randomtilings_b200 as rt
+
+    d = rt.DominoTiler.AztecDiamond(2000)
+    t0 = rt.DominoTiler.MinTiling(d)
+    n = int(round(t0.size ** 0.5))
+    att = (n - 2) * (n // 2 - 2)
+    steps = 4000
+    out = {"workload": "Aztec diamond n=2000 (4006x4006), minimal tiling, 4000 colour steps per walk",
+           "attempts_per_step": att, "unit": "attempts/s"}
+    global STEPS_PER_WALK
+    saved = STEPS_PER_WALK
+    STEPS_PER_WALK = steps
+    try:
+        for name, rng in (("fast_mode", rt.RT_RNG_PHILOX), ("bit_planes", rt.RT_RNG_PLANES)):
+            tl = rt.DominoTiler(device=device, rng=rng)
+            tl.upload(t0)
+            ms = time_device_walks(tl, max(1, args.steps), args.warmup, seed, flush)
+            tl.close()
+            out[name] = att * steps / (sum(ms) / len(ms) / 1e3)
+    finally:
+        STEPS_PER_WALK = saved
+    return out
+
+
+def run_cftp(args) -> None:
+    """CFTP on an Aztec diamond (order args.cftp_order), coupled
+    chains from the maximal and minimal tilings, doubling from 1,024 colour
+    steps, one run per master seed 0..args.cftp_seeds-1."""
+    import randomtilings_b200 as rt
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    d = rt.DominoTiler.AztecDiamond(args.cftp_order)
+    tmax, tmin = rt.DominoTiler.MaxTiling(d), rt.DominoTiler.MinTiling(d)
+    rng = {"tinymt": rt.RT_RNG_TINYMT, "philox": rt.RT_RNG_PHILOX, "planes": rt.RT_RNG_PLANES}[args.cftp_rng]
+    runs = []
+    for s in range(rank, args.cftp_seeds, world):
+        tl = rt.DominoTiler(device=local, kernel=rt.RT_KERNEL_CFTP, rng=rng)
+        a = time.perf_counter()
+        _, st = tl.CFTP(tmax, tmin, first_steps=1024, master_seed=s, max_trials=24)
+        st["wall_s"] = time.perf_counter() - a
+        st["seed"] = s
+        tl.close()
+        runs.append(st)
+        print(json.dumps(st), file=sys.stderr, flush=True)
+    if rank == 0:
+        steps = [r["total_steps"] for r in runs]
+        print(json.dumps({
+            "metric": "CFTP coalescence (colour steps from the past) and wall time",
+            "workload": f"Aztec diamond n={args.cftp_order}, domino heat bath, doubling from 1024 steps",
+            "rng": args.cftp_rng, "seeds": len(runs), "coalesced": sum(r["coalesced"] for r in runs),
+            "median_steps": statistics.median(steps), "max_steps": max(steps),
+            "median_sweeps": statistics.median(steps) / 2,
+            "total_wall_s": sum(r["wall_s"] for r in runs), "total_device_ms": sum(r["device_ms"] for r in runs),
+            "runs": runs}), flush=True)
 
 
 def measure_batch(args, rank: int, world: int, dist, peak: float) -> dict:
@@ -468,13 +543,20 @@ def main() -> None:
     ap.add_argument("--batch-chains", type=int, default=4096)
     ap.add_argument("--batch-sweeps", type=int, default=5000)
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--workload", choices=["walk", "cftp"], default="walk",
+                    help="walk: the headline line (default); cftp: CFTP runs on an Aztec diamond")
+    ap.add_argument("--cftp-order", type=int, default=500)
+    ap.add_argument("--cftp-seeds", type=int, default=32)
+    ap.add_argument("--cftp-rng", choices=["tinymt", "philox", "planes"], default="planes")
     ap.add_argument("--walk-steps", type=int, default=STEPS_PER_WALK,
                     help="colour steps per walk (default 60000 = 20000 sweeps; smaller only for profiling captures)")
     args = ap.parse_args()
     STEPS_PER_WALK = args.walk_steps
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    if args.impl == "reference":
+    if args.workload == "cftp":
+        run_cftp(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)

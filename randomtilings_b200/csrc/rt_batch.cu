@@ -303,6 +303,121 @@ __global__ void __launch_bounds__(1024, 1) batch_site_kernel(const __grid_consta
     }
 }
 
+// ---------------------------------------------------------------------------
+// Triangle dimers: the eight arrays in mixed widths (TriDimerRule::MixedCtx):
+// arrays 0-4 as bytes, 5-7 as 16-bit words, 52 KB for a side-64 chain
+// instead of 152 KB at int32, so four chains share an SM.
+// Shared memory: 5 byte planes, then 3 16-bit planes, of (rpc + 2) x wpad.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024, 1) batch_td_kernel(const __grid_constant__ BatchArgs b) {
+    using R = TriDimerRule;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int CL = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    const int ncl = gridDim.x / CL;
+    const int cid = blockIdx.x / CL;
+    const int BLOCK = blockDim.x, tid = threadIdx.x;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+
+    for (int q = cid; q < b.nchains; q += ncl) {
+        const BatchChain& ch = b.chains[b.order[q]];
+        const int rows = ch.rows, W = ch.wpad, width = ch.width;
+        const int rpc = (rows + CL - 1) / CL;
+        const int r0 = min(rows, rank * rpc), r1 = min(rows, r0 + rpc);
+        const int nrows = r1 - r0;
+        const int plane = (rpc + 2) * W;
+        uint8_t* p8 = smem_raw;
+        int16_t* p16 = reinterpret_cast<int16_t*>(smem_raw + ((5 * plane + 15) & ~15));
+        for (int c = 0; c < 8; ++c) {
+            const int32_t* g = static_cast<const int32_t*>(ch.arr[c]);
+            for (int e = tid; e < (nrows + 2) * W; e += BLOCK) {
+                const int rr = r0 - 1 + e / W, j = e % W;
+                int32_t v = 0;
+                if (rr >= 0 && rr < ch.arows && j < width) v = g[(size_t)rr * width + j];
+                if (c < 5)
+                    p8[c * plane + e] = (uint8_t)v;
+                else
+                    p16[(c - 5) * plane + e] = (int16_t)v;
+            }
+        }
+        __syncthreads();
+
+        const uint32_t key0 = (uint32_t)ch.key, key1 = (uint32_t)(ch.key >> 32);
+        int64_t dstep = *b.step0;
+        const int Gw = (width + 3) >> 2;
+        const int nq = nrows * Gw;
+        const int drr = BLOCK / Gw, dq = BLOCK - drr * Gw;
+        for (int64_t ph = 0; ph < b.nphases; ++ph) {
+            const uint32_t d = __ldg(b.phases + ph);
+            const bool draws = (d & PH_DRAWS) != 0u;
+            R::MixedCtx x;
+            x.p8 = p8;
+            x.p16 = p16;
+            x.plane = plane;
+            x.w = W;
+            x.m = ch.n / 2;
+            x.row0 = r0 - 1;
+            x.op = ph_op(d);
+            x.a = ph_a(d);
+            x.b = ph_b(d);
+            int rr = tid / Gw, cq = tid - (tid / Gw) * Gw;
+            for (int u = tid; u < nq; u += BLOCK) {
+                const int r = r0 + rr;
+                uint4 w4 = make_uint4(0u, 0u, 0u, 0u);
+                if (draws)
+                    w4 = philox4((uint32_t)(r * Gw + cq), (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32), ch.chain,
+                                 key0, key1);
+#pragma unroll
+                for (int bb = 0; bb < 4; ++bb) {
+                    const int j = 4 * cq + bb;
+                    if (j < width) R::site_on(x, r, j, quad_word(w4, bb) >> 9);
+                }
+                rr += drr;
+                cq += dq;
+                if (cq >= Gw) {
+                    cq -= Gw;
+                    ++rr;
+                }
+            }
+            if (draws) ++dstep;
+            if (CL > 1) {
+                cluster.sync();
+                uint32_t mask = R::written(d);
+                if (nrows > 0) {
+                    while (mask) {
+                        const int arr = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        for (int e = tid; e < 2 * W; e += BLOCK) {
+                            const int side = e >= W, xx = e - side * W;
+                            if ((side == 0 && rank == 0) || (side == 1 && r1 >= rows)) continue;
+                            const int mine = (side == 0 ? 0 : nrows + 1) * W + xx;
+                            const int theirs = (side == 0 ? rpc : 1) * W + xx;
+                            const int peer = rank + (side == 0 ? -1 : 1);
+                            if (arr < 5)
+                                p8[arr * plane + mine] = *cluster.map_shared_rank(p8 + arr * plane + theirs, peer);
+                            else
+                                p16[(arr - 5) * plane + mine] =
+                                    *cluster.map_shared_rank(p16 + (arr - 5) * plane + theirs, peer);
+                        }
+                    }
+                }
+                cluster.sync();
+            } else {
+                __syncthreads();
+            }
+        }
+        for (int c = 0; c < 8; ++c) {
+            int32_t* g = static_cast<int32_t*>(ch.arr[c]);
+            for (int e = tid; e < nrows * width; e += BLOCK) {
+                const int rr = e / width, j = e % width;
+                const int at = (rr + 1) * W + j;
+                g[(size_t)(r0 + rr) * width + j] = c < 5 ? (int32_t)p8[c * plane + at] : (int32_t)p16[(c - 5) * plane + at];
+            }
+        }
+        cluster_or_block_sync(cluster, CL);
+    }
+}
+
 using BatchFn = void (*)(BatchArgs);
 
 static BatchFn batch_fn(int family) {
@@ -311,7 +426,7 @@ static BatchFn batch_fn(int family) {
         case FAM_DOMINO_HB: return batch_word_kernel<FAM_DOMINO_HB>;
         case FAM_LOZENGE8: return batch_word_kernel<FAM_LOZENGE8>;
         case FAM_RECTTRI: return batch_site_kernel<ThreeColour<int32_t, RectTriRule>>;
-        case FAM_TRIDIMER: return batch_site_kernel<TriDimerRule>;
+        case FAM_TRIDIMER: return batch_td_kernel;
         default: return nullptr;
     }
 }
@@ -386,6 +501,10 @@ size_t smem_for(const Chain& c, int cl) {
     const int wpad = (c.width + 3) & ~3;
     if (word_fam(c.fam)) {
         return 16 + (size_t)c.ncol * (rpc + 2) * wpad + 16 + (size_t)((2 * rpc + 3) & ~3) + 2 * 4 * (size_t)(wpad / 4);
+    }
+    if (c.fam == FAM_TRIDIMER) {  // batch_td_kernel: 5 byte planes, then 3 16-bit planes
+        const size_t plane = (size_t)(rpc + 2) * wpad;
+        return ((5 * plane + 15) & ~(size_t)15) + 3 * plane * 2;
     }
     return (size_t)c.ncol * (rpc + 2) * wpad * 4;
 }
@@ -558,6 +677,13 @@ rt_status upload(rt_batch* b) {
             if (c.kind == 3) {
                 std::vector<int32_t> arrays((size_t)8 * c.arows * c.width);
                 td_split_host(c.start.data(), c.n, arrays.data());
+                // batch_td_kernel keeps arrays 0-4 as bytes and 5-7 as 16-bit words
+                const size_t per = (size_t)c.arows * c.width;
+                for (size_t e = 0; e < 8 * per; ++e) {
+                    const int32_t v = arrays[e];
+                    if (e < 5 * per ? (v < 0 || v > 255) : (v < -32768 || v > 32767))
+                        return b->fail(RT_E_INVAL, "triangle-dimer state out of range for the batch storage");
+                }
                 for (int a = 0; a < 8; ++a)
                     cudaMemcpyAsync(arr[a], arrays.data() + (size_t)a * c.arows * c.width,
                                     (size_t)c.arows * c.width * 4, cudaMemcpyHostToDevice, b->stream);

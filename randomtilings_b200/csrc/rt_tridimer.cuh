@@ -63,10 +63,35 @@ struct TriDimerRule {
             default: return 0u;
         }
     }
+    // Storage of the eight arrays: int32 planes (the walk kernels), or the
+    // batch kernel's mixed widths (MixedCtx).  Either way the rule reads and
+    // writes values through get / set, so the arithmetic is the same.
     struct Ctx {
         int32_t* base;
         int plane, w, m, row0;
         uint32_t op, a, b;
+        __device__ int32_t get(int arr, int ii, int jj) const { return base[arr * plane + (ii - row0) * w + jj]; }
+        __device__ void set(int arr, int ii, int jj, int32_t v) const { base[arr * plane + (ii - row0) * w + jj] = v; }
+    };
+    // The batch kernel's storage: arrays 0-4 (lozenge and triangle states,
+    // values < 64) as bytes, arrays 5-7 (butterfly states, values < 512) as
+    // 16-bit words; `plane` elements per array in either width.
+    struct MixedCtx {
+        uint8_t* p8;
+        int16_t* p16;
+        int plane, w, m, row0;
+        uint32_t op, a, b;
+        __device__ int32_t get(int arr, int ii, int jj) const {
+            const int o = (ii - row0) * w + jj;
+            return arr < 5 ? (int32_t)p8[arr * plane + o] : (int32_t)p16[(arr - 5) * plane + o];
+        }
+        __device__ void set(int arr, int ii, int jj, int32_t v) const {
+            const int o = (ii - row0) * w + jj;
+            if (arr < 5)
+                p8[arr * plane + o] = (uint8_t)v;
+            else
+                p16[(arr - 5) * plane + o] = (int16_t)v;
+        }
     };
     __device__ static Ctx ctx(const WalkArgs& ar, int32_t* planes, int plane, uint32_t d, int row0) {
         Ctx x;
@@ -94,8 +119,9 @@ struct TriDimerRule {
 
     // Butterfly state of orientation `which` from the lozenge arrays
     // (UpdateButterflys{H,L,R}FromLozenge, triangledimerkernel.cl:118-189).
-    template <class At>
-    __device__ static int32_t bfly_from_loz(At at, int which, int i, int j) {
+    template <class A>
+    __device__ static int32_t bfly_from_loz(const A& x, int which, int i, int j) {
+        auto at = [&](int arr, int ii, int jj) { return x.get(arr, ii, jj); };
         int t1, t4, t16, t64, c;
         if (which == 0) {
             const int32_t h = at(0, i, j), ru = at(2, i - 1, j), lu = at(1, i - 1, j + 1), r = at(2, i, j), l = at(1, i, j);
@@ -123,8 +149,9 @@ struct TriDimerRule {
     }
 
     // Up-triangle state from the lozenges (UpdateTriangleUFromLozenges, :96-116).
-    template <class At>
-    __device__ static int32_t up_from_loz(At at, int i, int j) {
+    template <class A>
+    __device__ static int32_t up_from_loz(const A& acc, int i, int j) {
+        auto at = [&](int arr, int ii, int jj) { return acc.get(arr, ii, jj); };
         const int32_t l0 = at(1, i, j), l1 = at(1, i, j + 1), h0 = at(0, i, j), h1 = at(0, i + 1, j);
         const int x = ((l0 & 1) ? 1 : 0) + ((h0 & 8) ? 2 : 0) + ((h1 & 1) ? 3 : 0);
         const int y = ((l1 & 1) ? 1 : 0) + ((h1 & 2) ? 2 : 0) + ((l1 & 2) ? 3 : 0);
@@ -135,18 +162,20 @@ struct TriDimerRule {
     __device__ static int slice(int t, int i, int j) { return t == 0 ? i % 3 : t == 1 ? j % 3 : (i + j) % 3; }
     __device__ static int bpar(int t, int i, int j) { return t == 1 ? (i & 1) : (j & 1); }
 
-    __device__ static void site(const WalkArgs&, const Ctx& x, int, int i, int j, uint32_t k) {
-        auto at = [&](int arr, int ii, int jj) -> int32_t& {
-            return x.base[arr * x.plane + (ii - x.row0) * x.w + jj];
-        };
+    __device__ static void site(const WalkArgs&, const Ctx& x, int, int i, int j, uint32_t k) { site_on(x, i, j, k); }
+
+    template <class A>
+    __device__ static void site_on(const A& x, int i, int j, uint32_t k) {
+        auto at = [&](int arr, int ii, int jj) { return x.get(arr, ii, jj); };
+        auto put = [&](int arr, int ii, int jj, int32_t v) { x.set(arr, ii, jj, v); };
         const bool interior = i >= 1 && i <= x.m - 2 && j >= 1 && j <= x.m - 2;
         const int t = (int)x.a;
         switch (x.op) {
             case TD_ROT_LOZ: {  // :4-22
                 const int cls = ((1 - (t & 1)) * i + ((1 + t) / 2) * j) % 2;
                 if (k < (1u << 22) && cls == (int)x.b) {
-                    int32_t& v = at(t, i, j);
-                    v = v == 5 ? 10 : v == 10 ? 5 : v;
+                    const int32_t v = at(t, i, j);
+                    put(t, i, j, v == 5 ? 10 : v == 10 ? 5 : v);
                 }
                 break;
             }
@@ -154,40 +183,40 @@ struct TriDimerRule {
                 const int cls = ((1 - (t & 1)) * i + ((1 + t) / 2) * j) % 2;
                 if (!interior || cls == (int)x.b) break;
                 const int dj = t & 1, di = (2 - t) / 2;
-                at(t, i, j) = ((at(t, i - 1, j + dj) >> 2) & 1) | (((at(t, i - di, j + 1) >> 3) & 1) << 1) |
-                              ((at(t, i + 1, j - dj) & 1) << 2) | (((at(t, i + di, j - 1) >> 1) & 1) << 3);
+                put(t, i, j, ((at(t, i - 1, j + dj) >> 2) & 1) | (((at(t, i - di, j + 1) >> 3) & 1) << 1) |
+                              ((at(t, i + 1, j - dj) & 1) << 2) | (((at(t, i + di, j - 1) >> 1) & 1) << 3));
                 break;
             }
             case TD_LOZ_OTHER: {  // :35-78
                 if (!interior) break;
                 if (t == 0) {
-                    at(1, i, j) = (at(1, i, j) & ~10) | ((at(0, i + 1, j) & 1) << 1) | ((at(0, i + 1, j - 1) & 1) << 3);
-                    at(2, i, j) = (at(2, i, j) & ~10) | (at(0, i + 1, j) & 2) | (at(0, i, j) & 8);
+                    put(1, i, j, (at(1, i, j) & ~10) | ((at(0, i + 1, j) & 1) << 1) | ((at(0, i + 1, j - 1) & 1) << 3));
+                    put(2, i, j, (at(2, i, j) & ~10) | (at(0, i + 1, j) & 2) | (at(0, i, j) & 8));
                 } else if (t == 1) {
-                    at(2, i, j) = (at(2, i, j) & ~5) | (at(1, i, j) & 1) | ((at(1, i + 1, j) & 1) << 2);
-                    at(0, i, j) = (at(0, i, j) & ~5) | ((at(1, i - 1, j) & 2) >> 1) | ((at(1, i, j) & 2) << 1);
+                    put(2, i, j, (at(2, i, j) & ~5) | (at(1, i, j) & 1) | ((at(1, i + 1, j) & 1) << 2));
+                    put(0, i, j, (at(0, i, j) & ~5) | ((at(1, i - 1, j) & 2) >> 1) | ((at(1, i, j) & 2) << 1));
                 } else {
-                    at(0, i, j) = (at(0, i, j) & ~10) | (at(2, i - 1, j) & 2) | ((at(2, i, j - 1) & 2) << 2);
-                    at(1, i, j) = (at(1, i, j) & ~5) | (at(2, i, j) & 1) | (at(2, i, j - 1) & 4);
+                    put(0, i, j, (at(0, i, j) & ~10) | (at(2, i - 1, j) & 2) | ((at(2, i, j - 1) & 2) << 2));
+                    put(1, i, j, (at(1, i, j) & ~5) | (at(2, i, j) & 1) | (at(2, i, j - 1) & 4));
                 }
                 break;
             }
             case TD_UP_FROM_LOZ:
-                if (interior) at(3, i, j) = up_from_loz(at, i, j);
+                if (interior) put(3, i, j, up_from_loz(x, i, j));
                 break;
             case TD_TRI_OTHER: {  // :255-275, then :118-189 for the butterflies in b
                 if (!interior) break;
                 const int src = t == 0 ? 3 : 4, dst = t == 0 ? 4 : 3, p = t == 0 ? -1 : 1;
-                at(dst, i, j) = tri_digit(at(src, i, j - 1 + t)) + 4 * tri_digit(at(src, i, j + t)) +
-                                16 * tri_digit(at(src, i + p, j));
+                put(dst, i, j, tri_digit(at(src, i, j - 1 + t)) + 4 * tri_digit(at(src, i, j + t)) +
+                                16 * tri_digit(at(src, i + p, j)));
                 for (int w = 0; w < 3; ++w)
-                    if (x.b & (1u << w)) at(5 + w, i, j) = bfly_from_loz(at, w, i, j);
+                    if (x.b & (1u << w)) put(5 + w, i, j, bfly_from_loz(x, w, i, j));
                 break;
             }
             case TD_ROT_TRI: {  // :191-211
                 if (k < (1u << 22) && ((j - i) % 3 + 3) % 3 == (int)x.b) {
-                    int32_t& v = at(t == 1 ? 4 : 3, i, j);
-                    v = v == 45 ? 54 : v == 54 ? 45 : v;
+                    const int32_t v = at(t == 1 ? 4 : 3, i, j);
+                    put(t == 1 ? 4 : 3, i, j, v == 45 ? 54 : v == 54 ? 45 : v);
                 }
                 break;
             }
@@ -203,29 +232,29 @@ struct TriDimerRule {
                 else
                     v = p ? dg(at(arr, i, j - 1), 1) + 4 * dg(at(arr, i + 1, j), 2) + 16 * dg(at(arr, i - 1, j + 1), 0)
                           : dg(at(arr, i + 1, j - 1), 2) + 4 * dg(at(arr, i, j + 1), 0) + 16 * dg(at(arr, i - 1, j), 1);
-                at(arr, i, j) = v;
+                put(arr, i, j, v);
                 break;
             }
             case TD_LOZ_FROM_TRI: {  // :277-329
                 if (!interior) break;
                 const int32_t dd = at(4, i, j), uh = at(3, i - 1, j), ul = at(3, i, j - 1), ur = at(3, i, j);
-                at(0, i, j) = ((dd & 48) == 32) + 2 * ((dd & 48) == 48) + 4 * ((uh & 48) == 48) + 8 * ((uh & 48) == 32);
-                at(1, i, j) = ((ul & 12) == 4) + 2 * ((ul & 12) == 12) + 4 * ((dd & 3) == 1) + 8 * ((dd & 3) == 2);
-                at(2, i, j) = ((ur & 3) == 1) + 2 * ((dd & 12) == 12) + 4 * ((dd & 12) == 4) + 8 * ((ur & 3) == 2);
+                put(0, i, j, ((dd & 48) == 32) + 2 * ((dd & 48) == 48) + 4 * ((uh & 48) == 48) + 8 * ((uh & 48) == 32));
+                put(1, i, j, ((ul & 12) == 4) + 2 * ((ul & 12) == 12) + 4 * ((dd & 3) == 1) + 8 * ((dd & 3) == 2));
+                put(2, i, j, ((ur & 3) == 1) + 2 * ((dd & 12) == 12) + 4 * ((dd & 12) == 4) + 8 * ((ur & 3) == 2));
                 break;
             }
             case TD_BFLY_FROM_LOZ:
                 if (!interior) break;
                 for (int w = 0; w < 3; ++w)
-                    if (x.b & (1u << w)) at(5 + w, i, j) = bfly_from_loz(at, w, i, j);
-                if (x.a) at(3, i, j) = up_from_loz(at, i, j);
+                    if (x.b & (1u << w)) put(5 + w, i, j, bfly_from_loz(x, w, i, j));
+                if (x.a) put(3, i, j, up_from_loz(x, i, j));
                 break;
             case TD_ROT_BFLY: {  // :331-353
                 const int p1 = (int)(x.b & 3), p2 = (int)(x.b >> 2);
                 const int b1 = 1 - (t & 1), b2 = (1 + t) / 2, b3 = t & 1;
                 if (k < (1u << 22) && (b1 * i + b2 * j) % 3 == p1 && ((b1 * j + b3 * i) & 1) == p2) {
-                    int32_t& v = at(5 + t, i, j);
-                    v = v == 170 ? 85 : v == 85 ? 170 : v;
+                    const int32_t v = at(5 + t, i, j);
+                    put(5 + t, i, j, v == 170 ? 85 : v == 85 ? 170 : v);
                 }
                 break;
             }
@@ -249,7 +278,7 @@ struct TriDimerRule {
                     t16 = cyc_up(dg(v, 3));
                     t64 = cyc_dn(dg(u, 2));
                 }
-                at(arr, i, j) = pack(t1, t4, t16, t64, c);
+                put(arr, i, j, pack(t1, t4, t16, t64, c));
                 break;
             }
             case TD_BFLY_21: {
@@ -275,7 +304,7 @@ struct TriDimerRule {
                     t16 = dg(f, 2);
                     t64 = dg(f, 3);
                 }
-                at(arr, i, j) = pack(t1, t4, t16, t64, c);
+                put(arr, i, j, pack(t1, t4, t16, t64, c));
                 break;
             }
             case TD_BFLY_22: {
@@ -303,7 +332,7 @@ struct TriDimerRule {
                     t16 = dg(f, 2) == 2 ? 2 : 3 * (dg(n3, 0) == 3) + (dg(n3, 1) == 3);
                     t64 = dg(f, 3) == 1 ? 1 : 2 * (dg(n4, 0) == 3) + 3 * (dg(n4, 1) == 3);
                 }
-                at(arr, i, j) = pack(t1, t4, t16, t64, c);
+                put(arr, i, j, pack(t1, t4, t16, t64, c));
                 break;
             }
             case TD_BFLY_23_LOZ: {
@@ -323,24 +352,24 @@ struct TriDimerRule {
                         t16 = (n3 & 256) ? 2 : (dg(f, 2) != 2) * dg(f, 2);
                         t64 = (n4 & 256) ? 1 : (dg(f, 3) != 1) * dg(f, 3);
                     }
-                    at(arr, i, j) = pack(t1, t4, t16, t64, (f >> 8) & 1);
+                    put(arr, i, j, pack(t1, t4, t16, t64, (f >> 8) & 1));
                 }
                 // UpdateLozengeFromButterflys{H,L,R} (:655-746), own site only.
                 const int32_t bf = at(arr, i, j);
                 const int d0 = dg(bf, 0), d1 = dg(bf, 1), d2 = dg(bf, 2), d3 = dg(bf, 3), c = (bf >> 8) & 1;
                 const int32_t own = (d0 == 3) + 2 * (d1 == 3) + 4 * (d2 == 3) + 8 * (d3 == 3);
                 if (t == 0) {
-                    at(0, i, j) = own;
-                    at(1, i, j) = c + 2 * (d2 == 3) + 4 * (d3 == 1) + 8 * (d3 == 2);
-                    at(2, i, j) = c + 2 * (d2 == 1) + 4 * (d2 == 2) + 8 * (d3 == 3);
+                    put(0, i, j, own);
+                    put(1, i, j, c + 2 * (d2 == 3) + 4 * (d3 == 1) + 8 * (d3 == 2));
+                    put(2, i, j, c + 2 * (d2 == 1) + 4 * (d2 == 2) + 8 * (d3 == 3));
                 } else if (t == 1) {
-                    at(1, i, j) = own;
-                    at(2, i, j) = (d0 == 3) + 2 * (d1 == 1) + 4 * (d1 == 2) + 8 * c;
-                    at(0, i, j) = (d0 == 1) + 2 * (d0 == 2) + 4 * (d1 == 3) + 8 * c;
+                    put(1, i, j, own);
+                    put(2, i, j, (d0 == 3) + 2 * (d1 == 1) + 4 * (d1 == 2) + 8 * c);
+                    put(0, i, j, (d0 == 1) + 2 * (d0 == 2) + 4 * (d1 == 3) + 8 * c);
                 } else {
-                    at(2, i, j) = own;
-                    at(0, i, j) = (d0 == 1) + 2 * (d0 == 2) + 4 * c + 8 * (d3 == 3);
-                    at(1, i, j) = (d0 == 3) + 2 * c + 4 * (d3 == 1) + 8 * (d3 == 2);
+                    put(2, i, j, own);
+                    put(0, i, j, (d0 == 1) + 2 * (d0 == 2) + 4 * c + 8 * (d3 == 3));
+                    put(1, i, j, (d0 == 3) + 2 * c + 4 * (d3 == 1) + 8 * (d3 == 2));
                 }
                 break;
             }

@@ -269,9 +269,9 @@ class WarmStart:
 
 
 class _Chains:
-    """Fast-mode chains that advance together: a Batch where the domain fits
-    one (cluster shared memory), else one Tiler per chain.  Chains given the
-    same key share their draws (coupled)."""
+    """Chains that advance together: a Batch (fast mode) where the domain is
+    small, else one bit-plane Tiler (RT_RNG_PLANES) per chain, which uses the
+    whole GPU for one lattice.  Chains given the same key share their draws."""
 
     def __init__(self, p: Prepared, starts: list[np.ndarray], keys: list[int], device: int, use_batch: bool,
                  heat_bath: bool = False):
@@ -290,7 +290,7 @@ class _Chains:
             if p.spec.q < 1.0:
                 raise ValueError("volume-weighted chains run in batches")
             for t in starts:
-                tl = p.spec.tiler(device=device, kernel=kernel, rng=_capi.RT_RNG_PHILOX)
+                tl = p.spec.tiler(device=device, kernel=kernel, rng=_capi.RT_RNG_PLANES)
                 tl.upload(t)
                 self.tilers.append(tl)
         self.device_ms = 0.0
@@ -331,20 +331,19 @@ class _Chains:
 
 
 def relax(p: Prepared, starts: dict, sweeps: int, points: int = 40, replicas: int = 1, seed: int = 0,
-          device: int = 0, use_batch: bool | None = None, ref_tail: float = 0.2, threshold: float = 0.005,
+          device: int = 0, use_batch: bool | None = None, ref_tail: float = 0.25, threshold: float = 0.005,
           cftp_ref: np.ndarray | None = None, heat_bath: bool = False, log=None) -> dict:
     """Error curves of the named starting tilings (e.g. {"cold": tmin, "warm": tw}).
 
-    Every start runs `replicas` chains (replica r of every start shares its
-    draws); one more chain starts from the maximal tiling with replica 0's
-    draws: with the monotone rules (lozenges; dominoes with heat_bath) it is
-    the top of a coupled sandwich whose bottom is the cold start, otherwise
-    its mean height approaches the equilibrium from above as the cold one
-    does from below.
+    Every start runs `replicas` independent chains (own Philox keys); as many
+    more start from the maximal tiling ("top"): their mean height approaches
+    the equilibrium from above as the cold start's does from below, and the
+    sandwich gap is the mean over vertices of |top mean - cold mean| / side.
     At `points` checkpoints (geometric in sweeps up to `sweeps`) the mean
     height of each start's replicas is recorded on the device.  The reference
     surface is `cftp_ref` when given, else the mean of all chains over the
-    checkpoints in the last `ref_tail` of the run."""
+    checkpoints in the last `ref_tail` of the run (eight evenly spaced ones
+    are added there to the geometric grid)."""
     import torch
 
     dev = f"cuda:{device}"
@@ -354,23 +353,18 @@ def relax(p: Prepared, starts: dict, sweeps: int, points: int = 40, replicas: in
         # small domains: many chains per launch; large ones: the whole GPU per chain
         use_batch = p.n <= 300 or (replicas > 1 and p.n <= 900)
     tilings, keys, owner = [], [], []
-    for name in names:
+    for x, name in enumerate(names + ["top"]):
         for r in range(replicas):
-            tilings.append(np.asarray(starts[name], dtype=np.int32))
-            keys.append(seed * 7919 + r)
+            tilings.append(np.asarray(starts[name] if name != "top" else p.tmax, dtype=np.int32))
+            keys.append((seed * 1_000_003 + x) * 7919 + r)
             owner.append(name)
-    tilings.append(p.tmax)
-    keys.append(seed * 7919)
-    owner.append("top")
     chains = _Chains(p, tilings, keys, device, use_batch, heat_bath)
     plan = HeightPlan(p.spec.model, p.domain, device)
     buf = torch.empty(p.n * p.n, dtype=torch.int32, device=dev)
     idx = torch.from_numpy(p.idx).to(dev)
-    marks = sorted({0} | {int(round(x)) for x in np.geomspace(1, sweeps, points)})
+    marks = sorted({0} | {int(round(x)) for x in np.geomspace(1, sweeps, points)} |
+                   {int(round(x)) for x in np.linspace((1.0 - ref_tail) * sweeps, sweeps, 8)})
     saved = {name: [] for name in names + ["top"]}
-    # bottom of the sandwich: the chain from the minimal tiling that shares the top's draws
-    bottom = next((c for c, (t, k) in enumerate(zip(tilings, keys))
-                   if k == keys[-1] and c < len(tilings) - 1 and np.array_equal(t, p.tmin)), None)
     gap = []
     done = 0
     t0 = time.perf_counter()
@@ -378,17 +372,12 @@ def relax(p: Prepared, starts: dict, sweeps: int, points: int = 40, replicas: in
         chains.advance(m - done)
         done = m
         sums = {name: torch.zeros(p.n * p.n, dtype=torch.int64, device=dev) for name in saved}
-        low = torch.zeros(p.n * p.n, dtype=torch.int64, device=dev)
         for c, name in enumerate(owner):
-            ptr = chains.tiling_ptr(c, buf)
-            plan.accumulate(ptr, sums[name].data_ptr())
-            if c == bottom:
-                plan.accumulate(ptr, low.data_ptr())
+            plan.accumulate(chains.tiling_ptr(c, buf), sums[name].data_ptr())
         for name in saved:
-            cnt = replicas if name != "top" else 1
-            saved[name].append((sums[name].index_select(0, idx).double() / cnt).float())
-        if bottom is not None:
-            gap.append(float((sums["top"] - low).index_select(0, idx).abs().double().mean() / side))
+            saved[name].append((sums[name].index_select(0, idx).double() / replicas).float())
+        if "cold" in saved:
+            gap.append(float((saved["top"][-1] - saved["cold"][-1]).abs().double().mean() / side))
         if log and len(saved[names[0]]) % 10 == 0:
             log(f"  {p.spec.label()}: {m} sweeps, wall {time.perf_counter() - t0:.0f} s")
     if cftp_ref is not None:
@@ -398,10 +387,9 @@ def relax(p: Prepared, starts: dict, sweeps: int, points: int = 40, replicas: in
         tail = [k for k, m in enumerate(marks) if m >= (1.0 - ref_tail) * sweeps] or [len(marks) - 1]
         acc = torch.zeros(p.idx.size, dtype=torch.float64, device=dev)
         for k in tail:
-            for name in names:
-                acc += saved[name][k].double() * replicas
-            acc += saved["top"][k].double()
-        ref = (acc / (len(tail) * (replicas * len(names) + 1))).float()
+            for name in saved:
+                acc += saved[name][k].double()
+        ref = (acc / (len(tail) * len(saved))).float()
         ref_kind = f"long-chain mean over the last {ref_tail:.0%} of the run"
     curves = {name: [float((h - ref).abs().double().mean() / side) for h in saved[name]] for name in saved}
     out = {"domain": p.spec.label(), "side": side, "sweeps": marks, "reference": ref_kind, "replicas": replicas,
@@ -431,7 +419,7 @@ def main(argv=None) -> None:
     ap.add_argument("--burn-factor", type=float, default=1.0)
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--eval", nargs="+", default=["aztec:2000", "hexagon:1000"])
-    ap.add_argument("--eval-sweeps", type=float, default=1.0,
+    ap.add_argument("--eval-sweeps", type=float, default=2.0,
                     help="length of the comparison, in units of the cold start's burn-in")
     ap.add_argument("--points", type=int, default=40)
     ap.add_argument("--seed", type=int, default=0)

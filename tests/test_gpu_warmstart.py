@@ -12,7 +12,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-THRESHOLD = 0.01  # mean-height error, fraction of the side (16 replicas per start at these sizes)
+THRESHOLD = 0.02  # mean-height error, fraction of the side (32 replicas per start at these sizes)
 
 
 @pytest.fixture(scope="module")
@@ -46,7 +46,7 @@ def test_warm_start_beats_cold_and_untrained(trained, kind, size):
     h = np.asarray(spec.tiler.TilingToHeightfunc(tw, p.domain), dtype=np.int64)
     assert np.all(h[p.idx] >= p.hmin[p.idx]) and np.all(h[p.idx] <= p.hmax[p.idx])
     tu, _ = ws.WarmStart(seed=11).warm_tiling(p)  # the same pipeline, untrained network
-    r = ws.relax(p, {"cold": p.tmin, "warm": tw, "untrained": tu}, ws.burn_sweeps(spec), points=30, replicas=16,
+    r = ws.relax(p, {"cold": p.tmin, "warm": tw, "untrained": tu}, 2 * ws.burn_sweeps(spec), points=30, replicas=32,
                  threshold=THRESHOLD)
     s = r["sweeps_to_threshold"]
     assert r["sandwich_gap"][-1] < THRESHOLD, r["sandwich_gap"][-5:]
