@@ -303,6 +303,41 @@ __global__ void __launch_bounds__(1024, 1) batch_site_kernel(const __grid_consta
     }
 }
 
+// One phase of op OP over the band rows [r0, r0 + nrows) of a triangle-dimer
+// chain: only the rows TriDimerRule::live_rows admits, four sites (one Philox
+// call in drawing phases) per work item.
+template <uint32_t OP>
+__device__ __forceinline__ void td_phase(const TriDimerRule::MixedCtx& x, int r0, int nrows, int width, int tid,
+                                         int BLOCK, int64_t dstep, uint32_t chain, uint32_t key0, uint32_t key1) {
+    constexpr bool DRAWS = OP == TD_ROT_LOZ || OP == TD_ROT_TRI || OP == TD_ROT_BFLY;
+    int S, o;
+    TriDimerRule::live_rows<OP>(x.a, x.b, &S, &o);
+    const int first = r0 + ((o - r0) % S + S) % S;
+    if (first >= r0 + nrows) return;
+    const int nlive = (r0 + nrows - first + S - 1) / S;
+    const int Gw = (width + 3) >> 2;
+    const int nq = nlive * Gw;
+    const int drr = BLOCK / Gw, dq = BLOCK - drr * Gw;
+    int rr = tid / Gw, cq = tid - (tid / Gw) * Gw;
+    for (int u = tid; u < nq; u += BLOCK) {
+        const int r = first + S * rr;
+        uint4 w4 = make_uint4(0u, 0u, 0u, 0u);
+        if (DRAWS)
+            w4 = philox4((uint32_t)(r * Gw + cq), (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32), chain, key0, key1);
+#pragma unroll
+        for (int bb = 0; bb < 4; ++bb) {
+            const int j = 4 * cq + bb;
+            if (j < width) TriDimerRule::site_op<OP>(x, r, j, quad_word(w4, bb) >> 9);
+        }
+        rr += drr;
+        cq += dq;
+        if (cq >= Gw) {
+            cq -= Gw;
+            ++rr;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Triangle dimers: the eight arrays in mixed widths (TriDimerRule::MixedCtx):
 // arrays 0-4 as bytes, 5-7 as 16-bit words, 52 KB for a side-64 chain
@@ -344,9 +379,6 @@ __global__ void __launch_bounds__(1024, 1) batch_td_kernel(const __grid_constant
 
         const uint32_t key0 = (uint32_t)ch.key, key1 = (uint32_t)(ch.key >> 32);
         int64_t dstep = *b.step0;
-        const int Gw = (width + 3) >> 2;
-        const int nq = nrows * Gw;
-        const int drr = BLOCK / Gw, dq = BLOCK - drr * Gw;
         for (int64_t ph = 0; ph < b.nphases; ++ph) {
             const uint32_t d = __ldg(b.phases + ph);
             const bool draws = (d & PH_DRAWS) != 0u;
@@ -360,24 +392,25 @@ __global__ void __launch_bounds__(1024, 1) batch_td_kernel(const __grid_constant
             x.op = ph_op(d);
             x.a = ph_a(d);
             x.b = ph_b(d);
-            int rr = tid / Gw, cq = tid - (tid / Gw) * Gw;
-            for (int u = tid; u < nq; u += BLOCK) {
-                const int r = r0 + rr;
-                uint4 w4 = make_uint4(0u, 0u, 0u, 0u);
-                if (draws)
-                    w4 = philox4((uint32_t)(r * Gw + cq), (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32), ch.chain,
-                                 key0, key1);
-#pragma unroll
-                for (int bb = 0; bb < 4; ++bb) {
-                    const int j = 4 * cq + bb;
-                    if (j < width) R::site_on(x, r, j, quad_word(w4, bb) >> 9);
-                }
-                rr += drr;
-                cq += dq;
-                if (cq >= Gw) {
-                    cq -= Gw;
-                    ++rr;
-                }
+            switch (x.op) {
+#define RT_TD_PHASE(OPC) \
+    case OPC: td_phase<OPC>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1); break;
+                RT_TD_PHASE(TD_ROT_LOZ)
+                RT_TD_PHASE(TD_LOZ_FLIPPED)
+                RT_TD_PHASE(TD_LOZ_OTHER)
+                RT_TD_PHASE(TD_UP_FROM_LOZ)
+                RT_TD_PHASE(TD_TRI_OTHER)
+                RT_TD_PHASE(TD_ROT_TRI)
+                RT_TD_PHASE(TD_TRI_FLIPPED)
+                RT_TD_PHASE(TD_LOZ_FROM_TRI)
+                RT_TD_PHASE(TD_BFLY_FROM_LOZ)
+                RT_TD_PHASE(TD_ROT_BFLY)
+                RT_TD_PHASE(TD_BFLY_SAME)
+                RT_TD_PHASE(TD_BFLY_21)
+                RT_TD_PHASE(TD_BFLY_22)
+                RT_TD_PHASE(TD_BFLY_23_LOZ)
+#undef RT_TD_PHASE
+                default: break;
             }
             if (draws) ++dstep;
             if (CL > 1) {

@@ -164,13 +164,15 @@ struct TriDimerRule {
 
     __device__ static void site(const WalkArgs&, const Ctx& x, int, int i, int j, uint32_t k) { site_on(x, i, j, k); }
 
-    template <class A>
-    __device__ static void site_on(const A& x, int i, int j, uint32_t k) {
+    // One site of the phase whose op is OP (a compile-time constant: every
+    // other case of the switch below folds away).
+    template <uint32_t OP, class A>
+    __device__ static void site_op(const A& x, int i, int j, uint32_t k) {
         auto at = [&](int arr, int ii, int jj) { return x.get(arr, ii, jj); };
         auto put = [&](int arr, int ii, int jj, int32_t v) { x.set(arr, ii, jj, v); };
         const bool interior = i >= 1 && i <= x.m - 2 && j >= 1 && j <= x.m - 2;
         const int t = (int)x.a;
-        switch (x.op) {
+        switch (OP) {
             case TD_ROT_LOZ: {  // :4-22
                 const int cls = ((1 - (t & 1)) * i + ((1 + t) / 2) * j) % 2;
                 if (k < (1u << 22) && cls == (int)x.b) {
@@ -375,6 +377,47 @@ struct TriDimerRule {
             }
             default: break;
         }
+    }
+
+    template <class A>
+    __device__ static void site_on(const A& x, int i, int j, uint32_t k) {
+        switch (x.op) {
+            case TD_ROT_LOZ: site_op<TD_ROT_LOZ>(x, i, j, k); break;
+            case TD_LOZ_FLIPPED: site_op<TD_LOZ_FLIPPED>(x, i, j, k); break;
+            case TD_LOZ_OTHER: site_op<TD_LOZ_OTHER>(x, i, j, k); break;
+            case TD_UP_FROM_LOZ: site_op<TD_UP_FROM_LOZ>(x, i, j, k); break;
+            case TD_TRI_OTHER: site_op<TD_TRI_OTHER>(x, i, j, k); break;
+            case TD_ROT_TRI: site_op<TD_ROT_TRI>(x, i, j, k); break;
+            case TD_TRI_FLIPPED: site_op<TD_TRI_FLIPPED>(x, i, j, k); break;
+            case TD_LOZ_FROM_TRI: site_op<TD_LOZ_FROM_TRI>(x, i, j, k); break;
+            case TD_BFLY_FROM_LOZ: site_op<TD_BFLY_FROM_LOZ>(x, i, j, k); break;
+            case TD_ROT_BFLY: site_op<TD_ROT_BFLY>(x, i, j, k); break;
+            case TD_BFLY_SAME: site_op<TD_BFLY_SAME>(x, i, j, k); break;
+            case TD_BFLY_21: site_op<TD_BFLY_21>(x, i, j, k); break;
+            case TD_BFLY_22: site_op<TD_BFLY_22>(x, i, j, k); break;
+            case TD_BFLY_23_LOZ: site_op<TD_BFLY_23_LOZ>(x, i, j, k); break;
+            default: break;
+        }
+    }
+
+    // The rows of phase (OP, a, b) that can hold a changing site: those with
+    // i = o (mod S).  Phases whose class condition depends on the row alone
+    // (i mod 2 or i mod 3 for orientation 0, i mod 2 for some of
+    // orientation 1) skip the other rows; all others have S = 1.
+    template <uint32_t OP>
+    __device__ static void live_rows(uint32_t a, uint32_t b, int* S, int* o) {
+        const int t = (int)a;
+        *S = 1;
+        *o = 0;
+        if (OP == TD_ROT_LOZ && t == 0) *S = 2, *o = (int)b;             // class i mod 2 == b
+        if (OP == TD_LOZ_FLIPPED && t == 0) *S = 2, *o = 1 - (int)b;     // class i mod 2 != b
+        if (OP == TD_ROT_BFLY || OP == TD_BFLY_SAME) {
+            const int p1 = (int)(b & 3), p2 = (int)(b >> 2);
+            if (t == 0) *S = 3, *o = p1;                                    // slice i mod 3 == p1
+            if (t == 1) *S = 2, *o = OP == TD_ROT_BFLY ? p2 : 1 - p2;      // parity i mod 2
+        }
+        if (OP == TD_BFLY_21 && t == 0) *S = 3, *o = ((int)b + 1) % 3;
+        if (OP == TD_BFLY_22 && t == 0) *S = 3, *o = ((int)b + 2) % 3;
     }
 };
 
