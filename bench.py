@@ -209,6 +209,46 @@ def time_e2e_walks(tiler_cls, kwargs, t0: np.ndarray, steps: int, warmup: int, s
     return out
 
 
+def run_legs(args) -> None:
+    """Profiling runs: only the walks named in args.legs (no JSON contract
+    line, no timing claims), each `args.steps` walks after `args.warmup`."""
+    import randomtilings_b200 as rt
+    from randomtilings_b200 import workloads
+
+    rt.load(build_if_missing=False)
+    legs = set(args.legs.split(","))
+    t0 = start_tiling()
+    kinds = {"headline": {}, "q": {"kernel": rt.RT_KERNEL_QWEIGHT, "q": 0.99, "qcmp": 0},
+             "fast": {"rng": rt.RT_RNG_PHILOX}, "planes": {"rng": rt.RT_RNG_PLANES}}
+    for name, kw in kinds.items():
+        if name not in legs:
+            continue
+        tl = rt.LozengeTiler(**kw)
+        tl.upload(t0)
+        for k in range(args.warmup + args.steps):
+            tl.run(STEPS_PER_WALK, SEED + k)
+        tl.synchronize()
+        tl.close()
+        print(f"{name}: {args.warmup + args.steps} walks of {STEPS_PER_WALK} colour steps", flush=True)
+    if "batch" in legs:
+        bt = rt.Batch()
+        models = None if args.batch_models == "all" else {int(m) for m in args.batch_models.split(",")}
+        n = 0
+        for seed in range(args.batch_chains):
+            model, spec = workloads.mixed_chain_spec(seed)
+            if models is not None and model not in models:
+                continue
+            bt.add(model, workloads.start_tiling(model, spec), key=seed, chain=seed)
+            n += 1
+        if args.batch_plan:
+            cl, block = (int(v) for v in args.batch_plan.split(","))
+            bt.set_tuning(False, cl, block)
+        bt.run(2)
+        bt.run(args.batch_sweeps)
+        print(f"batch: {n} chains, {args.batch_sweeps} sweeps, {bt.info()}", flush=True)
+        bt.close()
+
+
 def run_b200(args) -> None:
     import torch
 
@@ -538,11 +578,20 @@ def main() -> None:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--traffic", type=float, default=None,
+    # dram__bytes_read.sum + dram__bytes_write.sum of one word_kernel launch (ncu, 600-step capture,
+    # profiles/word_kernel_hex500.md): 1.146 MB + 3.1 KB; the lattice stays on chip, so a launch of
+    # any number of colour steps moves the same bytes.
+    ap.add_argument("--traffic", type=float, default=1149184.0,
                     help="dram bytes per walk launch from an ncu capture (reported in roofline.traffic)")
     ap.add_argument("--batch-chains", type=int, default=4096)
     ap.add_argument("--batch-sweeps", type=int, default=5000)
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--legs", default="all",
+                    help="profiling runs: comma-separated subset of headline,q,fast,planes,batch (no JSON line)")
+    ap.add_argument("--batch-models", default="all",
+                    help="with --legs batch: comma-separated rt_model values of the mixed workload to keep")
+    ap.add_argument("--batch-plan", default="",
+                    help="with --legs batch: 'cluster,block' instead of the autotuner (one launch per run)")
     ap.add_argument("--workload", choices=["walk", "cftp"], default="walk",
                     help="walk: the headline line (default); cftp: CFTP runs on an Aztec diamond")
     ap.add_argument("--cftp-order", type=int, default=500)
@@ -556,6 +605,8 @@ def main() -> None:
         ap.error("--warmup must be >= 3")
     if args.workload == "cftp":
         run_cftp(args)
+    elif args.legs != "all":
+        run_legs(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

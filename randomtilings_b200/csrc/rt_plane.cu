@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(LB, 1) plane_kernel(const __grid_constant__ Wa
     using M = PlaneModel<FAM>;
     constexpr int NC = M::NC, NP = M::NP;
     extern __shared__ __align__(16) uint32_t psm[];
-    __shared__ uint32_t s_dph[8];
+    __shared__ uint32_t s_dph[32];  // descriptors of the current block (depth <= 32)
     const int BLOCK = blockDim.x, tid = threadIdx.x;
     const int cta = blockIdx.x, nct = gridDim.x;
     const int H = a.depth, WW = a.pwords, RS = WW + 2;
@@ -79,10 +79,10 @@ __global__ void __launch_bounds__(LB, 1) plane_kernel(const __grid_constant__ Wa
     const int R = a.rows_per_cta + 2 * H;  // stored rows (rows_per_cta = ceil(rows / nct))
     const int a0 = r0 + M::ROFF;            // colour-array row of the band's first row
     const int N = a.n;
-    const size_t PLANE = (size_t)R * RS;
-    uint32_t* um_col = psm + (size_t)a.nlat * NC * NP * PLANE;
+    const int PLANE = R * RS;  // words per plane (shared memory: fits an int)
+    uint32_t* um_col = psm + a.nlat * NC * NP * PLANE;
     uint32_t* vm_col = um_col + WW;
-    auto pl = [&](int l, int c, int k) { return psm + ((size_t)(l * NC + c) * NP + k) * PLANE; };
+    auto pl = [&](int l, int c, int k) { return psm + ((l * NC + c) * NP + k) * PLANE; };
 
     for (int w = tid; w < WW; w += BLOCK) {
         um_col[w] = col_mask(w, 1, a.width - 1);
@@ -197,8 +197,26 @@ __global__ void __launch_bounds__(LB, 1) plane_kernel(const __grid_constant__ Wa
             const int s_lo = g_lo - (r0 - H);
             const int IPR = WPT == 1 ? WW : QPR;  // work items per row
             const int items = (g_hi - g_lo) * IPR;
+            // Plane offsets (32-bit shared-memory word indices) used by this phase,
+            // lattice 0; lattice l adds l * LAT.
+            const int LAT = NC * NP * PLANE;
+            int dst_off = 0, src_off = 0, tt_off = 0, t1_off = 0, t2_off = 0, ca_off = 0;
+            if (M::DOM) {
+                const int dst = step ? 1 - ca : ca;  // reference colour r flips array 1 - r
+                dst_off = dst * NP * PLANE;
+                src_off = (1 - dst) * NP * PLANE;
+            } else {
+                const int t1 = tt == 2 ? 0 : tt + 1, t2 = tt == 0 ? 2 : tt - 1;
+                tt_off = tt * NP * PLANE;
+                t1_off = t1 * NP * PLANE;
+                t2_off = t2 * NP * PLANE;
+                ca_off = ca * NP * PLANE;
+            }
+            const bool ca_is_t1 = !M::DOM && ca == (tt == 2 ? 0 : tt + 1);
+            int srow = s_lo + tid / IPR, it = tid - (tid / IPR) * IPR;
+            const int dsr = BLOCK / IPR, dit = BLOCK - dsr * IPR;
             for (int u = tid; u < items; u += BLOCK) {
-                const int s = s_lo + u / IPR, it = u % IPR;
+                const int s = srow;
                 const int i = a0 - H + s;  // colour-array row
                 uint4 r1 = make_uint4(0u, 0u, 0u, 0u), r2 = make_uint4(0u, 0u, 0u, 0u);
                 if (draws) {
@@ -208,29 +226,32 @@ __global__ void __launch_bounds__(LB, 1) plane_kernel(const __grid_constant__ Wa
                         r2 = philox4(c0 | 0x80000000u, (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32), a.chain,
                                      key0, key1);
                 }
+                const bool row_upd = i >= 1 && i <= N - 2;
+                const int p = (i ^ tt) & 1;                                                  // dominoes
+                const uint32_t sh = M::DOM ? 0u : (shifts >> (9 * tt + 3 * (i % 3))) & 7u;  // lozenges
 #pragma unroll
                 for (int x4 = 0; x4 < WPT; ++x4) {
                 const int w = WPT == 1 ? it : 4 * it + x4;
                 if (w >= WW) break;
-                const size_t o = (size_t)s * RS + w + 1;
-                const uint32_t um = (i >= 1 && i <= N - 2) ? um_col[w] : 0u;
+                const int o = s * RS + w + 1;
+                const uint32_t um = row_upd ? um_col[w] : 0u;
                 const uint32_t vm = vm_col[w];
                 const uint32_t b1 = quad_word(r1, w & 3), b2 = quad_word(r2, w & 3);
                 for (int l = 0; l < a.nlat; ++l) {
+                    uint32_t* const L = psm + l * LAT;
                     if (M::DOM) {
-                        // Reference colour r flips array 1 - r and refreshes array r from it.
-                        const int dst = step ? 1 - ca : ca, src = 1 - dst;
+                        uint32_t* const D = L + dst_off + o;
+                        const uint32_t* const S = L + src_off + o;
                         uint32_t v[4];
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) v[q] = pl(l, dst, q)[o];
+                        for (int q = 0; q < 4; ++q) v[q] = D[q * PLANE];
                         if (upd) {
                             // domino_refresh (dominokernel.cl:22-31): bit 1 <- up's bit 2,
                             // bit 2 <- down's bit 1, bit 4 <- west's bit 8, bit 8 <- east's bit 4;
                             // west / east share the column in rows of one parity.
-                            const int p = (i ^ tt) & 1;
-                            const uint32_t up = pl(l, src, 1)[o - RS], dn = pl(l, src, 0)[o + RS];
-                            const uint32_t* s3 = pl(l, src, 3) + o;
-                            const uint32_t* s2 = pl(l, src, 2) + o;
+                            const uint32_t up = S[PLANE - RS], dn = S[RS];
+                            const uint32_t* s3 = S + 3 * PLANE;
+                            const uint32_t* s2 = S + 2 * PLANE;
                             const uint32_t west = p ? s3[0] : col_prev(s3[-1], s3[0]);
                             const uint32_t east = p ? col_next(s2[0], s2[1]) : s2[0];
                             v[0] = (v[0] & ~um) | (up & um);
@@ -253,82 +274,81 @@ __global__ void __launch_bounds__(LB, 1) plane_kernel(const __grid_constant__ Wa
                             }
                         }
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) pl(l, dst, q)[o] = v[q];
+                        for (int q = 0; q < 4; ++q) D[q * PLANE] = v[q];
                     } else {
                         uint32_t v[6];
+                        uint32_t* const C = L + ca_off + o;
                         if (upd) {
                             // lozenge_refresh (lozengekernel.cl:36-54): colour t+1 takes bits
                             // {2, 4, 32} from the flipped colour t at (i-1, j+sa), (i, j-sw),
                             // (i+1, j); colour t+2 takes {1, 8, 16} from (i-1, j), (i, j+se),
                             // (i+1, j-sa).
-                            const int t1 = tt == 2 ? 0 : tt + 1, t2 = tt == 0 ? 2 : tt - 1;
-                            const uint32_t sh = (shifts >> (9 * tt + 3 * (i % 3))) & 7u;
-                            const uint32_t* f4 = pl(l, tt, 4) + o - RS;
-                            const uint32_t* f3 = pl(l, tt, 3) + o;
-                            const uint32_t* f1 = pl(l, tt, 1) + o + RS;
-                            const uint32_t* f2 = pl(l, tt, 2) + o;
+                            const uint32_t* const F = L + tt_off + o;
+                            const uint32_t* f4 = F + 4 * PLANE - RS;
+                            const uint32_t* f3 = F + 3 * PLANE;
+                            const uint32_t* f1 = F + PLANE + RS;
+                            const uint32_t* f2 = F + 2 * PLANE;
                             const uint32_t n1 = (sh & 1u) ? col_next(f4[0], f4[1]) : f4[0];
                             const uint32_t n2 = (sh & 2u) ? col_prev(f3[-1], f3[0]) : f3[0];
-                            const uint32_t n5 = pl(l, tt, 0)[o + RS];
-                            const uint32_t m0 = pl(l, tt, 5)[o - RS];
+                            const uint32_t n5 = F[RS];
+                            const uint32_t m0 = F[5 * PLANE - RS];
                             const uint32_t m3 = (sh & 4u) ? col_next(f2[0], f2[1]) : f2[0];
                             const uint32_t m4 = (sh & 1u) ? col_prev(f1[-1], f1[0]) : f1[0];
-                            uint32_t* A1 = pl(l, t1, 1);
-                            uint32_t* A2 = pl(l, t1, 2);
-                            uint32_t* A5 = pl(l, t1, 5);
-                            uint32_t* B0 = pl(l, t2, 0);
-                            uint32_t* B3 = pl(l, t2, 3);
-                            uint32_t* B4 = pl(l, t2, 4);
-                            const uint32_t a1 = (A1[o] & ~um) | (n1 & um), a2 = (A2[o] & ~um) | (n2 & um),
-                                           a5 = (A5[o] & ~um) | (n5 & um);
-                            const uint32_t c0v = (B0[o] & ~um) | (m0 & um), c3 = (B3[o] & ~um) | (m3 & um),
-                                           c4 = (B4[o] & ~um) | (m4 & um);
-                            if (step) {
-                                const int other = ca == t1 ? t2 : t1;
-                                // the colour not flipped now keeps its refreshed planes
-                                if (ca == t1) {
-                                    B0[o] = c0v;
-                                    B3[o] = c3;
-                                    B4[o] = c4;
-                                    v[1] = a1;
-                                    v[2] = a2;
-                                    v[5] = a5;
-                                    v[0] = pl(l, ca, 0)[o];
-                                    v[3] = pl(l, ca, 3)[o];
-                                    v[4] = pl(l, ca, 4)[o];
-                                } else {
-                                    A1[o] = a1;
-                                    A2[o] = a2;
-                                    A5[o] = a5;
-                                    v[0] = c0v;
-                                    v[3] = c3;
-                                    v[4] = c4;
-                                    v[1] = pl(l, ca, 1)[o];
-                                    v[2] = pl(l, ca, 2)[o];
-                                    v[5] = pl(l, ca, 5)[o];
-                                }
-                                (void)other;
-                            } else {
-                                A1[o] = a1;
-                                A2[o] = a2;
-                                A5[o] = a5;
-                                B0[o] = c0v;
-                                B3[o] = c3;
-                                B4[o] = c4;
+                            uint32_t* const A = L + t1_off + o;
+                            uint32_t* const B = L + t2_off + o;
+                            const uint32_t a1 = (A[PLANE] & ~um) | (n1 & um), a2 = (A[2 * PLANE] & ~um) | (n2 & um),
+                                           a5 = (A[5 * PLANE] & ~um) | (n5 & um);
+                            const uint32_t c0v = (B[0] & ~um) | (m0 & um), c3 = (B[3 * PLANE] & ~um) | (m3 & um),
+                                           c4 = (B[4 * PLANE] & ~um) | (m4 & um);
+                            if (!step) {
+                                A[PLANE] = a1;
+                                A[2 * PLANE] = a2;
+                                A[5 * PLANE] = a5;
+                                B[0] = c0v;
+                                B[3 * PLANE] = c3;
+                                B[4 * PLANE] = c4;
                                 continue;
+                            }
+                            // the colour not flipped now keeps its refreshed planes
+                            if (ca_is_t1) {
+                                B[0] = c0v;
+                                B[3 * PLANE] = c3;
+                                B[4 * PLANE] = c4;
+                                v[1] = a1;
+                                v[2] = a2;
+                                v[5] = a5;
+                                v[0] = C[0];
+                                v[3] = C[3 * PLANE];
+                                v[4] = C[4 * PLANE];
+                            } else {
+                                A[PLANE] = a1;
+                                A[2 * PLANE] = a2;
+                                A[5 * PLANE] = a5;
+                                v[0] = c0v;
+                                v[3] = c3;
+                                v[4] = c4;
+                                v[1] = C[PLANE];
+                                v[2] = C[2 * PLANE];
+                                v[5] = C[5 * PLANE];
                             }
                         } else {
 #pragma unroll
-                            for (int q = 0; q < 6; ++q) v[q] = pl(l, ca, q)[o];
+                            for (int q = 0; q < 6; ++q) v[q] = C[q * PLANE];
                         }
                         // heat bath: 25 (planes 0, 3, 4) -> 38 (planes 1, 2, 5) where the bit is 1, back where 0
                         const uint32_t e25 = v[0] & ~v[1] & ~v[2] & v[3] & v[4] & ~v[5];
                         const uint32_t e38 = ~v[0] & v[1] & v[2] & ~v[3] & ~v[4] & v[5];
                         const uint32_t tog = ((e25 & b1) | (e38 & ~b1)) & vm;
 #pragma unroll
-                        for (int q = 0; q < 6; ++q) pl(l, ca, q)[o] = v[q] ^ tog;
+                        for (int q = 0; q < 6; ++q) C[q * PLANE] = v[q] ^ tog;
                     }
                 }
+                }
+                srow += dsr;
+                it += dit;
+                if (it >= IPR) {
+                    it -= IPR;
+                    ++srow;
                 }
             }
             if (draws) ++dstep;
@@ -402,7 +422,7 @@ rt_status plan_plane_walk(int family, int device, int nlat, int rows, int width,
     int ctas = std::max(1, std::min(ctas_hint > 0 ? ctas_hint : sms, rows));
     const int rpc = (rows + ctas - 1) / ctas;
     const int min_rows = rows / ctas;
-    int depth = std::max(1, std::min(depth_hint > 0 ? depth_hint : 8, min_rows));
+    int depth = std::max(1, std::min(depth_hint > 0 ? std::min(depth_hint, 32) : 8, min_rows));
     if (ctas == 1) depth = 1;
     size_t smem = 0;
     for (;; --depth) {
