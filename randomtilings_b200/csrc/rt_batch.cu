@@ -513,6 +513,7 @@ struct FamilyState {
     int64_t nphases = 0, phases_sweeps = -1;
     Plan plan;
     bool planned = false;
+    double work = 0;  // relative cost of a sweep of the whole family (launch order)
 };
 
 int family_of(int32_t model, int32_t kernel) {
@@ -592,7 +593,8 @@ BatchArgs args_for(rt_batch* b, int f, const void* recs) {
     return a;
 }
 
-rt_status launch_family(rt_batch* b, int f, const Plan& p, const void* recs, cudaStream_t s) {
+// priority: a CUDA stream priority (lower = scheduled first); 0 = default.
+rt_status launch_family(rt_batch* b, int f, const Plan& p, const void* recs, cudaStream_t s, int priority = 0) {
     BatchFn fn = batch_fn(f);
     BatchArgs a = args_for(b, f, recs);
     cudaLaunchConfig_t cfg = {};
@@ -600,13 +602,15 @@ rt_status launch_family(rt_batch* b, int f, const Plan& p, const void* recs, cud
     cfg.blockDim = dim3((unsigned)p.block);
     cfg.dynamicSmemBytes = p.smem;
     cfg.stream = s;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = (unsigned)p.cl;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributePriority;
+    attr[1].val.priority = priority;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     cudaError_t e = cudaLaunchKernelEx(&cfg, fn, a);
     if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     return RT_OK;
@@ -647,6 +651,9 @@ bool fill_plan(rt_batch* b, int f, int cl, int block, Plan* p) {
     p->cl = cl;
     p->block = block;
     p->smem = smem;
+    // Every resident cluster slot is used (fewer clusters with full rounds
+    // measured slower: the families are bound by instruction issue and lose
+    // more from fewer resident warps than they gain from the shorter tail).
     p->clusters = std::min<int>((int)F.members.size(), active);
     return true;
 }
@@ -759,6 +766,7 @@ rt_status upload(rt_batch* b) {
 // few sweeps on a scratch copy of the family's lattices; the fastest wins.
 rt_status plan_family(rt_batch* b, int f) {
     FamilyState& F = b->fam[f];
+    F.work = 0;
     const int blocks[] = {256, 512, 1024};
     const int cls[] = {1, 2, 4, 8};
     std::vector<Plan> cand;
@@ -816,6 +824,7 @@ rt_status plan_family(rt_batch* b, int f) {
         cudaEventElapsedTime(&ms, b->t0, b->t1);
         if (ms < best) {
             best = ms;
+            F.work = ms;
             F.plan = p;
         }
     }
@@ -964,16 +973,39 @@ rt_status rt_batch_run(rt_batch* b, int64_t sweeps) {
             if (!b->fam[f].members.empty())
                 cudaFuncSetAttribute((const void*)batch_fn(f), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)b->fam[f].plan.smem);
-        // One graph: fork to a stream per family, one launch each, join.
+        // One graph: fork to a stream per family, one launch each, join.  The
+        // family with the most work goes first at the highest priority, so its
+        // CTAs take the SMs and the smaller families fill the slots its last
+        // round leaves idle.
+        // Work of a family: the autotuner's time of its best plan when every
+        // family has one, else its lattice bytes per sweep.
+        int order[kFamilies], nf = 0;
+        double est[kFamilies] = {};
+        bool timed = true;
+        for (int f = 0; f < kFamilies; ++f) {
+            if (b->fam[f].members.empty()) continue;
+            timed = timed && b->fam[f].work > 0;
+            for (int i : b->fam[f].members) {
+                const Chain& c = b->chains[i];
+                est[f] += (double)steps_per_sweep(c.kind) * c.ncol * c.arows * c.width * c.elem;
+            }
+            order[nf++] = f;
+        }
+        if (timed)
+            for (int k = 0; k < nf; ++k) est[order[k]] = b->fam[order[k]].work;
+        std::sort(order, order + nf, [&](int x, int y) { return est[x] > est[y]; });
+        int prio_low = 0, prio_high = 0;
+        cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
         cudaEventRecord(b->fork, b->stream);
         rt_status ls = RT_OK;
-        for (int f = 0; f < kFamilies && ls == RT_OK; ++f) {
-            if (b->fam[f].members.empty()) continue;
+        for (int k = 0; k < nf && ls == RT_OK; ++k) {
+            const int f = order[k];
             cudaStreamWaitEvent(b->fam_stream[f], b->fork, 0);
-            ls = launch_family(b, f, b->fam[f].plan, b->fam[f].recs.p, b->fam_stream[f]);
+            ls = launch_family(b, f, b->fam[f].plan, b->fam[f].recs.p, b->fam_stream[f],
+                               k == 0 ? prio_high : prio_low);
             cudaEventRecord(b->join[f], b->fam_stream[f]);
             cudaStreamWaitEvent(b->stream, b->join[f], 0);
         }
@@ -983,7 +1015,7 @@ rt_status rt_batch_run(rt_batch* b, int64_t sweeps) {
             return ls;
         }
         if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&b->exec, g, 0);
+        e = cudaGraphInstantiate(&b->exec, g, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) {
             b->exec = nullptr;

@@ -108,8 +108,9 @@ struct TriDimerRule {
 
     // ---- helpers ------------------------------------------------------------
     __device__ static int dg(int32_t x, int k) { return (int)(((uint32_t)x >> (2 * k)) & 3u); }
-    __device__ static int cyc_up(int v) { return v == 0 ? 0 : v % 3 + 1; }          // 1->2, 2->3, 3->1
-    __device__ static int cyc_dn(int v) { return v == 0 ? 0 : (v + 1) % 3 + 1; }    // 1->3, 2->1, 3->2
+    // 0->0, 1->2, 2->3, 3->1 and 0->0, 1->3, 2->1, 3->2 as 2-bit tables
+    __device__ static int cyc_up(int v) { return (int)((0x78u >> (2 * v)) & 3u); }
+    __device__ static int cyc_dn(int v) { return (int)((0x9Cu >> (2 * v)) & 3u); }
     __device__ static int32_t pack(int t1, int t4, int t16, int t64, int c) {
         return t1 + 4 * t4 + 16 * t16 + 64 * t64 + 256 * c;
     }
@@ -209,10 +210,18 @@ struct TriDimerRule {
             case TD_TRI_OTHER: {  // :255-275, then :118-189 for the butterflies in b
                 if (!interior) break;
                 const int src = t == 0 ? 3 : 4, dst = t == 0 ? 4 : 3, p = t == 0 ? -1 : 1;
-                put(dst, i, j, tri_digit(at(src, i, j - 1 + t)) + 4 * tri_digit(at(src, i, j + t)) +
-                                16 * tri_digit(at(src, i + p, j)));
+                // every value is computed before any is stored (the stores go to
+                // arrays the computations do not read)
+                const int32_t tv = tri_digit(at(src, i, j - 1 + t)) + 4 * tri_digit(at(src, i, j + t)) +
+                                   16 * tri_digit(at(src, i + p, j));
+                int32_t bv[3] = {0, 0, 0};
+#pragma unroll
                 for (int w = 0; w < 3; ++w)
-                    if (x.b & (1u << w)) put(5 + w, i, j, bfly_from_loz(x, w, i, j));
+                    if (x.b & (1u << w)) bv[w] = bfly_from_loz(x, w, i, j);
+                put(dst, i, j, tv);
+#pragma unroll
+                for (int w = 0; w < 3; ++w)
+                    if (x.b & (1u << w)) put(5 + w, i, j, bv[w]);
                 break;
             }
             case TD_ROT_TRI: {  // :191-211
@@ -245,12 +254,19 @@ struct TriDimerRule {
                 put(2, i, j, ((ur & 3) == 1) + 2 * ((dd & 12) == 12) + 4 * ((dd & 12) == 4) + 8 * ((ur & 3) == 2));
                 break;
             }
-            case TD_BFLY_FROM_LOZ:
+            case TD_BFLY_FROM_LOZ: {
                 if (!interior) break;
+                int32_t bv[3] = {0, 0, 0};
+#pragma unroll
                 for (int w = 0; w < 3; ++w)
-                    if (x.b & (1u << w)) put(5 + w, i, j, bfly_from_loz(x, w, i, j));
-                if (x.a) put(3, i, j, up_from_loz(x, i, j));
+                    if (x.b & (1u << w)) bv[w] = bfly_from_loz(x, w, i, j);
+                const int32_t uv = x.a ? up_from_loz(x, i, j) : 0;
+#pragma unroll
+                for (int w = 0; w < 3; ++w)
+                    if (x.b & (1u << w)) put(5 + w, i, j, bv[w]);
+                if (x.a) put(3, i, j, uv);
                 break;
+            }
             case TD_ROT_BFLY: {  // :331-353
                 const int p1 = (int)(x.b & 3), p2 = (int)(x.b >> 2);
                 const int b1 = 1 - (t & 1), b2 = (1 + t) / 2, b3 = t & 1;
