@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(1024, 1) batch_site_kernel(const __grid_consta
 // One phase of op OP over the band rows [r0, r0 + nrows) of a triangle-dimer
 // chain: only the rows TriDimerRule::live_rows admits, four sites (one Philox
 // call in drawing phases) per work item.
-template <uint32_t OP>
+template <uint32_t OP, int T, int B = -1>
 __device__ __forceinline__ void td_phase(const TriDimerRule::MixedCtx& x, int r0, int nrows, int width, int tid,
                                          int BLOCK, int64_t dstep, uint32_t chain, uint32_t key0, uint32_t key1) {
     constexpr bool DRAWS = OP == TD_ROT_LOZ || OP == TD_ROT_TRI || OP == TD_ROT_BFLY;
@@ -327,7 +327,7 @@ __device__ __forceinline__ void td_phase(const TriDimerRule::MixedCtx& x, int r0
 #pragma unroll
         for (int bb = 0; bb < 4; ++bb) {
             const int j = 4 * cq + bb;
-            if (j < width) TriDimerRule::site_op<OP>(x, r, j, quad_word(w4, bb) >> 9);
+            if (j < width) TriDimerRule::site_op<OP, T, B>(x, r, j, quad_word(w4, bb) >> 9);
         }
         rr += drr;
         cq += dq;
@@ -393,17 +393,44 @@ __global__ void __launch_bounds__(1024, 1) batch_td_kernel(const __grid_constant
             x.a = ph_a(d);
             x.b = ph_b(d);
             switch (x.op) {
-#define RT_TD_PHASE(OPC) \
-    case OPC: td_phase<OPC>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1); break;
+#define RT_TD_PHASE(OPC)                                                                        \
+    case OPC:                                                                                   \
+        if (x.a == 0)                                                                           \
+            td_phase<OPC, 0>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);     \
+        else if (x.a == 1)                                                                      \
+            td_phase<OPC, 1>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);     \
+        else                                                                                    \
+            td_phase<OPC, 2>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);     \
+        break;
                 RT_TD_PHASE(TD_ROT_LOZ)
                 RT_TD_PHASE(TD_LOZ_FLIPPED)
                 RT_TD_PHASE(TD_LOZ_OTHER)
                 RT_TD_PHASE(TD_UP_FROM_LOZ)
-                RT_TD_PHASE(TD_TRI_OTHER)
+                case TD_TRI_OTHER:  // (a, b) in {(0, 7), (0, 0), (1, 0)} in the phase program
+                    if (x.a == 0 && x.b == 7)
+                        td_phase<TD_TRI_OTHER, 0, 7>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                    else if (x.a == 0 && x.b == 0)
+                        td_phase<TD_TRI_OTHER, 0, 0>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                    else if (x.a == 1 && x.b == 0)
+                        td_phase<TD_TRI_OTHER, 1, 0>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                    else
+                        td_phase<TD_TRI_OTHER, -1>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                    break;
                 RT_TD_PHASE(TD_ROT_TRI)
                 RT_TD_PHASE(TD_TRI_FLIPPED)
                 RT_TD_PHASE(TD_LOZ_FROM_TRI)
-                RT_TD_PHASE(TD_BFLY_FROM_LOZ)
+                case TD_BFLY_FROM_LOZ:  // (a, b) in {(0, 7), (1, 3), (1, 5), (1, 6)}
+                    if (x.a == 0 && x.b == 7)
+                        td_phase<TD_BFLY_FROM_LOZ, 0, 7>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                    else if (x.a == 1 && x.b == 3)
+                        td_phase<TD_BFLY_FROM_LOZ, 1, 3>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                    else if (x.a == 1 && x.b == 5)
+                        td_phase<TD_BFLY_FROM_LOZ, 1, 5>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                    else if (x.a == 1 && x.b == 6)
+                        td_phase<TD_BFLY_FROM_LOZ, 1, 6>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                    else
+                        td_phase<TD_BFLY_FROM_LOZ, -1>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                    break;
                 RT_TD_PHASE(TD_ROT_BFLY)
                 RT_TD_PHASE(TD_BFLY_SAME)
                 RT_TD_PHASE(TD_BFLY_21)

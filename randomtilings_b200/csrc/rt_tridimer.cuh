@@ -166,13 +166,16 @@ struct TriDimerRule {
     __device__ static void site(const WalkArgs&, const Ctx& x, int, int i, int j, uint32_t k) { site_on(x, i, j, k); }
 
     // One site of the phase whose op is OP (a compile-time constant: every
-    // other case of the switch below folds away).
-    template <uint32_t OP, class A>
+    // other case of the switch below folds away).  T >= 0 fixes the phase's
+    // argument a (the orientation t) at compile time too, B >= 0 its
+    // argument b; negative values read x.a / x.b.
+    template <uint32_t OP, int T = -1, int B = -1, class A>
     __device__ static void site_op(const A& x, int i, int j, uint32_t k) {
         auto at = [&](int arr, int ii, int jj) { return x.get(arr, ii, jj); };
         auto put = [&](int arr, int ii, int jj, int32_t v) { x.set(arr, ii, jj, v); };
         const bool interior = i >= 1 && i <= x.m - 2 && j >= 1 && j <= x.m - 2;
-        const int t = (int)x.a;
+        const int t = T >= 0 ? T : (int)x.a;
+        const uint32_t bm = B >= 0 ? (uint32_t)B : x.b;  // butterfly masks of TRI_OTHER / BFLY_FROM_LOZ
         switch (OP) {
             case TD_ROT_LOZ: {  // :4-22
                 const int cls = ((1 - (t & 1)) * i + ((1 + t) / 2) * j) % 2;
@@ -217,22 +220,22 @@ struct TriDimerRule {
                 int32_t bv[3] = {0, 0, 0};
 #pragma unroll
                 for (int w = 0; w < 3; ++w)
-                    if (x.b & (1u << w)) bv[w] = bfly_from_loz(x, w, i, j);
+                    if (bm & (1u << w)) bv[w] = bfly_from_loz(x, w, i, j);
                 put(dst, i, j, tv);
 #pragma unroll
                 for (int w = 0; w < 3; ++w)
-                    if (x.b & (1u << w)) put(5 + w, i, j, bv[w]);
+                    if (bm & (1u << w)) put(5 + w, i, j, bv[w]);
                 break;
             }
             case TD_ROT_TRI: {  // :191-211
-                if (k < (1u << 22) && ((j - i) % 3 + 3) % 3 == (int)x.b) {
+                if (k < (1u << 22) && (j + 2 * i) % 3 == (int)x.b) {
                     const int32_t v = at(t == 1 ? 4 : 3, i, j);
                     put(t == 1 ? 4 : 3, i, j, v == 45 ? 54 : v == 54 ? 45 : v);
                 }
                 break;
             }
             case TD_TRI_FLIPPED: {  // :213-253
-                const int cls = ((j - i) % 3 + 3) % 3;
+                const int cls = (j + 2 * i) % 3;
                 if (!interior || cls == (int)x.b) break;
                 const int p = cls == ((int)x.b + 1) % 3;
                 const int arr = t == 1 ? 4 : 3;
@@ -259,12 +262,12 @@ struct TriDimerRule {
                 int32_t bv[3] = {0, 0, 0};
 #pragma unroll
                 for (int w = 0; w < 3; ++w)
-                    if (x.b & (1u << w)) bv[w] = bfly_from_loz(x, w, i, j);
-                const int32_t uv = x.a ? up_from_loz(x, i, j) : 0;
+                    if (bm & (1u << w)) bv[w] = bfly_from_loz(x, w, i, j);
+                const int32_t uv = t ? up_from_loz(x, i, j) : 0;  // a = 1: also U from the lozenges
 #pragma unroll
                 for (int w = 0; w < 3; ++w)
-                    if (x.b & (1u << w)) put(5 + w, i, j, bv[w]);
-                if (x.a) put(3, i, j, uv);
+                    if (bm & (1u << w)) put(5 + w, i, j, bv[w]);
+                if (t) put(3, i, j, uv);
                 break;
             }
             case TD_ROT_BFLY: {  // :331-353
