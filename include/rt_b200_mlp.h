@@ -5,8 +5,9 @@
  * height function (rt_b200_project.h) and turned into the start tiling of a
  * plain chain.  Architecture: IN = 8 input features -> 128 -> 128 -> 128 -> 1,
  * GELU (tanh form) after each hidden layer.  The two 128 x 128 layers run on
- * the tensor cores in BF16 with FP32 accumulation (forward, and both GEMMs of
- * the backward pass); the 8 -> 128 and 128 -> 1 layers and Adam run in FP32.
+ * the tensor cores (tcgen05.mma, accumulators in tensor memory) in BF16 with
+ * FP32 accumulation (forward, and both GEMMs of the backward pass); the
+ * 8 -> 128 and 128 -> 1 layers and Adam run in FP32.
  * Master parameters are FP32; BF16 copies of the 128 x 128 weights are made
  * after every update.  Loss: mean squared error.
  *

@@ -1,13 +1,14 @@
 // rt_mlp.cu -- training and inference kernels of the coordinate MLP
 // (include/rt_b200_mlp.h).
 //
-// Layers 1 and 2 (128 x 128) are tensor-core GEMMs: a CTA of four warps
-// computes a 64 x 64 tile of C = A * B with mma.sync m16n8k16 (BF16 inputs,
-// FP32 accumulators), A and B staged through shared memory 32 columns of K
-// at a time; each GEMM names its operands' layouts, so one kernel serves
-// the forward product X * W^T, the input gradient dZ * W and the weight
-// gradient dZ^T * X (the last split over K, reduced with FP32 atomics).
-// Epilogues fuse bias + GELU (forward) and the GELU derivative (backward).
+// Layers 1 and 2 (128 x 128) run on the fifth-generation tensor cores: a CTA
+// of four warps computes a 128 x 128 tile of C = A * B with tcgen05.mma
+// (BF16 inputs, FP32 accumulator in tensor memory), A and B staged through
+// shared memory 64 columns of K at a time; each GEMM names its operands'
+// layouts, so one kernel serves the forward product X * W^T, the input
+// gradient dZ * W and the weight gradient dZ^T * X (the last split over K,
+// reduced with FP32 atomics).  Epilogues, read from tensor memory with
+// tcgen05.ld, fuse bias + GELU (forward) and the GELU derivative (backward).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -52,18 +53,6 @@ __device__ __forceinline__ __nv_bfloat16 op_at(const Op& o, int r, int c) {
     return o.trans ? o.p[(size_t)c * o.ld + r] : o.p[(size_t)r * o.ld + c];
 }
 
-__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
-}
-
-__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
 enum Epi : int {
     EPI_FWD = 0,     // z = acc + bias[n]; out_f = z; out_h = bf16(gelu(z))
     EPI_DGELU = 1,   // d = acc * gelu'(zin[m][n]); out_f = d; out_h = bf16(d)
@@ -71,7 +60,7 @@ enum Epi : int {
 };
 
 struct GemmArgs {
-    Op A, B;        // C[M][N] = A[M][K] * B[K][N]
+    Op A, B;        // C[M][N] = A[M][K] * B[K][N], N = 128
     int M, N, K;
     int ksplit;     // K range per blockIdx.z
     int epi;
@@ -79,87 +68,214 @@ struct GemmArgs {
     const float* zin;   // EPI_DGELU: pre-activation [M][N]
     float* out_f;       // [M][N]
     __nv_bfloat16* out_h;  // [M][N] (EPI_FWD, EPI_DGELU)
+    int* err;           // set to 1 when a bounded wait gives up
 };
 
-constexpr int TM = 64, TN = 64, TK = 32, PAD = 8;
+// ---------------------------------------------------------------------------
+// tcgen05 GEMM.  A CTA of four warps computes a 128 x 128 tile of C in a
+// tensor-memory accumulator (128 lanes = rows, 128 FP32 columns).  K is
+// walked in chunks of 64: all threads stage the A chunk (128 x 64) and the B
+// chunk (as 128 n-rows x 64 k) into shared memory in the canonical K-major
+// layout without swizzle -- core matrices of 8 rows x 16 bytes, the 8 core
+// matrices of a row group side by side (leading byte offset 128 B, stride
+// byte offset 1 KB) -- then one thread issues the four K = 16 MMAs
+// (tcgen05.mma kind::f16, BF16 A and B, FP32 accumulate) and commits them to
+// an mbarrier that every thread waits on before the next chunk overwrites
+// the operands.  The epilogue reads the accumulator with tcgen05.ld (warp w
+// owns lanes 32w..32w+31, i.e. rows) 32 columns at a time.
+// ---------------------------------------------------------------------------
+constexpr int TBM = 128, TBN = 128, TBK = 64;
+constexpr uint32_t kTmemCols = 128;
+// Instruction descriptor (PTX ISA, kind::f16): D = F32 (bits 4-5 = 1), A = B =
+// BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at
+// bits 24-28.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TBN >> 3) << 17) | ((uint32_t)(TBM >> 4) << 24);
+constexpr unsigned long long kWaitLimit = 1ull << 28;  // mbarrier polls before giving up
 
-__global__ void __launch_bounds__(128) gemm_bf16(const __grid_constant__ GemmArgs g) {
-    __shared__ __align__(16) __nv_bfloat16 sA[TM][TK + PAD];  // [m][k]
-    __shared__ __align__(16) __nv_bfloat16 sB[TN][TK + PAD];  // [n][k]
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
-    const int k_begin = blockIdx.z * g.ksplit, k_end = min(g.K, k_begin + g.ksplit);
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;  // warp tile 32 x 32
-    const int grp = lane >> 2, tig = lane & 3;
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int x = 0; x < 4; ++x) acc[i][j][x] = 0.0f;
+// Shared-memory matrix descriptor (K-major, no swizzle): start address,
+// leading byte offset 128 B (next core matrix along K), stride byte offset
+// 1 KB (next group of 8 rows), version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46);
+}
+// Byte offset of element (row r, k) of a 128 x 64 operand chunk in that layout.
+__device__ __forceinline__ uint32_t chunk_off(int r, int k) {
+    return (uint32_t)(((r >> 3) * (TBK / 8) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
 
-    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
-    for (int k0 = k_begin; k0 < k_end; k0 += TK) {
-        for (int e = tid; e < TM * TK; e += 128) {
-            const int r = e / TK, c = e % TK;
-            const int gm = m0 + r, gk = k0 + c;
-            sA[r][c] = (gm < g.M && gk < k_end) ? op_at(g.A, gm, gk) : zero;
-        }
-        for (int e = tid; e < TN * TK; e += 128) {
-            const int r = e / TK, c = e % TK;  // r = n, c = k
-            const int gn = n0 + r, gk = k0 + c;
-            sB[r][c] = (gn < g.N && gk < k_end) ? op_at(g.B, gk, gn) : zero;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < TK; kk += 16) {
-            uint32_t a[2][4], b[4][2];
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-                const int r = wm + 16 * i + grp;
-                a[i][0] = pack2(sA[r][kk + 2 * tig], sA[r][kk + 2 * tig + 1]);
-                a[i][1] = pack2(sA[r + 8][kk + 2 * tig], sA[r + 8][kk + 2 * tig + 1]);
-                a[i][2] = pack2(sA[r][kk + 2 * tig + 8], sA[r][kk + 2 * tig + 9]);
-                a[i][3] = pack2(sA[r + 8][kk + 2 * tig + 8], sA[r + 8][kk + 2 * tig + 9]);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int nn = wn + 8 * j + grp;
-                b[j][0] = pack2(sB[nn][kk + 2 * tig], sB[nn][kk + 2 * tig + 1]);
-                b[j][1] = pack2(sB[nn][kk + 2 * tig + 8], sB[nn][kk + 2 * tig + 9]);
-            }
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) mma16816(acc[i][j], a[i], b[j]);
-        }
-        __syncthreads();
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    for (unsigned long long it = 0; it < kWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
     }
-    // Accumulator (i, j, x): row wm + 16 i + grp + 8 (x >> 1), column wn + 8 j + 2 tig + (x & 1).
+    return false;
+}
+
+// Stages rows [r0, r0 + 128) x k [k0, k_end) of a logical operand whose
+// element (r, k) is o[r][k] (kcontig: 8 consecutive k are one 16-byte load)
+// or o[k][r] (8 consecutive r are one 16-byte load, scattered over 8 core
+// matrix rows); rows >= rlim and k >= k_end read as zero.
+__device__ __forceinline__ void stage_chunk(unsigned char* dst, const __nv_bfloat16* p, int ld, bool kcontig, int r0,
+                                            int rlim, int k0, int k_end) {
+    const int tid = threadIdx.x;
+    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+    if (kcontig) {
+        for (int e = tid; e < TBM * (TBK / 8); e += 128) {
+            const int r = e / (TBK / 8), k8 = (e % (TBK / 8)) * 8;
+            const int gr = r0 + r, gk = k0 + k8;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (gr < rlim && gk + 8 <= k_end) {
+                v = *reinterpret_cast<const uint4*>(p + (size_t)gr * ld + gk);
+            } else if (gr < rlim) {
+                __nv_bfloat16 t[8];
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+                for (int x = 0; x < 8; ++x) t[x] = gk + x < k_end ? p[(size_t)gr * ld + gk + x] : zero;
+                v = *reinterpret_cast<const uint4*>(t);
+            }
+            *reinterpret_cast<uint4*>(dst + chunk_off(r, k8)) = v;
+        }
+    } else {
+        for (int e = tid; e < TBK * (TBM / 8); e += 128) {
+            const int k = e / (TBM / 8), r8 = (e % (TBM / 8)) * 8;
+            const int gr = r0 + r8, gk = k0 + k;
+            __nv_bfloat16 t[8];
+            if (gk < k_end && gr + 8 <= rlim) {
+                *reinterpret_cast<uint4*>(t) = *reinterpret_cast<const uint4*>(p + (size_t)gk * ld + gr);
+            } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+                for (int x = 0; x < 8; ++x) t[x] = (gk < k_end && gr + x < rlim) ? p[(size_t)gk * ld + gr + x] : zero;
+            }
 #pragma unroll
-            for (int x = 0; x < 4; ++x) {
-                const int m = m0 + wm + 16 * i + grp + 8 * (x >> 1);
-                const int n = n0 + wn + 8 * j + 2 * tig + (x & 1);
-                if (m >= g.M || n >= g.N) continue;
-                const float v = acc[i][j][x];
-                const size_t at = (size_t)m * g.N + n;
-                if (g.epi == EPI_FWD) {
-                    const float z = v + g.bias[n];
-                    g.out_f[at] = z;
-                    g.out_h[at] = __float2bfloat16(gelu(z));
-                } else if (g.epi == EPI_DGELU) {
-                    const float d = v * gelu_grad(g.zin[at]);
-                    g.out_f[at] = d;
-                    g.out_h[at] = __float2bfloat16(d);
-                } else {
-                    atomicAdd(g.out_f + at, v);
+            for (int x = 0; x < 8; ++x) *reinterpret_cast<__nv_bfloat16*>(dst + chunk_off(r8 + x, k)) = t[x];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128, 1) gemm_tc(const __grid_constant__ GemmArgs g) {
+    __shared__ __align__(128) unsigned char sA[TBM * TBK * 2];
+    __shared__ __align__(128) unsigned char sB[TBN * TBK * 2];
+    __shared__ __align__(8) unsigned long long mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TBM;
+    const int k_begin = blockIdx.z * g.ksplit, k_end = min(g.K, k_begin + g.ksplit);
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(sA), sb = (uint32_t)__cvta_generic_to_shared(sB);
+    const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+
+    if (warp == 0) {
+        const uint32_t slot = (uint32_t)__cvta_generic_to_shared(&tmem_slot);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_fail = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+
+    uint32_t parity = 0;
+    bool first = true;
+    for (int k0 = k_begin; k0 < k_end; k0 += TBK) {
+        // Stage A as (m, k) and B as (n, k) = B[k][n]; zero outside the matrices.
+        // A(m, k) is contiguous along k unless A is transposed; B(k, n) as (n, k)
+        // is contiguous along k when B is transposed.
+        stage_chunk(sA, g.A.p, g.A.ld, g.A.trans == 0, m0, g.M, k0, k_end);
+        stage_chunk(sB, g.B.p, g.B.ld, g.B.trans != 0, 0, g.N, k0, k_end);
+        // generic-proxy stores -> visible to the tensor core's async proxy
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int kk = 0; kk < TBK / 16; ++kk) {
+                // K = 16 per MMA: two core matrices along K = 256 bytes
+                const uint64_t da = smem_desc(sa + 256u * kk), db = smem_desc(sb + 256u * kk);
+                const uint32_t acc = (first && kk == 0) ? 0u : 1u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(kIdesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mb)
+                         : "memory");
+        }
+        first = false;
+        if (!mbar_wait(mb, parity)) {
+            s_fail = 1;  // racy but every writer writes 1
+            atomicOr(g.err, 1);
+        }
+        parity ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (s_fail) break;
+    }
+
+    if (!s_fail && !first) {
+        // Epilogue: this warp's 32 rows, 32 columns per tcgen05.ld.
+        const int m = m0 + 32 * warp + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < TBN; c0 += 32) {
+            uint32_t v[32];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(taddr)
+                : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m < g.M) {
+#pragma unroll
+                for (int x = 0; x < 32; ++x) {
+                    const int n = c0 + x;
+                    if (n >= g.N) continue;
+                    const float acc = __uint_as_float(v[x]);
+                    const size_t at = (size_t)m * g.N + n;
+                    if (g.epi == EPI_FWD) {
+                        const float z = acc + g.bias[n];
+                        g.out_f[at] = z;
+                        g.out_h[at] = __float2bfloat16(gelu(z));
+                    } else if (g.epi == EPI_DGELU) {
+                        const float dd = acc * gelu_grad(g.zin[at]);
+                        g.out_f[at] = dd;
+                        g.out_h[at] = __float2bfloat16(dd);
+                    } else {
+                        atomicAdd(g.out_f + at, acc);
+                    }
                 }
             }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        if (s_fail) {
+            // the MMAs may still be running: wait for them (bounded) before freeing their accumulator
+            mbar_wait(mb, parity ^ 1u);
+        }
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
 }
 
 // Layer 0 (IN -> H), FP32: z0 = x W0^T + b0, h1 = bf16(gelu(z0)).
@@ -320,6 +436,7 @@ struct rt_mlp {
     __nv_bfloat16 *h1 = nullptr, *h2 = nullptr, *h3 = nullptr, *d1h = nullptr, *d2h = nullptr;
     float *X = nullptr, *T = nullptr;
     int64_t rows = 0;
+    int* err = nullptr;  // device: set when a GEMM's bounded wait gave up
 };
 
 namespace {
@@ -366,9 +483,12 @@ GemmArgs gemm(Op A, Op B, int M, int N, int K, int epi) {
     return g;
 }
 
-void launch_gemm(const GemmArgs& g, int splits, cudaStream_t s) {
-    dim3 grid((g.N + TN - 1) / TN, (g.M + TM - 1) / TM, splits);
-    gemm_bf16<<<grid, 128, 0, s>>>(g);
+// N is always the hidden width (128 = one tile); M rows in tiles of 128, K
+// split over blockIdx.z for the weight gradients.
+void launch_gemm(rt_mlp* m, GemmArgs g, int splits, cudaStream_t s) {
+    g.err = m->err;
+    dim3 grid(1, (g.M + TBM - 1) / TBM, splits);
+    gemm_tc<<<grid, 128, 0, s>>>(g);
 }
 
 // Forward pass of the n rows in m->x; with `with_target`, also the loss and
@@ -382,12 +502,12 @@ void forward(rt_mlp* m, int n, bool with_target) {
     g.bias = m->P + OB1;
     g.out_f = m->z1;
     g.out_h = m->h2;
-    launch_gemm(g, 1, s);
+    launch_gemm(m, g, 1, s);
     g = gemm(Op{m->h2, H, 0}, Op{m->w2, H, 1}, n, H, H, EPI_FWD);
     g.bias = m->P + OB2;
     g.out_f = m->z2;
     g.out_h = m->h3;
-    launch_gemm(g, 1, s);
+    launch_gemm(m, g, 1, s);
     if (with_target) cudaMemsetAsync(m->loss, 0, 4, s);
     layer3_fwd<<<(n + 7) / 8, 256, 0, s>>>(m->h3, m->P, n, m->y, with_target ? m->t : nullptr, m->dy, m->loss);
 }
@@ -399,35 +519,40 @@ void backward(rt_mlp* m, int n) {
     cudaMemsetAsync(m->G, 0, NPARAM * 4, s);
     layer3_wgrad<<<H + 1, 256, 0, s>>>(m->h3, m->dy, n, m->G);
     layer3_bwd<<<(nh + 255) / 256, 256, 0, s>>>(m->z2, m->dy, m->P, n, m->d2, m->d2h);
-    const int splits = (n + 1023) / 1024;
-    const int ks = ((n + splits - 1) / splits + TK - 1) / TK * TK;
+    const int splits = (n + 255) / 256;  // weight-gradient GEMMs: K = rows, 256 per CTA
+    const int ks = ((n + splits - 1) / splits + TBK - 1) / TBK * TBK;
     // dW2 = dz2^T h2: A(o, r) = dz2[r][o] -> (d2h, H, trans); B(r, k) = h2[r][k]
     GemmArgs g = gemm(Op{m->d2h, H, 1}, Op{m->h2, H, 0}, H, H, n, EPI_ATOMIC);
     g.ksplit = ks;
     g.out_f = m->G + OW2;
-    launch_gemm(g, splits, s);
+    launch_gemm(m, g, splits, s);
     bias_grad<<<H, 256, 0, s>>>(m->d2, n, m->G, OB2);
     // dz1 = (dz2 W2) * gelu'(z1): A = dz2 [n][H], B(o, k) = W2[o][k]
     g = gemm(Op{m->d2h, H, 0}, Op{m->w2, H, 0}, n, H, H, EPI_DGELU);
     g.zin = m->z1;
     g.out_f = m->d1;
     g.out_h = m->d1h;
-    launch_gemm(g, 1, s);
+    launch_gemm(m, g, 1, s);
     g = gemm(Op{m->d1h, H, 1}, Op{m->h1, H, 0}, H, H, n, EPI_ATOMIC);
     g.ksplit = ks;
     g.out_f = m->G + OW1;
-    launch_gemm(g, splits, s);
+    launch_gemm(m, g, splits, s);
     bias_grad<<<H, 256, 0, s>>>(m->d1, n, m->G, OB1);
     g = gemm(Op{m->d1h, H, 0}, Op{m->w1, H, 0}, n, H, H, EPI_DGELU);
     g.zin = m->z0;
     g.out_f = m->d0;
     g.out_h = m->h3;  // scratch: the BF16 copy of dz0 is not needed
-    launch_gemm(g, 1, s);
+    launch_gemm(m, g, 1, s);
     layer0_wgrad<<<H, 256, 0, s>>>(m->d0, m->x, n, m->G);
     bias_grad<<<H, 256, 0, s>>>(m->d0, n, m->G, OB0);
 }
 
-rt_status sync(rt_mlp* m) { return cudaStreamSynchronize(m->s) == cudaSuccess ? RT_OK : RT_E_CUDA; }
+rt_status sync(rt_mlp* m) {
+    if (cudaStreamSynchronize(m->s) != cudaSuccess) return RT_E_CUDA;
+    int e = 0;
+    if (cudaMemcpy(&e, m->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return RT_E_CUDA;
+    return e ? RT_E_TIMEOUT : RT_OK;
+}
 
 }  // namespace
 
@@ -443,7 +568,8 @@ rt_status rt_mlp_create(int32_t device, uint64_t seed, rt_mlp** out) {
               cudaMalloc(&m->P, NPARAM * 4) == cudaSuccess && cudaMalloc(&m->G, NPARAM * 4) == cudaSuccess &&
               cudaMalloc(&m->M1, NPARAM * 4) == cudaSuccess && cudaMalloc(&m->M2, NPARAM * 4) == cudaSuccess &&
               cudaMalloc(&m->w1, H * H * 2) == cudaSuccess && cudaMalloc(&m->w2, H * H * 2) == cudaSuccess &&
-              cudaMalloc(&m->loss, 4) == cudaSuccess;
+              cudaMalloc(&m->loss, 4) == cudaSuccess && cudaMalloc(&m->err, sizeof(int)) == cudaSuccess &&
+              cudaMemset(m->err, 0, sizeof(int)) == cudaSuccess;
     if (!ok) {
         rt_mlp_destroy(m);
         return RT_E_NOMEM;
@@ -470,7 +596,7 @@ rt_status rt_mlp_destroy(rt_mlp* m) {
     cudaSetDevice(m->device);
     if (m->s) cudaStreamSynchronize(m->s);
     free_ws(m);
-    void* ps[] = {m->P, m->G, m->M1, m->M2, m->w1, m->w2, m->loss, m->X, m->T};
+    void* ps[] = {m->P, m->G, m->M1, m->M2, m->w1, m->w2, m->loss, m->X, m->T, m->err};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (m->s) cudaStreamDestroy(m->s);
