@@ -451,6 +451,45 @@ def run_cftp(args) -> None:
             "runs": runs}), flush=True)
 
 
+def run_extremal(args) -> None:
+    """Set-up of a large domain: MinTiling, MaxTiling and the TilingToHeightfunc
+    of both, on the host (the reference's flood) and on the device
+    (rt_extremal_tilings), on an Aztec diamond of order args.extremal_order
+    and an a=b=c hexagon of side args.extremal_side; results compared."""
+    import numpy as np
+
+    import randomtilings_b200 as rt
+    from randomtilings_b200 import builders
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    builders.extremal_tilings(rt.RT_DOMINO, rt.DominoTiler.AztecDiamond(4))  # context and module load
+    out = []
+    for model, cls, d, name in (
+            (rt.RT_DOMINO, rt.DominoTiler, rt.DominoTiler.AztecDiamond(args.extremal_order),
+             f"Aztec diamond n={args.extremal_order}"),
+            (rt.RT_LOZENGE, rt.LozengeTiler, rt.LozengeTiler.Hexagon(*[args.extremal_side] * 3),
+             f"hexagon a=b=c={args.extremal_side}")):
+        a = time.perf_counter()
+        tmin, tmax = cls.MinTiling(d), cls.MaxTiling(d)
+        hmin, hmax = cls.TilingToHeightfunc(tmin, d), cls.TilingToHeightfunc(tmax, d)
+        host_s = time.perf_counter() - a
+        walls, st = [], None
+        for _ in range(args.steps):
+            a = time.perf_counter()
+            dev, st = builders.extremal_tilings(model, d)
+            walls.append(time.perf_counter() - a)
+        equal = all(np.array_equal(dev[k], np.asarray(v)) for k, v in
+                    (("tmin", tmin), ("tmax", tmax), ("hmin", hmin), ("hmax", hmax)))
+        out.append({"domain": name, "n": st["n"], "equal_to_host": equal, "host_s": round(host_s, 4),
+                    "device_call_s": round(statistics.median(walls), 4), "device_ms": round(st["device_ms"], 3),
+                    "passes": st["passes"], "tile_updates": st["tile_updates"], "boundary": st["boundary"],
+                    "speedup_call": round(host_s / statistics.median(walls), 1)})
+        print(json.dumps(out[-1]), file=sys.stderr, flush=True)
+    print(json.dumps({"metric": "extremal tilings + heights set-up time (host flood vs device relaxation)",
+                      "unit": "s", "higher_is_better": False, "runs": out}), flush=True)
+
+
 def measure_batch(args, rank: int, world: int, dist, peak: float) -> dict:
     """The batched pattern: args.batch_chains chains of the mixed workload
     (chain seed s: domain type s mod 4, sizes from std::mt19937(s)), minimal
@@ -592,8 +631,11 @@ def main() -> None:
                     help="with --legs batch: comma-separated rt_model values of the mixed workload to keep")
     ap.add_argument("--batch-plan", default="",
                     help="with --legs batch: 'cluster,block' instead of the autotuner (one launch per run)")
-    ap.add_argument("--workload", choices=["walk", "cftp"], default="walk",
-                    help="walk: the headline line (default); cftp: CFTP runs on an Aztec diamond")
+    ap.add_argument("--workload", choices=["walk", "cftp", "extremal"], default="walk",
+                    help="walk: the headline line (default); cftp: CFTP runs on an Aztec diamond; "
+                         "extremal: host vs device extremal tilings of large domains")
+    ap.add_argument("--extremal-order", type=int, default=2000)
+    ap.add_argument("--extremal-side", type=int, default=1000)
     ap.add_argument("--cftp-order", type=int, default=500)
     ap.add_argument("--cftp-seeds", type=int, default=32)
     ap.add_argument("--cftp-rng", choices=["tinymt", "philox", "planes"], default="planes")
@@ -605,6 +647,8 @@ def main() -> None:
         ap.error("--warmup must be >= 3")
     if args.workload == "cftp":
         run_cftp(args)
+    elif args.workload == "extremal":
+        run_extremal(args)
     elif args.legs != "all":
         run_legs(args)
     elif args.impl == "reference":

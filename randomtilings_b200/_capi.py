@@ -188,6 +188,17 @@ class RtProjectStats(ctypes.Structure):
 SIGNATURES["rt_project_heights"] = (ctypes.c_int, [_I32, _P, _I64, _P, _P, _P, _P, _I64, _I32,
                                                    ctypes.POINTER(RtProjectStats)])
 
+
+
+class RtExtremalStats(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("boundary", ctypes.c_int64), ("passes", ctypes.c_int64),
+                ("tile_updates", ctypes.c_int64), ("device_ms", ctypes.c_double)]
+
+
+# include/rt_b200_extremal.h
+SIGNATURES["rt_extremal_tilings"] = (ctypes.c_int, [_I32, _P, _I64, _I32, _P, _P, _P, _P, _I64,
+                                                    ctypes.POINTER(RtExtremalStats)])
+
 # include/rt_b200_height.h
 SIGNATURES.update({
     "rt_hplan_create": (ctypes.c_int, [_I32, _P, _I64, _I32, ctypes.POINTER(_P)]),

@@ -46,6 +46,29 @@ def aztec_rectangle(order: int, remove) -> np.ndarray:
     return out
 
 
+def vertex_side(model: int, dlen: int) -> int:
+    """Vertex side n of a domino (M x M faces) or lozenge (M x 2M triangles) domain."""
+    m = int(round((dlen if model == _capi.RT_DOMINO else dlen // 2) ** 0.5))
+    return m + 1
+
+
+def extremal_tilings(model: int, domain, device: int = 0) -> tuple[dict, dict]:
+    """MinTiling, MaxTiling and their height functions, computed on the GPU
+    (include/rt_b200_extremal.h).  Returns ({"tmin", "tmax", "hmin", "hmax"},
+    stats); the arrays equal the host functions' results."""
+    lib = _capi.load()
+    d = _arr(domain)
+    n = vertex_side(model, d.size)
+    out = {k: np.zeros(n * n, dtype=np.int32) for k in ("tmin", "tmax", "hmin", "hmax")}
+    st = _capi.RtExtremalStats()
+    _capi.check(lib.rt_extremal_tilings(model, d.ctypes.data, d.size, device, out["tmin"].ctypes.data,
+                                        out["tmax"].ctypes.data, out["hmin"].ctypes.data, out["hmax"].ctypes.data,
+                                        n * n, ctypes.byref(st)))
+    stats = {"n": st.n, "boundary": st.boundary, "passes": st.passes, "tile_updates": st.tile_updates,
+             "device_ms": st.device_ms}
+    return out, stats
+
+
 def write(name: str, filename: str, *arrays) -> None:
     """Calls an SVG / text writer of include/rt_b200_svg.h; None arrays pass NULL."""
     lib = _capi.load()

@@ -16,8 +16,9 @@
 #include <cstdint>
 #include <deque>
 #include <map>
-#include <string>
 #include <random>
+#include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/rt_b200.h"
@@ -102,21 +103,30 @@ void dom_edge_faces(int i, int j, int nb, int f[4]) {
 // Height change along an edge, checkerboard rule of DominoTiler.cpp:221-231.
 int dom_dh(int i, int j, int nb) { return (nb > 1 ? 1 : -1) * (((i + j) % 2 == 0) ? 1 : -1); }
 
+int dom_face_p(const int32_t* d, int m, int i, int j) {
+    return (i >= 0 && j >= 0 && i < m && j < m) ? d[(int64_t)i * m + j] : 0;
+}
+
+// Kind of vertex (i, j): 0 outside the domain, 1 interior (all four faces in
+// it), 2 boundary (DomainToVertices, DominoTiler.cpp:479-506).
+int dom_vertex_kind(const int32_t* d, int m, int i, int j) {
+    if (i == 0 || j == 0 || i == m || j == m) {
+        const int i0 = i - (i == m), i1 = i - 1 + (i == 0), j0 = j - (j == m), j1 = j - 1 + (j == 0);
+        return (dom_face_p(d, m, i0, j0) || dom_face_p(d, m, i1, j0) || dom_face_p(d, m, i0, j1) ||
+                dom_face_p(d, m, i1, j1))
+                   ? 2
+                   : 0;
+    }
+    const int s = (d[(int64_t)(i - 1) * m + j - 1] != 0) + (d[(int64_t)(i - 1) * m + j] != 0) +
+                  (d[(int64_t)i * m + j - 1] != 0) + (d[(int64_t)i * m + j] != 0);
+    return s == 4 ? 1 : s > 0 ? 2 : 0;
+}
+
 Vec dom_vertices(const Vec& d, int m) {
     const int n = m + 1;
     Vec v((size_t)n * n, 0);
     for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) {
-            if (i == 0 || j == 0 || i == m || j == m) {
-                const int i0 = i - (i == m), i1 = i - 1 + (i == 0), j0 = j - (j == m), j1 = j - 1 + (j == 0);
-                if (dom_face(d, m, i0, j0) || dom_face(d, m, i1, j0) || dom_face(d, m, i0, j1) || dom_face(d, m, i1, j1))
-                    v[i * n + j] = 2;
-            } else {
-                const int s = (d[(i - 1) * m + j - 1] != 0) + (d[(i - 1) * m + j] != 0) + (d[i * m + j - 1] != 0) +
-                              (d[i * m + j] != 0);
-                v[i * n + j] = s == 4 ? 1 : s > 0 ? 2 : 0;
-            }
-        }
+        for (int j = 0; j < n; ++j) v[(size_t)i * n + j] = dom_vertex_kind(d.data(), m, i, j);
     return v;
 }
 
@@ -205,24 +215,35 @@ const int kLozBit[6] = {8, 2, 1, 4, 16, 32};
 // (row offset, offset from 2j) of the two triangles beside edge nb.
 const int kLozFace[6][4] = {{0, 0, -1, 1}, {-1, 1, -1, 0}, {-1, 0, -1, -1}, {-1, -1, 0, -2}, {0, -2, 0, -1}, {0, -1, 0, 0}};
 
-int loz_face(const Vec& d, int m, int r, int c) { return (r >= 0 && c >= 0 && r < m && c < 2 * m) ? d[r * 2 * m + c] : 0; }
+int loz_face_p(const int32_t* d, int m, int r, int c) {
+    return (r >= 0 && c >= 0 && r < m && c < 2 * m) ? d[(int64_t)r * 2 * m + c] : 0;
+}
+int loz_face(const Vec& d, int m, int r, int c) { return loz_face_p(d.data(), m, r, c); }
 
-bool loz_edge_in(const Vec& d, int m, int i, int j, int nb, bool exclusive) {
-    const int a = loz_face(d, m, i + kLozFace[nb][0], 2 * j + kLozFace[nb][1]) != 0;
-    const int b = loz_face(d, m, i + kLozFace[nb][2], 2 * j + kLozFace[nb][3]) != 0;
+bool loz_edge_in_p(const int32_t* d, int m, int i, int j, int nb, bool exclusive) {
+    const int a = loz_face_p(d, m, i + kLozFace[nb][0], 2 * j + kLozFace[nb][1]) != 0;
+    const int b = loz_face_p(d, m, i + kLozFace[nb][2], 2 * j + kLozFace[nb][3]) != 0;
     return exclusive ? (a != b) : (a || b);
+}
+bool loz_edge_in(const Vec& d, int m, int i, int j, int nb, bool exclusive) {
+    return loz_edge_in_p(d.data(), m, i, j, nb, exclusive);
+}
+
+// Kind of vertex (i, j) from its six triangles (DomainToVertices,
+// LozengeTiler.cpp:405-430); the border rows and columns are outside.
+int loz_vertex_kind(const int32_t* d, int m, int i, int j) {
+    if (i < 1 || j < 1 || i >= m || j >= m) return 0;
+    const int64_t r = (int64_t)i * 2 * m, u = (int64_t)(i - 1) * 2 * m;
+    const int s = (d[r + 2 * j] != 0) + (d[r + 2 * j - 1] != 0) + (d[r + 2 * j - 2] != 0) + (d[u + 2 * j] != 0) +
+                  (d[u + 2 * j + 1] != 0) + (d[u + 2 * j - 1] != 0);
+    return s == 6 ? 1 : s > 0 ? 2 : 0;
 }
 
 Vec loz_vertices(const Vec& d, int m) {
     const int n = m + 1;
     Vec v((size_t)n * n, 0);
     for (int i = 1; i < m; ++i)
-        for (int j = 1; j < m; ++j) {
-            const int s = (d[i * 2 * m + 2 * j] != 0) + (d[i * 2 * m + 2 * j - 1] != 0) + (d[i * 2 * m + 2 * j - 2] != 0) +
-                          (d[(i - 1) * 2 * m + 2 * j] != 0) + (d[(i - 1) * 2 * m + 2 * j + 1] != 0) +
-                          (d[(i - 1) * 2 * m + 2 * j - 1] != 0);
-            v[i * n + j] = s == 6 ? 1 : s > 0 ? 2 : 0;
-        }
+        for (int j = 1; j < m; ++j) v[(size_t)i * n + j] = loz_vertex_kind(d.data(), m, i, j);
     return v;
 }
 
@@ -946,6 +967,67 @@ bool lipschitz_graph(int model, const int32_t* d, int64_t dlen, int* n_out, std:
         return true;
     }
     return false;
+}
+
+// Heights of the boundary vertices reachable from the first boundary vertex
+// (row-major, height 0) along boundary edges -- edges with the domain on one
+// side only, which no tile crosses, so the height steps by the edge's
+// orientation -- exactly as the first step of dom_extremal / loz_extremal
+// (Thurston's construction, DominoTiler.cpp:214-399, LozengeTiler.cpp:140-318),
+// but with vertex kinds computed on the fly: only the rows up to the first
+// boundary vertex and the boundary itself are visited, never the whole
+// N x N grid.  Returns false when the domain has no boundary vertex or the
+// heights disagree around the boundary (not tileable).
+bool boundary_walk(int model, const int32_t* d, int64_t dlen, int* n_out, std::vector<int64_t>* idx,
+                   std::vector<int32_t>* h) {
+    if (!d || (model != RT_DOMINO && model != RT_LOZENGE)) return false;
+    const bool dom = model == RT_DOMINO;
+    const int m = dom ? isqrt_exact(dlen) : isqrt_exact(dlen / 2);
+    if (m < (dom ? 1 : 2) || (!dom && (int64_t)2 * m * m != dlen)) return false;
+    const int n = m + 1;
+    auto kind = [&](int i, int j) { return dom ? dom_vertex_kind(d, m, i, j) : loz_vertex_kind(d, m, i, j); };
+    int64_t start = -1;
+    for (int i = 0; i < n && start < 0; ++i)
+        for (int j = 0; j < n; ++j)
+            if (kind(i, j) == 2) {
+                start = (int64_t)i * n + j;
+                break;
+            }
+    if (start < 0) return false;
+    std::unordered_map<int64_t, int32_t> hf;
+    hf[start] = 0;
+    idx->assign(1, start);
+    h->assign(1, 0);
+    for (size_t at = 0; at < idx->size(); ++at) {
+        const int64_t v = (*idx)[at];
+        const int i = (int)(v / n), j = (int)(v % n);
+        const int32_t hv = (*h)[at];
+        for (int nb = 0; nb < (dom ? 4 : 6); ++nb) {
+            const int i2 = i + (dom ? kDomDi[nb] : kLozDi[nb]), j2 = j + (dom ? kDomDj[nb] : kLozDj[nb]);
+            if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n || kind(i2, j2) != 2) continue;
+            int32_t step;
+            if (dom) {
+                int f[4];
+                dom_edge_faces(i, j, nb, f);
+                if ((dom_face_p(d, m, f[0], f[1]) != 0) == (dom_face_p(d, m, f[2], f[3]) != 0)) continue;
+                step = dom_dh(i, j, nb);
+            } else {
+                if (!loz_edge_in_p(d, m, i, j, nb, true)) continue;
+                step = kLozDh[nb];
+            }
+            const int64_t w = (int64_t)i2 * n + j2;
+            auto it = hf.find(w);
+            if (it == hf.end()) {
+                hf.emplace(w, hv + step);
+                idx->push_back(w);
+                h->push_back(hv + step);
+            } else if (it->second != hv + step) {
+                return false;
+            }
+        }
+    }
+    *n_out = n;
+    return true;
 }
 
 }  // namespace rtb

@@ -67,6 +67,12 @@ void family_thresholds(int family, double q, int qcmp, uint32_t thr[4]);
 bool lipschitz_graph(int model, const int32_t* d, int64_t dlen, int* n_out, std::vector<uint8_t>* kind,
                      std::vector<uint8_t>* edges);
 
+// Boundary heights of a domino / lozenge domain (rt_host.cpp): the vertex
+// indices reachable from the first boundary vertex along boundary edges and
+// their heights (0 at the start), in visiting order; vertex side in *n_out.
+bool boundary_walk(int model, const int32_t* d, int64_t dlen, int* n_out, std::vector<int64_t>* idx,
+                   std::vector<int32_t>* h);
+
 // Host split of a triangle-dimer tiling into its eight M x M arrays
 // (H, L, R, U, D, BH, BL, BR), rt_host.cpp.
 void td_split_host(const int32_t* t, int n, int32_t* arrays);
