@@ -46,6 +46,14 @@ rt_status rt_tridimer_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d
 rt_status rt_save_matrix(const int32_t* a, int64_t len, const char* filename);
 rt_status rt_load_matrix(const char* filename, int32_t* out, int64_t cap, int64_t* len);
 
+/* Binary matrices (no reference counterpart): any int32 array (tilings,
+ * heights, domains) in the smallest of 1, 2, 4, 8, 16 or 32 bits per value
+ * that holds its range, with a checksum -- a domino tiling takes 4 bits a
+ * value.  The load returns the count in *len (out NULL: size query only) and
+ * RT_E_INVAL for a file that is not this format, truncated or corrupted. */
+rt_status rt_save_matrix_binary(const int32_t* a, int64_t len, const char* filename);
+rt_status rt_load_matrix_binary(const char* filename, int32_t* out, int64_t cap, int64_t* len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -162,6 +162,8 @@ SIGNATURES.update({
     "rt_tridimer_dimer_svg": (ctypes.c_int, [_P, _I64, _P, _I64, _S]),
     "rt_save_matrix": (ctypes.c_int, [_P, _I64, _S]),
     "rt_load_matrix": (ctypes.c_int, [_S, _P, _I64, _PL]),
+    "rt_save_matrix_binary": (ctypes.c_int, [_P, _I64, _S]),
+    "rt_load_matrix_binary": (ctypes.c_int, [_S, _P, _I64, _PL]),
 })
 
 # include/rt_b200_batch.h

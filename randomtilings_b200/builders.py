@@ -94,3 +94,18 @@ def load_matrix(filename: str) -> np.ndarray:
     out = np.zeros(max(n.value, 1), dtype=np.int32)
     _capi.check(lib.rt_load_matrix(str(filename).encode(), out.ctypes.data, out.size, ctypes.byref(n)))
     return out[: n.value]
+
+
+def save_matrix_binary(a, filename: str) -> None:
+    """Any int32 array in the compact binary format (include/rt_b200_svg.h)."""
+    arr = _arr(a)
+    _capi.check(_capi.load().rt_save_matrix_binary(arr.ctypes.data, arr.size, str(filename).encode()))
+
+
+def load_matrix_binary(filename: str) -> np.ndarray:
+    lib = _capi.load()
+    n = ctypes.c_int64()
+    _capi.check(lib.rt_load_matrix_binary(str(filename).encode(), None, 0, ctypes.byref(n)))
+    out = np.zeros(max(n.value, 1), dtype=np.int32)
+    _capi.check(lib.rt_load_matrix_binary(str(filename).encode(), out.ctypes.data, out.size, ctypes.byref(n)))
+    return out[: n.value]

@@ -1,15 +1,23 @@
 // rt_svg.cpp -- SVG and text output of domains, tilings and dimer covers.
 //
 // The reference draws with std::ofstream and the stream's default number
-// formatting (6 significant digits); these writers produce the same bytes,
-// so pictures and matrices written by either side are interchangeable (the
-// tests compare SHA-256 digests with the reference's own output).  Each
-// writer cites the reference function whose format it keeps.
+// formatting (6 significant digits); these writers produce the same bytes, so
+// pictures and matrices written by either side are interchangeable (the tests
+// compare SHA-256 digests with the reference's own output).  Each writer cites
+// the reference function whose format it keeps.  Output goes through Sink
+// (that formatting, written to the file in large blocks), and large pictures
+// are formatted by several threads, blocks of rows appended in row order.
+#include <algorithm>
+#include <charconv>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <fstream>
-#include <sstream>
 #include <string>
+#include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/rt_b200.h"
@@ -28,10 +36,132 @@ int side_of(int64_t len) {
     return (int)r;
 }
 
+// Text output with the number formatting of a default std::ostream -- the
+// C++ standard defines `os << double` at the default precision as printf's
+// "%.6g" and `os << int` as "%d" -- into a buffer that goes to the file in
+// large writes.  Without a file it is a plain buffer (one block of rows).
+class Sink {
+  public:
+    Sink() = default;
+    explicit Sink(const char* filename) : f_(std::fopen(filename, "wb")), ok_(f_ != nullptr) {}
+    Sink(const Sink&) = delete;
+    Sink& operator=(const Sink&) = delete;
+    Sink(Sink&&) = default;
+    ~Sink() { close(); }
+
+    Sink& operator<<(const char* s) {
+        buf_.append(s);
+        return spill();
+    }
+    Sink& operator<<(const std::string& s) {
+        buf_.append(s);
+        return spill();
+    }
+    template <class T, typename std::enable_if<std::is_integral<T>::value, int>::type = 0>
+    Sink& operator<<(T v) {
+        char tmp[24];
+        const auto r = std::to_chars(tmp, tmp + sizeof tmp, v);
+        buf_.append(tmp, r.ptr);
+        return spill();
+    }
+    Sink& operator<<(double x) {
+        put_double(x);
+        return spill();
+    }
+    void append(const Sink& o) {
+        buf_.append(o.buf_);
+        spill();
+    }
+    void clear() { buf_.clear(); }
+    // Flushes and closes the file; false if it could not be opened or written.
+    bool close() {
+        if (f_) {
+            if (!buf_.empty() && std::fwrite(buf_.data(), 1, buf_.size(), f_) != buf_.size()) ok_ = false;
+            buf_.clear();
+            if (std::fclose(f_) != 0) ok_ = false;
+            f_ = nullptr;
+        }
+        return ok_;
+    }
+
+  private:
+    Sink& spill() {
+        if (f_ && buf_.size() >= (1u << 22)) {
+            if (std::fwrite(buf_.data(), 1, buf_.size(), f_) != buf_.size()) ok_ = false;
+            buf_.clear();
+        }
+        return *this;
+    }
+    // "%.6g".  Exact multiples of 1/2 below 1e5 in magnitude -- every
+    // coordinate of the lattice pictures -- have at most six significant
+    // digits, which %.6g prints in full: the integer part, then ".5" for an
+    // odd half.  Anything else (and -0) goes through snprintf.
+    void put_double(double x) {
+        const double a = std::fabs(x), t = 2 * a;
+        if (a < 1e5 && t == std::floor(t) && !(x == 0 && std::signbit(x))) {
+            const int64_t k = (int64_t)t;
+            if (x < 0) buf_.push_back('-');
+            char tmp[24];
+            const auto r = std::to_chars(tmp, tmp + sizeof tmp, k >> 1);
+            buf_.append(tmp, r.ptr);
+            if (k & 1) buf_.append(".5");
+            return;
+        }
+        char tmp[48];
+        const int len = std::snprintf(tmp, sizeof tmp, "%.6g", x);
+        buf_.append(tmp, (size_t)std::max(0, len));
+    }
+
+    std::FILE* f_ = nullptr;
+    bool ok_ = true;
+    std::string buf_;
+};
+
+// Threads formatting rows: RT_WRITER_THREADS if set, else the host's cores (at most 64).
+unsigned writer_threads() {
+    if (const char* e = std::getenv("RT_WRITER_THREADS")) {
+        const long v = std::strtol(e, nullptr, 10);
+        if (v >= 1) return (unsigned)std::min(v, 256L);
+    }
+    return std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+}
+
+// row(s, i) writes row i (lo <= i < hi) to s.  Small pictures are written in
+// order on this thread; large ones in windows of consecutive row blocks,
+// one block per thread, each into its own buffer, appended in row order --
+// the same bytes as the sequential loop, whatever the thread count.
+template <class F>
+void for_rows(Sink& o, int lo, int hi, int64_t cells_per_row, const F& row) {
+    const int64_t rows = (int64_t)hi - lo;
+    const unsigned T = writer_threads();
+    if (rows <= 0) return;
+    if (T <= 1 || rows * std::max<int64_t>(1, cells_per_row) < (1 << 16)) {
+        for (int i = lo; i < hi; ++i) row(o, i);
+        return;
+    }
+    const int64_t blk = std::max<int64_t>(1, (1 << 15) / std::max<int64_t>(1, cells_per_row));
+    std::vector<Sink> part(T);
+    for (int64_t w0 = lo; w0 < hi; w0 += blk * T) {
+        std::vector<std::thread> th;
+        for (unsigned k = 0; k < T; ++k) {
+            const int64_t a = w0 + (int64_t)k * blk, b = std::min<int64_t>(hi, a + blk);
+            if (a >= b) break;
+            part[k].clear();
+            th.emplace_back([&row, &part, k, a, b] {
+                for (int64_t i = a; i < b; ++i) row(part[k], (int)i);
+            });
+        }
+        for (size_t k = 0; k < th.size(); ++k) {
+            th[k].join();
+            o.append(part[k]);
+        }
+    }
+}
+
 const char* kSvgOpen = "<svg xmlns='http://www.w3.org/2000/svg' xmlns:xlink=\"http://www.w3.org/1999/xlink\" ";
 
 // <use xlink:href = "#id" x = "X" y = "Y"/>  (the spaced form) or without spaces.
-void use(std::ostream& o, const char* id, double x, double y, bool spaced) {
+void use(Sink& o, const char* id, double x, double y, bool spaced) {
     if (spaced)
         o << "<use xlink:href = \"#" << id << "\" x = \"" << x << "\" y = \"" << y << "\"/>\n";
     else
@@ -39,21 +169,18 @@ void use(std::ostream& o, const char* id, double x, double y, bool spaced) {
 }
 
 // Header of the triangular-lattice pictures (viewBox 1.5 M, aspect 433.013:500).
-void tri_header(std::ostream& o, double m) {
+void tri_header(Sink& o, double m) {
     o << kSvgOpen << "height=\"433.013\" width=\"500\" viewBox=\"0 0 " << 3 / 2.0 * m << " " << 3 / 2.0 * m
       << "\" preserveAspectRatio=\"none\">\n";
 }
 
-rt_status finish(std::ofstream& f) {
-    f.close();
-    return f ? RT_OK : RT_E_INVAL;
-}
+rt_status finish(Sink& f) { return f.close() ? RT_OK : RT_E_INVAL; }
 
 // ---- rectangle-triangle face pictures (RectTriangleTiler.cpp:567-697) ----------
 double vx(int i, int j) { return 20 * (i * 1 / 2.0 + j); }
 double vy(int i, int) { return 20 * (i * kSqrt3 / 2.0); }
 
-std::string face_picture(int type, int i, int j) {
+void face_picture(Sink& o, int type, int i, int j) {
     static const char* kFill[4] = {
         "", "\" style=\"fill:midnightblue;stroke:midnightblue;stroke-width:.4\" />\n",
         "\" style=\"fill:slategrey;stroke:slategrey;stroke-width:.4\" />\n",
@@ -94,7 +221,6 @@ std::string face_picture(int type, int i, int j) {
     const double px = (Rx + Qx) / 2, py = (Ry + Qy) / 2;
     const double qx = (Px + Rx) / 2, qy = (Py + Ry) / 2;
     const double rx = (Px + Qx) / 2, ry = (Py + Qy) / 2;
-    std::stringstream o;
     auto poly = [&](double ax, double ay, double bx, double by, double cx, double cy, int colour) {
         o << "<polygon points=\"" << ax << "," << ay << " " << bx << "," << by << " " << cx << "," << cy << " "
           << kFill[colour];
@@ -115,7 +241,6 @@ std::string face_picture(int type, int i, int j) {
     if (p) line(Px, Py, px, py);
     if (q) line(Qx, Qy, qx, qy);
     if (r) line(Rx, Ry, rx, ry);
-    return o.str();
 }
 
 }  // namespace
@@ -126,15 +251,16 @@ extern "C" {
 rt_status rt_domino_domain_svg(const int32_t* d, int64_t dlen, const char* filename) {
     if (!d || !filename) return RT_E_INVAL;
     const int m = side_of(dlen);
-    std::ofstream o(filename);
+    Sink o(filename);
     o << kSvgOpen << "height=\"500\" width=\"500\" viewBox=\"0 0 " << m << " " << m << "\">\n";
     o << "<defs>\n";
     o << "<g id=\"b\">  <polygon points = \"-.5,-.5 .5,-.5 .5,.5 -.5,.5\" fill=\"blue\"/> </g>\n";
     o << "<g id=\"w\">  <polygon points = \"-.5,-.5 .5,-.5 .5,.5 -.5,.5\" fill=\"grey\"/> </g>\n";
     o << "</defs>\n";
-    for (int i = 0; i < m; ++i)
+    for_rows(o, 0, m, m, [&](Sink& o, int i) {
         for (int j = 0; j < m; ++j)
             if (d[(size_t)i * m + j] == 1) use(o, (i + j) % 2 == 0 ? "b" : "w", j + .5, i + .5, true);
+    });
     o << "</svg>";
     return finish(o);
 }
@@ -145,7 +271,7 @@ rt_status rt_domino_domain_svg(const int32_t* d, int64_t dlen, const char* filen
 static rt_status domino_pairs_svg(const int32_t* t, int64_t tlen, const char* filename, bool maya) {
     if (!t || !filename) return RT_E_INVAL;
     const int n = side_of(tlen);
-    std::ofstream o(filename);
+    Sink o(filename);
     o << kSvgOpen << "height=\"500\" width=\"500\" viewBox=\"0 0 " << (n - 1) << " " << (n - 1) << "\">\n";
     o << "<defs>\n";
     if (!maya) {
@@ -177,13 +303,14 @@ static rt_status domino_pairs_svg(const int32_t* t, int64_t tlen, const char* fi
         }
     }
     o << "</defs>\n";
-    for (int i = 0; i < n; ++i)
+    for_rows(o, 0, n, n, [&](Sink& o, int i) {
         for (int j = 0; j < n; ++j) {
             const int32_t v = t[(size_t)i * n + j];
             const bool odd = (i + j) % 2 == 1;
             if ((v & 1) == 1) use(o, odd ? "h1" : "h2", j, i, true);
             if ((v & 4) == 4) use(o, odd ? "v1" : "v2", j, i, true);
         }
+    });
     o << "</svg>";
     return finish(o);
 }
@@ -212,7 +339,7 @@ rt_status rt_domino_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d, 
     }
     if (dlen < (int64_t)m * m) return RT_E_INVAL;
     auto D = [&](int i, int j) { return d[(size_t)i * m + j]; };
-    std::ofstream o(filename);
+    Sink o(filename);
     o << kSvgOpen << "height=\"500\" width=\"500\" viewBox=\"0 0 " << m << " " << m << "\">\n";
     o << "<defs>\n";
     o << "<g id=\"hd\">  <polyline points= \"-.5,0 .5,0\" stroke=\"red\" stroke-width=\".05\"/> </g>\n";
@@ -222,14 +349,15 @@ rt_status rt_domino_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d, 
     o << "<g id=\"b\">  <circle cx=\"0\" cy=\"0\" r=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
     o << "<g id=\"w\">  <circle cx=\"0\" cy=\"0\" r=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"white\" /> </g>\n";
     o << "</defs>\n";
-    for (int i = 0; i < n; ++i)
+    for_rows(o, 0, n, n, [&](Sink& o, int i) {
         for (int j = 0; j < n; ++j) {
             const double x = j, y = i;
             const int32_t v = t[(size_t)i * n + j];
             if ((v & 1) == 1) use(o, "hd", x, y - .5, false);
             if ((v & 4) == 4) use(o, "vd", x - .5, y, false);
         }
-    for (int i = 1; i < m; ++i)
+    });
+    for_rows(o, 1, m, m, [&](Sink& o, int i) {
         for (int j = 1; j < m; ++j) {
             if (D(i, j) != 1) continue;
             const double x = j + .5, y = i + .5;
@@ -240,9 +368,11 @@ rt_status rt_domino_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d, 
             if (D(i - 1, j) == 1) use(o, "ve", x, y - .5, false);
             if (D(i + 1, j) == 1) use(o, "ve", x, y + .5, false);
         }
-    for (int i = 1; i < m; ++i)
+    });
+    for_rows(o, 1, m, m, [&](Sink& o, int i) {
         for (int j = 1; j < m; ++j)
             if (D(i, j) == 1) use(o, (i + j) % 2 == 0 ? "b" : "w", j + .5, i + .5, true);
+    });
     o << "</svg>";
     return finish(o);
 }
@@ -252,15 +382,16 @@ rt_status rt_domino_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d, 
 rt_status rt_lozenge_domain_svg(const int32_t* d, int64_t dlen, const char* filename) {
     if (!d || !filename) return RT_E_INVAL;
     const int m = side_of(dlen / 2);
-    std::ofstream o(filename);
+    Sink o(filename);
     tri_header(o, m);
     o << "<defs>\n";
     o << "<g id=\"w\">  <polygon points = \"0,1 .5,0 1,1\" fill=\"lightsteelblue\"/> </g>\n";
     o << "<g id=\"b\">  <polygon points = \"0,0 1,0 .5,1\" fill=\"slategrey\"/> </g>\n";
     o << "</defs>\n";
-    for (int i = 0; i < m; ++i)
+    for_rows(o, 0, m, 2 * m, [&](Sink& o, int i) {
         for (int j = 0; j < 2 * m; ++j)
             if (d[(size_t)i * 2 * m + j] == 1) use(o, j % 2 == 0 ? "b" : "w", .5 * j + .5 * i, i, true);
+    });
     o << "</svg>";
     return finish(o);
 }
@@ -269,20 +400,21 @@ rt_status rt_lozenge_domain_svg(const int32_t* d, int64_t dlen, const char* file
 rt_status rt_lozenge_tiling_svg(const int32_t* t, int64_t tlen, const char* filename) {
     if (!t || !filename) return RT_E_INVAL;
     const int n = side_of(tlen), m = n - 1;
-    std::ofstream o(filename);
+    Sink o(filename);
     tri_header(o, m);
     o << "<defs>\n";
     o << "<g id=\"r\">  <polygon points = \"0,0 -1,0 -.5,-1 .5,-1\" fill=\"midnightblue\"/> </g>\n";
     o << "<g id=\"g\">  <polygon points = \"0,0 1,0 .5,-1 -.5,-1\" fill=\"lightsteelblue\"/> </g>\n";
     o << "<g id=\"b\">  <polygon points = \"0,0 .5,-1 1,0 .5,1\" fill=\"slategrey\"/> </g>\n";
     o << "</defs>\n";
-    for (int i = 1; i < n - 1; ++i)
+    for_rows(o, 1, n - 1, n, [&](Sink& o, int i) {
         for (int j = 1; j < n - 1; ++j) {
             const int32_t v = t[(size_t)i * n + j];
             if ((v & 1) == 1) use(o, "r", j + .5 * i, i, true);
             if ((v & 2) == 2) use(o, "g", j + .5 * i, i, true);
             if ((v & 8) == 8) use(o, "b", j + .5 * i, i, true);
         }
+    });
     o << "</svg>";
     return finish(o);
 }
@@ -315,7 +447,7 @@ rt_status rt_lozenge_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d,
         d = dom.data();
     }
     auto D = [&](int i, int j) { return d[(size_t)i * m * 2 + j]; };
-    std::ofstream o(filename);
+    Sink o(filename);
     tri_header(o, m);
     o << "<defs>\n";
     o << "<g id=\"e1\">  <polyline points= \"-.5,-.33333333333 0,-.666666666666\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
@@ -327,23 +459,26 @@ rt_status rt_lozenge_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d,
     o << "<g id=\"b\">  <ellipse cx=\".5\" cy=\".333333333333\" rx=\".1\" ry=\".11547\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
     o << "<g id=\"w\">  <ellipse cx=\".5\" cy=\".666666666666\" rx=\".1\"  ry=\".11547\" stroke=\"black\" stroke-width=\".02\" fill=\"white\" /> </g>\n";
     o << "</defs>\n";
-    for (int i = 1; i < n - 1; ++i)
+    for_rows(o, 1, n - 1, n, [&](Sink& o, int i) {
         for (int j = 1; j < n - 1; ++j) {
             const int32_t v = t[(size_t)i * n + j];
             if ((v & 1) == 1) use(o, "d1", j + .5 * i, i, true);
             if ((v & 2) == 2) use(o, "d2", j + .5 * i, i, true);
             if ((v & 8) == 8) use(o, "d8", j + .5 * i, i, true);
         }
-    for (int i = 1; i < n - 1; ++i)
+    });
+    for_rows(o, 1, n - 1, 2 * n, [&](Sink& o, int i) {
         for (int j = 1; j < 2 * n - 1; ++j)
             if (D(i, j) == 1 && j % 2 == 0) {
                 if (D(i, j - 1) == 1) use(o, "e1", .5 + .5 * j + .5 * i, i + 1, true);
                 if (D(i, j + 1) == 1) use(o, "e2", .5 + .5 * j + .5 * i, i + 1, true);
                 if (D(i + 1, j - 1) == 1) use(o, "e8", .5 + .5 * j + .5 * i, i + 1, true);
             }
-    for (int i = 1; i < n - 1; ++i)
+    });
+    for_rows(o, 1, n - 1, 2 * n, [&](Sink& o, int i) {
         for (int j = 1; j < 2 * n - 1; ++j)
             if (D(i, j) == 1) use(o, j % 2 == 0 ? "b" : "w", .5 * i + .5 * j, i, true);
+    });
     o << "</svg>";
     return finish(o);
 }
@@ -352,11 +487,11 @@ rt_status rt_lozenge_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d,
 rt_status rt_lozenge_print_domain(const int32_t* d, int64_t dlen, const char* filename) {
     if (!d || !filename) return RT_E_INVAL;
     const int m = side_of(dlen / 2);
-    std::ofstream o(filename);
-    for (int i = 0; i < m; ++i) {
+    Sink o(filename);
+    for_rows(o, 0, m, 2 * m, [&](Sink& o, int i) {
         for (int j = 0; j < 2 * m; ++j) o << d[(size_t)i * 2 * m + j] << " ";
         o << "\n";
-    }
+    });
     return finish(o);
 }
 
@@ -365,13 +500,14 @@ rt_status rt_recttri_tiling_svg(const int32_t* t, int64_t tlen, const char* file
     if (!t || !filename) return RT_E_INVAL;
     const int n = side_of(tlen), m = n - 1;
     const double W = kSqrt3 * 2 * (n + 1), H = 3 / 2.0 * (n + 1), s = 20;
-    std::ofstream o(filename);
+    Sink o(filename);
     o << "<svg xmlns='http://www.w3.org/2000/svg' height=\"" << s * H << "\" width=\"" << s * W << "\" >\n";
-    for (int i = 0; i < m; ++i)
+    for_rows(o, 0, m, 8 * m, [&](Sink& o, int i) {
         for (int j = 0; j < m; ++j) {
-            o << face_picture((t[(size_t)i * n + j + 1] & (0xf << 4)) >> 4, i, 2 * j + 1);
-            o << face_picture(t[(size_t)i * n + j] & 0xf, i, 2 * j);
+            face_picture(o, (t[(size_t)i * n + j + 1] & (0xf << 4)) >> 4, i, 2 * j + 1);
+            face_picture(o, t[(size_t)i * n + j] & 0xf, i, 2 * j);
         }
+    });
     o << "</svg>";
     return finish(o);
 }
@@ -380,15 +516,16 @@ rt_status rt_recttri_tiling_svg(const int32_t* t, int64_t tlen, const char* file
 rt_status rt_tridimer_domain_svg(const int32_t* d, int64_t dlen, const char* filename) {
     if (!d || !filename) return RT_E_INVAL;
     const int m = side_of(dlen / 2);
-    std::ofstream o(filename);
+    Sink o(filename);
     tri_header(o, m);
     o << "<defs>\n";
     o << "<g id=\"w\">  <polygon points = \"0,1 .5,0 1,1\" fill=\"paleturquoise\"/> </g>\n";
     o << "<g id=\"b\">  <polygon points = \"0,0 1,0 .5,1\" fill=\"deepskyblue\"/> </g>\n";
     o << "</defs>\n";
-    for (int i = 0; i < m; ++i)
+    for_rows(o, 0, m, 2 * m, [&](Sink& o, int i) {
         for (int j = 0; j < 2 * m; ++j)
             if (d[(size_t)i * m * 2 + j] == 1) use(o, j % 2 == 0 ? "b" : "w", .5 * j + .5 * i, i, true);
+    });
     o << "</svg>";
     return finish(o);
 }
@@ -396,20 +533,21 @@ rt_status rt_tridimer_domain_svg(const int32_t* d, int64_t dlen, const char* fil
 rt_status rt_tridimer_tiling_svg(const int32_t* t, int64_t tlen, const char* filename) {
     if (!t || !filename) return RT_E_INVAL;
     const int n = side_of(tlen), m = n / 2;
-    std::ofstream o(filename);
+    Sink o(filename);
     tri_header(o, m);
     o << "<defs>\n";
     o << "<g id=\"dR\">  <polygon points = \"1,-0.6666666667 0.5,-0.3333333333 0.5,0.3333333333 0,0.6666666667 0,1.333333333 0.5,1.666666667 1,1.333333333 1,0.6666666667 1.5,0.3333333333 1.5,-0.3333333333\" fill=\"midnightblue\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
     o << "<g id=\"dL\">  <polygon points = \"0,-0.6666666667 0.5,-0.3333333333 0.5,0.3333333333 1,0.6666666667 1,1.333333333 0.5,1.666666667 0,1.333333333 0,0.6666666667 -0.5,0.3333333333 -0.5,-0.3333333333\" fill=\"lightsteelblue\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
     o << "<g id=\"dH\">  <polygon points = \"0,-0.6666666667 0.5,-0.3333333333 1,-0.6666666667 1.5,-0.3333333333 1.5,0.3333333333 1,0.6666666667 0.5,0.3333333333 0,0.6666666667 -0.5,0.3333333333 -0.5,-0.3333333333\" fill=\"slategrey\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
     o << "</defs>\n";
-    for (int i = 0; i < m - 1; ++i)
+    for_rows(o, 0, m - 1, m, [&](Sink& o, int i) {
         for (int j = 1; j < 2 * m - 1; j += 2) {
             const double x = .5 * j + .5 * i;
             if ((t[(size_t)2 * i * n + j] & 4) == 4) use(o, "dR", x, i, true);
             if ((t[(size_t)2 * i * n + j] & 8) == 8) use(o, "dL", x, i, true);
             if ((t[(size_t)(2 * i + 1) * n + j] & 1) == 1) use(o, "dH", x, i, true);
         }
+    });
     o << "</svg>";
     return finish(o);
 }
@@ -433,7 +571,7 @@ rt_status rt_tridimer_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d
     Vec pad((size_t)2 * m * (m + 2) + 2, 0);
     for (int64_t k = 0; k < dlen; ++k) pad[(size_t)k + 2 * m + 1] = d[k];
     auto D = [&](int i, int j) { return pad[(size_t)(i * 2 * m + j) + 2 * m + 1]; };
-    std::ofstream o(filename);
+    Sink o(filename);
     tri_header(o, m);
     o << "<defs>\n";
     o << "<g id=\"dR\">  <polyline points= \".5,1 1,0\" stroke=\"darkblue\" stroke-width=\".05\"/> </g>\n";
@@ -446,7 +584,7 @@ rt_status rt_tridimer_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d
     o << "<g id=\"v2\">  <ellipse cx=\"1.5\" cy=\"0\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
     o << "<g id=\"v3\">  <ellipse cx=\"1\" cy=\"1\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
     o << "</defs>\n";
-    for (int i = 0; i < m - 1; ++i)
+    for_rows(o, 0, m - 1, 2 * m, [&](Sink& o, int i) {
         for (int j = 1; j < 2 * m - 1; j += 2) {
             const double x = .5 * j + .5 * i;
             const int32_t a = t[(size_t)2 * i * n + j], h = t[(size_t)(2 * i + 1) * n + j];
@@ -459,13 +597,15 @@ rt_status rt_tridimer_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d
             if ((a & 4) == 0 && D(i, j) == 1) use(o, "eR", x, i, true);
             if ((a & 8) == 0 && D(i, j - 2) == 1 && j > 1) use(o, "eL", x, i, true);
         }
-    for (int i = 0; i < m; ++i)
+    });
+    for_rows(o, 0, m, 2 * m, [&](Sink& o, int i) {
         for (int j = 2; j < 2 * m; j += 2) {
             const double x = .5 * j + .5 * i;
             if (D(i, j) == 1 || D(i, j - 1) == 1) use(o, "v1", x, i, true);
             if (D(i, j) == 1 || D(i, j + 1) == 1) use(o, "v2", x, i, true);
             if (D(i, j) == 1 || D(i, j + 1) == 1 || D(i, j - 1) == 1) use(o, "v3", x, i, true);
         }
+    });
     o << "</svg>";
     return finish(o);
 }
@@ -475,11 +615,11 @@ rt_status rt_tridimer_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d
 rt_status rt_save_matrix(const int32_t* a, int64_t len, const char* filename) {
     if (!a || !filename) return RT_E_INVAL;
     const int n = side_of(len);
-    std::ofstream o(filename);
-    for (int i = 0; i < n; ++i) {
+    Sink o(filename);
+    for_rows(o, 0, n, n, [&](Sink& o, int i) {
         for (int j = 0; j < n; ++j) o << a[(size_t)i * n + j] << " ";
         o << "\n";
-    }
+    });
     return finish(o);
 }
 
@@ -507,6 +647,111 @@ rt_status rt_load_matrix(const char* filename, int32_t* out, int64_t cap, int64_
     if (!out) return RT_OK;
     if (cap < (int64_t)v.size()) return RT_E_INVAL;
     for (size_t k = 0; k < v.size(); ++k) out[k] = v[k];
+    return RT_OK;
+}
+
+// ---- binary matrices (no reference counterpart) ---------------------------------------------
+// Header (little-endian, 40 bytes): "RTBMAT1\0", int64 count, int32 bits per
+// value (1, 2, 4, 8, 16 or 32), int32 0, int64 base, uint64 FNV-1a of the
+// payload.  Payload: value - base in `bits` bits, LSB first within each byte
+// for bits < 8, little-endian words otherwise.  The smallest width that
+// holds max - min is chosen, so a domino tiling (values 0..15) takes 4 bits
+// a value, an eighth of the int32 array.
+namespace {
+const char kBinMagic[8] = {'R', 'T', 'B', 'M', 'A', 'T', '1', '\0'};
+constexpr size_t kBinHeader = 40;
+
+uint64_t fnv1a(const unsigned char* p, size_t n) {
+    uint64_t h = 1469598103934665603ull;
+    for (size_t k = 0; k < n; ++k) h = (h ^ p[k]) * 1099511628211ull;
+    return h;
+}
+
+size_t bin_payload(int64_t count, int bits) { return (size_t)(((uint64_t)count * (uint64_t)bits + 7) / 8); }
+}  // namespace
+
+rt_status rt_save_matrix_binary(const int32_t* a, int64_t len, const char* filename) {
+    if ((!a && len > 0) || len < 0 || !filename) return RT_E_INVAL;
+    int64_t lo = 0, hi = 0;
+    for (int64_t k = 0; k < len; ++k) {
+        if (k == 0 || a[k] < lo) lo = a[k];
+        if (k == 0 || a[k] > hi) hi = a[k];
+    }
+    const uint64_t span = (uint64_t)(hi - lo);
+    int bits = 32;
+    for (int b : {1, 2, 4, 8, 16})
+        if (span < (1ull << b)) {
+            bits = b;
+            break;
+        }
+    std::vector<unsigned char> pay(bin_payload(len, bits), 0);
+    for (int64_t k = 0; k < len; ++k) {
+        const uint32_t v = (uint32_t)((int64_t)a[k] - lo);
+        if (bits < 8) {
+            pay[(size_t)((k * bits) >> 3)] |= (unsigned char)(v << ((k * bits) & 7));
+        } else {
+            for (int byte = 0; byte < bits / 8; ++byte) pay[(size_t)k * (bits / 8) + byte] = (unsigned char)(v >> (8 * byte));
+        }
+    }
+    unsigned char head[kBinHeader] = {0};
+    std::memcpy(head, kBinMagic, 8);
+    const uint64_t cnt = (uint64_t)len, base = (uint64_t)lo, sum = fnv1a(pay.data(), pay.size());
+    for (int b = 0; b < 8; ++b) {
+        head[8 + b] = (unsigned char)(cnt >> (8 * b));
+        head[24 + b] = (unsigned char)(base >> (8 * b));
+        head[32 + b] = (unsigned char)(sum >> (8 * b));
+    }
+    for (int b = 0; b < 4; ++b) head[16 + b] = (unsigned char)((uint32_t)bits >> (8 * b));
+    std::FILE* f = std::fopen(filename, "wb");
+    if (!f) return RT_E_INVAL;
+    bool ok = std::fwrite(head, 1, kBinHeader, f) == kBinHeader &&
+              (pay.empty() || std::fwrite(pay.data(), 1, pay.size(), f) == pay.size());
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? RT_OK : RT_E_INVAL;
+}
+
+rt_status rt_load_matrix_binary(const char* filename, int32_t* out, int64_t cap, int64_t* len) {
+    if (!filename) return RT_E_INVAL;
+    std::FILE* f = std::fopen(filename, "rb");
+    if (!f) return RT_E_INVAL;
+    unsigned char head[kBinHeader];
+    std::vector<unsigned char> pay;
+    bool ok = std::fread(head, 1, kBinHeader, f) == kBinHeader && std::memcmp(head, kBinMagic, 8) == 0;
+    uint64_t cnt = 0, base = 0, sum = 0;
+    uint32_t bits = 0, zero = 0;
+    if (ok) {
+        for (int b = 0; b < 8; ++b) {
+            cnt |= (uint64_t)head[8 + b] << (8 * b);
+            base |= (uint64_t)head[24 + b] << (8 * b);
+            sum |= (uint64_t)head[32 + b] << (8 * b);
+        }
+        for (int b = 0; b < 4; ++b) {
+            bits |= (uint32_t)head[16 + b] << (8 * b);
+            zero |= (uint32_t)head[20 + b] << (8 * b);
+        }
+        ok = zero == 0 && (bits == 1 || bits == 2 || bits == 4 || bits == 8 || bits == 16 || bits == 32) &&
+             cnt <= (1ull << 40);
+    }
+    if (ok) {
+        pay.resize(bin_payload((int64_t)cnt, (int)bits));
+        ok = pay.empty() || std::fread(pay.data(), 1, pay.size(), f) == pay.size();
+        ok = ok && std::fgetc(f) == EOF && fnv1a(pay.data(), pay.size()) == sum;
+    }
+    std::fclose(f);
+    if (!ok) return RT_E_INVAL;  // not this format, truncated, trailing bytes or corrupted
+    if (len) *len = (int64_t)cnt;
+    if (!out) return RT_OK;
+    if (cap < (int64_t)cnt) return RT_E_INVAL;
+    const int64_t lo = (int64_t)base;
+    for (uint64_t k = 0; k < cnt; ++k) {
+        uint32_t v = 0;
+        if (bits < 8) {
+            v = (pay[(size_t)((k * bits) >> 3)] >> ((k * bits) & 7)) & ((1u << bits) - 1);
+        } else {
+            for (uint32_t byte = 0; byte < bits / 8; ++byte) v |= (uint32_t)pay[(size_t)k * (bits / 8) + byte] << (8 * byte);
+        }
+        out[k] = (int32_t)(lo + (int64_t)v);
+    }
     return RT_OK;
 }
 

@@ -43,6 +43,8 @@ class _Tiler:
     # common helpers (src/common/common.h:50-69)
     SaveMatrix = staticmethod(lambda a, f: builders.save_matrix(a, f))
     LoadMatrix = staticmethod(lambda f: builders.load_matrix(f))
+    SaveMatrixBinary = staticmethod(lambda a, f: builders.save_matrix_binary(a, f))
+    LoadMatrixBinary = staticmethod(lambda f: builders.load_matrix_binary(f))
 
     def __init__(self, device: int = 0, kernel: int = _capi.RT_KERNEL_DEFAULT, rng: int = _capi.RT_RNG_TINYMT,
                  q: float = 0.99, qcmp: int = _capi.RT_QCMP_FLOAT32, weights=None, stream=None, chain: int = 0):

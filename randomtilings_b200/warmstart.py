@@ -41,7 +41,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import _capi
+from . import _capi, builders
 from .batch import Batch
 from .heights import HeightPlan
 from .mlp import CoordinateMLP
@@ -97,13 +97,19 @@ class Prepared:
     idx: np.ndarray            # flat indices of the domain's vertices
 
 
-def prepare(spec: DomainSpec) -> Prepared:
+def prepare(spec: DomainSpec, device: int | None = None) -> Prepared:
+    """Extremal tilings and heights of the domain: on the host (the
+    reference's flood), or on `device` (rt_extremal_tilings, the same arrays)."""
     cls = spec.tiler
     d = spec.domain()
-    tmin = np.asarray(cls.MinTiling(d), dtype=np.int32)
-    tmax = np.asarray(cls.MaxTiling(d), dtype=np.int32)
-    a = np.asarray(cls.TilingToHeightfunc(tmin, d), dtype=np.int32)
-    b = np.asarray(cls.TilingToHeightfunc(tmax, d), dtype=np.int32)
+    if device is None:
+        tmin = np.asarray(cls.MinTiling(d), dtype=np.int32)
+        tmax = np.asarray(cls.MaxTiling(d), dtype=np.int32)
+        a = np.asarray(cls.TilingToHeightfunc(tmin, d), dtype=np.int32)
+        b = np.asarray(cls.TilingToHeightfunc(tmax, d), dtype=np.int32)
+    else:
+        ext, _ = builders.extremal_tilings(spec.model, d, device)
+        tmin, tmax, a, b = ext["tmin"], ext["tmax"], ext["hmin"], ext["hmax"]
     n = int(round(tmin.size ** 0.5))
     idx = np.flatnonzero(a != INF)
     return Prepared(spec, d, n, tmin, tmax, np.minimum(a, b), np.maximum(a, b), idx)
@@ -448,7 +454,7 @@ def main(argv=None) -> None:
         kind, size = e.split(":")
         sz = tuple(int(v) for v in size.split("x"))
         spec = DomainSpec(kind, sz if kind == AZTEC or len(sz) == 3 else sz * 3)
-        p = prepare(spec)
+        p = prepare(spec, ws.device)
         tw, st = ws.warm_tiling(p)
         r = relax(p, {"cold": p.tmin, "warm": tw}, int(a.eval_sweeps * burn_sweeps(spec)), points=a.points,
                   seed=a.seed + 1, log=log)

@@ -107,3 +107,14 @@ def test_large_aztec_and_hexagon_timing_is_reported():
     assert st["n"] == 2006 and st["device_ms"] > 0
     st = _check(1, rt.LozengeTiler.Hexagon(500, 500, 500))
     assert st["n"] == 1008
+
+
+@pytest.mark.parametrize("kind,size", [("aztec", (50,)), ("hexagon", (20, 30, 25))])
+def test_warm_start_preparation_on_the_device(kind, size):
+    from randomtilings_b200 import warmstart as ws
+
+    spec = ws.DomainSpec(kind, size)
+    a, b = ws.prepare(spec), ws.prepare(spec, 0)
+    for f in ("tmin", "tmax", "hmin", "hmax", "idx"):
+        assert np.array_equal(getattr(a, f), getattr(b, f)), f
+    assert a.n == b.n
