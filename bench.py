@@ -474,15 +474,18 @@ def run_extremal(args) -> None:
         tmin, tmax = cls.MinTiling(d), cls.MaxTiling(d)
         hmin, hmax = cls.TilingToHeightfunc(tmin, d), cls.TilingToHeightfunc(tmax, d)
         host_s = time.perf_counter() - a
-        walls, st = [], None
+        walls, st, phases = [], None, []
         for _ in range(args.steps):
             a = time.perf_counter()
             dev, st = builders.extremal_tilings(model, d)
             walls.append(time.perf_counter() - a)
+            phases.append({k: round(st[k], 2) for k in ("walk_ms", "alloc_ms", "upload_ms", "device_ms",
+                                                        "download_ms")})
         equal = all(np.array_equal(dev[k], np.asarray(v)) for k, v in
                     (("tmin", tmin), ("tmax", tmax), ("hmin", hmin), ("hmax", hmax)))
         out.append({"domain": name, "n": st["n"], "equal_to_host": equal, "host_s": round(host_s, 4),
-                    "device_call_s": round(statistics.median(walls), 4), "device_ms": round(st["device_ms"], 3),
+                    "device_call_s": round(statistics.median(walls), 4), "first_call_s": round(walls[0], 4),
+                    "phases_ms": phases, "device_ms": round(st["device_ms"], 3),
                     "passes": st["passes"], "tile_updates": st["tile_updates"], "boundary": st["boundary"],
                     "speedup_call": round(host_s / statistics.median(walls), 1)})
         print(json.dumps(out[-1]), file=sys.stderr, flush=True)

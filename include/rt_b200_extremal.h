@@ -39,6 +39,10 @@ typedef struct {
     int64_t passes;       /* relaxation passes over the tiles */
     int64_t tile_updates; /* tiles that changed, summed over the passes */
     double device_ms;     /* device time from the uploaded domain to the finished outputs */
+    double walk_ms;       /* host: the boundary walk */
+    double alloc_ms;      /* host: device allocations */
+    double upload_ms;     /* host: copy of the domain and the boundary heights to the device */
+    double download_ms;   /* host: copies of the requested outputs back */
 } rt_extremal_stats;
 
 /* model: RT_DOMINO or RT_LOZENGE.  d, dlen: the domain as the builders

@@ -194,7 +194,8 @@ SIGNATURES["rt_project_heights"] = (ctypes.c_int, [_I32, _P, _I64, _P, _P, _P, _
 
 class RtExtremalStats(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int32), ("boundary", ctypes.c_int64), ("passes", ctypes.c_int64),
-                ("tile_updates", ctypes.c_int64), ("device_ms", ctypes.c_double)]
+                ("tile_updates", ctypes.c_int64), ("device_ms", ctypes.c_double), ("walk_ms", ctypes.c_double),
+                ("alloc_ms", ctypes.c_double), ("upload_ms", ctypes.c_double), ("download_ms", ctypes.c_double)]
 
 
 # include/rt_b200_extremal.h

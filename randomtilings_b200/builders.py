@@ -64,8 +64,7 @@ def extremal_tilings(model: int, domain, device: int = 0) -> tuple[dict, dict]:
     _capi.check(lib.rt_extremal_tilings(model, d.ctypes.data, d.size, device, out["tmin"].ctypes.data,
                                         out["tmax"].ctypes.data, out["hmin"].ctypes.data, out["hmax"].ctypes.data,
                                         n * n, ctypes.byref(st)))
-    stats = {"n": st.n, "boundary": st.boundary, "passes": st.passes, "tile_updates": st.tile_updates,
-             "device_ms": st.device_ms}
+    stats = {k: getattr(st, k) for k, _ in _capi.RtExtremalStats._fields_}
     return out, stats
 
 

@@ -15,13 +15,14 @@
 // Layout: vertex kinds (uint8, 0 outside / 1 interior / 2 boundary) and the
 // two height arrays (int32) on the n x n vertex grid, row-major.  The
 // relaxation runs over 32 x 64-vertex tiles: a CTA loads its tile and a
-// one-vertex halo into shared memory, sweeps it until nothing changes
-// (alternating the row order so that values run both ways through a
-// thread's rows), writes back what changed and, if anything did, marks the
-// tile and its eight neighbours for the next pass.  Tiles not marked return
-// at once, so a pass costs in proportion to the moving front.
+// one-vertex halo into shared memory, each thread keeps an 8-vertex column
+// segment in registers and sweeps it down and up, the CTA iterating until
+// nothing changes; then it writes back what changed and marks for the next
+// pass the neighbours that read a changed border value.  Tiles not marked
+// return at once, so a pass costs in proportion to the moving front.
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <climits>
 #include <cstring>
 #include <vector>
@@ -110,6 +111,7 @@ __global__ void __launch_bounds__(XT) ext_relax(const uint8_t* __restrict__ kind
     if (!dirty_in[tile]) return;  // the same answer for the whole block
     __shared__ int32_t sx[XPR][XPC], sn[XPR][XPC];
     __shared__ uint8_t sk[XPR][XPC];
+    __shared__ unsigned s_mark;
     const int ty = tile / tiles_x, tx = tile % tiles_x;
     const int r0 = ty * XR, c0 = tx * XC;
     for (int e = threadIdx.x; e < XPR * XPC; e += XT) {
@@ -128,66 +130,132 @@ __global__ void __launch_bounds__(XT) ext_relax(const uint8_t* __restrict__ kind
         sn[r][c] = b;
     }
     __syncthreads();
-    if (threadIdx.x == 0) dirty_in[tile] = 0;  // nothing else writes dirty_in during this pass
+    if (threadIdx.x == 0) {
+        dirty_in[tile] = 0;  // nothing else writes dirty_in during this pass
+        s_mark = 0;          // read after the barriers of the sweep loop
+    }
 
+    // Thread: column c, rows 8 grp .. 8 grp + 7 of the tile, kept in registers
+    // (x = maximal, y = minimal function).  An iteration reads the values it
+    // needs from the neighbouring columns and the rows just outside its
+    // segment, sweeps the segment down and then up (vertical neighbours come
+    // from registers, already updated), and publishes what changed.
     const int c = threadIdx.x & (XC - 1), grp = threadIdx.x / XC;
-    const int cc = c + 1, gj = c0 + c;
-    uint32_t mine = 0;  // bit k: owned vertex k (row 8 grp + k) is interior
+    const int cc = c + 1, rb = 8 * grp + 1, gj = c0 + c;
+    const int p0 = (r0 + 8 * grp + gj) & 1;  // parity of the segment's first vertex (dominoes)
+    int32_t x[8], y[8];
+    uint32_t mine = 0;  // bit k: vertex k of the segment is interior
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        const int r = 8 * grp + k + 1;
-        if (sk[r][cc] == 1) mine |= 1u << k;
+        x[k] = sx[rb + k][cc];
+        y[k] = sn[rb + k][cc];
+        if (sk[rb + k][cc] == 1) mine |= 1u << k;
     }
-    uint32_t wrote = 0;  // bit k: maximal value of vertex k lowered; bit k + 8: minimal value raised
+    uint32_t wrote = 0;  // bit k: x[k] lowered; bit k + 8: y[k] raised
+    bool capped = true;
     for (int it = 0; it < kLocalCap; ++it) {
-        int ch = 0;
+        uint32_t chg = 0;
         if (mine) {
+            // candidates from the other columns, fixed for this iteration
+            int32_t ax[8], ay[8];
 #pragma unroll
-            for (int kk = 0; kk < 8; ++kk) {
-                const int k = (it & 1) ? 7 - kk : kk;
-                if (!(mine >> k & 1u)) continue;
-                const int r = 8 * grp + k + 1;
-                int32_t nx, nn;
+            for (int k = 0; k < 8; ++k) {
+                const int r = rb + k;
                 if (DOM) {
-                    if (((r0 + r - 1 + gj) & 1) == 0) {
-                        nx = min(sx[r - 1][cc], sx[r + 1][cc]) + 1;
-                        nn = max(sn[r][cc - 1], sn[r][cc + 1]) - 1;
+                    // even vertex: y from left / right; odd vertex: x from left / right
+                    if (((p0 ^ k) & 1) == 0) {
+                        ay[k] = max(sn[r][cc - 1], sn[r][cc + 1]);
+                        ax[k] = kBig;
                     } else {
-                        nx = min(sx[r][cc - 1], sx[r][cc + 1]) + 1;
-                        nn = max(sn[r - 1][cc], sn[r + 1][cc]) - 1;
+                        ax[k] = min(sx[r][cc - 1], sx[r][cc + 1]);
+                        ay[k] = -kBig;
                     }
                 } else {
-                    nx = min(min(sx[r][cc + 1], sx[r - 1][cc]), sx[r + 1][cc - 1]) + 1;
-                    nn = max(max(sn[r - 1][cc + 1], sn[r][cc - 1]), sn[r + 1][cc]) - 1;
-                }
-                if (nx < sx[r][cc]) {
-                    sx[r][cc] = nx;
-                    wrote |= 1u << k;
-                    ch = 1;
-                }
-                if (nn > sn[r][cc]) {
-                    sn[r][cc] = nn;
-                    wrote |= 1u << (k + 8);
-                    ch = 1;
+                    ax[k] = min(sx[r][cc + 1], sx[r + 1][cc - 1]);  // (0,+1), (+1,-1)
+                    ay[k] = max(sn[r - 1][cc + 1], sn[r][cc - 1]);  // (-1,+1), (0,-1)
                 }
             }
+            const int32_t xt = sx[rb - 1][cc], xb = sx[rb + 8][cc], yt = sn[rb - 1][cc], yb = sn[rb + 8][cc];
+#pragma unroll
+            for (int sweep = 0; sweep < 2; ++sweep) {
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk) {
+                    const int k = sweep == 0 ? kk : 7 - kk;
+                    if (!(mine >> k & 1u)) continue;
+                    const int32_t xu = k > 0 ? x[k - 1] : xt, xd = k < 7 ? x[k + 1] : xb;
+                    const int32_t yu = k > 0 ? y[k - 1] : yt, yd = k < 7 ? y[k + 1] : yb;
+                    int32_t nx, ny;
+                    if (DOM) {
+                        if (((p0 ^ k) & 1) == 0) {
+                            nx = min(xu, xd) + 1;
+                            ny = ay[k] - 1;
+                        } else {
+                            nx = ax[k] + 1;
+                            ny = max(yu, yd) - 1;
+                        }
+                    } else {
+                        nx = min(ax[k], xu) + 1;  // (-1,0) is up
+                        ny = max(ay[k], yd) - 1;  // (+1,0) is down
+                    }
+                    if (nx < x[k]) {
+                        x[k] = nx;
+                        chg |= 1u << k;
+                    }
+                    if (ny > y[k]) {
+                        y[k] = ny;
+                        chg |= 1u << (k + 8);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                if (chg >> k & 1u) sx[rb + k][cc] = x[k];
+                if (chg >> (k + 8) & 1u) sn[rb + k][cc] = y[k];
+            }
+            wrote |= chg;
         }
-        if (!__syncthreads_or(ch)) break;
+        if (!__syncthreads_or(chg != 0)) {
+            capped = false;
+            break;
+        }
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        const int r = 8 * grp + k + 1;
-        const int64_t g = (int64_t)(r0 + r - 1) * n + gj;
-        if (wrote >> k & 1u) hx[g] = sx[r][cc];
-        if (wrote >> (k + 8) & 1u) hn[g] = sn[r][cc];
+        const int64_t g = (int64_t)(r0 + 8 * grp + k) * n + gj;
+        if (wrote >> k & 1u) hx[g] = x[k];
+        if (wrote >> (k + 8) & 1u) hn[g] = y[k];
     }
-    if (__syncthreads_or(wrote != 0) && threadIdx.x == 0) {
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int y = ty + dy, x = tx + dx;
-                if (y >= 0 && x >= 0 && y < tiles_y && x < tiles_x) dirty_out[y * tiles_x + x] = 1;
-            }
-        atomicAdd(changed_tiles, 1u);
+    // Which neighbours read a changed value: the tile above reads row 0, the
+    // one below row XR-1, the side tiles the outer columns; lozenge rules also
+    // read the (-1,+1) and (+1,-1) diagonals, i.e. the corner vertices.  A
+    // tile that stopped at its sweep cap is marked again itself.
+    enum : unsigned { M_UP = 1, M_DOWN = 2, M_LEFT = 4, M_RIGHT = 8, M_UPRIGHT = 16, M_DOWNLEFT = 32, M_SELF = 64,
+                      M_ANY = 128 };
+    const uint32_t top = wrote & (1u | 1u << 8), bottom = wrote & (1u << 7 | 1u << 15);
+    unsigned mark = 0;
+    if (wrote) mark |= M_ANY;
+    if (grp == 0 && top) mark |= M_UP;
+    if (grp == XR / 8 - 1 && bottom) mark |= M_DOWN;
+    if (c == 0 && wrote) mark |= M_LEFT;
+    if (c == XC - 1 && wrote) mark |= M_RIGHT;
+    if (!DOM && grp == 0 && c == XC - 1 && top) mark |= M_UPRIGHT;
+    if (!DOM && grp == XR / 8 - 1 && c == 0 && bottom) mark |= M_DOWNLEFT;
+    if (capped && threadIdx.x == 0) mark |= M_SELF;
+    if (mark) atomicOr(&s_mark, mark);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_mark) {
+        const unsigned m = s_mark;
+        auto set = [&](int y, int x) {
+            if (y >= 0 && x >= 0 && y < tiles_y && x < tiles_x) dirty_out[y * tiles_x + x] = 1;
+        };
+        if (m & M_UP) set(ty - 1, tx);
+        if (m & M_DOWN) set(ty + 1, tx);
+        if (m & M_LEFT) set(ty, tx - 1);
+        if (m & M_RIGHT) set(ty, tx + 1);
+        if (m & M_UPRIGHT) set(ty - 1, tx + 1);
+        if (m & M_DOWNLEFT) set(ty + 1, tx - 1);
+        if (m & M_SELF) set(ty, tx);
+        if (m & M_ANY) atomicAdd(changed_tiles, 1u);
     }
 }
 
@@ -305,10 +373,14 @@ extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_
                                          rt_extremal_stats* stats) {
     if ((model != RT_DOMINO && model != RT_LOZENGE) || !d || dlen <= 0) return RT_E_INVAL;
     const bool dom = model == RT_DOMINO;
+    using clk = std::chrono::steady_clock;
+    auto ms_since = [](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };
+    auto t0 = clk::now();
     int n = 0;
     std::vector<int64_t> bidx;
     std::vector<int32_t> bh;
     if (!boundary_walk(model, d, dlen, &n, &bidx, &bh)) return RT_E_INVAL;
+    const double walk_ms = ms_since(t0);
     const int m = n - 1;
     const int64_t nn = (int64_t)n * n;
     if (len != nn) return RT_E_INVAL;
@@ -316,6 +388,7 @@ extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_
     const int tiles_x = (n + XC - 1) / XC, tiles_y = (n + XR - 1) / XR;
     const int64_t tiles = (int64_t)tiles_x * tiles_y;
     if (tiles > INT_MAX) return RT_E_INVAL;
+    t0 = clk::now();
     DevBuf dd, dk, dx, dn, dtx, dtn, dbi, dbh, dflag, dcnt;
     if (!dd.alloc((size_t)dlen * 4) || !dk.alloc((size_t)nn) || !dx.alloc((size_t)nn * 4) ||
         !dn.alloc((size_t)nn * 4) || !dtx.alloc((size_t)nn * 4) || !dtn.alloc((size_t)nn * 4) ||
@@ -327,6 +400,8 @@ extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_
         cudaEventCreate(&st.e0) != cudaSuccess || cudaEventCreate(&st.e1) != cudaSuccess)
         return RT_E_CUDA;
     cudaStream_t s = st.s;
+    const double alloc_ms = ms_since(t0);
+    t0 = clk::now();
     auto* K = static_cast<uint8_t*>(dk.p);
     auto* HX = static_cast<int32_t*>(dx.p);
     auto* HN = static_cast<int32_t*>(dn.p);
@@ -337,6 +412,8 @@ extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_
     cudaMemcpyAsync(dbh.p, bh.data(), bh.size() * 4, cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(F, 1, (size_t)tiles, s);
     cudaMemsetAsync(F + tiles, 0, (size_t)tiles, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return RT_E_CUDA;
+    const double upload_ms = ms_since(t0);
     cudaEventRecord(st.e0, s);
     const int T = 256;
     const unsigned vb = (unsigned)((nn + T - 1) / T);
@@ -390,6 +467,7 @@ extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_
     cudaMemcpyAsync(&bad, C + kGroup, 4, cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return RT_E_CUDA;
     if (bad) return RT_E_INVAL;  // not tileable: the flood ran past a boundary height
+    t0 = clk::now();
     if (tmin) cudaMemcpyAsync(tmin, TN, (size_t)nn * 4, cudaMemcpyDeviceToHost, s);
     if (tmax) cudaMemcpyAsync(tmax, TX, (size_t)nn * 4, cudaMemcpyDeviceToHost, s);
     if (hmin) cudaMemcpyAsync(hmin, HN, (size_t)nn * 4, cudaMemcpyDeviceToHost, s);
@@ -403,6 +481,10 @@ extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_
         stats->passes = passes;
         stats->tile_updates = updates;
         stats->device_ms = ms;
+        stats->walk_ms = walk_ms;
+        stats->alloc_ms = alloc_ms;
+        stats->upload_ms = upload_ms;
+        stats->download_ms = ms_since(t0);
     }
     return RT_OK;
 }
