@@ -7,8 +7,11 @@
 // shared memory 64 columns of K at a time; each GEMM names its operands'
 // layouts, so one kernel serves the forward product X * W^T, the input
 // gradient dZ * W and the weight gradient dZ^T * X (the last split over K,
-// reduced with FP32 atomics).  Epilogues, read from tensor memory with
-// tcgen05.ld, fuse bias + GELU (forward) and the GELU derivative (backward).
+// reduced with FP32 atomics).  Operands contiguous along K are staged with
+// 16-byte asynchronous copies, the others as 8 x 8 core matrices transposed
+// in registers.  Epilogues, read from tensor memory with tcgen05.ld and
+// turned through shared memory so that global accesses run along rows, fuse
+// bias + GELU (forward) and the GELU derivative (backward).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -119,49 +122,83 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
     return false;
 }
 
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+    // src_bytes 0: the 16 bytes are zero-filled and nothing is read
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+
 // Stages rows [r0, r0 + 128) x k [k0, k_end) of a logical operand whose
-// element (r, k) is o[r][k] (kcontig: 8 consecutive k are one 16-byte load)
-// or o[k][r] (8 consecutive r are one 16-byte load, scattered over 8 core
-// matrix rows); rows >= rlim and k >= k_end read as zero.
-__device__ __forceinline__ void stage_chunk(unsigned char* dst, const __nv_bfloat16* p, int ld, bool kcontig, int r0,
-                                            int rlim, int k0, int k_end) {
-    const int tid = threadIdx.x;
-    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
-    if (kcontig) {
-        for (int e = tid; e < TBM * (TBK / 8); e += 128) {
-            const int r = e / (TBK / 8), k8 = (e % (TBK / 8)) * 8;
-            const int gr = r0 + r, gk = k0 + k8;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (gr < rlim && gk + 8 <= k_end) {
-                v = *reinterpret_cast<const uint4*>(p + (size_t)gr * ld + gk);
-            } else if (gr < rlim) {
-                __nv_bfloat16 t[8];
+// element (r, k) is p[r * ld + k] into the canonical K-major layout: every
+// 16-byte group of 8 consecutive k is one asynchronous copy (zero-filled
+// for rows >= rlim), so all of a chunk's loads are in flight together; a
+// group cut by k_end is assembled element by element.
+__device__ __forceinline__ void stage_kcontig(uint32_t sdst, unsigned char* dst, const __nv_bfloat16* p, int ld,
+                                              int r0, int rlim, int k0, int k_end) {
+    const uint16_t* q = reinterpret_cast<const uint16_t*>(p);
+    for (int e = threadIdx.x; e < TBM * (TBK / 8); e += 128) {
+        const int r = e / (TBK / 8), k8 = (e % (TBK / 8)) * 8;
+        const int gr = r0 + r, gk = k0 + k8;
+        const uint32_t off = chunk_off(r, k8);
+        if (gr >= rlim || gk + 8 <= k_end) {
+            const bool in = gr < rlim;
+            cp_async16(sdst + off, in ? (const void*)(q + (size_t)gr * ld + gk) : (const void*)q, in ? 16u : 0u);
+        } else {
+            uint32_t w[4];
 #pragma unroll
-                for (int x = 0; x < 8; ++x) t[x] = gk + x < k_end ? p[(size_t)gr * ld + gk + x] : zero;
-                v = *reinterpret_cast<const uint4*>(t);
+            for (int x = 0; x < 4; ++x) {
+                const uint32_t lo = gk + 2 * x < k_end ? q[(size_t)gr * ld + gk + 2 * x] : 0u;
+                const uint32_t hi = gk + 2 * x + 1 < k_end ? q[(size_t)gr * ld + gk + 2 * x + 1] : 0u;
+                w[x] = lo | hi << 16;
             }
-            *reinterpret_cast<uint4*>(dst + chunk_off(r, k8)) = v;
-        }
-    } else {
-        for (int e = tid; e < TBK * (TBM / 8); e += 128) {
-            const int k = e / (TBM / 8), r8 = (e % (TBM / 8)) * 8;
-            const int gr = r0 + r8, gk = k0 + k;
-            __nv_bfloat16 t[8];
-            if (gk < k_end && gr + 8 <= rlim) {
-                *reinterpret_cast<uint4*>(t) = *reinterpret_cast<const uint4*>(p + (size_t)gk * ld + gr);
-            } else {
-#pragma unroll
-                for (int x = 0; x < 8; ++x) t[x] = (gk < k_end && gr + x < rlim) ? p[(size_t)gk * ld + gr + x] : zero;
-            }
-#pragma unroll
-            for (int x = 0; x < 8; ++x) *reinterpret_cast<__nv_bfloat16*>(dst + chunk_off(r8 + x, k)) = t[x];
+            *reinterpret_cast<uint4*>(dst + off) = make_uint4(w[0], w[1], w[2], w[3]);
         }
     }
 }
 
+// The same chunk of an operand stored the other way, element (r, k) at
+// p[k * ld + r].  Thread t builds core matrix (t / 8, t % 8) -- rows
+// 8 (t / 8) .. +7, k 8 (t % 8) .. +7: eight 16-byte loads along r, an 8 x 8
+// transpose of 16-bit values in registers, eight 16-byte stores that fill
+// the core matrix's 128 contiguous bytes.
+__device__ __forceinline__ void stage_mncontig(unsigned char* dst, const __nv_bfloat16* p, int ld, int r0, int rlim,
+                                               int k0, int k_end) {
+    const uint16_t* q = reinterpret_cast<const uint16_t*>(p);
+    const int rg = threadIdx.x >> 3, kg = threadIdx.x & 7;
+    const int gr = r0 + 8 * rg, gkb = k0 + 8 * kg;
+    uint32_t w[8][4];  // w[kk]: r = gr .. gr + 7 at k = gkb + kk, two per word
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+        const int gk = gkb + kk;
+        if (gk < k_end && gr + 8 <= rlim) {
+            const uint4 v = *reinterpret_cast<const uint4*>(q + (size_t)gk * ld + gr);
+            w[kk][0] = v.x, w[kk][1] = v.y, w[kk][2] = v.z, w[kk][3] = v.w;
+        } else {
+#pragma unroll
+            for (int x = 0; x < 4; ++x) {
+                const uint32_t lo = (gk < k_end && gr + 2 * x < rlim) ? q[(size_t)gk * ld + gr + 2 * x] : 0u;
+                const uint32_t hi = (gk < k_end && gr + 2 * x + 1 < rlim) ? q[(size_t)gk * ld + gr + 2 * x + 1] : 0u;
+                w[kk][x] = lo | hi << 16;
+            }
+        }
+    }
+#pragma unroll
+    for (int rr = 0; rr < 8; ++rr) {
+        uint32_t o[4];
+#pragma unroll
+        for (int x = 0; x < 4; ++x) {
+            const uint32_t a = (w[2 * x][rr >> 1] >> (16 * (rr & 1))) & 0xFFFFu;
+            const uint32_t b = (w[2 * x + 1][rr >> 1] >> (16 * (rr & 1))) & 0xFFFFu;
+            o[x] = a | b << 16;
+        }
+        *reinterpret_cast<uint4*>(dst + chunk_off(8 * rg + rr, 8 * kg)) = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+}
+
 __global__ void __launch_bounds__(128, 1) gemm_tc(const __grid_constant__ GemmArgs g) {
-    __shared__ __align__(128) unsigned char sA[TBM * TBK * 2];
-    __shared__ __align__(128) unsigned char sB[TBN * TBK * 2];
+    // A and B chunks; after the last MMA the epilogue's per-warp staging
+    __shared__ __align__(128) unsigned char sAB[(TBM + TBN) * TBK * 2];
+    unsigned char* sA = sAB;
+    unsigned char* sB = sAB + TBM * TBK * 2;
     __shared__ __align__(8) unsigned long long mbar;
     __shared__ uint32_t tmem_slot;
     __shared__ int s_fail;
@@ -193,9 +230,16 @@ __global__ void __launch_bounds__(128, 1) gemm_tc(const __grid_constant__ GemmAr
         // Stage A as (m, k) and B as (n, k) = B[k][n]; zero outside the matrices.
         // A(m, k) is contiguous along k unless A is transposed; B(k, n) as (n, k)
         // is contiguous along k when B is transposed.
-        stage_chunk(sA, g.A.p, g.A.ld, g.A.trans == 0, m0, g.M, k0, k_end);
-        stage_chunk(sB, g.B.p, g.B.ld, g.B.trans != 0, 0, g.N, k0, k_end);
-        // generic-proxy stores -> visible to the tensor core's async proxy
+        if (g.A.trans == 0)
+            stage_kcontig(sa, sA, g.A.p, g.A.ld, m0, g.M, k0, k_end);
+        else
+            stage_mncontig(sA, g.A.p, g.A.ld, m0, g.M, k0, k_end);
+        if (g.B.trans != 0)
+            stage_kcontig(sb, sB, g.B.p, g.B.ld, 0, g.N, k0, k_end);
+        else
+            stage_mncontig(sB, g.B.p, g.B.ld, 0, g.N, k0, k_end);
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        // shared-memory writes -> visible to the tensor core's async proxy
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
@@ -227,8 +271,12 @@ __global__ void __launch_bounds__(128, 1) gemm_tc(const __grid_constant__ GemmAr
     }
 
     if (!s_fail && !first) {
-        // Epilogue: this warp's 32 rows, 32 columns per tcgen05.ld.
-        const int m = m0 + 32 * warp + lane;
+        // Epilogue: this warp's 32 rows (TMEM lanes 32w .. 32w + 31), 32
+        // columns per tcgen05.ld (lane = row), turned through shared memory
+        // (32 x 33 floats per warp) so that the global loads and stores run
+        // along rows: lane = column.
+        float* stg = reinterpret_cast<float*>(sAB) + warp * (32 * 33);
+        const int mrow = m0 + 32 * warp;
 #pragma unroll 1
         for (int c0 = 0; c0 < TBN; c0 += 32) {
             uint32_t v[32];
@@ -245,26 +293,30 @@ __global__ void __launch_bounds__(128, 1) gemm_tc(const __grid_constant__ GemmAr
                 : "r"(taddr)
                 : "memory");
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (m < g.M) {
 #pragma unroll
-                for (int x = 0; x < 32; ++x) {
-                    const int n = c0 + x;
-                    if (n >= g.N) continue;
-                    const float acc = __uint_as_float(v[x]);
-                    const size_t at = (size_t)m * g.N + n;
-                    if (g.epi == EPI_FWD) {
-                        const float z = acc + g.bias[n];
-                        g.out_f[at] = z;
-                        g.out_h[at] = __float2bfloat16(gelu(z));
-                    } else if (g.epi == EPI_DGELU) {
-                        const float dd = acc * gelu_grad(g.zin[at]);
-                        g.out_f[at] = dd;
-                        g.out_h[at] = __float2bfloat16(dd);
-                    } else {
-                        atomicAdd(g.out_f + at, acc);
-                    }
+            for (int x = 0; x < 32; ++x) stg[lane * 33 + x] = __uint_as_float(v[x]);
+            __syncwarp();
+            const int n = c0 + lane;
+            const float b = (g.epi == EPI_FWD && n < g.N) ? g.bias[n] : 0.0f;
+#pragma unroll 4
+            for (int rr = 0; rr < 32; ++rr) {
+                const int m = mrow + rr;
+                if (m >= g.M || n >= g.N) continue;
+                const float acc = stg[rr * 33 + lane];
+                const size_t at = (size_t)m * g.N + n;
+                if (g.epi == EPI_FWD) {
+                    const float z = acc + b;
+                    g.out_f[at] = z;
+                    g.out_h[at] = __float2bfloat16(gelu(z));
+                } else if (g.epi == EPI_DGELU) {
+                    const float dd = acc * gelu_grad(g.zin[at]);
+                    g.out_f[at] = dd;
+                    g.out_h[at] = __float2bfloat16(dd);
+                } else {
+                    atomicAdd(g.out_f + at, acc);
                 }
             }
+            __syncwarp();
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
