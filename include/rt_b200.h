@@ -94,6 +94,21 @@ rt_status rt_load_rng_params(rt_tiler* h, const char* path, int64_t n);
 /* Same, from memory: 3*n uint32 (mat1, mat2, tmat per id). */
 rt_status rt_set_rng_params(rt_tiler* h, const uint32_t* table, int64_t n);
 
+/* Weighted dominoes (no reference counterpart; the reference's heat-bath
+ * kernel dominokernelCFTP.cl:19-28 is the uniform case): the heat-bath
+ * kernel (RT_KERNEL_CFTP) with periodic domino weights.  A domino covering
+ * squares (r, c) and (r, c+1) weighs wh[(r mod P) P + (c mod P)], one
+ * covering (r, c) and (r+1, c) wv[(r mod P) P + (c mod P)] (square (r, c)
+ * spans vertices (r..r+1, c..c+1)); period P is 1, 2 or 4, weights finite
+ * and > 0.  At a rotatable vertex (i, j) the two horizontal dominoes (state
+ * 3) weigh w3 = wh(i-1, j-1) wh(i, j-1) and the two vertical ones (state 12)
+ * w12 = wv(i-1, j-1) wv(i-1, j); the site becomes 12 when the draw is below
+ * w12 / (w3 + w12), else 3 -- for equal weights exactly the reference's
+ * 0.5.  The walk, epoch walk and CFTP of the handle use them in the TinyMT
+ * and Philox modes; RT_RNG_PLANES (one random bit per site) rejects them.
+ * period = 0 returns to uniform weights. */
+rt_status rt_set_domino_weights(rt_tiler* h, int32_t period, const double* wh, const double* wv);
+
 /* Replaces Walk(tiling&, long steps, long seed) src/Domino/DominoTiler.cpp:9-55,
  * Walk(tiling&, int, long) src/Lozenge/LozengeTiler.cpp:18-88,
  * src/RectTriangle/RectTriangleTiler.cpp:17-92,

@@ -57,6 +57,8 @@ def oracle() -> ctypes.CDLL:
                                                 ctypes.c_double, ctypes.c_int]
         lib.orc_philox4x32_10.argtypes = [_P, _P, _P]
         lib.orc_domino_walk_fast.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.c_int]
+        lib.orc_domino_walk_weighted.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_uint32, _P, _I64, ctypes.c_int, _P, _P]
         lib.orc_domino_walk_planes.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.c_int]
         lib.orc_lozenge_walk_planes.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32]
         lib.orc_lozenge_walk_fast.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.c_int,
@@ -130,6 +132,21 @@ def domino_walk_epochs(t, steps, seeds, cftp=True, params=None) -> np.ndarray:
     p, np_, keep = _table(params)
     _check(oracle().orc_domino_walk_epochs(a.ctypes.data, n, st.ctypes.data, se.ctypes.data, st.size, p, np_,
                                            int(cftp)), "orc_domino_walk_epochs")
+    return a
+
+
+def domino_walk_weighted(t, steps, seeds, wh, wv, fast=False, single_walk=False, chain=0, params=None) -> np.ndarray:
+    """The heat-bath domino walk with periodic weights (orc_domino_walk_weighted);
+    steps / seeds are per epoch (one each for a single walk)."""
+    a, n = _tiling(t)
+    st = np.ascontiguousarray(np.atleast_1d(steps), dtype=np.int64)
+    se = np.ascontiguousarray(np.atleast_1d(seeds), dtype=np.int64)
+    h = np.ascontiguousarray(wh, dtype=np.float64)
+    v = np.ascontiguousarray(wv, dtype=np.float64)
+    p, np_, keep = _table(params)
+    _check(oracle().orc_domino_walk_weighted(a.ctypes.data, n, st.ctypes.data, se.ctypes.data, st.size,
+                                             int(single_walk), int(fast), chain, p, np_, h.shape[0], h.ctypes.data,
+                                             v.ctypes.data), "orc_domino_walk_weighted")
     return a
 
 
@@ -233,13 +250,16 @@ def walk_planes(model: str, t, steps, keys, chain: int = 0) -> np.ndarray:
 
 
 def cftp(tmax, tmin, first_steps: int, master_seed: int, schedule: str = "doubling", max_trials: int = 30,
-         model: str = "domino_cftp", fast: bool = False, planes: bool = False, **kw):
+         model: str = "domino_cftp", fast: bool = False, planes: bool = False, weights=None, **kw):
     """CFTP composed from the restated epoch walks, following
     Examples/AztecDiamondCftpEx.cpp:42-68 (seeds: successive mt19937 outputs,
     newest epoch first; in fast mode each seed is its epoch's Philox key).
-    model: "domino_cftp", "lozenge" or "qlozenge" (kw: q, qcmp_double).
+    model: "domino_cftp", "lozenge" or "qlozenge" (kw: q, qcmp_double);
+    weights: (wh, wv) periodic domino weights for "domino_cftp".
     Returns (tiling, trials, total_steps, coalesced)."""
     def run(t, steps, seeds):
+        if weights is not None:
+            return domino_walk_weighted(t, steps, seeds, weights[0], weights[1], fast=fast, **kw)
         if planes:
             return walk_planes(model, t, steps, seeds, **kw)
         if fast:

@@ -311,14 +311,37 @@ int orc_lozenge_colours(int64_t seed, int64_t steps, uint8_t* out) {
  * dominokernelCFTP.cl:11-31 (heat bath: rd < .5 -> 12, else -> 3).
  * Work item (g0, g1) of the (N-2) x (N/2-2) range owns site (g0+1, g1+1) and
  * TinyMT stream g1 + (N/2-2) g0 (src/TinyMT/tinymt.clh:24-30). */
-static void domino_rotate(int8_t* a, int n, orc_draws* rng, int cftp) {
+/* Periodic domino weights (no reference counterpart): NULL = uniform. */
+typedef struct {
+    int period;
+    const double* wh; /* horizontal domino on squares (r, c), (r, c+1): wh[(r mod P) P + c mod P] */
+    const double* wv; /* vertical domino on squares (r, c), (r+1, c) */
+} orc_weights;
+
+static double weight_at(const double* w, int P, int r, int c) { return w[(((r % P) + P) % P) * P + (((c % P) + P) % P)]; }
+
+/* Heat-bath probability of state 12 (two vertical dominoes) at vertex (i, j):
+ * w12 / (w3 + w12), w3 the two horizontal dominoes' weights (squares
+ * (i-1, j-1)-(i-1, j) and (i, j-1)-(i, j)), w12 the two vertical ones'
+ * ((i-1, j-1)-(i, j-1) and (i-1, j)-(i, j)). */
+static double weighted_p12(const orc_weights* w, int i, int j) {
+    const int P = w->period;
+    const double w3 = weight_at(w->wh, P, i - 1, j - 1) * weight_at(w->wh, P, i, j - 1);
+    const double w12 = weight_at(w->wv, P, i - 1, j - 1) * weight_at(w->wv, P, i - 1, j);
+    return w12 / (w3 + w12);
+}
+
+static void domino_rotate(int8_t* a, int n, orc_draws* rng, int cftp, const orc_weights* wts, int black) {
     const int h = n / 2, gw = h - 2;
     for (int g0 = 0; g0 < n - 2; ++g0)
         for (int g1 = 0; g1 < gw; ++g1) {
             const float rd = orc_draw(rng, g0, g1);
             int8_t* v = &a[(g0 + 1) * h + (g1 + 1)];
             if (cftp) {
-                if ((double)rd < 0.5) {
+                /* array column c of the black / white array is vertex column 2c + parity */
+                const int i = g0 + 1, j = 2 * (g1 + 1) + (black ? (i & 1) : 1 - (i & 1));
+                const double p = wts ? weighted_p12(wts, i, j) : 0.5;
+                if ((double)rd < p) {
                     if (*v == 3) *v = 12;
                 } else if (*v == 12) {
                     *v = 3;
@@ -375,7 +398,8 @@ static void domino_merge(int32_t* t, int n, const int8_t* b, const int8_t* w) {
 }
 
 static int domino_run(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k, int single_walk,
-                      const uint32_t* params, int64_t nparams, int cftp, int fast, uint32_t chain) {
+                      const uint32_t* params, int64_t nparams, int cftp, int fast, uint32_t chain,
+                      const orc_weights* wts) {
     /* fast == 2: bit-plane mode (Philox bits, same colour cycle as fast mode) */
     const int planes = fast == 2;
     if (n < 6 || n % 2) return ORC_EINVAL;
@@ -407,13 +431,13 @@ static int domino_run(int32_t* t, int n, const int64_t* steps, const int64_t* se
                 if (planes)
                     domino_rotate_planes(b, n, &rng, cftp);
                 else
-                    domino_rotate(b, n, &rng, cftp);
+                    domino_rotate(b, n, &rng, cftp, wts, 1);
                 domino_update(w, b, n, 1);
             } else {
                 if (planes)
                     domino_rotate_planes(w, n, &rng, cftp);
                 else
-                    domino_rotate(w, n, &rng, cftp);
+                    domino_rotate(w, n, &rng, cftp, wts, 0);
                 domino_update(b, w, n, 0);
             }
             draws_next(&rng);
@@ -428,25 +452,33 @@ static int domino_run(int32_t* t, int n, const int64_t* steps, const int64_t* se
 
 int orc_domino_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
                     int cftp_kernel) {
-    return domino_run(t, n, &steps, &seed, 1, 1, params, nparams, cftp_kernel, 0, 0);
+    return domino_run(t, n, &steps, &seed, 1, 1, params, nparams, cftp_kernel, 0, 0, NULL);
 }
 
 int orc_domino_walk_epochs(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k,
                            const uint32_t* params, int64_t nparams, int cftp_kernel) {
     if (k < 0) return ORC_EINVAL;
-    return domino_run(t, n, steps, seeds, k, 0, params, nparams, cftp_kernel, 0, 0);
+    return domino_run(t, n, steps, seeds, k, 0, params, nparams, cftp_kernel, 0, 0, NULL);
 }
 
 int orc_domino_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
                          int cftp_kernel) {
     if (k < 0) return ORC_EINVAL;
-    return domino_run(t, n, steps, keys, k, 0, NULL, 0, cftp_kernel, 1, chain);
+    return domino_run(t, n, steps, keys, k, 0, NULL, 0, cftp_kernel, 1, chain, NULL);
+}
+
+int orc_domino_walk_weighted(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k, int single_walk,
+                             int fast, uint32_t chain, const uint32_t* params, int64_t nparams, int period,
+                             const double* wh, const double* wv) {
+    if (k < 0 || (period != 1 && period != 2 && period != 4) || !wh || !wv) return ORC_EINVAL;
+    const orc_weights w = {period, wh, wv};
+    return domino_run(t, n, steps, seeds, k, single_walk, params, nparams, 1, fast ? 1 : 0, chain, &w);
 }
 
 int orc_domino_walk_planes(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
                            int heat_bath) {
     if (k < 0) return ORC_EINVAL;
-    return domino_run(t, n, steps, keys, k, 0, NULL, 0, heat_bath, 2, chain);
+    return domino_run(t, n, steps, keys, k, 0, NULL, 0, heat_bath, 2, chain, NULL);
 }
 
 /* ------------------------------------------------------------------------ */

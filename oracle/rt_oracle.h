@@ -82,6 +82,15 @@ int orc_lozenge_walk_epochs(int32_t* t, int n, const int64_t* steps, const int64
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 int orc_domino_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
                          int cftp_kernel);
+/* Weighted heat bath (no reference counterpart; rt_set_domino_weights):
+ * dominokernelCFTP.cl's rule with the threshold 0.5 replaced at vertex (i, j)
+ * by w12 / (w3 + w12) from period x period tables of horizontal (wh) and
+ * vertical (wv) domino weights indexed by the domino's top-left square.
+ * fast = 0: TinyMT draws and the reference's colour order (single_walk as
+ * orc_domino_walk, else as orc_domino_walk_epochs); fast = 1: Philox. */
+int orc_domino_walk_weighted(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k, int single_walk,
+                             int fast, uint32_t chain, const uint32_t* params, int64_t nparams, int period,
+                             const double* wh, const double* wv);
 int orc_lozenge_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
                           int qmode, double q, int qcmp);
 /* Bit-plane mode (RT_RNG_PLANES): the same colour cycle as fast mode, one

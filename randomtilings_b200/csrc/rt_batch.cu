@@ -223,6 +223,7 @@ __global__ void __launch_bounds__(1024, 1) batch_site_kernel(const __grid_consta
             wa.wpad = W;
             for (int x = 0; x < 4; ++x) wa.thr[x] = b.thr[x];
             for (int x = 0; x < 16; ++x) wa.weights[x] = b.weights[x];
+            wa.wper = 0;  // no weighted dominoes in batches
         }
         for (int c = 0; c < NC; ++c) {
             const T* g = static_cast<const T*>(ch.arr[c]);

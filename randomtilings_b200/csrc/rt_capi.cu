@@ -205,6 +205,8 @@ struct rt_tiler {
     int64_t drop_phase = -1;  // RT_TEST_DROP_PUBLISH: a phase whose rows CTA 0 withholds (bounded-wait tests)
     int64_t last_phases = 0, last_launches = 0;
     uint64_t timeout_ns = 5000000000ull;
+    int wper = 0;           // weighted domino heat bath: period (0 = uniform)
+    uint32_t wthr[16] = {};
 
     rt_status fail(rt_status s, const std::string& msg) {
         err = msg;
@@ -343,6 +345,32 @@ rt_status rt_destroy(rt_tiler* h) {
 const char* rt_last_error(rt_tiler* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
 
 void* rt_stream(rt_tiler* h) { return h ? static_cast<void*>(h->stream) : nullptr; }
+
+rt_status rt_set_domino_weights(rt_tiler* h, int32_t period, const double* wh, const double* wv) {
+    if (!h) return RT_E_INVAL;
+    if (h->family != FAM_DOMINO_HB) return h->fail(RT_E_INVAL, "weights need the domino heat-bath kernel (RT_KERNEL_CFTP)");
+    if (h->cfg.rng == RT_RNG_PLANES) return h->fail(RT_E_INVAL, "the bit-plane mode draws one bit per site: no weights");
+    if (period == 0) {
+        h->wper = 0;
+        return RT_OK;
+    }
+    if ((period != 1 && period != 2 && period != 4) || !wh || !wv)
+        return h->fail(RT_E_INVAL, "weight period must be 1, 2 or 4, with two period x period tables");
+    const int P = period;
+    for (int k = 0; k < P * P; ++k)
+        if (!(wh[k] > 0 && wv[k] > 0) || !std::isfinite(wh[k]) || !std::isfinite(wv[k]))
+            return h->fail(RT_E_INVAL, "domino weights must be finite and > 0");
+    auto W = [&](const double* w, int r, int c) { return w[(((r % P) + P) % P) * P + (((c % P) + P) % P)]; };
+    for (int i = 0; i < P; ++i)
+        for (int j = 0; j < P; ++j) {
+            // vertex class (i, j): the squares (i-1, j-1), (i-1, j), (i, j-1) around it
+            const double w3 = W(wh, i - 1, j - 1) * W(wh, i, j - 1);
+            const double w12 = W(wv, i - 1, j - 1) * W(wv, i - 1, j);
+            h->wthr[i * P + j] = below_threshold(w12 / (w3 + w12));
+        }
+    h->wper = P;
+    return RT_OK;
+}
 
 rt_status rt_set_rng_params(rt_tiler* h, const uint32_t* table, int64_t n) {
     if (!h || (!table && n > 0) || n < 0) return h ? h->fail(RT_E_INVAL, "bad parameter table") : RT_E_INVAL;
@@ -656,6 +684,8 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     a.nepochs = k;
     family_thresholds(h->family, h->cfg.q, h->cfg.qcmp, a.thr);
     std::memcpy(a.weights, h->cfg.weights, sizeof a.weights);
+    a.wper = h->wper;
+    std::memcpy(a.wthr, h->wthr, sizeof a.wthr);
     a.xbuf = static_cast<unsigned long long*>(h->d_xbuf.p);
     a.err = static_cast<int*>(h->d_err.p);
     a.timeout_ns = h->timeout_ns;

@@ -50,7 +50,15 @@ struct WalkArgs {
     int64_t drop_phase;   // tests of the bounded waits: CTA 0 does not publish this phase's rows (-1: none)
     int depth;            // bit-plane kernel: phases per halo exchange
     int pwords;           // bit-plane kernel: 32-bit words per colour-array row
+    int wper;             // domino heat bath with periodic weights: period P (1, 2 or 4), 0 = unweighted
+    uint32_t wthr[16];    // ... its threshold at vertex (i, j): wthr[(i mod P) P + (j mod P)]
 };
+
+// Threshold of the weighted domino heat bath at vertex (i, j).
+__device__ __forceinline__ uint32_t domino_weight_thr(const WalkArgs& a, int i, int j) {
+    const int m = a.wper - 1;
+    return a.wthr[(i & m) * a.wper + (j & m)];
+}
 
 // ---------------------------------------------------------------------------
 // Model interface.  Per phase every thread builds a small context once (the
@@ -81,6 +89,7 @@ struct DominoRule {
         int t;              // the reference's colour of the pending Update
         bool step, upd;
         int w;
+        int arr;            // the array rotated (0 black, 1 white)
         uint32_t thr;
     };
     __device__ static uint32_t written(uint32_t d) { return ph_op(d) == OP_STEP ? 1u << flipped((int)ph_a(d)) : 0u; }
@@ -90,6 +99,7 @@ struct DominoRule {
         x.step = op == (int)OP_STEP;
         x.w = a.wpad;
         x.thr = a.thr[0];
+        x.arr = 1 - ca;
         if (x.step) {
             x.upd = cb != (int)NO_COLOUR && cb != ca;
             x.dst = planes + (1 - ca) * plane;
@@ -118,10 +128,12 @@ struct DominoRule {
         if (HEAT_BATH) return k < thr ? (v == 3 ? 12 : v) : (v == 12 ? 3 : v);
         return k < thr ? (v == 3 ? 12 : (v == 12 ? 3 : v)) : v;
     }
-    __device__ static void site(const WalkArgs&, const Ctx& x, int off, int i, int, uint32_t k) {
+    __device__ static void site(const WalkArgs& a, const Ctx& x, int off, int i, int j, uint32_t k) {
         if (x.step) {
             const int v = x.upd ? refreshed(x, off, i) : (int)x.dst[off];
-            x.dst[off] = (int8_t)flip(v, k, x.thr);
+            // weighted heat bath: array column j is vertex column 2 j + ((i + arr) & 1)
+            const uint32_t thr = HEAT_BATH && a.wper ? domino_weight_thr(a, i, 2 * j + ((i + x.arr) & 1)) : x.thr;
+            x.dst[off] = (int8_t)flip(v, k, thr);
         } else {
             x.dst[off] = (int8_t)refreshed(x, off, i);
         }

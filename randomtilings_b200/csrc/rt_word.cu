@@ -157,7 +157,16 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
         auto apply = [&](const WordInfo& wi, const uint32_t (&k)[4]) {
             uint32_t m0 = 0, m1 = 0;
             if (draws) {
-                m0 = below4(k, a.thr[0]);
+                if (FAM == FAM_DOMINO_HB && a.wper) {
+                    // weighted heat bath: a threshold per site from its vertex (i, j);
+                    // array column c of the rotated array A is vertex column 2 c + ((i + A) & 1)
+                    const int i = a0 + wi.off / W - 1, c0 = wi.off % W, par = (i + 1 - (int)ph_a(d)) & 1;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        m0 |= (uint32_t)(k[b] < domino_weight_thr(a, i, 2 * (c0 + b) + par)) << (8 * b);
+                } else {
+                    m0 = below4(k, a.thr[0]);
+                }
                 if (!M::DOM) m1 = below4(k, a.thr[1]) & ~m0;
             }
             word_phase<FAM>(P, 0, W, wi, m0, m1);

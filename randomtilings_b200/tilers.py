@@ -162,6 +162,20 @@ class DominoTiler(_Tiler):
         d, f = (None, args[0]) if len(args) == 1 else args
         builders.write("rt_domino_dimer_svg", f, t, d)
 
+    def SetWeights(self, wh=None, wv=None) -> None:
+        """Periodic domino weights for the heat-bath kernel (rt_set_domino_weights):
+        wh / wv are P x P tables (P = 1, 2 or 4) of horizontal / vertical domino
+        weights by the domino's top-left square (row mod P, column mod P);
+        None returns to uniform weights."""
+        if wh is None:
+            self._check(_capi.load().rt_set_domino_weights(self._h, 0, None, None))
+            return
+        a = np.ascontiguousarray(wh, dtype=np.float64)
+        b = np.ascontiguousarray(wv, dtype=np.float64)
+        if a.ndim != 2 or a.shape[0] != a.shape[1] or b.shape != a.shape:
+            raise ValueError("wh and wv must be P x P tables of the same shape")
+        self._check(_capi.load().rt_set_domino_weights(self._h, a.shape[0], a.ctypes.data, b.ctypes.data))
+
     def Walk(self, t, steps, seed=None) -> None:  # noqa: N802 -- reference name
         """Walk(t, steps, seed) or Walk(t, [steps...], [seeds...]) (DominoTiler.h:73,76)."""
         if isinstance(steps, (list, tuple, np.ndarray)):

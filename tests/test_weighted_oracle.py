@@ -1,0 +1,67 @@
+"""The oracle's weighted domino heat bath (orc_domino_walk_weighted, the
+checker of rt_set_domino_weights): equal weights give the reference's
+unweighted heat bath bit for bit (TinyMT single and epoch walks, Philox),
+and with unequal weights the chain's stationary law is the weighted one,
+P(T) proportional to the product of T's domino weights, checked on the
+Aztec diamond of order 2 (8 tilings).  CPU only."""
+from __future__ import annotations
+
+from collections import Counter
+
+import numpy as np
+import pytest
+from scipy import stats
+
+from conftest import golden
+from oracle import pyoracle as po
+
+WH = np.array([[1.0, 0.3], [0.5, 2.0]])
+WV = np.array([[0.7, 1.5], [1.0, 0.2]])
+
+
+def tiling_weight(t, wh, wv):
+    """Product of the domino weights: a horizontal domino once, at the vertex
+    whose up edge it crosses (bit 1: top-left square (i-1, j-1)); a vertical
+    one at the vertex whose edge towards j+1 it crosses (bit 8: (i-1, j))."""
+    t = np.asarray(t).reshape(-1)
+    n = int(round(t.size ** 0.5))
+    p = wh.shape[0]
+    w = 1.0
+    for i in range(n):
+        for j in range(n):
+            v = int(t[i * n + j])
+            if v & 1:
+                w *= wh[(i - 1) % p, (j - 1) % p]
+            if v & 8:
+                w *= wv[(i - 1) % p, j % p]
+    return w
+
+
+@pytest.mark.parametrize("period", [1, 2, 4])
+def test_equal_weights_are_the_reference_heat_bath(period):
+    t = golden("builders")["domino/aztec13/min"]
+    one = np.full((period, period), 1.3)
+    assert np.array_equal(po.domino_walk_weighted(t, [700], [5], one, one, single_walk=True),
+                          po.domino_walk(t, 700, 5, cftp=True))
+    assert np.array_equal(po.domino_walk_weighted(t, [300, 200], [5, 9], one, one),
+                          po.domino_walk_epochs(t, [300, 200], [5, 9], cftp=True))
+    assert np.array_equal(po.domino_walk_weighted(t, [300, 200], [5, 2**40 + 1], one, one, fast=True),
+                          po.walk_fast("domino_cftp", t, [300, 200], [5, 2**40 + 1]))
+
+
+def test_unequal_weights_change_the_walk():
+    t = golden("builders")["domino/aztec13/min"]
+    assert not np.array_equal(po.domino_walk_weighted(t, [700], [5], WH, WV, single_walk=True),
+                              po.domino_walk(t, 700, 5, cftp=True))
+
+
+def test_stationary_law_is_the_weighted_one():
+    t0 = golden("builders")["domino/aztec2/min"]
+    ends = [po.domino_walk_weighted(t0, [200], [key], WH, WV, fast=True) for key in range(4000)]
+    c = Counter(e.tobytes() for e in ends)
+    assert len(c) == 8
+    keys = sorted(c)
+    w = np.array([tiling_weight(np.frombuffer(k, dtype=np.int32), WH, WV) for k in keys])
+    obs = np.array([c[k] for k in keys], dtype=float)
+    assert stats.chisquare(obs, obs.sum() * w / w.sum()).pvalue > 1e-4
+    assert stats.chisquare(obs).pvalue < 1e-6  # not the uniform law
