@@ -429,9 +429,12 @@ def run_cftp(args) -> None:
     d = rt.DominoTiler.AztecDiamond(args.cftp_order)
     tmax, tmin = rt.DominoTiler.MaxTiling(d), rt.DominoTiler.MinTiling(d)
     rng = {"tinymt": rt.RT_RNG_TINYMT, "philox": rt.RT_RNG_PHILOX, "planes": rt.RT_RNG_PLANES}[args.cftp_rng]
+    weights = [float(v) for v in args.cftp_weights.split(",")] if args.cftp_weights else None
     runs = []
     for s in range(rank, args.cftp_seeds, world):
         tl = rt.DominoTiler(device=local, kernel=rt.RT_KERNEL_CFTP, rng=rng)
+        if weights:
+            tl.SetWeights(*rt.DominoTiler.TwoPeriodicWeights(*weights))
         a = time.perf_counter()
         _, st = tl.CFTP(tmax, tmin, first_steps=1024, master_seed=s, max_trials=24)
         st["wall_s"] = time.perf_counter() - a
@@ -443,7 +446,9 @@ def run_cftp(args) -> None:
         steps = [r["total_steps"] for r in runs]
         print(json.dumps({
             "metric": "CFTP coalescence (colour steps from the past) and wall time",
-            "workload": f"Aztec diamond n={args.cftp_order}, domino heat bath, doubling from 1024 steps",
+            "workload": f"Aztec diamond n={args.cftp_order}, domino heat bath"
+                        + (f", two-periodic weights a,b = {args.cftp_weights}" if weights else "")
+                        + ", doubling from 1024 steps",
             "rng": args.cftp_rng, "seeds": len(runs), "coalesced": sum(r["coalesced"] for r in runs),
             "median_steps": statistics.median(steps), "max_steps": max(steps),
             "median_sweeps": statistics.median(steps) / 2,
@@ -642,6 +647,8 @@ def main() -> None:
     ap.add_argument("--cftp-order", type=int, default=500)
     ap.add_argument("--cftp-seeds", type=int, default=32)
     ap.add_argument("--cftp-rng", choices=["tinymt", "philox", "planes"], default="planes")
+    ap.add_argument("--cftp-weights", default="",
+                    help="'a,b': two-periodic domino weights (TinyMT or Philox draws)")
     ap.add_argument("--walk-steps", type=int, default=STEPS_PER_WALK,
                     help="colour steps per walk (default 60000 = 20000 sweeps; smaller only for profiling captures)")
     args = ap.parse_args()

@@ -162,6 +162,23 @@ class DominoTiler(_Tiler):
         d, f = (None, args[0]) if len(args) == 1 else args
         builders.write("rt_domino_dimer_svg", f, t, d)
 
+    @staticmethod
+    def TwoPeriodicWeights(a: float, b: float):
+        """(wh, wv) of the two-periodic weighting: every domino borders exactly
+        one even lattice vertex (i + j even, a face of the dual graph) and takes
+        its weight, a when that vertex's row is even, b when it is odd.  Flips
+        at even vertices are then fair; at odd ones the vertical pair wins with
+        probability a^2 / (a^2 + b^2) or b^2 / (a^2 + b^2), rows alternating."""
+        wh, wv = np.zeros((2, 2)), np.zeros((2, 2))
+        for r in range(2):
+            for c in range(2):
+                # horizontal domino on squares (r, c), (r, c+1): vertices (r, c+1), (r+1, c+1)
+                row = r if (r + c + 1) % 2 == 0 else r + 1
+                wh[r, c] = a if row % 2 == 0 else b
+                # vertical domino on squares (r, c), (r+1, c): vertices (r+1, c), (r+1, c+1)
+                wv[r, c] = a if (r + 1) % 2 == 0 else b
+        return wh, wv
+
     def SetWeights(self, wh=None, wv=None) -> None:
         """Periodic domino weights for the heat-bath kernel (rt_set_domino_weights):
         wh / wv are P x P tables (P = 1, 2 or 4) of horizontal / vertical domino

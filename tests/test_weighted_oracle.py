@@ -65,3 +65,27 @@ def test_stationary_law_is_the_weighted_one():
     obs = np.array([c[k] for k in keys], dtype=float)
     assert stats.chisquare(obs, obs.sum() * w / w.sum()).pvalue > 1e-4
     assert stats.chisquare(obs).pvalue < 1e-6  # not the uniform law
+
+
+def _p12(wh, wv, i, j):
+    p = wh.shape[0]
+    w3 = wh[(i - 1) % p, (j - 1) % p] * wh[i % p, (j - 1) % p]
+    w12 = wv[(i - 1) % p, (j - 1) % p] * wv[(i - 1) % p, j % p]
+    return w12 / (w3 + w12)
+
+
+def test_two_periodic_weights():
+    import randomtilings_b200 as rt
+
+    a, b = 1.0, 0.5
+    wh, wv = rt.DominoTiler.TwoPeriodicWeights(a, b)
+    odd = set()
+    for i in range(4):
+        for j in range(4):
+            if (i + j) % 2 == 0:
+                assert _p12(wh, wv, i, j) == 0.5  # even faces: all four dominoes share one weight
+            else:
+                odd.add(round(_p12(wh, wv, i, j), 12))
+    assert odd == {round(a * a / (a * a + b * b), 12), round(b * b / (a * a + b * b), 12)}
+    u, v = rt.DominoTiler.TwoPeriodicWeights(0.7, 0.7)
+    assert np.all(u == 0.7) and np.all(v == 0.7)
