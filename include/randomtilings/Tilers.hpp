@@ -118,6 +118,13 @@ public:
                                      (int32_t)st.size()),
                       h_);
     }
+    // Periodic domino weights for the heat bath (rt_set_domino_weights): P x P
+    // row-major tables, P = 1, 2 or 4; P = 0 returns to uniform weights.
+    void SetWeights(int P, const std::vector<double>& wh, const std::vector<double>& wv) {
+        if (P != 0 && (wh.size() != (size_t)(P * P) || wv.size() != (size_t)(P * P)))
+            throw Error(RT_E_INVAL, "weight tables must hold P x P values");
+        detail::check(rt_set_domino_weights(h_, P, P ? wh.data() : nullptr, P ? wv.data() : nullptr), h_);
+    }
     static domain Rectangle(int M, int N) {
         return detail::build([&](int32_t* o, int64_t c, int64_t* l) { return rt_domino_rectangle(M, N, o, c, l); });
     }

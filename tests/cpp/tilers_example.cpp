@@ -36,8 +36,13 @@ int main(int argc, char** argv) {
             save(f, "lozenge_walk", t);
             rt::DominoTiler D(0, /*cftp=*/true);
             std::vector<long> steps{256, 128}, seeds{2718281, 345903};
+            rt::tiling m2 = m;
             D.Walk(m, steps, seeds);
             save(f, "aztec_epochs", m);
+            rt::DominoTiler W(0, /*cftp=*/true);
+            W.SetWeights(2, {1.0, 0.3, 0.5, 2.0}, {0.7, 1.5, 1.0, 0.2});
+            W.Walk(m2, steps, seeds);
+            save(f, "aztec_weighted", m2);
             rt::TriangleDimerTiler T(0);
             T.Walk(cone, 800, 9);
             save(f, "cone_walk", cone);

@@ -57,3 +57,6 @@ def test_cpp_layer_walks(tmp_path):
     assert np.array_equal(got["cone_walk"], po.tridimer_walk(b["tridimer/cone10_3/tiling"], 800, 9))
     assert np.array_equal(got["aztec_epochs"],
                           po.domino_walk_epochs(got["aztec_min"], [256, 128], [2718281, 345903], cftp=True))
+    wh, wv = np.array([[1.0, 0.3], [0.5, 2.0]]), np.array([[0.7, 1.5], [1.0, 0.2]])
+    assert np.array_equal(got["aztec_weighted"],
+                          po.domino_walk_weighted(got["aztec_min"], [256, 128], [2718281, 345903], wh, wv))
