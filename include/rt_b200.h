@@ -109,6 +109,21 @@ rt_status rt_set_rng_params(rt_tiler* h, const uint32_t* table, int64_t n);
  * period = 0 returns to uniform weights. */
 rt_status rt_set_domino_weights(rt_tiler* h, int32_t period, const double* wh, const double* wv);
 
+/* Weighted lozenges (no reference counterpart; lozengekernel.cl:19-31 is
+ * the uniform case): the uniform-lozenge kernel (char storage) with
+ * periodic lozenge weights.  A lozenge is weighed by the lattice edge it
+ * covers, named by its lower end (i, j): w0 for the edge to (i, j+1) (bit
+ * 8), w1 for (i-1, j+1) (bit 2), w2 for (i-1, j) (bit 1), each table
+ * indexed [(i mod P) P + (j mod P)], P = 1, 2 or 4, weights finite and
+ * > 0.  At a flippable vertex (i, j), state 25 weighs
+ * W25 = w2(i, j) w0(i, j) w1(i+1, j-1) and state 38
+ * W38 = w1(i, j) w0(i, j-1) w2(i+1, j); with p = W38 / (W25 + W38) a draw
+ * below 0.8 p turns 25 into 38 and one in [0.8 p, 0.8) turns 38 into 25 --
+ * for equal weights exactly the reference's 0.4 / 0.8.  Walks, epoch walks
+ * and CFTP of the handle use them in the TinyMT and Philox modes;
+ * RT_RNG_PLANES rejects them.  period = 0 returns to uniform weights. */
+rt_status rt_set_lozenge_weights(rt_tiler* h, int32_t period, const double* w0, const double* w1, const double* w2);
+
 /* Replaces Walk(tiling&, long steps, long seed) src/Domino/DominoTiler.cpp:9-55,
  * Walk(tiling&, int, long) src/Lozenge/LozengeTiler.cpp:18-88,
  * src/RectTriangle/RectTriangleTiler.cpp:17-92,

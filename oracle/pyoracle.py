@@ -59,6 +59,8 @@ def oracle() -> ctypes.CDLL:
         lib.orc_domino_walk_fast.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.c_int]
         lib.orc_domino_walk_weighted.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_uint32, _P, _I64, ctypes.c_int, _P, _P]
+        lib.orc_lozenge_walk_weighted.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_uint32, _P, _I64, ctypes.c_int, _P, _P, _P]
         lib.orc_domino_walk_planes.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.c_int]
         lib.orc_lozenge_walk_planes.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32]
         lib.orc_lozenge_walk_fast.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, ctypes.c_int,
@@ -147,6 +149,20 @@ def domino_walk_weighted(t, steps, seeds, wh, wv, fast=False, single_walk=False,
     _check(oracle().orc_domino_walk_weighted(a.ctypes.data, n, st.ctypes.data, se.ctypes.data, st.size,
                                              int(single_walk), int(fast), chain, p, np_, h.shape[0], h.ctypes.data,
                                              v.ctypes.data), "orc_domino_walk_weighted")
+    return a
+
+
+def lozenge_walk_weighted(t, steps, seeds, w0, w1, w2, fast=False, chain=0, params=None) -> np.ndarray:
+    """The uniform lozenge walk with periodic weights (orc_lozenge_walk_weighted);
+    steps / seeds are per epoch."""
+    a, n = _tiling(t)
+    st = np.ascontiguousarray(np.atleast_1d(steps), dtype=np.int64)
+    se = np.ascontiguousarray(np.atleast_1d(seeds), dtype=np.int64)
+    w = [np.ascontiguousarray(x, dtype=np.float64) for x in (w0, w1, w2)]
+    p, np_, keep = _table(params)
+    _check(oracle().orc_lozenge_walk_weighted(a.ctypes.data, n, st.ctypes.data, se.ctypes.data, st.size, int(fast),
+                                              chain, p, np_, w[0].shape[0], *(x.ctypes.data for x in w)),
+           "orc_lozenge_walk_weighted")
     return a
 
 
@@ -255,9 +271,12 @@ def cftp(tmax, tmin, first_steps: int, master_seed: int, schedule: str = "doubli
     Examples/AztecDiamondCftpEx.cpp:42-68 (seeds: successive mt19937 outputs,
     newest epoch first; in fast mode each seed is its epoch's Philox key).
     model: "domino_cftp", "lozenge" or "qlozenge" (kw: q, qcmp_double);
-    weights: (wh, wv) periodic domino weights for "domino_cftp".
+    weights: (wh, wv) periodic domino weights for "domino_cftp", (w0, w1, w2)
+    periodic lozenge weights for "lozenge".
     Returns (tiling, trials, total_steps, coalesced)."""
     def run(t, steps, seeds):
+        if weights is not None and model == "lozenge":
+            return lozenge_walk_weighted(t, steps, seeds, *weights, fast=fast, **kw)
         if weights is not None:
             return domino_walk_weighted(t, steps, seeds, weights[0], weights[1], fast=fast, **kw)
         if planes:

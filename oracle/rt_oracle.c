@@ -491,7 +491,24 @@ int orc_domino_walk_planes(int32_t* t, int n, const int64_t* steps, const int64_
 
 /* RotateTiles, lozengekernel.cl:3-34 (uniform) and qlozengekernel.cl:5-32
  * (q-weighted).  Work item (i, j) owns stream j + (N/3) i. */
-static void lozenge_rotate(void* arr, int isint, int n, orc_draws* rng, int qmode, double q, int qcmp) {
+/* Periodic lozenge weights (no reference counterpart): a lozenge weighs the
+ * table entry of the lattice edge it covers, named by its lower end (i, j):
+ * w[0] the edge to (i, j+1), w[1] to (i-1, j+1), w[2] to (i-1, j). */
+typedef struct {
+    int period;
+    const double* w[3];
+} orc_lweights;
+
+/* Probability of state 38 (the cube) at vertex (i, j): W38 / (W25 + W38). */
+static double lozenge_p38(const orc_lweights* lw, int i, int j) {
+    const int P = lw->period;
+    const double w25 = weight_at(lw->w[2], P, i, j) * weight_at(lw->w[0], P, i, j) * weight_at(lw->w[1], P, i + 1, j - 1);
+    const double w38 = weight_at(lw->w[1], P, i, j) * weight_at(lw->w[0], P, i, j - 1) * weight_at(lw->w[2], P, i + 1, j);
+    return w38 / (w25 + w38);
+}
+
+static void lozenge_rotate(void* arr, int isint, int n, orc_draws* rng, int qmode, double q, int qcmp,
+                           const orc_lweights* lw, int colour) {
     const int m = n / 3;
     const float qf = (float)q;
     const float qinvf = 1.0f / qf;
@@ -501,7 +518,15 @@ static void lozenge_rotate(void* arr, int isint, int n, orc_draws* rng, int qmod
             const int64_t at = (int64_t)i * m + j;
             const int v = isint ? ((int32_t*)arr)[at] : ((int8_t*)arr)[at];
             int nv = v;
-            if (qmode == 2) {
+            if (lw) {
+                /* array column j of this colour is vertex column 3j + (colour + i) mod 3 */
+                const double add = 0.8 * lozenge_p38(lw, i, 3 * j + (colour + i) % 3);
+                if ((double)rd < add) {
+                    if (v == 25) nv = 38;
+                } else if ((double)rd < 0.8) {
+                    if (v == 38) nv = 25;
+                }
+            } else if (qmode == 2) {
                 /* volume weight q in the int8 fast rule of the batched chains: add below 0.4 q */
                 if ((double)rd < 0.4 * q) {
                     if (v == 25) nv = 38;
@@ -577,7 +602,8 @@ static void lozenge_update(const void* fv, void* av, void* bv, int isint, int n,
  * epoch e restarts the colour engine and the draws from seeds[e].  The
  * reference's single Walk (LozengeTiler.cpp:18-88) is the one-epoch case. */
 static int lozenge_run(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k, const uint32_t* params,
-                       int64_t nparams, int qmode, double q, int qcmp, int fast, uint32_t chain) {
+                       int64_t nparams, int qmode, double q, int qcmp, int fast, uint32_t chain,
+                       const orc_lweights* lw) {
     if (n < 3 || n % 3 || k < 0) return ORC_EINVAL;
     const int m = n / 3;
     const int isint = qmode == 1; /* lozengekernel.cl stores char, qlozengekernel.cl int */
@@ -610,7 +636,7 @@ static int lozenge_run(int32_t* t, int n, const int64_t* steps, const int64_t* s
             if (fast == 2)
                 lozenge_rotate_planes((int8_t*)arr[r], n, &rng);
             else
-                lozenge_rotate(arr[r], isint, n, &rng, qmode, q, qcmp);
+                lozenge_rotate(arr[r], isint, n, &rng, qmode, q, qcmp, lw, r);
             lozenge_update(arr[r], arr[(r + 1) % 3], arr[(r + 2) % 3], isint, n, r);
             draws_next(&rng);
         }
@@ -629,21 +655,29 @@ static int lozenge_run(int32_t* t, int n, const int64_t* steps, const int64_t* s
 
 int orc_lozenge_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
                      int qmode, double q, int qcmp) {
-    return lozenge_run(t, n, &steps, &seed, 1, params, nparams, qmode, q, qcmp, 0, 0);
+    return lozenge_run(t, n, &steps, &seed, 1, params, nparams, qmode, q, qcmp, 0, 0, NULL);
 }
 
 int orc_lozenge_walk_epochs(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k,
                             const uint32_t* params, int64_t nparams, int qmode, double q, int qcmp) {
-    return lozenge_run(t, n, steps, seeds, k, params, nparams, qmode, q, qcmp, 0, 0);
+    return lozenge_run(t, n, steps, seeds, k, params, nparams, qmode, q, qcmp, 0, 0, NULL);
 }
 
 int orc_lozenge_walk_fast(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain,
                           int qmode, double q, int qcmp) {
-    return lozenge_run(t, n, steps, keys, k, NULL, 0, qmode, q, qcmp, 1, chain);
+    return lozenge_run(t, n, steps, keys, k, NULL, 0, qmode, q, qcmp, 1, chain, NULL);
 }
 
 int orc_lozenge_walk_planes(int32_t* t, int n, const int64_t* steps, const int64_t* keys, int k, uint32_t chain) {
-    return lozenge_run(t, n, steps, keys, k, NULL, 0, 0, 1.0, 0, 2, chain);
+    return lozenge_run(t, n, steps, keys, k, NULL, 0, 0, 1.0, 0, 2, chain, NULL);
+}
+
+int orc_lozenge_walk_weighted(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k, int fast,
+                              uint32_t chain, const uint32_t* params, int64_t nparams, int period, const double* w0,
+                              const double* w1, const double* w2) {
+    if (k < 0 || (period != 1 && period != 2 && period != 4) || !w0 || !w1 || !w2) return ORC_EINVAL;
+    const orc_lweights lw = {period, {w0, w1, w2}};
+    return lozenge_run(t, n, steps, seeds, k, params, nparams, 0, 1.0, 0, fast ? 1 : 0, chain, &lw);
 }
 
 /* ------------------------------------------------------------------------ */

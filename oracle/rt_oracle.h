@@ -71,6 +71,14 @@ int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint
  * and the TinyMT streams from seeds[e], as the domino epoch Walk does). */
 int orc_lozenge_walk_epochs(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k,
                             const uint32_t* params, int64_t nparams, int qmode, double q, int qcmp);
+/* Weighted lozenges (no reference counterpart; rt_set_lozenge_weights): the
+ * uniform rule with the add threshold 0.4 replaced at vertex (i, j) by
+ * 0.8 W38 / (W25 + W38) from period x period tables w0, w1, w2 of the
+ * lozenges covering the edge from (i, j) to (i, j+1), (i-1, j+1), (i-1, j);
+ * fast = 0 TinyMT (epochs as orc_lozenge_walk_epochs), 1 Philox. */
+int orc_lozenge_walk_weighted(int32_t* t, int n, const int64_t* steps, const int64_t* seeds, int k, int fast,
+                              uint32_t chain, const uint32_t* params, int64_t nparams, int period, const double* w0,
+                              const double* w1, const double* w2);
 
 /* ---- fast mode (no reference counterpart) ----
  * Counter-based draws: Philox4x32-10 keyed by the epoch key, counter =

@@ -96,6 +96,7 @@ SIGNATURES = {
     "rt_load_rng_params": (ctypes.c_int, [_P, ctypes.c_char_p, _I64]),
     "rt_set_rng_params": (ctypes.c_int, [_P, _P, _I64]),
     "rt_set_domino_weights": (ctypes.c_int, [_P, _I32, _P, _P]),
+    "rt_set_lozenge_weights": (ctypes.c_int, [_P, _I32, _P, _P, _P]),
     "rt_walk": (ctypes.c_int, [_P, _P, _I32, _I64, _I64]),
     "rt_walk_epochs": (ctypes.c_int, [_P, _P, _I32, _P, _P, _I32]),
     "rt_cftp": (ctypes.c_int, [_P, _P, _P, _I32, _I64, _I32, _I64, _I32, _P, ctypes.POINTER(RtCftpStats)]),

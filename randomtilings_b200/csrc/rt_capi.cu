@@ -372,6 +372,31 @@ rt_status rt_set_domino_weights(rt_tiler* h, int32_t period, const double* wh, c
     return RT_OK;
 }
 
+rt_status rt_set_lozenge_weights(rt_tiler* h, int32_t period, const double* w0, const double* w1, const double* w2) {
+    if (!h) return RT_E_INVAL;
+    if (h->family != FAM_LOZENGE8) return h->fail(RT_E_INVAL, "weights need the uniform lozenge kernel (char storage)");
+    if (h->cfg.rng == RT_RNG_PLANES) return h->fail(RT_E_INVAL, "the bit-plane mode draws one bit per site: no weights");
+    if (period == 0) {
+        h->wper = 0;
+        return RT_OK;
+    }
+    if ((period != 1 && period != 2 && period != 4) || !w0 || !w1 || !w2)
+        return h->fail(RT_E_INVAL, "weight period must be 1, 2 or 4, with three period x period tables");
+    const int P = period;
+    for (int k = 0; k < P * P; ++k)
+        for (const double* w : {w0, w1, w2})
+            if (!(w[k] > 0) || !std::isfinite(w[k])) return h->fail(RT_E_INVAL, "lozenge weights must be finite and > 0");
+    auto W = [&](const double* w, int r, int c) { return w[(((r % P) + P) % P) * P + (((c % P) + P) % P)]; };
+    for (int i = 0; i < P; ++i)
+        for (int j = 0; j < P; ++j) {
+            const double w25 = W(w2, i, j) * W(w0, i, j) * W(w1, i + 1, j - 1);
+            const double w38 = W(w1, i, j) * W(w0, i, j - 1) * W(w2, i + 1, j);
+            h->wthr[i * P + j] = below_threshold(0.8 * (w38 / (w25 + w38)));
+        }
+    h->wper = P;
+    return RT_OK;
+}
+
 rt_status rt_set_rng_params(rt_tiler* h, const uint32_t* table, int64_t n) {
     if (!h || (!table && n > 0) || n < 0) return h ? h->fail(RT_E_INVAL, "bad parameter table") : RT_E_INVAL;
     h->table.assign(table, table + 3 * n);

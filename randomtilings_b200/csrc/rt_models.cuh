@@ -50,12 +50,14 @@ struct WalkArgs {
     int64_t drop_phase;   // tests of the bounded waits: CTA 0 does not publish this phase's rows (-1: none)
     int depth;            // bit-plane kernel: phases per halo exchange
     int pwords;           // bit-plane kernel: 32-bit words per colour-array row
-    int wper;             // domino heat bath with periodic weights: period P (1, 2 or 4), 0 = unweighted
-    uint32_t wthr[16];    // ... its threshold at vertex (i, j): wthr[(i mod P) P + (j mod P)]
+    int wper;             // periodic weights (domino heat bath, uniform lozenges): period P (1, 2, 4), 0 = none
+    uint32_t wthr[16];    // ... the vertex's threshold at (i, j): wthr[(i mod P) P + (j mod P)]
 };
 
-// Threshold of the weighted domino heat bath at vertex (i, j).
-__device__ __forceinline__ uint32_t domino_weight_thr(const WalkArgs& a, int i, int j) {
+// Threshold of a weighted rule at vertex (i, j): dominoes, the heat bath's
+// draw below which the site becomes 12; lozenges, the draw below which a
+// cube is added (removal stays below thr[1]).
+__device__ __forceinline__ uint32_t weight_thr(const WalkArgs& a, int i, int j) {
     const int m = a.wper - 1;
     return a.wthr[(i & m) * a.wper + (j & m)];
 }
@@ -132,7 +134,7 @@ struct DominoRule {
         if (x.step) {
             const int v = x.upd ? refreshed(x, off, i) : (int)x.dst[off];
             // weighted heat bath: array column j is vertex column 2 j + ((i + arr) & 1)
-            const uint32_t thr = HEAT_BATH && a.wper ? domino_weight_thr(a, i, 2 * j + ((i + x.arr) & 1)) : x.thr;
+            const uint32_t thr = HEAT_BATH && a.wper ? weight_thr(a, i, 2 * j + ((i + x.arr) & 1)) : x.thr;
             x.dst[off] = (int8_t)flip(v, k, thr);
         } else {
             x.dst[off] = (int8_t)refreshed(x, off, i);
@@ -164,12 +166,14 @@ struct ThreeColour {
         bool step, upd, keep_a;
         uint32_t shifts;
         int w, imax, jmax;
+        int col;     // colour flipped (STEP)
     };
     __device__ static uint32_t written(uint32_t d) { return ph_op(d) == OP_STEP ? 1u << flipped((int)ph_a(d)) : 0u; }
     __device__ static Ctx ctx(const WalkArgs& a, T* planes, int plane, uint32_t d, int) {
         const int op = (int)ph_op(d), ca = (int)ph_a(d), cb = (int)ph_b(d);
         Ctx x;
         x.step = op == (int)OP_STEP;
+        x.col = ca;
         x.w = a.wpad;
         x.imax = a.n - 2;
         x.jmax = a.n / 3 - 2;
@@ -201,7 +205,13 @@ struct ThreeColour {
             } else {
                 v = (int)x.cur[off];
             }
-            x.cur[off] = (T)Rule::flip(v, k, a);
+            if constexpr (Rule::kSiteWeights) {
+                // weighted lozenges: array column j of colour c is vertex column 3 j + (c + i) mod 3
+                const uint32_t t0 = a.wper ? weight_thr(a, i, 3 * j + (x.col + i) % 3) : a.thr[0];
+                x.cur[off] = (T)Rule::flip_w(v, k, t0, a.thr[1]);
+            } else {
+                x.cur[off] = (T)Rule::flip(v, k, a);
+            }
         } else if (interior) {
             int na, nb;
             Rule::refresh(x.f, off, x.w, (x.shifts >> (3 * (i % 3))) & 7u, (int)x.pa[off], (int)x.pb[off], na, nb);
@@ -215,6 +225,7 @@ struct ThreeColour {
 // Flippable vertices: 25 = 1+8+16 (no cube) and 38 = 2+4+32 (cube).
 template <bool QWEIGHT>
 struct LozengeRule {
+    static constexpr bool kSiteWeights = !QWEIGHT;  // periodic weights on the uniform (char) kernel
     // UpdateTiles (lozengekernel.cl:36-54): colour t+1 refreshes bits {2,4,32},
     // colour t+2 bits {1,8,16}.  Per row class i mod 3: bit 0 = shift of the
     // upper-right / lower-left reads, bit 1 = of the left read, bit 2 = of
@@ -250,11 +261,19 @@ struct LozengeRule {
         if (k < (1u << 22)) return (v == 25 && k <= a.thr[0]) ? 38 : v;
         return (v == 38 && (k - (1u << 22)) <= a.thr[1]) ? 25 : v;
     }
+    // The uniform rule with the add threshold of the site: k < t0 adds a
+    // cube, t0 <= k < t1 removes one.
+    __device__ static int flip_w(int v, uint32_t k, uint32_t t0, uint32_t t1) {
+        if (k < t0) return v == 25 ? 38 : v;
+        if (k < t1) return v == 38 ? 25 : v;
+        return v;
+    }
 };
 
 // Rectangle-triangle (src/RectTriangle/RectTriangleTiler.cpp:17-92;
 // recttrianglekernel.cl).  A site holds six hex face digits.
 struct RectTriRule {
+    static constexpr bool kSiteWeights = false;
     __device__ static int digit(int x, int k) { return (int)(((unsigned)x >> (4 * k)) & 0xfu); }
     // updateTiles1 / updateTiles2 (recttrianglekernel.cl:120-146).  Per row
     // class: bit 0 = shift of the side read of colour t+1 (s1), bit 1 = of

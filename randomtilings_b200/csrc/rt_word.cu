@@ -163,7 +163,14 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
                     const int i = a0 + wi.off / W - 1, c0 = wi.off % W, par = (i + 1 - (int)ph_a(d)) & 1;
 #pragma unroll
                     for (int b = 0; b < 4; ++b)
-                        m0 |= (uint32_t)(k[b] < domino_weight_thr(a, i, 2 * (c0 + b) + par)) << (8 * b);
+                        m0 |= (uint32_t)(k[b] < weight_thr(a, i, 2 * (c0 + b) + par)) << (8 * b);
+                } else if (FAM == FAM_LOZENGE8 && a.wper) {
+                    // weighted lozenges: the add threshold of each site's vertex; array
+                    // column c of colour C is vertex column 3 c + (C + i) mod 3
+                    const int i = a0 + wi.off / W - 1, c0 = wi.off % W, rem = ((int)ph_a(d) + i) % 3;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        m0 |= (uint32_t)(k[b] < weight_thr(a, i, 3 * (c0 + b) + rem)) << (8 * b);
                 } else {
                     m0 = below4(k, a.thr[0]);
                 }

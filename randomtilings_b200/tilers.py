@@ -223,6 +223,19 @@ class LozengeTiler(_Tiler):
     TilingToSVG = staticmethod(lambda t, f: builders.write("rt_lozenge_tiling_svg", f, t))
     PrintDomain = staticmethod(lambda d, f: builders.write("rt_lozenge_print_domain", f, d))
 
+    def SetWeights(self, w0=None, w1=None, w2=None) -> None:
+        """Periodic lozenge weights for the uniform kernel (rt_set_lozenge_weights):
+        P x P tables (P = 1, 2 or 4) for the lozenges covering the edge from
+        (i, j) to (i, j+1), (i-1, j+1) and (i-1, j), indexed by (i mod P, j mod P);
+        None returns to uniform weights."""
+        if w0 is None:
+            self._check(_capi.load().rt_set_lozenge_weights(self._h, 0, None, None, None))
+            return
+        t = [np.ascontiguousarray(w, dtype=np.float64) for w in (w0, w1, w2)]
+        if t[0].ndim != 2 or t[0].shape[0] != t[0].shape[1] or any(w.shape != t[0].shape for w in t):
+            raise ValueError("w0, w1 and w2 must be P x P tables of the same shape")
+        self._check(_capi.load().rt_set_lozenge_weights(self._h, t[0].shape[0], *(w.ctypes.data for w in t)))
+
     @staticmethod
     def DimerToSVG(t, *args):
         d, f = (None, args[0]) if len(args) == 1 else args

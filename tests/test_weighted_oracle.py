@@ -89,3 +89,48 @@ def test_two_periodic_weights():
     assert odd == {round(a * a / (a * a + b * b), 12), round(b * b / (a * a + b * b), 12)}
     u, v = rt.DominoTiler.TwoPeriodicWeights(0.7, 0.7)
     assert np.all(u == 0.7) and np.all(v == 0.7)
+
+
+# ---- lozenges ----
+LW = (np.array([[1.0, 0.4], [1.6, 0.8]]), np.array([[0.5, 1.2], [2.0, 1.0]]), np.array([[1.5, 0.7], [0.9, 1.1]]))
+
+
+def lozenge_tiling_weight(t, w0, w1, w2):
+    """Product of the lozenge weights: each lozenge once, at the lower end
+    (i, j) of the edge it covers: bit 8 (edge to (i, j+1)) -> w0, bit 2 (to
+    (i-1, j+1)) -> w1, bit 1 (to (i-1, j)) -> w2."""
+    t = np.asarray(t).reshape(-1)
+    n = int(round(t.size ** 0.5))
+    p = w0.shape[0]
+    w = 1.0
+    for i in range(n):
+        for j in range(n):
+            v = int(t[i * n + j])
+            for bit, table in ((8, w0), (2, w1), (1, w2)):
+                if v & bit:
+                    w *= table[i % p, j % p]
+    return w
+
+
+@pytest.mark.parametrize("period", [1, 2, 4])
+def test_equal_lozenge_weights_are_the_reference_rule(period):
+    t = golden("builders")["lozenge/hex10_2/max"]
+    one = np.full((period, period), 0.9)
+    assert np.array_equal(po.lozenge_walk_weighted(t, [300, 200], [5, 9], one, one, one),
+                          po.lozenge_walk_epochs(t, [300, 200], [5, 9]))
+    assert np.array_equal(po.lozenge_walk_weighted(t, [500], [5 + 2**40], one, one, one, fast=True),
+                          po.walk_fast("lozenge", t, [500], [5 + 2**40]))
+
+
+def test_lozenge_stationary_law_is_the_weighted_one():
+    import randomtilings_b200 as rt
+
+    t0 = np.asarray(rt.LozengeTiler.MinTiling(rt.LozengeTiler.Hexagon(2, 2, 2)))
+    ends = [po.lozenge_walk_weighted(t0, [300], [key], *LW, fast=True) for key in range(4000)]
+    c = Counter(e.tobytes() for e in ends)
+    assert len(c) == 20  # plane partitions in a 2 x 2 x 2 box
+    keys = sorted(c)
+    w = np.array([lozenge_tiling_weight(np.frombuffer(k, dtype=np.int32), *LW) for k in keys])
+    obs = np.array([c[k] for k in keys], dtype=float)
+    assert stats.chisquare(obs, obs.sum() * w / w.sum()).pvalue > 1e-4
+    assert stats.chisquare(obs).pvalue < 1e-6
