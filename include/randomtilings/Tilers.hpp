@@ -188,6 +188,17 @@ public:
     explicit LozengeTiler(int device = 0, bool qweight = false)
         : TilerBase(RT_LOZENGE, device, qweight ? RT_KERNEL_QWEIGHT : RT_KERNEL_DEFAULT) {}
     explicit LozengeTiler(const rt_config& cfg) : TilerBase(cfg) {}
+    // Periodic lozenge weights for the uniform kernel (rt_set_lozenge_weights):
+    // P x P row-major tables w0, w1, w2, P = 1, 2 or 4; P = 0 returns to uniform.
+    void SetWeights(int P, const std::vector<double>& w0, const std::vector<double>& w1,
+                    const std::vector<double>& w2) {
+        const size_t nn = (size_t)(P * P);
+        if (P != 0 && (w0.size() != nn || w1.size() != nn || w2.size() != nn))
+            throw Error(RT_E_INVAL, "weight tables must hold P x P values");
+        detail::check(rt_set_lozenge_weights(h_, P, P ? w0.data() : nullptr, P ? w1.data() : nullptr,
+                                             P ? w2.data() : nullptr),
+                      h_);
+    }
     static domain AlmostHexDomain(int N, int M) {
         return detail::build([&](int32_t* o, int64_t c, int64_t* l) { return rt_lozenge_almost_hex(N, M, o, c, l); });
     }

@@ -31,9 +31,14 @@ int main(int argc, char** argv) {
         rt::tiling m = rt::DominoTiler::MinTiling(a);
         save(f, "aztec_min", m);
         if (walk) {
+            rt::tiling t2 = t;
             rt::LozengeTiler L(0);
             L.Walk(t, 1000, 42);
             save(f, "lozenge_walk", t);
+            rt::LozengeTiler LW(0);
+            LW.SetWeights(2, {1.0, 0.4, 1.6, 0.8}, {0.5, 1.2, 2.0, 1.0}, {1.5, 0.7, 0.9, 1.1});
+            LW.Walk(t2, 1000, 42);
+            save(f, "lozenge_weighted", t2);
             rt::DominoTiler D(0, /*cftp=*/true);
             std::vector<long> steps{256, 128}, seeds{2718281, 345903};
             rt::tiling m2 = m;

@@ -54,6 +54,8 @@ def test_cpp_layer_walks(tmp_path):
     subprocess.run([exe, "walk", out], check=True)
     got, b = _read(out), golden("builders")
     assert np.array_equal(got["lozenge_walk"], po.lozenge_walk(b["lozenge/hex10_2/max"], 1000, 42))
+    lw = (np.array([[1.0, 0.4], [1.6, 0.8]]), np.array([[0.5, 1.2], [2.0, 1.0]]), np.array([[1.5, 0.7], [0.9, 1.1]]))
+    assert np.array_equal(got["lozenge_weighted"], po.lozenge_walk_weighted(b["lozenge/hex10_2/max"], [1000], [42], *lw))
     assert np.array_equal(got["cone_walk"], po.tridimer_walk(b["tridimer/cone10_3/tiling"], 800, 9))
     assert np.array_equal(got["aztec_epochs"],
                           po.domino_walk_epochs(got["aztec_min"], [256, 128], [2718281, 345903], cftp=True))
