@@ -199,6 +199,7 @@ struct rt_tiler {
     WalkPlan plan;
     int plan_rows = -1, plan_cols = -1, plan_nlat = -1;
     bool plan_uniform = true;
+    bool plan_weighted = false;
     int kernel_choice = 0;  // 0 auto, 1 generic walk kernel only, 2 word kernel only (RT_WALK_KERNEL)
     int ctas_hint = 0;      // word kernel grid (RT_WALK_CTAS; 0 = one CTA per SM)
     int depth_hint = 0;     // bit-plane kernel: phases per halo exchange (RT_PLANE_DEPTH; 0 = up to 8)
@@ -650,7 +651,9 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
 
     const int width = h->width;
     const bool uniform = fast || h->table.empty();
-    if (h->plan_rows != h->rows || h->plan_cols != h->cols || h->plan_nlat != h->nlat || h->plan_uniform != uniform) {
+    const bool weighted = h->wper > 0;
+    if (h->plan_rows != h->rows || h->plan_cols != h->cols || h->plan_nlat != h->nlat || h->plan_uniform != uniform ||
+        h->plan_weighted != weighted) {
         // The word kernel serves the int8 models with uniform generator
         // parameters; everything else (and any band it cannot hold) runs on
         // the generic walk kernel.  Bit-plane mode has its own kernel.
@@ -661,7 +664,7 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
             if (s != RT_OK) return s;
         } else if (h->kernel_choice != 1 && uniform && word_family(h->family))
             s = plan_word_walk(h->family, h->cfg.device, h->nlat, h->rows, width, fast, h->ctas_hint, &h->plan,
-                               &h->err);
+                               &h->err, weighted);
         if (s != RT_OK && h->kernel_choice == 2) return s;
         if (s != RT_OK)
             s = plan_walk(h->family, h->cfg.device, h->nlat, h->rows, h->cols, width, uniform, fast, &h->plan, &h->err);
@@ -670,6 +673,7 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
         h->plan_cols = h->cols;
         h->plan_nlat = h->nlat;
         h->plan_uniform = uniform;
+        h->plan_weighted = weighted;
     }
     const int64_t ids = (int64_t)h->rows * h->cols;
     rt_status s = fast ? RT_OK : stage_params(h, ids);

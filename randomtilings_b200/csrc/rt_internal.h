@@ -41,8 +41,9 @@ rt_status launch_walk(const WalkPlan& plan, WalkArgs& args, cudaStream_t stream,
 // Word-parallel kernel of the int8 models (rt_word.cu): uniform TinyMT32J
 // parameters or fast mode.  ctas_hint <= 0: one CTA per SM.
 bool word_family(int family);
+// weighted: the instantiation that reads per-site thresholds (WalkArgs::wper > 0).
 rt_status plan_word_walk(int family, int device, int nlat, int rows, int width, bool philox, int ctas_hint,
-                         WalkPlan* plan, std::string* err);
+                         WalkPlan* plan, std::string* err, bool weighted = false);
 // Bit-plane kernel of the int8 models (rt_plane.cu, RT_RNG_PLANES).
 // ctas_hint / depth_hint <= 0: one CTA per SM / the largest depth up to 8.
 rt_status plan_plane_walk(int family, int device, int nlat, int rows, int width, int ctas_hint, int depth_hint,

@@ -29,7 +29,9 @@ constexpr int kWordBlockMax = 512;
 // (band rows + 2 halo rows) x wpad bytes, then 16 bytes of slack (the funnel
 // shifts read one word beyond a row; those bytes only reach sites outside
 // the update / flip masks).
-template <int FAM, int MAXW, bool PHILOX, int LB>
+// WT: periodic weights (a.wper > 0) -- a per-site threshold instead of thr[0];
+// a separate instantiation, so that the unweighted kernel carries none of it.
+template <int FAM, int MAXW, bool PHILOX, int LB, bool WT>
 __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ WalkArgs a) {
     using M = WordModel<FAM>;
     constexpr int NC = M::NC;
@@ -157,14 +159,14 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
         auto apply = [&](const WordInfo& wi, const uint32_t (&k)[4]) {
             uint32_t m0 = 0, m1 = 0;
             if (draws) {
-                if (FAM == FAM_DOMINO_HB && a.wper) {
+                if (WT && FAM == FAM_DOMINO_HB) {
                     // weighted heat bath: a threshold per site from its vertex (i, j);
                     // array column c of the rotated array A is vertex column 2 c + ((i + A) & 1)
                     const int i = a0 + wi.off / W - 1, c0 = wi.off % W, par = (i + 1 - (int)ph_a(d)) & 1;
 #pragma unroll
                     for (int b = 0; b < 4; ++b)
                         m0 |= (uint32_t)(k[b] < weight_thr(a, i, 2 * (c0 + b) + par)) << (8 * b);
-                } else if (FAM == FAM_LOZENGE8 && a.wper) {
+                } else if (WT && FAM == FAM_LOZENGE8) {
                     // weighted lozenges: the add threshold of each site's vertex; array
                     // column c of colour C is vertex column 3 c + (C + i) mod 3
                     const int i = a0 + wi.off / W - 1, c0 = wi.off % W, rem = ((int)ph_a(d) + i) % 3;
@@ -308,30 +310,32 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
 
 using KernelFn = void (*)(WalkArgs);
 
-template <int FAM>
+template <int FAM, bool WT>
 static KernelFn word_fn(int maxw, bool philox) {
     if (philox) {
         switch (maxw) {
-            case 0: return word_kernel<FAM, 0, true, 1024>;
-            case 1: return word_kernel<FAM, 1, true, 1024>;
-            case 2: return word_kernel<FAM, 2, true, 1024>;
-            case 4: return word_kernel<FAM, 4, true, 1024>;
+            case 0: return word_kernel<FAM, 0, true, 1024, WT>;
+            case 1: return word_kernel<FAM, 1, true, 1024, WT>;
+            case 2: return word_kernel<FAM, 2, true, 1024, WT>;
+            case 4: return word_kernel<FAM, 4, true, 1024, WT>;
             default: return nullptr;
         }
     }
     switch (maxw) {
-        case 1: return word_kernel<FAM, 1, false, 1024>;
-        case 2: return word_kernel<FAM, 2, false, 512>;
-        case 4: return word_kernel<FAM, 4, false, 512>;
+        case 1: return word_kernel<FAM, 1, false, 1024, WT>;
+        case 2: return word_kernel<FAM, 2, false, 512, WT>;
+        case 4: return word_kernel<FAM, 4, false, 512, WT>;
         default: return nullptr;
     }
 }
 
-static KernelFn word_kernel_for(int family, int maxw, bool philox) {
+static KernelFn word_kernel_for(int family, int maxw, bool philox, bool weighted) {
     switch (family) {
-        case FAM_DOMINO: return word_fn<FAM_DOMINO>(maxw, philox);
-        case FAM_DOMINO_HB: return word_fn<FAM_DOMINO_HB>(maxw, philox);
-        case FAM_LOZENGE8: return word_fn<FAM_LOZENGE8>(maxw, philox);
+        case FAM_DOMINO: return word_fn<FAM_DOMINO, false>(maxw, philox);
+        case FAM_DOMINO_HB:
+            return weighted ? word_fn<FAM_DOMINO_HB, true>(maxw, philox) : word_fn<FAM_DOMINO_HB, false>(maxw, philox);
+        case FAM_LOZENGE8:
+            return weighted ? word_fn<FAM_LOZENGE8, true>(maxw, philox) : word_fn<FAM_LOZENGE8, false>(maxw, philox);
         default: return nullptr;
     }
 }
@@ -339,7 +343,7 @@ static KernelFn word_kernel_for(int family, int maxw, bool philox) {
 bool word_family(int family) { return family == FAM_DOMINO || family == FAM_DOMINO_HB || family == FAM_LOZENGE8; }
 
 rt_status plan_word_walk(int family, int device, int nlat, int rows, int width, bool philox, int ctas_hint,
-                         WalkPlan* plan, std::string* err) {
+                         WalkPlan* plan, std::string* err, bool weighted) {
     if (!word_family(family)) {
         *err = "no word kernel for this model";
         return RT_E_INVAL;
@@ -381,7 +385,7 @@ rt_status plan_word_walk(int family, int device, int nlat, int rows, int width, 
         *err = "band does not fit in shared memory";
         return RT_E_INVAL;
     }
-    KernelFn fn = word_kernel_for(family, maxw, philox);
+    KernelFn fn = word_kernel_for(family, maxw, philox, weighted);
     if (!fn) {
         *err = "no word kernel for this configuration";
         return RT_E_INVAL;
