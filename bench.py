@@ -459,8 +459,11 @@ def run_cftp(args) -> None:
 def run_extremal(args) -> None:
     """Set-up of a large domain: MinTiling, MaxTiling and the TilingToHeightfunc
     of both, on the host (the reference's flood) and on the device
-    (rt_extremal_tilings), on an Aztec diamond of order args.extremal_order
-    and an a=b=c hexagon of side args.extremal_side; results compared."""
+    (rt_extremal_tilings into host arrays; rt_extremal_tilings_device into
+    device buffers), on an Aztec diamond of order args.extremal_order and an
+    a=b=c hexagon of side args.extremal_side; results compared.  The
+    device-buffer leg runs after every host-output leg (its torch buffers stay
+    cached in the process)."""
     import numpy as np
 
     import randomtilings_b200 as rt
@@ -469,7 +472,7 @@ def run_extremal(args) -> None:
     if int(os.environ.get("RANK", "0")) != 0:
         return
     builders.extremal_tilings(rt.RT_DOMINO, rt.DominoTiler.AztecDiamond(4))  # context and module load
-    out = []
+    out, kept = [], []
     for model, cls, d, name in (
             (rt.RT_DOMINO, rt.DominoTiler, rt.DominoTiler.AztecDiamond(args.extremal_order),
              f"Aztec diamond n={args.extremal_order}"),
@@ -493,7 +496,21 @@ def run_extremal(args) -> None:
                     "phases_ms": phases, "device_ms": round(st["device_ms"], 3),
                     "passes": st["passes"], "tile_updates": st["tile_updates"], "boundary": st["boundary"],
                     "speedup_call": round(host_s / statistics.median(walls), 1)})
-        print(json.dumps(out[-1]), file=sys.stderr, flush=True)
+        kept.append((model, d, dev))
+    # the same into device buffers (rt_extremal_tilings_device): no copies back
+    import torch
+
+    for r, (model, d, dev) in zip(out, kept):
+        bufs = {k: torch.empty(dev[k].size, dtype=torch.int32, device="cuda:0") for k in dev}
+        dwalls = []
+        for _ in range(args.steps):
+            a = time.perf_counter()
+            builders.extremal_tilings_device(model, d, **{k: v.data_ptr() for k, v in bufs.items()})
+            dwalls.append(time.perf_counter() - a)
+        r["equal_to_host"] = r["equal_to_host"] and all(np.array_equal(bufs[k].cpu().numpy(), dev[k]) for k in dev)
+        r["device_outputs_call_s"] = round(statistics.median(dwalls), 4)
+        r["speedup_device_outputs"] = round(r["host_s"] / statistics.median(dwalls), 1)
+        print(json.dumps(r), file=sys.stderr, flush=True)
     print(json.dumps({"metric": "extremal tilings + heights set-up time (host flood vs device relaxation)",
                       "unit": "s", "higher_is_better": False, "runs": out}), flush=True)
 

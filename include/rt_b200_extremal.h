@@ -54,6 +54,16 @@ typedef struct {
 rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_t dlen, int32_t device, int32_t* tmin,
                               int32_t* tmax, int32_t* hmin, int32_t* hmax, int64_t len, rt_extremal_stats* stats);
 
+/* The same results written into the caller's device buffers (each NULL or
+ * n*n int32 of device memory on `device`, which also serve as the working
+ * arrays): no copy back to the host, for callers that go on on the GPU
+ * (e.g. rt_walk_device_noalloc from d_tmin).  Outputs that are not device
+ * memory of `device` are rejected with RT_E_INVAL before anything runs.
+ * Synchronous; the stats' download_ms is then only the final wait. */
+rt_status rt_extremal_tilings_device(int32_t model, const int32_t* d, int64_t dlen, int32_t device, int32_t* d_tmin,
+                                     int32_t* d_tmax, int32_t* d_hmin, int32_t* d_hmax, int64_t len,
+                                     rt_extremal_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -203,6 +203,8 @@ class RtExtremalStats(ctypes.Structure):
 # include/rt_b200_extremal.h
 SIGNATURES["rt_extremal_tilings"] = (ctypes.c_int, [_I32, _P, _I64, _I32, _P, _P, _P, _P, _I64,
                                                     ctypes.POINTER(RtExtremalStats)])
+SIGNATURES["rt_extremal_tilings_device"] = (ctypes.c_int, [_I32, _P, _I64, _I32, _P, _P, _P, _P, _I64,
+                                                           ctypes.POINTER(RtExtremalStats)])
 
 # include/rt_b200_height.h
 SIGNATURES.update({

@@ -108,3 +108,16 @@ def load_matrix_binary(filename: str) -> np.ndarray:
     out = np.zeros(max(n.value, 1), dtype=np.int32)
     _capi.check(lib.rt_load_matrix_binary(str(filename).encode(), out.ctypes.data, out.size, ctypes.byref(n)))
     return out[: n.value]
+
+
+def extremal_tilings_device(model: int, domain, tmin=0, tmax=0, hmin=0, hmax=0, device: int = 0) -> dict:
+    """rt_extremal_tilings_device: the same arrays as extremal_tilings written
+    into caller-owned device buffers (device pointers as ints, 0 = not wanted,
+    each n*n int32 on `device`; e.g. torch tensors' data_ptr()).  Returns the stats."""
+    lib = _capi.load()
+    d = _arr(domain)
+    n = vertex_side(model, d.size)
+    st = _capi.RtExtremalStats()
+    _capi.check(lib.rt_extremal_tilings_device(model, d.ctypes.data, d.size, device, tmin or None, tmax or None,
+                                               hmin or None, hmax or None, n * n, ctypes.byref(st)))
+    return {k: getattr(st, k) for k, _ in _capi.RtExtremalStats._fields_}

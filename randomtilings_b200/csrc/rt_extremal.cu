@@ -368,9 +368,23 @@ struct Stream {
 
 using namespace rtb;
 
-extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_t dlen, int32_t device, int32_t* tmin,
-                                         int32_t* tmax, int32_t* hmin, int32_t* hmax, int64_t len,
-                                         rt_extremal_stats* stats) {
+namespace {
+
+// Device memory of `device` (or managed memory), the only kind the kernels may write.
+bool device_memory(const void* p, int device) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == device;
+}
+
+// Both entry points: outputs in host memory (copied back) or, with dev_out,
+// the caller's device buffers (the relaxation and the tilings are written
+// there directly).
+rt_status extremal_run(int32_t model, const int32_t* d, int64_t dlen, int32_t device, int32_t* tmin, int32_t* tmax,
+                       int32_t* hmin, int32_t* hmax, int64_t len, rt_extremal_stats* stats, bool dev_out) {
     if ((model != RT_DOMINO && model != RT_LOZENGE) || !d || dlen <= 0) return RT_E_INVAL;
     const bool dom = model == RT_DOMINO;
     using clk = std::chrono::steady_clock;
@@ -385,15 +399,21 @@ extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_
     const int64_t nn = (int64_t)n * n;
     if (len != nn) return RT_E_INVAL;
     if (cudaSetDevice(device) != cudaSuccess) return RT_E_NODEVICE;
+    if (dev_out)
+        for (const int32_t* o : {tmin, tmax, hmin, hmax})
+            if (o && !device_memory(o, device)) return RT_E_INVAL;
     const int tiles_x = (n + XC - 1) / XC, tiles_y = (n + XR - 1) / XR;
     const int64_t tiles = (int64_t)tiles_x * tiles_y;
     if (tiles > INT_MAX) return RT_E_INVAL;
     t0 = clk::now();
     DevBuf dd, dk, dx, dn, dtx, dtn, dbi, dbh, dflag, dcnt;
-    if (!dd.alloc((size_t)dlen * 4) || !dk.alloc((size_t)nn) || !dx.alloc((size_t)nn * 4) ||
-        !dn.alloc((size_t)nn * 4) || !dtx.alloc((size_t)nn * 4) || !dtn.alloc((size_t)nn * 4) ||
-        !dbi.alloc(bidx.size() * 8) || !dbh.alloc(bh.size() * 4) || !dflag.alloc((size_t)tiles * 2) ||
-        !dcnt.alloc((kGroup + 1) * 4))
+    // the caller's device buffers serve as the work arrays where given
+    const bool own_hx = !(dev_out && hmax), own_hn = !(dev_out && hmin), tilings = tmin || tmax;
+    const bool own_tx = tilings && !(dev_out && tmax), own_tn = tilings && !(dev_out && tmin);
+    if (!dd.alloc((size_t)dlen * 4) || !dk.alloc((size_t)nn) || (own_hx && !dx.alloc((size_t)nn * 4)) ||
+        (own_hn && !dn.alloc((size_t)nn * 4)) || (own_tx && !dtx.alloc((size_t)nn * 4)) ||
+        (own_tn && !dtn.alloc((size_t)nn * 4)) || !dbi.alloc(bidx.size() * 8) || !dbh.alloc(bh.size() * 4) ||
+        !dflag.alloc((size_t)tiles * 2) || !dcnt.alloc((kGroup + 1) * 4))
         return RT_E_NOMEM;
     Stream st;
     if (cudaStreamCreateWithFlags(&st.s, cudaStreamNonBlocking) != cudaSuccess ||
@@ -403,8 +423,8 @@ extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_
     const double alloc_ms = ms_since(t0);
     t0 = clk::now();
     auto* K = static_cast<uint8_t*>(dk.p);
-    auto* HX = static_cast<int32_t*>(dx.p);
-    auto* HN = static_cast<int32_t*>(dn.p);
+    auto* HX = own_hx ? static_cast<int32_t*>(dx.p) : hmax;
+    auto* HN = own_hn ? static_cast<int32_t*>(dn.p) : hmin;
     auto* F = static_cast<uint8_t*>(dflag.p);
     auto* C = static_cast<unsigned*>(dcnt.p);
     cudaMemcpyAsync(dd.p, d, (size_t)dlen * 4, cudaMemcpyHostToDevice, s);
@@ -454,9 +474,9 @@ extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_
     else
         ext_check<false><<<vb, T, 0, s>>>(K, HX, HN, n, C + kGroup);
     ext_finish<<<vb, T, 0, s>>>(K, HX, HN, nn);
-    auto* TX = static_cast<int32_t*>(dtx.p);
-    auto* TN = static_cast<int32_t*>(dtn.p);
-    if (tmin || tmax) {
+    auto* TX = own_tx ? static_cast<int32_t*>(dtx.p) : tmax;
+    auto* TN = own_tn ? static_cast<int32_t*>(dtn.p) : tmin;
+    if (tilings) {
         if (dom)
             ext_tiling<true><<<vb, T, 0, s>>>(D, m, HN, HX, TN, TX);
         else
@@ -468,10 +488,12 @@ extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_
     if (cudaStreamSynchronize(s) != cudaSuccess) return RT_E_CUDA;
     if (bad) return RT_E_INVAL;  // not tileable: the flood ran past a boundary height
     t0 = clk::now();
-    if (tmin) cudaMemcpyAsync(tmin, TN, (size_t)nn * 4, cudaMemcpyDeviceToHost, s);
-    if (tmax) cudaMemcpyAsync(tmax, TX, (size_t)nn * 4, cudaMemcpyDeviceToHost, s);
-    if (hmin) cudaMemcpyAsync(hmin, HN, (size_t)nn * 4, cudaMemcpyDeviceToHost, s);
-    if (hmax) cudaMemcpyAsync(hmax, HX, (size_t)nn * 4, cudaMemcpyDeviceToHost, s);
+    if (!dev_out) {
+        if (tmin) cudaMemcpyAsync(tmin, TN, (size_t)nn * 4, cudaMemcpyDeviceToHost, s);
+        if (tmax) cudaMemcpyAsync(tmax, TX, (size_t)nn * 4, cudaMemcpyDeviceToHost, s);
+        if (hmin) cudaMemcpyAsync(hmin, HN, (size_t)nn * 4, cudaMemcpyDeviceToHost, s);
+        if (hmax) cudaMemcpyAsync(hmax, HX, (size_t)nn * 4, cudaMemcpyDeviceToHost, s);
+    }
     if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return RT_E_CUDA;
     if (stats) {
         float ms = 0;
@@ -487,4 +509,18 @@ extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_
         stats->download_ms = ms_since(t0);
     }
     return RT_OK;
+}
+
+}  // namespace
+
+extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_t dlen, int32_t device, int32_t* tmin,
+                                         int32_t* tmax, int32_t* hmin, int32_t* hmax, int64_t len,
+                                         rt_extremal_stats* stats) {
+    return extremal_run(model, d, dlen, device, tmin, tmax, hmin, hmax, len, stats, false);
+}
+
+extern "C" rt_status rt_extremal_tilings_device(int32_t model, const int32_t* d, int64_t dlen, int32_t device,
+                                                int32_t* d_tmin, int32_t* d_tmax, int32_t* d_hmin, int32_t* d_hmax,
+                                                int64_t len, rt_extremal_stats* stats) {
+    return extremal_run(model, d, dlen, device, d_tmin, d_tmax, d_hmin, d_hmax, len, stats, true);
 }

@@ -118,3 +118,36 @@ def test_warm_start_preparation_on_the_device(kind, size):
     for f in ("tmin", "tmax", "hmin", "hmax", "idx"):
         assert np.array_equal(getattr(a, f), getattr(b, f)), f
     assert a.n == b.n
+
+
+@pytest.mark.parametrize("model,make", [(0, lambda rt: rt.DominoTiler.AztecDiamond(60)),
+                                        (1, lambda rt: rt.LozengeTiler.Hexagon(40, 30, 50))])
+def test_device_outputs_equal_host_outputs(model, make):
+    """rt_extremal_tilings_device writes the same arrays into device buffers,
+    for every output or any subset of them."""
+    import torch
+
+    import randomtilings_b200 as rt
+    from randomtilings_b200 import builders
+
+    d = make(rt)
+    ref, _ = builders.extremal_tilings(model, d)
+    n2 = ref["tmin"].size
+    names = ("tmin", "tmax", "hmin", "hmax")
+    for subset in (names, ("tmin",), ("hmax", "tmax"), ("hmin",)):
+        out = {k: torch.full((n2,), -7, dtype=torch.int32, device="cuda:0") for k in subset}
+        st = builders.extremal_tilings_device(model, d, **{k: v.data_ptr() for k, v in out.items()})
+        torch.cuda.synchronize()
+        for k, v in out.items():
+            assert np.array_equal(v.cpu().numpy(), ref[k]), (subset, k)
+        assert st["passes"] >= 8
+
+
+def test_device_outputs_must_be_device_memory():
+    import randomtilings_b200 as rt
+    from randomtilings_b200 import _capi, builders
+
+    d = rt.DominoTiler.AztecDiamond(10)
+    host = np.zeros(builders.vertex_side(0, len(d)) ** 2, dtype=np.int32)
+    with pytest.raises(_capi.RtError):
+        builders.extremal_tilings_device(0, d, tmin=host.ctypes.data)
