@@ -21,6 +21,11 @@ or the oracle's C restatement where oracle/_ref is absent.
 Multi-GPU: one walk is a single lattice, which this path does not split, so
 --gpus N runs N independent replicas (seeds 42 + rank), value = total
 attempts / max over ranks of the device time.
+
+Other workloads (their own JSON line, not the headline): --workload cftp
+(coupling from the past on an Aztec diamond, optionally with two-periodic
+domino weights), --workload extremal (extremal tilings of large domains, host
+flood vs device), --legs (single legs for profiling captures).
 """
 from __future__ import annotations
 
