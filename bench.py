@@ -1,4 +1,4 @@
-"""Benchmark of the bit-exact flip dynamics on the configs[1] workload.
+"""Benchmark of the bit-exact flip dynamics on the a=b=c=500 hexagon.
 
 Workload: lozenge tilings of the a=b=c=500 hexagon (LozengeTiler::AlmostHexDomain
 (500, 0) -> MinTiling, 1008 x 1008 tiling, 338,688 flip attempts per colour
@@ -423,7 +423,7 @@ def measure_aztec2000(args, device: int, seed: int, flush) -> dict:
 
 
 def run_cftp(args) -> None:
-    """configs[2]: CFTP on an Aztec diamond (order args.cftp_order), coupled
+    """CFTP on an Aztec diamond (order args.cftp_order), coupled
     chains from the maximal and minimal tilings, doubling from 1,024 colour
     steps, one run per master seed 0..args.cftp_seeds-1."""
     import randomtilings_b200 as rt

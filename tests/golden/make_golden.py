@@ -130,8 +130,8 @@ def walks(start: dict) -> dict:
     return out
 
 
-def config0(start: dict) -> dict:
-    """Aztec diamond n=100 from the minimal tiling, seed 42."""
+def aztec100(start: dict) -> dict:
+    """Aztec diamond n=100 from the minimal tiling, seed 42: the reference's walk."""
     out = {}
     t = start["domino/aztec100/min"]
     d = start["domino/aztec100/domain"]
@@ -232,8 +232,8 @@ def main() -> None:
     w = walks(start)
     print(f"walks: {len(w)} arrays", flush=True)
     np.savez_compressed(os.path.join(OUT, "walks.npz"), **w)
-    c0 = config0(start)
-    np.savez_compressed(os.path.join(OUT, "config0.npz"), **c0)
+    c0 = aztec100(start)
+    np.savez_compressed(os.path.join(OUT, "aztec100.npz"), **c0)
     with open(os.path.join(OUT, "svg_digests.json"), "w") as f:
         json.dump(svg_digests(start, w), f, indent=1)
     if os.path.isdir(os.path.join(REF, "Examples")):

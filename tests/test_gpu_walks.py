@@ -1,7 +1,7 @@
 """GPU parity of the bit-exact walks, through the C ABI (librt_b200.so).
 
 Every case compares the CUDA result with the oracle on the same input:
-the golden reference outputs (tests/golden/walks.npz, config0.npz) and the
+the golden reference outputs (tests/golden/walks.npz, aztec100.npz) and the
 C restatement on further seeds / sizes.  Integer tilings: bit-exact.
 """
 from __future__ import annotations
@@ -72,9 +72,9 @@ def test_recttri_golden(rt, key):
 
 
 @pytest.mark.parametrize("steps", [10000, 20000])
-def test_config0_aztec100(rt, steps):
-    """bit-exact with the reference's kernels run on the host CPU."""
-    b, c = golden("builders"), golden("config0")
+def test_aztec100(rt, steps):
+    """Aztec diamond n=100, seed 42: bit-exact with the reference's kernels run on the host CPU."""
+    b, c = golden("builders"), golden("aztec100")
     tl = rt.DominoTiler()
     got = _walk(tl, b["domino/aztec100/min"], steps, 42)
     assert np.array_equal(got, c[f"cfg0/s{steps}/end"])

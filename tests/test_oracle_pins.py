@@ -78,9 +78,9 @@ def test_recttri_walk_matches_reference(key):
 
 
 @pytest.mark.parametrize("steps", [10000, 20000])
-def test_config0_aztec100_matches_reference(steps):
-    """configs[0]: Aztec n=100 from the minimal tiling, seed 42."""
-    b, c = golden("builders"), golden("config0")
+def test_aztec100_matches_reference(steps):
+    """Aztec n=100 from the minimal tiling, seed 42."""
+    b, c = golden("builders"), golden("aztec100")
     got = po.domino_walk(b["domino/aztec100/min"], steps, 42)
     assert np.array_equal(got, c[f"cfg0/s{steps}/end"])
 
