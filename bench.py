@@ -157,14 +157,41 @@ def dist_setup(ngpus: int):
     return 0, 1, 0, None
 
 
+def _reduce_device(dist) -> str:
+    # NCCL reduces CUDA tensors; the gloo backend (the CPU tests of this code) host ones
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
 def all_max(dist, x: float) -> float:
+    """The largest x over the ranks (device times: the job is as slow as its slowest GPU)."""
     if dist is None:
         return x
     import torch
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device(dist))
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def all_sum(dist, xs: list[float]) -> list[float]:
+    """Element-wise sums over the ranks (attempts, bytes)."""
+    if dist is None:
+        return list(xs)
+    import torch
+
+    t = torch.tensor(xs, dtype=torch.float64, device=_reduce_device(dist))
+    dist.all_reduce(t)
+    return [float(v) for v in t.tolist()]
+
+
+def shard(count: int, rank: int, world: int) -> range:
+    """Independent units (batch chains, CFTP seeds) dealt round-robin to the ranks."""
+    return range(rank, count, world)
+
+
+def replica_seed(rank: int) -> int:
+    """Seed of rank r's replica walk (the ranks walk independent replicas)."""
+    return SEED + rank
 
 
 def barrier(dist):
@@ -264,7 +291,7 @@ def run_b200(args) -> None:
     t0 = start_tiling()
     n = int(round(t0.size ** 0.5))
     attempts = n * (n // 3)
-    seed = SEED + rank
+    seed = replica_seed(rank)
     flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
     def flush():
@@ -436,7 +463,7 @@ def run_cftp(args) -> None:
     rng = {"tinymt": rt.RT_RNG_TINYMT, "philox": rt.RT_RNG_PHILOX, "planes": rt.RT_RNG_PLANES}[args.cftp_rng]
     weights = [float(v) for v in args.cftp_weights.split(",")] if args.cftp_weights else None
     runs = []
-    for s in range(rank, args.cftp_seeds, world):
+    for s in shard(args.cftp_seeds, rank, world):
         tl = rt.DominoTiler(device=local, kernel=rt.RT_KERNEL_CFTP, rng=rng)
         if weights:
             tl.SetWeights(*rt.DominoTiler.TwoPeriodicWeights(*weights))
@@ -531,7 +558,7 @@ def measure_batch(args, rank: int, world: int, dist, peak: float) -> dict:
 
     bt = rt.Batch(device=int(os.environ.get("LOCAL_RANK", "0")))
     kinds = {}
-    for seed in range(rank, args.batch_chains, world):
+    for seed in shard(args.batch_chains, rank, world):
         model, t = workloads.mixed_chain(seed)
         bt.add(model, t, key=seed, chain=seed)
         kinds[model] = kinds.get(model, 0) + 1
@@ -542,13 +569,7 @@ def measure_batch(args, rank: int, world: int, dist, peak: float) -> dict:
     info = bt.info()
     bt.close()
     ms = all_max(dist, info["run_ms"])
-    total_attempts, total_bytes = float(info["attempts"]), float(info["algorithmic_bytes"])
-    if dist is not None:
-        import torch
-
-        x = torch.tensor([total_attempts, total_bytes], dtype=torch.float64, device="cuda")
-        dist.all_reduce(x)
-        total_attempts, total_bytes = float(x[0]), float(x[1])
+    total_attempts, total_bytes = all_sum(dist, [float(info["attempts"]), float(info["algorithmic_bytes"])])
     achieved = total_bytes / world / (ms / 1e3) / 1e9  # per GPU
     return {
         "workload": f"{args.batch_chains} chains of the mixed workload (seed s: s mod 4 -> Aztec diamond n in "
