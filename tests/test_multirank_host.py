@@ -36,3 +36,20 @@ def test_two_ranks_shard_and_reduce(tmp_path):
     assert r[0]["max"] == r[1]["max"] == 2.5
     assert r[0]["sum"] == r[1]["sum"] == [3.0, 30.0]
     assert r[1].get("reference_arm_returned") and "reference_arm_returned" not in r[0]
+
+
+def test_a_lost_rank_ends_the_next_reduction_with_an_error(tmp_path):
+    """Rank 1 leaves between steps; rank 0's reduction of the timings fails
+    with an exception (no hang), well inside the group's 10 s timeout bound."""
+    worker = os.path.join(ROOT, "tests", "multirank_worker.py")
+    port = _free_port()
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, RANK=str(rank), WORLD_SIZE="2", LOCAL_RANK=str(rank),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, worker, str(tmp_path), "lost"], cwd=ROOT, env=env,
+                                      stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
+    codes = [p.wait(timeout=120) for p in procs]
+    assert codes == [0, 3]
+    r = json.load(open(tmp_path / "rank0.json"))
+    assert r["error"] is not None and r["seconds"] < 60
