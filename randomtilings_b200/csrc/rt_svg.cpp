@@ -257,9 +257,9 @@ rt_status rt_domino_domain_svg(const int32_t* d, int64_t dlen, const char* filen
     o << "<g id=\"b\">  <polygon points = \"-.5,-.5 .5,-.5 .5,.5 -.5,.5\" fill=\"blue\"/> </g>\n";
     o << "<g id=\"w\">  <polygon points = \"-.5,-.5 .5,-.5 .5,.5 -.5,.5\" fill=\"grey\"/> </g>\n";
     o << "</defs>\n";
-    for_rows(o, 0, m, m, [&](Sink& o, int i) {
+    for_rows(o, 0, m, m, [&](Sink& row_out, int i) {
         for (int j = 0; j < m; ++j)
-            if (d[(size_t)i * m + j] == 1) use(o, (i + j) % 2 == 0 ? "b" : "w", j + .5, i + .5, true);
+            if (d[(size_t)i * m + j] == 1) use(row_out, (i + j) % 2 == 0 ? "b" : "w", j + .5, i + .5, true);
     });
     o << "</svg>";
     return finish(o);
@@ -303,12 +303,12 @@ static rt_status domino_pairs_svg(const int32_t* t, int64_t tlen, const char* fi
         }
     }
     o << "</defs>\n";
-    for_rows(o, 0, n, n, [&](Sink& o, int i) {
+    for_rows(o, 0, n, n, [&](Sink& row_out, int i) {
         for (int j = 0; j < n; ++j) {
             const int32_t v = t[(size_t)i * n + j];
             const bool odd = (i + j) % 2 == 1;
-            if ((v & 1) == 1) use(o, odd ? "h1" : "h2", j, i, true);
-            if ((v & 4) == 4) use(o, odd ? "v1" : "v2", j, i, true);
+            if ((v & 1) == 1) use(row_out, odd ? "h1" : "h2", j, i, true);
+            if ((v & 4) == 4) use(row_out, odd ? "v1" : "v2", j, i, true);
         }
     });
     o << "</svg>";
@@ -349,29 +349,29 @@ rt_status rt_domino_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d, 
     o << "<g id=\"b\">  <circle cx=\"0\" cy=\"0\" r=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
     o << "<g id=\"w\">  <circle cx=\"0\" cy=\"0\" r=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"white\" /> </g>\n";
     o << "</defs>\n";
-    for_rows(o, 0, n, n, [&](Sink& o, int i) {
+    for_rows(o, 0, n, n, [&](Sink& row_out, int i) {
         for (int j = 0; j < n; ++j) {
             const double x = j, y = i;
             const int32_t v = t[(size_t)i * n + j];
-            if ((v & 1) == 1) use(o, "hd", x, y - .5, false);
-            if ((v & 4) == 4) use(o, "vd", x - .5, y, false);
+            if ((v & 1) == 1) use(row_out, "hd", x, y - .5, false);
+            if ((v & 4) == 4) use(row_out, "vd", x - .5, y, false);
         }
     });
-    for_rows(o, 1, m, m, [&](Sink& o, int i) {
+    for_rows(o, 1, m, m, [&](Sink& row_out, int i) {
         for (int j = 1; j < m; ++j) {
             if (D(i, j) != 1) continue;
             const double x = j + .5, y = i + .5;
             if ((i + j) % 2 == 1) {
-                if (D(i, j + 1) == 1) use(o, "he", x + .5, y, false);
-                if (D(i, j - 1) == 1) use(o, "he", x - .5, y, false);
+                if (D(i, j + 1) == 1) use(row_out, "he", x + .5, y, false);
+                if (D(i, j - 1) == 1) use(row_out, "he", x - .5, y, false);
             }
-            if (D(i - 1, j) == 1) use(o, "ve", x, y - .5, false);
-            if (D(i + 1, j) == 1) use(o, "ve", x, y + .5, false);
+            if (D(i - 1, j) == 1) use(row_out, "ve", x, y - .5, false);
+            if (D(i + 1, j) == 1) use(row_out, "ve", x, y + .5, false);
         }
     });
-    for_rows(o, 1, m, m, [&](Sink& o, int i) {
+    for_rows(o, 1, m, m, [&](Sink& row_out, int i) {
         for (int j = 1; j < m; ++j)
-            if (D(i, j) == 1) use(o, (i + j) % 2 == 0 ? "b" : "w", j + .5, i + .5, true);
+            if (D(i, j) == 1) use(row_out, (i + j) % 2 == 0 ? "b" : "w", j + .5, i + .5, true);
     });
     o << "</svg>";
     return finish(o);
@@ -388,9 +388,9 @@ rt_status rt_lozenge_domain_svg(const int32_t* d, int64_t dlen, const char* file
     o << "<g id=\"w\">  <polygon points = \"0,1 .5,0 1,1\" fill=\"lightsteelblue\"/> </g>\n";
     o << "<g id=\"b\">  <polygon points = \"0,0 1,0 .5,1\" fill=\"slategrey\"/> </g>\n";
     o << "</defs>\n";
-    for_rows(o, 0, m, 2 * m, [&](Sink& o, int i) {
+    for_rows(o, 0, m, 2 * m, [&](Sink& row_out, int i) {
         for (int j = 0; j < 2 * m; ++j)
-            if (d[(size_t)i * 2 * m + j] == 1) use(o, j % 2 == 0 ? "b" : "w", .5 * j + .5 * i, i, true);
+            if (d[(size_t)i * 2 * m + j] == 1) use(row_out, j % 2 == 0 ? "b" : "w", .5 * j + .5 * i, i, true);
     });
     o << "</svg>";
     return finish(o);
@@ -407,12 +407,12 @@ rt_status rt_lozenge_tiling_svg(const int32_t* t, int64_t tlen, const char* file
     o << "<g id=\"g\">  <polygon points = \"0,0 1,0 .5,-1 -.5,-1\" fill=\"lightsteelblue\"/> </g>\n";
     o << "<g id=\"b\">  <polygon points = \"0,0 .5,-1 1,0 .5,1\" fill=\"slategrey\"/> </g>\n";
     o << "</defs>\n";
-    for_rows(o, 1, n - 1, n, [&](Sink& o, int i) {
+    for_rows(o, 1, n - 1, n, [&](Sink& row_out, int i) {
         for (int j = 1; j < n - 1; ++j) {
             const int32_t v = t[(size_t)i * n + j];
-            if ((v & 1) == 1) use(o, "r", j + .5 * i, i, true);
-            if ((v & 2) == 2) use(o, "g", j + .5 * i, i, true);
-            if ((v & 8) == 8) use(o, "b", j + .5 * i, i, true);
+            if ((v & 1) == 1) use(row_out, "r", j + .5 * i, i, true);
+            if ((v & 2) == 2) use(row_out, "g", j + .5 * i, i, true);
+            if ((v & 8) == 8) use(row_out, "b", j + .5 * i, i, true);
         }
     });
     o << "</svg>";
@@ -459,25 +459,25 @@ rt_status rt_lozenge_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d,
     o << "<g id=\"b\">  <ellipse cx=\".5\" cy=\".333333333333\" rx=\".1\" ry=\".11547\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
     o << "<g id=\"w\">  <ellipse cx=\".5\" cy=\".666666666666\" rx=\".1\"  ry=\".11547\" stroke=\"black\" stroke-width=\".02\" fill=\"white\" /> </g>\n";
     o << "</defs>\n";
-    for_rows(o, 1, n - 1, n, [&](Sink& o, int i) {
+    for_rows(o, 1, n - 1, n, [&](Sink& row_out, int i) {
         for (int j = 1; j < n - 1; ++j) {
             const int32_t v = t[(size_t)i * n + j];
-            if ((v & 1) == 1) use(o, "d1", j + .5 * i, i, true);
-            if ((v & 2) == 2) use(o, "d2", j + .5 * i, i, true);
-            if ((v & 8) == 8) use(o, "d8", j + .5 * i, i, true);
+            if ((v & 1) == 1) use(row_out, "d1", j + .5 * i, i, true);
+            if ((v & 2) == 2) use(row_out, "d2", j + .5 * i, i, true);
+            if ((v & 8) == 8) use(row_out, "d8", j + .5 * i, i, true);
         }
     });
-    for_rows(o, 1, n - 1, 2 * n, [&](Sink& o, int i) {
+    for_rows(o, 1, n - 1, 2 * n, [&](Sink& row_out, int i) {
         for (int j = 1; j < 2 * n - 1; ++j)
             if (D(i, j) == 1 && j % 2 == 0) {
-                if (D(i, j - 1) == 1) use(o, "e1", .5 + .5 * j + .5 * i, i + 1, true);
-                if (D(i, j + 1) == 1) use(o, "e2", .5 + .5 * j + .5 * i, i + 1, true);
-                if (D(i + 1, j - 1) == 1) use(o, "e8", .5 + .5 * j + .5 * i, i + 1, true);
+                if (D(i, j - 1) == 1) use(row_out, "e1", .5 + .5 * j + .5 * i, i + 1, true);
+                if (D(i, j + 1) == 1) use(row_out, "e2", .5 + .5 * j + .5 * i, i + 1, true);
+                if (D(i + 1, j - 1) == 1) use(row_out, "e8", .5 + .5 * j + .5 * i, i + 1, true);
             }
     });
-    for_rows(o, 1, n - 1, 2 * n, [&](Sink& o, int i) {
+    for_rows(o, 1, n - 1, 2 * n, [&](Sink& row_out, int i) {
         for (int j = 1; j < 2 * n - 1; ++j)
-            if (D(i, j) == 1) use(o, j % 2 == 0 ? "b" : "w", .5 * i + .5 * j, i, true);
+            if (D(i, j) == 1) use(row_out, j % 2 == 0 ? "b" : "w", .5 * i + .5 * j, i, true);
     });
     o << "</svg>";
     return finish(o);
@@ -488,9 +488,9 @@ rt_status rt_lozenge_print_domain(const int32_t* d, int64_t dlen, const char* fi
     if (!d || !filename) return RT_E_INVAL;
     const int m = side_of(dlen / 2);
     Sink o(filename);
-    for_rows(o, 0, m, 2 * m, [&](Sink& o, int i) {
-        for (int j = 0; j < 2 * m; ++j) o << d[(size_t)i * 2 * m + j] << " ";
-        o << "\n";
+    for_rows(o, 0, m, 2 * m, [&](Sink& row_out, int i) {
+        for (int j = 0; j < 2 * m; ++j) row_out << d[(size_t)i * 2 * m + j] << " ";
+        row_out << "\n";
     });
     return finish(o);
 }
@@ -502,10 +502,10 @@ rt_status rt_recttri_tiling_svg(const int32_t* t, int64_t tlen, const char* file
     const double W = kSqrt3 * 2 * (n + 1), H = 3 / 2.0 * (n + 1), s = 20;
     Sink o(filename);
     o << "<svg xmlns='http://www.w3.org/2000/svg' height=\"" << s * H << "\" width=\"" << s * W << "\" >\n";
-    for_rows(o, 0, m, 8 * m, [&](Sink& o, int i) {
+    for_rows(o, 0, m, 8 * m, [&](Sink& row_out, int i) {
         for (int j = 0; j < m; ++j) {
-            face_picture(o, (t[(size_t)i * n + j + 1] & (0xf << 4)) >> 4, i, 2 * j + 1);
-            face_picture(o, t[(size_t)i * n + j] & 0xf, i, 2 * j);
+            face_picture(row_out, (t[(size_t)i * n + j + 1] & (0xf << 4)) >> 4, i, 2 * j + 1);
+            face_picture(row_out, t[(size_t)i * n + j] & 0xf, i, 2 * j);
         }
     });
     o << "</svg>";
@@ -522,9 +522,9 @@ rt_status rt_tridimer_domain_svg(const int32_t* d, int64_t dlen, const char* fil
     o << "<g id=\"w\">  <polygon points = \"0,1 .5,0 1,1\" fill=\"paleturquoise\"/> </g>\n";
     o << "<g id=\"b\">  <polygon points = \"0,0 1,0 .5,1\" fill=\"deepskyblue\"/> </g>\n";
     o << "</defs>\n";
-    for_rows(o, 0, m, 2 * m, [&](Sink& o, int i) {
+    for_rows(o, 0, m, 2 * m, [&](Sink& row_out, int i) {
         for (int j = 0; j < 2 * m; ++j)
-            if (d[(size_t)i * m * 2 + j] == 1) use(o, j % 2 == 0 ? "b" : "w", .5 * j + .5 * i, i, true);
+            if (d[(size_t)i * m * 2 + j] == 1) use(row_out, j % 2 == 0 ? "b" : "w", .5 * j + .5 * i, i, true);
     });
     o << "</svg>";
     return finish(o);
@@ -540,12 +540,12 @@ rt_status rt_tridimer_tiling_svg(const int32_t* t, int64_t tlen, const char* fil
     o << "<g id=\"dL\">  <polygon points = \"0,-0.6666666667 0.5,-0.3333333333 0.5,0.3333333333 1,0.6666666667 1,1.333333333 0.5,1.666666667 0,1.333333333 0,0.6666666667 -0.5,0.3333333333 -0.5,-0.3333333333\" fill=\"lightsteelblue\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
     o << "<g id=\"dH\">  <polygon points = \"0,-0.6666666667 0.5,-0.3333333333 1,-0.6666666667 1.5,-0.3333333333 1.5,0.3333333333 1,0.6666666667 0.5,0.3333333333 0,0.6666666667 -0.5,0.3333333333 -0.5,-0.3333333333\" fill=\"slategrey\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
     o << "</defs>\n";
-    for_rows(o, 0, m - 1, m, [&](Sink& o, int i) {
+    for_rows(o, 0, m - 1, m, [&](Sink& row_out, int i) {
         for (int j = 1; j < 2 * m - 1; j += 2) {
             const double x = .5 * j + .5 * i;
-            if ((t[(size_t)2 * i * n + j] & 4) == 4) use(o, "dR", x, i, true);
-            if ((t[(size_t)2 * i * n + j] & 8) == 8) use(o, "dL", x, i, true);
-            if ((t[(size_t)(2 * i + 1) * n + j] & 1) == 1) use(o, "dH", x, i, true);
+            if ((t[(size_t)2 * i * n + j] & 4) == 4) use(row_out, "dR", x, i, true);
+            if ((t[(size_t)2 * i * n + j] & 8) == 8) use(row_out, "dL", x, i, true);
+            if ((t[(size_t)(2 * i + 1) * n + j] & 1) == 1) use(row_out, "dH", x, i, true);
         }
     });
     o << "</svg>";
@@ -584,26 +584,26 @@ rt_status rt_tridimer_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d
     o << "<g id=\"v2\">  <ellipse cx=\"1.5\" cy=\"0\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
     o << "<g id=\"v3\">  <ellipse cx=\"1\" cy=\"1\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
     o << "</defs>\n";
-    for_rows(o, 0, m - 1, 2 * m, [&](Sink& o, int i) {
+    for_rows(o, 0, m - 1, 2 * m, [&](Sink& row_out, int i) {
         for (int j = 1; j < 2 * m - 1; j += 2) {
             const double x = .5 * j + .5 * i;
             const int32_t a = t[(size_t)2 * i * n + j], h = t[(size_t)(2 * i + 1) * n + j];
-            if ((a & 4) == 4) use(o, "dR", x, i, true);
-            else if (D(i, j - 1) == 1) use(o, "eR", x, i, true);
-            if ((a & 8) == 8) use(o, "dL", x, i, true);
-            else if (D(i, j - 1) == 1) use(o, "eL", x, i, true);
-            if ((h & 1) == 1) use(o, "dH", x, i, true);
-            else if (D(i, j - 1) == 1 || D(i - 1, j) == 1) use(o, "eH", x, i, true);
-            if ((a & 4) == 0 && D(i, j) == 1) use(o, "eR", x, i, true);
-            if ((a & 8) == 0 && D(i, j - 2) == 1 && j > 1) use(o, "eL", x, i, true);
+            if ((a & 4) == 4) use(row_out, "dR", x, i, true);
+            else if (D(i, j - 1) == 1) use(row_out, "eR", x, i, true);
+            if ((a & 8) == 8) use(row_out, "dL", x, i, true);
+            else if (D(i, j - 1) == 1) use(row_out, "eL", x, i, true);
+            if ((h & 1) == 1) use(row_out, "dH", x, i, true);
+            else if (D(i, j - 1) == 1 || D(i - 1, j) == 1) use(row_out, "eH", x, i, true);
+            if ((a & 4) == 0 && D(i, j) == 1) use(row_out, "eR", x, i, true);
+            if ((a & 8) == 0 && D(i, j - 2) == 1 && j > 1) use(row_out, "eL", x, i, true);
         }
     });
-    for_rows(o, 0, m, 2 * m, [&](Sink& o, int i) {
+    for_rows(o, 0, m, 2 * m, [&](Sink& row_out, int i) {
         for (int j = 2; j < 2 * m; j += 2) {
             const double x = .5 * j + .5 * i;
-            if (D(i, j) == 1 || D(i, j - 1) == 1) use(o, "v1", x, i, true);
-            if (D(i, j) == 1 || D(i, j + 1) == 1) use(o, "v2", x, i, true);
-            if (D(i, j) == 1 || D(i, j + 1) == 1 || D(i, j - 1) == 1) use(o, "v3", x, i, true);
+            if (D(i, j) == 1 || D(i, j - 1) == 1) use(row_out, "v1", x, i, true);
+            if (D(i, j) == 1 || D(i, j + 1) == 1) use(row_out, "v2", x, i, true);
+            if (D(i, j) == 1 || D(i, j + 1) == 1 || D(i, j - 1) == 1) use(row_out, "v3", x, i, true);
         }
     });
     o << "</svg>";
@@ -616,9 +616,9 @@ rt_status rt_save_matrix(const int32_t* a, int64_t len, const char* filename) {
     if (!a || !filename) return RT_E_INVAL;
     const int n = side_of(len);
     Sink o(filename);
-    for_rows(o, 0, n, n, [&](Sink& o, int i) {
-        for (int j = 0; j < n; ++j) o << a[(size_t)i * n + j] << " ";
-        o << "\n";
+    for_rows(o, 0, n, n, [&](Sink& row_out, int i) {
+        for (int j = 0; j < n; ++j) row_out << a[(size_t)i * n + j] << " ";
+        row_out << "\n";
     });
     return finish(o);
 }
