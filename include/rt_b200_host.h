@@ -4,7 +4,9 @@
  * These replace the static helpers of the reference's Tiler classes.  Every
  * function writes a variable-length int32 array: *len receives the length;
  * the array is written when out != NULL and cap >= *len (out == NULL is a
- * size query).  Domains, tilings and height functions use the reference's
+ * size query; where the length follows from the input sizes -- extremal
+ * tilings, heights, vertex kinds -- the query computes nothing else, so
+ * checks of the domain itself come with the call that fills the array).  Domains, tilings and height functions use the reference's
  * encodings and sizes, so outputs are interchangeable with it.  Heights are
  * normalised as the reference does: 0 at the first boundary vertex in
  * row-major order, INT_MAX outside the domain.  A domain that is not

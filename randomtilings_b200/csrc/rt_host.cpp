@@ -45,6 +45,23 @@ rt_status emit(const Vec& v, int32_t* out, int64_t cap, int64_t* len) {
     return RT_OK;
 }
 
+// Size queries (out == NULL) of the functions whose length follows from the
+// input sizes: nothing else is computed.
+rt_status size_only(int64_t n, int64_t* len) {
+    if (len) *len = n;
+    return RT_OK;
+}
+// Extremal tilings: the (M+1) x (M+1) vertices of an M x M domino domain ...
+rt_status dom_side_query(int64_t dlen, int64_t* len) {
+    const int m = isqrt_exact(dlen);
+    return m < 1 ? RT_E_INVAL : size_only((int64_t)(m + 1) * (m + 1), len);
+}
+// ... or of an M x 2M lozenge domain.
+rt_status loz_side_query(int64_t dlen, int64_t* len) {
+    const int m = isqrt_exact(dlen / 2);
+    return (m < 2 || (int64_t)2 * m * m != dlen) ? RT_E_INVAL : size_only((int64_t)(m + 1) * (m + 1), len);
+}
+
 // Dijkstra with unit steps from all seeded vertices; `dir` = +1 grows heights
 // from the lowest (maximal height function), -1 shrinks them from the highest
 // (minimal one).  allowed(v, nb) says whether the move v -> nb is one that
@@ -372,11 +389,13 @@ rt_status rt_domino_aztec(int32_t order, int32_t* out, int64_t cap, int64_t* len
 rt_status rt_domino_domain_to_vertices(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
     const int m = isqrt_exact(dlen);
     if (!d || m < 1) return RT_E_INVAL;
+    if (!out) return size_only((int64_t)(m + 1) * (m + 1), len);
     return emit(dom_vertices(Vec(d, d + dlen), m), out, cap, len);
 }
 
 rt_status rt_domino_max_tiling(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
     if (!d) return RT_E_INVAL;
+    if (!out) return dom_side_query(dlen, len);
     Vec t;
     rt_status s = dom_extremal(Vec(d, d + dlen), +1, &t);
     return s != RT_OK ? s : emit(t, out, cap, len);
@@ -384,6 +403,7 @@ rt_status rt_domino_max_tiling(const int32_t* d, int64_t dlen, int32_t* out, int
 
 rt_status rt_domino_min_tiling(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
     if (!d) return RT_E_INVAL;
+    if (!out) return dom_side_query(dlen, len);
     Vec t;
     rt_status s = dom_extremal(Vec(d, d + dlen), -1, &t);
     return s != RT_OK ? s : emit(t, out, cap, len);
@@ -393,6 +413,7 @@ rt_status rt_domino_height_to_tiling(const int32_t* h, int64_t hlen, const int32
                                      int64_t cap, int64_t* len) {
     const int n = isqrt_exact(hlen);
     if (!h || !d || n < 2 || (int64_t)(n - 1) * (n - 1) != dlen) return RT_E_INVAL;
+    if (!out) return size_only(hlen, len);
     return emit(dom_height_to_tiling(Vec(h, h + hlen), Vec(d, d + dlen), n), out, cap, len);
 }
 
@@ -400,6 +421,7 @@ rt_status rt_domino_tiling_to_height(const int32_t* t, int64_t tlen, const int32
                                      int64_t cap, int64_t* len) {
     const int n = isqrt_exact(tlen);
     if (!t || !d || n < 2 || (int64_t)(n - 1) * (n - 1) != dlen) return RT_E_INVAL;
+    if (!out) return size_only(tlen, len);
     const int m = n - 1;
     const Vec D(d, d + dlen);
     const Vec verts = dom_vertices(D, m);
@@ -493,11 +515,13 @@ rt_status rt_lozenge_hexagon(int32_t a, int32_t b, int32_t c, int32_t* out, int6
 rt_status rt_lozenge_domain_to_vertices(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
     const int m = isqrt_exact(dlen / 2);
     if (!d || m < 2 || (int64_t)2 * m * m != dlen) return RT_E_INVAL;
+    if (!out) return size_only((int64_t)(m + 1) * (m + 1), len);
     return emit(loz_vertices(Vec(d, d + dlen), m), out, cap, len);
 }
 
 rt_status rt_lozenge_max_tiling(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
     if (!d) return RT_E_INVAL;
+    if (!out) return loz_side_query(dlen, len);
     Vec t;
     rt_status s = loz_extremal(Vec(d, d + dlen), +1, &t);
     return s != RT_OK ? s : emit(t, out, cap, len);
@@ -505,6 +529,7 @@ rt_status rt_lozenge_max_tiling(const int32_t* d, int64_t dlen, int32_t* out, in
 
 rt_status rt_lozenge_min_tiling(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
     if (!d) return RT_E_INVAL;
+    if (!out) return loz_side_query(dlen, len);
     Vec t;
     rt_status s = loz_extremal(Vec(d, d + dlen), -1, &t);
     return s != RT_OK ? s : emit(t, out, cap, len);
@@ -514,6 +539,7 @@ rt_status rt_lozenge_height_to_tiling(const int32_t* h, int64_t hlen, const int3
                                       int64_t cap, int64_t* len) {
     const int n = isqrt_exact(hlen);
     if (!h || !d || n < 3 || (int64_t)2 * (n - 1) * (n - 1) != dlen) return RT_E_INVAL;
+    if (!out) return size_only(hlen, len);
     return emit(loz_height_to_tiling(Vec(h, h + hlen), Vec(d, d + dlen), n), out, cap, len);
 }
 
@@ -521,6 +547,7 @@ rt_status rt_lozenge_tiling_to_height(const int32_t* t, int64_t tlen, const int3
                                       int64_t cap, int64_t* len) {
     const int n = isqrt_exact(tlen);
     if (!t || !d || n < 3 || (int64_t)2 * (n - 1) * (n - 1) != dlen) return RT_E_INVAL;
+    if (!out) return size_only(tlen, len);
     const int m = n - 1;
     const Vec D(d, d + dlen);
     const Vec verts = loz_vertices(D, m);
