@@ -68,6 +68,12 @@ def oracle() -> ctypes.CDLL:
         lib.orc_recttri_walk_fast.argtypes = [_P, ctypes.c_int, _I64, _I64, ctypes.c_uint32, _P]
         lib.orc_tridimer_walk_fast.argtypes = [_P, ctypes.c_int, _I64, _I64, ctypes.c_uint32]
         lib.orc_project_heights.argtypes = [ctypes.c_int, _P, _I64, _P, _P, _P, _P, ctypes.c_int, _P]
+        lib.orc_lozenge_q_divergence.argtypes = [_P, ctypes.c_int, _I64, _I64, ctypes.c_double]
+        lib.orc_lozenge_q_divergence.restype = _I64
+        lib.orc_sixv_dwbc.argtypes = [ctypes.c_int, _P, _P]
+        lib.orc_sixv_vertex_type.argtypes = [ctypes.c_int] * 4
+        lib.orc_sixv_thresholds.argtypes = [_P, _P]
+        lib.orc_sixv_walk.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, _P]
         lib.orc_tinymt_init.argtypes = [_P, ctypes.c_uint32]
         lib.orc_tinymt_bits12.argtypes = [_P]
         lib.orc_tinymt_bits12.restype = ctypes.c_uint32
@@ -313,8 +319,113 @@ def project_heights(model: str, domain, hmin, hmax, target) -> np.ndarray:
     return out
 
 
+def lozenge_q_divergence(t, seed: int, max_steps: int, q: float = 0.99) -> int:
+    """First step count after which the q-weighted walk of t differs between
+    the float32 and the double comparison of qlozengekernel.cl:25 (0: none
+    within max_steps)."""
+    a, n = _tiling(t)
+    r = oracle().orc_lozenge_q_divergence(a.ctypes.data, n, seed, max_steps, q)
+    if r < 0:
+        raise RuntimeError("orc_lozenge_q_divergence failed")
+    return int(r)
+
+
+# ---- six-vertex model (sixv_oracle.c) ----------------------------------------
+SIXV_UNIFORM = (1.0, 1.0, 1.0, 1.0, 1.0, 1.0)
+
+
+def sixv_dwbc(n: int) -> tuple[np.ndarray, np.ndarray]:
+    """(h_min, h_max) of the domain-wall boundary, (n+1)^2 int32 each."""
+    lo = np.zeros((n + 1) ** 2, dtype=np.int32)
+    hi = np.zeros((n + 1) ** 2, dtype=np.int32)
+    oracle().orc_sixv_dwbc(n, lo.ctypes.data, hi.ctypes.data)
+    return lo, hi
+
+
+def sixv_thresholds(w=SIXV_UNIFORM) -> np.ndarray:
+    ww = np.ascontiguousarray(w, dtype=np.float64)
+    out = np.zeros(16, dtype=np.uint32)
+    oracle().orc_sixv_thresholds(ww.ctypes.data, out.ctypes.data)
+    return out
+
+
+def sixv_walk(h, sweeps, keys, chain: int = 0, w=SIXV_UNIFORM) -> np.ndarray:
+    """The six-vertex heat bath on heights h ((n+1)^2); sweeps / keys one value
+    or one per epoch."""
+    a = np.array(h, dtype=np.int32).reshape(-1).copy()
+    n = int(round(a.size ** 0.5)) - 1
+    st, ke = _epochs(sweeps, keys)
+    ww = np.ascontiguousarray(w, dtype=np.float64)
+    _check(oracle().orc_sixv_walk(a.ctypes.data, n, st.ctypes.data, ke.ctypes.data, st.size, chain, ww.ctypes.data),
+           "orc_sixv_walk")
+    return a
+
+
+def sixv_cftp(n: int, first_sweeps: int, master_seed: int, max_trials: int = 30, w=SIXV_UNIFORM, chain: int = 0):
+    """CFTP from the maximal and minimal heights as rt_sixv_cftp composes it:
+    epoch keys are successive std::mt19937(master_seed) outputs, newest epoch
+    first; the schedule doubles.  Returns (heights, trials, total sweeps,
+    coalesced)."""
+    lo, hi = sixv_dwbc(n)
+    keys_out = np.zeros(max_trials + 1, dtype=np.uint32)
+    oracle().orc_mt19937_stream(master_seed, max_trials + 1, keys_out.ctypes.data)
+    sweeps, keys = [first_sweeps], [int(keys_out[0])]
+    top = hi
+    for trial in range(max_trials):
+        top, bot = sixv_walk(hi, sweeps, keys, chain, w), sixv_walk(lo, sweeps, keys, chain, w)
+        if np.array_equal(top, bot):
+            return top, trial + 1, sum(sweeps), True
+        sweeps.insert(0, sum(sweeps))
+        keys.insert(0, int(keys_out[trial + 1]))
+    return top, max_trials, sum(sweeps), False
+
+
+def sixv_vertex_types(h) -> np.ndarray:
+    """n x n vertex types (0..5: a1 a2 b1 b2 c1 c2) of heights h; -1 where invalid."""
+    a = np.asarray(h, dtype=np.int64).reshape(-1)
+    n1 = int(round(a.size ** 0.5))
+    H = a.reshape(n1, n1)
+    lib = oracle()
+    return np.array([[lib.orc_sixv_vertex_type(int(H[i - 1, j - 1]), int(H[i - 1, j]), int(H[i, j - 1]), int(H[i, j]))
+                      for j in range(1, n1)] for i in range(1, n1)], dtype=np.int32)
+
+
+def sixv_enumerate(n: int) -> list[np.ndarray]:
+    """Every domain-wall height function of the n x n grid (the alternating-sign
+    matrices of order n), by depth-first filling of the interior faces in row
+    order (small n only: 1, 2, 7, 42, 429, 7436 configurations)."""
+    lo, hi = sixv_dwbc(n)
+    N1 = n + 1
+    h = lo.astype(np.int64).reshape(N1, N1).copy()
+    lo2, hi2 = lo.reshape(N1, N1), hi.reshape(N1, N1)
+    cells = [(i, j) for i in range(1, n) for j in range(1, n)]
+    out = []
+
+    def rec(k):
+        if k == len(cells):
+            out.append(h.reshape(-1).astype(np.int32).copy())
+            return
+        i, j = cells[k]
+        for v in (h[i - 1, j] - 1, h[i - 1, j] + 1):
+            if lo2[i, j] <= v <= hi2[i, j] and abs(v - h[i, j - 1]) == 1:
+                h[i, j] = v
+                rec(k + 1)
+        h[i, j] = lo2[i, j]
+
+    rec(0)
+    return out
+
+
+def sixv_weight(h, w=SIXV_UNIFORM) -> float:
+    t = sixv_vertex_types(h)
+    assert (t >= 0).all()
+    return float(np.prod(np.asarray(w, dtype=np.float64)[t]))
+
+
 # ---- the reference's own code (oracle/_ref) --------------------------------
-REF_MODELS = {"domino": 0, "domino_cftp": 1, "lozenge": 2, "qlozenge": 3, "recttri": 4, "tridimer": 5}
+# "qlozenge_f32": qlozengekernel.cl compiled with single-precision arithmetic (an fp32-only device)
+REF_MODELS = {"domino": 0, "domino_cftp": 1, "lozenge": 2, "qlozenge": 3, "recttri": 4, "tridimer": 5,
+              "qlozenge_f32": 6}
 
 
 class RefTiler:

@@ -86,7 +86,17 @@ public:
     }
 };
 
-enum Model { M_DOMINO = 0, M_DOMINO_CFTP = 1, M_LOZENGE = 2, M_QLOZENGE = 3, M_RECTTRI = 4, M_TRIDIMER = 5 };
+// M_QLOZENGE_F32: the same loop over qlozengekernel.cl compiled with single-precision
+// arithmetic (k_qlozenge_f32.cpp), the comparison of an fp32-only OpenCL device.
+enum Model {
+    M_DOMINO = 0,
+    M_DOMINO_CFTP = 1,
+    M_LOZENGE = 2,
+    M_QLOZENGE = 3,
+    M_RECTTRI = 4,
+    M_TRIDIMER = 5,
+    M_QLOZENGE_F32 = 6
+};
 
 struct Handle {
     int model;
@@ -107,7 +117,7 @@ struct Handle {
     }
 };
 
-const char* kProgramIds[] = {"domino", "domino_cftp", "lozenge", "qlozenge", "recttri", "tridimer"};
+const char* kProgramIds[] = {"domino", "domino_cftp", "lozenge", "qlozenge", "recttri", "tridimer", "qlozenge_f32"};
 
 long emit(const std::vector<int>& v, int* out, long cap) {
     const long n = static_cast<long>(v.size());
@@ -136,7 +146,7 @@ int ref_write_params(const char* path, long count, unsigned mat1, unsigned mat2,
 }
 
 void* ref_tiler_create(int model, const char* params_path, long n_params) {
-    if (model < 0 || model > 5) return nullptr;
+    if (model < 0 || model > 6) return nullptr;
     try {
         Handle* h = new Handle();
         h->model = model;
@@ -155,6 +165,7 @@ void* ref_tiler_create(int model, const char* params_path, long n_params) {
                 h->lozenge->LoadTinyMT(params_path, static_cast<int>(n_params));
                 break;
             case M_QLOZENGE:
+            case M_QLOZENGE_F32:
                 h->qlozenge = new QLozengeLoop(h->context, h->queue, h->devices, src);
                 h->qlozenge->LoadTinyMT(params_path, static_cast<int>(n_params));
                 break;
@@ -190,6 +201,7 @@ int ref_tiler_walk(void* p, int* t, long tlen, long steps, long seed) {
                 h->lozenge->Walk(T, static_cast<int>(steps), seed);
                 break;
             case M_QLOZENGE:
+            case M_QLOZENGE_F32:
                 h->qlozenge->Walk(T, static_cast<int>(steps), seed);
                 break;
             case M_RECTTRI:

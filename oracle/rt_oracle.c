@@ -653,6 +653,52 @@ static int lozenge_run(int32_t* t, int n, const int64_t* steps, const int64_t* s
     return err;
 }
 
+/* The first step count after which the q-weighted walk (qlozengekernel.cl,
+ * TinyMT32J streams, seed) differs between the float32 and the double
+ * comparison, or 0 when it does not within max_steps.  Both walks agree up to
+ * the first draw that a site can accept in one comparison and not in the
+ * other, so one walk in the double comparison finds it.  Used to pick fixture
+ * step counts that tell the two comparisons apart. */
+int64_t orc_lozenge_q_divergence(const int32_t* t, int n, int64_t seed, int64_t max_steps, double q) {
+    if (n < 3 || n % 3) return -1;
+    const int m = n / 3;
+    const float qf = (float)q, qinvf = 1.0f / qf;
+    int32_t* arr[3];
+    for (int c = 0; c < 3; ++c) arr[c] = calloc((size_t)n * m, 4);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) arr[((j - i) % 3 + 3) % 3][(int64_t)i * m + j / 3] = t[(int64_t)i * n + j];
+    orc_draws rng;
+    int64_t found = 0;
+    if (draws_begin(&rng, 0, (int64_t)n * m, m, 0, 0, m, (uint32_t)(uint64_t)seed, 0, NULL, 0) != ORC_OK) found = -1;
+    minstd g;
+    minstd_seed(&g, seed);
+    for (int64_t s = 0; s < max_steps && found == 0; ++s) {
+        const int r = uniform_int(&g, 2);
+        /* the Rotate of qlozengekernel.cl:18-29 in the double comparison, watching the float32 one */
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < m; ++j) {
+                const float rd = orc_draw(&rng, i, j);
+                int32_t* v = &arr[r][(int64_t)i * m + j];
+                if (rd < 0.5f) {
+                    const float x = rd / 0.5f;
+                    const int okd = q >= (double)x, okf = qf >= x;
+                    if (*v == 25 && okd != okf && found == 0) found = s + 1;
+                    if (*v == 25 && okd) *v = 38;
+                } else {
+                    const float x = (rd - 0.5f) * 0.5f;
+                    const int okd = 1.0 / q >= (double)x, okf = qinvf >= x;
+                    if (*v == 38 && okd != okf && found == 0) found = s + 1;
+                    if (*v == 38 && okd) *v = 25;
+                }
+            }
+        lozenge_update(arr[r], arr[(r + 1) % 3], arr[(r + 2) % 3], 1, n, r);
+        draws_next(&rng);
+    }
+    if (found >= 0) draws_end(&rng);
+    for (int c = 0; c < 3; ++c) free(arr[c]);
+    return found;
+}
+
 int orc_lozenge_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
                      int qmode, double q, int qcmp) {
     return lozenge_run(t, n, &steps, &seed, 1, params, nparams, qmode, q, qcmp, 0, 0, NULL);

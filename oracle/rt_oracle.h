@@ -120,6 +120,20 @@ int orc_project_heights(int model, const int32_t* d, int64_t dlen, const int32_t
 int orc_domino_colours(int64_t seed, int64_t steps, int single_walk, uint8_t* out);
 int orc_lozenge_colours(int64_t seed, int64_t steps, uint8_t* out);
 
+/* First step count after which the q-weighted walk differs between the
+ * float32 and the double comparison (0: not within max_steps). */
+int64_t orc_lozenge_q_divergence(const int32_t* t, int n, int64_t seed, int64_t max_steps, double q);
+
+/* ---- six-vertex model (sixv_oracle.c; no reference code: README.md:3 names
+ * the model only).  Heights on the (n+1) x (n+1) faces of an n x n grid with
+ * domain-wall boundary conditions; weights w[6] of the vertex types
+ * a1, a2, b1, b2, c1, c2; Philox draws as the CUDA walk takes them. ---- */
+void orc_sixv_dwbc(int n, int32_t* hmin, int32_t* hmax);
+int orc_sixv_vertex_type(int a, int b, int c, int d);
+void orc_sixv_thresholds(const double w[6], uint32_t thr[16]);
+int orc_sixv_walk(int32_t* h, int n, const int64_t* sweeps, const int64_t* keys, int k, uint32_t chain,
+                  const double w[6]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,10 +1,16 @@
 """Regenerates the golden fixtures in this directory from the reference itself.
 
-Run from the repository root, on a machine that has the reference source tree
-(REF, default /root/reference) and has built oracle/_ref/libref.so
-(`make -C oracle ref`):
+Run from the repository root, on a machine that has built oracle/_ref/libref.so
+from the reference source tree (`make -C oracle ref REF=<reference tree>`), with
+REF naming that tree for the example-output digests:
 
-    python tests/golden/make_golden.py
+    REF=<reference tree> python tests/golden/make_golden.py [--only part,part]
+
+Parts: builders, walks, aztec100, svg, examples (the original fixtures),
+qf32 (q-lozenge walks on which the float32 and double comparisons of
+qlozengekernel.cl part, from the reference kernel compiled both ways:
+qlozenge_f32.npz) and bench (SHA-256 digests of the bench workloads run by
+the reference and the oracle at their full sizes: bench_parity.json).
 
 Everything here comes out of the reference's own code (its Tiler classes and
 OpenCL kernels compiled for the CPU through oracle/shim): domains, extremal
@@ -15,6 +21,7 @@ files written here; nothing reads the reference tree at test time.
 """
 from __future__ import annotations
 
+import argparse
 import hashlib
 import json
 import os
@@ -27,12 +34,24 @@ ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
 sys.path.insert(0, ROOT)
 from oracle import pyoracle as po  # noqa: E402
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("REF", "")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
 def side(a) -> int:
     return int(round(np.asarray(a).size ** 0.5))
+
+
+def digest(a) -> str:
+    """SHA-256 of an int32 array's little-endian bytes (the tests hash the same way)."""
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<i4").tobytes()).hexdigest()
+
+
+def q_divergence(t, seed: int, max_steps: int) -> int:
+    """The smallest step count <= max_steps after which the q = 0.99 walk of
+    tiling t (seed) differs between the float32 and the double comparison
+    (the oracle's finder; 0 when none)."""
+    return po.lozenge_q_divergence(t, seed, max_steps, 0.99)
 
 
 def builders() -> dict:
@@ -146,6 +165,102 @@ def aztec100(start: dict) -> dict:
     return out
 
 
+def qlozenge_f32(start: dict) -> dict:
+    """q = 0.99 walks from qlozengekernel.cl compiled with single-precision
+    arithmetic (an fp32-only OpenCL device), beside the double build: the
+    seeds of the small hexagons, and walks of an a=b=c=40 hexagon stopped
+    right after a draw at which the two comparisons part (the chains are
+    monotone and heal such a difference within a few sweeps, so the step
+    count matters).  Seeds 10000 m keep the work-item streams of different
+    seeds apart (seed + id)."""
+    out = {}
+    cases = []
+    for key in ("lozenge/hex4_1", "lozenge/hex10_2", "lozenge/hex13_5"):
+        for seed in (42, 5):
+            cases.append((f"qlozenge_f32/{key.split('/')[1]}/s{seed}", start[f"{key}/min"], 700, seed))
+    d = po.ref_build("lozenge_almost_hex", p0=40, p1=0)
+    t40 = po.ref_build("lozenge_min", d)
+    found = 0
+    for m in range(1, 400):
+        steps = q_divergence(t40, 10000 * m, 3000)
+        if steps:
+            cases.append((f"qlozenge_f32/hex40_0/s{10000 * m}", t40, steps, 10000 * m))
+            found += 1
+            if found == 3:
+                break
+    for key, t, steps, seed in cases:
+        f32 = po.RefTiler("qlozenge_f32", side(t) ** 2)
+        dbl = po.RefTiler("qlozenge", side(t) ** 2)
+        out[f"{key}/start"] = t
+        out[f"{key}/steps"] = np.array([steps])
+        out[f"{key}/seed"] = np.array([seed])
+        out[f"{key}/end"] = f32.walk(t, steps, seed)
+        out[f"{key}/end_double"] = dbl.walk(t, steps, seed)
+        f32.close()
+        dbl.close()
+    return out
+
+
+BENCH_SEGMENT = 3000  # colour steps per bench step (1,000 sweeps of the three colours)
+
+
+def bench_parity() -> dict:
+    """Digests of the bench's own workloads at their full sizes.
+
+    hex500: LozengeTiler::AlmostHexDomain(500, 0) -> MinTiling (1008 x 1008),
+    walked as the bench walks it -- 20 Walk calls of 3,000 colour steps with
+    seeds 42..61, each continuing from the last (20,000 sweeps) -- by the
+    reference's LozengeTiler::Walk and kernels (OpenMP over work items); the
+    q = 0.99 int32 walk (qlozengekernel.cl, float32 and double comparisons);
+    the fast and bit-plane modes (no reference counterpart: the oracle's
+    replay).  The q walk starts from the uniform walk's final tiling (a minimal
+    tiling has too few flippable sites for the comparisons to part within a
+    test's walk) and runs, with the first seed from 42 on that gives one, to
+    the step after which float32 and double differ.  aztec2000:
+    AztecDiamond(2000) -> MinTiling (4006 x 4006), fast and bit-plane walks
+    (the oracle's replay)."""
+    threads = os.cpu_count() or 1
+    out = {}
+    t0 = time.time()
+    d = po.ref_build("lozenge_almost_hex", p0=500, p1=0)
+    t = po.ref_build("lozenge_min", d)
+    out["hex500/start"] = digest(t)
+    rt = po.RefTiler("lozenge", side(t) ** 2, threads=threads)
+    a = t.copy()
+    for k in range(20):
+        a = rt.walk(a, BENCH_SEGMENT, 42 + k)
+        out[f"hex500/uniform/segment{k}"] = digest(a)
+        print(f"  hex500 segment {k}: {time.time() - t0:.0f}s", flush=True)
+    out["hex500/uniform/s42/600"] = digest(rt.walk(t, 600, 42))
+    rt.close()
+    qseed, qsteps = 0, 0
+    for qseed in range(42, 142):
+        qsteps = q_divergence(a, qseed, 1000)
+        if qsteps:
+            break
+    assert qsteps, "no float32/double divergence"
+    out["hex500/q/start"] = "hex500/uniform/segment19"
+    out["hex500/q/seed"] = qseed
+    out["hex500/q/steps"] = qsteps
+    print(f"  hex500 q: seed {qseed}, parts after {qsteps} steps: {time.time() - t0:.0f}s", flush=True)
+    for name, model in (("qf32", "qlozenge_f32"), ("qdouble", "qlozenge")):
+        rt = po.RefTiler(model, side(t) ** 2, threads=threads)
+        out[f"hex500/{name}"] = digest(rt.walk(a, qsteps, qseed))
+        rt.close()
+    assert out["hex500/qf32"] != out["hex500/qdouble"]
+    out["hex500/fast/k42/600"] = digest(po.walk_fast("lozenge", t, 600, 42))
+    out["hex500/planes/k42/600"] = digest(po.walk_planes("lozenge", t, 600, 42))
+    print(f"  hex500 done: {time.time() - t0:.0f}s", flush=True)
+    d = po.ref_build("domino_aztec", p0=2000)
+    t = po.ref_build("domino_min", d)
+    out["aztec2000/start"] = digest(t)
+    out["aztec2000/fast/k42/100"] = digest(po.walk_fast("domino", t, 100, 42))
+    out["aztec2000/planes/k42/100"] = digest(po.walk_planes("domino", t, 100, 42))
+    out["aztec2000/planes_hb/k42/100"] = digest(po.walk_planes("domino_cftp", t, 100, 42))
+    print(f"  aztec2000 done: {time.time() - t0:.0f}s", flush=True)
+    return out
+
+
 def example_outputs() -> dict:
     """SHA-256 of the deterministic Examples/ExampleOuts files, each checked
     against the reference's code run here."""
@@ -222,25 +337,44 @@ def svg_digests(b: dict, w: dict) -> dict:
     return out
 
 
+PARTS = ("builders", "walks", "aztec100", "svg", "examples", "qf32", "bench")
+
+
 def main() -> None:
+    ap = argparse.ArgumentParser(description="regenerate the golden fixtures from the reference")
+    ap.add_argument("--only", default=",".join(PARTS), help="comma-separated subset of " + ",".join(PARTS))
+    parts = set(ap.parse_args().only.split(","))
     if not po.have_ref():
-        sys.exit("oracle/_ref/libref.so is missing: run `make -C oracle ref` where the reference tree exists")
+        sys.exit("oracle/_ref/libref.so is missing: run `make -C oracle ref REF=<reference tree>`")
     t0 = time.time()
     start = builders()
     print(f"builders: {len(start)} arrays", flush=True)
-    np.savez_compressed(os.path.join(OUT, "builders.npz"), **start)
-    w = walks(start)
-    print(f"walks: {len(w)} arrays", flush=True)
-    np.savez_compressed(os.path.join(OUT, "walks.npz"), **w)
-    c0 = aztec100(start)
-    np.savez_compressed(os.path.join(OUT, "aztec100.npz"), **c0)
-    with open(os.path.join(OUT, "svg_digests.json"), "w") as f:
-        json.dump(svg_digests(start, w), f, indent=1)
-    if os.path.isdir(os.path.join(REF, "Examples")):
+    if "builders" in parts:
+        np.savez_compressed(os.path.join(OUT, "builders.npz"), **start)
+    w = None
+    if parts & {"walks", "svg"}:
+        w = walks(start)
+        print(f"walks: {len(w)} arrays", flush=True)
+    if "walks" in parts:
+        np.savez_compressed(os.path.join(OUT, "walks.npz"), **w)
+    if "aztec100" in parts:
+        c0 = aztec100(start)
+        np.savez_compressed(os.path.join(OUT, "aztec100.npz"), **c0)
+    if "svg" in parts:
+        with open(os.path.join(OUT, "svg_digests.json"), "w") as f:
+            json.dump(svg_digests(start, w), f, indent=1)
+    if "examples" in parts and REF and os.path.isdir(os.path.join(REF, "Examples")):
         with open(os.path.join(OUT, "example_outputs.json"), "w") as f:
             json.dump(example_outputs(), f, indent=1, sort_keys=True)
+    if "qf32" in parts:
+        q = qlozenge_f32(start)
+        print(f"qf32: {len(q)} arrays", flush=True)
+        np.savez_compressed(os.path.join(OUT, "qlozenge_f32.npz"), **q)
+    if "bench" in parts:
+        res = bench_parity()
+        with open(os.path.join(OUT, "bench_parity.json"), "w") as f:
+            json.dump(res, f, indent=1, sort_keys=True)
     print(f"done in {time.time() - t0:.1f}s")
-
 
 if __name__ == "__main__":
     main()
