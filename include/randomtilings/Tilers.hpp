@@ -18,6 +18,7 @@
 
 #include "../rt_b200.h"
 #include "../rt_b200_host.h"
+#include "../rt_b200_sixv.h"
 #include "../rt_b200_svg.h"
 
 namespace rt {
@@ -315,6 +316,58 @@ public:
     }
     static void DimerToSVG(const tiling& t, const domain& d, const std::string& f) {
         detail::check(rt_tridimer_dimer_svg(detail::p(t), t.size(), detail::p(d), d.size(), f.c_str()), nullptr);
+    }
+};
+
+// The six-vertex model with domain-wall boundary conditions (no reference
+// class: the reference's README.md:3 names the model only).  States are
+// height functions on the (n+1) x (n+1) faces, as heightfunc vectors.
+class SixVertexTiler {
+    rt_sixv* h_ = nullptr;
+    void check(rt_status s) const {
+        if (s != RT_OK) throw Error(s, rt_sixv_last_error(h_));
+    }
+    static int side1(const heightfunc& v) { return detail::side(v) - 1; }
+
+public:
+    explicit SixVertexTiler(int device = 0) {
+        if (rt_sixv_create(device, &h_) != RT_OK) throw Error(RT_E_NODEVICE, "rt_sixv_create failed");
+    }
+    SixVertexTiler(const SixVertexTiler&) = delete;
+    SixVertexTiler& operator=(const SixVertexTiler&) = delete;
+    ~SixVertexTiler() {
+        if (h_) rt_sixv_destroy(h_);
+    }
+    // Weights of the vertex types a1, a2, b1, b2, c1, c2.
+    void SetWeights(const std::vector<double>& w) {
+        if (w.size() != 6) throw Error(RT_E_INVAL, "six weights expected");
+        check(rt_sixv_set_weights(h_, w.data()));
+    }
+    static heightfunc MinHeights(int n) {
+        heightfunc h((size_t)(n + 1) * (n + 1));
+        detail::check(rt_sixv_dwbc_heights(n, reinterpret_cast<int32_t*>(h.data()), nullptr), nullptr);
+        return h;
+    }
+    static heightfunc MaxHeights(int n) {
+        heightfunc h((size_t)(n + 1) * (n + 1));
+        detail::check(rt_sixv_dwbc_heights(n, nullptr, reinterpret_cast<int32_t*>(h.data())), nullptr);
+        return h;
+    }
+    static std::vector<int> HeightsToASM(const heightfunc& h) {
+        const int n = side1(h);
+        std::vector<int> a((size_t)n * n);
+        detail::check(rt_sixv_to_asm(detail::p(h), n, reinterpret_cast<int32_t*>(a.data())), nullptr);
+        return a;
+    }
+    void Walk(heightfunc& h, long sweeps, long seed) {
+        check(rt_sixv_walk(h_, reinterpret_cast<int32_t*>(h.data()), side1(h), sweeps, (uint64_t)seed, 0));
+    }
+    heightfunc CFTP(int n, long first_sweeps, long master_seed, rt_cftp_stats* stats = nullptr) {
+        heightfunc h((size_t)(n + 1) * (n + 1));
+        rt_cftp_stats local{};
+        check(rt_sixv_cftp(h_, n, first_sweeps, master_seed, 30, reinterpret_cast<int32_t*>(h.data()),
+                           stats ? stats : &local));
+        return h;
     }
 };
 

@@ -8,9 +8,10 @@ from ._capi import (RT_CFTP_DOUBLING, RT_CFTP_REFERENCE, RT_DOMINO, RT_KERNEL_CF
                     RT_KERNEL_QWEIGHT, RT_LOZENGE, RT_QCMP_DOUBLE, RT_QCMP_FLOAT32, RT_RECTTRI, RT_RNG_PHILOX, RT_RNG_PLANES,
                     RT_RNG_TINYMT, RT_TRIDIMER, RtError, load)
 from .batch import Batch  # noqa: F401
+from .sixvertex import SixVertexTiler  # noqa: F401
 from .tilers import DominoTiler, LozengeTiler, RectTriangleTiler, TriangleDimerTiler  # noqa: F401
 
-__all__ = ["DominoTiler", "LozengeTiler", "RectTriangleTiler", "TriangleDimerTiler", "Batch", "RtError", "load",
+__all__ = ["DominoTiler", "LozengeTiler", "RectTriangleTiler", "TriangleDimerTiler", "SixVertexTiler", "Batch", "RtError", "load",
            "RT_KERNEL_DEFAULT", "RT_KERNEL_CFTP", "RT_KERNEL_QWEIGHT", "RT_RNG_TINYMT", "RT_RNG_PHILOX", "RT_RNG_PLANES",
            "RT_QCMP_FLOAT32", "RT_QCMP_DOUBLE", "RT_CFTP_DOUBLING", "RT_CFTP_REFERENCE", "RT_DOMINO", "RT_LOZENGE",
            "RT_RECTTRI", "RT_TRIDIMER"]

@@ -232,6 +232,21 @@ SIGNATURES.update({
                                     ctypes.POINTER(ctypes.c_float)]),
 })
 
+# include/rt_b200_sixv.h
+SIGNATURES.update({
+    "rt_sixv_create": (ctypes.c_int, [_I32, ctypes.POINTER(_P)]),
+    "rt_sixv_destroy": (ctypes.c_int, [_P]),
+    "rt_sixv_last_error": (ctypes.c_char_p, [_P]),
+    "rt_sixv_set_weights": (ctypes.c_int, [_P, _P]),
+    "rt_sixv_thresholds": (ctypes.c_int, [_P, _P, ctypes.POINTER(_I32)]),
+    "rt_sixv_dwbc_heights": (ctypes.c_int, [_I32, _P, _P]),
+    "rt_sixv_check": (ctypes.c_int, [_P, _I32]),
+    "rt_sixv_to_asm": (ctypes.c_int, [_P, _I32, _P]),
+    "rt_sixv_vertex_types": (ctypes.c_int, [_P, _I32, _P]),
+    "rt_sixv_walk": (ctypes.c_int, [_P, _P, _I32, _I64, ctypes.c_uint64, ctypes.c_uint32]),
+    "rt_sixv_cftp": (ctypes.c_int, [_P, _I32, _I64, _I64, _I32, _P, ctypes.POINTER(RtCftpStats)]),
+})
+
 _lib = None
 
 

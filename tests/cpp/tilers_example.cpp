@@ -27,6 +27,8 @@ int main(int argc, char** argv) {
         rt::tiling cone = rt::TriangleDimerTiler::IceCreamCone(10, 3);
         save(f, "cone", cone);
         if (argc > 3) rt::LozengeTiler::TilingToSVG(t, argv[3]);
+        save(f, "sixv_max", rt::SixVertexTiler::MaxHeights(6));
+        save(f, "sixv_asm_max", rt::SixVertexTiler::HeightsToASM(rt::SixVertexTiler::MaxHeights(6)));
         rt::domain a = rt::DominoTiler::AztecDiamond(12);
         rt::tiling m = rt::DominoTiler::MinTiling(a);
         save(f, "aztec_min", m);
@@ -48,6 +50,11 @@ int main(int argc, char** argv) {
             W.SetWeights(2, {1.0, 0.3, 0.5, 2.0}, {0.7, 1.5, 1.0, 0.2});
             W.Walk(m2, steps, seeds);
             save(f, "aztec_weighted", m2);
+            rt::SixVertexTiler S(0);
+            rt::heightfunc sh = rt::SixVertexTiler::MinHeights(20);
+            S.Walk(sh, 300, 5);
+            save(f, "sixv_walk", sh);
+            save(f, "sixv_cftp", S.CFTP(8, 8, 3));
             rt::TriangleDimerTiler T(0);
             T.Walk(cone, 800, 9);
             save(f, "cone_walk", cone);

@@ -45,6 +45,9 @@ def test_cpp_layer_builders(tmp_path):
     assert np.array_equal(got["lozenge_hmax"], b["lozenge/hex10_2/hmax"])
     d = b["domino/aztec13/domain"]
     assert got["aztec_min"].size == (2 * 12 + 6) ** 2 and d.size == (2 * 13 + 5) ** 2
+    lo, hi = po.sixv_dwbc(6)
+    assert np.array_equal(got["sixv_max"], hi)
+    assert np.array_equal(got["sixv_asm_max"].reshape(6, 6), np.fliplr(np.eye(6, dtype=np.int64)))
 
 
 @pytest.mark.gpu
@@ -59,6 +62,8 @@ def test_cpp_layer_walks(tmp_path):
     assert np.array_equal(got["cone_walk"], po.tridimer_walk(b["tridimer/cone10_3/tiling"], 800, 9))
     assert np.array_equal(got["aztec_epochs"],
                           po.domino_walk_epochs(got["aztec_min"], [256, 128], [2718281, 345903], cftp=True))
+    assert np.array_equal(got["sixv_walk"], po.sixv_walk(po.sixv_dwbc(20)[0], 300, 5))
+    assert np.array_equal(got["sixv_cftp"], po.sixv_cftp(8, 8, 3)[0])
     wh, wv = np.array([[1.0, 0.3], [0.5, 2.0]]), np.array([[0.7, 1.5], [1.0, 0.2]])
     assert np.array_equal(got["aztec_weighted"],
                           po.domino_walk_weighted(got["aztec_min"], [256, 128], [2718281, 345903], wh, wv))
