@@ -77,8 +77,8 @@ const char* rt_batch_last_error(rt_batch* b);
  * std::mt19937(seed) through std::uniform_int_distribution<int>:
  *   0: domino, Aztec diamond of order n in [16, 256]           p = {n}
  *   1: lozenge, hexagon with sides a, b, c each in [8, 128]       p = {a, b, c}
- *   2: triangle dimer, IceCreamCone(64, 1) (side 64; the
- *      reference builds no other triangle-dimer domain)          p = {64, 1}
+ *   2: triangle dimer, bibone hexagon of side 64 with its
+ *      canonical start (rt_tridimer_hexagon)                      p = {64}
  *   3: rectangle-triangle, minimal tiling of the side-64 hexagon p = {64}
  * Writes the model to *model and its size parameters to p[0..2]. */
 rt_status rt_mixed_chain_spec(int64_t seed, int32_t* model, int32_t* p);

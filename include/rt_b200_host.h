@@ -77,6 +77,18 @@ rt_status rt_recttri_from_lozenge(const int32_t* tl, int64_t tlen, const int32_t
 /* ---- triangular-lattice dimers (src/TriangleDimer/TriangleDimerTiler.h:182-195) ---- */
 /* TriangleDimerTiler::IceCreamCone(N, M), src/TriangleDimer/TriangleDimerTiler.cpp:485-581 */
 rt_status rt_tridimer_ice_cream_cone(int32_t side, int32_t cut, int32_t* out, int64_t cap, int64_t* len);
+/* No reference counterpart (the reference builds only IceCreamCone): a
+ * "bibone" hexagon -- the triangular-lattice vertices (x, y), 0 <= x, y <= 2s,
+ * s <= x + y <= 3s (a hexagon of side s edges, 3s(s+1) + 1 vertices: always
+ * odd) without its top-left corner (0, s), so that dimers can cover it --
+ * with its canonical start: row by row from the top, a row whose count of
+ * free vertices is odd pairs one end vertex with the same end of the next
+ * row (the right end, unless the row above took that one), and the rest of
+ * the row is paired horizontally from the left.  Vertex (x, y) sits at
+ * (x + 3, y + 3) of the eSize = 2s + 8 vertex grid, so the tiling is N x N
+ * with N = 4s + 16 and the three outer rows and columns the walk needs stay
+ * empty.  1 <= side <= 4096. */
+rt_status rt_tridimer_hexagon(int32_t side, int32_t* out, int64_t cap, int64_t* len);
 /* TriangleDimerTiler::TestButterfly(type), :583-632 */
 rt_status rt_tridimer_test_butterfly(int32_t kind, int32_t* out, int64_t cap, int64_t* len);
 /* TriangleDimerTiler::TilingToTriangleFlips / TilingToButterflyFlips, :634-709 */

@@ -138,6 +138,7 @@ HOST_SIGNATURES = {
     "rt_recttri_from_lozenge": [_P, _I64, _P, _I64],
     "rt_tridimer_ice_cream_cone": [_I32, _I32],
     "rt_tridimer_test_butterfly": [_I32],
+    "rt_tridimer_hexagon": [_I32],
     "rt_tridimer_triangle_flips": [_P, _I64],
     "rt_tridimer_butterfly_flips": [_P, _I64],
     "rt_tridimer_vertices": [_P, _I64],

@@ -736,6 +736,49 @@ rt_status rt_tridimer_ice_cream_cone(int32_t side, int32_t cut, int32_t* out, in
     return emit(td_tiles_from_edges(h, l, r, e), out, cap, len);
 }
 
+rt_status rt_tridimer_hexagon(int32_t side, int32_t* out, int64_t cap, int64_t* len) {
+    // Edges in the encoding of the IceCreamCone builder: h(i, j) joins (i, j)
+    // and (i, j+1), l(i, j) joins (i, j) and (i+1, j), r(i, j) joins (i, j+1)
+    // and (i+1, j) (the neighbours TilingToVertices reads, :711-737).
+    if (side < 1 || side > 4096) return RT_E_INVAL;
+    const int s = side, e = 2 * s + 8, off = 3;
+    Vec h((size_t)e * e, 0), l((size_t)e * e, 0), r((size_t)e * e, 0);
+    auto lo_y = [&](int x) { return std::max(0, s - x) + (x == 0 ? 1 : 0); };  // corner (0, s) removed
+    auto hi_y = [&](int x) { return std::min(2 * s, 3 * s - x); };
+    auto at = [&](int x, int y) { return (size_t)(x + off) * e + (y + off); };
+    // A row whose count of free vertices is odd pairs one end vertex with the
+    // matching end of the next row: the right end unless the row above took
+    // that one, then the left end -- so every row's free vertices stay one
+    // run, paired horizontally from the left.
+    int taken = 0;  // end of this row already paired with the row above: 0 none, 1 left, 2 right
+    for (int x = 0; x <= 2 * s; ++x) {
+        const int above = taken;
+        int a = lo_y(x) + (above == 1), b = hi_y(x) - (above == 2);
+        taken = 0;
+        if ((b - a + 1) % 2 != 0) {
+            if (x == 2 * s) return RT_E_STATE;  // unreachable: the vertex count is even
+            if (above == 2) {
+                // left end (x, a) with the first vertex of the next row
+                const int t = lo_y(x + 1);
+                if (t == a) l[at(x, a)] = 1;
+                else if (t == a - 1) r[at(x, a - 1)] = 1;
+                else return RT_E_STATE;
+                taken = 1;
+                ++a;
+            } else {
+                const int t = hi_y(x + 1);
+                if (t == b) l[at(x, b)] = 1;
+                else if (t == b - 1) r[at(x, b - 1)] = 1;
+                else return RT_E_STATE;
+                taken = 2;
+                --b;
+            }
+        }
+        for (int y = a; y < b; y += 2) h[at(x, y)] = 1;
+    }
+    return emit(td_tiles_from_edges(h, l, r, e), out, cap, len);
+}
+
 rt_status rt_tridimer_test_butterfly(int32_t kind, int32_t* out, int64_t cap, int64_t* len) {
     // One butterfly of orientation H (0), L (1) or R (2) (TriangleDimerTiler.cpp:334-383).
     if (kind < 0 || kind > 2) return RT_E_INVAL;
@@ -923,10 +966,9 @@ extern "C" rt_status rt_mixed_chain_spec(int64_t seed, int32_t* model, int32_t* 
             p[2] = side(mt);
             break;
         }
-        case 2:
+        case 2:  // bibone hexagon of side 64 (rt_tridimer_hexagon)
             *model = RT_TRIDIMER;
             p[0] = 64;
-            p[1] = 1;
             break;
         default:
             *model = RT_RECTTRI;

@@ -258,6 +258,8 @@ class TriangleDimerTiler(_Tiler):
     # static helpers (src/TriangleDimer/TriangleDimerTiler.h:182-195)
     IceCreamCone = staticmethod(lambda n, m: builders.call("rt_tridimer_ice_cream_cone", n, m))
     TestButterfly = staticmethod(lambda k: builders.call("rt_tridimer_test_butterfly", k))
+    # no reference counterpart: a hexagon of side s edges less one corner, canonical start (rt_b200_host.h)
+    BiboneHexagon = staticmethod(lambda s: builders.call("rt_tridimer_hexagon", s))
     TilingToTriangleFlips = staticmethod(lambda t: builders.call("rt_tridimer_triangle_flips", t))
     TilingToButterflyFlips = staticmethod(lambda t: builders.call("rt_tridimer_butterfly_flips", t))
     TilingToVertices = staticmethod(lambda t: builders.call("rt_tridimer_vertices", t))

@@ -19,13 +19,15 @@ def mixed_chain_spec(seed: int) -> tuple[int, list[int]]:
 
 
 def start_tiling(model: int, p: list[int]):
-    """Minimal tiling of the domain (p as mixed_chain_spec returns it)."""
+    """Minimal tiling of the domain (p as mixed_chain_spec returns it); for the
+    triangle dimers, which have no height function, the bibone hexagon's
+    canonical start."""
     if model == _capi.RT_DOMINO:
         return DominoTiler.MinTiling(DominoTiler.AztecDiamond(p[0]))
     if model == _capi.RT_LOZENGE:
         return LozengeTiler.MinTiling(LozengeTiler.Hexagon(p[0], p[1], p[2]))
     if model == _capi.RT_TRIDIMER:
-        return TriangleDimerTiler.IceCreamCone(p[0], p[1])
+        return TriangleDimerTiler.BiboneHexagon(p[0])
     return RectTriangleTiler.minHex(p[0])
 
 

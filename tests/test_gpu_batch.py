@@ -29,6 +29,7 @@ def _chains(rt):
         (R, 0, b["recttri/max_hex20"], 17, "recttri"),
         (T, 0, rt.TriangleDimerTiler.IceCreamCone(12, 0), 18, "tridimer"),
         (T, 0, rt.TriangleDimerTiler.IceCreamCone(25, 7), 19, "tridimer"),
+        (T, 0, rt.TriangleDimerTiler.BiboneHexagon(7), 20, "tridimer"),
     ]
 
 
