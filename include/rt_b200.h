@@ -190,8 +190,10 @@ rt_status rt_last_run_info(rt_tiler* h, int64_t* phases, int64_t* launches);
  * (tiling side x steps) are rejected with RT_E_INVAL.  The first call on a
  * device looks the array up on that device; make it before any stream
  * capture.  Calls share the array: calls that overlap on one GPU race.
- * Synchronous on cfg->stream (NULL = the default stream).  A failure message
- * goes to errbuf (errcap bytes) when errbuf is not NULL. */
+ * Runs on cfg->stream (NULL = the default stream) and returns after the walk
+ * has finished there.  The tiling is written back only after a walk that
+ * finished: after RT_E_INVAL or RT_E_TIMEOUT it holds its input unchanged.
+ * A failure message goes to errbuf (errcap bytes) when errbuf is not NULL. */
 rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_tiling, int32_t n, int64_t steps, int64_t seed,
                                  char* errbuf, size_t errcap);
 

@@ -140,6 +140,17 @@ void fast_phases(int kind, int64_t steps, std::vector<uint32_t>& ph) {
     ph.resize((size_t)at);
 }
 
+rt_status choose_plan(int family, int device, int nlat, int rows, int cols, int width, bool uniform, bool fast,
+                      bool planes, bool weighted, int kernel_choice, int ctas_hint, int depth_hint, WalkPlan* plan,
+                      std::string* err) {
+    if (planes) return plan_plane_walk(family, device, nlat, rows, width, ctas_hint, depth_hint, plan, err);
+    rt_status s = RT_E_INVAL;
+    if (kernel_choice != 1 && uniform && word_family(family))
+        s = plan_word_walk(family, device, nlat, rows, width, fast, ctas_hint, plan, err, weighted);
+    if (s == RT_OK || kernel_choice == 2) return s;
+    return plan_walk(family, device, nlat, rows, cols, width, uniform, fast, plan, err);
+}
+
 void family_thresholds(int family, double q, int qcmp, uint32_t thr[4]) {
     thr[0] = thr[1] = thr[2] = thr[3] = 0;
     switch (family) {
@@ -654,20 +665,8 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     const bool weighted = h->wper > 0;
     if (h->plan_rows != h->rows || h->plan_cols != h->cols || h->plan_nlat != h->nlat || h->plan_uniform != uniform ||
         h->plan_weighted != weighted) {
-        // The word kernel serves the int8 models with uniform generator
-        // parameters; everything else (and any band it cannot hold) runs on
-        // the generic walk kernel.  Bit-plane mode has its own kernel.
-        rt_status s = RT_E_INVAL;
-        if (planes) {
-            s = plan_plane_walk(h->family, h->cfg.device, h->nlat, h->rows, width, h->ctas_hint, h->depth_hint,
-                                &h->plan, &h->err);
-            if (s != RT_OK) return s;
-        } else if (h->kernel_choice != 1 && uniform && word_family(h->family))
-            s = plan_word_walk(h->family, h->cfg.device, h->nlat, h->rows, width, fast, h->ctas_hint, &h->plan,
-                               &h->err, weighted);
-        if (s != RT_OK && h->kernel_choice == 2) return s;
-        if (s != RT_OK)
-            s = plan_walk(h->family, h->cfg.device, h->nlat, h->rows, h->cols, width, uniform, fast, &h->plan, &h->err);
+        rt_status s = choose_plan(h->family, h->cfg.device, h->nlat, h->rows, h->cols, width, uniform, fast, planes,
+                                  weighted, h->kernel_choice, h->ctas_hint, h->depth_hint, &h->plan, &h->err);
         if (s != RT_OK) return s;
         h->plan_rows = h->rows;
         h->plan_cols = h->cols;

@@ -48,6 +48,14 @@ rt_status plan_word_walk(int family, int device, int nlat, int rows, int width, 
 // ctas_hint / depth_hint <= 0: one CTA per SM / the largest depth up to 8.
 rt_status plan_plane_walk(int family, int device, int nlat, int rows, int width, int ctas_hint, int depth_hint,
                           WalkPlan* plan, std::string* err);
+// The kernel a walk runs on, as every walk entry point chooses it: the
+// bit-plane kernel in RT_RNG_PLANES mode; otherwise the word kernel for the
+// int8 models with uniform generator parameters (unless kernel_choice = 1),
+// falling back to the generic walk kernel for every other case and for any
+// band the word kernel cannot hold (kernel_choice = 2 forbids the fallback).
+rt_status choose_plan(int family, int device, int nlat, int rows, int cols, int width, bool uniform, bool fast,
+                      bool planes, bool weighted, int kernel_choice, int ctas_hint, int depth_hint, WalkPlan* plan,
+                      std::string* err);
 // kind: 0 domino, 1 lozenge, 2 rect-triangle, 3 triangle-dimer (merge only).
 rt_status launch_split(bool merge, int elem_bytes, int kind, int ncol, int n, int32_t* tiling, void* const* arr,
                        cudaStream_t stream, std::string* err);

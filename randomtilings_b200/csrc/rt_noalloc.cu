@@ -70,15 +70,6 @@ rt_status scratch_on(int dev, unsigned char** out, char* eb, size_t ec) {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-uint32_t below(double x) {  // smallest K with (k * 2^-23 < x) <=> (k < K)
-    const double s = std::ceil(x * 8388608.0);
-    return s <= 0 ? 0u : s >= 4294967295.0 ? 0xffffffffu : (uint32_t)s;
-}
-uint32_t floor_scaled(double x, int e) {
-    const double s = std::floor(std::ldexp(x, e));
-    return s <= 0 ? 0u : s >= 4294967295.0 ? 0xffffffffu : (uint32_t)s;
-}
-
 }  // namespace
 
 extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_tiling, int32_t n, int64_t steps,
@@ -86,6 +77,13 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
     if (errbuf && errcap) errbuf[0] = '\0';
     if (!cfg || !d_tiling || steps < 0) {
         say(errbuf, errcap, "null configuration or tiling, or negative step count");
+        return RT_E_INVAL;
+    }
+    // One 4-byte phase per step lives in the array: larger step counts can
+    // never fit, and bounding them first keeps the size arithmetic below exact.
+    if (steps > (int64_t)(kScratchBytes / 4) - 1) {
+        say(errbuf, errcap, "%lld steps do not fit the built-in %zu-byte scratch array", (long long)steps,
+            kScratchBytes);
         return RT_E_INVAL;
     }
     int family = -1, ncol = 0, kind = 0, elem = 1;
@@ -108,6 +106,11 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
     }
     if ((kind == 0 && (n < 6 || n % 2 != 0)) || (kind != 0 && (n < 9 || n % 3 != 0))) {
         say(errbuf, errcap, "tiling side %d not allowed for this model", (int)n);
+        return RT_E_INVAL;
+    }
+    // The colour arrays alone (n x n bytes at least) must fit the array.
+    if ((int64_t)n * n > (int64_t)kScratchBytes) {
+        say(errbuf, errcap, "tiling side %d does not fit the built-in %zu-byte scratch array", (int)n, kScratchBytes);
         return RT_E_INVAL;
     }
     int ndev = 0;
@@ -140,7 +143,9 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
     }
     std::string perr;  // filled only on a failure path
     WalkPlan plan;
-    s = plan_walk(family, cfg->device, 1, rows, cols, width, true, false, &plan, &perr);
+    // The kernel rt_walk would run for this walk (word kernel for the int8
+    // models, the generic walk kernel otherwise).
+    s = choose_plan(family, cfg->device, 1, rows, cols, width, true, false, false, false, 0, 0, 0, &plan, &perr);
     if (s != RT_OK) {
         say(errbuf, errcap, "%s", perr.c_str());
         return s;
@@ -152,7 +157,7 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
     const size_t off_ph = per_arr * ncol;
     const size_t off_ep = off_ph + align256((size_t)nph * 4);
     const size_t off_x = off_ep + 256;
-    const size_t xbytes = (size_t)plan.ctas * 2 * 2 * plan.xwords * sizeof(unsigned long long);
+    const size_t xbytes = (size_t)plan.ctas * 2 * 2 * plan.xslots * plan.xwords * sizeof(unsigned long long);
     const size_t off_err = off_x + align256(xbytes);
     const size_t need = off_err + 256;
     if (need > kScratchBytes) {
@@ -245,22 +250,7 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
         a.epoch_start = reinterpret_cast<const int64_t*>(base + off_ep);
         a.epoch_seed = reinterpret_cast<const uint64_t*>(base + off_ep + 8);
         a.nepochs = 1;
-        switch (family) {
-            case FAM_DOMINO: a.thr[0] = below(0.8); break;
-            case FAM_DOMINO_HB: a.thr[0] = below(0.5); break;
-            case FAM_LOZENGE8: a.thr[0] = below(0.4), a.thr[1] = below(0.8); break;
-            case FAM_QLOZENGE32:
-                if (cfg->qcmp == RT_QCMP_DOUBLE) {
-                    a.thr[0] = floor_scaled(cfg->q, 22);
-                    a.thr[1] = floor_scaled(1.0 / cfg->q, 24);
-                } else {
-                    const float qf = (float)cfg->q;
-                    a.thr[0] = floor_scaled((double)qf, 22);
-                    a.thr[1] = floor_scaled((double)(1.0f / qf), 24);
-                }
-                break;
-            default: break;
-        }
+        family_thresholds(family, cfg->q, cfg->qcmp, a.thr);
         std::memcpy(a.weights, cfg->weights, sizeof a.weights);
         a.xbuf = reinterpret_cast<unsigned long long*>(base + off_x);
         a.err = reinterpret_cast<int*>(base + off_err);
@@ -271,18 +261,13 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
             say(errbuf, errcap, "%s", perr.c_str());
             return s;
         }
-    }
-    s = launch_split(true, elem, kind, ncol, n, d_tiling, arr, stream, &perr);
-    if (s != RT_OK) {
-        say(errbuf, errcap, "%s", perr.c_str());
-        return s;
-    }
-    e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess) {
-        say(errbuf, errcap, "walk failed: %s", cudaGetErrorString(e));
-        return RT_E_CUDA;
-    }
-    if (nph > 0) {
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) {
+            say(errbuf, errcap, "walk failed: %s", cudaGetErrorString(e));
+            return RT_E_CUDA;
+        }
+        // The caller's tiling is written back only after a walk that finished:
+        // a walk stopped by a timed-out wait leaves it as it was.
         int code = 0;
         e = cudaMemcpy(&code, base + off_err, sizeof code, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) {
@@ -297,6 +282,16 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
             say(errbuf, errcap, "device error word %d", code);
             return RT_E_CUDA;
         }
+    }
+    s = launch_split(true, elem, kind, ncol, n, d_tiling, arr, stream, &perr);
+    if (s != RT_OK) {
+        say(errbuf, errcap, "%s", perr.c_str());
+        return s;
+    }
+    e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        say(errbuf, errcap, "merge failed: %s", cudaGetErrorString(e));
+        return RT_E_CUDA;
     }
     return RT_OK;
 }

@@ -58,7 +58,10 @@ def test_noalloc_walk_matches_rt_walk_twice(model, kernel, key):
     ref.close()
 
 
-def test_noalloc_rejects_walks_beyond_its_scratch():
+@pytest.mark.parametrize("steps", [10_000_000, 1 << 62, (1 << 63) - 1])
+def test_noalloc_rejects_walks_beyond_its_scratch(steps):
+    """Step counts whose schedule cannot fit the built-in array, up to the
+    largest int64, are refused before anything touches the tiling."""
     import torch
 
     from randomtilings_b200 import _capi
@@ -70,7 +73,7 @@ def test_noalloc_rejects_walks_beyond_its_scratch():
     n = int(round(t0.size ** 0.5))
     dev = torch.from_numpy(t0.copy()).cuda()
     buf = ctypes.create_string_buffer(512)
-    st = lib.rt_walk_device_noalloc(ctypes.byref(cfg), ctypes.c_void_p(dev.data_ptr()), n, 10_000_000, 1, buf,
+    st = lib.rt_walk_device_noalloc(ctypes.byref(cfg), ctypes.c_void_p(dev.data_ptr()), n, steps, 1, buf,
                                     len(buf))
     assert st == _capi.RT_E_INVAL
     assert b"scratch" in buf.value
