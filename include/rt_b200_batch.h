@@ -10,9 +10,9 @@
  * (Philox4x32-10, cyclic colours; see rt_b200.h), so chain c with key k gives
  * the tiling that rt_walk gives for a handle created with rng = RT_RNG_PHILOX
  * and chain = c, run with seed k for the same number of colour steps.
- * Cluster size and CTA size per family are picked by an autotuner that times
- * candidate plans on a scratch copy of the chains (the chains themselves are
- * not advanced).
+ * Cluster size and CTA size per family, and then the number of sweeps one
+ * launch runs, are picked by an autotuner that times candidate plans on a
+ * scratch copy of the chains (the chains themselves are not advanced).
  */
 #ifndef RT_B200_BATCH_H
 #define RT_B200_BATCH_H
@@ -46,6 +46,8 @@ typedef struct {
     double run_ms;            /* device time of the last rt_batch_run (graph launch to end) */
     int64_t attempts;         /* flip attempts in the last rt_batch_run (all chains) */
     int64_t algorithmic_bytes;/* lattice bytes read + written per colour step, summed over the last run */
+    int64_t sweeps_per_launch[6]; /* per family: a run of S sweeps is S / this launches (+ one for the rest);
+                                     0 = one launch per run */
 } rt_batch_info;
 
 rt_status rt_batch_create(int32_t device, rt_batch** out);
@@ -63,6 +65,11 @@ rt_status rt_batch_set_tuning(rt_batch* b, int32_t autotune, int32_t cluster, in
  * rectangle-triangles, 30 for triangle dimers.  Synchronous.  The Philox step
  * counter continues across runs (a run of s1 sweeps then one of s2 equals a
  * run of s1 + s2). */
+/* Sweeps one launch of a family runs (a run of S sweeps becomes S / sweeps
+ * launches plus one for the rest, each continuing the chains' draws), for
+ * every family: > 0 fixes it, 0 asks for one launch per run, -1 (the
+ * default) lets the autotuner choose. */
+rt_status rt_batch_set_sweeps_per_launch(rt_batch* b, int64_t sweeps);
 rt_status rt_batch_run(rt_batch* b, int64_t sweeps);
 rt_status rt_batch_download(rt_batch* b, int64_t index, int32_t* tiling);
 /* Device form of rt_batch_download: chain `index`'s N x N tiling into the

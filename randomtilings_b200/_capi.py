@@ -82,6 +82,7 @@ class RtBatchInfo(ctypes.Structure):
         ("run_ms", ctypes.c_double),
         ("attempts", ctypes.c_int64),
         ("algorithmic_bytes", ctypes.c_int64),
+        ("sweeps_per_launch", ctypes.c_int64 * 6),
     ]
 
 _P = ctypes.c_void_p
@@ -176,6 +177,7 @@ SIGNATURES.update({
     "rt_batch_add": (ctypes.c_int, [_P, ctypes.POINTER(RtChain), _P, _I32, _PL]),
     "rt_batch_set_tuning": (ctypes.c_int, [_P, _I32, _I32, _I32]),
     "rt_batch_run": (ctypes.c_int, [_P, _I64]),
+    "rt_batch_set_sweeps_per_launch": (ctypes.c_int, [_P, _I64]),
     "rt_batch_download": (ctypes.c_int, [_P, _I64, _P]),
     "rt_batch_device_tiling": (ctypes.c_int, [_P, _I64, _P, _P]),
     "rt_batch_get_info": (ctypes.c_int, [_P, ctypes.POINTER(RtBatchInfo)]),

@@ -65,6 +65,10 @@ class Batch:
     def set_tuning(self, autotune: bool = True, cluster: int = 0, block: int = 0) -> None:
         self._check(self._lib.rt_batch_set_tuning(self._h, int(autotune), cluster, block))
 
+    def set_sweeps_per_launch(self, sweeps: int) -> None:
+        """> 0: launches of that many sweeps; 0: one launch per run; -1: the autotuner chooses."""
+        self._check(self._lib.rt_batch_set_sweeps_per_launch(self._h, int(sweeps)))
+
     def run(self, sweeps: int) -> None:
         self._check(self._lib.rt_batch_run(self._h, int(sweeps)))
 
@@ -81,7 +85,8 @@ class Batch:
     def info(self) -> dict:
         i = _capi.RtBatchInfo()
         self._check(self._lib.rt_batch_get_info(self._h, ctypes.byref(i)))
-        plans = {FAMILY_NAMES[f]: {"cluster": i.cluster[f], "block": i.block[f], "clusters": i.clusters[f]}
+        plans = {FAMILY_NAMES[f]: {"cluster": i.cluster[f], "block": i.block[f], "clusters": i.clusters[f],
+                                   "sweeps_per_launch": i.sweeps_per_launch[f]}
                  for f in range(6) if i.cluster[f]}
         return {"chains": i.chains, "plans": plans, "tune_ms": i.tune_ms, "run_ms": i.run_ms,
                 "attempts": i.attempts, "algorithmic_bytes": i.algorithmic_bytes}

@@ -47,6 +47,7 @@ struct BatchArgs {
     const uint32_t* phases;
     int64_t nphases;
     const int64_t* step0;  // colour steps the chains have already made (Philox step counter offset)
+    int64_t step_add;      // colour steps of this run made by the family's earlier launches in it
     uint32_t thr[4];
     float weights[16];
 };
@@ -125,7 +126,7 @@ __global__ void __launch_bounds__(1024, 1) batch_word_kernel(const __grid_consta
         __syncthreads();
 
         const uint32_t key0 = (uint32_t)ch.key, key1 = (uint32_t)(ch.key >> 32);
-        int64_t dstep = *b.step0;
+        int64_t dstep = *b.step0 + b.step_add;
         const int nwords = nrows * Gw;
         const int drr = BLOCK / Gw, dw = BLOCK - drr * Gw;
         for (int64_t ph = 0; ph < b.nphases; ++ph) {
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(1024, 1) batch_site_kernel(const __grid_consta
         __syncthreads();
 
         const uint32_t key0 = (uint32_t)ch.key, key1 = (uint32_t)(ch.key >> 32);
-        int64_t dstep = *b.step0;
+        int64_t dstep = *b.step0 + b.step_add;
         const int Gw = (width + 3) >> 2;
         const int qlo = Model::COFF >> 2;
         const int G = ((Model::COFF + cols - 1) >> 2) - qlo + 1;
@@ -379,7 +380,7 @@ __global__ void __launch_bounds__(1024, 1) batch_td_kernel(const __grid_constant
         __syncthreads();
 
         const uint32_t key0 = (uint32_t)ch.key, key1 = (uint32_t)(ch.key >> 32);
-        int64_t dstep = *b.step0;
+        int64_t dstep = *b.step0 + b.step_add;
         for (int64_t ph = 0; ph < b.nphases; ++ph) {
             const uint32_t d = __ldg(b.phases + ph);
             const bool draws = (d & PH_DRAWS) != 0u;
@@ -531,14 +532,16 @@ struct Dev {
 struct Plan {
     int cl = 1, block = 256, clusters = 1;
     size_t smem = 0;
+    int64_t spl = 0;  // sweeps per launch: a run of S sweeps is S / spl launches (+ one for the rest); 0 = one
 };
 
 struct FamilyState {
     std::vector<int> members;  // chain indices
     std::vector<int> order;    // members sorted by lattice size, largest first (as indices into members)
     size_t bytes = 0;
-    Dev data, recs, ord, phases, scratch, scratch_recs, step0;
-    int64_t nphases = 0, phases_sweeps = -1;
+    Dev data, recs, ord, phases, phases2, scratch, scratch_recs, step0;
+    int64_t nphases = 0, phases_sweeps = -1;    // phases: one launch's sweeps
+    int64_t nphases2 = 0, phases2_sweeps = -1;  // phases2: the last launch's, when shorter
     Plan plan;
     bool planned = false;
     double work = 0;  // relative cost of a sweep of the whole family (launch order)
@@ -583,6 +586,7 @@ struct rt_batch {
     FamilyState fam[kFamilies];
     bool uploaded = false;
     int autotune = 1, force_cl = 0, force_block = 0;
+    int64_t force_spl = -1;  // sweeps per launch set by the caller (-1: the autotuner's, or one launch)
     double tune_ms = 0, run_ms = 0;
     int64_t last_attempts = 0, last_bytes = 0;
     int64_t sweeps_done = 0;       // sweeps every chain has made so far
@@ -605,16 +609,19 @@ namespace {
 
 thread_local std::string g_batch_create_error;
 
-BatchArgs args_for(rt_batch* b, int f, const void* recs) {
+// rest: the launch runs the shorter phase list (the last launch of a run
+// whose sweeps the plan's sweeps per launch do not divide).
+BatchArgs args_for(rt_batch* b, int f, const void* recs, int64_t step_add = 0, bool rest = false) {
     FamilyState& F = b->fam[f];
     BatchArgs a;
     std::memset(&a, 0, sizeof a);
     a.chains = static_cast<const BatchChain*>(recs);
     a.order = static_cast<const int*>(F.ord.p);
     a.nchains = (int)F.members.size();
-    a.phases = static_cast<const uint32_t*>(F.phases.p);
-    a.nphases = F.nphases;
+    a.phases = static_cast<const uint32_t*>(rest ? F.phases2.p : F.phases.p);
+    a.nphases = rest ? F.nphases2 : F.nphases;
     a.step0 = static_cast<const int64_t*>(F.step0.p);
+    a.step_add = step_add;
     family_thresholds(f, 0.99, RT_QCMP_FLOAT32, a.thr);
     a.weights[0] = 0.0f;  // recttrianglekernel.cl:13
     for (int i = 1; i < 16; ++i) a.weights[i] = 1.0f;
@@ -622,9 +629,10 @@ BatchArgs args_for(rt_batch* b, int f, const void* recs) {
 }
 
 // priority: a CUDA stream priority (lower = scheduled first); 0 = default.
-rt_status launch_family(rt_batch* b, int f, const Plan& p, const void* recs, cudaStream_t s, int priority = 0) {
+rt_status launch_family(rt_batch* b, int f, const Plan& p, const void* recs, cudaStream_t s, int priority = 0,
+                        int64_t step_add = 0, bool rest = false) {
     BatchFn fn = batch_fn(f);
-    BatchArgs a = args_for(b, f, recs);
+    BatchArgs a = args_for(b, f, recs, step_add, rest);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(p.clusters * p.cl));
     cfg.blockDim = dim3((unsigned)p.block);
@@ -686,17 +694,33 @@ bool fill_plan(rt_batch* b, int f, int cl, int block, Plan* p) {
     return true;
 }
 
-rt_status stage_phases(rt_batch* b, int f, int64_t sweeps) {
+// The phase list of a launch of `sweeps` sweeps, into the family's first
+// (rest = false) or second list.  Launches compose: each ends with the last
+// colour's Update and the next starts with no Update pending, the same
+// sequence of site updates as one longer launch.
+rt_status stage_phases(rt_batch* b, int f, int64_t sweeps, bool rest = false) {
     FamilyState& F = b->fam[f];
-    if (F.phases_sweeps == sweeps) return RT_OK;
+    int64_t& have = rest ? F.phases2_sweeps : F.phases_sweeps;
+    if (have == sweeps) return RT_OK;
     std::vector<uint32_t> ph;
     fast_phases(kind_of(f), sweeps * steps_per_sweep(kind_of(f)), ph);
-    if (!F.phases.reserve(std::max<size_t>(4, ph.size() * 4))) return b->fail(RT_E_NOMEM, "phase list");
-    cudaError_t e = cudaMemcpy(F.phases.p, ph.data(), ph.size() * 4, cudaMemcpyHostToDevice);
+    Dev& buf = rest ? F.phases2 : F.phases;
+    if (!buf.reserve(std::max<size_t>(4, ph.size() * 4))) return b->fail(RT_E_NOMEM, "phase list");
+    cudaError_t e = cudaMemcpy(buf.p, ph.data(), ph.size() * 4, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("phase upload: ") + cudaGetErrorString(e));
-    F.nphases = (int64_t)ph.size();
-    F.phases_sweeps = sweeps;
+    (rest ? F.nphases2 : F.nphases) = (int64_t)ph.size();
+    have = sweeps;
     return RT_OK;
+}
+
+// Launches of a run of `sweeps` sweeps under sweeps-per-launch spl:
+// (full launches, sweeps each, sweeps of the last shorter launch or 0).
+struct LaunchSplit {
+    int64_t full, per, rest;
+};
+LaunchSplit split_run(int64_t sweeps, int64_t spl) {
+    if (spl <= 0 || spl >= sweeps) return {1, sweeps, 0};
+    return {sweeps / spl, spl, sweeps % spl};
 }
 
 // Chain records whose arrays live at `base` (the family buffer or its scratch copy).
@@ -813,6 +837,7 @@ rt_status plan_family(rt_batch* b, int f) {
                 }
             if (!ok) return b->fail(RT_E_INVAL, "no cluster size holds the largest chain of a family in shared memory");
         }
+        p.spl = b->force_spl > 0 ? b->force_spl : 0;
         F.plan = p;
         F.planned = true;
         return RT_OK;
@@ -825,6 +850,7 @@ rt_status plan_family(rt_batch* b, int f) {
     if (cand.empty()) return b->fail(RT_E_INVAL, "no cluster size holds the largest chain of a family in shared memory");
     if (cand.size() == 1) {
         F.plan = cand[0];
+        F.plan.spl = b->force_spl > 0 ? b->force_spl : 0;
         F.planned = true;
         return RT_OK;
     }
@@ -856,6 +882,32 @@ rt_status plan_family(rt_batch* b, int f) {
             F.plan = p;
         }
     }
+    // Sweeps per launch at the chosen shape: a run of 32 sweeps as one
+    // launch, against four launches of 8 (each reloading the lattices from
+    // global memory, with its own tail of uneven chains).
+    cudaFuncSetAttribute((const void*)batch_fn(f), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F.plan.smem);
+    if ((s = stage_phases(b, f, 32)) != RT_OK || (s = stage_phases(b, f, 8, true)) != RT_OK) return s;
+    float best_spl = 1e30f;
+    for (const int64_t spl : {(int64_t)0, (int64_t)8}) {
+        cudaMemcpyAsync(F.scratch.p, F.data.p, F.bytes, cudaMemcpyDeviceToDevice, b->stream);
+        cudaEventRecord(b->t0, b->stream);
+        const int nl = spl == 0 ? 1 : 32 / (int)spl;
+        for (int k = 0; k < nl && s == RT_OK; ++k)
+            s = launch_family(b, f, F.plan, F.scratch_recs.p, b->stream, 0,
+                              (int64_t)k * 8 * steps_per_sweep(kind_of(f)), spl != 0);
+        if (s != RT_OK) return s;
+        cudaEventRecord(b->t1, b->stream);
+        cudaError_t e = cudaEventSynchronize(b->t1);
+        if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("autotuner run: ") + cudaGetErrorString(e));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, b->t0, b->t1);
+        if (ms < best_spl) {
+            best_spl = ms;
+            F.plan.spl = spl;
+        }
+    }
+    F.phases_sweeps = F.phases2_sweeps = -1;  // the run stages its own lists
+    if (b->force_spl >= 0) F.plan.spl = b->force_spl;
     F.planned = true;
     return RT_OK;
 }
@@ -972,6 +1024,15 @@ rt_status rt_batch_set_tuning(rt_batch* b, int32_t autotune, int32_t cluster, in
     return RT_OK;
 }
 
+rt_status rt_batch_set_sweeps_per_launch(rt_batch* b, int64_t sweeps) {
+    if (!b) return RT_E_INVAL;
+    if (sweeps < -1) return b->fail(RT_E_INVAL, "sweeps per launch must be >= -1");
+    b->force_spl = sweeps;
+    for (int f = 0; f < kFamilies; ++f) b->fam[f].planned = false;
+    b->drop_graph();
+    return RT_OK;
+}
+
 rt_status rt_batch_run(rt_batch* b, int64_t sweeps) {
     if (!b) return RT_E_INVAL;
     if (sweeps < 0) return b->fail(RT_E_INVAL, "negative sweep count");
@@ -991,9 +1052,13 @@ rt_status rt_batch_run(rt_batch* b, int64_t sweeps) {
     if (tuned)
         b->tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
     for (int f = 0; f < kFamilies; ++f) {
-        if (b->fam[f].members.empty()) continue;
-        if (b->fam[f].phases_sweeps != sweeps) b->drop_graph();
-        s = stage_phases(b, f, sweeps);
+        FamilyState& F = b->fam[f];
+        if (F.members.empty()) continue;
+        const LaunchSplit ls = split_run(sweeps, F.plan.spl);
+        if (F.phases_sweeps != ls.per || (ls.rest && F.phases2_sweeps != ls.rest) || b->exec_sweeps != sweeps)
+            b->drop_graph();
+        s = stage_phases(b, f, ls.per);
+        if (s == RT_OK && ls.rest) s = stage_phases(b, f, ls.rest, true);
         if (s != RT_OK) return s;
     }
     if (!b->exec) {
@@ -1031,9 +1096,12 @@ rt_status rt_batch_run(rt_batch* b, int64_t sweeps) {
         rt_status ls = RT_OK;
         for (int k = 0; k < nf && ls == RT_OK; ++k) {
             const int f = order[k];
+            const LaunchSplit sp = split_run(sweeps, b->fam[f].plan.spl);
+            const int64_t sps = steps_per_sweep(kind_of(f));
             cudaStreamWaitEvent(b->fam_stream[f], b->fork, 0);
-            ls = launch_family(b, f, b->fam[f].plan, b->fam[f].recs.p, b->fam_stream[f],
-                               k == 0 ? prio_high : prio_low);
+            for (int64_t l = 0; l < sp.full + (sp.rest ? 1 : 0) && ls == RT_OK; ++l)
+                ls = launch_family(b, f, b->fam[f].plan, b->fam[f].recs.p, b->fam_stream[f],
+                                   k == 0 ? prio_high : prio_low, l * sp.per * sps, l == sp.full);
             cudaEventRecord(b->join[f], b->fam_stream[f]);
             cudaStreamWaitEvent(b->stream, b->join[f], 0);
         }
@@ -1130,6 +1198,7 @@ rt_status rt_batch_get_info(rt_batch* b, rt_batch_info* info) {
         info->cluster[f] = b->fam[f].plan.cl;
         info->block[f] = b->fam[f].plan.block;
         info->clusters[f] = b->fam[f].plan.clusters;
+        info->sweeps_per_launch[f] = b->fam[f].plan.spl;
     }
     info->tune_ms = b->tune_ms;
     info->run_ms = b->run_ms;

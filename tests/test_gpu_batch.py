@@ -104,6 +104,21 @@ def test_batch_runs_compose(rt, singles):
         assert np.array_equal(got, singles[c])
 
 
+@pytest.mark.parametrize("spl", [3, 4])
+def test_sweeps_per_launch_compose(rt, singles, spl):
+    """A run split into launches of `spl` sweeps (plus one shorter launch for
+    the rest) equals the single-chain walks."""
+    bt = rt.Batch()
+    for model, kernel, t, key, _ in _chains(rt):
+        bt.add(model, t, key=key, chain=len(bt), kernel=kernel)
+    bt.set_sweeps_per_launch(spl)
+    bt.run(SWEEPS)
+    assert all(p["sweeps_per_launch"] == spl for p in bt.info()["plans"].values())
+    for c in range(len(bt)):
+        assert np.array_equal(bt.download(c), singles[c]), c
+    bt.close()
+
+
 def test_mixed_workload_chains(rt):
     """The first chains of the mixed benchmark workload (Aztec diamonds up to
     order 256 need 2-CTA clusters), two sweeps."""
