@@ -1,22 +1,31 @@
 """Benchmark of the bit-exact flip dynamics on the a=b=c=500 hexagon.
 
-Workload: lozenge tilings of the a=b=c=500 hexagon (LozengeTiler::AlmostHexDomain
-(500, 0) -> MinTiling, 1008 x 1008 tiling, 338,688 flip attempts per colour
-step), started from the minimal tiling, 20,000 sweeps = 60,000 reference colour
-steps per walk, TinyMT streams seeded from 42.  One bench "step" is one such
-walk.  Uniform weights (int8 storage) are the headline; the q = 0.99 int32
-walk (float32 comparison) is reported beside it.
+Workload (both arms): lozenge tilings of the a=b=c=500 hexagon
+(LozengeTiler::AlmostHexDomain(500, 0) -> MinTiling: a 1008 x 1008 tiling,
+338,688 flip attempts per colour step), started from the minimal tiling,
+TinyMT streams, uniform weights (int8 storage).  One bench step is one Walk
+call of 3,000 reference colour steps (1,000 sweeps) with seed 42 + k,
+continuing from the previous call's tiling; 20 steps are the 20,000-sweep
+walk.  After the warm-up steps the chain restarts from the minimal tiling, so
+the timed steps are always the same walk.
 
-  value : attempts/s with the lattice already resident on the device
-          (rt_upload outside the timed region; rt_run inside), CUDA events on
-          the library's stream, L2 flushed between walks;
-  e2e   : the same metric through rt_walk (the reference's Walk contract:
-          host int32 tiling in, host tiling out, H2D + split + walk + merge +
-          D2H every walk).
+  value : attempts/s with the lattice resident on the device (rt_upload before
+          the timed steps; rt_run per step), CUDA events on the library's
+          stream, L2 flushed (256 MiB write) before every step;
+  e2e   : the same steps through rt_walk (the reference's Walk contract: host
+          int32 tiling in pinned memory, H2D + split + walk + merge + D2H
+          every step), wall clock around the synchronous call.
 
-`--impl reference` times the reference's own CPU code (its kernels and
-LozengeTiler::Walk built through oracle/shim: oracle/_ref) on the host cores,
-or the oracle's C restatement where oracle/_ref is absent.
+Beside the headline the line carries the q = 0.99 int32 walk, the fast and
+bit-plane modes, the Aztec diamond of order 2000, the batched workload of 4,096
+mixed chains (per kernel family), a short CFTP run, the six-vertex model and
+the warm vs cold start comparison (sweeps to 0.5 % mean-height error), each in
+its own key.
+
+`--impl reference` runs the same steps with the reference's own CPU code (its
+kernels and LozengeTiler::Walk built through oracle/shim: oracle/_ref, OpenMP
+over work items on every host core), or the oracle's C restatement where
+oracle/_ref is absent.
 
 Multi-GPU: one walk is a single lattice, which this path does not split, so
 --gpus N runs N independent replicas (seeds 42 + rank), value = total
@@ -45,22 +54,26 @@ sys.path.insert(0, ROOT)
 
 METRIC = "flip attempts/s & HBM GB/s vs peak; sweeps-to-0.5% height error, warm vs cold"
 HEX_SIDE = 500
-STEPS_PER_WALK = 60000  # reference colour steps = 20,000 sweeps of the three colours
+SEGMENT = 3000  # reference colour steps per bench step (1,000 sweeps of the three colours)
 SEED = 42
 L2_FLUSH_BYTES = 256 << 20
+FALLBACK_HBM_GBS = 6650.0
 
 
-def workload_config() -> dict:
+def workload_config(world: int = 1) -> dict:
+    """The workload of both arms (identical dicts)."""
     return {
-        "workload": "lozenge hexagon a=b=c=500 (1008x1008 tiling), minimal tiling start, "
-                    "20000 sweeps = 60000 colour steps per walk, TinyMT bit-exact mode",
+        "workload": "lozenge hexagon a=b=c=500 (1008x1008 tiling, 338688 attempts per colour step), minimal "
+                    "tiling start, TinyMT bit-exact mode, uniform weights; one step = one Walk call of 3000 colour "
+                    "steps (1000 sweeps), seed 42+k, continuing the chain; 20 steps = the 20000-sweep walk",
         "domain": "LozengeTiler::AlmostHexDomain(500,0)",
         "tiling_side": 1008,
-        "attempts_per_step": 1008 * 336,
-        "steps_per_walk": STEPS_PER_WALK,
+        "attempts_per_colour_step": 1008 * 336,
+        "colour_steps_per_step": SEGMENT,
         "seed": SEED,
-        "weights": "uniform (int8 lattice); q=0.99 int32 in `q_weighted`",
-        "l2": "flushed (256 MiB write) between timed walks",
+        "weights": "uniform (int8 lattice)",
+        "l2": "flushed (256 MiB write) before every timed step",
+        "parallelism": f"replicas{world}",
     }
 
 
@@ -70,19 +83,20 @@ def peaks() -> tuple[float, str]:
         with open(p) as f:
             return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
-        return 6650.0, "fallback"
+        return FALLBACK_HBM_GBS, "fallback"
 
 
 def start_tiling():
     import randomtilings_b200 as rt
 
     d = rt.LozengeTiler.AlmostHexDomain(HEX_SIDE, 0)
-    return rt.LozengeTiler.MinTiling(d)
+    return np.asarray(rt.LozengeTiler.MinTiling(d), dtype=np.int32)
 
 
 def algorithmic_bytes_per_step(n: int, elem: int, rng_state: bool = True) -> int:
-    """Lattice read + write of every colour-array site, plus the TinyMT state
-    (s0..s3 read + write, 32 B) of every attempt (none in fast mode)."""
+    """Bytes a colour step would move through HBM: every colour-array site read
+    and written once, plus the TinyMT state (s0..s3 read + write, 32 B) of
+    every attempt (none in the counter-based modes)."""
     sites = n * n
     attempts = n * (n // 3)
     return 2 * sites * elem + (attempts * 32 if rng_state else 0)
@@ -106,7 +120,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
@@ -199,45 +213,313 @@ def barrier(dist):
         dist.barrier()
 
 
-def time_device_walks(tiler, steps: int, warmup: int, seed: int, flush) -> list[float]:
-    """Per-walk device milliseconds (events on the library's stream)."""
+def time_device_steps(tiler, t0: np.ndarray, steps: int, warmup: int, seed: int, flush,
+                      colour_steps: int = SEGMENT) -> tuple[list[float], np.ndarray]:
+    """Device milliseconds of `steps` bench steps (CUDA events on the library's
+    stream), after `warmup` untimed ones; the chain restarts from t0 before the
+    timed steps.  Returns the times and the final tiling."""
     import torch
 
     s = torch.cuda.ExternalStream(tiler.stream)
+    tiler.upload(t0)
     for w in range(warmup):
-        tiler.run(STEPS_PER_WALK, seed + 1000 + w)
+        tiler.run(colour_steps, seed + w)
     tiler.synchronize()
+    tiler.upload(t0)
     out = []
     for k in range(steps):
         flush()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
-        tiler.run(STEPS_PER_WALK, seed + k)
+        tiler.run(colour_steps, seed + k)
         e1.record(s)
         tiler.synchronize()
         out.append(e0.elapsed_time(e1))
-    return out
+    final = np.empty_like(t0)
+    tiler.download(final)
+    return out, final
 
 
-def time_e2e_walks(tiler_cls, kwargs, t0: np.ndarray, steps: int, warmup: int, seed: int, flush) -> list[float]:
-    """rt_walk with a host tiling: wall time per walk (the call is synchronous)."""
+def time_e2e_steps(tiler_cls, kwargs, t0: np.ndarray, steps: int, warmup: int, seed: int,
+                   flush) -> tuple[list[float], np.ndarray]:
+    """The same steps through rt_walk with a host tiling in pinned memory: wall
+    time of each synchronous call (H2D, split, walk, merge, D2H)."""
     import torch
 
     tl = tiler_cls(**kwargs)
-    host = np.array(t0, dtype=np.int32)
+    host = torch.empty(t0.size, dtype=torch.int32).pin_memory().numpy()
+    host[:] = t0.reshape(-1)
     for w in range(warmup):
-        host[:] = t0
-        tl.Walk(host, STEPS_PER_WALK, seed + 1000 + w)
+        tl.Walk(host, SEGMENT, seed + w)
+    host[:] = t0.reshape(-1)
     out = []
     for k in range(steps):
-        host[:] = t0
         flush()
         torch.cuda.synchronize()
         a = time.perf_counter()
-        tl.Walk(host, STEPS_PER_WALK, seed + k)
+        tl.Walk(host, SEGMENT, seed + k)
         out.append((time.perf_counter() - a) * 1e3)
     tl.close()
+    return out, host.copy()
+
+
+def golden_digest(steps: int) -> str | None:
+    """The reference's own result after `steps` bench steps from seed 42
+    (tests/golden/bench_parity.json), when that fixture covers them."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "bench_parity.json")) as f:
+            return json.load(f).get(f"hex500/uniform/segment{steps - 1}")
+    except OSError:
+        return None
+
+
+def digest(a: np.ndarray) -> str:
+    import hashlib
+
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<i4").tobytes()).hexdigest()
+
+
+def leg(ms: list[float], attempts: int, world: int, dist, extra: dict | None = None) -> dict:
+    total = all_max(dist, sum(ms))
+    out = {"value": attempts * SEGMENT * len(ms) * world / (total / 1e3), "unit": "attempts/s",
+           "ms_per_step": total / len(ms), "us_per_colour_step": total / len(ms) / SEGMENT * 1e3}
+    out.update(extra or {})
+    return out
+
+
+def run_b200(args) -> None:
+    import torch
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    import randomtilings_b200 as rt
+
+    rt.load(build_if_missing=False)
+    t0 = start_tiling()
+    n = int(round(t0.size ** 0.5))
+    attempts = n * (n // 3)
+    seed = replica_seed(rank)
+    flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def flush():
+        flush_buf.fill_(1.0)
+
+    tl = rt.LozengeTiler(device=local)
+    tq = rt.LozengeTiler(device=local, kernel=rt.RT_KERNEL_QWEIGHT, q=0.99, qcmp=rt.RT_QCMP_FLOAT32)
+    tf = rt.LozengeTiler(device=local, rng=rt.RT_RNG_PHILOX)
+    tp = rt.LozengeTiler(device=local, rng=rt.RT_RNG_PLANES)
+
+    barrier(dist)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        wall0 = time.perf_counter()
+        ms, final = time_device_steps(tl, t0, args.steps, args.warmup, seed, flush)
+        wall = time.perf_counter() - wall0
+        torch.cuda.synchronize()
+        barrier(dist)
+        phases, launches = tl.last_run_info()
+        e2e_ms, e2e_final = time_e2e_steps(rt.LozengeTiler, {"device": local}, t0, args.steps, args.warmup, seed,
+                                           flush)
+        ms_q, _ = time_device_steps(tq, t0, args.steps, args.warmup, seed, flush)
+        ms_f, _ = time_device_steps(tf, t0, args.steps, args.warmup, seed, flush)
+        ms_p, _ = time_device_steps(tp, t0, args.steps, args.warmup, seed, flush)
+    clocks = clk.summary()
+    for t in (tl, tq, tf, tp):
+        t.close()
+
+    total_ms = all_max(dist, sum(ms))
+    total_e2e = all_max(dist, sum(e2e_ms))
+    value = attempts * SEGMENT * args.steps * world / (total_ms / 1e3)
+    per_launch_ms = sum(ms) / len(ms)
+    peak, peak_kind = peaks()
+    algo = algorithmic_bytes_per_step(n, 1) * SEGMENT
+    achieved = algo / (per_launch_ms / 1e3) / 1e9
+    want = golden_digest(args.steps) if seed == SEED else None
+    parity = {"final_tiling_sha256": digest(final), "e2e_equal": bool(np.array_equal(final, e2e_final)),
+              "reference_sha256": want, "equal_to_reference": None if want is None else digest(final) == want}
+
+    aztec = measure_aztec2000(args, local, seed, flush)
+    sixv = measure_sixv(args, local)
+    batched = None if args.no_batch else measure_batch(args, rank, world, dist, peak)
+    cftp = None if args.no_cftp else measure_cftp_small(args, rank, world, dist)
+    warm = measure_warm_cold(args, local) if (rank == 0 and not args.no_warm) else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(segments=args.cpu_segments)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "attempts/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "int8",
+            "data": "synthetic (the reference's own domain builder; no dataset)",
+            "config": workload_config(world),
+            "impl": "b200",
+            "us_per_colour_step": per_launch_ms / SEGMENT * 1e3,
+            "sweeps_per_s": value / attempts / 3,
+            "parity": parity,
+            "e2e": {
+                "value": attempts * SEGMENT * args.steps * world / (total_e2e / 1e3),
+                "unit": "attempts/s",
+                "h2d_bytes_per_step": n * n * 4,
+                "d2h_bytes_per_step": n * n * 4,
+                "ms_per_step": total_e2e / args.steps,
+                "host_buffer": "pinned",
+            },
+            "roofline": {
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": achieved / peak,
+                "peak_kind": peak_kind,
+                "traffic": args.traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this kernel "
+                                  "on this workload; a launch reads the lattice in and writes it back once "
+                                  "whatever its step count",
+                "dram_gbs": args.traffic / (per_launch_ms / 1e3) / 1e9,
+                "limiter": "phase latency: the lattice and the TinyMT states stay on chip for the whole launch, "
+                           "so a colour step costs the latency of one word's update plus the exchange of edge "
+                           "rows between neighbouring CTAs, not DRAM bandwidth",
+                "kernel": "rtb::word_kernel<FAM_LOZENGE8, 1, bit-exact> (one cooperative launch per step)",
+                "algorithmic_bytes_per_launch": algo,
+                "launch_ms": per_launch_ms,
+            },
+            "q_weighted": leg(ms_q, attempts, world, dist, {
+                "q": 0.99, "compare": "float32", "dtype": "int32",
+                "hbm_gbs_algorithmic": algorithmic_bytes_per_step(n, 4) * SEGMENT / (sum(ms_q) / len(ms_q) / 1e3) / 1e9}),
+            "fast_mode": leg(ms_f, attempts, world, dist, {
+                "rng": "Philox4x32-10 keyed by (position quad, step, chain), cyclic colours", "dtype": "int8"}),
+            "bit_planes": leg(ms_p, attempts, world, dist, {
+                "rng": "one Philox4x32-10 bit per site, heat-bath rule, lattice as bit planes, cyclic colours"}),
+            "aztec2000": aztec,
+            "six_vertex": sixv,
+            "batched": batched,
+            "cftp": cftp,
+            "warm_vs_cold": warm,
+            "gpu_launches": int(launches) * args.steps,
+            "phases_per_launch": int(phases),
+            "clocks": clocks,
+            "wall_s_timed_region": wall,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def measure_aztec2000(args, device: int, seed: int, flush) -> dict:
+    """The large lattice of the warm-start evaluation (Aztec diamond of order
+    2000, 4006 x 4006 tiling, 8,012,004 attempts per colour step): fast mode and
+    bit-plane mode, walks of 4,000 colour steps."""
+    import randomtilings_b200 as rt
+
+    d = rt.DominoTiler.AztecDiamond(2000)
+    t0 = np.asarray(rt.DominoTiler.MinTiling(d), dtype=np.int32)
+    n = int(round(t0.size ** 0.5))
+    att = (n - 2) * (n // 2 - 2)
+    steps = 4000
+    out = {"workload": "Aztec diamond n=2000 (4006x4006), minimal tiling, walks of 4000 colour steps",
+           "attempts_per_colour_step": att, "unit": "attempts/s"}
+    for name, rng in (("fast_mode", rt.RT_RNG_PHILOX), ("bit_planes", rt.RT_RNG_PLANES)):
+        tl = rt.DominoTiler(device=device, rng=rng)
+        ms, _ = time_device_steps(tl, t0, 2, 3, seed, flush, colour_steps=steps)
+        tl.close()
+        out[name] = att * steps / (sum(ms) / len(ms) / 1e3)
+    return out
+
+
+def measure_sixv(args, device: int) -> dict:
+    """The six-vertex model (domain-wall boundary, n = 1000, uniform weights):
+    attempts/s of a walk of 400 sweeps from the minimal heights, wall clock
+    around the synchronous call after one warm-up walk."""
+    import randomtilings_b200 as rt
+
+    n, sweeps = 1000, 400
+    tl = rt.SixVertexTiler(device=device)
+    h = rt.SixVertexTiler.MinHeights(n)
+    tl.Walk(h.copy(), 20, 1)
+    a = time.perf_counter()
+    tl.Walk(h, sweeps, 2)
+    dt = time.perf_counter() - a
+    tl.close()
+    return {"workload": f"six-vertex, domain-wall boundary n={n}, {sweeps} sweeps (4 colour steps each), "
+                        "uniform weights, heat bath", "value": (n - 1) ** 2 * sweeps / dt, "unit": "attempts/s",
+            "wall_s": dt, "valid": bool(rt.SixVertexTiler.IsValid(h))}
+
+
+def measure_cftp_small(args, rank: int, world: int, dist) -> dict:
+    """Coupling from the past in the default run (the configs[2] run at order
+    500 and 32 seeds is --workload cftp): an Aztec diamond of order
+    args.cftp_small_order, bit-plane heat bath, coupled maximal and minimal
+    chains in one launch, doubling from 1,024 colour steps, master seeds
+    0..args.cftp_small_seeds-1 dealt to the ranks."""
+    import randomtilings_b200 as rt
+
+    d = rt.DominoTiler.AztecDiamond(args.cftp_small_order)
+    tmax, tmin = rt.DominoTiler.MaxTiling(d), rt.DominoTiler.MinTiling(d)
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    runs = []
+    for s in shard(args.cftp_small_seeds, rank, world):
+        tl = rt.DominoTiler(device=local, kernel=rt.RT_KERNEL_CFTP, rng=rt.RT_RNG_PLANES)
+        a = time.perf_counter()
+        _, st = tl.CFTP(tmax, tmin, first_steps=1024, master_seed=s, max_trials=24)
+        st["wall_s"] = time.perf_counter() - a
+        tl.close()
+        runs.append(st)
+    steps = [r["total_steps"] for r in runs]
+    co = all_sum(dist, [float(sum(r["coalesced"] for r in runs)), float(len(runs))])
+    wall = all_max(dist, sum(r["wall_s"] for r in runs))
+    return {"workload": f"Aztec diamond n={args.cftp_small_order}, domino heat bath (bit planes), coupled max/min "
+                        "chains, doubling from 1024 colour steps",
+            "seeds": int(co[1]), "coalesced": int(co[0]),
+            "median_colour_steps_rank0": statistics.median(steps) if steps else None,
+            "max_colour_steps_rank0": max(steps) if steps else None,
+            "device_ms_rank0": sum(r["device_ms"] for r in runs), "wall_s": wall}
+
+
+def measure_warm_cold(args, device: int) -> dict:
+    """Sweeps to a mean-height error of 0.5 % of the side, warm start vs cold
+    start, at reduced size: the coordinate MLP is trained in the run on its own
+    kernels from the mean heights of short plain chains (Aztec diamonds of order
+    16-96, hexagons of sides 8-48), then judged on an Aztec diamond of order
+    args.warm_aztec and an a=b=c=args.warm_hexagon hexagon against the long-chain
+    mean, the max / min sandwich certifying convergence."""
+    from randomtilings_b200 import warmstart as ws
+
+    t0 = time.perf_counter()
+    specs = ws.training_specs(args.warm_domains, seed=0, aztec=(16, 96), hexagon=(8, 48), q=(0.98, 1.0))
+    x, y, _ = ws.generate_dataset(specs, device=device, samples=8)
+    t_data = time.perf_counter() - t0
+    w = ws.WarmStart(device=device, seed=0)
+    t1 = time.perf_counter()
+    losses = w.fit(x, y, steps=1500, batch=8192, lr=3e-3)
+    t_train = time.perf_counter() - t1
+    out = {"threshold": 0.005, "train_domains": len(specs), "train_rows": int(x.shape[0]),
+           "dataset_s": round(t_data, 2), "train_s": round(t_train, 2), "final_loss": float(losses[-1]), "eval": []}
+    for kind, size in (("aztec", (args.warm_aztec,)), ("hexagon", (args.warm_hexagon,) * 3)):
+        spec = ws.DomainSpec(kind, size)
+        p = ws.prepare(spec, device)
+        tw, st = w.warm_tiling(p)
+        r = ws.relax(p, {"cold": p.tmin, "warm": tw}, int(1.5 * ws.burn_sweeps(spec)), points=40,
+                     replicas=args.warm_replicas, device=device, threshold=0.005)
+        s = r["sweeps_to_threshold"]
+        out["eval"].append({
+            "domain": spec.label(), "sweeps_to_0.5pct": s, "speedup": ws.speedup(r),
+            "error_at_sweep0": {k: round(v[0], 5) for k, v in r["curves"].items()},
+            "final_sandwich_gap": round(r["sandwich_gap"][-1], 5), "replicas": args.warm_replicas,
+            "sweeps_run": r["sweeps"][-1], "device_ms": round(r["device_ms"], 1)})
+    out["wall_s"] = round(time.perf_counter() - t0, 2)
     return out
 
 
@@ -258,10 +540,10 @@ def run_legs(args) -> None:
         tl = rt.LozengeTiler(**kw)
         tl.upload(t0)
         for k in range(args.warmup + args.steps):
-            tl.run(STEPS_PER_WALK, SEED + k)
+            tl.run(args.walk_steps, SEED + k)
         tl.synchronize()
         tl.close()
-        print(f"{name}: {args.warmup + args.steps} walks of {STEPS_PER_WALK} colour steps", flush=True)
+        print(f"{name}: {args.warmup + args.steps} walks of {args.walk_steps} colour steps", flush=True)
     if "batch" in legs:
         bt = rt.Batch()
         models = None if args.batch_models == "all" else {int(m) for m in args.batch_models.split(",")}
@@ -279,174 +561,6 @@ def run_legs(args) -> None:
         bt.run(args.batch_sweeps)
         print(f"batch: {n} chains, {args.batch_sweeps} sweeps, {bt.info()}", flush=True)
         bt.close()
-
-
-def run_b200(args) -> None:
-    import torch
-
-    rank, world, local, dist = dist_setup(args.gpus)
-    import randomtilings_b200 as rt
-
-    rt.load(build_if_missing=False)
-    t0 = start_tiling()
-    n = int(round(t0.size ** 0.5))
-    attempts = n * (n // 3)
-    seed = replica_seed(rank)
-    flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-
-    def flush():
-        flush_buf.fill_(1.0)
-
-    tl = rt.LozengeTiler(device=local)
-    tl.upload(t0)
-    tq = rt.LozengeTiler(device=local, kernel=2, q=0.99, qcmp=0)
-    tq.upload(t0)
-    tf = rt.LozengeTiler(device=local, rng=rt.RT_RNG_PHILOX)
-    tf.upload(t0)
-    tp = rt.LozengeTiler(device=local, rng=rt.RT_RNG_PLANES)
-    tp.upload(t0)
-
-    barrier(dist)
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        wall0 = time.perf_counter()
-        ms = time_device_walks(tl, args.steps, args.warmup, seed, flush)
-        wall = time.perf_counter() - wall0
-    torch.cuda.synchronize()
-    barrier(dist)
-    clocks = clk.summary()
-    ms_q = time_device_walks(tq, args.steps, args.warmup, seed, flush)
-    ms_f = time_device_walks(tf, args.steps, args.warmup, seed, flush)
-    ms_p = time_device_walks(tp, args.steps, args.warmup, seed, flush)
-    aztec = measure_aztec2000(args, local, seed, flush)
-    e2e_ms = time_e2e_walks(rt.LozengeTiler, {"device": local}, t0, args.steps, min(args.warmup, 3), seed, flush)
-    phases, launches = tl.last_run_info()
-
-    total_ms = all_max(dist, sum(ms))
-    total_q = all_max(dist, sum(ms_q))
-    total_f = all_max(dist, sum(ms_f))
-    total_p = all_max(dist, sum(ms_p))
-    total_e2e = all_max(dist, sum(e2e_ms))
-    work = attempts * STEPS_PER_WALK * args.steps * world
-    value = work / (total_ms / 1e3)
-    per_launch_ms = sum(ms) / len(ms)
-    algo = algorithmic_bytes_per_step(n, 1) * STEPS_PER_WALK
-    peak, peak_kind = peaks()
-    achieved = algo / (per_launch_ms / 1e3) / 1e9
-    algo_q = algorithmic_bytes_per_step(n, 4) * STEPS_PER_WALK
-    achieved_q = algo_q / (sum(ms_q) / len(ms_q) / 1e3) / 1e9
-    algo_f = algorithmic_bytes_per_step(n, 1, rng_state=False) * STEPS_PER_WALK
-    achieved_f = algo_f / (sum(ms_f) / len(ms_f) / 1e3) / 1e9
-
-    batched = None if args.no_batch else measure_batch(args, rank, world, dist, peaks()[0])
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(t0, seconds=args.cpu_seconds)
-
-    if rank == 0:
-        line = {
-            "metric": METRIC,
-            "value": value,
-            "unit": "attempts/s",
-            "n_gpus": world,
-            "steps": args.steps,
-            "warmup": args.warmup,
-            "ms_per_step": total_ms / args.steps,
-            "higher_is_better": True,
-            "scaling": "weak",
-            "vs_baseline": None,
-            "dtype": "int8",
-            "data": "synthetic (the reference's own domain builder; no dataset)",
-            "config": workload_config() | {"parallelism": f"replicas{world}"},
-            "impl": "b200",
-            "hbm_gbs_algorithmic": achieved,
-            "sweeps_per_s": value / attempts / 3,
-            "e2e": {
-                "value": attempts * STEPS_PER_WALK * args.steps * world / (total_e2e / 1e3),
-                "unit": "attempts/s",
-                "h2d_bytes_per_step": n * n * 4,
-                "d2h_bytes_per_step": n * n * 4,
-                "ms_per_step": total_e2e / args.steps,
-            },
-            "roofline": {
-                "bound": "hbm",
-                "achieved": achieved,
-                "peak": peak,
-                "unit": "GB/s",
-                "frac": achieved / peak,
-                "peak_kind": peak_kind,
-                "traffic": args.traffic,
-                "kernel": "rtb::walk_kernel (one cooperative launch per walk)",
-                "algorithmic_bytes_per_launch": algo,
-                "launch_ms": per_launch_ms,
-            },
-            "q_weighted": {
-                "q": 0.99, "compare": "float32", "dtype": "int32",
-                "value": attempts * STEPS_PER_WALK * args.steps * world / (total_q / 1e3),
-                "unit": "attempts/s",
-                "ms_per_step": total_q / args.steps,
-                "hbm_gbs_algorithmic": achieved_q,
-                "frac": achieved_q / peak,
-            },
-            "fast_mode": {
-                "rng": "Philox4x32-10 keyed by (position quad, step, chain), cyclic colours", "dtype": "int8",
-                "value": attempts * STEPS_PER_WALK * args.steps * world / (total_f / 1e3),
-                "unit": "attempts/s",
-                "ms_per_step": total_f / args.steps,
-                "hbm_gbs_algorithmic": achieved_f,
-                "frac": achieved_f / peak,
-            },
-            "bit_planes": {
-                "rng": "one Philox4x32-10 bit per site, heat-bath rule, lattice as bit planes, cyclic colours",
-                "value": attempts * STEPS_PER_WALK * args.steps * world / (total_p / 1e3),
-                "unit": "attempts/s",
-                "ms_per_step": total_p / args.steps,
-            },
-            "aztec2000": aztec,
-            "batched": batched,
-            "gpu_launches": int(launches) * args.steps,
-            "phases_per_launch": int(phases),
-            "clocks": clocks,
-            "wall_s_timed_region": wall,
-        }
-        if cpu is not None:
-            line["cpu_baseline"] = cpu
-        print(json.dumps(line), flush=True)
-    tl.close()
-    tq.close()
-    tf.close()
-    tp.close()
-    if dist is not None:
-        dist.destroy_process_group()
-
-
-def measure_aztec2000(args, device: int, seed: int, flush) -> dict:
-    """The large lattice of the warm-start evaluation (Aztec diamond of order
-    2000, 4006 x 4006 tiling, 8,016,008 attempts per colour step): fast mode and
-    bit-plane mode, 4,000 colour steps per walk."""
-    import randomtilings_b200 as rt
-
-    d = rt.DominoTiler.AztecDiamond(2000)
-    t0 = rt.DominoTiler.MinTiling(d)
-    n = int(round(t0.size ** 0.5))
-    att = (n - 2) * (n // 2 - 2)
-    steps = 4000
-    out = {"workload": "Aztec diamond n=2000 (4006x4006), minimal tiling, 4000 colour steps per walk",
-           "attempts_per_step": att, "unit": "attempts/s"}
-    global STEPS_PER_WALK
-    saved = STEPS_PER_WALK
-    STEPS_PER_WALK = steps
-    try:
-        for name, rng in (("fast_mode", rt.RT_RNG_PHILOX), ("bit_planes", rt.RT_RNG_PLANES)):
-            tl = rt.DominoTiler(device=device, rng=rng)
-            tl.upload(t0)
-            ms = time_device_walks(tl, max(1, args.steps), args.warmup, seed, flush)
-            tl.close()
-            out[name] = att * steps / (sum(ms) / len(ms) / 1e3)
-    finally:
-        STEPS_PER_WALK = saved
-    return out
 
 
 def run_cftp(args) -> None:
@@ -547,21 +661,60 @@ def run_extremal(args) -> None:
                       "unit": "s", "higher_is_better": False, "runs": out}), flush=True)
 
 
+FAMILY_NAMES = {0: "domino", 1: "lozenge", 2: "rect_triangle", 3: "triangle_dimer"}
+STEPS_PER_SWEEP = {0: 2, 1: 3, 2: 3, 3: 30}
+
+
+def chain_costs(model: int, n: int) -> tuple[int, int, int]:
+    """(attempts, bytes at the batched kernels' stored widths, bytes at the
+    reference's storage widths) of one sweep of a chain of tiling side n:
+    every colour step reads and writes each colour-array site once.  Stored
+    widths: dominoes and lozenges 1 B; rectangle-triangles 4 B; triangle
+    dimers 5 byte planes and 3 16-bit planes (11 B for the 8 arrays' sites,
+    against 32 B as the reference's int arrays)."""
+    steps = STEPS_PER_SWEEP[model]
+    if model == 0:
+        att, stored, ref = (n - 2) * (n // 2 - 2), n * n, n * n
+    elif model in (1, 2):
+        att = n * (n // 3)
+        stored = ref = n * n * (1 if model == 1 else 4)
+    else:
+        m = n // 2
+        att, stored, ref = m * m, 11 * m * m, 32 * m * m
+    return att * steps, 2 * stored * steps, 2 * ref * steps
+
+
 def measure_batch(args, rank: int, world: int, dist, peak: float) -> dict:
     """The batched pattern: args.batch_chains chains of the mixed workload
     (chain seed s: domain type s mod 4, sizes from std::mt19937(s)), minimal
-    tilings, args.batch_sweeps sweeps each in fast mode, as one graph of one
-    persistent cluster launch per kernel family.  Ranks take seeds round-robin
-    (no communication); value = all ranks' attempts / max device time."""
+    tilings (bibone hexagons: their canonical start), args.batch_sweeps sweeps
+    each in fast mode, as one graph of persistent cluster launches per kernel
+    family; then each family alone for a shorter run.  Ranks take seeds
+    round-robin (no communication); value = all ranks' attempts / max device
+    time.  Bytes are counted at the widths the kernels store (the lattices stay
+    in shared memory, so they are what a streaming walk would move)."""
     import randomtilings_b200 as rt
     from randomtilings_b200 import workloads
 
-    bt = rt.Batch(device=int(os.environ.get("LOCAL_RANK", "0")))
-    kinds = {}
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    chains = []
     for seed in shard(args.batch_chains, rank, world):
         model, t = workloads.mixed_chain(seed)
+        chains.append((seed, model, t))
+    per_fam = {}
+    for seed, model, t in chains:
+        n = int(round(np.asarray(t).size ** 0.5))
+        a, b_st, b_ref = chain_costs(model, n)
+        f = per_fam.setdefault(model, {"chains": 0, "attempts_per_sweep": 0, "stored_bytes_per_sweep": 0,
+                                       "ref_bytes_per_sweep": 0})
+        f["chains"] += 1
+        f["attempts_per_sweep"] += a
+        f["stored_bytes_per_sweep"] += b_st
+        f["ref_bytes_per_sweep"] += b_ref
+
+    bt = rt.Batch(device=local)
+    for seed, model, t in chains:
         bt.add(model, t, key=seed, chain=seed)
-        kinds[model] = kinds.get(model, 0) + 1
     bt.run(2)  # autotuner (on a scratch copy) + graph build; then a short warm-up run
     bt.run(2)
     barrier(dist)
@@ -569,113 +722,155 @@ def measure_batch(args, rank: int, world: int, dist, peak: float) -> dict:
     info = bt.info()
     bt.close()
     ms = all_max(dist, info["run_ms"])
-    total_attempts, total_bytes = all_sum(dist, [float(info["attempts"]), float(info["algorithmic_bytes"])])
-    achieved = total_bytes / world / (ms / 1e3) / 1e9  # per GPU
+    att = sum(f["attempts_per_sweep"] for f in per_fam.values()) * args.batch_sweeps
+    stored = sum(f["stored_bytes_per_sweep"] for f in per_fam.values()) * args.batch_sweeps
+    ref = sum(f["ref_bytes_per_sweep"] for f in per_fam.values()) * args.batch_sweeps
+    tot_att, tot_stored, tot_ref = all_sum(dist, [float(att), float(stored), float(ref)])
+    achieved = tot_stored / world / (ms / 1e3) / 1e9  # per GPU
+
+    families = {}
+    sweeps_f = max(1, min(args.batch_sweeps, args.batch_family_sweeps))
+    for model, f in sorted(per_fam.items()):
+        bf = rt.Batch(device=local)
+        for seed, m_, t in chains:
+            if m_ == model:
+                bf.add(m_, t, key=seed, chain=seed)
+        bf.run(2)
+        bf.run(sweeps_f)
+        fi = bf.info()
+        bf.close()
+        fms = fi["run_ms"]
+        gbs = f["stored_bytes_per_sweep"] * sweeps_f / (fms / 1e3) / 1e9
+        families[FAMILY_NAMES[model]] = {
+            "chains_rank0": f["chains"], "sweeps": sweeps_f, "ms": fms,
+            "attempts_per_s": f["attempts_per_sweep"] * sweeps_f / (fms / 1e3),
+            "stored_gbs": gbs, "frac_stored": gbs / peak,
+            "ref_width_gbs": f["ref_bytes_per_sweep"] * sweeps_f / (fms / 1e3) / 1e9,
+            "plan": next(iter(fi["plans"].values()), None)}
     return {
         "workload": f"{args.batch_chains} chains of the mixed workload (seed s: s mod 4 -> Aztec diamond n in "
-                    "[16,256] / hexagon a,b,c in [8,128] / triangle-dimer IceCreamCone(64,1) / rectangle-triangle "
-                    f"hexagon 64; sizes from std::mt19937(s)), minimal tilings, {args.batch_sweeps} sweeps, "
-                    "fast mode (Philox), one CUDA graph",
-        "chains_per_model_rank0": {str(k): v for k, v in sorted(kinds.items())},
-        "value": total_attempts / (ms / 1e3),
+                    "[16,256] / hexagon a,b,c in [8,128] / bibone (triangle-dimer) hexagon side 64 / "
+                    f"rectangle-triangle hexagon 64; sizes from std::mt19937(s)), minimal tilings, {args.batch_sweeps} "
+                    "sweeps, fast mode (Philox), one CUDA graph",
+        "value": tot_att / (ms / 1e3),
         "unit": "attempts/s",
         "ms": ms,
-        "hbm_gbs_algorithmic": achieved,
+        "hbm_gbs_stored_widths": achieved,
         "frac": achieved / peak,
+        "hbm_gbs_reference_widths": tot_ref / world / (ms / 1e3) / 1e9,
+        "bytes_note": "frac counts every colour step reading and writing each site at the width the batched "
+                      "kernels store it; the lattices stay in shared memory, so DRAM traffic is the load and "
+                      "store of each chain once per launch",
+        "families": families,
         "plans_rank0": info["plans"],
         "tune_ms_rank0": info["tune_ms"],
         "graph_launches": 1,
     }
 
 
-def cpu_baseline(t0: np.ndarray, seconds: float = 15.0, threads: int | None = None) -> dict:
-    """The reference's own kernels + LozengeTiler::Walk on the host cores
-    (oracle/_ref), else the oracle's C restatement; a bounded sample of the
-    same walk (same domain, start and seed), timed with a wall clock."""
+def reference_walker(threads: int):
+    """(start tiling, step function, kind, cores) of the reference's own CPU
+    code: oracle/_ref's LozengeTiler::Walk over its kernels with OpenMP over
+    work items, its own AlmostHexDomain / MinTiling for the start; else the
+    oracle's C restatement (one core) on the library's builders."""
     from oracle import pyoracle as po
 
-    n = int(round(t0.size ** 0.5))
-    attempts = n * (n // 3)
-    threads = threads or os.cpu_count() or 1
     if po.have_ref():
-        rt = po.RefTiler("lozenge", attempts, threads=threads)
-        run = lambda s: rt.walk(t0, s, SEED)  # noqa: E731
-        kind, cores = "reference", threads
-    else:
-        run = lambda s: po.lozenge_walk(t0, s, SEED)  # noqa: E731
-        kind, cores = "port", 1
-    probe = 20
-    a = time.perf_counter()
-    run(probe)
-    dt = time.perf_counter() - a
-    steps = max(probe, int(probe * seconds / max(dt, 1e-6)))
-    a = time.perf_counter()
-    run(steps)
-    dt = time.perf_counter() - a
-    return {
-        "value": attempts * steps / dt,
-        "unit": "attempts/s",
-        "cores": cores,
-        "kind": kind,
-        "sample": f"hex a=b=c=500 walk, first {steps} colour steps (of 60000), seed {SEED}, {dt:.1f} s",
-    }
+        d = po.ref_build("lozenge_almost_hex", p0=HEX_SIDE, p1=0)
+        t0 = po.ref_build("lozenge_min", d).astype(np.int32)
+        tiler = po.RefTiler("lozenge", t0.size, threads=threads)
+        return t0, (lambda t, s: tiler.walk(t, SEGMENT, s)), "reference", threads
+    t0 = start_tiling()
+    return t0, (lambda t, s: po.lozenge_walk(t, SEGMENT, s)), "port", 1
+
+
+def cpu_baseline(segments: int = 2) -> dict:
+    """A bounded sample of the workload on the host cores: the first
+    `segments` bench steps from the minimal tiling, wall clock."""
+    threads = os.cpu_count() or 1
+    t0, step, kind, cores = reference_walker(threads)
+    attempts = t0.size // 3
+    a = t0.copy()
+    t = time.perf_counter()
+    for k in range(segments):
+        a = step(a, SEED + k)
+    dt = time.perf_counter() - t
+    return {"value": attempts * SEGMENT * segments / dt, "unit": "attempts/s", "cores": cores, "kind": kind,
+            "sample": f"the first {segments} steps ({segments * SEGMENT} colour steps) of the hexagon walk from the "
+                      f"minimal tiling, seed {SEED}, {dt:.1f} s"}
 
 
 def run_reference(args) -> None:
+    """The reference arm: the same steps (one Walk of 3,000 colour steps each,
+    seeds 42 + k, continuing the chain) with the reference's own code on every
+    host core; rank 0 alone under torchrun."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import randomtilings_b200 as rt  # builders only (host C++)
-
-    t0 = start_tiling()
-    n = int(round(t0.size ** 0.5))
-    attempts = n * (n // 3)
-    per_step_s = max(1.0, args.cpu_seconds / max(args.steps, 1))
-    for _ in range(args.warmup):
-        cpu_baseline(t0, seconds=0.5)
-    vals = [cpu_baseline(t0, seconds=per_step_s) for _ in range(args.steps)]
-    value = statistics.median(v["value"] for v in vals)
-    ms_per_step = attempts * STEPS_PER_WALK / value * 1e3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    threads = os.cpu_count() or 1
+    t0, step, kind, cores = reference_walker(threads)
+    attempts = t0.size // 3
+    a = t0.copy()
+    for w in range(args.warmup):
+        a = step(a, SEED + w)
+    a = t0.copy()
+    times = []
+    for k in range(args.steps):
+        t = time.perf_counter()
+        a = step(a, SEED + k)
+        times.append((time.perf_counter() - t) * 1e3)
+    value = attempts * SEGMENT * args.steps / (sum(times) / 1e3)
+    want = golden_digest(args.steps)
     line = {
         "metric": METRIC,
         "value": value,
         "unit": "attempts/s",
-        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": ms_per_step,
+        "ms_per_step": sum(times) / len(times),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "int8",
         "data": "synthetic (the reference's own domain builder; no dataset)",
-        "config": workload_config() | {"parallelism": "cpu"},
+        "config": workload_config(world),
         "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": "attempts/s", "cores": vals[0]["cores"], "kind": vals[0]["kind"],
-                         "sample": vals[0]["sample"]},
+        "parity": {"final_tiling_sha256": digest(a), "reference_sha256": want,
+                   "equal_to_reference": None if want is None else digest(a) == want},
+        "cpu_baseline": {"value": value, "unit": "attempts/s", "cores": cores, "kind": kind,
+                         "sample": f"the full timed run: {args.steps} steps of {SEGMENT} colour steps"},
         "e2e": {"value": value, "unit": "attempts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    del rt
     print(json.dumps(line), flush=True)
 
 
 def main() -> None:
-    global STEPS_PER_WALK
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-segments", type=int, default=2, help="steps timed for cpu_baseline (about 10 s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    # dram__bytes_read.sum + dram__bytes_write.sum of one word_kernel launch (ncu, 600-step capture,
-    # profiles/word_kernel_hex500.md): 1.146 MB + 3.1 KB; the lattice stays on chip, so a launch of
-    # any number of colour steps moves the same bytes.
+    # dram__bytes_read.sum + dram__bytes_write.sum of one word_kernel launch on this workload (ncu, one
+    # pass): the lattice stays on chip, so a launch of any number of colour steps moves the same bytes.
     ap.add_argument("--traffic", type=float, default=1149184.0,
                     help="dram bytes per walk launch from an ncu capture (reported in roofline.traffic)")
     ap.add_argument("--batch-chains", type=int, default=4096)
     ap.add_argument("--batch-sweeps", type=int, default=5000)
+    ap.add_argument("--batch-family-sweeps", type=int, default=500,
+                    help="sweeps of each kernel family run alone (per-family figures)")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-cftp", action="store_true")
+    ap.add_argument("--cftp-small-order", type=int, default=100)
+    ap.add_argument("--cftp-small-seeds", type=int, default=8)
+    ap.add_argument("--no-warm", action="store_true")
+    ap.add_argument("--warm-domains", type=int, default=128)
+    ap.add_argument("--warm-aztec", type=int, default=200)
+    ap.add_argument("--warm-hexagon", type=int, default=100)
+    ap.add_argument("--warm-replicas", type=int, default=16)
     ap.add_argument("--legs", default="all",
                     help="profiling runs: comma-separated subset of headline,q,fast,planes,batch (no JSON line)")
     ap.add_argument("--batch-models", default="all",
@@ -692,10 +887,8 @@ def main() -> None:
     ap.add_argument("--cftp-rng", choices=["tinymt", "philox", "planes"], default="planes")
     ap.add_argument("--cftp-weights", default="",
                     help="'a,b': two-periodic domino weights (TinyMT or Philox draws)")
-    ap.add_argument("--walk-steps", type=int, default=STEPS_PER_WALK,
-                    help="colour steps per walk (default 60000 = 20000 sweeps; smaller only for profiling captures)")
+    ap.add_argument("--walk-steps", type=int, default=SEGMENT, help="with --legs: colour steps per walk")
     args = ap.parse_args()
-    STEPS_PER_WALK = args.walk_steps
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.workload == "cftp":
