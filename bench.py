@@ -288,6 +288,16 @@ def leg(ms: list[float], attempts: int, world: int, dist, extra: dict | None = N
     return out
 
 
+def side_leg(fn, *a):
+    """A leg beside the headline: its figures, or the error that stopped it
+    (the headline line is printed either way)."""
+    try:
+        return fn(*a)
+    except Exception as e:  # reported in the JSON line, not swallowed
+        print(f"{fn.__name__} failed: {e!r}", file=sys.stderr, flush=True)
+        return {"error": repr(e)}
+
+
 def run_b200(args) -> None:
     import torch
 
@@ -338,11 +348,11 @@ def run_b200(args) -> None:
     parity = {"final_tiling_sha256": digest(final), "e2e_equal": bool(np.array_equal(final, e2e_final)),
               "reference_sha256": want, "equal_to_reference": None if want is None else digest(final) == want}
 
-    aztec = measure_aztec2000(args, local, seed, flush)
-    sixv = measure_sixv(args, local)
-    batched = None if args.no_batch else measure_batch(args, rank, world, dist, peak)
-    cftp = None if args.no_cftp else measure_cftp_small(args, rank, world, dist)
-    warm = measure_warm_cold(args, local) if (rank == 0 and not args.no_warm) else None
+    aztec = side_leg(measure_aztec2000, args, local, seed, flush)
+    sixv = side_leg(measure_sixv, args, local)
+    batched = None if args.no_batch else side_leg(measure_batch, args, rank, world, dist, peak)
+    cftp = None if args.no_cftp else side_leg(measure_cftp_small, args, rank, world, dist)
+    warm = side_leg(measure_warm_cold, args, local) if (rank == 0 and not args.no_warm) else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
