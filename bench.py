@@ -501,19 +501,21 @@ def measure_cftp_small(args, rank: int, world: int, dist) -> dict:
 def measure_warm_cold(args, device: int) -> dict:
     """Sweeps to a mean-height error of 0.5 % of the side, warm start vs cold
     start, at reduced size: the coordinate MLP is trained in the run on its own
-    kernels from the mean heights of short plain chains (Aztec diamonds of order
-    16-96, hexagons of sides 8-48), then judged on an Aztec diamond of order
-    args.warm_aztec and an a=b=c=args.warm_hexagon hexagon against the long-chain
-    mean, the max / min sandwich certifying convergence."""
+    kernels from the mean heights of plain chains (Aztec diamonds of orders
+    args.warm_train_aztec, hexagons of sides args.warm_train_hexagon), then
+    judged on an Aztec diamond of order args.warm_aztec and an
+    a=b=c=args.warm_hexagon hexagon against the long-chain mean, the max / min
+    sandwich certifying convergence."""
     from randomtilings_b200 import warmstart as ws
 
     t0 = time.perf_counter()
-    specs = ws.training_specs(args.warm_domains, seed=0, aztec=(16, 96), hexagon=(8, 48), q=(0.98, 1.0))
+    specs = ws.training_specs(args.warm_domains, seed=0, aztec=tuple(args.warm_train_aztec),
+                              hexagon=tuple(args.warm_train_hexagon), q=(0.98, 1.0))
     x, y, _ = ws.generate_dataset(specs, device=device, samples=8)
     t_data = time.perf_counter() - t0
     w = ws.WarmStart(device=device, seed=0)
     t1 = time.perf_counter()
-    losses = w.fit(x, y, steps=1500, batch=8192, lr=3e-3)
+    losses = w.fit(x, y, steps=args.warm_train_steps, batch=8192, lr=3e-3)
     t_train = time.perf_counter() - t1
     out = {"threshold": 0.005, "train_domains": len(specs), "train_rows": int(x.shape[0]),
            "dataset_s": round(t_data, 2), "train_s": round(t_train, 2), "final_loss": float(losses[-1]), "eval": []}
@@ -881,6 +883,9 @@ def main() -> None:
     ap.add_argument("--warm-aztec", type=int, default=200)
     ap.add_argument("--warm-hexagon", type=int, default=100)
     ap.add_argument("--warm-replicas", type=int, default=16)
+    ap.add_argument("--warm-train-aztec", type=int, nargs=2, default=(16, 96))
+    ap.add_argument("--warm-train-hexagon", type=int, nargs=2, default=(8, 48))
+    ap.add_argument("--warm-train-steps", type=int, default=1500)
     ap.add_argument("--legs", default="all",
                     help="profiling runs: comma-separated subset of headline,q,fast,planes,batch (no JSON line)")
     ap.add_argument("--batch-models", default="all",
