@@ -8,11 +8,9 @@
 // words), the flip test is a per-byte compare, and each thread keeps the
 // TinyMT states of the four positions of each of its words in registers for
 // the whole walk (bit-exact mode) or draws them from one Philox call per word
-// (fast mode).  Schedule, bands and bounded waits are those of the generic
-// walk kernel (rt_walk.cu), and it produces the same bytes; the halo exchange
-// is per word: the thread that updates a band-edge word polls the neighbour
-// words its Update reads and publishes its own result, so one CTA barrier per
-// phase remains.
+// (fast mode).  Schedule, bands, halo exchange and bounded waits are those of
+// the generic walk kernel (rt_walk.cu); only the per-site arithmetic differs,
+// and it produces the same bytes.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -65,6 +63,7 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
         }
 
     const bool has_top = cta > 0, has_bot = cta + 1 < nct;
+    const bool bot_edge = has_bot && !(has_top && nrows == 1);
     // Update mask of band row rr / word w: rows 1..N-2, columns 1..width-2;
     // Rotate positions: columns COFF..COFF+cols-1 (all band rows).
     auto info_at = [&](int rr, int w) {
@@ -85,11 +84,9 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
         wi.vm = lane_bytes(vb);
         return wi;
     };
-    // Edge flags of band row rr: bit 0 the first row under a neighbour band
-    // (reads that band's last row, publishes to it), bit 1 the last row above
-    // one.  A one-row band between two neighbours is both.
-    auto edges_of = [&](int rr) -> uint32_t {
-        return (has_top && rr == 0 ? 1u : 0u) | (has_bot && rr == nrows - 1 ? 2u : 0u);
+    auto is_edge = [&](int u) {
+        const int rr = u / Gw;
+        return (has_top && rr == 0) || (bot_edge && rr == nrows - 1);
     };
     // Lozenge column shifts for each colour t whose Update is applied.
     uint32_t shift_tab[3] = {0u, 0u, 0u};
@@ -98,6 +95,9 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
         shift_tab[1] = lozenge_shift_table(1);
         shift_tab[2] = lozenge_shift_table(2);
     }
+    // This thread's share of the halo exchange: words e = tid + x * BLOCK of
+    // [side][lattice][word] (one array per phase in these models).
+    const int per_side = a.nlat * a.xwords;
 
     // The words u = tid + m * BLOCK (m < MAXW) of this thread, their facts
     // and (bit-exact mode) their positions' TinyMT states, all in registers.
@@ -105,14 +105,14 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
     constexpr int NW = MAXW > 0 ? MAXW : 1;
     WordInfo winfo[NW];
     TinyState st[PHILOX ? 1 : NW][4];
-    uint32_t wflags = 0;  // 4 bits per word m: bit 0 it exists, bits 1-2 its edge flags
+    uint32_t wflags = 0;  // bit 2m: word m exists, bit 2m+1: it is an edge word
     if (MAXW > 0) {
 #pragma unroll
         for (int m = 0; m < MAXW; ++m) {
             const int u = tid + m * BLOCK;
             if (u < nwords) {
                 winfo[m] = info_at(u / Gw, u % Gw);
-                wflags |= (1u | (edges_of(u / Gw) << 1)) << (4 * m);
+                wflags |= (1u << (2 * m)) | ((is_edge(u) ? 1u : 0u) << (2 * m + 1));
             } else {
                 winfo[m] = WordInfo{0, 0, 0u, 0u};
             }
@@ -139,14 +139,14 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
                 key1 = (uint32_t)(eseed >> 32);
                 dstep = 0;
             } else {
-                // Every byte of a word gets a stream; bytes that are not Rotate
-                // positions draw from theirs unobserved (their flips are masked).
 #pragma unroll
                 for (int m = 0; m < NW; ++m) {
+                    if (!(wflags & (1u << (2 * m)))) continue;
                     const int rpos = r0 + winfo[m].off / W - 1;  // position row
                     const int jw = winfo[m].off % W;             // 4 * word
 #pragma unroll
                     for (int b = 0; b < 4; ++b) {
+                        if (!(winfo[m].vm & (1u << (8 * b)))) continue;
                         const uint32_t sid = (uint32_t)(jw + b - M::COFF) + (uint32_t)a.cols * (uint32_t)rpos;
                         tiny_seed(st[m][b], tp, (uint32_t)eseed + sid);
                     }
@@ -156,24 +156,7 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
         const bool draws = (d & PH_DRAWS) != 0u;
         const WordPhase P = word_phase_of<FAM>(d, lat, plane, shift_tab);
         const int lat1 = NC * plane;  // second lattice (coupled CFTP chains)
-        // Halo protocol.  After a step phase, each band publishes its edge rows
-        // of the array it flipped: the thread that updated an edge word stores
-        // it, tagged with the next phase, into the band's slot.  In the next
-        // phase an edge word's thread polls the neighbour's words that its
-        // Update reads and copies them into the shared halo row itself, so no
-        // block-wide barrier sits between the neighbour's store and this
-        // band's own edge words.  Every phase after a step waits, which keeps
-        // neighbouring bands within one phase of each other: a slot (two per
-        // side, by phase parity) is rewritten only after every reader of its
-        // words has published words computed from them.
-        const uint32_t wprev = M::written(d_prev);
-        const bool wait_halo = ph > 0 && wprev != 0u;
-        const bool publish = ph + 1 < a.nphases && M::written(d) != 0u && !(cta == 0 && ph == a.drop_phase);
-        const int harr = wait_halo ? __ffs(wprev) - 1 : 0;
-        const int hpar = (int)((ph - 1) & 1);
-        const int ppar = (int)(ph & 1);
-
-        auto apply = [&](const WordInfo& wi, const uint32_t (&k)[4], uint32_t (&v)[2]) {
+        auto apply = [&](const WordInfo& wi, const uint32_t (&k)[4]) {
             uint32_t m0 = 0, m1 = 0;
             if (draws) {
                 if (WT && FAM == FAM_DOMINO_HB) {
@@ -195,139 +178,124 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
                 }
                 if (!M::DOM) m1 = below4(k, a.thr[1]) & ~m0;
             }
-            v[0] = word_phase<FAM>(P, 0, W, wi, m0, m1);
-            v[1] = a.nlat > 1 ? word_phase<FAM>(P, lat1, W, wi, m0, m1) : 0u;
+            word_phase<FAM>(P, 0, W, wi, m0, m1);
+            if (a.nlat > 1) word_phase<FAM>(P, lat1, W, wi, m0, m1);
         };
-        // Draws of word m of this thread (u = tid + m * BLOCK of the band).
-        auto own_draws = [&](int m, uint32_t (&k)[4]) {
-            k[0] = k[1] = k[2] = k[3] = 0u;
-            if (!draws) return;
-            if (PHILOX) {
-                const int u = tid + m * BLOCK;
-                const uint4 w4 = philox4((uint32_t)(a0 * Gw + u), (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32),
-                                         a.chain, key0, key1);
+        // Word m of this thread (u = tid + m * BLOCK of the band).
+        auto own_word = [&](int m) {
+            uint32_t k[4] = {0u, 0u, 0u, 0u};
+            if (draws) {
+                if (PHILOX) {
+                    const int u = tid + m * BLOCK;
+                    const uint4 w4 = philox4((uint32_t)(a0 * Gw + u), (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32),
+                                             a.chain, key0, key1);
+                    k[0] = w4.x >> 9;
+                    k[1] = w4.y >> 9;
+                    k[2] = w4.z >> 9;
+                    k[3] = w4.w >> 9;
+                } else {
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        if (winfo[m].vm & (1u << (8 * b))) k[b] = tiny_draw23(st[PHILOX ? 0 : m][b], tp);
+                }
+            }
+            apply(winfo[m], k);
+        };
+        auto philox_word = [&](int rr, int w) {
+            const WordInfo wi = info_at(rr, w);
+            uint32_t k[4] = {0u, 0u, 0u, 0u};
+            if (draws) {
+                const uint4 w4 = philox4((uint32_t)((a0 + rr) * Gw + w), (uint32_t)dstep,
+                                         (uint32_t)((uint64_t)dstep >> 32), a.chain, key0, key1);
                 k[0] = w4.x >> 9;
                 k[1] = w4.y >> 9;
                 k[2] = w4.z >> 9;
                 k[3] = w4.w >> 9;
-            } else {
-#pragma unroll
-                for (int b = 0; b < 4; ++b) k[b] = tiny_draw23(st[PHILOX ? 0 : m][b], tp);
             }
+            apply(wi, k);
         };
-        auto philox_draws = [&](int rr, int w, uint32_t (&k)[4]) {
-            k[0] = k[1] = k[2] = k[3] = 0u;
-            if (!draws) return;
-            const uint4 w4 = philox4((uint32_t)((a0 + rr) * Gw + w), (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32),
-                                     a.chain, key0, key1);
-            k[0] = w4.x >> 9;
-            k[1] = w4.y >> 9;
-            k[2] = w4.z >> 9;
-            k[3] = w4.w >> 9;
-        };
-        // The neighbours' words that the Update of edge word w reads, into the
-        // halo rows: dominoes word w; lozenges w, w+1 above and w-1, w below
-        // (the funnel shifts' other word lies beyond the row only for bytes
-        // outside the update mask).  False when a wait gave up.
-        auto fetch_halo = [&](int w, uint32_t edges) -> bool {
-            if (!wait_halo) return true;
-#pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                if (!(edges & (1u << side))) continue;
-                const int src = side == 0 ? cta - 1 : cta + 1;
-                const int wlo = max(0, M::DOM || side == 0 ? w : w - 1);
-                const int whi = min(Gw - 1, M::DOM || side == 1 ? w : w + 1);
-                for (int l = 0; l < a.nlat; ++l) {
-                    const unsigned long long* sl = slot(a, src, 1 - side, hpar, l, 0);
-                    unsigned char* row = lat + (l * NC + harr) * plane + (side == 0 ? 0 : nrows + 1) * W;
-                    for (int x = wlo; x <= whi; ++x) {
-                        uint32_t val;
-                        if (!wait_word(a, sl + x, (uint32_t)ph, &val)) return false;
-                        sts(row + 4 * x, val);
-                    }
+        // Fast mode: words u = lo + tid + x * BLOCK < hi, walked with an
+        // incremental (row, word) pair.
+        auto philox_range = [&](int lo, int hi) {
+            int u = lo + tid;
+            if (u >= hi) return;
+            int rr = u / Gw, w = u - rr * Gw;
+            const int drr = BLOCK / Gw, dw = BLOCK - drr * Gw;
+            for (; u < hi; u += BLOCK) {
+                philox_word(rr, w);
+                rr += drr;
+                w += dw;
+                if (w >= Gw) {
+                    w -= Gw;
+                    ++rr;
                 }
             }
-            return true;
-        };
-        auto publish_word = [&](int w, uint32_t edges, const uint32_t (&v)[2]) {
-            if (!publish) return;
-            const unsigned long long tag = (unsigned long long)(uint32_t)(ph + 1) << 32;
-#pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                if (!(edges & (1u << side))) continue;
-#pragma unroll
-                for (int l = 0; l < 2; ++l)
-                    if (l < a.nlat) st_relaxed64(slot(a, cta, side, ppar, l, 0) + w, tag | v[l]);
-            }
-        };
-        // An edge word: its draws first (they do not depend on the lattice),
-        // then the neighbours' words, the update and this word's publication.
-        auto edge_word = [&](const WordInfo& wi, int w, uint32_t edges, const uint32_t (&k)[4]) -> bool {
-            asm volatile("" ::"r"(k[0]), "r"(k[1]), "r"(k[2]), "r"(k[3]));
-            if (!fetch_halo(w, edges)) return false;
-            uint32_t v[2];
-            apply(wi, k, v);
-            publish_word(w, edges, v);
-            return true;
         };
 
-        bool ok = true;
+        // Words away from the band's edge rows first, overlapping the neighbours' progress.
         if (MAXW == 0) {
-            // Fast mode on wide bands: words u = lo + tid + x * BLOCK < hi,
-            // walked with an incremental (row, word) pair; band-edge rows last.
-            const int rlo = has_top ? 1 : 0, rhi = has_bot ? nrows - 1 : nrows;
-            if (rhi > rlo) {
-                const int hi = rhi * Gw;
-                int u = rlo * Gw + tid;
-                int rr = u / Gw, w = u - rr * Gw;
-                const int drr = BLOCK / Gw, dw = BLOCK - drr * Gw;
-                for (; u < hi; u += BLOCK) {
-                    uint32_t k[4], v[2];
-                    philox_draws(rr, w, k);
-                    apply(info_at(rr, w), k, v);
-                    rr += drr;
-                    w += dw;
-                    if (w >= Gw) {
-                        w -= Gw;
-                        ++rr;
-                    }
-                }
-            }
-            for (int e = 0; e < 2 && ok; ++e) {
-                const int rr = e == 0 ? 0 : nrows - 1;
-                if (e == 1 && rr == 0) break;
-                const uint32_t edges = edges_of(rr);
-                if (!edges) continue;
-                for (int w = tid; w < Gw && ok; w += BLOCK) {
-                    uint32_t k[4];
-                    philox_draws(rr, w, k);
-                    ok = edge_word(info_at(rr, w), w, edges, k);
-                }
-            }
+            const int lo = has_top ? Gw : 0;
+            philox_range(lo, max(lo, nwords - (has_bot ? Gw : 0)));
         } else {
-            // Words away from the band's edge rows first, overlapping the neighbours' progress.
 #pragma unroll
             for (int m = 0; m < NW; ++m)
-                if (((wflags >> (4 * m)) & 7u) == 1u) {
-                    uint32_t k[4], v[2];
-                    own_draws(m, k);
-                    apply(winfo[m], k, v);
+                if ((wflags >> (2 * m) & 3u) == 1u) own_word(m);
+        }
+        if (ph > 0) {
+            // Halo rows of the array the neighbours flipped in the previous phase.
+            const uint32_t mask = M::written(d_prev);
+            bool ok = true;
+            if (mask) {
+                const int arr = __ffs(mask) - 1;
+                const int par = (int)((ph - 1) & 1);
+                const uint32_t tag = (uint32_t)ph;
+                for (int e = tid; e < 2 * per_side && ok; e += BLOCK) {
+                    const int side = e >= per_side;  // 0: row above (from cta-1), 1: row below (from cta+1)
+                    const int rem = e - side * per_side;
+                    const int l = rem >= a.xwords;
+                    const int w = rem - l * a.xwords;
+                    const int src = side == 0 ? cta - 1 : cta + 1;
+                    if (src < 0 || src >= nct) continue;
+                    uint32_t v;
+                    ok = wait_word(a, slot(a, src, 1 - side, par, l, 0) + w, tag, &v);
+                    if (ok) sts(lat + (l * NC + arr) * plane + (side == 0 ? 0 : nrows + 1) * W + 4 * w, v);
                 }
+            }
+            if (__syncthreads_or(!ok)) return;
+        }
+        if (MAXW == 0) {
+            if (has_top) philox_range(0, Gw);
+            if (bot_edge) philox_range(nwords - Gw, nwords);
+        } else {
 #pragma unroll
-            for (int m = 0; m < NW; ++m) {
-                const uint32_t f = (wflags >> (4 * m)) & 7u;
-                if (f > 1u && ok) {
-                    uint32_t k[4];
-                    own_draws(m, k);
-                    ok = edge_word(winfo[m], (tid + m * BLOCK) % Gw, f >> 1, k);
+            for (int m = 0; m < NW; ++m)
+                if ((wflags >> (2 * m) & 3u) == 3u) own_word(m);
+        }
+        __syncthreads();
+        if (ph + 1 < a.nphases && !(cta == 0 && ph == a.drop_phase)) {
+            // Publish the band's first / last row of the array flipped in this phase.
+            const uint32_t mask = M::written(d);
+            if (mask) {
+                const int arr = __ffs(mask) - 1;
+                const int par = (int)(ph & 1);
+                const unsigned long long tag = (unsigned long long)(uint32_t)(ph + 1) << 32;
+                for (int e = tid; e < 2 * per_side; e += BLOCK) {
+                    const int side = e >= per_side;  // 0: first row (read by cta-1), 1: last row (read by cta+1)
+                    const int rem = e - side * per_side;
+                    const int l = rem >= a.xwords;
+                    const int w = rem - l * a.xwords;
+                    const int dst = side == 0 ? cta - 1 : cta + 1;
+                    if (dst < 0 || dst >= nct) continue;
+                    const unsigned char* row = lat + (l * NC + arr) * plane + (side == 0 ? 1 : nrows) * W;
+                    st_relaxed64(slot(a, cta, side, par, l, 0) + w, tag | lds(row + 4 * w));
                 }
             }
         }
-        if (__syncthreads_or(!ok)) return;
         if (PHILOX && draws) ++dstep;
         d_prev = d;
         d = d_next;
     }
+
     __syncthreads();
     for (int l = 0; l < a.nlat; ++l)
         for (int c = 0; c < NC; ++c) {

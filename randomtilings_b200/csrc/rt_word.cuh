@@ -108,11 +108,9 @@ __device__ __forceinline__ uint32_t lozenge_shift_table(int t) {
 // lattice's planes from those the phase descriptor points at.
 // m0 / m1: per-byte draw masks (0x01) -- dominoes: k < thr[0]; lozenges:
 // k < thr[0] (add a cube) and thr[0] <= k < thr[1] (remove one).
-// Returns the word's new value in the array flipped by a step phase (the
-// value a band edge publishes to its neighbour), 0 for an Update-only phase.
 template <int FAM>
-__device__ __forceinline__ uint32_t word_phase(const WordPhase& P, int lo, int W, const WordInfo& wi, uint32_t m0,
-                                               uint32_t m1) {
+__device__ __forceinline__ void word_phase(const WordPhase& P, int lo, int W, const WordInfo& wi, uint32_t m0,
+                                           uint32_t m1) {
     const int off = wi.off + lo;
     if (FAM != FAM_LOZENGE8) {
         uint32_t v = lds(P.dst + off);
@@ -127,7 +125,6 @@ __device__ __forceinline__ uint32_t word_phase(const WordPhase& P, int lo, int W
             v ^= (tog & wi.vm) * 15u;
         }
         sts(P.dst + off, v);
-        return v;
     } else {
         if (P.step) {
             uint32_t v;
@@ -151,14 +148,12 @@ __device__ __forceinline__ uint32_t word_phase(const WordPhase& P, int lo, int W
             const uint32_t tog = (eq_bytes(v, 0x19191919u) & m0) | (eq_bytes(v, 0x26262626u) & m1);
             v ^= (tog & wi.vm) * 63u;
             sts(P.dst + off, v);
-            return v;
         } else {
             const uint32_t ao = lds(P.pa + off), bo = lds(P.pb + off);
             uint32_t na, nb;
             lozenge_refresh(P.src, off, W, (P.shifts >> (3 * wi.cls)) & 7u, ao, bo, na, nb);
             sts(P.pa + off, merge(ao, na, wi.um));
             sts(P.pb + off, merge(bo, nb, wi.um));
-            return 0u;
         }
     }
 }
