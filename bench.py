@@ -879,13 +879,13 @@ def main() -> None:
     ap.add_argument("--cftp-small-order", type=int, default=100)
     ap.add_argument("--cftp-small-seeds", type=int, default=8)
     ap.add_argument("--no-warm", action="store_true")
-    ap.add_argument("--warm-domains", type=int, default=128)
+    ap.add_argument("--warm-domains", type=int, default=384)
     ap.add_argument("--warm-aztec", type=int, default=200)
     ap.add_argument("--warm-hexagon", type=int, default=100)
     ap.add_argument("--warm-replicas", type=int, default=16)
-    ap.add_argument("--warm-train-aztec", type=int, nargs=2, default=(16, 96))
-    ap.add_argument("--warm-train-hexagon", type=int, nargs=2, default=(8, 48))
-    ap.add_argument("--warm-train-steps", type=int, default=1500)
+    ap.add_argument("--warm-train-aztec", type=int, nargs=2, default=(16, 160))
+    ap.add_argument("--warm-train-hexagon", type=int, nargs=2, default=(8, 100))
+    ap.add_argument("--warm-train-steps", type=int, default=3000)
     ap.add_argument("--legs", default="all",
                     help="profiling runs: comma-separated subset of headline,q,fast,planes,batch (no JSON line)")
     ap.add_argument("--batch-models", default="all",
