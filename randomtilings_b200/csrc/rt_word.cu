@@ -8,9 +8,13 @@
 // words), the flip test is a per-byte compare, and each thread keeps the
 // TinyMT states of the four positions of each of its words in registers for
 // the whole walk (bit-exact mode) or draws them from one Philox call per word
-// (fast mode).  Schedule, bands, halo exchange and bounded waits are those of
-// the generic walk kernel (rt_walk.cu); only the per-site arithmetic differs,
-// and it produces the same bytes.
+// (fast mode).  Schedule, bands, tagged halo slots and bounded waits are
+// those of the generic walk kernel (rt_walk.cu) and it produces the same
+// bytes.  With one word per thread, the owners of the band's edge words poll
+// their halo words themselves and only their warps meet at the halo barrier,
+// so the interior words of the other warps overlap the exchange; a colour
+// step then costs the longer of one interior word and (halo wait + one edge
+// word) rather than their sum.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -24,6 +28,18 @@
 namespace rtb {
 
 constexpr int kWordBlockMax = 512;
+
+// bar.red.or on named barrier `id`, which `n` threads (whole warps) execute;
+// returns the OR of their `v`.
+__device__ __forceinline__ bool bar_red_or_n(int id, int n, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, %2, %3, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id), "r"(n)
+        : "memory");
+    return r != 0u;
+}
 
 // Shared memory: 16 bytes of slack, then for each lattice NC colour planes of
 // (band rows + 2 halo rows) x wpad bytes, then 16 bytes of slack (the funnel
@@ -120,6 +136,22 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
     }
     const TinyParams tp{a.mat1, a.mat2, a.tmat};
 
+    // One word per thread: the owner of word w of the band's first row polls
+    // word w of the row above, the owner of word w of its last row the row
+    // below, and only the warps that hold edge words meet at the halo
+    // barrier -- the other warps' words overlap the whole exchange.
+    bool poll_top = false, poll_bot = false, in_group = false;
+    int gthreads = 0;
+    if (MAXW == 1) {
+        const int rr = tid / Gw;
+        poll_top = tid < nwords && has_top && rr == 0;
+        poll_bot = tid < nwords && has_bot && rr == nrows - 1;
+        in_group = __any_sync(0xffffffffu, poll_top || poll_bot);
+        gthreads = 32 * __syncthreads_count((tid & 31) == 0 && in_group);
+    }
+    // The split only pays when some warps hold no edge word.
+    const bool split = MAXW == 1 && gthreads < BLOCK;
+
     int epoch = -1;
     int64_t next_epoch = a.nepochs > 0 ? a.epoch_start[0] : INT64_MAX;
     uint32_t key0 = 0, key1 = 0;
@@ -194,9 +226,21 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
                     k[2] = w4.z >> 9;
                     k[3] = w4.w >> 9;
                 } else {
+                    // The four generators advance side by side; a site that is
+                    // not a Rotate position keeps its state (and draws nothing).
 #pragma unroll
-                    for (int b = 0; b < 4; ++b)
-                        if (winfo[m].vm & (1u << (8 * b))) k[b] = tiny_draw23(st[PHILOX ? 0 : m][b], tp);
+                    for (int b = 0; b < 4; ++b) {
+                        TinyState& sb = st[PHILOX ? 0 : m][b];
+                        TinyState nx = sb;
+                        tiny_advance(nx, tp);
+                        const uint32_t out = tiny_output(nx, tp) >> 9;
+                        const bool on = (winfo[m].vm >> (8 * b)) & 1u;
+                        k[b] = on ? out : 0u;
+                        sb.s0 = on ? nx.s0 : sb.s0;
+                        sb.s1 = on ? nx.s1 : sb.s1;
+                        sb.s2 = on ? nx.s2 : sb.s2;
+                        sb.s3 = on ? nx.s3 : sb.s3;
+                    }
                 }
             }
             apply(winfo[m], k);
@@ -232,46 +276,79 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
             }
         };
 
-        // Words away from the band's edge rows first, overlapping the neighbours' progress.
-        if (MAXW == 0) {
-            const int lo = has_top ? Gw : 0;
-            philox_range(lo, max(lo, nwords - (has_bot ? Gw : 0)));
-        } else {
-#pragma unroll
-            for (int m = 0; m < NW; ++m)
-                if ((wflags >> (2 * m) & 3u) == 1u) own_word(m);
-        }
-        if (ph > 0) {
-            // Halo rows of the array the neighbours flipped in the previous phase.
-            const uint32_t mask = M::written(d_prev);
-            bool ok = true;
-            if (mask) {
-                const int arr = __ffs(mask) - 1;
-                const int par = (int)((ph - 1) & 1);
-                const uint32_t tag = (uint32_t)ph;
-                for (int e = tid; e < 2 * per_side && ok; e += BLOCK) {
-                    const int side = e >= per_side;  // 0: row above (from cta-1), 1: row below (from cta+1)
-                    const int rem = e - side * per_side;
-                    const int l = rem >= a.xwords;
-                    const int w = rem - l * a.xwords;
-                    const int src = side == 0 ? cta - 1 : cta + 1;
-                    if (src < 0 || src >= nct) continue;
-                    uint32_t v;
-                    ok = wait_word(a, slot(a, src, 1 - side, par, l, 0) + w, tag, &v);
-                    if (ok) sts(lat + (l * NC + arr) * plane + (side == 0 ? 0 : nrows + 1) * W + 4 * w, v);
+        if (MAXW == 1 && split) {
+            bool fail = false;
+            if (!in_group) {
+                if (wflags & 1u) own_word(0);
+            } else {
+                if (ph > 0 && gthreads > 0) {
+                    // Halo words of the array the neighbours flipped in the previous phase.
+                    const uint32_t mask = M::written(d_prev);
+                    bool ok = true;
+                    if (mask && (poll_top || poll_bot)) {
+                        const int arr = __ffs(mask) - 1;
+                        const int par = (int)((ph - 1) & 1);
+                        const uint32_t tag = (uint32_t)ph;
+                        const int w = tid % Gw;
+                        for (int l = 0; l < a.nlat && ok; ++l) {
+                            uint32_t v;
+                            if (poll_top) {
+                                ok = wait_word(a, slot(a, cta - 1, 1, par, l, 0) + w, tag, &v);
+                                if (ok) sts(lat + (l * NC + arr) * plane + 4 * w, v);
+                            }
+                            if (poll_bot && ok) {
+                                ok = wait_word(a, slot(a, cta + 1, 0, par, l, 0) + w, tag, &v);
+                                if (ok) sts(lat + (l * NC + arr) * plane + (nrows + 1) * W + 4 * w, v);
+                            }
+                        }
+                    }
+                    fail = bar_red_or_n(1, gthreads, !ok);
                 }
+                if (!fail && wflags) own_word(0);  // the edge word, or a word of the row next to it
             }
-            if (__syncthreads_or(!ok)) return;
-        }
-        if (MAXW == 0) {
-            if (has_top) philox_range(0, Gw);
-            if (bot_edge) philox_range(nwords - Gw, nwords);
+            if (__syncthreads_or(fail)) return;
         } else {
+            // Words away from the band's edge rows first, overlapping the neighbours' progress.
+            if (MAXW == 0) {
+                const int lo = has_top ? Gw : 0;
+                philox_range(lo, max(lo, nwords - (has_bot ? Gw : 0)));
+            } else {
 #pragma unroll
-            for (int m = 0; m < NW; ++m)
-                if ((wflags >> (2 * m) & 3u) == 3u) own_word(m);
+                for (int m = 0; m < NW; ++m)
+                    if ((wflags >> (2 * m) & 3u) == 1u) own_word(m);
+            }
+            if (ph > 0) {
+                // Halo rows of the array the neighbours flipped in the previous phase.
+                const uint32_t mask = M::written(d_prev);
+                bool ok = true;
+                if (mask) {
+                    const int arr = __ffs(mask) - 1;
+                    const int par = (int)((ph - 1) & 1);
+                    const uint32_t tag = (uint32_t)ph;
+                    for (int e = tid; e < 2 * per_side && ok; e += BLOCK) {
+                        const int side = e >= per_side;  // 0: row above (from cta-1), 1: row below (from cta+1)
+                        const int rem = e - side * per_side;
+                        const int l = rem >= a.xwords;
+                        const int w = rem - l * a.xwords;
+                        const int src = side == 0 ? cta - 1 : cta + 1;
+                        if (src < 0 || src >= nct) continue;
+                        uint32_t v;
+                        ok = wait_word(a, slot(a, src, 1 - side, par, l, 0) + w, tag, &v);
+                        if (ok) sts(lat + (l * NC + arr) * plane + (side == 0 ? 0 : nrows + 1) * W + 4 * w, v);
+                    }
+                }
+                if (__syncthreads_or(!ok)) return;
+            }
+            if (MAXW == 0) {
+                if (has_top) philox_range(0, Gw);
+                if (bot_edge) philox_range(nwords - Gw, nwords);
+            } else {
+#pragma unroll
+                for (int m = 0; m < NW; ++m)
+                    if ((wflags >> (2 * m) & 3u) == 3u) own_word(m);
+            }
+            __syncthreads();
         }
-        __syncthreads();
         if (ph + 1 < a.nphases && !(cta == 0 && ph == a.drop_phase)) {
             // Publish the band's first / last row of the array flipped in this phase.
             const uint32_t mask = M::written(d);
