@@ -5,8 +5,10 @@ dominoes on Aztec diamonds and lozenges on a x b x c hexagons (volume weight
 q) from the chains themselves:
 
 1. dataset: plain fast-mode chains from the minimal tiling, run as batches
-   (include/rt_b200_batch.h) for a burn-in proportional to the side squared,
-   then sampled; their heights are summed on the device
+   (include/rt_b200_batch.h) -- chains too large for one cluster's shared
+   memory one at a time on a single-lattice walk over the whole GPU -- for a
+   burn-in proportional to the side squared, then sampled; their heights are
+   summed on the device
    (include/rt_b200_height.h) and the mean surface becomes training rows
    (features of a vertex -> where its mean height sits between the extremal
    height functions, a fraction in [0, 1]);
@@ -50,6 +52,14 @@ from .tilers import DominoTiler, LozengeTiler
 
 AZTEC, HEXAGON = "aztec", "hexagon"
 INF = np.iinfo(np.int32).max
+
+# Tiling sides (square root of the tiling's length) up to which a dataset
+# chain runs in the batched kernels: Aztec diamonds to order 470, hexagons to
+# sides 192 x 192 x 192, the sizes their cluster plans have held.  A larger
+# chain runs alone on a single-lattice walk: dominoes and uniform lozenges on
+# the bit-plane kernel, volume-weighted lozenges on the int32 kernel with
+# Philox draws.
+BATCH_MAX_SIDE = {AZTEC: 945, HEXAGON: 560}
 
 
 @dataclass(frozen=True)
@@ -185,12 +195,79 @@ def _prepare_all(specs, threads: int | None = None) -> list[Prepared]:
         return list(ex.map(prepare, specs))
 
 
+def _single_tiler(p: Prepared, device: int):
+    if p.spec.kind == AZTEC:
+        return DominoTiler(device=device, rng=_capi.RT_RNG_PLANES)
+    if p.spec.q < 1.0:
+        return LozengeTiler(device=device, kernel=_capi.RT_KERNEL_QWEIGHT, q=p.spec.q, rng=_capi.RT_RNG_PHILOX)
+    return LozengeTiler(device=device, rng=_capi.RT_RNG_PLANES)
+
+
+def single_chain_mean(p: Prepared, key: int, burn: int, gap: int, samples: int, device: int = 0):
+    """Mean height function of one chain run alone on the whole GPU: `burn`
+    sweeps from the minimal tiling, then `samples` samples `gap` sweeps apart,
+    summed on the device on the walk's own stream.  Returns (mean heights,
+    device milliseconds of the walk)."""
+    import torch
+
+    tl = _single_tiler(p, device)
+    plan = HeightPlan(p.spec.model, p.domain, device)
+    try:
+        sums = torch.zeros(p.n ** 2, dtype=torch.int64, device=f"cuda:{device}")
+        tl.upload(p.tmin)
+        stream = tl.stream
+        s = torch.cuda.ExternalStream(stream)
+        ms = 0.0
+        for seg, sweeps in enumerate([burn] + [gap] * samples):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            tl.run(sweeps * p.spec.steps_per_sweep, (key * 0x9E3779B1 + seg) & 0x7FFFFFFFFFFF)
+            e1.record(s)
+            if seg > 0:
+                plan.accumulate(tl.device_tiling(), sums.data_ptr(), stream)
+            tl.synchronize()
+            ms += e0.elapsed_time(e1)
+        return sums.cpu().numpy().astype(np.float64) / samples, ms
+    finally:
+        plan.close()
+        tl.close()
+
+
 def generate_dataset(specs, device: int = 0, samples: int = 8, burn_factor: float = 1.0, gap_factor: float = 0.05,
                      rows_per_domain: int = 4096, group_ratio: float = 2.0, seed: int = 0, log=None):
     """Training rows (X, y) from plain chains on `specs`, and per-domain stats."""
     import torch
 
-    order = sorted(range(len(specs)), key=lambda k: burn_sweeps(specs[k], burn_factor))
+    rng = np.random.default_rng(seed + 1)
+    xs, ys, stats = [], [], []
+
+    def add_rows(p: Prepared, k: int, hmean: np.ndarray, sweeps: int, alone: bool) -> None:
+        f, live = fraction(p, hmean)
+        x = features(p)
+        sel = np.flatnonzero(live)
+        if sel.size > rows_per_domain:
+            sel = rng.choice(sel, rows_per_domain, replace=False)
+        xs.append(x[sel])
+        ys.append(f[sel])
+        stats.append({"domain": p.spec.label(), "sweeps": sweeps, "rows": int(sel.size), "alone": alone})
+
+    def side(spec: DomainSpec) -> int:
+        return int(round(np.asarray(spec.domain()).size ** 0.5))
+
+    alone = [k for k in range(len(specs)) if side(specs[k]) > BATCH_MAX_SIDE[specs[k].kind]]
+    for k in alone:
+        t0 = time.perf_counter()
+        p = prepare(specs[k], device)
+        burn = burn_sweeps(specs[k], burn_factor)
+        gap = max(1, int(gap_factor * burn))
+        hmean, ms = single_chain_mean(p, seed * 1_000_003 + k, burn, gap, samples, device)
+        add_rows(p, k, hmean, burn + samples * gap, True)
+        if log:
+            log(f"dataset chain {p.spec.label()} alone, {burn + samples * gap} sweeps, device {ms:.0f} ms, "
+                f"wall {time.perf_counter() - t0:.1f} s")
+    specs_b = [k for k in range(len(specs)) if k not in set(alone)]
+
+    order = sorted(specs_b, key=lambda k: burn_sweeps(specs[k], burn_factor))
     groups, cur = [], []
     for k in order:
         if cur and burn_sweeps(specs[k], burn_factor) > group_ratio * burn_sweeps(specs[cur[0]], burn_factor):
@@ -199,8 +276,6 @@ def generate_dataset(specs, device: int = 0, samples: int = 8, burn_factor: floa
         cur.append(k)
     if cur:
         groups.append(cur)
-    rng = np.random.default_rng(seed + 1)
-    xs, ys, stats = [], [], []
     for g in groups:
         t0 = time.perf_counter()
         prep = dict(zip(g, _prepare_all([specs[k] for k in g])))
@@ -224,16 +299,7 @@ def generate_dataset(specs, device: int = 0, samples: int = 8, burn_factor: floa
                 plans[c].accumulate(buf.data_ptr(), sums[c].data_ptr())
         torch.cuda.synchronize(device)
         for c, k in enumerate(g):
-            p = prep[k]
-            hmean = sums[c].cpu().numpy().astype(np.float64) / samples
-            f, live = fraction(p, hmean)
-            x = features(p)
-            sel = np.flatnonzero(live)
-            if sel.size > rows_per_domain:
-                sel = rng.choice(sel, rows_per_domain, replace=False)
-            xs.append(x[sel])
-            ys.append(f[sel])
-            stats.append({"domain": p.spec.label(), "sweeps": burn + samples * gap, "rows": int(sel.size)})
+            add_rows(prep[k], k, sums[c].cpu().numpy().astype(np.float64) / samples, burn + samples * gap, False)
             plans[c].close()
         bt.close()
         if log:
