@@ -682,8 +682,8 @@ def chain_costs(model: int, n: int) -> tuple[int, int, int]:
     reference's storage widths) of one sweep of a chain of tiling side n:
     every colour step reads and writes each colour-array site once.  Stored
     widths: dominoes and lozenges 1 B; rectangle-triangles 4 B; triangle
-    dimers 5 byte planes and 3 16-bit planes (11 B for the 8 arrays' sites,
-    against 32 B as the reference's int arrays)."""
+    dimers 51 bit planes (6.375 B for the 8 arrays' sites, against 32 B as
+    the reference's int arrays)."""
     steps = STEPS_PER_SWEEP[model]
     if model == 0:
         att, stored, ref = (n - 2) * (n // 2 - 2), n * n, n * n
@@ -692,7 +692,7 @@ def chain_costs(model: int, n: int) -> tuple[int, int, int]:
         stored = ref = n * n * (1 if model == 1 else 4)
     else:
         m = n // 2
-        att, stored, ref = m * m, 11 * m * m, 32 * m * m
+        att, stored, ref = m * m, 51 * m * m / 8, 32 * m * m
     return att * steps, 2 * stored * steps, 2 * ref * steps
 
 

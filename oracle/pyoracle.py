@@ -67,6 +67,7 @@ def oracle() -> ctypes.CDLL:
                                               ctypes.c_double, ctypes.c_int]
         lib.orc_recttri_walk_fast.argtypes = [_P, ctypes.c_int, _I64, _I64, ctypes.c_uint32, _P]
         lib.orc_tridimer_walk_fast.argtypes = [_P, ctypes.c_int, _I64, _I64, ctypes.c_uint32]
+        lib.orc_tridimer_arrays.argtypes = [_P, ctypes.c_int, _P]
         lib.orc_project_heights.argtypes = [ctypes.c_int, _P, _I64, _P, _P, _P, _P, ctypes.c_int, _P]
         lib.orc_lozenge_q_divergence.argtypes = [_P, ctypes.c_int, _I64, _I64, ctypes.c_double]
         lib.orc_lozenge_q_divergence.restype = _I64
@@ -194,6 +195,15 @@ def tridimer_walk(t, steps, seed, params=None) -> np.ndarray:
     p, np_, keep = _table(params)
     _check(oracle().orc_tridimer_walk(a.ctypes.data, n, steps, seed, p, np_), "orc_tridimer_walk")
     return a
+
+
+def tridimer_arrays(t) -> np.ndarray:
+    """The eight state arrays (H, L, R, U, D, BH, BL, BR) of a triangle-dimer
+    tiling, shape (8, n/2, n/2) (rt_oracle.c: orc_tridimer_arrays)."""
+    a, n = _tiling(t)
+    out = np.zeros((8, n // 2, n // 2), dtype=np.int32)
+    _check(oracle().orc_tridimer_arrays(a.ctypes.data, n, out.ctypes.data), "orc_tridimer_arrays")
+    return out
 
 
 def lozenge_walk_epochs(t, steps, seeds, qweight=False, q=0.99, qcmp_double=False, params=None) -> np.ndarray:

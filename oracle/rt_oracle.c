@@ -1335,6 +1335,42 @@ static int tridimer_run(int32_t* t, int n, int64_t steps, int64_t seed, const ui
     return err;
 }
 
+/* The eight state arrays of a tiling, m x m each (m = n / 2), in the order
+ * H, L, R, U, D, BH, BL, BR: the split of TriangleDimerTiler.cpp:107-133 as
+ * tridimer_run performs it. */
+int orc_tridimer_arrays(const int32_t* t, int n, int32_t* out8) {
+    if (n < 8 || n % 2 || !t || !out8) return ORC_EINVAL;
+    const int m = n / 2;
+    const size_t mm = (size_t)m * m;
+    int32_t* tri = (int32_t*)calloc((size_t)(n / 2) * n, sizeof(int32_t));
+    int32_t* bfl = (int32_t*)calloc((size_t)n * n, sizeof(int32_t));
+    if (!tri || !bfl) {
+        free(tri);
+        free(bfl);
+        return ORC_ENOMEM;
+    }
+    td_derive(t, n, tri, bfl);
+    int32_t *H = out8, *L = out8 + mm, *R = out8 + 2 * mm, *U = out8 + 3 * mm, *D = out8 + 4 * mm;
+    int32_t *BH = out8 + 5 * mm, *BL = out8 + 6 * mm, *BR = out8 + 7 * mm;
+    for (size_t e = 0; e < 8 * mm; ++e) out8[e] = 0;
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            const int64_t at = (int64_t)(i / 2) * m + j / 2;
+            if (i % 2 == 0) {
+                if (j % 2 == 1) H[at] = t[(int64_t)i * n + j], BH[at] = bfl[(int64_t)i * n + j];
+            } else if (j % 2 == 0) {
+                L[at] = t[(int64_t)i * n + j], BL[at] = bfl[(int64_t)i * n + j];
+            } else {
+                R[at] = t[(int64_t)i * n + j], BR[at] = bfl[(int64_t)i * n + j];
+            }
+        }
+    for (int i = 0; i < n / 2; ++i)
+        for (int j = 0; j < n; ++j) (j % 2 == 0 ? D : U)[(int64_t)i * m + j / 2] = tri[(int64_t)i * n + j];
+    free(tri);
+    free(bfl);
+    return ORC_OK;
+}
+
 int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams) {
     return tridimer_run(t, n, steps, seed, params, nparams, 0, 0);
 }

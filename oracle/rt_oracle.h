@@ -66,6 +66,9 @@ int orc_lozenge_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint3
 int orc_recttri_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams,
                      const float* weights);
 int orc_tridimer_walk(int32_t* t, int n, int64_t steps, int64_t seed, const uint32_t* params, int64_t nparams);
+/* The eight triangle-dimer state arrays (H, L, R, U, D, BH, BL, BR; m x m
+ * each, m = n / 2) of a tiling, as the walks split it. */
+int orc_tridimer_arrays(const int32_t* t, int n, int32_t* out8);
 
 /* Epoch walks of the lozenge models (each epoch restarts the colour engine
  * and the TinyMT streams from seeds[e], as the domino epoch Walk does). */

@@ -24,6 +24,7 @@
 #include "../../include/rt_b200_batch.h"
 #include "rt_internal.h"
 #include "rt_models.cuh"
+#include "rt_tdplane.cuh"
 #include "rt_tridimer.cuh"
 #include "rt_word.cuh"
 
@@ -306,47 +307,51 @@ __global__ void __launch_bounds__(1024, 1) batch_site_kernel(const __grid_consta
 }
 
 // One phase of op OP over the band rows [r0, r0 + nrows) of a triangle-dimer
-// chain: only the rows TriDimerRule::live_rows admits, four sites (one Philox
-// call in drawing phases) per work item.
+// chain held as bit planes: only the rows TriDimerRule::live_rows admits, one
+// 32-site word per work item.  Drawing ops take the fast mode's draws: quad
+// cq of array row r is Philox4x32-10 of (r Gw + cq, step, chain), and a site
+// flips when its output word is below 2^31 (k = word >> 9 below 2^22).
 template <uint32_t OP, int T, int B = -1>
-__device__ __forceinline__ void td_phase(const TriDimerRule::MixedCtx& x, int r0, int nrows, int width, int tid,
-                                         int BLOCK, int64_t dstep, uint32_t chain, uint32_t key0, uint32_t key1) {
+__device__ __forceinline__ void tdp_phase(uint32_t* planes, int ps, int rs, int row0, uint32_t a, uint32_t b, int m,
+                                          int width, int r0, int nrows, int wb, int tid, int BLOCK, int64_t dstep,
+                                          uint32_t chain, uint32_t key0, uint32_t key1) {
     constexpr bool DRAWS = OP == TD_ROT_LOZ || OP == TD_ROT_TRI || OP == TD_ROT_BFLY;
     int S, o;
-    TriDimerRule::live_rows<OP>(x.a, x.b, &S, &o);
+    TriDimerRule::live_rows<OP>(a, b, &S, &o);
     const int first = r0 + ((o - r0) % S + S) % S;
     if (first >= r0 + nrows) return;
     const int nlive = (r0 + nrows - first + S - 1) / S;
+    const int items = nlive * wb;
     const int Gw = (width + 3) >> 2;
-    const int nq = nlive * Gw;
-    const int drr = BLOCK / Gw, dq = BLOCK - drr * Gw;
-    int rr = tid / Gw, cq = tid - (tid / Gw) * Gw;
-    for (int u = tid; u < nq; u += BLOCK) {
+    for (int u = tid; u < items; u += BLOCK) {
+        const int rr = u / wb, c = u - rr * wb;
         const int r = first + S * rr;
-        uint4 w4 = make_uint4(0u, 0u, 0u, 0u);
-        if (DRAWS)
-            w4 = philox4((uint32_t)(r * Gw + cq), (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32), chain, key0, key1);
+        uint32_t draw = 0u;
+        if (DRAWS) {
 #pragma unroll
-        for (int bb = 0; bb < 4; ++bb) {
-            const int j = 4 * cq + bb;
-            if (j < width) TriDimerRule::site_op<OP, T, B>(x, r, j, quad_word(w4, bb) >> 9);
+            for (int q = 0; q < 8; ++q) {
+                const int cq = 8 * c + q;
+                if (cq < Gw) {
+                    const uint4 w4 = philox4((uint32_t)(r * Gw + cq), (uint32_t)dstep, (uint32_t)((uint64_t)dstep >> 32),
+                                             chain, key0, key1);
+                    draw |= ((~w4.x >> 31) | ((~w4.y >> 31) << 1) | ((~w4.z >> 31) << 2) | ((~w4.w >> 31) << 3))
+                            << (4 * q);
+                }
+            }
         }
-        rr += drr;
-        cq += dq;
-        if (cq >= Gw) {
-            cq -= Gw;
-            ++rr;
-        }
+        const tdp::View v{planes, ps, rs, row0, r, c};
+        tdp::word_op<OP, T, B>(v, a, b, m, width, draw);
     }
 }
 
 // ---------------------------------------------------------------------------
-// Triangle dimers: the eight arrays in mixed widths (TriDimerRule::MixedCtx):
-// arrays 0-4 as bytes, 5-7 as 16-bit words, 52 KB for a side-64 chain
-// instead of 152 KB at int32, so four chains share an SM.
-// Shared memory: 5 byte planes, then 3 16-bit planes, of (rpc + 2) x wpad.
+// Triangle dimers: the eight arrays as 51 bit planes (rt_tdplane.cuh), 32
+// sites per word.  Shared memory: one zero word, then per plane (rpc + 2)
+// rows of wb + 1 words (the last word of a row stays zero), wb = words per
+// array row.  Rows move between global int32 arrays and planes one warp per
+// 32 columns, with a ballot per bit.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024, 1) batch_td_kernel(const __grid_constant__ BatchArgs b) {
+__global__ void __launch_bounds__(512, 1) batch_td_kernel(const __grid_constant__ BatchArgs b) {
     using R = TriDimerRule;
     cg::cluster_group cluster = cg::this_cluster();
     const int CL = (int)cluster.num_blocks();
@@ -354,84 +359,79 @@ __global__ void __launch_bounds__(1024, 1) batch_td_kernel(const __grid_constant
     const int ncl = gridDim.x / CL;
     const int cid = blockIdx.x / CL;
     const int BLOCK = blockDim.x, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = BLOCK >> 5;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);
 
     for (int q = cid; q < b.nchains; q += ncl) {
         const BatchChain& ch = b.chains[b.order[q]];
-        const int rows = ch.rows, W = ch.wpad, width = ch.width;
+        const int rows = ch.rows, width = ch.width;
         const int rpc = (rows + CL - 1) / CL;
         const int r0 = min(rows, rank * rpc), r1 = min(rows, r0 + rpc);
         const int nrows = r1 - r0;
-        const int plane = (rpc + 2) * W;
-        uint8_t* p8 = smem_raw;
-        int16_t* p16 = reinterpret_cast<int16_t*>(smem_raw + ((5 * plane + 15) & ~15));
-        for (int c = 0; c < 8; ++c) {
-            const int32_t* g = static_cast<const int32_t*>(ch.arr[c]);
-            for (int e = tid; e < (nrows + 2) * W; e += BLOCK) {
-                const int rr = r0 - 1 + e / W, j = e % W;
-                int32_t v = 0;
-                if (rr >= 0 && rr < ch.arows && j < width) v = g[(size_t)rr * width + j];
-                if (c < 5)
-                    p8[c * plane + e] = (uint8_t)v;
-                else
-                    p16[(c - 5) * plane + e] = (int16_t)v;
+        const int wb = (width + 31) >> 5, rs = wb + 1, ps = (rpc + 2) * rs;
+        uint32_t* planes = sm + 1;
+        for (int e = tid; e < 1 + tdp::kPlanes * ps; e += BLOCK) sm[e] = 0u;
+        __syncthreads();
+        // global int32 rows r0 - 1 .. r1 -> planes
+        for (int it = warp; it < (nrows + 2) * 8 * wb; it += nwarps) {
+            const int sr = it / (8 * wb), rem = it - sr * 8 * wb, arr = rem / wb, c = rem - arr * wb;
+            const int rr = r0 - 1 + sr, j = 32 * c + lane;
+            int32_t v = 0;
+            if (rr >= 0 && rr < ch.arows && j < width) v = static_cast<const int32_t*>(ch.arr[arr])[(size_t)rr * width + j];
+            for (int k = 0; k < tdp::bits_of(arr); ++k) {
+                const uint32_t w = __ballot_sync(0xffffffffu, (v >> k) & 1);
+                if (lane == 0) planes[(tdp::plane_of(arr) + k) * ps + sr * rs + c] = w;
             }
         }
         __syncthreads();
 
         const uint32_t key0 = (uint32_t)ch.key, key1 = (uint32_t)(ch.key >> 32);
+        const int m = ch.n / 2, row0 = r0 - 1;
         int64_t dstep = *b.step0 + b.step_add;
         for (int64_t ph = 0; ph < b.nphases; ++ph) {
             const uint32_t d = __ldg(b.phases + ph);
             const bool draws = (d & PH_DRAWS) != 0u;
-            R::MixedCtx x;
-            x.p8 = p8;
-            x.p16 = p16;
-            x.plane = plane;
-            x.w = W;
-            x.m = ch.n / 2;
-            x.row0 = r0 - 1;
-            x.op = ph_op(d);
-            x.a = ph_a(d);
-            x.b = ph_b(d);
-            switch (x.op) {
-#define RT_TD_PHASE(OPC)                                                                        \
-    case OPC:                                                                                   \
-        if (x.a == 0)                                                                           \
-            td_phase<OPC, 0>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);     \
-        else if (x.a == 1)                                                                      \
-            td_phase<OPC, 1>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);     \
-        else                                                                                    \
-            td_phase<OPC, 2>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);     \
+            const uint32_t op = ph_op(d), pa = ph_a(d), pb = ph_b(d);
+#define RT_TDP_ARGS planes, ps, rs, row0, pa, pb, m, width, r0, nrows, wb, tid, BLOCK, dstep, ch.chain, key0, key1
+            switch (op) {
+#define RT_TD_PHASE(OPC)                           \
+    case OPC:                                      \
+        if (pa == 0)                               \
+            tdp_phase<OPC, 0>(RT_TDP_ARGS);        \
+        else if (pa == 1)                          \
+            tdp_phase<OPC, 1>(RT_TDP_ARGS);        \
+        else                                       \
+            tdp_phase<OPC, 2>(RT_TDP_ARGS);        \
         break;
                 RT_TD_PHASE(TD_ROT_LOZ)
                 RT_TD_PHASE(TD_LOZ_FLIPPED)
                 RT_TD_PHASE(TD_LOZ_OTHER)
                 RT_TD_PHASE(TD_UP_FROM_LOZ)
                 case TD_TRI_OTHER:  // (a, b) in {(0, 7), (0, 0), (1, 0)} in the phase program
-                    if (x.a == 0 && x.b == 7)
-                        td_phase<TD_TRI_OTHER, 0, 7>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
-                    else if (x.a == 0 && x.b == 0)
-                        td_phase<TD_TRI_OTHER, 0, 0>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
-                    else if (x.a == 1 && x.b == 0)
-                        td_phase<TD_TRI_OTHER, 1, 0>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                    if (pa == 0 && pb == 7)
+                        tdp_phase<TD_TRI_OTHER, 0, 7>(RT_TDP_ARGS);
+                    else if (pa == 0 && pb == 0)
+                        tdp_phase<TD_TRI_OTHER, 0, 0>(RT_TDP_ARGS);
+                    else if (pa == 1 && pb == 0)
+                        tdp_phase<TD_TRI_OTHER, 1, 0>(RT_TDP_ARGS);
                     else
-                        td_phase<TD_TRI_OTHER, -1>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                        tdp_phase<TD_TRI_OTHER, -1>(RT_TDP_ARGS);
                     break;
                 RT_TD_PHASE(TD_ROT_TRI)
                 RT_TD_PHASE(TD_TRI_FLIPPED)
                 RT_TD_PHASE(TD_LOZ_FROM_TRI)
                 case TD_BFLY_FROM_LOZ:  // (a, b) in {(0, 7), (1, 3), (1, 5), (1, 6)}
-                    if (x.a == 0 && x.b == 7)
-                        td_phase<TD_BFLY_FROM_LOZ, 0, 7>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
-                    else if (x.a == 1 && x.b == 3)
-                        td_phase<TD_BFLY_FROM_LOZ, 1, 3>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
-                    else if (x.a == 1 && x.b == 5)
-                        td_phase<TD_BFLY_FROM_LOZ, 1, 5>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
-                    else if (x.a == 1 && x.b == 6)
-                        td_phase<TD_BFLY_FROM_LOZ, 1, 6>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                    if (pa == 0 && pb == 7)
+                        tdp_phase<TD_BFLY_FROM_LOZ, 0, 7>(RT_TDP_ARGS);
+                    else if (pa == 1 && pb == 3)
+                        tdp_phase<TD_BFLY_FROM_LOZ, 1, 3>(RT_TDP_ARGS);
+                    else if (pa == 1 && pb == 5)
+                        tdp_phase<TD_BFLY_FROM_LOZ, 1, 5>(RT_TDP_ARGS);
+                    else if (pa == 1 && pb == 6)
+                        tdp_phase<TD_BFLY_FROM_LOZ, 1, 6>(RT_TDP_ARGS);
                     else
-                        td_phase<TD_BFLY_FROM_LOZ, -1>(x, r0, nrows, width, tid, BLOCK, dstep, ch.chain, key0, key1);
+                        tdp_phase<TD_BFLY_FROM_LOZ, -1>(RT_TDP_ARGS);
                     break;
                 RT_TD_PHASE(TD_ROT_BFLY)
                 RT_TD_PHASE(TD_BFLY_SAME)
@@ -439,6 +439,7 @@ __global__ void __launch_bounds__(1024, 1) batch_td_kernel(const __grid_constant
                 RT_TD_PHASE(TD_BFLY_22)
                 RT_TD_PHASE(TD_BFLY_23_LOZ)
 #undef RT_TD_PHASE
+#undef RT_TDP_ARGS
                 default: break;
             }
             if (draws) ++dstep;
@@ -449,17 +450,13 @@ __global__ void __launch_bounds__(1024, 1) batch_td_kernel(const __grid_constant
                     while (mask) {
                         const int arr = __ffs(mask) - 1;
                         mask &= mask - 1;
-                        for (int e = tid; e < 2 * W; e += BLOCK) {
-                            const int side = e >= W, xx = e - side * W;
+                        const int nb = tdp::bits_of(arr), p0 = tdp::plane_of(arr);
+                        for (int e = tid; e < 2 * nb * wb; e += BLOCK) {
+                            const int side = e >= nb * wb, rem = e - side * nb * wb, k = rem / wb, c = rem - k * wb;
                             if ((side == 0 && rank == 0) || (side == 1 && r1 >= rows)) continue;
-                            const int mine = (side == 0 ? 0 : nrows + 1) * W + xx;
-                            const int theirs = (side == 0 ? rpc : 1) * W + xx;
-                            const int peer = rank + (side == 0 ? -1 : 1);
-                            if (arr < 5)
-                                p8[arr * plane + mine] = *cluster.map_shared_rank(p8 + arr * plane + theirs, peer);
-                            else
-                                p16[(arr - 5) * plane + mine] =
-                                    *cluster.map_shared_rank(p16 + (arr - 5) * plane + theirs, peer);
+                            const int mine = (p0 + k) * ps + (side == 0 ? 0 : nrows + 1) * rs + c;
+                            const int theirs = (p0 + k) * ps + (side == 0 ? rpc : 1) * rs + c;
+                            planes[mine] = *cluster.map_shared_rank(planes + theirs, rank + (side == 0 ? -1 : 1));
                         }
                     }
                 }
@@ -468,13 +465,14 @@ __global__ void __launch_bounds__(1024, 1) batch_td_kernel(const __grid_constant
                 __syncthreads();
             }
         }
-        for (int c = 0; c < 8; ++c) {
-            int32_t* g = static_cast<int32_t*>(ch.arr[c]);
-            for (int e = tid; e < nrows * width; e += BLOCK) {
-                const int rr = e / width, j = e % width;
-                const int at = (rr + 1) * W + j;
-                g[(size_t)(r0 + rr) * width + j] = c < 5 ? (int32_t)p8[c * plane + at] : (int32_t)p16[(c - 5) * plane + at];
-            }
+        // planes -> global int32 rows r0 .. r1 - 1
+        for (int it = warp; it < nrows * 8 * wb; it += nwarps) {
+            const int sr = 1 + it / (8 * wb), rem = it - (sr - 1) * 8 * wb, arr = rem / wb, c = rem - arr * wb;
+            const int j = 32 * c + lane;
+            int32_t v = 0;
+            for (int k = 0; k < tdp::bits_of(arr); ++k)
+                v |= (int32_t)((planes[(tdp::plane_of(arr) + k) * ps + sr * rs + c] >> lane) & 1u) << k;
+            if (j < width) static_cast<int32_t*>(ch.arr[arr])[(size_t)(r0 - 1 + sr) * width + j] = v;
         }
         cluster_or_block_sync(cluster, CL);
     }
@@ -567,9 +565,9 @@ size_t smem_for(const Chain& c, int cl) {
     if (word_fam(c.fam)) {
         return 16 + (size_t)c.ncol * (rpc + 2) * wpad + 16 + (size_t)((2 * rpc + 3) & ~3) + 2 * 4 * (size_t)(wpad / 4);
     }
-    if (c.fam == FAM_TRIDIMER) {  // batch_td_kernel: 5 byte planes, then 3 16-bit planes
-        const size_t plane = (size_t)(rpc + 2) * wpad;
-        return ((5 * plane + 15) & ~(size_t)15) + 3 * plane * 2;
+    if (c.fam == FAM_TRIDIMER) {  // batch_td_kernel: one zero word, then 51 planes of (rpc + 2) x (wb + 1) words
+        const size_t wb = (size_t)(c.width + 31) / 32;
+        return 4 * (1 + (size_t)tdp::kPlanes * (rpc + 2) * (wb + 1));
     }
     return (size_t)c.ncol * (rpc + 2) * wpad * 4;
 }
@@ -663,7 +661,10 @@ bool fill_plan(rt_batch* b, int f, int cl, int block, Plan* p) {
     BatchFn fn = batch_fn(f);
     cudaFuncAttributes fa;
     if (cudaFuncGetAttributes(&fa, (const void*)fn) != cudaSuccess) return false;
-    if (smem + fa.sharedSizeBytes > (size_t)optin || block > fa.maxThreadsPerBlock) return false;
+    // A family's kernel may be built for fewer threads than asked for (the
+    // bit-plane triangle-dimer kernel: 512); it then runs with its maximum.
+    block = std::min(block, fa.maxThreadsPerBlock);
+    if (smem + fa.sharedSizeBytes > (size_t)optin) return false;
     if (cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return false;
     if (cl > 8 && cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
@@ -769,12 +770,12 @@ rt_status upload(rt_batch* b) {
             if (c.kind == 3) {
                 std::vector<int32_t> arrays((size_t)8 * c.arows * c.width);
                 td_split_host(c.start.data(), c.n, arrays.data());
-                // batch_td_kernel keeps arrays 0-4 as bytes and 5-7 as 16-bit words
+                // batch_td_kernel keeps array a as tdp::bits_of(a) bit planes
                 const size_t per = (size_t)c.arows * c.width;
                 for (size_t e = 0; e < 8 * per; ++e) {
                     const int32_t v = arrays[e];
-                    if (e < 5 * per ? (v < 0 || v > 255) : (v < -32768 || v > 32767))
-                        return b->fail(RT_E_INVAL, "triangle-dimer state out of range for the batch storage");
+                    if (v < 0 || v >= (1 << tdp::bits_of((int)(e / per))))
+                        return b->fail(RT_E_INVAL, "triangle-dimer state out of range for the bit planes");
                 }
                 for (int a = 0; a < 8; ++a)
                     cudaMemcpyAsync(arr[a], arrays.data() + (size_t)a * c.arows * c.width,
@@ -845,7 +846,10 @@ rt_status plan_family(rt_batch* b, int f) {
     for (int c : cls)
         for (int bl : blocks) {
             Plan p;
-            if (fill_plan(b, f, c, bl, &p)) cand.push_back(p);
+            if (!fill_plan(b, f, c, bl, &p)) continue;
+            bool seen = false;  // a capped block size can repeat a candidate
+            for (const Plan& q : cand) seen = seen || (q.cl == p.cl && q.block == p.block);
+            if (!seen) cand.push_back(p);
         }
     if (cand.empty()) return b->fail(RT_E_INVAL, "no cluster size holds the largest chain of a family in shared memory");
     if (cand.size() == 1) {

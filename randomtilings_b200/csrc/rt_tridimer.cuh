@@ -13,37 +13,24 @@
 // (M, M) NDRange owns stream j + M i (src/TinyMT/tinymt.clh:24-30).
 #pragma once
 
+#include "rt_tdops.h"
+#ifdef __CUDACC__
 #include "rt_models.cuh"
+#endif
 
 namespace rtb {
 
-enum : uint32_t {
-    TD_ROT_LOZ = 16,        // a = orientation t, b = class c           (RotateLozenges)            [draws]
-    TD_LOZ_FLIPPED = 17,    // a = t, b = c                             (UpdateLozengesFlipped)
-    TD_LOZ_OTHER = 18,      // a = t                                    (UpdateLozenges0/1/2)
-    TD_UP_FROM_LOZ = 19,    //                                          (UpdateTriangleUFromLozenges)
-    TD_TRI_OTHER = 20,      // a = 0: D from U, 1: U from D; b = butterflies refreshed from lozenges
-    TD_ROT_TRI = 21,        // a = 1: down, 0: up; b = class c          (RotateTriangles)           [draws]
-    TD_TRI_FLIPPED = 22,    // a = 1: down, 0: up; b = c                (UpdateTrianglesFlipped1/0)
-    TD_LOZ_FROM_TRI = 23,   //                                          (UpdateLozenge{H,L,R}FromTriangles)
-    TD_BFLY_FROM_LOZ = 24,  // b = butterfly mask; a = 1: also U from lozenges
-    TD_ROT_BFLY = 25,       // a = t, b = p1 | p2 << 2                  (RotateButterflys)          [draws]
-    TD_BFLY_SAME = 26,      // a = t, b = p1 | p2 << 2                  (UpdateButterflysFlipped?1)
-    TD_BFLY_21 = 27,        // a = t, b = p1
-    TD_BFLY_22 = 28,        // a = t, b = p1
-    TD_BFLY_23_LOZ = 29     // a = t, b = p1: pass 23, then the lozenges from that butterfly array
-};
 
 struct TriDimerRule {
     using Elem = int32_t;
     static constexpr int NCOL = 8;
     static constexpr int ROFF = 0;
     static constexpr int COFF = 0;
-    __device__ static uint32_t stream_id(const WalkArgs& a, int r, int c) {
+    TD_HD static uint32_t stream_id(const WalkArgs& a, int r, int c) {
         return (uint32_t)c + (uint32_t)(a.n / 2) * (uint32_t)r;
     }
     // Arrays a phase writes (bit k = array k); their halo rows are exchanged.
-    __device__ static uint32_t written(uint32_t d) {
+    TD_HD static uint32_t written(uint32_t d) {
         const uint32_t op = ph_op(d), a = ph_a(d), b = ph_b(d);
         switch (op) {
             case TD_ROT_LOZ:
@@ -63,37 +50,18 @@ struct TriDimerRule {
             default: return 0u;
         }
     }
-    // Storage of the eight arrays: int32 planes (the walk kernels), or the
-    // batch kernel's mixed widths (MixedCtx).  Either way the rule reads and
-    // writes values through get / set, so the arithmetic is the same.
+    // Storage of the eight arrays: int32 planes of the walk kernels.  The
+    // rule reads and writes values through get / set (accessors of other
+    // layouts plug in the same way); the batch kernel keeps the arrays as
+    // bit planes instead (rt_tdplane.cuh), with the same arithmetic.
     struct Ctx {
         int32_t* base;
         int plane, w, m, row0;
         uint32_t op, a, b;
-        __device__ int32_t get(int arr, int ii, int jj) const { return base[arr * plane + (ii - row0) * w + jj]; }
-        __device__ void set(int arr, int ii, int jj, int32_t v) const { base[arr * plane + (ii - row0) * w + jj] = v; }
+        TD_HD int32_t get(int arr, int ii, int jj) const { return base[arr * plane + (ii - row0) * w + jj]; }
+        TD_HD void set(int arr, int ii, int jj, int32_t v) const { base[arr * plane + (ii - row0) * w + jj] = v; }
     };
-    // The batch kernel's storage: arrays 0-4 (lozenge and triangle states,
-    // values < 64) as bytes, arrays 5-7 (butterfly states, values < 512) as
-    // 16-bit words; `plane` elements per array in either width.
-    struct MixedCtx {
-        uint8_t* p8;
-        int16_t* p16;
-        int plane, w, m, row0;
-        uint32_t op, a, b;
-        __device__ int32_t get(int arr, int ii, int jj) const {
-            const int o = (ii - row0) * w + jj;
-            return arr < 5 ? (int32_t)p8[arr * plane + o] : (int32_t)p16[(arr - 5) * plane + o];
-        }
-        __device__ void set(int arr, int ii, int jj, int32_t v) const {
-            const int o = (ii - row0) * w + jj;
-            if (arr < 5)
-                p8[arr * plane + o] = (uint8_t)v;
-            else
-                p16[(arr - 5) * plane + o] = (int16_t)v;
-        }
-    };
-    __device__ static Ctx ctx(const WalkArgs& ar, int32_t* planes, int plane, uint32_t d, int row0) {
+    TD_HD static Ctx ctx(const WalkArgs& ar, int32_t* planes, int plane, uint32_t d, int row0) {
         Ctx x;
         x.row0 = row0;
         x.base = planes;
@@ -107,21 +75,21 @@ struct TriDimerRule {
     }
 
     // ---- helpers ------------------------------------------------------------
-    __device__ static int dg(int32_t x, int k) { return (int)(((uint32_t)x >> (2 * k)) & 3u); }
+    TD_HD static int dg(int32_t x, int k) { return (int)(((uint32_t)x >> (2 * k)) & 3u); }
     // 0->0, 1->2, 2->3, 3->1 and 0->0, 1->3, 2->1, 3->2 as 2-bit tables
-    __device__ static int cyc_up(int v) { return (int)((0x78u >> (2 * v)) & 3u); }
-    __device__ static int cyc_dn(int v) { return (int)((0x9Cu >> (2 * v)) & 3u); }
-    __device__ static int32_t pack(int t1, int t4, int t16, int t64, int c) {
+    TD_HD static int cyc_up(int v) { return (int)((0x78u >> (2 * v)) & 3u); }
+    TD_HD static int cyc_dn(int v) { return (int)((0x9Cu >> (2 * v)) & 3u); }
+    TD_HD static int32_t pack(int t1, int t4, int t16, int t64, int c) {
         return t1 + 4 * t4 + 16 * t16 + 64 * t64 + 256 * c;
     }
-    __device__ static int tri_digit(int32_t v) {
+    TD_HD static int tri_digit(int32_t v) {
         return ((v & 48) == 16 ? 1 : 0) + ((v & 3) == 3 ? 2 : 0) + ((v & 12) == 8 ? 3 : 0);
     }
 
     // Butterfly state of orientation `which` from the lozenge arrays
     // (UpdateButterflys{H,L,R}FromLozenge, triangledimerkernel.cl:118-189).
     template <class A>
-    __device__ static int32_t bfly_from_loz(const A& x, int which, int i, int j) {
+    TD_HD static int32_t bfly_from_loz(const A& x, int which, int i, int j) {
         auto at = [&](int arr, int ii, int jj) { return x.get(arr, ii, jj); };
         int t1, t4, t16, t64, c;
         if (which == 0) {
@@ -151,7 +119,7 @@ struct TriDimerRule {
 
     // Up-triangle state from the lozenges (UpdateTriangleUFromLozenges, :96-116).
     template <class A>
-    __device__ static int32_t up_from_loz(const A& acc, int i, int j) {
+    TD_HD static int32_t up_from_loz(const A& acc, int i, int j) {
         auto at = [&](int arr, int ii, int jj) { return acc.get(arr, ii, jj); };
         const int32_t l0 = at(1, i, j), l1 = at(1, i, j + 1), h0 = at(0, i, j), h1 = at(0, i + 1, j);
         const int x = ((l0 & 1) ? 1 : 0) + ((h0 & 8) ? 2 : 0) + ((h1 & 1) ? 3 : 0);
@@ -160,17 +128,17 @@ struct TriDimerRule {
         return x + 4 * y + 16 * z;
     }
 
-    __device__ static int slice(int t, int i, int j) { return t == 0 ? i % 3 : t == 1 ? j % 3 : (i + j) % 3; }
-    __device__ static int bpar(int t, int i, int j) { return t == 1 ? (i & 1) : (j & 1); }
+    TD_HD static int slice(int t, int i, int j) { return t == 0 ? i % 3 : t == 1 ? j % 3 : (i + j) % 3; }
+    TD_HD static int bpar(int t, int i, int j) { return t == 1 ? (i & 1) : (j & 1); }
 
-    __device__ static void site(const WalkArgs&, const Ctx& x, int, int i, int j, uint32_t k) { site_on(x, i, j, k); }
+    TD_HD static void site(const WalkArgs&, const Ctx& x, int, int i, int j, uint32_t k) { site_on(x, i, j, k); }
 
     // One site of the phase whose op is OP (a compile-time constant: every
     // other case of the switch below folds away).  T >= 0 fixes the phase's
     // argument a (the orientation t) at compile time too, B >= 0 its
     // argument b; negative values read x.a / x.b.
     template <uint32_t OP, int T = -1, int B = -1, class A>
-    __device__ static void site_op(const A& x, int i, int j, uint32_t k) {
+    TD_HD static void site_op(const A& x, int i, int j, uint32_t k) {
         auto at = [&](int arr, int ii, int jj) { return x.get(arr, ii, jj); };
         auto put = [&](int arr, int ii, int jj, int32_t v) { x.set(arr, ii, jj, v); };
         const bool interior = i >= 1 && i <= x.m - 2 && j >= 1 && j <= x.m - 2;
@@ -399,7 +367,7 @@ struct TriDimerRule {
     }
 
     template <class A>
-    __device__ static void site_on(const A& x, int i, int j, uint32_t k) {
+    TD_HD static void site_on(const A& x, int i, int j, uint32_t k) {
         switch (x.op) {
             case TD_ROT_LOZ: site_op<TD_ROT_LOZ>(x, i, j, k); break;
             case TD_LOZ_FLIPPED: site_op<TD_LOZ_FLIPPED>(x, i, j, k); break;
@@ -424,7 +392,7 @@ struct TriDimerRule {
     // (i mod 2 or i mod 3 for orientation 0, i mod 2 for some of
     // orientation 1) skip the other rows; all others have S = 1.
     template <uint32_t OP>
-    __device__ static void live_rows(uint32_t a, uint32_t b, int* S, int* o) {
+    TD_HD static void live_rows(uint32_t a, uint32_t b, int* S, int* o) {
         const int t = (int)a;
         *S = 1;
         *o = 0;
