@@ -187,11 +187,11 @@ rt_status rt_last_run_info(rt_tiler* h, int64_t* phases, int64_t* launches);
  * the caller's DEVICE buffer (N*N int32, in and out) and no handle exists:
  * every other byte the walk needs sits in one built-in device array of
  * 16 MiB per GPU, kept until the process exits.  Walks that need more
- * (tiling side x steps) are rejected with RT_E_INVAL.  The first call on a
- * device looks the array up on that device; make it before any stream
- * capture.  Calls share the array: calls that overlap on one GPU race.
- * Runs on cfg->stream (NULL = the default stream) and returns after the walk
- * has finished there.  The tiling is written back only after a walk that
+ * (tiling side x steps) are rejected with RT_E_INVAL.  Calls share the
+ * array: calls that overlap on one GPU race.  Runs on cfg->stream (NULL =
+ * the default stream) and returns after the walk has finished there: the
+ * call is synchronous and must not be made while that stream is being
+ * captured into a graph.  The tiling is written back only after a walk that
  * finished: after RT_E_INVAL or RT_E_TIMEOUT it holds its input unchanged.
  * A failure message goes to errbuf (errcap bytes) when errbuf is not NULL. */
 rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_tiling, int32_t n, int64_t steps, int64_t seed,
