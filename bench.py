@@ -393,9 +393,9 @@ def run_b200(args) -> None:
                 "frac": achieved / peak,
                 "peak_kind": peak_kind,
                 "traffic": args.traffic,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this kernel "
-                                  "on this workload; a launch reads the lattice in and writes it back once "
-                                  "whatever its step count",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 600-colour-step "
+                                  "launch of this kernel on this workload (a capture, not this run); a launch "
+                                  "reads the lattice in and writes it back once whatever its step count",
                 "dram_gbs": args.traffic / (per_launch_ms / 1e3) / 1e9,
                 "limiter": "phase latency: the lattice and the TinyMT states stay on chip for the whole launch, "
                            "so a colour step costs the latency of one word's update plus the exchange of edge "
@@ -866,9 +866,11 @@ def main() -> None:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--cpu-segments", type=int, default=2, help="steps timed for cpu_baseline (about 10 s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    # dram__bytes_read.sum + dram__bytes_write.sum of one word_kernel launch on this workload (ncu, one
-    # pass): the lattice stays on chip, so a launch of any number of colour steps moves the same bytes.
-    ap.add_argument("--traffic", type=float, default=1149184.0,
+    # dram__bytes_read.sum + dram__bytes_write.sum of one word_kernel launch on this workload (ncu
+    # --set full of a 600-colour-step launch of this build: 1,160,960 B read, 0 written).  The
+    # lattice stays on chip, so a launch of any number of colour steps moves the same bytes; a
+    # timed run cannot read DRAM counters, so the figure comes from that capture.
+    ap.add_argument("--traffic", type=float, default=1160960.0,
                     help="dram bytes per walk launch from an ncu capture (reported in roofline.traffic)")
     ap.add_argument("--batch-chains", type=int, default=4096)
     ap.add_argument("--batch-sweeps", type=int, default=5000)
