@@ -405,8 +405,9 @@ def run_b200(args) -> None:
                 "launch_ms": per_launch_ms,
             },
             "q_weighted": leg(ms_q, attempts, world, dist, {
-                "q": 0.99, "compare": "float32", "dtype": "int32",
-                "hbm_gbs_algorithmic": algorithmic_bytes_per_step(n, 4) * SEGMENT / (sum(ms_q) / len(ms_q) / 1e3) / 1e9}),
+                "q": 0.99, "compare": "float32", "dtype": "int8",
+                "kernel": "rtb::word_kernel<FAM_LOZENGE8, 1, bit-exact, q> (add below thr[2], remove in [2^22, thr[3]))",
+                "hbm_gbs_algorithmic": algorithmic_bytes_per_step(n, 1) * SEGMENT / (sum(ms_q) / len(ms_q) / 1e3) / 1e9}),
             "fast_mode": leg(ms_f, attempts, world, dist, {
                 "rng": "Philox4x32-10 keyed by (position quad, step, chain), cyclic colours", "dtype": "int8"}),
             "bit_planes": leg(ms_p, attempts, world, dist, {

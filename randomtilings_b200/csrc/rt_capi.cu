@@ -145,7 +145,7 @@ rt_status choose_plan(int family, int device, int nlat, int rows, int cols, int 
                       std::string* err) {
     if (planes) return plan_plane_walk(family, device, nlat, rows, width, ctas_hint, depth_hint, plan, err);
     rt_status s = RT_E_INVAL;
-    if (kernel_choice != 1 && uniform && word_family(family))
+    if (kernel_choice != 1 && uniform && (word_family(family) || family == FAM_QLOZENGE8))
         s = plan_word_walk(family, device, nlat, rows, width, fast, ctas_hint, plan, err, weighted);
     if (s == RT_OK || kernel_choice == 2) return s;
     return plan_walk(family, device, nlat, rows, cols, width, uniform, fast, plan, err);
@@ -160,7 +160,7 @@ void family_thresholds(int family, double q, int qcmp, uint32_t thr[4]) {
             thr[0] = below_threshold(0.4);
             thr[1] = below_threshold(0.8);
             break;
-        case FAM_QLOZENGE32:  // qlozengekernel.cl:18-26
+        case FAM_QLOZENGE8:  // qlozengekernel.cl:18-26
             if (qcmp == RT_QCMP_DOUBLE) {
                 thr[0] = floor_scaled(q, 22);
                 thr[1] = floor_scaled(1.0 / q, 24);
@@ -170,6 +170,11 @@ void family_thresholds(int family, double q, int qcmp, uint32_t thr[4]) {
                 thr[0] = floor_scaled((double)qf, 22);
                 thr[1] = floor_scaled((double)inv, 24);
             }
+            // The same rule as bounds on k for the word kernel: add iff
+            // k < thr[2] (k < 2^22 and k <= thr[0]); remove iff
+            // 2^22 <= k < thr[3] (k - 2^22 <= thr[1]); k < 2^23 always.
+            thr[2] = (uint32_t)std::min<uint64_t>(1u << 22, (uint64_t)thr[0] + 1);
+            thr[3] = (uint32_t)std::min<uint64_t>(1u << 23, (uint64_t)(1u << 22) + thr[1] + 1);
             break;
         default: break;
     }
@@ -262,7 +267,7 @@ rt_status rt_create(const rt_config* cfg, rt_tiler** out) {
             break;
         case RT_LOZENGE:
             if (cfg->kernel == RT_KERNEL_DEFAULT) family = FAM_LOZENGE8, elem = 1;
-            else if (cfg->kernel == RT_KERNEL_QWEIGHT) family = FAM_QLOZENGE32, elem = 4;
+            else if (cfg->kernel == RT_KERNEL_QWEIGHT) family = FAM_QLOZENGE8, elem = 1;
             ncol = 3, kind = 1;
             break;
         case RT_RECTTRI:
@@ -288,7 +293,7 @@ rt_status rt_create(const rt_config* cfg, rt_tiler** out) {
         g_create_error = "bit-plane mode exists for dominoes and uniform lozenges";
         return RT_E_INVAL;
     }
-    if (family == FAM_QLOZENGE32 && (!(cfg->q >= 0.0) || !std::isfinite(cfg->q))) {
+    if (family == FAM_QLOZENGE8 && (!(cfg->q >= 0.0) || !std::isfinite(cfg->q))) {
         g_create_error = "q must be a finite non-negative number";
         return RT_E_INVAL;
     }
@@ -773,7 +778,7 @@ rt_status rt_cftp(rt_tiler* h, const int32_t* tmax, const int32_t* tmin, int32_t
                   int32_t schedule, int64_t master_seed, int32_t max_trials, int32_t* out_tiling,
                   rt_cftp_stats* stats) {
     if (!h) return RT_E_INVAL;
-    if (h->family != FAM_DOMINO_HB && h->family != FAM_LOZENGE8 && h->family != FAM_QLOZENGE32)
+    if (h->family != FAM_DOMINO_HB && h->family != FAM_LOZENGE8 && h->family != FAM_QLOZENGE8)
         return h->fail(RT_E_INVAL,
                        "CFTP needs a monotone kernel: the domino heat bath (RT_KERNEL_CFTP, dominokernelCFTP.cl) "
                        "or a lozenge kernel");

@@ -16,7 +16,7 @@ enum Family : int {
     FAM_DOMINO = 0,      // dominokernel.cl, int8
     FAM_DOMINO_HB = 1,   // dominokernelCFTP.cl, int8
     FAM_LOZENGE8 = 2,    // lozengekernel.cl, int8
-    FAM_QLOZENGE32 = 3,  // qlozengekernel.cl, int32
+    FAM_QLOZENGE8 = 3,   // qlozengekernel.cl; int8 (the reference's int states are below 64)
     FAM_RECTTRI = 4,     // recttrianglekernel.cl, int32
     FAM_TRIDIMER = 5     // triangledimerkernel.cl, 8 int32 arrays
 };

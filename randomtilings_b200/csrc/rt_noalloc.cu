@@ -92,7 +92,7 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
     } else if (cfg->model == RT_LOZENGE && cfg->kernel == RT_KERNEL_DEFAULT) {
         family = FAM_LOZENGE8, ncol = 3, kind = 1, elem = 1;
     } else if (cfg->model == RT_LOZENGE && cfg->kernel == RT_KERNEL_QWEIGHT) {
-        family = FAM_QLOZENGE32, ncol = 3, kind = 1, elem = 4;
+        family = FAM_QLOZENGE8, ncol = 3, kind = 1, elem = 1;
     } else if (cfg->model == RT_RECTTRI && cfg->kernel == RT_KERNEL_DEFAULT) {
         family = FAM_RECTTRI, ncol = 3, kind = 2, elem = 4;
     }
@@ -100,7 +100,7 @@ extern "C" rt_status rt_walk_device_noalloc(const rt_config* cfg, int32_t* d_til
         say(errbuf, errcap, "unsupported model / kernel / rng combination");
         return RT_E_INVAL;
     }
-    if (family == FAM_QLOZENGE32 && !(cfg->q >= 0.0 && std::isfinite(cfg->q))) {
+    if (family == FAM_QLOZENGE8 && !(cfg->q >= 0.0 && std::isfinite(cfg->q))) {
         say(errbuf, errcap, "q must be a finite non-negative number");
         return RT_E_INVAL;
     }

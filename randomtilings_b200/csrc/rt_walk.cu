@@ -274,7 +274,7 @@ static KernelFn kernel_for(int family, bool uniform, bool philox) {
         case FAM_DOMINO: return pick_kernel<DominoRule<false>>(uniform, philox);
         case FAM_DOMINO_HB: return pick_kernel<DominoRule<true>>(uniform, philox);
         case FAM_LOZENGE8: return pick_kernel<ThreeColour<int8_t, LozengeRule<false>>>(uniform, philox);
-        case FAM_QLOZENGE32: return pick_kernel<ThreeColour<int32_t, LozengeRule<true>>>(uniform, philox);
+        case FAM_QLOZENGE8: return pick_kernel<ThreeColour<int8_t, LozengeRule<true>>>(uniform, philox);
         case FAM_RECTTRI: return pick_kernel<ThreeColour<int32_t, RectTriRule>>(uniform, philox);
         case FAM_TRIDIMER: return pick_kernel<TriDimerRule>(uniform, philox);
         default: return nullptr;
@@ -282,7 +282,7 @@ static KernelFn kernel_for(int family, bool uniform, bool philox) {
 }
 
 static int family_ncol(int family) { return family <= FAM_DOMINO_HB ? 2 : family == FAM_TRIDIMER ? 8 : 3; }
-static int family_elem(int family) { return family == FAM_LOZENGE8 || family <= FAM_DOMINO_HB ? 1 : 4; }
+static int family_elem(int family) { return family <= FAM_QLOZENGE8 ? 1 : 4; }
 static int family_xslots(int family) { return family == FAM_TRIDIMER ? 4 : 1; }
 
 size_t walk_smem_bytes(int family, int nlat, int rows_per_cta, int cols, int width, bool philox) {

@@ -45,9 +45,11 @@ __device__ __forceinline__ bool bar_red_or_n(int id, int n, bool v) {
 // (band rows + 2 halo rows) x wpad bytes, then 16 bytes of slack (the funnel
 // shifts read one word beyond a row; those bytes only reach sites outside
 // the update / flip masks).
-// WT: periodic weights (a.wper > 0) -- a per-site threshold instead of thr[0];
-// a separate instantiation, so that the unweighted kernel carries none of it.
-template <int FAM, int MAXW, bool PHILOX, int LB, bool WT>
+// WT: 0 the uniform rules; 1 periodic weights (a.wper > 0), a per-site
+// threshold instead of thr[0]; 2 the lozenges' volume weight q
+// (qlozengekernel.cl), add below thr[2], remove in [2^22, thr[3]).  Separate
+// instantiations, so that the uniform kernel carries none of it.
+template <int FAM, int MAXW, bool PHILOX, int LB, int WT>
 __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ WalkArgs a) {
     using M = WordModel<FAM>;
     constexpr int NC = M::NC;
@@ -191,24 +193,29 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
         auto apply = [&](const WordInfo& wi, const uint32_t (&k)[4]) {
             uint32_t m0 = 0, m1 = 0;
             if (draws) {
-                if (WT && FAM == FAM_DOMINO_HB) {
+                if (WT == 1 && FAM == FAM_DOMINO_HB) {
                     // weighted heat bath: a threshold per site from its vertex (i, j);
                     // array column c of the rotated array A is vertex column 2 c + ((i + A) & 1)
                     const int i = a0 + wi.off / W - 1, c0 = wi.off % W, par = (i + 1 - (int)ph_a(d)) & 1;
 #pragma unroll
                     for (int b = 0; b < 4; ++b)
                         m0 |= (uint32_t)(k[b] < weight_thr(a, i, 2 * (c0 + b) + par)) << (8 * b);
-                } else if (WT && FAM == FAM_LOZENGE8) {
+                } else if (WT == 1 && FAM == FAM_LOZENGE8) {
                     // weighted lozenges: the add threshold of each site's vertex; array
                     // column c of colour C is vertex column 3 c + (C + i) mod 3
                     const int i = a0 + wi.off / W - 1, c0 = wi.off % W, rem = ((int)ph_a(d) + i) % 3;
 #pragma unroll
                     for (int b = 0; b < 4; ++b)
                         m0 |= (uint32_t)(k[b] < weight_thr(a, i, 3 * (c0 + b) + rem)) << (8 * b);
+                } else if (WT == 2) {
+                    m0 = below4(k, a.thr[2]);
                 } else {
                     m0 = below4(k, a.thr[0]);
                 }
-                if (!M::DOM) m1 = below4(k, a.thr[1]) & ~m0;
+                if (WT == 2)
+                    m1 = below4(k, a.thr[3]) & ~below4(k, 1u << 22);
+                else if (!M::DOM)
+                    m1 = below4(k, a.thr[1]) & ~m0;
             }
             word_phase<FAM>(P, 0, W, wi, m0, m1);
             if (a.nlat > 1) word_phase<FAM>(P, lat1, W, wi, m0, m1);
@@ -387,7 +394,7 @@ __global__ void __launch_bounds__(LB, 1) word_kernel(const __grid_constant__ Wal
 
 using KernelFn = void (*)(WalkArgs);
 
-template <int FAM, bool WT>
+template <int FAM, int WT>
 static KernelFn word_fn(int maxw, bool philox) {
     if (philox) {
         switch (maxw) {
@@ -408,11 +415,12 @@ static KernelFn word_fn(int maxw, bool philox) {
 
 static KernelFn word_kernel_for(int family, int maxw, bool philox, bool weighted) {
     switch (family) {
-        case FAM_DOMINO: return word_fn<FAM_DOMINO, false>(maxw, philox);
+        case FAM_DOMINO: return word_fn<FAM_DOMINO, 0>(maxw, philox);
         case FAM_DOMINO_HB:
-            return weighted ? word_fn<FAM_DOMINO_HB, true>(maxw, philox) : word_fn<FAM_DOMINO_HB, false>(maxw, philox);
+            return weighted ? word_fn<FAM_DOMINO_HB, 1>(maxw, philox) : word_fn<FAM_DOMINO_HB, 0>(maxw, philox);
         case FAM_LOZENGE8:
-            return weighted ? word_fn<FAM_LOZENGE8, true>(maxw, philox) : word_fn<FAM_LOZENGE8, false>(maxw, philox);
+            return weighted ? word_fn<FAM_LOZENGE8, 1>(maxw, philox) : word_fn<FAM_LOZENGE8, 0>(maxw, philox);
+        case FAM_QLOZENGE8: return weighted ? nullptr : word_fn<FAM_LOZENGE8, 2>(maxw, philox);
         default: return nullptr;
     }
 }
@@ -421,7 +429,7 @@ bool word_family(int family) { return family == FAM_DOMINO || family == FAM_DOMI
 
 rt_status plan_word_walk(int family, int device, int nlat, int rows, int width, bool philox, int ctas_hint,
                          WalkPlan* plan, std::string* err, bool weighted) {
-    if (!word_family(family)) {
+    if (!word_family(family) && family != FAM_QLOZENGE8) {
         *err = "no word kernel for this model";
         return RT_E_INVAL;
     }
@@ -431,7 +439,7 @@ rt_status plan_word_walk(int family, int device, int nlat, int rows, int width, 
         *err = "cudaDeviceGetAttribute failed";
         return RT_E_CUDA;
     }
-    const int nc = family == FAM_LOZENGE8 ? 3 : 2;
+    const int nc = family == FAM_LOZENGE8 || family == FAM_QLOZENGE8 ? 3 : 2;
     const int wpad = (width + 3) & ~3;
     const int gw = wpad / 4;
     int ctas = std::max(1, std::min(ctas_hint > 0 ? ctas_hint : sms, rows));
