@@ -2,9 +2,10 @@
 // conditions (include/rt_b200_sixv.h).
 //
 // The reference names the model (README.md:3) without code; this is the
-// domino height machinery applied to it.  Heights live on the faces as int16
-// in HBM; one launch per colour step updates one of the four face classes
-// (i mod 2, j mod 2).  A thread owns four faces of its class in one row,
+// domino height machinery applied to it.  Heights live on the faces as int16.
+// A colour step updates one of the four face classes (i mod 2, j mod 2); an
+// epoch's steps run in one launch of the band kernel below when the bands
+// fit shared memory, else one launch per step on the heights in HBM.  A thread owns four faces of its class in one row,
 // (i, 8q + p + 2b) for b = 0..3, takes the four output words of one
 // Philox4x32-10 call as their draws, and applies the heat bath: a face whose
 // four edge neighbours share the height m becomes m+1 when its draw is below
@@ -57,6 +58,138 @@ __global__ void __launch_bounds__(256) sixv_step_kernel(const __grid_constant__ 
             *f = (int16_t)(k < a.thr[p] ? m + 1 : m - 1);
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// The heights on chip for a whole epoch: CTA c owns face rows [r0, r1) of
+// every lattice in shared memory (row stride sp = n + 1 rounded up to even,
+// plus the rows r0 - 1 and r1 as halo).  Each colour step updates the band's
+// faces of its class exactly as sixv_step_kernel does (same draws, same
+// rule), then the band's first and last rows go to the neighbours through
+// tagged 64-bit global slots (32 bits of heights and the step + 1), double-
+// buffered by step parity; a CTA reads its halo rows before each step.  A
+// CTA starts step s only after both neighbours finished step s - 1, so a
+// slot is rewritten only after it was read.  Every wait is bounded: past
+// timeout_ns the CTA sets ERR_TIMEOUT in *err and returns, and the others see
+// it.  The launch is cooperative, so every CTA is resident.
+// ---------------------------------------------------------------------------
+struct SixvBandArgs {
+    int16_t* h[2];
+    int nlat, n, Q;
+    uint32_t chain, k0, k1;
+    uint32_t thr[16];
+    int64_t steps;
+    int rows_per_cta, sp, xwords;
+    unsigned long long* xbuf;  // [cta][side][parity][lattice][xwords]
+    int* err;
+    uint64_t timeout_ns;
+};
+
+__device__ __forceinline__ unsigned long long* sixv_slot(const SixvBandArgs& a, int cta, int side, int par, int l) {
+    return a.xbuf + ((((size_t)cta * 2 + side) * 2 + par) * a.nlat + l) * a.xwords;
+}
+
+__device__ __forceinline__ bool sixv_wait(const SixvBandArgs& a, const unsigned long long* p, uint32_t tag,
+                                          uint32_t* out) {
+    unsigned spins = 0;
+    uint64_t t0 = 0;
+    for (;;) {
+        unsigned long long x;
+        asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(x) : "l"(p) : "memory");
+        if ((uint32_t)(x >> 32) == tag) {
+            *out = (uint32_t)x;
+            return true;
+        }
+        if ((++spins & 63u) == 0u) {
+            if (*(volatile int*)a.err) return false;
+            const uint64_t now = global_ns();
+            if (t0 == 0) {
+                t0 = now;
+            } else if (now - t0 > a.timeout_ns) {
+                atomicOr(a.err, ERR_TIMEOUT);
+                return false;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(512, 1) sixv_band_kernel(const __grid_constant__ SixvBandArgs a) {
+    extern __shared__ __align__(16) int16_t sh[];
+    const int S = a.n + 1, sp = a.sp, X = a.xwords;
+    const int cta = blockIdx.x, nct = gridDim.x, tid = threadIdx.x, BLOCK = blockDim.x;
+    const int r0 = min(S, cta * a.rows_per_cta), r1 = min(S, r0 + a.rows_per_cta), nrows = r1 - r0;
+    const int plane = (a.rows_per_cta + 2) * sp;  // per lattice; band row i sits at row i - r0 + 1
+    for (int l = 0; l < a.nlat; ++l)
+        for (int e = tid; e < (nrows + 2) * sp; e += BLOCK) {
+            const int rr = r0 - 1 + e / sp, j = e % sp;
+            sh[l * plane + e] = rr >= 0 && rr < S && j < S ? a.h[l][(size_t)rr * S + j] : (int16_t)0;
+        }
+    __syncthreads();
+    for (int64_t s = 0; s < a.steps; ++s) {
+        if (s > 0) {
+            // halo rows: the neighbours' edge rows after step s - 1
+            bool ok = true;
+            const int par = (int)((s - 1) & 1);
+            const uint32_t tag = (uint32_t)s;
+            for (int e = tid; e < 2 * a.nlat * X && ok; e += BLOCK) {
+                const int side = e >= a.nlat * X, rem = e - side * a.nlat * X, l = rem / X, w = rem - l * X;
+                const int from = side == 0 ? cta - 1 : cta + 1;
+                if (from < 0 || from >= nct || nrows <= 0) continue;
+                uint32_t v;
+                ok = sixv_wait(a, sixv_slot(a, from, 1 - side, par, l) + w, tag, &v);
+                if (ok)
+                    reinterpret_cast<uint32_t*>(sh + l * plane + (side == 0 ? 0 : nrows + 1) * sp)[w] = v;
+            }
+            if (__syncthreads_or(!ok)) return;
+        }
+        // this step's class: row parity (s mod 4) / 2, column parity s mod 2
+        const int pi = (int)((s & 3) >> 1), pj = (int)(s & 1);
+        const int par_row = pi == 0 ? 0 : 1;  // rows 2, 4, .. or 1, 3, .. up to n - 1
+        const int lo = max(r0, 1), hi = min(r1, a.n);
+        const int first = lo + ((lo & 1) != par_row);
+        const int nlive = first < hi ? (hi - first + 1) / 2 : 0;
+        const uint32_t s_lo = (uint32_t)s, s_hi = (uint32_t)((uint64_t)s >> 32);
+        for (int u = tid; u < nlive * a.Q; u += BLOCK) {
+            const int rr = u / a.Q, q = u - rr * a.Q;
+            const int i = first + 2 * rr;
+            const uint4 w4 = philox4((uint32_t)(i * a.Q + q), s_lo, s_hi, a.chain, a.k0, a.k1);
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int j = 8 * q + pj + 2 * b;
+                if (j < 1 || j > a.n - 1) continue;
+                const uint32_t k = quad_word(w4, b) >> 9;
+                for (int l = 0; l < a.nlat; ++l) {
+                    int16_t* f = sh + l * plane + (i - r0 + 1) * sp + j;
+                    const int m = f[-sp];
+                    if (f[sp] != m || f[-1] != m || f[1] != m) continue;
+                    const int p = (f[-sp - 1] > m) | ((f[-sp + 1] > m) << 1) | ((f[sp - 1] > m) << 2) |
+                                  ((f[sp + 1] > m) << 3);
+                    *f = (int16_t)(k < a.thr[p] ? m + 1 : m - 1);
+                }
+            }
+        }
+        __syncthreads();
+        if (s + 1 < a.steps && nrows > 0) {
+            // the band's first and last rows, for the neighbours' next step
+            const int par = (int)(s & 1);
+            const unsigned long long tag = (unsigned long long)(uint32_t)(s + 1) << 32;
+            for (int e = tid; e < 2 * a.nlat * X; e += BLOCK) {
+                const int side = e >= a.nlat * X, rem = e - side * a.nlat * X, l = rem / X, w = rem - l * X;
+                const int to = side == 0 ? cta - 1 : cta + 1;
+                if (to < 0 || to >= nct) continue;
+                const uint32_t v =
+                    reinterpret_cast<const uint32_t*>(sh + l * plane + (side == 0 ? 1 : nrows) * sp)[w];
+                unsigned long long* dst = sixv_slot(a, cta, side, par, l) + w;
+                asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(dst), "l"(tag | v) : "memory");
+            }
+        }
+    }
+    __syncthreads();
+    for (int l = 0; l < a.nlat; ++l)
+        for (int e = tid; e < nrows * S; e += BLOCK) {
+            const int rr = e / S, j = e - rr * S;
+            a.h[l][(size_t)(r0 + rr) * S + j] = sh[l * plane + (rr + 1) * sp + j];
+        }
 }
 
 __global__ void sixv_narrow_kernel(const int32_t* __restrict__ src, int16_t* __restrict__ dst, int64_t count) {
@@ -113,6 +246,9 @@ struct rt_sixv {
     int32_t* d_wide = nullptr;          // int32 staging
     size_t wide_cap = 0;
     unsigned long long* d_count = nullptr;
+    unsigned long long* d_xbuf = nullptr;  // band kernel: halo slots
+    size_t xcap = 0;
+    int* d_err = nullptr;                  // band kernel: error word
 
     rt_status fail(rt_status s, const std::string& m) {
         err = m;
@@ -148,6 +284,8 @@ struct rt_sixv {
             if (p) cudaFree(p);
         if (d_wide) cudaFree(d_wide);
         if (d_count) cudaFree(d_count);
+        if (d_xbuf) cudaFree(d_xbuf);
+        if (d_err) cudaFree(d_err);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -193,6 +331,67 @@ rt_status run_epoch(rt_sixv* h, int n, int nlat, int64_t sweeps, uint64_t key, u
     a.k0 = (uint32_t)key;
     a.k1 = (uint32_t)(key >> 32);
     std::memcpy(a.thr, h->thr, sizeof a.thr);
+    if (sweeps <= 0) return RT_OK;
+    {
+        // The band kernel, when every CTA's rows (and halo) fit shared memory.
+        int dev = 0, sms = 0, optin = 0;
+        const int S = n + 1, sp = (S + 1) & ~1;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && sms > 0) {
+            int ctas = std::min(sms, S);
+            const int rpc = (S + ctas - 1) / ctas;
+            ctas = (S + rpc - 1) / rpc;
+            const size_t smem = (size_t)nlat * (rpc + 2) * sp * sizeof(int16_t);
+            const size_t xbytes = (size_t)ctas * 2 * 2 * nlat * (sp / 2) * sizeof(unsigned long long);
+            bool ready = smem <= (size_t)optin &&
+                         cudaFuncSetAttribute((const void*)sixv_band_kernel,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess;
+            if (ready && xbytes > h->xcap) {
+                if (h->d_xbuf) cudaFree(h->d_xbuf);
+                h->d_xbuf = nullptr;
+                h->xcap = 0;
+                ready = cudaMalloc(&h->d_xbuf, xbytes) == cudaSuccess;
+                if (ready) h->xcap = xbytes;
+            }
+            if (ready && !h->d_err) ready = cudaMalloc(&h->d_err, sizeof(int)) == cudaSuccess;
+            if (ready) {
+                SixvBandArgs b;
+                std::memset(&b, 0, sizeof b);
+                b.h[0] = a.h[0];
+                b.h[1] = a.h[1];
+                b.nlat = nlat;
+                b.n = n;
+                b.Q = a.Q;
+                b.chain = a.chain;
+                b.k0 = a.k0;
+                b.k1 = a.k1;
+                std::memcpy(b.thr, a.thr, sizeof b.thr);
+                b.steps = 4 * sweeps;
+                b.rows_per_cta = rpc;
+                b.sp = sp;
+                b.xwords = sp / 2;
+                b.xbuf = h->d_xbuf;
+                b.err = h->d_err;
+                b.timeout_ns = 5000000000ull;
+                void* args[] = {&b};
+                cudaError_t e = cudaMemsetAsync(h->d_xbuf, 0, xbytes, h->stream);
+                if (e == cudaSuccess) e = cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream);
+                if (e == cudaSuccess)
+                    e = cudaLaunchCooperativeKernel((const void*)sixv_band_kernel, dim3((unsigned)ctas), dim3(512),
+                                                    args, smem, h->stream);
+                if (e == cudaSuccess) {
+                    int flag = 0;
+                    e = cudaMemcpyAsync(&flag, h->d_err, sizeof flag, cudaMemcpyDeviceToHost, h->stream);
+                    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+                    if (e != cudaSuccess) return h->cuda_fail(e, "six-vertex band walk");
+                    if (flag) return h->fail(RT_E_TIMEOUT, "six-vertex band walk: a halo wait timed out");
+                    return RT_OK;
+                }
+                cudaGetLastError();  // not launched: one launch per colour step below
+            }
+        }
+    }
     for (int64_t s = 0; s < 4 * sweeps; ++s) {
         a.pi = (int)((s & 3) >> 1);
         a.pj = (int)(s & 1);

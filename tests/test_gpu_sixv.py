@@ -76,3 +76,15 @@ def test_large_walk_stays_valid(rt):
     a = rt.SixVertexTiler.HeightsToASM(h)
     assert (a.sum(axis=0) == 1).all() and (a.sum(axis=1) == 1).all()
     tl.close()
+
+
+def test_wide_walk_matches_restatement(rt):
+    """n = 6000: the bands do not fit shared memory, so the walk takes one
+    launch per colour step; the result is the restatement's all the same."""
+    n = 6000
+    start = rt.SixVertexTiler.MinHeights(n)
+    h = start.copy()
+    tl = rt.SixVertexTiler()
+    tl.Walk(h, 1, 77, 2)
+    tl.close()
+    assert np.array_equal(h, po.sixv_walk(start, 1, 77, chain=2))
