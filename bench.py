@@ -557,6 +557,15 @@ def run_legs(args) -> None:
         tl.synchronize()
         tl.close()
         print(f"{name}: {args.warmup + args.steps} walks of {args.walk_steps} colour steps", flush=True)
+    if "sixv" in legs:
+        # the six-vertex model at n = 1000, walks of walk_steps / 4 sweeps
+        tl = rt.SixVertexTiler()
+        h = rt.SixVertexTiler.MinHeights(1000)
+        sweeps = max(1, args.walk_steps // 4)
+        for k in range(args.warmup + args.steps):
+            tl.Walk(h, sweeps, k + 1)
+        tl.close()
+        print(f"sixv: {args.warmup + args.steps} walks of {sweeps} sweeps", flush=True)
     if "batch" in legs:
         bt = rt.Batch()
         models = None if args.batch_models == "all" else {int(m) for m in args.batch_models.split(",")}
@@ -890,7 +899,7 @@ def main() -> None:
     ap.add_argument("--warm-train-hexagon", type=int, nargs=2, default=(8, 100))
     ap.add_argument("--warm-train-steps", type=int, default=3000)
     ap.add_argument("--legs", default="all",
-                    help="profiling runs: comma-separated subset of headline,q,fast,planes,batch (no JSON line)")
+                    help="profiling runs: comma-separated subset of headline,q,fast,planes,batch,sixv (no JSON line)")
     ap.add_argument("--batch-models", default="all",
                     help="with --legs batch: comma-separated rt_model values of the mixed workload to keep")
     ap.add_argument("--batch-plan", default="",

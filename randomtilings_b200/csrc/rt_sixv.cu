@@ -113,7 +113,7 @@ __device__ __forceinline__ bool sixv_wait(const SixvBandArgs& a, const unsigned 
     }
 }
 
-__global__ void __launch_bounds__(512, 1) sixv_band_kernel(const __grid_constant__ SixvBandArgs a) {
+__global__ void __launch_bounds__(1024, 1) sixv_band_kernel(const __grid_constant__ SixvBandArgs a) {
     extern __shared__ __align__(16) int16_t sh[];
     const int S = a.n + 1, sp = a.sp, X = a.xwords;
     const int cta = blockIdx.x, nct = gridDim.x, tid = threadIdx.x, BLOCK = blockDim.x;
@@ -378,7 +378,7 @@ rt_status run_epoch(rt_sixv* h, int n, int nlat, int64_t sweeps, uint64_t key, u
                 cudaError_t e = cudaMemsetAsync(h->d_xbuf, 0, xbytes, h->stream);
                 if (e == cudaSuccess) e = cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream);
                 if (e == cudaSuccess)
-                    e = cudaLaunchCooperativeKernel((const void*)sixv_band_kernel, dim3((unsigned)ctas), dim3(512),
+                    e = cudaLaunchCooperativeKernel((const void*)sixv_band_kernel, dim3((unsigned)ctas), dim3(1024),
                                                     args, smem, h->stream);
                 if (e == cudaSuccess) {
                     int flag = 0;
