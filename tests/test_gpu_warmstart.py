@@ -95,3 +95,17 @@ def test_warm_start_reaches_half_percent_five_times_sooner(trained_full, kind, s
     assert s["warm"] is not None, r["curves"]["warm"]
     cold = s["cold"] if s["cold"] is not None else r["sweeps"][-1]  # the cold chain never got there
     assert cold >= TARGET_SPEEDUP * max(1, s["warm"]), s
+
+
+def test_dataset_runs_chains_too_large_for_a_cluster_alone():
+    """Chains beyond the batched kernels' sizes (an Aztec diamond of order 480,
+    a volume-weighted 200-hexagon) run one at a time on a single-lattice walk;
+    their rows are fractions between the extremal height functions."""
+    from randomtilings_b200 import warmstart as ws
+
+    specs = [ws.DomainSpec("aztec", (480,)), ws.DomainSpec("hexagon", (200, 200, 200), 0.99),
+             ws.DomainSpec("aztec", (24,))]
+    x, y, stats = ws.generate_dataset(specs, samples=2, burn_factor=0.002, rows_per_domain=512)
+    assert [s["alone"] for s in stats[:2]] == [True, True] and stats[2]["alone"] is False
+    assert x.shape == (y.size, 8) and y.size == 3 * 512
+    assert np.all((y >= 0) & (y <= 1)) and 0.0 < float(y.mean()) < 1.0
