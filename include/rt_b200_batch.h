@@ -58,7 +58,9 @@ rt_status rt_batch_destroy(rt_batch* b);
 rt_status rt_batch_add(rt_batch* b, const rt_chain* c, const int32_t* tiling, int32_t n, int64_t* index);
 /* autotune = 1 (default): time the candidate plans at the first run;
  * autotune = 0: use `cluster` CTAs per cluster and `block` threads per CTA
- * for every family (0 = the planner's default). */
+ * for every family (0 = the planner's default); a family whose kernel is
+ * built for fewer threads (the triangle dimers': 512) runs with its maximum,
+ * which rt_batch_get_info reports. */
 rt_status rt_batch_set_tuning(rt_batch* b, int32_t autotune, int32_t cluster, int32_t block);
 /* Advances every chain by `sweeps` sweeps: a sweep is every colour (flip
  * class) once -- 2 colour steps for dominoes, 3 for lozenges and
