@@ -9,9 +9,13 @@
 // agree at every site.
 //
 //   tdplane_check ARRAYS_FILE M STEPS
+//   tdplane_check random M ROUNDS   (every phase of the 30 moves on random
+//       states of each array's bit width, ROUNDS times; values compared
+//       modulo 2^bits, the width the planes keep)
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 namespace rtb {
@@ -92,27 +96,35 @@ void plane_op(const tdp::View& v, const Phase& p, int m, uint32_t draw) {
 
 int main(int argc, char** argv) {
     if (argc != 4) {
-        fprintf(stderr, "usage: tdplane_check ARRAYS_FILE M STEPS\n");
+        fprintf(stderr, "usage: tdplane_check ARRAYS_FILE M STEPS | tdplane_check random M ROUNDS\n");
         return 2;
     }
     const int m = atoi(argv[2]), steps = atoi(argv[3]);
     const size_t mm = (size_t)m * m;
     std::vector<int32_t> A(8 * mm), B;
-    FILE* f = fopen(argv[1], "rb");
-    if (!f || fread(A.data(), sizeof(int32_t), A.size(), f) != A.size()) {
-        fprintf(stderr, "cannot read %s\n", argv[1]);
-        return 2;
+    const bool random = std::string(argv[1]) == "random";
+    if (!random) {
+        FILE* f = fopen(argv[1], "rb");
+        if (!f || fread(A.data(), sizeof(int32_t), A.size(), f) != A.size()) {
+            fprintf(stderr, "cannot read %s\n", argv[1]);
+            return 2;
+        }
+        fclose(f);
     }
-    fclose(f);
     // planes: rows -1 .. m (zero halo rows), each row a zero word then wb words then a zero word
     const int wb = (m + 31) / 32, rs = wb + 2, ps = (m + 2) * rs;
     std::vector<uint32_t> P((size_t)tdp::kPlanes * ps);
     auto bit_at = [&](int plane, int i, int j) -> uint32_t& { return P[(size_t)plane * ps + (size_t)(i + 1) * rs + 1 + j / 32]; };
     long checked = 0, changed = 0;
-    for (int s = 0; s < steps; ++s) {
+    const int moves = random ? 30 * steps : steps;
+    for (int s = 0; s < moves; ++s) {
         const std::vector<Phase> ph = phases_of(s % 30);
         for (size_t q = 0; q < ph.size(); ++q) {
             const Phase& p = ph[q];
+            if (random)  // a fresh random state of each array's width before every phase
+                for (int arr = 0; arr < 8; ++arr)
+                    for (size_t e = 0; e < mm; ++e)
+                        A[arr * mm + e] = (int32_t)(mix(0x5eedull + s, q + 97, arr * mm + e) & ((1u << tdp::bits_of(arr)) - 1));
             std::vector<uint32_t> K(mm);
             for (size_t e = 0; e < mm; ++e) K[e] = mix((uint64_t)s, q, e) >> 9;
             // the integer rule, in place (a phase reads no site it writes)
@@ -153,9 +165,10 @@ int main(int argc, char** argv) {
                         for (int k = 0; k < tdp::bits_of(arr); ++k)
                             if ((bit_at(tdp::plane_of(arr) + k, i, j) >> (j % 32)) & 1u) got |= 1 << k;
                         const size_t at = arr * mm + (size_t)i * m + j;
+                        const int32_t want = random ? B[at] & ((1 << tdp::bits_of(arr)) - 1) : B[at];
                         ++checked;
                         changed += B[at] != A[at];
-                        if (got != B[at]) {
+                        if (got != want) {
                             printf("MISMATCH move %d phase %zu (op %u a %u b %u): array %d site (%d, %d): old %d, rule %d, "
                                    "planes %d\n",
                                    s, q, p.op, p.a, p.b, arr, i, j, A[at], B[at], got);
@@ -165,6 +178,6 @@ int main(int argc, char** argv) {
             A.swap(B);
         }
     }
-    printf("ok %d moves, %ld values checked, %ld changed\n", steps, checked, changed);
+    printf("ok %d moves, %ld values checked, %ld changed\n", moves, checked, changed);
     return 0;
 }

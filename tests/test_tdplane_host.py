@@ -44,6 +44,15 @@ def test_bit_plane_ops_equal_the_integer_rule(checker, tmp_path, k):
     assert changed > 1000, (name, out.stdout)  # the chain moved: the comparison covered real flips
 
 
+def test_bit_plane_ops_on_random_states(checker):
+    """Every phase of the 30 moves on random states of each array's bit width:
+    the digit sums' adder paths (conditions that overlap, which chains from
+    valid tilings never produce) agree with the integer rule modulo the width
+    the planes keep."""
+    out = subprocess.run([checker, "random", "40", "3"], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.startswith("ok"), (out.stdout, out.stderr)
+
+
 def test_oracle_split_fits_the_bit_planes():
     import randomtilings_b200 as rt
 
