@@ -9,7 +9,8 @@
 // updates 32 sites of a row at once.  A neighbour at column j +- 1 is a
 // funnel shift of two adjacent words.  Sums of weighted conditions (the
 // digits a + 2 b + 3 c of the reference's rules) use a bit-sliced ripple
-// adder, so every value is the one the integer rule computes.
+// adder, so every value is the one the integer rule computes, modulo the
+// array's width (states reached from a valid tiling never exceed it).
 //
 // Sites outside an op's mask keep their bits; within one phase no op reads a
 // site it writes (the reference's parallel kernels rely on the same), so the
