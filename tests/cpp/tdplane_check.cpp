@@ -12,6 +12,7 @@
 //   tdplane_check random M ROUNDS   (every phase of the 30 moves on random
 //       states of each array's bit width, ROUNDS times; values compared
 //       modulo 2^bits, the width the planes keep)
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
