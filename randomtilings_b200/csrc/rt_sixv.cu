@@ -65,13 +65,16 @@ __global__ void __launch_bounds__(256) sixv_step_kernel(const __grid_constant__ 
 // every lattice in shared memory (row stride sp = n + 1 rounded up to even,
 // plus the rows r0 - 1 and r1 as halo).  Each colour step updates the band's
 // faces of its class exactly as sixv_step_kernel does (same draws, same
-// rule), then the band's first and last rows go to the neighbours through
-// tagged 64-bit global slots (32 bits of heights and the step + 1), double-
-// buffered by step parity; a CTA reads its halo rows before each step.  A
-// CTA starts step s only after both neighbours finished step s - 1, so a
-// slot is rewritten only after it was read.  Every wait is bounded: past
-// timeout_ns the CTA sets ERR_TIMEOUT in *err and returns, and the others see
-// it.  The launch is cooperative, so every CTA is resident.
+// rule).  Steps 2t and 2t + 1 update rows of one parity, so the halo rows
+// (the other parity) cannot change between them: after each odd step the
+// band's first and last rows go to the neighbours through tagged 64-bit
+// global slots (32 bits of heights and the step + 1), double-buffered by
+// the parity of the exchange's number, and a CTA reads its halo rows before
+// each even step.  A CTA publishes exchange t + 1 only after it read
+// exchange t, which each neighbour published after reading exchange t - 1
+// from it, so a slot is rewritten only after it was read.  Every wait is
+// bounded: past timeout_ns the CTA sets ERR_TIMEOUT in *err and returns, and
+// the others see it.  The launch is cooperative, so every CTA is resident.
 // ---------------------------------------------------------------------------
 struct SixvBandArgs {
     int16_t* h[2];
@@ -126,10 +129,10 @@ __global__ void __launch_bounds__(1024, 1) sixv_band_kernel(const __grid_constan
         }
     __syncthreads();
     for (int64_t s = 0; s < a.steps; ++s) {
-        if (s > 0) {
-            // halo rows: the neighbours' edge rows after step s - 1
+        if (s > 0 && (s & 1) == 0) {
+            // halo rows: the neighbours' edge rows after step s - 1 (exchange s / 2)
             bool ok = true;
-            const int par = (int)((s - 1) & 1);
+            const int par = (int)((s >> 1) & 1);
             const uint32_t tag = (uint32_t)s;
             for (int e = tid; e < 2 * a.nlat * X && ok; e += BLOCK) {
                 const int side = e >= a.nlat * X, rem = e - side * a.nlat * X, l = rem / X, w = rem - l * X;
@@ -169,9 +172,9 @@ __global__ void __launch_bounds__(1024, 1) sixv_band_kernel(const __grid_constan
             }
         }
         __syncthreads();
-        if (s + 1 < a.steps && nrows > 0) {
-            // the band's first and last rows, for the neighbours' next step
-            const int par = (int)(s & 1);
+        if ((s & 1) && s + 1 < a.steps && nrows > 0) {
+            // the band's first and last rows, for the neighbours' next two steps
+            const int par = (int)(((s + 1) >> 1) & 1);
             const unsigned long long tag = (unsigned long long)(uint32_t)(s + 1) << 32;
             for (int e = tid; e < 2 * a.nlat * X; e += BLOCK) {
                 const int side = e >= a.nlat * X, rem = e - side * a.nlat * X, l = rem / X, w = rem - l * X;

@@ -88,3 +88,15 @@ def test_wide_walk_matches_restatement(rt):
     tl.Walk(h, 1, 77, 2)
     tl.close()
     assert np.array_equal(h, po.sixv_walk(start, 1, 77, chain=2))
+
+
+def test_bench_walk_matches_restatement(rt):
+    """The walk the benchmark times (n = 1000, 400 sweeps from the minimal
+    heights, key 2): many bands, every halo exchange of a long launch."""
+    n = 1000
+    start = rt.SixVertexTiler.MinHeights(n)
+    h = start.copy()
+    tl = rt.SixVertexTiler()
+    tl.Walk(h, 400, 2)
+    tl.close()
+    assert np.array_equal(h, po.sixv_walk(start, 400, 2))
