@@ -116,13 +116,14 @@ __device__ __forceinline__ bool sixv_wait(const SixvBandArgs& a, const unsigned 
     }
 }
 
+template <int NLAT>
 __global__ void __launch_bounds__(1024, 1) sixv_band_kernel(const __grid_constant__ SixvBandArgs a) {
     extern __shared__ __align__(16) int16_t sh[];
     const int S = a.n + 1, sp = a.sp, X = a.xwords;
     const int cta = blockIdx.x, nct = gridDim.x, tid = threadIdx.x, BLOCK = blockDim.x;
     const int r0 = min(S, cta * a.rows_per_cta), r1 = min(S, r0 + a.rows_per_cta), nrows = r1 - r0;
     const int plane = (a.rows_per_cta + 2) * sp;  // per lattice; band row i sits at row i - r0 + 1
-    for (int l = 0; l < a.nlat; ++l)
+    for (int l = 0; l < NLAT; ++l)
         for (int e = tid; e < (nrows + 2) * sp; e += BLOCK) {
             const int rr = r0 - 1 + e / sp, j = e % sp;
             sh[l * plane + e] = rr >= 0 && rr < S && j < S ? a.h[l][(size_t)rr * S + j] : (int16_t)0;
@@ -134,8 +135,8 @@ __global__ void __launch_bounds__(1024, 1) sixv_band_kernel(const __grid_constan
             bool ok = true;
             const int par = (int)((s >> 1) & 1);
             const uint32_t tag = (uint32_t)s;
-            for (int e = tid; e < 2 * a.nlat * X && ok; e += BLOCK) {
-                const int side = e >= a.nlat * X, rem = e - side * a.nlat * X, l = rem / X, w = rem - l * X;
+            for (int e = tid; e < 2 * NLAT * X && ok; e += BLOCK) {
+                const int side = e >= NLAT * X, rem = e - side * NLAT * X, l = rem / X, w = rem - l * X;
                 const int from = side == 0 ? cta - 1 : cta + 1;
                 if (from < 0 || from >= nct || nrows <= 0) continue;
                 uint32_t v;
@@ -156,18 +157,33 @@ __global__ void __launch_bounds__(1024, 1) sixv_band_kernel(const __grid_constan
             const int rr = u / a.Q, q = u - rr * a.Q;
             const int i = first + 2 * rr;
             const uint4 w4 = philox4((uint32_t)(i * a.Q + q), s_lo, s_hi, a.chain, a.k0, a.k1);
+            const int j0 = 8 * q + pj;  // the faces j0, j0 + 2, j0 + 4, j0 + 6
+            // Columns j0 - 1 .. j0 + 7 clamped to the row: a clamped column
+            // serves only faces outside 1 .. n - 1, which are skipped.  All
+            // reads come before the writes (no face of the class is another's
+            // neighbour), so they need not wait on them.
+            int col[9];
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int j = 8 * q + pj + 2 * b;
-                if (j < 1 || j > a.n - 1) continue;
-                const uint32_t k = quad_word(w4, b) >> 9;
-                for (int l = 0; l < a.nlat; ++l) {
-                    int16_t* f = sh + l * plane + (i - r0 + 1) * sp + j;
-                    const int m = f[-sp];
-                    if (f[sp] != m || f[-1] != m || f[1] != m) continue;
-                    const int p = (f[-sp - 1] > m) | ((f[-sp + 1] > m) << 1) | ((f[sp - 1] > m) << 2) |
-                                  ((f[sp + 1] > m) << 3);
-                    *f = (int16_t)(k < a.thr[p] ? m + 1 : m - 1);
+            for (int t = 0; t < 9; ++t) col[t] = min(max(j0 - 1 + t, 0), sp - 1);
+#pragma unroll
+            for (int l = 0; l < NLAT; ++l) {
+                int16_t* row = sh + l * plane + (i - r0 + 1) * sp;
+                int up[9], dn[9], md[5];
+#pragma unroll
+                for (int t = 0; t < 9; ++t) {
+                    up[t] = row[col[t] - sp];
+                    dn[t] = row[col[t] + sp];
+                }
+#pragma unroll
+                for (int t = 0; t < 5; ++t) md[t] = row[col[2 * t]];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int j = j0 + 2 * b, m = up[2 * b + 1];
+                    if (j < 1 || j > a.n - 1 || dn[2 * b + 1] != m || md[b] != m || md[b + 1] != m) continue;
+                    const int p = (up[2 * b] > m) | ((up[2 * b + 2] > m) << 1) | ((dn[2 * b] > m) << 2) |
+                                  ((dn[2 * b + 2] > m) << 3);
+                    const uint32_t k = quad_word(w4, b) >> 9;
+                    row[j] = (int16_t)(k < a.thr[p] ? m + 1 : m - 1);
                 }
             }
         }
@@ -176,8 +192,8 @@ __global__ void __launch_bounds__(1024, 1) sixv_band_kernel(const __grid_constan
             // the band's first and last rows, for the neighbours' next two steps
             const int par = (int)(((s + 1) >> 1) & 1);
             const unsigned long long tag = (unsigned long long)(uint32_t)(s + 1) << 32;
-            for (int e = tid; e < 2 * a.nlat * X; e += BLOCK) {
-                const int side = e >= a.nlat * X, rem = e - side * a.nlat * X, l = rem / X, w = rem - l * X;
+            for (int e = tid; e < 2 * NLAT * X; e += BLOCK) {
+                const int side = e >= NLAT * X, rem = e - side * NLAT * X, l = rem / X, w = rem - l * X;
                 const int to = side == 0 ? cta - 1 : cta + 1;
                 if (to < 0 || to >= nct) continue;
                 const uint32_t v =
@@ -188,7 +204,7 @@ __global__ void __launch_bounds__(1024, 1) sixv_band_kernel(const __grid_constan
         }
     }
     __syncthreads();
-    for (int l = 0; l < a.nlat; ++l)
+    for (int l = 0; l < NLAT; ++l)
         for (int e = tid; e < nrows * S; e += BLOCK) {
             const int rr = e / S, j = e - rr * S;
             a.h[l][(size_t)(r0 + rr) * S + j] = sh[l * plane + (rr + 1) * sp + j];
@@ -347,8 +363,9 @@ rt_status run_epoch(rt_sixv* h, int n, int nlat, int64_t sweeps, uint64_t key, u
             ctas = (S + rpc - 1) / rpc;
             const size_t smem = (size_t)nlat * (rpc + 2) * sp * sizeof(int16_t);
             const size_t xbytes = (size_t)ctas * 2 * 2 * nlat * (sp / 2) * sizeof(unsigned long long);
+            const void* band_fn = nlat == 2 ? (const void*)sixv_band_kernel<2> : (const void*)sixv_band_kernel<1>;
             bool ready = smem <= (size_t)optin &&
-                         cudaFuncSetAttribute((const void*)sixv_band_kernel,
+                         cudaFuncSetAttribute(band_fn,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess;
             if (ready && xbytes > h->xcap) {
                 if (h->d_xbuf) cudaFree(h->d_xbuf);
@@ -381,7 +398,7 @@ rt_status run_epoch(rt_sixv* h, int n, int nlat, int64_t sweeps, uint64_t key, u
                 cudaError_t e = cudaMemsetAsync(h->d_xbuf, 0, xbytes, h->stream);
                 if (e == cudaSuccess) e = cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream);
                 if (e == cudaSuccess)
-                    e = cudaLaunchCooperativeKernel((const void*)sixv_band_kernel, dim3((unsigned)ctas), dim3(1024),
+                    e = cudaLaunchCooperativeKernel(band_fn, dim3((unsigned)ctas), dim3(1024),
                                                     args, smem, h->stream);
                 if (e == cudaSuccess) {
                     int flag = 0;
