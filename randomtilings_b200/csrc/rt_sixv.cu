@@ -5,8 +5,9 @@
 // domino height machinery applied to it.  Heights live on the faces as int16.
 // A colour step updates one of the four face classes (i mod 2, j mod 2); an
 // epoch's steps run in one launch of the band kernel below when the bands
-// fit shared memory, else one launch per step on the heights in HBM.  A thread owns four faces of its class in one row,
-// (i, 8q + p + 2b) for b = 0..3, takes the four output words of one
+// fit shared memory, else one launch per step on the heights in HBM.  A
+// thread owns four faces of its class in one row, (i, 8q + p + 2b) for
+// b = 0..3, takes the four output words of one
 // Philox4x32-10 call as their draws, and applies the heat bath: a face whose
 // four edge neighbours share the height m becomes m+1 when its draw is below
 // the threshold of its diagonal pattern, else m-1.  Faces of one class share
