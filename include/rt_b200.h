@@ -128,7 +128,9 @@ rt_status rt_set_lozenge_weights(rt_tiler* h, int32_t period, const double* w0, 
  * Walk(tiling&, int, long) src/Lozenge/LozengeTiler.cpp:18-88,
  * src/RectTriangle/RectTriangleTiler.cpp:17-92,
  * src/TriangleDimer/TriangleDimerTiler.cpp:86-483.  `tiling` (N*N int32,
- * host) is updated in place; synchronous, like the reference. */
+ * host) is updated in place; synchronous, like the reference.  A call (and
+ * each rt_walk_epochs / rt_run / CFTP trial, all epochs together) takes at
+ * most 2^40 steps; more is RT_E_INVAL, with the tiling left as it was. */
 rt_status rt_walk(rt_tiler* h, int32_t* tiling, int32_t n, int64_t steps, int64_t seed);
 
 /* Replaces DominoTiler::Walk(tiling&, vector<long> steps, vector<long> seeds)

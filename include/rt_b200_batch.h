@@ -66,7 +66,8 @@ rt_status rt_batch_set_tuning(rt_batch* b, int32_t autotune, int32_t cluster, in
  * class) once -- 2 colour steps for dominoes, 3 for lozenges and
  * rectangle-triangles, 30 for triangle dimers.  Synchronous.  The Philox step
  * counter continues across runs (a run of s1 sweeps then one of s2 equals a
- * run of s1 + s2). */
+ * run of s1 + s2).  At most 2^35 sweeps per run (and per launch); more is
+ * RT_E_INVAL. */
 /* Sweeps one launch of a family runs (a run of S sweeps becomes S / sweeps
  * launches plus one for the rest, each continuing the chains' draws), for
  * every family: > 0 fixes it, 0 asks for one launch per run, -1 (the

@@ -67,7 +67,7 @@ rt_status rt_sixv_vertex_types(const int32_t* heights, int32_t n, int32_t* types
 
 /* `sweeps` sweeps of the heat bath on the host heights ((n+1)^2, updated in
  * place; n <= 32000), epoch key `key`, Philox counter word 3 `chain`.
- * Synchronous. */
+ * Synchronous.  At most 2^38 sweeps; more is RT_E_INVAL. */
 rt_status rt_sixv_walk(rt_sixv* h, int32_t* heights, int32_t n, int64_t sweeps, uint64_t key, uint32_t chain);
 
 /* Coupling from the past (no reference counterpart beyond the domino driver
@@ -77,7 +77,8 @@ rt_status rt_sixv_walk(rt_sixv* h, int32_t* heights, int32_t n, int64_t sweeps, 
  * std::mt19937(master_seed) outputs; the schedule doubles from first_sweeps
  * until they agree.  Exact when the weights are monotone (see
  * rt_sixv_thresholds), else RT_E_INVAL.  out_heights (optional) receives the
- * sample; stats counts colour steps (four per sweep). */
+ * sample; stats counts colour steps (four per sweep).  A schedule that
+ * would pass 2^38 sweeps in one trial ends with RT_E_INVAL. */
 rt_status rt_sixv_cftp(rt_sixv* h, int32_t n, int64_t first_sweeps, int64_t master_seed, int32_t max_trials,
                        int32_t* out_heights, rt_cftp_stats* stats);
 

@@ -1031,6 +1031,7 @@ rt_status rt_batch_set_tuning(rt_batch* b, int32_t autotune, int32_t cluster, in
 rt_status rt_batch_set_sweeps_per_launch(rt_batch* b, int64_t sweeps) {
     if (!b) return RT_E_INVAL;
     if (sweeps < -1) return b->fail(RT_E_INVAL, "sweeps per launch must be >= -1");
+    if (sweeps > kMaxColourSteps / 32) return b->fail(RT_E_INVAL, "more than 2^35 sweeps per launch");
     b->force_spl = sweeps;
     for (int f = 0; f < kFamilies; ++f) b->fam[f].planned = false;
     b->drop_graph();
@@ -1040,6 +1041,7 @@ rt_status rt_batch_set_sweeps_per_launch(rt_batch* b, int64_t sweeps) {
 rt_status rt_batch_run(rt_batch* b, int64_t sweeps) {
     if (!b) return RT_E_INVAL;
     if (sweeps < 0) return b->fail(RT_E_INVAL, "negative sweep count");
+    if (sweeps > kMaxColourSteps / 32) return b->fail(RT_E_INVAL, "more than 2^35 sweeps in one call");
     if (b->chains.empty() || sweeps == 0) return RT_OK;
     cudaSetDevice(b->device);
     rt_status s = upload(b);

@@ -600,6 +600,7 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
     int64_t total = 0;
     for (int e = 0; e < k; ++e) {
         if (steps[e] < 0) return h->fail(RT_E_INVAL, "negative step count");
+        if (steps[e] > kMaxColourSteps - total) return h->fail(RT_E_INVAL, "more than 2^40 steps in one call");
         total += steps[e];
     }
     h->last_phases = 0;

@@ -21,6 +21,12 @@ enum Family : int {
     FAM_TRIDIMER = 5     // triangledimerkernel.cl, 8 int32 arrays
 };
 
+// The most colour steps one call may ask for, about 1.1e12: weeks of device
+// time even on small lattices.  Every entry point that sizes a schedule or a
+// phase list from a step or sweep count refuses larger counts first, so no
+// size computed from a count can wrap.
+constexpr int64_t kMaxColourSteps = int64_t(1) << 40;
+
 struct WalkPlan {
     int items = 0;
     int block = 0;

@@ -7,10 +7,10 @@
 // epoch's steps run in one launch of the band kernel below when the bands
 // fit shared memory, else one launch per step on the heights in HBM.  A
 // thread owns four faces of its class in one row, (i, 8q + p + 2b) for
-// b = 0..3, takes the four output words of one
-// Philox4x32-10 call as their draws, and applies the heat bath: a face whose
-// four edge neighbours share the height m becomes m+1 when its draw is below
-// the threshold of its diagonal pattern, else m-1.  Faces of one class share
+// b = 0..3, takes the four output words of one Philox4x32-10 call as their
+// draws, and applies the heat bath: a face whose four edge neighbours share
+// the height m becomes m+1 when its draw is below the threshold of its
+// diagonal pattern, else m-1.  Faces of one class share
 // no neighbour (edge or diagonal), so a launch is race-free and the result is
 // independent of the order of the threads.  Coupled CFTP chains are two
 // lattices of the same launch fed the same draws.
@@ -531,6 +531,7 @@ rt_status rt_sixv_vertex_types(const int32_t* heights, int32_t n, int32_t* types
 rt_status rt_sixv_walk(rt_sixv* h, int32_t* heights, int32_t n, int64_t sweeps, uint64_t key, uint32_t chain) {
     if (!h) return RT_E_INVAL;
     if (!heights || !valid_n(n) || sweeps < 0) return h->fail(RT_E_INVAL, "bad arguments");
+    if (sweeps > kMaxColourSteps / 4) return h->fail(RT_E_INVAL, "more than 2^38 sweeps in one call");
     if (rt_sixv_check(heights, n) != RT_OK)
         return h->fail(RT_E_INVAL, "not a domain-wall height function of this size");
     cudaSetDevice(h->device);
@@ -545,6 +546,7 @@ rt_status rt_sixv_cftp(rt_sixv* h, int32_t n, int64_t first_sweeps, int64_t mast
                        int32_t* out_heights, rt_cftp_stats* stats) {
     if (!h) return RT_E_INVAL;
     if (!valid_n(n) || first_sweeps <= 0 || max_trials <= 0) return h->fail(RT_E_INVAL, "bad CFTP arguments");
+    if (first_sweeps > kMaxColourSteps / 4) return h->fail(RT_E_INVAL, "more than 2^38 sweeps in one call");
     if (!h->monotone) return h->fail(RT_E_INVAL, "these weights give a heat bath that is not monotone: no CFTP");
     cudaSetDevice(h->device);
     if (!h->reserve(n)) return h->fail(RT_E_NOMEM, "cudaMalloc six-vertex lattices");
@@ -585,6 +587,11 @@ rt_status rt_sixv_cftp(rt_sixv* h, int32_t n, int64_t first_sweeps, int64_t mast
         st.total_steps = 4 * total;
         if (diff == 0) {
             st.coalesced = 1;
+            break;
+        }
+        if (trial + 1 < max_trials && total > kMaxColourSteps / 8) {
+            // the next trial would run 2 total sweeps
+            s = h->fail(RT_E_INVAL, "CFTP schedule beyond 2^38 sweeps without coalescence");
             break;
         }
         sweeps.insert(sweeps.begin(), total);
