@@ -23,18 +23,27 @@
 
 #include "../../include/rt_b200.h"
 #include "../../include/rt_b200_host.h"
+#include "rt_guard.h"
+
+using rtb::guarded;
 
 namespace {
 
 constexpr int32_t INF = INT_MAX;
 using Vec = std::vector<int32_t>;
 
+// The largest side of a square array any function here takes or builds:
+// 2 kMaxSide^2 (a lozenge domain's entries) still fits an int32 index.
+constexpr int64_t kMaxSide = 32767;
+
+// The side of a square array of n entries; -1 if n is not a square or the
+// side exceeds kMaxSide.
 int isqrt_exact(int64_t n) {
-    if (n < 0) return -1;
+    if (n < 0 || n > (int64_t)1 << 40) return -1;
     int64_t r = (int64_t)std::llround(std::sqrt((double)n));
     while (r * r > n) --r;
     while ((r + 1) * (r + 1) <= n) ++r;
-    return r * r == n ? (int)r : -1;
+    return r * r == n && r <= kMaxSide ? (int)r : -1;
 }
 
 rt_status emit(const Vec& v, int32_t* out, int64_t cap, int64_t* len) {
@@ -342,146 +351,166 @@ extern "C" {
 
 // ---- dominoes ----------------------------------------------------------------
 rt_status rt_domino_rectangle(int32_t rows, int32_t cols, int32_t* out, int64_t cap, int64_t* len) {
-    if (rows < 0 || cols < 0) return RT_E_INVAL;
-    int dim = std::max(rows, cols) + 4;
-    if (dim % 2 == 0) ++dim;
-    Vec d((size_t)dim * dim, 0);
-    for (int i = 0; i < rows; ++i)
-        for (int j = 0; j < cols; ++j) d[(size_t)(i + 2) * dim + j + 2] = 1;
-    return emit(d, out, cap, len);
+    return guarded([&]() -> rt_status {
+        if (rows < 0 || cols < 0 || std::max<int64_t>(rows, cols) + 5 > kMaxSide) return RT_E_INVAL;
+        int dim = std::max(rows, cols) + 4;
+        if (dim % 2 == 0) ++dim;
+        Vec d((size_t)dim * dim, 0);
+        for (int i = 0; i < rows; ++i)
+            for (int j = 0; j < cols; ++j) d[(size_t)(i + 2) * dim + j + 2] = 1;
+        return emit(d, out, cap, len);
+    });
 }
 
 rt_status rt_domino_aztec_rectangle(int32_t order, const int32_t* remove, int32_t k, int32_t* out, int64_t cap,
                                     int64_t* len) {
-    if (order < 1 || k < 0 || k >= 2 * order) return RT_E_INVAL;
-    const int n = order, m = 2 * n - k;
-    Vec d((size_t)m * m, 0);
-    for (int i = 0; i < m; ++i) {
-        int lo, hi;
-        if (i == 0 || i == m - 1) {
-            lo = (n - k) + (i == m - 1) * k - 1;
-            hi = lo + 1;
-        } else if (i < n - k) {
-            lo = n - k - i - 1, hi = n - k + i;
-        } else if (i > n - 1) {
-            lo = i - n + k, hi = 3 * n - k - i - 1;
-        } else {
-            lo = i - (n - k), hi = i + (n - k);
+    return guarded([&]() -> rt_status {
+        if (order < 1 || order > (kMaxSide - 5) / 2 || k < 0 || k >= 2 * order) return RT_E_INVAL;
+        const int n = order, m = 2 * n - k;
+        Vec d((size_t)m * m, 0);
+        for (int i = 0; i < m; ++i) {
+            int lo, hi;
+            if (i == 0 || i == m - 1) {
+                lo = (n - k) + (i == m - 1) * k - 1;
+                hi = lo + 1;
+            } else if (i < n - k) {
+                lo = n - k - i - 1, hi = n - k + i;
+            } else if (i > n - 1) {
+                lo = i - n + k, hi = 3 * n - k - i - 1;
+            } else {
+                lo = i - (n - k), hi = i + (n - k);
+            }
+            for (int j = std::max(lo, 0); j <= std::min(hi, m - 1); ++j) d[(size_t)i * m + j] = 1;
         }
-        for (int j = std::max(lo, 0); j <= std::min(hi, m - 1); ++j) d[(size_t)i * m + j] = 1;
-    }
-    for (int r = 0; r < k; ++r) {
-        const int i0 = n - k + remove[r], j0 = remove[r];
-        if (i0 < 0 || j0 < 0 || i0 >= m || j0 >= m) return RT_E_INVAL;
-        d[(size_t)i0 * m + j0] = 0;
-    }
-    const int m2 = m + 4 + (1 - m % 2);  // odd side -> even tiling side (DominoTiler.cpp:183-184)
-    Vec d2((size_t)m2 * m2, 0);
-    for (int i = 0; i < m; ++i)
-        for (int j = 0; j < m; ++j) d2[(size_t)(i + 2) * m2 + j + 2] = d[(size_t)i * m + j];
-    return emit(d2, out, cap, len);
+        for (int r = 0; r < k; ++r) {
+            const int i0 = n - k + remove[r], j0 = remove[r];
+            if (i0 < 0 || j0 < 0 || i0 >= m || j0 >= m) return RT_E_INVAL;
+            d[(size_t)i0 * m + j0] = 0;
+        }
+        const int m2 = m + 4 + (1 - m % 2);  // odd side -> even tiling side (DominoTiler.cpp:183-184)
+        Vec d2((size_t)m2 * m2, 0);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) d2[(size_t)(i + 2) * m2 + j + 2] = d[(size_t)i * m + j];
+        return emit(d2, out, cap, len);
+    });
 }
 
 rt_status rt_domino_aztec(int32_t order, int32_t* out, int64_t cap, int64_t* len) {
-    return rt_domino_aztec_rectangle(order, nullptr, 0, out, cap, len);
+    return guarded([&]() -> rt_status {
+        return rt_domino_aztec_rectangle(order, nullptr, 0, out, cap, len);
+    });
 }
 
 rt_status rt_domino_domain_to_vertices(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
-    const int m = isqrt_exact(dlen);
-    if (!d || m < 1) return RT_E_INVAL;
-    if (!out) return size_only((int64_t)(m + 1) * (m + 1), len);
-    return emit(dom_vertices(Vec(d, d + dlen), m), out, cap, len);
+    return guarded([&]() -> rt_status {
+        const int m = isqrt_exact(dlen);
+        if (!d || m < 1) return RT_E_INVAL;
+        if (!out) return size_only((int64_t)(m + 1) * (m + 1), len);
+        return emit(dom_vertices(Vec(d, d + dlen), m), out, cap, len);
+    });
 }
 
 rt_status rt_domino_max_tiling(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
-    if (!d) return RT_E_INVAL;
-    if (!out) return dom_side_query(dlen, len);
-    Vec t;
-    rt_status s = dom_extremal(Vec(d, d + dlen), +1, &t);
-    return s != RT_OK ? s : emit(t, out, cap, len);
+    return guarded([&]() -> rt_status {
+        if (!d) return RT_E_INVAL;
+        if (!out) return dom_side_query(dlen, len);
+        Vec t;
+        rt_status s = dom_extremal(Vec(d, d + dlen), +1, &t);
+        return s != RT_OK ? s : emit(t, out, cap, len);
+    });
 }
 
 rt_status rt_domino_min_tiling(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
-    if (!d) return RT_E_INVAL;
-    if (!out) return dom_side_query(dlen, len);
-    Vec t;
-    rt_status s = dom_extremal(Vec(d, d + dlen), -1, &t);
-    return s != RT_OK ? s : emit(t, out, cap, len);
+    return guarded([&]() -> rt_status {
+        if (!d) return RT_E_INVAL;
+        if (!out) return dom_side_query(dlen, len);
+        Vec t;
+        rt_status s = dom_extremal(Vec(d, d + dlen), -1, &t);
+        return s != RT_OK ? s : emit(t, out, cap, len);
+    });
 }
 
 rt_status rt_domino_height_to_tiling(const int32_t* h, int64_t hlen, const int32_t* d, int64_t dlen, int32_t* out,
                                      int64_t cap, int64_t* len) {
-    const int n = isqrt_exact(hlen);
-    if (!h || !d || n < 2 || (int64_t)(n - 1) * (n - 1) != dlen) return RT_E_INVAL;
-    if (!out) return size_only(hlen, len);
-    return emit(dom_height_to_tiling(Vec(h, h + hlen), Vec(d, d + dlen), n), out, cap, len);
+    return guarded([&]() -> rt_status {
+        const int n = isqrt_exact(hlen);
+        if (!h || !d || n < 2 || (int64_t)(n - 1) * (n - 1) != dlen) return RT_E_INVAL;
+        if (!out) return size_only(hlen, len);
+        return emit(dom_height_to_tiling(Vec(h, h + hlen), Vec(d, d + dlen), n), out, cap, len);
+    });
 }
 
 rt_status rt_domino_tiling_to_height(const int32_t* t, int64_t tlen, const int32_t* d, int64_t dlen, int32_t* out,
                                      int64_t cap, int64_t* len) {
-    const int n = isqrt_exact(tlen);
-    if (!t || !d || n < 2 || (int64_t)(n - 1) * (n - 1) != dlen) return RT_E_INVAL;
-    if (!out) return size_only(tlen, len);
-    const int m = n - 1;
-    const Vec D(d, d + dlen);
-    const Vec verts = dom_vertices(D, m);
-    Vec hf((size_t)n * n, INF);
-    const int start = first_boundary(verts);
-    if (start >= 0) {
-        hf[start] = 0;
-        std::deque<int> q{start};
-        while (!q.empty()) {
-            const int v = q.front();
-            q.pop_front();
-            const int i = v / n, j = v % n;
-            for (int nb = 0; nb < 4; ++nb) {
-                if (t[v] & kDomBit[nb]) continue;  // a domino crosses this edge
-                const int i2 = i + kDomDi[nb], j2 = j + kDomDj[nb];
-                if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n) continue;
-                const int w = i2 * n + j2;
-                if (verts[w] == 0 || hf[w] != INF) continue;
-                int f[4];
-                dom_edge_faces(i, j, nb, f);
-                if (!dom_face(D, m, f[0], f[1]) && !dom_face(D, m, f[2], f[3])) continue;
-                hf[w] = hf[v] + dom_dh(i, j, nb);
-                q.push_back(w);
+    return guarded([&]() -> rt_status {
+        const int n = isqrt_exact(tlen);
+        if (!t || !d || n < 2 || (int64_t)(n - 1) * (n - 1) != dlen) return RT_E_INVAL;
+        if (!out) return size_only(tlen, len);
+        const int m = n - 1;
+        const Vec D(d, d + dlen);
+        const Vec verts = dom_vertices(D, m);
+        Vec hf((size_t)n * n, INF);
+        const int start = first_boundary(verts);
+        if (start >= 0) {
+            hf[start] = 0;
+            std::deque<int> q{start};
+            while (!q.empty()) {
+                const int v = q.front();
+                q.pop_front();
+                const int i = v / n, j = v % n;
+                for (int nb = 0; nb < 4; ++nb) {
+                    if (t[v] & kDomBit[nb]) continue;  // a domino crosses this edge
+                    const int i2 = i + kDomDi[nb], j2 = j + kDomDj[nb];
+                    if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n) continue;
+                    const int w = i2 * n + j2;
+                    if (verts[w] == 0 || hf[w] != INF) continue;
+                    int f[4];
+                    dom_edge_faces(i, j, nb, f);
+                    if (!dom_face(D, m, f[0], f[1]) && !dom_face(D, m, f[2], f[3])) continue;
+                    hf[w] = hf[v] + dom_dh(i, j, nb);
+                    q.push_back(w);
+                }
             }
         }
-    }
-    return emit(hf, out, cap, len);
+        return emit(hf, out, cap, len);
+    });
 }
 
 rt_status rt_domino_tiling_to_domain(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len) {
-    const int n = isqrt_exact(tlen);
-    if (!t || n < 2) return RT_E_INVAL;
-    const int m = n - 1;
-    Vec d((size_t)m * m, 0);
-    for (int i = 0; i < m; ++i)
-        for (int j = 0; j < m; ++j)
-            if ((t[i * n + j] & (2 + 8)) || (t[(i + 1) * n + j + 1] & (1 + 4))) d[(size_t)i * m + j] = 1;
-    return emit(d, out, cap, len);
+    return guarded([&]() -> rt_status {
+        const int n = isqrt_exact(tlen);
+        if (!t || n < 2) return RT_E_INVAL;
+        const int m = n - 1;
+        Vec d((size_t)m * m, 0);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j)
+                if ((t[i * n + j] & (2 + 8)) || (t[(i + 1) * n + j + 1] & (1 + 4))) d[(size_t)i * m + j] = 1;
+        return emit(d, out, cap, len);
+    });
 }
 
 // ---- lozenges ------------------------------------------------------------------
 rt_status rt_lozenge_almost_hex(int32_t side, int32_t cut, int32_t* out, int64_t cap, int64_t* len) {
-    if (side < 1 || cut < 0 || cut > side) return RT_E_INVAL;
-    const int n = side;
-    const int rows = 2 * n, cols = 4 * n;
-    Vec d((size_t)rows * cols, 0);
-    for (int i = 0; i < rows; ++i)
-        for (int j = 0; j < cols; ++j)
-            d[(size_t)i * cols + j] = i < n ? (2 * i + j - 1 >= 2 * n - 2) : (2 * i + j <= 6 * n - 2);
-    for (int i = 0; i < cut; ++i)
-        for (int j = cols - 2 * cut; j < cols; ++j) d[(size_t)i * cols + j] = 0;
-    // 3 rows / 6 triangles of padding, then grow to a vertex side divisible by 3
-    // (LozengeTiler.cpp:370-388).
-    const int m2 = rows + 6;
-    const int k = (3 - (m2 + 1) % 3) % 3;
-    const int m3 = m2 + k;
-    Vec d3((size_t)m3 * 2 * m3, 0);
-    for (int i = 0; i < rows; ++i)
-        for (int j = 0; j < cols; ++j) d3[(size_t)(i + 3) * 2 * m3 + j + 6] = d[(size_t)i * cols + j];
-    return emit(d3, out, cap, len);
+    return guarded([&]() -> rt_status {
+        if (side < 1 || side > (kMaxSide - 9) / 2 || cut < 0 || cut > side) return RT_E_INVAL;
+        const int n = side;
+        const int rows = 2 * n, cols = 4 * n;
+        Vec d((size_t)rows * cols, 0);
+        for (int i = 0; i < rows; ++i)
+            for (int j = 0; j < cols; ++j)
+                d[(size_t)i * cols + j] = i < n ? (2 * i + j - 1 >= 2 * n - 2) : (2 * i + j <= 6 * n - 2);
+        for (int i = 0; i < cut; ++i)
+            for (int j = cols - 2 * cut; j < cols; ++j) d[(size_t)i * cols + j] = 0;
+        // 3 rows / 6 triangles of padding, then grow to a vertex side divisible by 3
+        // (LozengeTiler.cpp:370-388).
+        const int m2 = rows + 6;
+        const int k = (3 - (m2 + 1) % 3) % 3;
+        const int m3 = m2 + k;
+        Vec d3((size_t)m3 * 2 * m3, 0);
+        for (int i = 0; i < rows; ++i)
+            for (int j = 0; j < cols; ++j) d3[(size_t)(i + 3) * 2 * m3 + j + 6] = d[(size_t)i * cols + j];
+        return emit(d3, out, cap, len);
+    });
 }
 
 // Hexagon with sides a (top), b, c, a, b, c in the triangle-row encoding of
@@ -493,164 +522,183 @@ rt_status rt_lozenge_almost_hex(int32_t side, int32_t cut, int32_t* out, int64_t
 // is vertical for c rows, the lower-right one slants for b rows).  The same
 // padding as AlmostHexDomain follows.  No reference counterpart.
 rt_status rt_lozenge_hexagon(int32_t a, int32_t b, int32_t c, int32_t* out, int64_t cap, int64_t* len) {
-    if (a < 1 || b < 1 || c < 1) return RT_E_INVAL;
-    const int rows = b + c, cols = 2 * a + 2 * b;
-    Vec d((size_t)rows * cols, 0);
-    for (int i = 0; i < rows; ++i) {
-        const int lo = std::max(0, 2 * b - 1 - 2 * i);
-        const int hi = i < c ? 2 * a + 2 * b - 1 : 2 * a + 2 * b - 2 - 2 * (i - c);
-        for (int j = lo; j <= hi && j < cols; ++j) d[(size_t)i * cols + j] = 1;
-    }
-    // 3 rows / 6 triangles of padding, then a square array of side m3
-    // (vertex side divisible by 3) as LozengeTiler.cpp:370-388 builds it.
-    const int m2 = std::max(rows + 6, (cols + 12 + 1) / 2);
-    const int k = (3 - (m2 + 1) % 3) % 3;
-    const int m3 = m2 + k;
-    Vec d3((size_t)m3 * 2 * m3, 0);
-    for (int i = 0; i < rows; ++i)
-        for (int j = 0; j < cols; ++j) d3[(size_t)(i + 3) * 2 * m3 + j + 6] = d[(size_t)i * cols + j];
-    return emit(d3, out, cap, len);
+    return guarded([&]() -> rt_status {
+        if (a < 1 || b < 1 || c < 1 || (int64_t)b + c + 8 > kMaxSide || (int64_t)a + b + 9 > kMaxSide)
+            return RT_E_INVAL;
+        const int rows = b + c, cols = 2 * a + 2 * b;
+        Vec d((size_t)rows * cols, 0);
+        for (int i = 0; i < rows; ++i) {
+            const int lo = std::max(0, 2 * b - 1 - 2 * i);
+            const int hi = i < c ? 2 * a + 2 * b - 1 : 2 * a + 2 * b - 2 - 2 * (i - c);
+            for (int j = lo; j <= hi && j < cols; ++j) d[(size_t)i * cols + j] = 1;
+        }
+        // 3 rows / 6 triangles of padding, then a square array of side m3
+        // (vertex side divisible by 3) as LozengeTiler.cpp:370-388 builds it.
+        const int m2 = std::max(rows + 6, (cols + 12 + 1) / 2);
+        const int k = (3 - (m2 + 1) % 3) % 3;
+        const int m3 = m2 + k;
+        Vec d3((size_t)m3 * 2 * m3, 0);
+        for (int i = 0; i < rows; ++i)
+            for (int j = 0; j < cols; ++j) d3[(size_t)(i + 3) * 2 * m3 + j + 6] = d[(size_t)i * cols + j];
+        return emit(d3, out, cap, len);
+    });
 }
 
 rt_status rt_lozenge_domain_to_vertices(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
-    const int m = isqrt_exact(dlen / 2);
-    if (!d || m < 2 || (int64_t)2 * m * m != dlen) return RT_E_INVAL;
-    if (!out) return size_only((int64_t)(m + 1) * (m + 1), len);
-    return emit(loz_vertices(Vec(d, d + dlen), m), out, cap, len);
+    return guarded([&]() -> rt_status {
+        const int m = isqrt_exact(dlen / 2);
+        if (!d || m < 2 || (int64_t)2 * m * m != dlen) return RT_E_INVAL;
+        if (!out) return size_only((int64_t)(m + 1) * (m + 1), len);
+        return emit(loz_vertices(Vec(d, d + dlen), m), out, cap, len);
+    });
 }
 
 rt_status rt_lozenge_max_tiling(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
-    if (!d) return RT_E_INVAL;
-    if (!out) return loz_side_query(dlen, len);
-    Vec t;
-    rt_status s = loz_extremal(Vec(d, d + dlen), +1, &t);
-    return s != RT_OK ? s : emit(t, out, cap, len);
+    return guarded([&]() -> rt_status {
+        if (!d) return RT_E_INVAL;
+        if (!out) return loz_side_query(dlen, len);
+        Vec t;
+        rt_status s = loz_extremal(Vec(d, d + dlen), +1, &t);
+        return s != RT_OK ? s : emit(t, out, cap, len);
+    });
 }
 
 rt_status rt_lozenge_min_tiling(const int32_t* d, int64_t dlen, int32_t* out, int64_t cap, int64_t* len) {
-    if (!d) return RT_E_INVAL;
-    if (!out) return loz_side_query(dlen, len);
-    Vec t;
-    rt_status s = loz_extremal(Vec(d, d + dlen), -1, &t);
-    return s != RT_OK ? s : emit(t, out, cap, len);
+    return guarded([&]() -> rt_status {
+        if (!d) return RT_E_INVAL;
+        if (!out) return loz_side_query(dlen, len);
+        Vec t;
+        rt_status s = loz_extremal(Vec(d, d + dlen), -1, &t);
+        return s != RT_OK ? s : emit(t, out, cap, len);
+    });
 }
 
 rt_status rt_lozenge_height_to_tiling(const int32_t* h, int64_t hlen, const int32_t* d, int64_t dlen, int32_t* out,
                                       int64_t cap, int64_t* len) {
-    const int n = isqrt_exact(hlen);
-    if (!h || !d || n < 3 || (int64_t)2 * (n - 1) * (n - 1) != dlen) return RT_E_INVAL;
-    if (!out) return size_only(hlen, len);
-    return emit(loz_height_to_tiling(Vec(h, h + hlen), Vec(d, d + dlen), n), out, cap, len);
+    return guarded([&]() -> rt_status {
+        const int n = isqrt_exact(hlen);
+        if (!h || !d || n < 3 || (int64_t)2 * (n - 1) * (n - 1) != dlen) return RT_E_INVAL;
+        if (!out) return size_only(hlen, len);
+        return emit(loz_height_to_tiling(Vec(h, h + hlen), Vec(d, d + dlen), n), out, cap, len);
+    });
 }
 
 rt_status rt_lozenge_tiling_to_height(const int32_t* t, int64_t tlen, const int32_t* d, int64_t dlen, int32_t* out,
                                       int64_t cap, int64_t* len) {
-    const int n = isqrt_exact(tlen);
-    if (!t || !d || n < 3 || (int64_t)2 * (n - 1) * (n - 1) != dlen) return RT_E_INVAL;
-    if (!out) return size_only(tlen, len);
-    const int m = n - 1;
-    const Vec D(d, d + dlen);
-    const Vec verts = loz_vertices(D, m);
-    Vec hf((size_t)n * n, INF);
-    const int start = first_boundary(verts);
-    if (start >= 0) {
-        hf[start] = 0;
-        std::deque<int> q{start};
-        while (!q.empty()) {
-            const int v = q.front();
-            q.pop_front();
-            const int i = v / n, j = v % n;
-            for (int nb = 0; nb < 6; ++nb) {
-                if (t[v] & kLozBit[nb]) continue;  // a lozenge covers this edge
-                const int i2 = i + kLozDi[nb], j2 = j + kLozDj[nb];
-                if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n) continue;
-                const int w = i2 * n + j2;
-                if (verts[w] == 0 || hf[w] != INF || !loz_edge_in(D, m, i, j, nb, false)) continue;
-                hf[w] = hf[v] + kLozDh[nb];
-                q.push_back(w);
+    return guarded([&]() -> rt_status {
+        const int n = isqrt_exact(tlen);
+        if (!t || !d || n < 3 || (int64_t)2 * (n - 1) * (n - 1) != dlen) return RT_E_INVAL;
+        if (!out) return size_only(tlen, len);
+        const int m = n - 1;
+        const Vec D(d, d + dlen);
+        const Vec verts = loz_vertices(D, m);
+        Vec hf((size_t)n * n, INF);
+        const int start = first_boundary(verts);
+        if (start >= 0) {
+            hf[start] = 0;
+            std::deque<int> q{start};
+            while (!q.empty()) {
+                const int v = q.front();
+                q.pop_front();
+                const int i = v / n, j = v % n;
+                for (int nb = 0; nb < 6; ++nb) {
+                    if (t[v] & kLozBit[nb]) continue;  // a lozenge covers this edge
+                    const int i2 = i + kLozDi[nb], j2 = j + kLozDj[nb];
+                    if (i2 < 0 || j2 < 0 || i2 >= n || j2 >= n) continue;
+                    const int w = i2 * n + j2;
+                    if (verts[w] == 0 || hf[w] != INF || !loz_edge_in(D, m, i, j, nb, false)) continue;
+                    hf[w] = hf[v] + kLozDh[nb];
+                    q.push_back(w);
+                }
             }
         }
-    }
-    return emit(hf, out, cap, len);
+        return emit(hf, out, cap, len);
+    });
 }
 
 rt_status rt_lozenge_tiling_to_domain(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len) {
-    const int n = isqrt_exact(tlen);
-    if (!t || n < 3) return RT_E_INVAL;
-    const int m = n - 1;
-    Vec d((size_t)2 * m * m, 0);
-    auto set = [&](int r, int c) {
-        if (r >= 0 && r < m && c >= 0 && c < 2 * m) d[(size_t)r * 2 * m + c] = 1;
-    };
-    for (int i = 0; i < n - 1; ++i)
-        for (int j = 0; j < n - 1; ++j) {
-            const int v = t[i * n + j];
-            if (v & 1) set(i - 1, 2 * j), set(i - 1, 2 * j - 1);
-            if (v & 2) set(i - 1, 2 * j), set(i - 1, 2 * j + 1);
-            if (v & 8) set(i - 1, 2 * j + 1), set(i, 2 * j);
-        }
-    return emit(d, out, cap, len);
+    return guarded([&]() -> rt_status {
+        const int n = isqrt_exact(tlen);
+        if (!t || n < 3) return RT_E_INVAL;
+        const int m = n - 1;
+        Vec d((size_t)2 * m * m, 0);
+        auto set = [&](int r, int c) {
+            if (r >= 0 && r < m && c >= 0 && c < 2 * m) d[(size_t)r * 2 * m + c] = 1;
+        };
+        for (int i = 0; i < n - 1; ++i)
+            for (int j = 0; j < n - 1; ++j) {
+                const int v = t[i * n + j];
+                if (v & 1) set(i - 1, 2 * j), set(i - 1, 2 * j - 1);
+                if (v & 2) set(i - 1, 2 * j), set(i - 1, 2 * j + 1);
+                if (v & 8) set(i - 1, 2 * j + 1), set(i, 2 * j);
+            }
+        return emit(d, out, cap, len);
+    });
 }
 
 // ---- rectangle-triangle hexagons -------------------------------------------------
 rt_status rt_recttri_max_hex(int32_t side, int32_t* out, int64_t cap, int64_t* len) {
-    if (side < 1) return RT_E_INVAL;
-    const int n = side, m = 2 * n + 1;
-    Vec g((size_t)m * m, 0);
-    auto at = [&](int i, int j) -> int32_t& { return g[(size_t)i * m + j]; };
-    for (int i = 1; i < m - 1; ++i)
-        for (int j = 0; j < m; ++j) {
-            int32_t v;
-            if (j - i > n || i - j > n) v = 0;
-            else if (i < n && j < n) v = 0x333333;
-            else if (i < j && j > n) v = 0x111111;
-            else if (i > n && i > j) v = 0x222222;
-            else if (i == n && j < n) v = 0x333222;
-            else if (i < n && j == n) v = 0x331311;
-            else if (i == j && i > n) v = 0x211221;
-            else v = 0x331221;  // the centre, i == j == n
-            at(i, j) = v;
-        }
-    for (int i = 1; i < n; ++i) at(i, 0) = 0x003033, at(0, i) = 0x000333;
-    for (int i = n + 1; i < m - 1; ++i) at(i, m - 1) = 0x110100, at(m - 1, i) = 0x222000;
-    for (int i = 1; i < n; ++i) at(i, i + n) = 0x100110, at(i + n, i) = 0x022002;
-    at(0, 0) = 0x000033;
-    at(n, 0) = 0x003002;
-    at(0, n) = 0x000310;
-    at(m - 1, m - 1) = 0x210000;
-    at(n, m - 1) = 0x100100;
-    at(m - 1, n) = 0x022000;
-    return emit(rt_shear(g, n, m), out, cap, len);
+    return guarded([&]() -> rt_status {
+        if (side < 1 || side > (kMaxSide - 9) / 2) return RT_E_INVAL;
+        const int n = side, m = 2 * n + 1;
+        Vec g((size_t)m * m, 0);
+        auto at = [&](int i, int j) -> int32_t& { return g[(size_t)i * m + j]; };
+        for (int i = 1; i < m - 1; ++i)
+            for (int j = 0; j < m; ++j) {
+                int32_t v;
+                if (j - i > n || i - j > n) v = 0;
+                else if (i < n && j < n) v = 0x333333;
+                else if (i < j && j > n) v = 0x111111;
+                else if (i > n && i > j) v = 0x222222;
+                else if (i == n && j < n) v = 0x333222;
+                else if (i < n && j == n) v = 0x331311;
+                else if (i == j && i > n) v = 0x211221;
+                else v = 0x331221;  // the centre, i == j == n
+                at(i, j) = v;
+            }
+        for (int i = 1; i < n; ++i) at(i, 0) = 0x003033, at(0, i) = 0x000333;
+        for (int i = n + 1; i < m - 1; ++i) at(i, m - 1) = 0x110100, at(m - 1, i) = 0x222000;
+        for (int i = 1; i < n; ++i) at(i, i + n) = 0x100110, at(i + n, i) = 0x022002;
+        at(0, 0) = 0x000033;
+        at(n, 0) = 0x003002;
+        at(0, n) = 0x000310;
+        at(m - 1, m - 1) = 0x210000;
+        at(n, m - 1) = 0x100100;
+        at(m - 1, n) = 0x022000;
+        return emit(rt_shear(g, n, m), out, cap, len);
+    });
 }
 
 rt_status rt_recttri_min_hex(int32_t side, int32_t* out, int64_t cap, int64_t* len) {
-    if (side < 1) return RT_E_INVAL;
-    const int n = side, m = 2 * n + 1;
-    Vec g((size_t)m * m, 0);
-    auto at = [&](int i, int j) -> int32_t& { return g[(size_t)i * m + j]; };
-    for (int i = 1; i < m - 1; ++i)
-        for (int j = 1; j < m - 1; ++j) {
-            int32_t v;
-            if (j - i > n || i - j > n) v = 0;
-            else if (i > n && j > n) v = 0x333333;
-            else if (i > j && j < n) v = 0x111111;
-            else if (i < n && i < j) v = 0x222222;
-            else if (i == n && j > n) v = 0x222333;
-            else if (i > n && j == n) v = 0x113133;
-            else if (i == j && i < n) v = 0x122112;
-            else v = 0x122133;  // the centre
-            at(i, j) = v;
-        }
-    for (int i = 1; i < n; ++i) at(i, 0) = 0x001011, at(0, i) = 0x000222;
-    for (int i = n + 1; i < m - 1; ++i) at(i, m - 1) = 0x330300, at(m - 1, i) = 0x333000;
-    for (int i = 1; i < n; ++i) at(i, i + n) = 0x200220, at(i + n, i) = 0x011001;
-    at(0, 0) = 0x000012;
-    at(m - 1, n) = 0x013000;
-    at(n, m - 1) = 0x200300;
-    at(0, n) = 0x000220;
-    at(n, 0) = 0x001001;
-    at(m - 1, m - 1) = 0x330000;
-    return emit(rt_shear(g, n, m), out, cap, len);
+    return guarded([&]() -> rt_status {
+        if (side < 1 || side > (kMaxSide - 9) / 2) return RT_E_INVAL;
+        const int n = side, m = 2 * n + 1;
+        Vec g((size_t)m * m, 0);
+        auto at = [&](int i, int j) -> int32_t& { return g[(size_t)i * m + j]; };
+        for (int i = 1; i < m - 1; ++i)
+            for (int j = 1; j < m - 1; ++j) {
+                int32_t v;
+                if (j - i > n || i - j > n) v = 0;
+                else if (i > n && j > n) v = 0x333333;
+                else if (i > j && j < n) v = 0x111111;
+                else if (i < n && i < j) v = 0x222222;
+                else if (i == n && j > n) v = 0x222333;
+                else if (i > n && j == n) v = 0x113133;
+                else if (i == j && i < n) v = 0x122112;
+                else v = 0x122133;  // the centre
+                at(i, j) = v;
+            }
+        for (int i = 1; i < n; ++i) at(i, 0) = 0x001011, at(0, i) = 0x000222;
+        for (int i = n + 1; i < m - 1; ++i) at(i, m - 1) = 0x330300, at(m - 1, i) = 0x333000;
+        for (int i = 1; i < n; ++i) at(i, i + n) = 0x200220, at(i + n, i) = 0x011001;
+        at(0, 0) = 0x000012;
+        at(m - 1, n) = 0x013000;
+        at(n, m - 1) = 0x200300;
+        at(0, n) = 0x000220;
+        at(n, 0) = 0x001001;
+        at(m - 1, m - 1) = 0x330000;
+        return emit(rt_shear(g, n, m), out, cap, len);
+    });
 }
 
 // LozengeToRectTriangle (RectTriangleTiler.cpp:523-565): each triangle of the
@@ -658,28 +706,30 @@ rt_status rt_recttri_min_hex(int32_t side, int32_t* out, int64_t cap, int64_t* l
 // covering it) on its three corner vertices.
 rt_status rt_recttri_from_lozenge(const int32_t* tl, int64_t tlen, const int32_t* dl, int64_t dlen, int32_t* out,
                                   int64_t cap, int64_t* len) {
-    const int n = isqrt_exact(tlen), m = isqrt_exact(dlen / 2);
-    if (!tl || !dl || n < 2 || m < 1 || (int64_t)2 * m * m != dlen || m + 1 > n) return RT_E_INVAL;
-    Vec t((size_t)n * n, 0);
-    for (int i = 0; i < m; ++i)
-        for (int j = 0; j < 2 * m; ++j) {
-            if (dl[(size_t)i * 2 * m + j] != 1) continue;
-            const int c = j / 2;
-            if (j % 2 == 0) {  // downward-pointing face: corners (i, c), (i, c+1), (i+1, c)
-                const int v = tl[(size_t)i * n + c];
-                const int dgt = (v & 8) ? 1 : (v & 32) ? 3 : 2;
-                t[(size_t)i * n + c] += dgt;
-                t[(size_t)i * n + c + 1] += dgt << 8;
-                t[(size_t)(i + 1) * n + c] += dgt << 16;
-            } else {  // upward face: corners (i, c+1), (i+1, c), (i+1, c+1)
-                const int v = tl[(size_t)i * n + c + 1];
-                const int dgt = (v & 16) ? 2 : (v & 32) ? 3 : 1;
-                t[(size_t)i * n + c + 1] += dgt << 4;
-                t[(size_t)(i + 1) * n + c] += dgt << 12;
-                t[(size_t)(i + 1) * n + c + 1] += dgt << 20;
+    return guarded([&]() -> rt_status {
+        const int n = isqrt_exact(tlen), m = isqrt_exact(dlen / 2);
+        if (!tl || !dl || n < 2 || m < 1 || (int64_t)2 * m * m != dlen || m + 1 > n) return RT_E_INVAL;
+        Vec t((size_t)n * n, 0);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < 2 * m; ++j) {
+                if (dl[(size_t)i * 2 * m + j] != 1) continue;
+                const int c = j / 2;
+                if (j % 2 == 0) {  // downward-pointing face: corners (i, c), (i, c+1), (i+1, c)
+                    const int v = tl[(size_t)i * n + c];
+                    const int dgt = (v & 8) ? 1 : (v & 32) ? 3 : 2;
+                    t[(size_t)i * n + c] += dgt;
+                    t[(size_t)i * n + c + 1] += dgt << 8;
+                    t[(size_t)(i + 1) * n + c] += dgt << 16;
+                } else {  // upward face: corners (i, c+1), (i+1, c), (i+1, c+1)
+                    const int v = tl[(size_t)i * n + c + 1];
+                    const int dgt = (v & 16) ? 2 : (v & 32) ? 3 : 1;
+                    t[(size_t)i * n + c + 1] += dgt << 4;
+                    t[(size_t)(i + 1) * n + c] += dgt << 12;
+                    t[(size_t)(i + 1) * n + c + 1] += dgt << 20;
+                }
             }
-        }
-    return emit(t, out, cap, len);
+        return emit(t, out, cap, len);
+    });
 }
 
 // ---- dimers on the triangular lattice -------------------------------------------
@@ -712,82 +762,88 @@ static Vec td_tiles_from_edges(const Vec& h, const Vec& l, const Vec& r, int e) 
 }
 
 rt_status rt_tridimer_ice_cream_cone(int32_t side, int32_t cut, int32_t* out, int64_t cap, int64_t* len) {
-    // A downward equilateral triangle of side N with a triangle of side M cut
-    // from its top-left corner, as a dimer cover built row by row
-    // (TriangleDimerTiler.cpp:236-332).  Parities the reference only warns
-    // about are accepted (its construction then covers a slightly different
-    // domain); cut > side - 1 is rejected.
-    if (side < 1 || cut < 0 || cut > side - 1) return RT_E_INVAL;
-    const int n = side, m = cut, e = n + 4;
-    const int k = ((n + 1) * (n + 2) / 2) % 2;
-    Vec h((size_t)e * e, 0), l((size_t)e * e, 0), r((size_t)e * e, 0);
-    for (int i = 2; i < e - 2; ++i)
-        for (int j = 2; j < e - i; ++j) {
-            const size_t at = (size_t)i * e + j;
-            if (i < m + 2) {
-                if ((i + j) % 2 == m % 2 && m != 0 && j > m + 3 - i) h[at] = 1;
-                if ((n - m) % 2 == 0 && i % 2 == 0 && j == e - i - 1) r[at] = 1;
-            } else {
-                if (j % 2 == 0) h[at] = 1;
-                if (i % 4 == (3 + n % 2 + 2 * k) % 4 && j == e - i - 1) h[at] = 0, l[at] = 1;
-                if (i % 4 == (2 + n % 2 + 2 * k) % 4 && j == e - i - 1) r[at] = 1;
+    return guarded([&]() -> rt_status {
+        // A downward equilateral triangle of side N with a triangle of side M cut
+        // from its top-left corner, as a dimer cover built row by row
+        // (TriangleDimerTiler.cpp:236-332).  Parities the reference only warns
+        // about are accepted (its construction then covers a slightly different
+        // domain); cut > side - 1 is rejected.
+        if (side < 1 || side > (kMaxSide - 8) / 2 || cut < 0 || cut > side - 1) return RT_E_INVAL;
+        const int n = side, m = cut, e = n + 4;
+        const int k = ((n + 1) * (n + 2) / 2) % 2;
+        Vec h((size_t)e * e, 0), l((size_t)e * e, 0), r((size_t)e * e, 0);
+        for (int i = 2; i < e - 2; ++i)
+            for (int j = 2; j < e - i; ++j) {
+                const size_t at = (size_t)i * e + j;
+                if (i < m + 2) {
+                    if ((i + j) % 2 == m % 2 && m != 0 && j > m + 3 - i) h[at] = 1;
+                    if ((n - m) % 2 == 0 && i % 2 == 0 && j == e - i - 1) r[at] = 1;
+                } else {
+                    if (j % 2 == 0) h[at] = 1;
+                    if (i % 4 == (3 + n % 2 + 2 * k) % 4 && j == e - i - 1) h[at] = 0, l[at] = 1;
+                    if (i % 4 == (2 + n % 2 + 2 * k) % 4 && j == e - i - 1) r[at] = 1;
+                }
             }
-        }
-    return emit(td_tiles_from_edges(h, l, r, e), out, cap, len);
+        return emit(td_tiles_from_edges(h, l, r, e), out, cap, len);
+    });
 }
 
 rt_status rt_tridimer_hexagon(int32_t side, int32_t* out, int64_t cap, int64_t* len) {
-    // Edges in the encoding of the IceCreamCone builder: h(i, j) joins (i, j)
-    // and (i, j+1), l(i, j) joins (i, j) and (i+1, j), r(i, j) joins (i, j+1)
-    // and (i+1, j) (the neighbours TilingToVertices reads, :711-737).
-    if (side < 1 || side > 4096) return RT_E_INVAL;
-    const int s = side, e = 2 * s + 8, off = 3;
-    Vec h((size_t)e * e, 0), l((size_t)e * e, 0), r((size_t)e * e, 0);
-    auto lo_y = [&](int x) { return std::max(0, s - x) + (x == 0 ? 1 : 0); };  // corner (0, s) removed
-    auto hi_y = [&](int x) { return std::min(2 * s, 3 * s - x); };
-    auto at = [&](int x, int y) { return (size_t)(x + off) * e + (y + off); };
-    // A row whose count of free vertices is odd pairs one end vertex with the
-    // matching end of the next row: the right end unless the row above took
-    // that one, then the left end -- so every row's free vertices stay one
-    // run, paired horizontally from the left.
-    int taken = 0;  // end of this row already paired with the row above: 0 none, 1 left, 2 right
-    for (int x = 0; x <= 2 * s; ++x) {
-        const int above = taken;
-        int a = lo_y(x) + (above == 1), b = hi_y(x) - (above == 2);
-        taken = 0;
-        if ((b - a + 1) % 2 != 0) {
-            if (x == 2 * s) return RT_E_STATE;  // unreachable: the vertex count is even
-            if (above == 2) {
-                // left end (x, a) with the first vertex of the next row
-                const int t = lo_y(x + 1);
-                if (t == a) l[at(x, a)] = 1;
-                else if (t == a - 1) r[at(x, a - 1)] = 1;
-                else return RT_E_STATE;
-                taken = 1;
-                ++a;
-            } else {
-                const int t = hi_y(x + 1);
-                if (t == b) l[at(x, b)] = 1;
-                else if (t == b - 1) r[at(x, b - 1)] = 1;
-                else return RT_E_STATE;
-                taken = 2;
-                --b;
+    return guarded([&]() -> rt_status {
+        // Edges in the encoding of the IceCreamCone builder: h(i, j) joins (i, j)
+        // and (i, j+1), l(i, j) joins (i, j) and (i+1, j), r(i, j) joins (i, j+1)
+        // and (i+1, j) (the neighbours TilingToVertices reads, :711-737).
+        if (side < 1 || side > 4096) return RT_E_INVAL;
+        const int s = side, e = 2 * s + 8, off = 3;
+        Vec h((size_t)e * e, 0), l((size_t)e * e, 0), r((size_t)e * e, 0);
+        auto lo_y = [&](int x) { return std::max(0, s - x) + (x == 0 ? 1 : 0); };  // corner (0, s) removed
+        auto hi_y = [&](int x) { return std::min(2 * s, 3 * s - x); };
+        auto at = [&](int x, int y) { return (size_t)(x + off) * e + (y + off); };
+        // A row whose count of free vertices is odd pairs one end vertex with the
+        // matching end of the next row: the right end unless the row above took
+        // that one, then the left end -- so every row's free vertices stay one
+        // run, paired horizontally from the left.
+        int taken = 0;  // end of this row already paired with the row above: 0 none, 1 left, 2 right
+        for (int x = 0; x <= 2 * s; ++x) {
+            const int above = taken;
+            int a = lo_y(x) + (above == 1), b = hi_y(x) - (above == 2);
+            taken = 0;
+            if ((b - a + 1) % 2 != 0) {
+                if (x == 2 * s) return RT_E_STATE;  // unreachable: the vertex count is even
+                if (above == 2) {
+                    // left end (x, a) with the first vertex of the next row
+                    const int t = lo_y(x + 1);
+                    if (t == a) l[at(x, a)] = 1;
+                    else if (t == a - 1) r[at(x, a - 1)] = 1;
+                    else return RT_E_STATE;
+                    taken = 1;
+                    ++a;
+                } else {
+                    const int t = hi_y(x + 1);
+                    if (t == b) l[at(x, b)] = 1;
+                    else if (t == b - 1) r[at(x, b - 1)] = 1;
+                    else return RT_E_STATE;
+                    taken = 2;
+                    --b;
+                }
             }
+            for (int y = a; y < b; y += 2) h[at(x, y)] = 1;
         }
-        for (int y = a; y < b; y += 2) h[at(x, y)] = 1;
-    }
-    return emit(td_tiles_from_edges(h, l, r, e), out, cap, len);
+        return emit(td_tiles_from_edges(h, l, r, e), out, cap, len);
+    });
 }
 
 rt_status rt_tridimer_test_butterfly(int32_t kind, int32_t* out, int64_t cap, int64_t* len) {
-    // One butterfly of orientation H (0), L (1) or R (2) (TriangleDimerTiler.cpp:334-383).
-    if (kind < 0 || kind > 2) return RT_E_INVAL;
-    const int e = 8;
-    Vec h((size_t)e * e, 0), l((size_t)e * e, 0), r((size_t)e * e, 0);
-    if (kind == 0) h[2 * e + 3] = h[4 * e + 3] = r[2 * e + 4] = r[3 * e + 2] = 1;
-    if (kind == 1) r[2 * e + 3] = r[4 * e + 2] = l[3 * e + 2] = l[3 * e + 4] = 1;
-    if (kind == 2) l[2 * e + 4] = l[4 * e + 3] = r[3 * e + 2] = r[3 * e + 4] = 1;
-    return emit(td_tiles_from_edges(h, l, r, e), out, cap, len);
+    return guarded([&]() -> rt_status {
+        // One butterfly of orientation H (0), L (1) or R (2) (TriangleDimerTiler.cpp:334-383).
+        if (kind < 0 || kind > 2) return RT_E_INVAL;
+        const int e = 8;
+        Vec h((size_t)e * e, 0), l((size_t)e * e, 0), r((size_t)e * e, 0);
+        if (kind == 0) h[2 * e + 3] = h[4 * e + 3] = r[2 * e + 4] = r[3 * e + 2] = 1;
+        if (kind == 1) r[2 * e + 3] = r[4 * e + 2] = l[3 * e + 2] = l[3 * e + 4] = 1;
+        if (kind == 2) l[2 * e + 4] = l[4 * e + 3] = r[3 * e + 2] = r[3 * e + 4] = 1;
+        return emit(td_tiles_from_edges(h, l, r, e), out, cap, len);
+    });
 }
 
 }  // extern "C"
@@ -877,19 +933,23 @@ void td_split_host(const int32_t* t, int n, int32_t* arrays) {
 extern "C" {
 
 rt_status rt_tridimer_triangle_flips(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len) {
-    const int n = isqrt_exact(tlen);
-    if (!t || n < 2 || n % 2) return RT_E_INVAL;
-    Vec tri((size_t)(n / 2) * n), bfl((size_t)n * n);
-    rtb::td_derived_states(t, n, tri.data(), bfl.data());
-    return emit(tri, out, cap, len);
+    return guarded([&]() -> rt_status {
+        const int n = isqrt_exact(tlen);
+        if (!t || n < 2 || n % 2) return RT_E_INVAL;
+        Vec tri((size_t)(n / 2) * n), bfl((size_t)n * n);
+        rtb::td_derived_states(t, n, tri.data(), bfl.data());
+        return emit(tri, out, cap, len);
+    });
 }
 
 rt_status rt_tridimer_butterfly_flips(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len) {
-    const int n = isqrt_exact(tlen);
-    if (!t || n < 2 || n % 2) return RT_E_INVAL;
-    Vec tri((size_t)(n / 2) * n), bfl((size_t)n * n);
-    rtb::td_derived_states(t, n, tri.data(), bfl.data());
-    return emit(bfl, out, cap, len);
+    return guarded([&]() -> rt_status {
+        const int n = isqrt_exact(tlen);
+        if (!t || n < 2 || n % 2) return RT_E_INVAL;
+        Vec tri((size_t)(n / 2) * n), bfl((size_t)n * n);
+        rtb::td_derived_states(t, n, tri.data(), bfl.data());
+        return emit(bfl, out, cap, len);
+    });
 }
 
 // Vertices covered by a dimer ((N/2+1)^2, TilingToVertices :711-737).
@@ -906,26 +966,30 @@ static Vec td_vertices(const int32_t* t, int n) {
 }
 
 rt_status rt_tridimer_vertices(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len) {
-    const int n = isqrt_exact(tlen);
-    if (!t || n < 8 || n % 2) return RT_E_INVAL;
-    return emit(td_vertices(t, n), out, cap, len);
+    return guarded([&]() -> rt_status {
+        const int n = isqrt_exact(tlen);
+        if (!t || n < 8 || n % 2) return RT_E_INVAL;
+        return emit(td_vertices(t, n), out, cap, len);
+    });
 }
 
 // Triangles whose three corners are covered (TilingToDomain :739-770).
 rt_status rt_tridimer_tiling_to_domain(const int32_t* t, int64_t tlen, int32_t* out, int64_t cap, int64_t* len) {
-    const int n = isqrt_exact(tlen);
-    if (!t || n < 8 || n % 2) return RT_E_INVAL;
-    const int m = n / 2 + 1;
-    const Vec v = td_vertices(t, n);
-    Vec d((size_t)(m - 1) * 2 * (m - 1), 0);
-    auto V = [&](int i, int j) { return v[(size_t)i * m + j] == 1; };
-    for (int i = 0; i < m - 1; ++i)
-        for (int j = 0; j < 2 * (m - 1); ++j) {
-            const bool in = j % 2 == 0 ? (V(i, j / 2) && V(i, j / 2 + 1) && V(i + 1, j / 2))
-                                       : (V(i, j / 2 + 1) && V(i + 1, j / 2) && V(i + 1, j / 2 + 1));
-            d[(size_t)i * 2 * (m - 1) + j] = in;
-        }
-    return emit(d, out, cap, len);
+    return guarded([&]() -> rt_status {
+        const int n = isqrt_exact(tlen);
+        if (!t || n < 8 || n % 2) return RT_E_INVAL;
+        const int m = n / 2 + 1;
+        const Vec v = td_vertices(t, n);
+        Vec d((size_t)(m - 1) * 2 * (m - 1), 0);
+        auto V = [&](int i, int j) { return v[(size_t)i * m + j] == 1; };
+        for (int i = 0; i < m - 1; ++i)
+            for (int j = 0; j < 2 * (m - 1); ++j) {
+                const bool in = j % 2 == 0 ? (V(i, j / 2) && V(i, j / 2 + 1) && V(i + 1, j / 2))
+                                           : (V(i, j / 2 + 1) && V(i + 1, j / 2) && V(i + 1, j / 2 + 1));
+                d[(size_t)i * 2 * (m - 1) + j] = in;
+            }
+        return emit(d, out, cap, len);
+    });
 }
 
 // 0/1 indicator of dimers of one orientation (DimerIndicator :20-84; the
@@ -933,16 +997,18 @@ rt_status rt_tridimer_tiling_to_domain(const int32_t* t, int64_t tlen, int32_t* 
 // the (odd, odd) cells, bits 8, 4 and 1 respectively).
 rt_status rt_tridimer_dimer_indicator(const int32_t* t, int64_t tlen, int32_t orient, int32_t* out, int64_t cap,
                                       int64_t* len) {
-    const int n = isqrt_exact(tlen);
-    if (!t || n < 2 || n % 2 || orient < 0 || orient > 2) return RT_E_INVAL;
-    const int m = n / 2;
-    Vec dd((size_t)m * m, 0);
-    const int bit = orient == 1 ? 8 : orient == 2 ? 4 : 1;
-    const int ri = orient == 0 ? 1 : 0;
-    for (int i = 0; i < m; ++i)
-        for (int j = 0; j < m; ++j)
-            dd[(size_t)i * m + j] = (t[(size_t)(2 * i + ri) * n + 2 * j + 1] & bit) == bit;
-    return emit(dd, out, cap, len);
+    return guarded([&]() -> rt_status {
+        const int n = isqrt_exact(tlen);
+        if (!t || n < 2 || n % 2 || orient < 0 || orient > 2) return RT_E_INVAL;
+        const int m = n / 2;
+        Vec dd((size_t)m * m, 0);
+        const int bit = orient == 1 ? 8 : orient == 2 ? 4 : 1;
+        const int ri = orient == 0 ? 1 : 0;
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j)
+                dd[(size_t)i * m + j] = (t[(size_t)(2 * i + ri) * n + 2 * j + 1] & bit) == bit;
+        return emit(dd, out, cap, len);
+    });
 }
 
 }  // extern "C"

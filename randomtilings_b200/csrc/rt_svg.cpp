@@ -23,13 +23,18 @@
 #include "../../include/rt_b200.h"
 #include "../../include/rt_b200_host.h"
 #include "../../include/rt_b200_svg.h"
+#include "rt_guard.h"
+
+using rtb::guarded;
 
 namespace {
 
 using Vec = std::vector<int32_t>;
 const double kSqrt3 = 1.7320508075688772935274;  // common.h:41
 
+// floor(sqrt(len)), 0 for lengths outside [0, 2^40].
 int side_of(int64_t len) {
+    if (len < 0 || len > (int64_t)1 << 40) return 0;
     int64_t r = (int64_t)std::llround(std::sqrt((double)len));
     while (r * r > len) --r;
     while ((r + 1) * (r + 1) <= len) ++r;
@@ -249,20 +254,22 @@ extern "C" {
 
 // ---- dominoes ------------------------------------------------------------------
 rt_status rt_domino_domain_svg(const int32_t* d, int64_t dlen, const char* filename) {
-    if (!d || !filename) return RT_E_INVAL;
-    const int m = side_of(dlen);
-    Sink o(filename);
-    o << kSvgOpen << "height=\"500\" width=\"500\" viewBox=\"0 0 " << m << " " << m << "\">\n";
-    o << "<defs>\n";
-    o << "<g id=\"b\">  <polygon points = \"-.5,-.5 .5,-.5 .5,.5 -.5,.5\" fill=\"blue\"/> </g>\n";
-    o << "<g id=\"w\">  <polygon points = \"-.5,-.5 .5,-.5 .5,.5 -.5,.5\" fill=\"grey\"/> </g>\n";
-    o << "</defs>\n";
-    for_rows(o, 0, m, m, [&](Sink& row_out, int i) {
-        for (int j = 0; j < m; ++j)
-            if (d[(size_t)i * m + j] == 1) use(row_out, (i + j) % 2 == 0 ? "b" : "w", j + .5, i + .5, true);
+    return guarded([&]() -> rt_status {
+        if (!d || !filename) return RT_E_INVAL;
+        const int m = side_of(dlen);
+        Sink o(filename);
+        o << kSvgOpen << "height=\"500\" width=\"500\" viewBox=\"0 0 " << m << " " << m << "\">\n";
+        o << "<defs>\n";
+        o << "<g id=\"b\">  <polygon points = \"-.5,-.5 .5,-.5 .5,.5 -.5,.5\" fill=\"blue\"/> </g>\n";
+        o << "<g id=\"w\">  <polygon points = \"-.5,-.5 .5,-.5 .5,.5 -.5,.5\" fill=\"grey\"/> </g>\n";
+        o << "</defs>\n";
+        for_rows(o, 0, m, m, [&](Sink& row_out, int i) {
+            for (int j = 0; j < m; ++j)
+                if (d[(size_t)i * m + j] == 1) use(row_out, (i + j) % 2 == 0 ? "b" : "w", j + .5, i + .5, true);
+        });
+        o << "</svg>";
+        return finish(o);
     });
-    o << "</svg>";
-    return finish(o);
 }
 
 // Dominoes as rectangles anchored at the vertex whose up (1) / left-edge (4)
@@ -316,338 +323,364 @@ static rt_status domino_pairs_svg(const int32_t* t, int64_t tlen, const char* fi
 }
 
 rt_status rt_domino_tiling_svg(const int32_t* t, int64_t tlen, const char* filename) {
-    return domino_pairs_svg(t, tlen, filename, false);
+    return guarded([&]() -> rt_status {
+        return domino_pairs_svg(t, tlen, filename, false);
+    });
 }
 
 rt_status rt_domino_maya_svg(const int32_t* t, int64_t tlen, const char* filename) {
-    return domino_pairs_svg(t, tlen, filename, true);
+    return guarded([&]() -> rt_status {
+        return domino_pairs_svg(t, tlen, filename, true);
+    });
 }
 
 // DominoTiler::DimerToSVG(t, d) (DominoTiler.cpp:538-611); d = NULL takes the
 // domain from the tiling (DimerToSVG(t), :533-536).
 rt_status rt_domino_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d, int64_t dlen, const char* filename) {
-    if (!t || !filename) return RT_E_INVAL;
-    const int n = side_of(tlen), m = n - 1;
-    Vec dom;
-    if (!d) {
-        dom.assign((size_t)m * m, 0);
-        for (int i = 0; i < m; ++i)
-            for (int j = 0; j < m; ++j)
-                if ((t[(size_t)i * n + j] & (2 + 8)) || (t[(size_t)(i + 1) * n + j + 1] & (1 + 4))) dom[(size_t)i * m + j] = 1;
-        d = dom.data();
-        dlen = (int64_t)dom.size();
-    }
-    if (dlen < (int64_t)m * m) return RT_E_INVAL;
-    auto D = [&](int i, int j) { return d[(size_t)i * m + j]; };
-    Sink o(filename);
-    o << kSvgOpen << "height=\"500\" width=\"500\" viewBox=\"0 0 " << m << " " << m << "\">\n";
-    o << "<defs>\n";
-    o << "<g id=\"hd\">  <polyline points= \"-.5,0 .5,0\" stroke=\"red\" stroke-width=\".05\"/> </g>\n";
-    o << "<g id=\"he\">  <polyline points= \"-.5,0 .5,0\" stroke=\"black\" stroke-width=\".01\"/> </g>\n";
-    o << "<g id=\"vd\">  <polyline points= \"0,-.5 0,.5\" stroke=\"red\" stroke-width=\".05\"/> </g>\n";
-    o << "<g id=\"ve\">  <polyline points= \"0,-.5 0,.5\" stroke=\"black\" stroke-width=\".01\"/> </g>\n";
-    o << "<g id=\"b\">  <circle cx=\"0\" cy=\"0\" r=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
-    o << "<g id=\"w\">  <circle cx=\"0\" cy=\"0\" r=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"white\" /> </g>\n";
-    o << "</defs>\n";
-    for_rows(o, 0, n, n, [&](Sink& row_out, int i) {
-        for (int j = 0; j < n; ++j) {
-            const double x = j, y = i;
-            const int32_t v = t[(size_t)i * n + j];
-            if ((v & 1) == 1) use(row_out, "hd", x, y - .5, false);
-            if ((v & 4) == 4) use(row_out, "vd", x - .5, y, false);
+    return guarded([&]() -> rt_status {
+        if (!t || !filename) return RT_E_INVAL;
+        const int n = side_of(tlen), m = n - 1;
+        Vec dom;
+        if (!d) {
+            dom.assign((size_t)m * m, 0);
+            for (int i = 0; i < m; ++i)
+                for (int j = 0; j < m; ++j)
+                    if ((t[(size_t)i * n + j] & (2 + 8)) || (t[(size_t)(i + 1) * n + j + 1] & (1 + 4))) dom[(size_t)i * m + j] = 1;
+            d = dom.data();
+            dlen = (int64_t)dom.size();
         }
-    });
-    for_rows(o, 1, m, m, [&](Sink& row_out, int i) {
-        for (int j = 1; j < m; ++j) {
-            if (D(i, j) != 1) continue;
-            const double x = j + .5, y = i + .5;
-            if ((i + j) % 2 == 1) {
-                if (D(i, j + 1) == 1) use(row_out, "he", x + .5, y, false);
-                if (D(i, j - 1) == 1) use(row_out, "he", x - .5, y, false);
+        if (dlen < (int64_t)m * m) return RT_E_INVAL;
+        auto D = [&](int i, int j) { return d[(size_t)i * m + j]; };
+        Sink o(filename);
+        o << kSvgOpen << "height=\"500\" width=\"500\" viewBox=\"0 0 " << m << " " << m << "\">\n";
+        o << "<defs>\n";
+        o << "<g id=\"hd\">  <polyline points= \"-.5,0 .5,0\" stroke=\"red\" stroke-width=\".05\"/> </g>\n";
+        o << "<g id=\"he\">  <polyline points= \"-.5,0 .5,0\" stroke=\"black\" stroke-width=\".01\"/> </g>\n";
+        o << "<g id=\"vd\">  <polyline points= \"0,-.5 0,.5\" stroke=\"red\" stroke-width=\".05\"/> </g>\n";
+        o << "<g id=\"ve\">  <polyline points= \"0,-.5 0,.5\" stroke=\"black\" stroke-width=\".01\"/> </g>\n";
+        o << "<g id=\"b\">  <circle cx=\"0\" cy=\"0\" r=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
+        o << "<g id=\"w\">  <circle cx=\"0\" cy=\"0\" r=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"white\" /> </g>\n";
+        o << "</defs>\n";
+        for_rows(o, 0, n, n, [&](Sink& row_out, int i) {
+            for (int j = 0; j < n; ++j) {
+                const double x = j, y = i;
+                const int32_t v = t[(size_t)i * n + j];
+                if ((v & 1) == 1) use(row_out, "hd", x, y - .5, false);
+                if ((v & 4) == 4) use(row_out, "vd", x - .5, y, false);
             }
-            if (D(i - 1, j) == 1) use(row_out, "ve", x, y - .5, false);
-            if (D(i + 1, j) == 1) use(row_out, "ve", x, y + .5, false);
-        }
+        });
+        for_rows(o, 1, m, m, [&](Sink& row_out, int i) {
+            for (int j = 1; j < m; ++j) {
+                if (D(i, j) != 1) continue;
+                const double x = j + .5, y = i + .5;
+                if ((i + j) % 2 == 1) {
+                    if (D(i, j + 1) == 1) use(row_out, "he", x + .5, y, false);
+                    if (D(i, j - 1) == 1) use(row_out, "he", x - .5, y, false);
+                }
+                if (D(i - 1, j) == 1) use(row_out, "ve", x, y - .5, false);
+                if (D(i + 1, j) == 1) use(row_out, "ve", x, y + .5, false);
+            }
+        });
+        for_rows(o, 1, m, m, [&](Sink& row_out, int i) {
+            for (int j = 1; j < m; ++j)
+                if (D(i, j) == 1) use(row_out, (i + j) % 2 == 0 ? "b" : "w", j + .5, i + .5, true);
+        });
+        o << "</svg>";
+        return finish(o);
     });
-    for_rows(o, 1, m, m, [&](Sink& row_out, int i) {
-        for (int j = 1; j < m; ++j)
-            if (D(i, j) == 1) use(row_out, (i + j) % 2 == 0 ? "b" : "w", j + .5, i + .5, true);
-    });
-    o << "</svg>";
-    return finish(o);
 }
 
 // ---- lozenges ----------------------------------------------------------------------
 // LozengeTiler::DomainToSVG (LozengeTiler.cpp:593-613).
 rt_status rt_lozenge_domain_svg(const int32_t* d, int64_t dlen, const char* filename) {
-    if (!d || !filename) return RT_E_INVAL;
-    const int m = side_of(dlen / 2);
-    Sink o(filename);
-    tri_header(o, m);
-    o << "<defs>\n";
-    o << "<g id=\"w\">  <polygon points = \"0,1 .5,0 1,1\" fill=\"lightsteelblue\"/> </g>\n";
-    o << "<g id=\"b\">  <polygon points = \"0,0 1,0 .5,1\" fill=\"slategrey\"/> </g>\n";
-    o << "</defs>\n";
-    for_rows(o, 0, m, 2 * m, [&](Sink& row_out, int i) {
-        for (int j = 0; j < 2 * m; ++j)
-            if (d[(size_t)i * 2 * m + j] == 1) use(row_out, j % 2 == 0 ? "b" : "w", .5 * j + .5 * i, i, true);
+    return guarded([&]() -> rt_status {
+        if (!d || !filename) return RT_E_INVAL;
+        const int m = side_of(dlen / 2);
+        Sink o(filename);
+        tri_header(o, m);
+        o << "<defs>\n";
+        o << "<g id=\"w\">  <polygon points = \"0,1 .5,0 1,1\" fill=\"lightsteelblue\"/> </g>\n";
+        o << "<g id=\"b\">  <polygon points = \"0,0 1,0 .5,1\" fill=\"slategrey\"/> </g>\n";
+        o << "</defs>\n";
+        for_rows(o, 0, m, 2 * m, [&](Sink& row_out, int i) {
+            for (int j = 0; j < 2 * m; ++j)
+                if (d[(size_t)i * 2 * m + j] == 1) use(row_out, j % 2 == 0 ? "b" : "w", .5 * j + .5 * i, i, true);
+        });
+        o << "</svg>";
+        return finish(o);
     });
-    o << "</svg>";
-    return finish(o);
 }
 
 // LozengeTiler::TilingToSVG (LozengeTiler.cpp:565-590).
 rt_status rt_lozenge_tiling_svg(const int32_t* t, int64_t tlen, const char* filename) {
-    if (!t || !filename) return RT_E_INVAL;
-    const int n = side_of(tlen), m = n - 1;
-    Sink o(filename);
-    tri_header(o, m);
-    o << "<defs>\n";
-    o << "<g id=\"r\">  <polygon points = \"0,0 -1,0 -.5,-1 .5,-1\" fill=\"midnightblue\"/> </g>\n";
-    o << "<g id=\"g\">  <polygon points = \"0,0 1,0 .5,-1 -.5,-1\" fill=\"lightsteelblue\"/> </g>\n";
-    o << "<g id=\"b\">  <polygon points = \"0,0 .5,-1 1,0 .5,1\" fill=\"slategrey\"/> </g>\n";
-    o << "</defs>\n";
-    for_rows(o, 1, n - 1, n, [&](Sink& row_out, int i) {
-        for (int j = 1; j < n - 1; ++j) {
-            const int32_t v = t[(size_t)i * n + j];
-            if ((v & 1) == 1) use(row_out, "r", j + .5 * i, i, true);
-            if ((v & 2) == 2) use(row_out, "g", j + .5 * i, i, true);
-            if ((v & 8) == 8) use(row_out, "b", j + .5 * i, i, true);
-        }
+    return guarded([&]() -> rt_status {
+        if (!t || !filename) return RT_E_INVAL;
+        const int n = side_of(tlen), m = n - 1;
+        Sink o(filename);
+        tri_header(o, m);
+        o << "<defs>\n";
+        o << "<g id=\"r\">  <polygon points = \"0,0 -1,0 -.5,-1 .5,-1\" fill=\"midnightblue\"/> </g>\n";
+        o << "<g id=\"g\">  <polygon points = \"0,0 1,0 .5,-1 -.5,-1\" fill=\"lightsteelblue\"/> </g>\n";
+        o << "<g id=\"b\">  <polygon points = \"0,0 .5,-1 1,0 .5,1\" fill=\"slategrey\"/> </g>\n";
+        o << "</defs>\n";
+        for_rows(o, 1, n - 1, n, [&](Sink& row_out, int i) {
+            for (int j = 1; j < n - 1; ++j) {
+                const int32_t v = t[(size_t)i * n + j];
+                if ((v & 1) == 1) use(row_out, "r", j + .5 * i, i, true);
+                if ((v & 2) == 2) use(row_out, "g", j + .5 * i, i, true);
+                if ((v & 8) == 8) use(row_out, "b", j + .5 * i, i, true);
+            }
+        });
+        o << "</svg>";
+        return finish(o);
     });
-    o << "</svg>";
-    return finish(o);
 }
 
 // LozengeTiler::DimerToSVG(t, d) (LozengeTiler.cpp:487-562); d = NULL takes
 // the domain from the tiling (TilingToDomain, :436-462).
 rt_status rt_lozenge_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d, int64_t dlen, const char* filename) {
-    if (!t || !filename) return RT_E_INVAL;
-    const int n = side_of(tlen), m = n - 1;
-    Vec dom;
-    if (!d) {
-        dom.assign((size_t)2 * m * m, 0);
-        auto set = [&](int r, int c) {
-            if (r >= 0 && r < m && c >= 0 && c < 2 * m) dom[(size_t)r * 2 * m + c] = 1;
-        };
-        for (int i = 0; i < n - 1; ++i)
-            for (int j = 0; j < n - 1; ++j) {
-                const int32_t v = t[(size_t)i * n + j];
-                if (v & 1) set(i - 1, 2 * j), set(i - 1, 2 * j - 1);
-                if (v & 2) set(i - 1, 2 * j), set(i - 1, 2 * j + 1);
-                if (v & 8) set(i - 1, 2 * j + 1), set(i, 2 * j);
-            }
-        d = dom.data();
-        dlen = (int64_t)dom.size();
-    }
-    if (dlen < (int64_t)2 * m * m + 2 * m) {  // the reference reads row N-1 (one past the domain)
-        Vec pad(d, d + dlen);
-        pad.resize((size_t)2 * m * (m + 2), 0);
-        dom.swap(pad);
-        d = dom.data();
-    }
-    auto D = [&](int i, int j) { return d[(size_t)i * m * 2 + j]; };
-    Sink o(filename);
-    tri_header(o, m);
-    o << "<defs>\n";
-    o << "<g id=\"e1\">  <polyline points= \"-.5,-.33333333333 0,-.666666666666\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
-    o << "<g id=\"e2\">  <polyline points= \"0,-.666666666 .5,-.333333333333\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
-    o << "<g id=\"e8\">  <polyline points= \".5,-.333333333333 .5,.333333333333\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
-    o << "<g id=\"d1\">  <polyline points= \"-.5,-.33333333333 0,-.666666666666\" stroke=\"black\" stroke-width=\".025\"/> </g>\n";
-    o << "<g id=\"d2\">  <polyline points= \"0,-.666666666 .5,-.333333333333\" stroke=\"black\" stroke-width=\".025\"/> </g>\n";
-    o << "<g id=\"d8\">  <polyline points= \".5,-.333333333333 .5,.333333333333\" stroke=\"black\" stroke-width=\".025\"/> </g>\n";
-    o << "<g id=\"b\">  <ellipse cx=\".5\" cy=\".333333333333\" rx=\".1\" ry=\".11547\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
-    o << "<g id=\"w\">  <ellipse cx=\".5\" cy=\".666666666666\" rx=\".1\"  ry=\".11547\" stroke=\"black\" stroke-width=\".02\" fill=\"white\" /> </g>\n";
-    o << "</defs>\n";
-    for_rows(o, 1, n - 1, n, [&](Sink& row_out, int i) {
-        for (int j = 1; j < n - 1; ++j) {
-            const int32_t v = t[(size_t)i * n + j];
-            if ((v & 1) == 1) use(row_out, "d1", j + .5 * i, i, true);
-            if ((v & 2) == 2) use(row_out, "d2", j + .5 * i, i, true);
-            if ((v & 8) == 8) use(row_out, "d8", j + .5 * i, i, true);
+    return guarded([&]() -> rt_status {
+        if (!t || !filename) return RT_E_INVAL;
+        const int n = side_of(tlen), m = n - 1;
+        Vec dom;
+        if (!d) {
+            dom.assign((size_t)2 * m * m, 0);
+            auto set = [&](int r, int c) {
+                if (r >= 0 && r < m && c >= 0 && c < 2 * m) dom[(size_t)r * 2 * m + c] = 1;
+            };
+            for (int i = 0; i < n - 1; ++i)
+                for (int j = 0; j < n - 1; ++j) {
+                    const int32_t v = t[(size_t)i * n + j];
+                    if (v & 1) set(i - 1, 2 * j), set(i - 1, 2 * j - 1);
+                    if (v & 2) set(i - 1, 2 * j), set(i - 1, 2 * j + 1);
+                    if (v & 8) set(i - 1, 2 * j + 1), set(i, 2 * j);
+                }
+            d = dom.data();
+            dlen = (int64_t)dom.size();
         }
-    });
-    for_rows(o, 1, n - 1, 2 * n, [&](Sink& row_out, int i) {
-        for (int j = 1; j < 2 * n - 1; ++j)
-            if (D(i, j) == 1 && j % 2 == 0) {
-                if (D(i, j - 1) == 1) use(row_out, "e1", .5 + .5 * j + .5 * i, i + 1, true);
-                if (D(i, j + 1) == 1) use(row_out, "e2", .5 + .5 * j + .5 * i, i + 1, true);
-                if (D(i + 1, j - 1) == 1) use(row_out, "e8", .5 + .5 * j + .5 * i, i + 1, true);
+        if (dlen < (int64_t)2 * m * m + 2 * m) {  // the reference reads row N-1 (one past the domain)
+            Vec pad(d, d + dlen);
+            pad.resize((size_t)2 * m * (m + 2), 0);
+            dom.swap(pad);
+            d = dom.data();
+        }
+        auto D = [&](int i, int j) { return d[(size_t)i * m * 2 + j]; };
+        Sink o(filename);
+        tri_header(o, m);
+        o << "<defs>\n";
+        o << "<g id=\"e1\">  <polyline points= \"-.5,-.33333333333 0,-.666666666666\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
+        o << "<g id=\"e2\">  <polyline points= \"0,-.666666666 .5,-.333333333333\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
+        o << "<g id=\"e8\">  <polyline points= \".5,-.333333333333 .5,.333333333333\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
+        o << "<g id=\"d1\">  <polyline points= \"-.5,-.33333333333 0,-.666666666666\" stroke=\"black\" stroke-width=\".025\"/> </g>\n";
+        o << "<g id=\"d2\">  <polyline points= \"0,-.666666666 .5,-.333333333333\" stroke=\"black\" stroke-width=\".025\"/> </g>\n";
+        o << "<g id=\"d8\">  <polyline points= \".5,-.333333333333 .5,.333333333333\" stroke=\"black\" stroke-width=\".025\"/> </g>\n";
+        o << "<g id=\"b\">  <ellipse cx=\".5\" cy=\".333333333333\" rx=\".1\" ry=\".11547\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
+        o << "<g id=\"w\">  <ellipse cx=\".5\" cy=\".666666666666\" rx=\".1\"  ry=\".11547\" stroke=\"black\" stroke-width=\".02\" fill=\"white\" /> </g>\n";
+        o << "</defs>\n";
+        for_rows(o, 1, n - 1, n, [&](Sink& row_out, int i) {
+            for (int j = 1; j < n - 1; ++j) {
+                const int32_t v = t[(size_t)i * n + j];
+                if ((v & 1) == 1) use(row_out, "d1", j + .5 * i, i, true);
+                if ((v & 2) == 2) use(row_out, "d2", j + .5 * i, i, true);
+                if ((v & 8) == 8) use(row_out, "d8", j + .5 * i, i, true);
             }
+        });
+        for_rows(o, 1, n - 1, 2 * n, [&](Sink& row_out, int i) {
+            for (int j = 1; j < 2 * n - 1; ++j)
+                if (D(i, j) == 1 && j % 2 == 0) {
+                    if (D(i, j - 1) == 1) use(row_out, "e1", .5 + .5 * j + .5 * i, i + 1, true);
+                    if (D(i, j + 1) == 1) use(row_out, "e2", .5 + .5 * j + .5 * i, i + 1, true);
+                    if (D(i + 1, j - 1) == 1) use(row_out, "e8", .5 + .5 * j + .5 * i, i + 1, true);
+                }
+        });
+        for_rows(o, 1, n - 1, 2 * n, [&](Sink& row_out, int i) {
+            for (int j = 1; j < 2 * n - 1; ++j)
+                if (D(i, j) == 1) use(row_out, j % 2 == 0 ? "b" : "w", .5 * i + .5 * j, i, true);
+        });
+        o << "</svg>";
+        return finish(o);
     });
-    for_rows(o, 1, n - 1, 2 * n, [&](Sink& row_out, int i) {
-        for (int j = 1; j < 2 * n - 1; ++j)
-            if (D(i, j) == 1) use(row_out, j % 2 == 0 ? "b" : "w", .5 * i + .5 * j, i, true);
-    });
-    o << "</svg>";
-    return finish(o);
 }
 
 // LozengeTiler::PrintDomain (LozengeTiler.cpp:391-403): the M x 2M domain as text.
 rt_status rt_lozenge_print_domain(const int32_t* d, int64_t dlen, const char* filename) {
-    if (!d || !filename) return RT_E_INVAL;
-    const int m = side_of(dlen / 2);
-    Sink o(filename);
-    for_rows(o, 0, m, 2 * m, [&](Sink& row_out, int i) {
-        for (int j = 0; j < 2 * m; ++j) row_out << d[(size_t)i * 2 * m + j] << " ";
-        row_out << "\n";
+    return guarded([&]() -> rt_status {
+        if (!d || !filename) return RT_E_INVAL;
+        const int m = side_of(dlen / 2);
+        Sink o(filename);
+        for_rows(o, 0, m, 2 * m, [&](Sink& row_out, int i) {
+            for (int j = 0; j < 2 * m; ++j) row_out << d[(size_t)i * 2 * m + j] << " ";
+            row_out << "\n";
+        });
+        return finish(o);
     });
-    return finish(o);
 }
 
 // ---- rectangle-triangle (RectTriangleTiler::TilingToSVG, :567-592) -------------------
 rt_status rt_recttri_tiling_svg(const int32_t* t, int64_t tlen, const char* filename) {
-    if (!t || !filename) return RT_E_INVAL;
-    const int n = side_of(tlen), m = n - 1;
-    const double W = kSqrt3 * 2 * (n + 1), H = 3 / 2.0 * (n + 1), s = 20;
-    Sink o(filename);
-    o << "<svg xmlns='http://www.w3.org/2000/svg' height=\"" << s * H << "\" width=\"" << s * W << "\" >\n";
-    for_rows(o, 0, m, 8 * m, [&](Sink& row_out, int i) {
-        for (int j = 0; j < m; ++j) {
-            face_picture(row_out, (t[(size_t)i * n + j + 1] & (0xf << 4)) >> 4, i, 2 * j + 1);
-            face_picture(row_out, t[(size_t)i * n + j] & 0xf, i, 2 * j);
-        }
+    return guarded([&]() -> rt_status {
+        if (!t || !filename) return RT_E_INVAL;
+        const int n = side_of(tlen), m = n - 1;
+        const double W = kSqrt3 * 2 * (n + 1), H = 3 / 2.0 * (n + 1), s = 20;
+        Sink o(filename);
+        o << "<svg xmlns='http://www.w3.org/2000/svg' height=\"" << s * H << "\" width=\"" << s * W << "\" >\n";
+        for_rows(o, 0, m, 8 * m, [&](Sink& row_out, int i) {
+            for (int j = 0; j < m; ++j) {
+                face_picture(row_out, (t[(size_t)i * n + j + 1] & (0xf << 4)) >> 4, i, 2 * j + 1);
+                face_picture(row_out, t[(size_t)i * n + j] & 0xf, i, 2 * j);
+            }
+        });
+        o << "</svg>";
+        return finish(o);
     });
-    o << "</svg>";
-    return finish(o);
 }
 
 // ---- triangular-lattice dimers (TriangleDimerTiler.cpp:772-902) ------------------------
 rt_status rt_tridimer_domain_svg(const int32_t* d, int64_t dlen, const char* filename) {
-    if (!d || !filename) return RT_E_INVAL;
-    const int m = side_of(dlen / 2);
-    Sink o(filename);
-    tri_header(o, m);
-    o << "<defs>\n";
-    o << "<g id=\"w\">  <polygon points = \"0,1 .5,0 1,1\" fill=\"paleturquoise\"/> </g>\n";
-    o << "<g id=\"b\">  <polygon points = \"0,0 1,0 .5,1\" fill=\"deepskyblue\"/> </g>\n";
-    o << "</defs>\n";
-    for_rows(o, 0, m, 2 * m, [&](Sink& row_out, int i) {
-        for (int j = 0; j < 2 * m; ++j)
-            if (d[(size_t)i * m * 2 + j] == 1) use(row_out, j % 2 == 0 ? "b" : "w", .5 * j + .5 * i, i, true);
+    return guarded([&]() -> rt_status {
+        if (!d || !filename) return RT_E_INVAL;
+        const int m = side_of(dlen / 2);
+        Sink o(filename);
+        tri_header(o, m);
+        o << "<defs>\n";
+        o << "<g id=\"w\">  <polygon points = \"0,1 .5,0 1,1\" fill=\"paleturquoise\"/> </g>\n";
+        o << "<g id=\"b\">  <polygon points = \"0,0 1,0 .5,1\" fill=\"deepskyblue\"/> </g>\n";
+        o << "</defs>\n";
+        for_rows(o, 0, m, 2 * m, [&](Sink& row_out, int i) {
+            for (int j = 0; j < 2 * m; ++j)
+                if (d[(size_t)i * m * 2 + j] == 1) use(row_out, j % 2 == 0 ? "b" : "w", .5 * j + .5 * i, i, true);
+        });
+        o << "</svg>";
+        return finish(o);
     });
-    o << "</svg>";
-    return finish(o);
 }
 
 rt_status rt_tridimer_tiling_svg(const int32_t* t, int64_t tlen, const char* filename) {
-    if (!t || !filename) return RT_E_INVAL;
-    const int n = side_of(tlen), m = n / 2;
-    Sink o(filename);
-    tri_header(o, m);
-    o << "<defs>\n";
-    o << "<g id=\"dR\">  <polygon points = \"1,-0.6666666667 0.5,-0.3333333333 0.5,0.3333333333 0,0.6666666667 0,1.333333333 0.5,1.666666667 1,1.333333333 1,0.6666666667 1.5,0.3333333333 1.5,-0.3333333333\" fill=\"midnightblue\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
-    o << "<g id=\"dL\">  <polygon points = \"0,-0.6666666667 0.5,-0.3333333333 0.5,0.3333333333 1,0.6666666667 1,1.333333333 0.5,1.666666667 0,1.333333333 0,0.6666666667 -0.5,0.3333333333 -0.5,-0.3333333333\" fill=\"lightsteelblue\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
-    o << "<g id=\"dH\">  <polygon points = \"0,-0.6666666667 0.5,-0.3333333333 1,-0.6666666667 1.5,-0.3333333333 1.5,0.3333333333 1,0.6666666667 0.5,0.3333333333 0,0.6666666667 -0.5,0.3333333333 -0.5,-0.3333333333\" fill=\"slategrey\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
-    o << "</defs>\n";
-    for_rows(o, 0, m - 1, m, [&](Sink& row_out, int i) {
-        for (int j = 1; j < 2 * m - 1; j += 2) {
-            const double x = .5 * j + .5 * i;
-            if ((t[(size_t)2 * i * n + j] & 4) == 4) use(row_out, "dR", x, i, true);
-            if ((t[(size_t)2 * i * n + j] & 8) == 8) use(row_out, "dL", x, i, true);
-            if ((t[(size_t)(2 * i + 1) * n + j] & 1) == 1) use(row_out, "dH", x, i, true);
-        }
+    return guarded([&]() -> rt_status {
+        if (!t || !filename) return RT_E_INVAL;
+        const int n = side_of(tlen), m = n / 2;
+        Sink o(filename);
+        tri_header(o, m);
+        o << "<defs>\n";
+        o << "<g id=\"dR\">  <polygon points = \"1,-0.6666666667 0.5,-0.3333333333 0.5,0.3333333333 0,0.6666666667 0,1.333333333 0.5,1.666666667 1,1.333333333 1,0.6666666667 1.5,0.3333333333 1.5,-0.3333333333\" fill=\"midnightblue\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
+        o << "<g id=\"dL\">  <polygon points = \"0,-0.6666666667 0.5,-0.3333333333 0.5,0.3333333333 1,0.6666666667 1,1.333333333 0.5,1.666666667 0,1.333333333 0,0.6666666667 -0.5,0.3333333333 -0.5,-0.3333333333\" fill=\"lightsteelblue\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
+        o << "<g id=\"dH\">  <polygon points = \"0,-0.6666666667 0.5,-0.3333333333 1,-0.6666666667 1.5,-0.3333333333 1.5,0.3333333333 1,0.6666666667 0.5,0.3333333333 0,0.6666666667 -0.5,0.3333333333 -0.5,-0.3333333333\" fill=\"slategrey\" stroke=\"black\" stroke-width=\".05\"/></g>\n";
+        o << "</defs>\n";
+        for_rows(o, 0, m - 1, m, [&](Sink& row_out, int i) {
+            for (int j = 1; j < 2 * m - 1; j += 2) {
+                const double x = .5 * j + .5 * i;
+                if ((t[(size_t)2 * i * n + j] & 4) == 4) use(row_out, "dR", x, i, true);
+                if ((t[(size_t)2 * i * n + j] & 8) == 8) use(row_out, "dL", x, i, true);
+                if ((t[(size_t)(2 * i + 1) * n + j] & 1) == 1) use(row_out, "dH", x, i, true);
+            }
+        });
+        o << "</svg>";
+        return finish(o);
     });
-    o << "</svg>";
-    return finish(o);
 }
 
 // TriangleDimerTiler::DimerToSVG(t, d) (:841-902); d = NULL takes the domain
 // from the tiling (TilingToDomain).
 rt_status rt_tridimer_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d, int64_t dlen, const char* filename) {
-    if (!t || !filename) return RT_E_INVAL;
-    const int n = side_of(tlen);
-    Vec dom;
-    if (!d) {
-        int64_t len = 0;
-        if (rt_tridimer_tiling_to_domain(t, tlen, nullptr, 0, &len) != RT_OK) return RT_E_INVAL;
-        dom.resize((size_t)len);
-        if (rt_tridimer_tiling_to_domain(t, tlen, dom.data(), len, &len) != RT_OK) return RT_E_INVAL;
-        d = dom.data();
-        dlen = len;
-    }
-    const int m = side_of(dlen / 2);
-    // The reference also reads one cell before the domain and one row past it.
-    Vec pad((size_t)2 * m * (m + 2) + 2, 0);
-    for (int64_t k = 0; k < dlen; ++k) pad[(size_t)k + 2 * m + 1] = d[k];
-    auto D = [&](int i, int j) { return pad[(size_t)(i * 2 * m + j) + 2 * m + 1]; };
-    Sink o(filename);
-    tri_header(o, m);
-    o << "<defs>\n";
-    o << "<g id=\"dR\">  <polyline points= \".5,1 1,0\" stroke=\"darkblue\" stroke-width=\".05\"/> </g>\n";
-    o << "<g id=\"dL\">  <polyline points= \".5,1 0,0\" stroke=\"darkred\" stroke-width=\".05\"/> </g>\n";
-    o << "<g id=\"dH\">  <polyline points= \"1,0 0,0\" stroke=\"darkgreen\" stroke-width=\".05\"/> </g>\n";
-    o << "<g id=\"eR\">  <polyline points= \".5,1 1,0\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
-    o << "<g id=\"eL\">  <polyline points= \".5,1 0,0\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
-    o << "<g id=\"eH\">  <polyline points= \"1,0 0,0\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
-    o << "<g id=\"v1\">  <ellipse cx=\".5\" cy=\"0\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
-    o << "<g id=\"v2\">  <ellipse cx=\"1.5\" cy=\"0\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
-    o << "<g id=\"v3\">  <ellipse cx=\"1\" cy=\"1\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
-    o << "</defs>\n";
-    for_rows(o, 0, m - 1, 2 * m, [&](Sink& row_out, int i) {
-        for (int j = 1; j < 2 * m - 1; j += 2) {
-            const double x = .5 * j + .5 * i;
-            const int32_t a = t[(size_t)2 * i * n + j], h = t[(size_t)(2 * i + 1) * n + j];
-            if ((a & 4) == 4) use(row_out, "dR", x, i, true);
-            else if (D(i, j - 1) == 1) use(row_out, "eR", x, i, true);
-            if ((a & 8) == 8) use(row_out, "dL", x, i, true);
-            else if (D(i, j - 1) == 1) use(row_out, "eL", x, i, true);
-            if ((h & 1) == 1) use(row_out, "dH", x, i, true);
-            else if (D(i, j - 1) == 1 || D(i - 1, j) == 1) use(row_out, "eH", x, i, true);
-            if ((a & 4) == 0 && D(i, j) == 1) use(row_out, "eR", x, i, true);
-            if ((a & 8) == 0 && D(i, j - 2) == 1 && j > 1) use(row_out, "eL", x, i, true);
+    return guarded([&]() -> rt_status {
+        if (!t || !filename) return RT_E_INVAL;
+        const int n = side_of(tlen);
+        Vec dom;
+        if (!d) {
+            int64_t len = 0;
+            if (rt_tridimer_tiling_to_domain(t, tlen, nullptr, 0, &len) != RT_OK) return RT_E_INVAL;
+            dom.resize((size_t)len);
+            if (rt_tridimer_tiling_to_domain(t, tlen, dom.data(), len, &len) != RT_OK) return RT_E_INVAL;
+            d = dom.data();
+            dlen = len;
         }
+        const int m = side_of(dlen / 2);
+        // The reference also reads one cell before the domain and one row past it.
+        Vec pad((size_t)2 * m * (m + 2) + 2, 0);
+        for (int64_t k = 0; k < dlen; ++k) pad[(size_t)k + 2 * m + 1] = d[k];
+        auto D = [&](int i, int j) { return pad[(size_t)(i * 2 * m + j) + 2 * m + 1]; };
+        Sink o(filename);
+        tri_header(o, m);
+        o << "<defs>\n";
+        o << "<g id=\"dR\">  <polyline points= \".5,1 1,0\" stroke=\"darkblue\" stroke-width=\".05\"/> </g>\n";
+        o << "<g id=\"dL\">  <polyline points= \".5,1 0,0\" stroke=\"darkred\" stroke-width=\".05\"/> </g>\n";
+        o << "<g id=\"dH\">  <polyline points= \"1,0 0,0\" stroke=\"darkgreen\" stroke-width=\".05\"/> </g>\n";
+        o << "<g id=\"eR\">  <polyline points= \".5,1 1,0\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
+        o << "<g id=\"eL\">  <polyline points= \".5,1 0,0\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
+        o << "<g id=\"eH\">  <polyline points= \"1,0 0,0\" stroke=\"black\" stroke-width=\".001\"/> </g>\n";
+        o << "<g id=\"v1\">  <ellipse cx=\".5\" cy=\"0\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
+        o << "<g id=\"v2\">  <ellipse cx=\"1.5\" cy=\"0\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
+        o << "<g id=\"v3\">  <ellipse cx=\"1\" cy=\"1\" rx=\".1\" ry=\".1\" stroke=\"black\" stroke-width=\".02\" fill=\"black\"/> </g> \n";
+        o << "</defs>\n";
+        for_rows(o, 0, m - 1, 2 * m, [&](Sink& row_out, int i) {
+            for (int j = 1; j < 2 * m - 1; j += 2) {
+                const double x = .5 * j + .5 * i;
+                const int32_t a = t[(size_t)2 * i * n + j], h = t[(size_t)(2 * i + 1) * n + j];
+                if ((a & 4) == 4) use(row_out, "dR", x, i, true);
+                else if (D(i, j - 1) == 1) use(row_out, "eR", x, i, true);
+                if ((a & 8) == 8) use(row_out, "dL", x, i, true);
+                else if (D(i, j - 1) == 1) use(row_out, "eL", x, i, true);
+                if ((h & 1) == 1) use(row_out, "dH", x, i, true);
+                else if (D(i, j - 1) == 1 || D(i - 1, j) == 1) use(row_out, "eH", x, i, true);
+                if ((a & 4) == 0 && D(i, j) == 1) use(row_out, "eR", x, i, true);
+                if ((a & 8) == 0 && D(i, j - 2) == 1 && j > 1) use(row_out, "eL", x, i, true);
+            }
+        });
+        for_rows(o, 0, m, 2 * m, [&](Sink& row_out, int i) {
+            for (int j = 2; j < 2 * m; j += 2) {
+                const double x = .5 * j + .5 * i;
+                if (D(i, j) == 1 || D(i, j - 1) == 1) use(row_out, "v1", x, i, true);
+                if (D(i, j) == 1 || D(i, j + 1) == 1) use(row_out, "v2", x, i, true);
+                if (D(i, j) == 1 || D(i, j + 1) == 1 || D(i, j - 1) == 1) use(row_out, "v3", x, i, true);
+            }
+        });
+        o << "</svg>";
+        return finish(o);
     });
-    for_rows(o, 0, m, 2 * m, [&](Sink& row_out, int i) {
-        for (int j = 2; j < 2 * m; j += 2) {
-            const double x = .5 * j + .5 * i;
-            if (D(i, j) == 1 || D(i, j - 1) == 1) use(row_out, "v1", x, i, true);
-            if (D(i, j) == 1 || D(i, j + 1) == 1) use(row_out, "v2", x, i, true);
-            if (D(i, j) == 1 || D(i, j + 1) == 1 || D(i, j - 1) == 1) use(row_out, "v3", x, i, true);
-        }
-    });
-    o << "</svg>";
-    return finish(o);
 }
 
 // ---- text matrices (common.cpp:82-161) ---------------------------------------------------
 // SaveMatrix: sqrt(size) rows of sqrt(size) values, each followed by a space.
 rt_status rt_save_matrix(const int32_t* a, int64_t len, const char* filename) {
-    if (!a || !filename) return RT_E_INVAL;
-    const int n = side_of(len);
-    Sink o(filename);
-    for_rows(o, 0, n, n, [&](Sink& row_out, int i) {
-        for (int j = 0; j < n; ++j) row_out << a[(size_t)i * n + j] << " ";
-        row_out << "\n";
+    return guarded([&]() -> rt_status {
+        if (!a || !filename) return RT_E_INVAL;
+        const int n = side_of(len);
+        Sink o(filename);
+        for_rows(o, 0, n, n, [&](Sink& row_out, int i) {
+            for (int j = 0; j < n; ++j) row_out << a[(size_t)i * n + j] << " ";
+            row_out << "\n";
+        });
+        return finish(o);
     });
-    return finish(o);
 }
 
 // LoadMatrix: every maximal run of decimal digits is one value (like the
 // reference, minus signs are not read).
 rt_status rt_load_matrix(const char* filename, int32_t* out, int64_t cap, int64_t* len) {
-    if (!filename) return RT_E_INVAL;
-    std::ifstream in(filename);
-    if (!in) return RT_E_INVAL;
-    std::vector<int32_t> v;
-    char c;
-    bool inside = false;
-    int64_t cur = 0;
-    while (in.get(c)) {
-        if (c >= '0' && c <= '9') {
-            cur = inside ? cur * 10 + (c - '0') : (c - '0');
-            inside = true;
-        } else if (inside) {
-            v.push_back((int32_t)cur);
-            inside = false;
+    return guarded([&]() -> rt_status {
+        if (!filename) return RT_E_INVAL;
+        std::ifstream in(filename);
+        if (!in) return RT_E_INVAL;
+        std::vector<int32_t> v;
+        char c;
+        bool inside = false;
+        int64_t cur = 0;
+        while (in.get(c)) {
+            if (c >= '0' && c <= '9') {
+                cur = inside ? cur * 10 + (c - '0') : (c - '0');
+                inside = true;
+            } else if (inside) {
+                v.push_back((int32_t)cur);
+                inside = false;
+            }
         }
-    }
-    if (inside) v.push_back((int32_t)cur);
-    if (len) *len = (int64_t)v.size();
-    if (!out) return RT_OK;
-    if (cap < (int64_t)v.size()) return RT_E_INVAL;
-    for (size_t k = 0; k < v.size(); ++k) out[k] = v[k];
-    return RT_OK;
+        if (inside) v.push_back((int32_t)cur);
+        if (len) *len = (int64_t)v.size();
+        if (!out) return RT_OK;
+        if (cap < (int64_t)v.size()) return RT_E_INVAL;
+        for (size_t k = 0; k < v.size(); ++k) out[k] = v[k];
+        return RT_OK;
+    });
 }
 
 // ---- binary matrices (no reference counterpart) ---------------------------------------------
@@ -671,88 +704,100 @@ size_t bin_payload(int64_t count, int bits) { return (size_t)(((uint64_t)count *
 }  // namespace
 
 rt_status rt_save_matrix_binary(const int32_t* a, int64_t len, const char* filename) {
-    if ((!a && len > 0) || len < 0 || !filename) return RT_E_INVAL;
-    int64_t lo = 0, hi = 0;
-    for (int64_t k = 0; k < len; ++k) {
-        if (k == 0 || a[k] < lo) lo = a[k];
-        if (k == 0 || a[k] > hi) hi = a[k];
-    }
-    const uint64_t span = (uint64_t)(hi - lo);
-    int bits = 32;
-    for (int b : {1, 2, 4, 8, 16})
-        if (span < (1ull << b)) {
-            bits = b;
-            break;
+    return guarded([&]() -> rt_status {
+        if ((!a && len > 0) || len < 0 || !filename) return RT_E_INVAL;
+        int64_t lo = 0, hi = 0;
+        for (int64_t k = 0; k < len; ++k) {
+            if (k == 0 || a[k] < lo) lo = a[k];
+            if (k == 0 || a[k] > hi) hi = a[k];
         }
-    std::vector<unsigned char> pay(bin_payload(len, bits), 0);
-    for (int64_t k = 0; k < len; ++k) {
-        const uint32_t v = (uint32_t)((int64_t)a[k] - lo);
-        if (bits < 8) {
-            pay[(size_t)((k * bits) >> 3)] |= (unsigned char)(v << ((k * bits) & 7));
-        } else {
-            for (int byte = 0; byte < bits / 8; ++byte) pay[(size_t)k * (bits / 8) + byte] = (unsigned char)(v >> (8 * byte));
+        const uint64_t span = (uint64_t)(hi - lo);
+        int bits = 32;
+        for (int b : {1, 2, 4, 8, 16})
+            if (span < (1ull << b)) {
+                bits = b;
+                break;
+            }
+        std::vector<unsigned char> pay(bin_payload(len, bits), 0);
+        for (int64_t k = 0; k < len; ++k) {
+            const uint32_t v = (uint32_t)((int64_t)a[k] - lo);
+            if (bits < 8) {
+                pay[(size_t)((k * bits) >> 3)] |= (unsigned char)(v << ((k * bits) & 7));
+            } else {
+                for (int byte = 0; byte < bits / 8; ++byte) pay[(size_t)k * (bits / 8) + byte] = (unsigned char)(v >> (8 * byte));
+            }
         }
-    }
-    unsigned char head[kBinHeader] = {0};
-    std::memcpy(head, kBinMagic, 8);
-    const uint64_t cnt = (uint64_t)len, base = (uint64_t)lo, sum = fnv1a(pay.data(), pay.size());
-    for (int b = 0; b < 8; ++b) {
-        head[8 + b] = (unsigned char)(cnt >> (8 * b));
-        head[24 + b] = (unsigned char)(base >> (8 * b));
-        head[32 + b] = (unsigned char)(sum >> (8 * b));
-    }
-    for (int b = 0; b < 4; ++b) head[16 + b] = (unsigned char)((uint32_t)bits >> (8 * b));
-    std::FILE* f = std::fopen(filename, "wb");
-    if (!f) return RT_E_INVAL;
-    bool ok = std::fwrite(head, 1, kBinHeader, f) == kBinHeader &&
-              (pay.empty() || std::fwrite(pay.data(), 1, pay.size(), f) == pay.size());
-    ok = (std::fclose(f) == 0) && ok;
-    return ok ? RT_OK : RT_E_INVAL;
+        unsigned char head[kBinHeader] = {0};
+        std::memcpy(head, kBinMagic, 8);
+        const uint64_t cnt = (uint64_t)len, base = (uint64_t)lo, sum = fnv1a(pay.data(), pay.size());
+        for (int b = 0; b < 8; ++b) {
+            head[8 + b] = (unsigned char)(cnt >> (8 * b));
+            head[24 + b] = (unsigned char)(base >> (8 * b));
+            head[32 + b] = (unsigned char)(sum >> (8 * b));
+        }
+        for (int b = 0; b < 4; ++b) head[16 + b] = (unsigned char)((uint32_t)bits >> (8 * b));
+        std::FILE* f = std::fopen(filename, "wb");
+        if (!f) return RT_E_INVAL;
+        bool ok = std::fwrite(head, 1, kBinHeader, f) == kBinHeader &&
+                  (pay.empty() || std::fwrite(pay.data(), 1, pay.size(), f) == pay.size());
+        ok = (std::fclose(f) == 0) && ok;
+        return ok ? RT_OK : RT_E_INVAL;
+    });
 }
 
 rt_status rt_load_matrix_binary(const char* filename, int32_t* out, int64_t cap, int64_t* len) {
-    if (!filename) return RT_E_INVAL;
-    std::FILE* f = std::fopen(filename, "rb");
-    if (!f) return RT_E_INVAL;
-    unsigned char head[kBinHeader];
-    std::vector<unsigned char> pay;
-    bool ok = std::fread(head, 1, kBinHeader, f) == kBinHeader && std::memcmp(head, kBinMagic, 8) == 0;
-    uint64_t cnt = 0, base = 0, sum = 0;
-    uint32_t bits = 0, zero = 0;
-    if (ok) {
-        for (int b = 0; b < 8; ++b) {
-            cnt |= (uint64_t)head[8 + b] << (8 * b);
-            base |= (uint64_t)head[24 + b] << (8 * b);
-            sum |= (uint64_t)head[32 + b] << (8 * b);
+    return guarded([&]() -> rt_status {
+        if (!filename) return RT_E_INVAL;
+        std::FILE* f = std::fopen(filename, "rb");
+        if (!f) return RT_E_INVAL;
+        unsigned char head[kBinHeader];
+        std::vector<unsigned char> pay;
+        bool ok = std::fread(head, 1, kBinHeader, f) == kBinHeader && std::memcmp(head, kBinMagic, 8) == 0;
+        uint64_t cnt = 0, base = 0, sum = 0;
+        uint32_t bits = 0, zero = 0;
+        if (ok) {
+            for (int b = 0; b < 8; ++b) {
+                cnt |= (uint64_t)head[8 + b] << (8 * b);
+                base |= (uint64_t)head[24 + b] << (8 * b);
+                sum |= (uint64_t)head[32 + b] << (8 * b);
+            }
+            for (int b = 0; b < 4; ++b) {
+                bits |= (uint32_t)head[16 + b] << (8 * b);
+                zero |= (uint32_t)head[20 + b] << (8 * b);
+            }
+            ok = zero == 0 && (bits == 1 || bits == 2 || bits == 4 || bits == 8 || bits == 16 || bits == 32) &&
+                 cnt <= (1ull << 40);
         }
-        for (int b = 0; b < 4; ++b) {
-            bits |= (uint32_t)head[16 + b] << (8 * b);
-            zero |= (uint32_t)head[20 + b] << (8 * b);
+        if (ok) {
+            // The file must hold exactly the payload its header announces; check
+            // its size before the payload buffer is sized from the header.
+            const size_t want = bin_payload((int64_t)cnt, (int)bits);
+            const long at = std::ftell(f);
+            ok = at == (long)kBinHeader && std::fseek(f, 0, SEEK_END) == 0 &&
+                 std::ftell(f) == (long)(kBinHeader + want) && std::fseek(f, at, SEEK_SET) == 0;
+            if (ok) {
+                pay.resize(want);
+                ok = pay.empty() || std::fread(pay.data(), 1, pay.size(), f) == pay.size();
+                ok = ok && std::fgetc(f) == EOF && fnv1a(pay.data(), pay.size()) == sum;
+            }
         }
-        ok = zero == 0 && (bits == 1 || bits == 2 || bits == 4 || bits == 8 || bits == 16 || bits == 32) &&
-             cnt <= (1ull << 40);
-    }
-    if (ok) {
-        pay.resize(bin_payload((int64_t)cnt, (int)bits));
-        ok = pay.empty() || std::fread(pay.data(), 1, pay.size(), f) == pay.size();
-        ok = ok && std::fgetc(f) == EOF && fnv1a(pay.data(), pay.size()) == sum;
-    }
-    std::fclose(f);
-    if (!ok) return RT_E_INVAL;  // not this format, truncated, trailing bytes or corrupted
-    if (len) *len = (int64_t)cnt;
-    if (!out) return RT_OK;
-    if (cap < (int64_t)cnt) return RT_E_INVAL;
-    const int64_t lo = (int64_t)base;
-    for (uint64_t k = 0; k < cnt; ++k) {
-        uint32_t v = 0;
-        if (bits < 8) {
-            v = (pay[(size_t)((k * bits) >> 3)] >> ((k * bits) & 7)) & ((1u << bits) - 1);
-        } else {
-            for (uint32_t byte = 0; byte < bits / 8; ++byte) v |= (uint32_t)pay[(size_t)k * (bits / 8) + byte] << (8 * byte);
+        std::fclose(f);
+        if (!ok) return RT_E_INVAL;  // not this format, truncated, trailing bytes or corrupted
+        if (len) *len = (int64_t)cnt;
+        if (!out) return RT_OK;
+        if (cap < (int64_t)cnt) return RT_E_INVAL;
+        const int64_t lo = (int64_t)base;
+        for (uint64_t k = 0; k < cnt; ++k) {
+            uint32_t v = 0;
+            if (bits < 8) {
+                v = (pay[(size_t)((k * bits) >> 3)] >> ((k * bits) & 7)) & ((1u << bits) - 1);
+            } else {
+                for (uint32_t byte = 0; byte < bits / 8; ++byte) v |= (uint32_t)pay[(size_t)k * (bits / 8) + byte] << (8 * byte);
+            }
+            out[k] = (int32_t)(lo + (int64_t)v);
         }
-        out[k] = (int32_t)(lo + (int64_t)v);
-    }
-    return RT_OK;
+        return RT_OK;
+    });
 }
 
 }  // extern "C"

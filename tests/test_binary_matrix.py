@@ -84,3 +84,22 @@ def test_text_file_is_not_binary(tmp_path):
     builders.save_matrix(np.arange(16, dtype=np.int32), p)
     with pytest.raises(_capi.RtError):
         builders.load_matrix_binary(p)
+
+
+@pytest.mark.parametrize("count,bits", [(1 << 40, 32), ((1 << 40) - 1, 1), (1 << 33, 8), (5, 32)])
+def test_header_that_overstates_the_payload_is_refused(count, bits, tmp_path):
+    """A header announcing more values than the file holds is refused from the
+    file's size, before a buffer is sized from the header: a count of 2^40
+    32-bit values must not become a 4 TB allocation."""
+    p = tmp_path / "forged.bin"
+    head = bytearray(HEADER)
+    head[:8] = b"RTBMAT1\0"
+    head[8:16] = count.to_bytes(8, "little")
+    head[16:20] = bits.to_bytes(4, "little")
+    open(p, "wb").write(bytes(head) + b"\0" * 16)
+    lib = _capi.load()
+    import ctypes
+
+    n = ctypes.c_int64(-1)
+    assert lib.rt_load_matrix_binary(str(p).encode(), None, 0, ctypes.byref(n)) == _capi.RT_E_INVAL
+    assert n.value == -1
