@@ -23,10 +23,13 @@
 
 #include "../../include/rt_b200_batch.h"
 #include "rt_internal.h"
+#include "rt_guard.h"
 #include "rt_models.cuh"
 #include "rt_tdplane.cuh"
 #include "rt_tridimer.cuh"
 #include "rt_word.cuh"
+
+using rtb::guarded;
 
 namespace cg = cooperative_groups;
 
@@ -921,296 +924,314 @@ rt_status plan_family(rt_batch* b, int f) {
 extern "C" {
 
 rt_status rt_batch_create(int32_t device, rt_batch** out) {
-    if (!out) return RT_E_INVAL;
-    *out = nullptr;
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
-        g_batch_create_error = "no CUDA device with that ordinal";
-        return RT_E_NODEVICE;
-    }
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
-        g_batch_create_error = "device is not sm_100";
-        return RT_E_NODEVICE;
-    }
-    cudaSetDevice(device);
-    rt_batch* b = new rt_batch();
-    b->device = device;
-    bool ok = cudaMallocHost(&b->h_step0, kFamilies * sizeof(int64_t)) == cudaSuccess &&
-              cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
-              cudaEventCreate(&b->t0) == cudaSuccess && cudaEventCreate(&b->t1) == cudaSuccess;
-    for (int f = 0; f < kFamilies && ok; ++f)
-        ok = cudaStreamCreateWithFlags(&b->fam_stream[f], cudaStreamNonBlocking) == cudaSuccess &&
-             cudaEventCreateWithFlags(&b->join[f], cudaEventDisableTiming) == cudaSuccess;
-    if (!ok) {
-        rt_batch_destroy(b);
-        g_batch_create_error = "stream / event creation failed";
-        return RT_E_CUDA;
-    }
-    *out = b;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!out) return RT_E_INVAL;
+        *out = nullptr;
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+            g_batch_create_error = "no CUDA device with that ordinal";
+            return RT_E_NODEVICE;
+        }
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+            g_batch_create_error = "device is not sm_100";
+            return RT_E_NODEVICE;
+        }
+        cudaSetDevice(device);
+        rt_batch* b = new rt_batch();
+        b->device = device;
+        bool ok = cudaMallocHost(&b->h_step0, kFamilies * sizeof(int64_t)) == cudaSuccess &&
+                  cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
+                  cudaEventCreate(&b->t0) == cudaSuccess && cudaEventCreate(&b->t1) == cudaSuccess;
+        for (int f = 0; f < kFamilies && ok; ++f)
+            ok = cudaStreamCreateWithFlags(&b->fam_stream[f], cudaStreamNonBlocking) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&b->join[f], cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) {
+            rt_batch_destroy(b);
+            g_batch_create_error = "stream / event creation failed";
+            return RT_E_CUDA;
+        }
+        *out = b;
+        return RT_OK;
+    });
 }
 
 rt_status rt_batch_destroy(rt_batch* b) {
-    if (!b) return RT_E_INVAL;
-    cudaSetDevice(b->device);
-    if (b->stream) cudaStreamSynchronize(b->stream);
-    b->drop_graph();
-    for (int f = 0; f < kFamilies; ++f) {
-        if (b->fam_stream[f]) cudaStreamDestroy(b->fam_stream[f]);
-        if (b->join[f]) cudaEventDestroy(b->join[f]);
-    }
-    if (b->fork) cudaEventDestroy(b->fork);
-    if (b->t0) cudaEventDestroy(b->t0);
-    if (b->t1) cudaEventDestroy(b->t1);
-    if (b->stream) cudaStreamDestroy(b->stream);
-    if (b->h_step0) cudaFreeHost(b->h_step0);
-    delete b;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!b) return RT_E_INVAL;
+        cudaSetDevice(b->device);
+        if (b->stream) cudaStreamSynchronize(b->stream);
+        b->drop_graph();
+        for (int f = 0; f < kFamilies; ++f) {
+            if (b->fam_stream[f]) cudaStreamDestroy(b->fam_stream[f]);
+            if (b->join[f]) cudaEventDestroy(b->join[f]);
+        }
+        if (b->fork) cudaEventDestroy(b->fork);
+        if (b->t0) cudaEventDestroy(b->t0);
+        if (b->t1) cudaEventDestroy(b->t1);
+        if (b->stream) cudaStreamDestroy(b->stream);
+        if (b->h_step0) cudaFreeHost(b->h_step0);
+        delete b;
+        return RT_OK;
+    });
 }
 
 const char* rt_batch_last_error(rt_batch* b) { return b ? b->err.c_str() : g_batch_create_error.c_str(); }
 
 rt_status rt_batch_add(rt_batch* b, const rt_chain* c, const int32_t* tiling, int32_t n, int64_t* index) {
-    if (!b || !c || !tiling) return b ? b->fail(RT_E_INVAL, "null argument") : RT_E_INVAL;
-    if (b->sweeps_done > 0) return b->fail(RT_E_STATE, "chains are added before the first run");
-    const int f = family_of(c->model, c->kernel);
-    if (f < 0) return b->fail(RT_E_INVAL, "unsupported model / kernel in a batch");
-    Chain ch;
-    ch.fam = f;
-    ch.kind = kind_of(f);
-    ch.ncol = ncol_of(f);
-    ch.elem = elem_of(f);
-    ch.n = n;
-    if (ch.kind == 0 && (n < 6 || n % 2)) return b->fail(RT_E_INVAL, "domino tiling side must be even and >= 6");
-    if ((ch.kind == 1 || ch.kind == 2) && (n < 9 || n % 3))
-        return b->fail(RT_E_INVAL, "tiling side must be a multiple of 3 and >= 9");
-    if (ch.kind == 3 && (n < 8 || n % 2)) return b->fail(RT_E_INVAL, "triangle-dimer tiling side must be even and >= 8");
-    if (ch.kind == 0) {
-        ch.rows = n - 2, ch.cols = n / 2 - 2, ch.arows = n, ch.width = n / 2;
-    } else if (ch.kind == 3) {
-        ch.rows = n / 2, ch.cols = n / 2, ch.arows = n / 2, ch.width = n / 2;
-    } else {
-        ch.rows = n, ch.cols = n / 3, ch.arows = n, ch.width = n / 3;
-    }
-    ch.per_arr = ((size_t)ch.arows * ch.width * ch.elem + 255) & ~(size_t)255;
-    const double q = c->q == 0.0f ? 1.0 : (double)c->q;
-    if (!(q > 0.0 && q <= 1.0) || (ch.kind != 1 && q != 1.0))
-        return b->fail(RT_E_INVAL, "q must lie in (0, 1] (lozenges) or be 0");
-    if (ch.kind == 1) {
-        ch.thr[0] = below_threshold(0.4 * q);
-        ch.thr[1] = below_threshold(0.8);
-        ch.thr[2] = below_threshold(0.4);
-    }
-    ch.chain = c->chain;
-    ch.key = (uint64_t)c->key;
-    ch.start.assign(tiling, tiling + (size_t)n * n);
-    if (index) *index = (int64_t)b->chains.size();
-    b->fam[f].members.push_back((int)b->chains.size());
-    b->fam[f].planned = false;
-    b->chains.push_back(std::move(ch));
-    b->uploaded = false;
-    b->drop_graph();
-    for (int x = 0; x < kFamilies; ++x) b->fam[x].phases_sweeps = -1;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!b || !c || !tiling) return b ? b->fail(RT_E_INVAL, "null argument") : RT_E_INVAL;
+        if (b->sweeps_done > 0) return b->fail(RT_E_STATE, "chains are added before the first run");
+        const int f = family_of(c->model, c->kernel);
+        if (f < 0) return b->fail(RT_E_INVAL, "unsupported model / kernel in a batch");
+        Chain ch;
+        ch.fam = f;
+        ch.kind = kind_of(f);
+        ch.ncol = ncol_of(f);
+        ch.elem = elem_of(f);
+        ch.n = n;
+        if (ch.kind == 0 && (n < 6 || n % 2)) return b->fail(RT_E_INVAL, "domino tiling side must be even and >= 6");
+        if ((ch.kind == 1 || ch.kind == 2) && (n < 9 || n % 3))
+            return b->fail(RT_E_INVAL, "tiling side must be a multiple of 3 and >= 9");
+        if (ch.kind == 3 && (n < 8 || n % 2)) return b->fail(RT_E_INVAL, "triangle-dimer tiling side must be even and >= 8");
+        if (ch.kind == 0) {
+            ch.rows = n - 2, ch.cols = n / 2 - 2, ch.arows = n, ch.width = n / 2;
+        } else if (ch.kind == 3) {
+            ch.rows = n / 2, ch.cols = n / 2, ch.arows = n / 2, ch.width = n / 2;
+        } else {
+            ch.rows = n, ch.cols = n / 3, ch.arows = n, ch.width = n / 3;
+        }
+        ch.per_arr = ((size_t)ch.arows * ch.width * ch.elem + 255) & ~(size_t)255;
+        const double q = c->q == 0.0f ? 1.0 : (double)c->q;
+        if (!(q > 0.0 && q <= 1.0) || (ch.kind != 1 && q != 1.0))
+            return b->fail(RT_E_INVAL, "q must lie in (0, 1] (lozenges) or be 0");
+        if (ch.kind == 1) {
+            ch.thr[0] = below_threshold(0.4 * q);
+            ch.thr[1] = below_threshold(0.8);
+            ch.thr[2] = below_threshold(0.4);
+        }
+        ch.chain = c->chain;
+        ch.key = (uint64_t)c->key;
+        ch.start.assign(tiling, tiling + (size_t)n * n);
+        if (index) *index = (int64_t)b->chains.size();
+        b->fam[f].members.push_back((int)b->chains.size());
+        b->fam[f].planned = false;
+        b->chains.push_back(std::move(ch));
+        b->uploaded = false;
+        b->drop_graph();
+        for (int x = 0; x < kFamilies; ++x) b->fam[x].phases_sweeps = -1;
+        return RT_OK;
+    });
 }
 
 rt_status rt_batch_set_tuning(rt_batch* b, int32_t autotune, int32_t cluster, int32_t block) {
-    if (!b) return RT_E_INVAL;
-    if (cluster < 0 || cluster > 16 || block < 0 || block > 1024 || block % 32)
-        return b->fail(RT_E_INVAL, "cluster size must be 0..16, block a multiple of 32 up to 1024");
-    b->autotune = autotune ? 1 : 0;
-    b->force_cl = cluster;
-    b->force_block = block;
-    for (int f = 0; f < kFamilies; ++f) b->fam[f].planned = false;
-    b->drop_graph();
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!b) return RT_E_INVAL;
+        if (cluster < 0 || cluster > 16 || block < 0 || block > 1024 || block % 32)
+            return b->fail(RT_E_INVAL, "cluster size must be 0..16, block a multiple of 32 up to 1024");
+        b->autotune = autotune ? 1 : 0;
+        b->force_cl = cluster;
+        b->force_block = block;
+        for (int f = 0; f < kFamilies; ++f) b->fam[f].planned = false;
+        b->drop_graph();
+        return RT_OK;
+    });
 }
 
 rt_status rt_batch_set_sweeps_per_launch(rt_batch* b, int64_t sweeps) {
-    if (!b) return RT_E_INVAL;
-    if (sweeps < -1) return b->fail(RT_E_INVAL, "sweeps per launch must be >= -1");
-    if (sweeps > kMaxColourSteps / 32) return b->fail(RT_E_INVAL, "more than 2^35 sweeps per launch");
-    b->force_spl = sweeps;
-    for (int f = 0; f < kFamilies; ++f) b->fam[f].planned = false;
-    b->drop_graph();
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!b) return RT_E_INVAL;
+        if (sweeps < -1) return b->fail(RT_E_INVAL, "sweeps per launch must be >= -1");
+        if (sweeps > kMaxColourSteps / 32) return b->fail(RT_E_INVAL, "more than 2^35 sweeps per launch");
+        b->force_spl = sweeps;
+        for (int f = 0; f < kFamilies; ++f) b->fam[f].planned = false;
+        b->drop_graph();
+        return RT_OK;
+    });
 }
 
 rt_status rt_batch_run(rt_batch* b, int64_t sweeps) {
-    if (!b) return RT_E_INVAL;
-    if (sweeps < 0) return b->fail(RT_E_INVAL, "negative sweep count");
-    if (sweeps > kMaxColourSteps / 32) return b->fail(RT_E_INVAL, "more than 2^35 sweeps in one call");
-    if (b->chains.empty() || sweeps == 0) return RT_OK;
-    cudaSetDevice(b->device);
-    rt_status s = upload(b);
-    if (s != RT_OK) return s;
-    const auto w0 = std::chrono::steady_clock::now();
-    bool tuned = false;
-    for (int f = 0; f < kFamilies; ++f) {
-        if (b->fam[f].members.empty() || b->fam[f].planned) continue;
-        s = plan_family(b, f);
+    return guarded([&]() -> rt_status {
+        if (!b) return RT_E_INVAL;
+        if (sweeps < 0) return b->fail(RT_E_INVAL, "negative sweep count");
+        if (sweeps > kMaxColourSteps / 32) return b->fail(RT_E_INVAL, "more than 2^35 sweeps in one call");
+        if (b->chains.empty() || sweeps == 0) return RT_OK;
+        cudaSetDevice(b->device);
+        rt_status s = upload(b);
         if (s != RT_OK) return s;
-        tuned = true;
-        b->drop_graph();
-    }
-    if (tuned)
-        b->tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
-    for (int f = 0; f < kFamilies; ++f) {
-        FamilyState& F = b->fam[f];
-        if (F.members.empty()) continue;
-        const LaunchSplit ls = split_run(sweeps, F.plan.spl);
-        if (F.phases_sweeps != ls.per || (ls.rest && F.phases2_sweeps != ls.rest) || b->exec_sweeps != sweeps)
+        const auto w0 = std::chrono::steady_clock::now();
+        bool tuned = false;
+        for (int f = 0; f < kFamilies; ++f) {
+            if (b->fam[f].members.empty() || b->fam[f].planned) continue;
+            s = plan_family(b, f);
+            if (s != RT_OK) return s;
+            tuned = true;
             b->drop_graph();
-        s = stage_phases(b, f, ls.per);
-        if (s == RT_OK && ls.rest) s = stage_phases(b, f, ls.rest, true);
-        if (s != RT_OK) return s;
-    }
-    if (!b->exec) {
-        for (int f = 0; f < kFamilies; ++f)
-            if (!b->fam[f].members.empty())
-                cudaFuncSetAttribute((const void*)batch_fn(f), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)b->fam[f].plan.smem);
-        // One graph: fork to a stream per family, one launch each, join.  The
-        // family with the most work goes first at the highest priority, so its
-        // CTAs take the SMs and the smaller families fill the slots its last
-        // round leaves idle.
-        // Work of a family: the autotuner's time of its best plan when every
-        // family has one, else its lattice bytes per sweep.
-        int order[kFamilies], nf = 0;
-        double est[kFamilies] = {};
-        bool timed = true;
+        }
+        if (tuned)
+            b->tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
+        for (int f = 0; f < kFamilies; ++f) {
+            FamilyState& F = b->fam[f];
+            if (F.members.empty()) continue;
+            const LaunchSplit ls = split_run(sweeps, F.plan.spl);
+            if (F.phases_sweeps != ls.per || (ls.rest && F.phases2_sweeps != ls.rest) || b->exec_sweeps != sweeps)
+                b->drop_graph();
+            s = stage_phases(b, f, ls.per);
+            if (s == RT_OK && ls.rest) s = stage_phases(b, f, ls.rest, true);
+            if (s != RT_OK) return s;
+        }
+        if (!b->exec) {
+            for (int f = 0; f < kFamilies; ++f)
+                if (!b->fam[f].members.empty())
+                    cudaFuncSetAttribute((const void*)batch_fn(f), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)b->fam[f].plan.smem);
+            // One graph: fork to a stream per family, one launch each, join.  The
+            // family with the most work goes first at the highest priority, so its
+            // CTAs take the SMs and the smaller families fill the slots its last
+            // round leaves idle.
+            // Work of a family: the autotuner's time of its best plan when every
+            // family has one, else its lattice bytes per sweep.
+            int order[kFamilies], nf = 0;
+            double est[kFamilies] = {};
+            bool timed = true;
+            for (int f = 0; f < kFamilies; ++f) {
+                if (b->fam[f].members.empty()) continue;
+                timed = timed && b->fam[f].work > 0;
+                for (int i : b->fam[f].members) {
+                    const Chain& c = b->chains[i];
+                    est[f] += (double)steps_per_sweep(c.kind) * c.ncol * c.arows * c.width * c.elem;
+                }
+                order[nf++] = f;
+            }
+            if (timed)
+                for (int k = 0; k < nf; ++k) est[order[k]] = b->fam[order[k]].work;
+            std::sort(order, order + nf, [&](int x, int y) { return est[x] > est[y]; });
+            int prio_low = 0, prio_high = 0;
+            cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            cudaEventRecord(b->fork, b->stream);
+            rt_status ls = RT_OK;
+            for (int k = 0; k < nf && ls == RT_OK; ++k) {
+                const int f = order[k];
+                const LaunchSplit sp = split_run(sweeps, b->fam[f].plan.spl);
+                const int64_t sps = steps_per_sweep(kind_of(f));
+                cudaStreamWaitEvent(b->fam_stream[f], b->fork, 0);
+                for (int64_t l = 0; l < sp.full + (sp.rest ? 1 : 0) && ls == RT_OK; ++l)
+                    ls = launch_family(b, f, b->fam[f].plan, b->fam[f].recs.p, b->fam_stream[f],
+                                       k == 0 ? prio_high : prio_low, l * sp.per * sps, l == sp.full);
+                cudaEventRecord(b->join[f], b->fam_stream[f]);
+                cudaStreamWaitEvent(b->stream, b->join[f], 0);
+            }
+            e = cudaStreamEndCapture(b->stream, &g);
+            if (ls != RT_OK) {
+                if (g) cudaGraphDestroy(g);
+                return ls;
+            }
+            if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&b->exec, g, cudaGraphInstantiateFlagUseNodePriority);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                b->exec = nullptr;
+                return b->fail(RT_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            }
+            b->exec_sweeps = sweeps;
+        }
+        // Philox step counters continue where the previous run stopped, so two
+        // runs of s1 and s2 sweeps equal one run of s1 + s2.
         for (int f = 0; f < kFamilies; ++f) {
             if (b->fam[f].members.empty()) continue;
-            timed = timed && b->fam[f].work > 0;
-            for (int i : b->fam[f].members) {
-                const Chain& c = b->chains[i];
-                est[f] += (double)steps_per_sweep(c.kind) * c.ncol * c.arows * c.width * c.elem;
-            }
-            order[nf++] = f;
+            b->h_step0[f] = b->sweeps_done * steps_per_sweep(kind_of(f));
+            cudaMemcpyAsync(b->fam[f].step0.p, &b->h_step0[f], sizeof(int64_t), cudaMemcpyHostToDevice, b->stream);
         }
-        if (timed)
-            for (int k = 0; k < nf; ++k) est[order[k]] = b->fam[order[k]].work;
-        std::sort(order, order + nf, [&](int x, int y) { return est[x] > est[y]; });
-        int prio_low = 0, prio_high = 0;
-        cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
-        cudaGraph_t g = nullptr;
-        cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-        cudaEventRecord(b->fork, b->stream);
-        rt_status ls = RT_OK;
-        for (int k = 0; k < nf && ls == RT_OK; ++k) {
-            const int f = order[k];
-            const LaunchSplit sp = split_run(sweeps, b->fam[f].plan.spl);
-            const int64_t sps = steps_per_sweep(kind_of(f));
-            cudaStreamWaitEvent(b->fam_stream[f], b->fork, 0);
-            for (int64_t l = 0; l < sp.full + (sp.rest ? 1 : 0) && ls == RT_OK; ++l)
-                ls = launch_family(b, f, b->fam[f].plan, b->fam[f].recs.p, b->fam_stream[f],
-                                   k == 0 ? prio_high : prio_low, l * sp.per * sps, l == sp.full);
-            cudaEventRecord(b->join[f], b->fam_stream[f]);
-            cudaStreamWaitEvent(b->stream, b->join[f], 0);
+        cudaEventRecord(b->t0, b->stream);
+        cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
+        if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+        cudaEventRecord(b->t1, b->stream);
+        e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("batch run: ") + cudaGetErrorString(e));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, b->t0, b->t1);
+        b->run_ms = ms;
+        b->sweeps_done += sweeps;
+        int64_t att = 0, bytes = 0;
+        for (const Chain& c : b->chains) {
+            const int64_t steps = sweeps * steps_per_sweep(c.kind);
+            att += steps * (int64_t)c.rows * c.cols;
+            bytes += steps * 2 * (int64_t)c.ncol * c.arows * c.width * c.elem;
         }
-        e = cudaStreamEndCapture(b->stream, &g);
-        if (ls != RT_OK) {
-            if (g) cudaGraphDestroy(g);
-            return ls;
-        }
-        if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&b->exec, g, cudaGraphInstantiateFlagUseNodePriority);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) {
-            b->exec = nullptr;
-            return b->fail(RT_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-        }
-        b->exec_sweeps = sweeps;
-    }
-    // Philox step counters continue where the previous run stopped, so two
-    // runs of s1 and s2 sweeps equal one run of s1 + s2.
-    for (int f = 0; f < kFamilies; ++f) {
-        if (b->fam[f].members.empty()) continue;
-        b->h_step0[f] = b->sweeps_done * steps_per_sweep(kind_of(f));
-        cudaMemcpyAsync(b->fam[f].step0.p, &b->h_step0[f], sizeof(int64_t), cudaMemcpyHostToDevice, b->stream);
-    }
-    cudaEventRecord(b->t0, b->stream);
-    cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
-    if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
-    cudaEventRecord(b->t1, b->stream);
-    e = cudaStreamSynchronize(b->stream);
-    if (e != cudaSuccess) return b->fail(RT_E_CUDA, std::string("batch run: ") + cudaGetErrorString(e));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, b->t0, b->t1);
-    b->run_ms = ms;
-    b->sweeps_done += sweeps;
-    int64_t att = 0, bytes = 0;
-    for (const Chain& c : b->chains) {
-        const int64_t steps = sweeps * steps_per_sweep(c.kind);
-        att += steps * (int64_t)c.rows * c.cols;
-        bytes += steps * 2 * (int64_t)c.ncol * c.arows * c.width * c.elem;
-    }
-    b->last_attempts = att;
-    b->last_bytes = bytes;
-    return RT_OK;
+        b->last_attempts = att;
+        b->last_bytes = bytes;
+        return RT_OK;
+    });
 }
 
 rt_status rt_batch_download(rt_batch* b, int64_t index, int32_t* tiling) {
-    if (!b || !tiling) return b ? b->fail(RT_E_INVAL, "null tiling") : RT_E_INVAL;
-    if (index < 0 || index >= (int64_t)b->chains.size()) return b->fail(RT_E_INVAL, "no chain with that index");
-    cudaSetDevice(b->device);
-    rt_status s = upload(b);
-    if (s != RT_OK) return s;
-    const Chain& c = b->chains[(size_t)index];
-    FamilyState& F = b->fam[c.fam];
-    char* base = static_cast<char*>(F.data.p) + c.off;
-    void* arr[8] = {};
-    for (int a = 0; a < c.ncol; ++a) arr[a] = base + a * c.per_arr;
-    Dev tmp;
-    const size_t tb = (size_t)c.n * c.n * 4;
-    if (!tmp.reserve(tb)) return b->fail(RT_E_NOMEM, "staging buffer");
-    cudaMemcpyAsync(tmp.p, c.start.data(), tb, cudaMemcpyHostToDevice, b->stream);
-    void* merge_arr[3] = {arr[0], arr[1], arr[2]};
-    std::string e;
-    if (launch_split(true, c.elem, c.kind, c.ncol, c.n, static_cast<int32_t*>(tmp.p), merge_arr, b->stream, &e) != RT_OK)
-        return b->fail(RT_E_CUDA, e);
-    cudaError_t ce = cudaMemcpyAsync(tiling, tmp.p, tb, cudaMemcpyDeviceToHost, b->stream);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(b->stream);
-    if (ce != cudaSuccess) return b->fail(RT_E_CUDA, std::string("batch download: ") + cudaGetErrorString(ce));
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!b || !tiling) return b ? b->fail(RT_E_INVAL, "null tiling") : RT_E_INVAL;
+        if (index < 0 || index >= (int64_t)b->chains.size()) return b->fail(RT_E_INVAL, "no chain with that index");
+        cudaSetDevice(b->device);
+        rt_status s = upload(b);
+        if (s != RT_OK) return s;
+        const Chain& c = b->chains[(size_t)index];
+        FamilyState& F = b->fam[c.fam];
+        char* base = static_cast<char*>(F.data.p) + c.off;
+        void* arr[8] = {};
+        for (int a = 0; a < c.ncol; ++a) arr[a] = base + a * c.per_arr;
+        Dev tmp;
+        const size_t tb = (size_t)c.n * c.n * 4;
+        if (!tmp.reserve(tb)) return b->fail(RT_E_NOMEM, "staging buffer");
+        cudaMemcpyAsync(tmp.p, c.start.data(), tb, cudaMemcpyHostToDevice, b->stream);
+        void* merge_arr[3] = {arr[0], arr[1], arr[2]};
+        std::string e;
+        if (launch_split(true, c.elem, c.kind, c.ncol, c.n, static_cast<int32_t*>(tmp.p), merge_arr, b->stream, &e) != RT_OK)
+            return b->fail(RT_E_CUDA, e);
+        cudaError_t ce = cudaMemcpyAsync(tiling, tmp.p, tb, cudaMemcpyDeviceToHost, b->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(b->stream);
+        if (ce != cudaSuccess) return b->fail(RT_E_CUDA, std::string("batch download: ") + cudaGetErrorString(ce));
+        return RT_OK;
+    });
 }
 
 rt_status rt_batch_device_tiling(rt_batch* b, int64_t index, int32_t* d_tiling, void* stream) {
-    if (!b || !d_tiling) return b ? b->fail(RT_E_INVAL, "null tiling") : RT_E_INVAL;
-    if (index < 0 || index >= (int64_t)b->chains.size()) return b->fail(RT_E_INVAL, "no chain with that index");
-    cudaSetDevice(b->device);
-    rt_status s = upload(b);
-    if (s != RT_OK) return s;
-    const Chain& c = b->chains[(size_t)index];
-    if (c.kind == 3) return b->fail(RT_E_INVAL, "device tilings of triangle-dimer chains are not merged on the device");
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    // The merge writes every cell of the colour models' tilings.
-    char* base = static_cast<char*>(b->fam[c.fam].data.p) + c.off;
-    void* arr[3] = {base, base + c.per_arr, c.ncol > 2 ? base + 2 * c.per_arr : nullptr};
-    std::string e;
-    if (launch_split(true, c.elem, c.kind, c.ncol, c.n, d_tiling, arr, st, &e) != RT_OK) return b->fail(RT_E_CUDA, e);
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!b || !d_tiling) return b ? b->fail(RT_E_INVAL, "null tiling") : RT_E_INVAL;
+        if (index < 0 || index >= (int64_t)b->chains.size()) return b->fail(RT_E_INVAL, "no chain with that index");
+        cudaSetDevice(b->device);
+        rt_status s = upload(b);
+        if (s != RT_OK) return s;
+        const Chain& c = b->chains[(size_t)index];
+        if (c.kind == 3) return b->fail(RT_E_INVAL, "device tilings of triangle-dimer chains are not merged on the device");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        // The merge writes every cell of the colour models' tilings.
+        char* base = static_cast<char*>(b->fam[c.fam].data.p) + c.off;
+        void* arr[3] = {base, base + c.per_arr, c.ncol > 2 ? base + 2 * c.per_arr : nullptr};
+        std::string e;
+        if (launch_split(true, c.elem, c.kind, c.ncol, c.n, d_tiling, arr, st, &e) != RT_OK) return b->fail(RT_E_CUDA, e);
+        return RT_OK;
+    });
 }
 
 rt_status rt_batch_get_info(rt_batch* b, rt_batch_info* info) {
-    if (!b || !info) return RT_E_INVAL;
-    std::memset(info, 0, sizeof *info);
-    info->chains = (int32_t)b->chains.size();
-    for (int f = 0; f < kFamilies; ++f) {
-        if (b->fam[f].members.empty() || !b->fam[f].planned) continue;
-        info->cluster[f] = b->fam[f].plan.cl;
-        info->block[f] = b->fam[f].plan.block;
-        info->clusters[f] = b->fam[f].plan.clusters;
-        info->sweeps_per_launch[f] = b->fam[f].plan.spl;
-    }
-    info->tune_ms = b->tune_ms;
-    info->run_ms = b->run_ms;
-    info->attempts = b->last_attempts;
-    info->algorithmic_bytes = b->last_bytes;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!b || !info) return RT_E_INVAL;
+        std::memset(info, 0, sizeof *info);
+        info->chains = (int32_t)b->chains.size();
+        for (int f = 0; f < kFamilies; ++f) {
+            if (b->fam[f].members.empty() || !b->fam[f].planned) continue;
+            info->cluster[f] = b->fam[f].plan.cl;
+            info->block[f] = b->fam[f].plan.block;
+            info->clusters[f] = b->fam[f].plan.clusters;
+            info->sweeps_per_launch[f] = b->fam[f].plan.spl;
+        }
+        info->tune_ms = b->tune_ms;
+        info->run_ms = b->run_ms;
+        info->attempts = b->last_attempts;
+        info->algorithmic_bytes = b->last_bytes;
+        return RT_OK;
+    });
 }
 
 }  // extern "C"

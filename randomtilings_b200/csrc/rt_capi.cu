@@ -19,8 +19,11 @@
 #include <vector>
 
 #include "rt_internal.h"
+#include "rt_guard.h"
 #include "rt_models.cuh"
 #include "rt_tridimer.cuh"
+
+using rtb::guarded;
 
 using namespace rtb;
 
@@ -253,110 +256,114 @@ void rt_config_default(rt_config* cfg, int32_t model) {
 }
 
 rt_status rt_create(const rt_config* cfg, rt_tiler** out) {
-    if (!cfg || !out) {
-        g_create_error = "null argument";
-        return RT_E_INVAL;
-    }
-    *out = nullptr;
-    int family = -1, ncol = 0, kind = 0, elem = 1;
-    switch (cfg->model) {
-        case RT_DOMINO:
-            if (cfg->kernel != RT_KERNEL_DEFAULT && cfg->kernel != RT_KERNEL_CFTP) break;
-            family = cfg->kernel == RT_KERNEL_CFTP ? FAM_DOMINO_HB : FAM_DOMINO;
-            ncol = 2, kind = 0, elem = 1;
-            break;
-        case RT_LOZENGE:
-            if (cfg->kernel == RT_KERNEL_DEFAULT) family = FAM_LOZENGE8, elem = 1;
-            else if (cfg->kernel == RT_KERNEL_QWEIGHT) family = FAM_QLOZENGE8, elem = 1;
-            ncol = 3, kind = 1;
-            break;
-        case RT_RECTTRI:
-            if (cfg->kernel != RT_KERNEL_DEFAULT) break;
-            family = FAM_RECTTRI, ncol = 3, kind = 2, elem = 4;
-            break;
-        case RT_TRIDIMER:
-            if (cfg->kernel != RT_KERNEL_DEFAULT) break;
-            family = FAM_TRIDIMER, ncol = 8, kind = 3, elem = 4;
-            break;
-        default:
-            break;
-    }
-    if (family < 0) {
-        g_create_error = "unsupported model/kernel combination";
-        return RT_E_INVAL;
-    }
-    if (cfg->rng != RT_RNG_TINYMT && cfg->rng != RT_RNG_PHILOX && cfg->rng != RT_RNG_PLANES) {
-        g_create_error = "unknown rng mode";
-        return RT_E_INVAL;
-    }
-    if (cfg->rng == RT_RNG_PLANES && !word_family(family)) {
-        g_create_error = "bit-plane mode exists for dominoes and uniform lozenges";
-        return RT_E_INVAL;
-    }
-    if (family == FAM_QLOZENGE8 && (!(cfg->q >= 0.0) || !std::isfinite(cfg->q))) {
-        g_create_error = "q must be a finite non-negative number";
-        return RT_E_INVAL;
-    }
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) {
-        g_create_error = "no CUDA device with that ordinal";
-        return RT_E_NODEVICE;
-    }
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || prop.major != 10) {
-        g_create_error = "device is not sm_100 (this library carries sm_100a code only)";
-        return RT_E_NODEVICE;
-    }
-    if (!prop.cooperativeLaunch) {
-        g_create_error = "device does not support cooperative launches";
-        return RT_E_NODEVICE;
-    }
-    cudaSetDevice(cfg->device);
-    rt_tiler* h = new rt_tiler();
-    h->cfg = *cfg;
-    h->family = family;
-    h->ncol = ncol;
-    h->kind = kind;
-    h->elem = elem;
-    if (cfg->stream) {
-        h->stream = static_cast<cudaStream_t>(cfg->stream);
-    } else {
-        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    return guarded([&]() -> rt_status {
+        if (!cfg || !out) {
+            g_create_error = "null argument";
+            return RT_E_INVAL;
+        }
+        *out = nullptr;
+        int family = -1, ncol = 0, kind = 0, elem = 1;
+        switch (cfg->model) {
+            case RT_DOMINO:
+                if (cfg->kernel != RT_KERNEL_DEFAULT && cfg->kernel != RT_KERNEL_CFTP) break;
+                family = cfg->kernel == RT_KERNEL_CFTP ? FAM_DOMINO_HB : FAM_DOMINO;
+                ncol = 2, kind = 0, elem = 1;
+                break;
+            case RT_LOZENGE:
+                if (cfg->kernel == RT_KERNEL_DEFAULT) family = FAM_LOZENGE8, elem = 1;
+                else if (cfg->kernel == RT_KERNEL_QWEIGHT) family = FAM_QLOZENGE8, elem = 1;
+                ncol = 3, kind = 1;
+                break;
+            case RT_RECTTRI:
+                if (cfg->kernel != RT_KERNEL_DEFAULT) break;
+                family = FAM_RECTTRI, ncol = 3, kind = 2, elem = 4;
+                break;
+            case RT_TRIDIMER:
+                if (cfg->kernel != RT_KERNEL_DEFAULT) break;
+                family = FAM_TRIDIMER, ncol = 8, kind = 3, elem = 4;
+                break;
+            default:
+                break;
+        }
+        if (family < 0) {
+            g_create_error = "unsupported model/kernel combination";
+            return RT_E_INVAL;
+        }
+        if (cfg->rng != RT_RNG_TINYMT && cfg->rng != RT_RNG_PHILOX && cfg->rng != RT_RNG_PLANES) {
+            g_create_error = "unknown rng mode";
+            return RT_E_INVAL;
+        }
+        if (cfg->rng == RT_RNG_PLANES && !word_family(family)) {
+            g_create_error = "bit-plane mode exists for dominoes and uniform lozenges";
+            return RT_E_INVAL;
+        }
+        if (family == FAM_QLOZENGE8 && (!(cfg->q >= 0.0) || !std::isfinite(cfg->q))) {
+            g_create_error = "q must be a finite non-negative number";
+            return RT_E_INVAL;
+        }
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) {
+            g_create_error = "no CUDA device with that ordinal";
+            return RT_E_NODEVICE;
+        }
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || prop.major != 10) {
+            g_create_error = "device is not sm_100 (this library carries sm_100a code only)";
+            return RT_E_NODEVICE;
+        }
+        if (!prop.cooperativeLaunch) {
+            g_create_error = "device does not support cooperative launches";
+            return RT_E_NODEVICE;
+        }
+        cudaSetDevice(cfg->device);
+        rt_tiler* h = new rt_tiler();
+        h->cfg = *cfg;
+        h->family = family;
+        h->ncol = ncol;
+        h->kind = kind;
+        h->elem = elem;
+        if (cfg->stream) {
+            h->stream = static_cast<cudaStream_t>(cfg->stream);
+        } else {
+            if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+                delete h;
+                g_create_error = "cudaStreamCreate failed";
+                return RT_E_CUDA;
+            }
+            h->own_stream = true;
+        }
+        if (cudaEventCreateWithFlags(&h->ev_staged, cudaEventDisableTiming) != cudaSuccess) {
+            if (h->own_stream) cudaStreamDestroy(h->stream);
             delete h;
-            g_create_error = "cudaStreamCreate failed";
+            g_create_error = "cudaEventCreate failed";
             return RT_E_CUDA;
         }
-        h->own_stream = true;
-    }
-    if (cudaEventCreateWithFlags(&h->ev_staged, cudaEventDisableTiming) != cudaSuccess) {
-        if (h->own_stream) cudaStreamDestroy(h->stream);
-        delete h;
-        g_create_error = "cudaEventCreate failed";
-        return RT_E_CUDA;
-    }
-    if (const char* kc = std::getenv("RT_WALK_KERNEL")) {
-        if (std::strcmp(kc, "generic") == 0) h->kernel_choice = 1;
-        if (std::strcmp(kc, "word") == 0) h->kernel_choice = 2;
-    }
-    if (const char* ct = std::getenv("RT_WALK_CTAS")) h->ctas_hint = std::max(0, std::atoi(ct));
-    if (const char* dp = std::getenv("RT_PLANE_DEPTH")) h->depth_hint = std::max(0, std::atoi(dp));
-    if (const char* dp = std::getenv("RT_TEST_DROP_PUBLISH")) h->drop_phase = std::atoll(dp);
-    if (const char* t = std::getenv("RT_WAIT_TIMEOUT_MS")) {
-        const long ms = std::atol(t);
-        if (ms > 0) h->timeout_ns = (uint64_t)ms * 1000000ull;
-    }
-    *out = h;
-    return RT_OK;
+        if (const char* kc = std::getenv("RT_WALK_KERNEL")) {
+            if (std::strcmp(kc, "generic") == 0) h->kernel_choice = 1;
+            if (std::strcmp(kc, "word") == 0) h->kernel_choice = 2;
+        }
+        if (const char* ct = std::getenv("RT_WALK_CTAS")) h->ctas_hint = std::max(0, std::atoi(ct));
+        if (const char* dp = std::getenv("RT_PLANE_DEPTH")) h->depth_hint = std::max(0, std::atoi(dp));
+        if (const char* dp = std::getenv("RT_TEST_DROP_PUBLISH")) h->drop_phase = std::atoll(dp);
+        if (const char* t = std::getenv("RT_WAIT_TIMEOUT_MS")) {
+            const long ms = std::atol(t);
+            if (ms > 0) h->timeout_ns = (uint64_t)ms * 1000000ull;
+        }
+        *out = h;
+        return RT_OK;
+    });
 }
 
 rt_status rt_destroy(rt_tiler* h) {
-    if (!h) return RT_E_INVAL;
-    cudaSetDevice(h->cfg.device);
-    cudaStreamSynchronize(h->stream);
-    if (h->ev_staged) cudaEventDestroy(h->ev_staged);
-    if (h->own_stream) cudaStreamDestroy(h->stream);
-    delete h;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        cudaSetDevice(h->cfg.device);
+        cudaStreamSynchronize(h->stream);
+        if (h->ev_staged) cudaEventDestroy(h->ev_staged);
+        if (h->own_stream) cudaStreamDestroy(h->stream);
+        delete h;
+        return RT_OK;
+    });
 }
 
 const char* rt_last_error(rt_tiler* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
@@ -364,88 +371,96 @@ const char* rt_last_error(rt_tiler* h) { return h ? h->err.c_str() : g_create_er
 void* rt_stream(rt_tiler* h) { return h ? static_cast<void*>(h->stream) : nullptr; }
 
 rt_status rt_set_domino_weights(rt_tiler* h, int32_t period, const double* wh, const double* wv) {
-    if (!h) return RT_E_INVAL;
-    if (h->family != FAM_DOMINO_HB) return h->fail(RT_E_INVAL, "weights need the domino heat-bath kernel (RT_KERNEL_CFTP)");
-    if (h->cfg.rng == RT_RNG_PLANES) return h->fail(RT_E_INVAL, "the bit-plane mode draws one bit per site: no weights");
-    if (period == 0) {
-        h->wper = 0;
-        return RT_OK;
-    }
-    if ((period != 1 && period != 2 && period != 4) || !wh || !wv)
-        return h->fail(RT_E_INVAL, "weight period must be 1, 2 or 4, with two period x period tables");
-    const int P = period;
-    for (int k = 0; k < P * P; ++k)
-        if (!(wh[k] > 0 && wv[k] > 0) || !std::isfinite(wh[k]) || !std::isfinite(wv[k]))
-            return h->fail(RT_E_INVAL, "domino weights must be finite and > 0");
-    auto W = [&](const double* w, int r, int c) { return w[(((r % P) + P) % P) * P + (((c % P) + P) % P)]; };
-    for (int i = 0; i < P; ++i)
-        for (int j = 0; j < P; ++j) {
-            // vertex class (i, j): the squares (i-1, j-1), (i-1, j), (i, j-1) around it
-            const double w3 = W(wh, i - 1, j - 1) * W(wh, i, j - 1);
-            const double w12 = W(wv, i - 1, j - 1) * W(wv, i - 1, j);
-            h->wthr[i * P + j] = below_threshold(w12 / (w3 + w12));
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        if (h->family != FAM_DOMINO_HB) return h->fail(RT_E_INVAL, "weights need the domino heat-bath kernel (RT_KERNEL_CFTP)");
+        if (h->cfg.rng == RT_RNG_PLANES) return h->fail(RT_E_INVAL, "the bit-plane mode draws one bit per site: no weights");
+        if (period == 0) {
+            h->wper = 0;
+            return RT_OK;
         }
-    h->wper = P;
-    return RT_OK;
+        if ((period != 1 && period != 2 && period != 4) || !wh || !wv)
+            return h->fail(RT_E_INVAL, "weight period must be 1, 2 or 4, with two period x period tables");
+        const int P = period;
+        for (int k = 0; k < P * P; ++k)
+            if (!(wh[k] > 0 && wv[k] > 0) || !std::isfinite(wh[k]) || !std::isfinite(wv[k]))
+                return h->fail(RT_E_INVAL, "domino weights must be finite and > 0");
+        auto W = [&](const double* w, int r, int c) { return w[(((r % P) + P) % P) * P + (((c % P) + P) % P)]; };
+        for (int i = 0; i < P; ++i)
+            for (int j = 0; j < P; ++j) {
+                // vertex class (i, j): the squares (i-1, j-1), (i-1, j), (i, j-1) around it
+                const double w3 = W(wh, i - 1, j - 1) * W(wh, i, j - 1);
+                const double w12 = W(wv, i - 1, j - 1) * W(wv, i - 1, j);
+                h->wthr[i * P + j] = below_threshold(w12 / (w3 + w12));
+            }
+        h->wper = P;
+        return RT_OK;
+    });
 }
 
 rt_status rt_set_lozenge_weights(rt_tiler* h, int32_t period, const double* w0, const double* w1, const double* w2) {
-    if (!h) return RT_E_INVAL;
-    if (h->family != FAM_LOZENGE8) return h->fail(RT_E_INVAL, "weights need the uniform lozenge kernel (char storage)");
-    if (h->cfg.rng == RT_RNG_PLANES) return h->fail(RT_E_INVAL, "the bit-plane mode draws one bit per site: no weights");
-    if (period == 0) {
-        h->wper = 0;
-        return RT_OK;
-    }
-    if ((period != 1 && period != 2 && period != 4) || !w0 || !w1 || !w2)
-        return h->fail(RT_E_INVAL, "weight period must be 1, 2 or 4, with three period x period tables");
-    const int P = period;
-    for (int k = 0; k < P * P; ++k)
-        for (const double* w : {w0, w1, w2})
-            if (!(w[k] > 0) || !std::isfinite(w[k])) return h->fail(RT_E_INVAL, "lozenge weights must be finite and > 0");
-    auto W = [&](const double* w, int r, int c) { return w[(((r % P) + P) % P) * P + (((c % P) + P) % P)]; };
-    for (int i = 0; i < P; ++i)
-        for (int j = 0; j < P; ++j) {
-            const double w25 = W(w2, i, j) * W(w0, i, j) * W(w1, i + 1, j - 1);
-            const double w38 = W(w1, i, j) * W(w0, i, j - 1) * W(w2, i + 1, j);
-            h->wthr[i * P + j] = below_threshold(0.8 * (w38 / (w25 + w38)));
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        if (h->family != FAM_LOZENGE8) return h->fail(RT_E_INVAL, "weights need the uniform lozenge kernel (char storage)");
+        if (h->cfg.rng == RT_RNG_PLANES) return h->fail(RT_E_INVAL, "the bit-plane mode draws one bit per site: no weights");
+        if (period == 0) {
+            h->wper = 0;
+            return RT_OK;
         }
-    h->wper = P;
-    return RT_OK;
+        if ((period != 1 && period != 2 && period != 4) || !w0 || !w1 || !w2)
+            return h->fail(RT_E_INVAL, "weight period must be 1, 2 or 4, with three period x period tables");
+        const int P = period;
+        for (int k = 0; k < P * P; ++k)
+            for (const double* w : {w0, w1, w2})
+                if (!(w[k] > 0) || !std::isfinite(w[k])) return h->fail(RT_E_INVAL, "lozenge weights must be finite and > 0");
+        auto W = [&](const double* w, int r, int c) { return w[(((r % P) + P) % P) * P + (((c % P) + P) % P)]; };
+        for (int i = 0; i < P; ++i)
+            for (int j = 0; j < P; ++j) {
+                const double w25 = W(w2, i, j) * W(w0, i, j) * W(w1, i + 1, j - 1);
+                const double w38 = W(w1, i, j) * W(w0, i, j - 1) * W(w2, i + 1, j);
+                h->wthr[i * P + j] = below_threshold(0.8 * (w38 / (w25 + w38)));
+            }
+        h->wper = P;
+        return RT_OK;
+    });
 }
 
 rt_status rt_set_rng_params(rt_tiler* h, const uint32_t* table, int64_t n) {
-    if (!h || (!table && n > 0) || n < 0) return h ? h->fail(RT_E_INVAL, "bad parameter table") : RT_E_INVAL;
-    h->table.assign(table, table + 3 * n);
-    h->table_dirty = true;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!h || (!table && n > 0) || n < 0) return h ? h->fail(RT_E_INVAL, "bad parameter table") : RT_E_INVAL;
+        h->table.assign(table, table + 3 * n);
+        h->table_dirty = true;
+        return RT_OK;
+    });
 }
 
 // The layout src/TinyMT/file_reader.cpp:51-70,139-166 reads: lines starting
 // with '#' are skipped; mat1, mat2 and tmat are the hexadecimal fields after
 // the 3rd, 4th and 5th comma.
 rt_status rt_load_rng_params(rt_tiler* h, const char* path, int64_t n) {
-    if (!h || !path || n < 0) return h ? h->fail(RT_E_INVAL, "bad arguments") : RT_E_INVAL;
-    std::ifstream in(path);
-    if (!in) return h->fail(RT_E_PARAMS, std::string("cannot open parameter file ") + path);
-    std::vector<uint32_t> t;
-    t.reserve((size_t)(3 * n));
-    std::string line;
-    int64_t got = 0;
-    while (got < n && std::getline(in, line)) {
-        if (!line.empty() && line[0] == '#') continue;
-        size_t pos[5];
-        int commas = 0;
-        for (size_t i = 0; i < line.size() && commas < 5; ++i)
-            if (line[i] == ',') pos[commas++] = i;
-        if (commas < 5) return h->fail(RT_E_PARAMS, "parameter line " + std::to_string(got) + ": comma not found");
-        for (int f = 2; f < 5; ++f) t.push_back((uint32_t)std::strtoul(line.c_str() + pos[f] + 1, nullptr, 16));
-        ++got;
-    }
-    if (got < n) return h->fail(RT_E_PARAMS, "parameter file has " + std::to_string(got) + " entries, need " + std::to_string(n));
-    h->table.swap(t);
-    h->table_dirty = true;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!h || !path || n < 0) return h ? h->fail(RT_E_INVAL, "bad arguments") : RT_E_INVAL;
+        std::ifstream in(path);
+        if (!in) return h->fail(RT_E_PARAMS, std::string("cannot open parameter file ") + path);
+        std::vector<uint32_t> t;
+        t.reserve((size_t)(3 * n));
+        std::string line;
+        int64_t got = 0;
+        while (got < n && std::getline(in, line)) {
+            if (!line.empty() && line[0] == '#') continue;
+            size_t pos[5];
+            int commas = 0;
+            for (size_t i = 0; i < line.size() && commas < 5; ++i)
+                if (line[i] == ',') pos[commas++] = i;
+            if (commas < 5) return h->fail(RT_E_PARAMS, "parameter line " + std::to_string(got) + ": comma not found");
+            for (int f = 2; f < 5; ++f) t.push_back((uint32_t)std::strtoul(line.c_str() + pos[f] + 1, nullptr, 16));
+            ++got;
+        }
+        if (got < n) return h->fail(RT_E_PARAMS, "parameter file has " + std::to_string(got) + " entries, need " + std::to_string(n));
+        h->table.swap(t);
+        h->table_dirty = true;
+        return RT_OK;
+    });
 }
 
 static rt_status check_size(rt_tiler* h, int n) {
@@ -483,87 +498,95 @@ static void array_shape(const rt_tiler* h, int n, int* arows, int* width) {
 }
 
 rt_status rt_upload(rt_tiler* h, const int32_t* tiling, int32_t n) {
-    if (!h || !tiling) return h ? h->fail(RT_E_INVAL, "null tiling") : RT_E_INVAL;
-    rt_status s = check_size(h, n);
-    if (s != RT_OK) return s;
-    cudaSetDevice(h->cfg.device);
-    int arows, width;
-    array_shape(h, n, &arows, &width);
-    const size_t per_arr = (size_t)arows * (size_t)width * (size_t)h->elem;
-    const size_t per_arr_al = (per_arr + 255) & ~(size_t)255;
-    h->per_arr_al = per_arr_al;
-    if (!h->d_arr_block.reserve(per_arr_al * h->ncol * 2)) return h->fail(RT_E_NOMEM, "cudaMalloc lattice");
-    if (!h->d_tiling.reserve((size_t)n * n * 4)) return h->fail(RT_E_NOMEM, "cudaMalloc tiling");
-    for (int l = 0; l < 2; ++l)
-        for (int c = 0; c < 8; ++c)
-            h->d_arr[l][c] = c < h->ncol ? static_cast<char*>(h->d_arr_block.p) + (l * h->ncol + c) * per_arr_al : nullptr;
-    // Alignment padding between the colour arrays is compared by the CFTP
-    // coalescence test, so it must hold the same bytes in both lattices.
-    cudaError_t e = cudaMemsetAsync(h->d_arr_block.p, 0, per_arr_al * h->ncol * 2, h->stream);
-    if (e != cudaSuccess) return h->cuda_fail(e, "memset lattice");
-    e = cudaMemcpyAsync(h->d_tiling.p, tiling, (size_t)n * n * 4, cudaMemcpyHostToDevice, h->stream);
-    if (e != cudaSuccess) return h->cuda_fail(e, "upload");
-    if (h->kind == 3) {
-        // The eight triangle-dimer arrays are derived on the host
-        // (TriangleDimerTiler.cpp:90-133) and copied up as they are.
-        std::vector<int32_t> arrays((size_t)8 * arows * width);
-        td_split_host(tiling, n, arrays.data());
-        for (int c = 0; c < 8 && e == cudaSuccess; ++c)
-            e = cudaMemcpy(h->d_arr[0][c], arrays.data() + (size_t)c * arows * width, per_arr, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) return h->cuda_fail(e, "upload of the triangle-dimer arrays");
-    } else {
-        s = launch_split(false, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0],
-                         h->stream, &h->err);
+    return guarded([&]() -> rt_status {
+        if (!h || !tiling) return h ? h->fail(RT_E_INVAL, "null tiling") : RT_E_INVAL;
+        rt_status s = check_size(h, n);
         if (s != RT_OK) return s;
-    }
-    if (!h->d_err.reserve(sizeof(int)) || !h->h_err.reserve(sizeof(int))) return h->fail(RT_E_NOMEM, "error word");
-    e = cudaMemsetAsync(h->d_err.p, 0, sizeof(int), h->stream);
-    if (e != cudaSuccess) return h->cuda_fail(e, "memset");
-    h->n = n;
-    h->arows = arows;
-    h->width = width;
-    grid_of(h, n, &h->rows, &h->cols);
-    h->uploaded = true;
-    return RT_OK;
+        cudaSetDevice(h->cfg.device);
+        int arows, width;
+        array_shape(h, n, &arows, &width);
+        const size_t per_arr = (size_t)arows * (size_t)width * (size_t)h->elem;
+        const size_t per_arr_al = (per_arr + 255) & ~(size_t)255;
+        h->per_arr_al = per_arr_al;
+        if (!h->d_arr_block.reserve(per_arr_al * h->ncol * 2)) return h->fail(RT_E_NOMEM, "cudaMalloc lattice");
+        if (!h->d_tiling.reserve((size_t)n * n * 4)) return h->fail(RT_E_NOMEM, "cudaMalloc tiling");
+        for (int l = 0; l < 2; ++l)
+            for (int c = 0; c < 8; ++c)
+                h->d_arr[l][c] = c < h->ncol ? static_cast<char*>(h->d_arr_block.p) + (l * h->ncol + c) * per_arr_al : nullptr;
+        // Alignment padding between the colour arrays is compared by the CFTP
+        // coalescence test, so it must hold the same bytes in both lattices.
+        cudaError_t e = cudaMemsetAsync(h->d_arr_block.p, 0, per_arr_al * h->ncol * 2, h->stream);
+        if (e != cudaSuccess) return h->cuda_fail(e, "memset lattice");
+        e = cudaMemcpyAsync(h->d_tiling.p, tiling, (size_t)n * n * 4, cudaMemcpyHostToDevice, h->stream);
+        if (e != cudaSuccess) return h->cuda_fail(e, "upload");
+        if (h->kind == 3) {
+            // The eight triangle-dimer arrays are derived on the host
+            // (TriangleDimerTiler.cpp:90-133) and copied up as they are.
+            std::vector<int32_t> arrays((size_t)8 * arows * width);
+            td_split_host(tiling, n, arrays.data());
+            for (int c = 0; c < 8 && e == cudaSuccess; ++c)
+                e = cudaMemcpy(h->d_arr[0][c], arrays.data() + (size_t)c * arows * width, per_arr, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return h->cuda_fail(e, "upload of the triangle-dimer arrays");
+        } else {
+            s = launch_split(false, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0],
+                             h->stream, &h->err);
+            if (s != RT_OK) return s;
+        }
+        if (!h->d_err.reserve(sizeof(int)) || !h->h_err.reserve(sizeof(int))) return h->fail(RT_E_NOMEM, "error word");
+        e = cudaMemsetAsync(h->d_err.p, 0, sizeof(int), h->stream);
+        if (e != cudaSuccess) return h->cuda_fail(e, "memset");
+        h->n = n;
+        h->arows = arows;
+        h->width = width;
+        grid_of(h, n, &h->rows, &h->cols);
+        h->uploaded = true;
+        return RT_OK;
+    });
 }
 
 rt_status rt_download(rt_tiler* h, int32_t* tiling) {
-    if (!h || !tiling) return h ? h->fail(RT_E_INVAL, "null tiling") : RT_E_INVAL;
-    if (!h->uploaded) return h->fail(RT_E_STATE, "download before upload");
-    cudaSetDevice(h->cfg.device);
-    const int n = h->n;
-    rt_status s = launch_split(true, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0],
-                               h->stream, &h->err);
-    if (s != RT_OK) return s;
-    cudaError_t e = cudaMemcpyAsync(tiling, h->d_tiling.p, (size_t)n * n * 4, cudaMemcpyDeviceToHost, h->stream);
-    if (e != cudaSuccess) return h->cuda_fail(e, "download");
-    return rt_synchronize(h);
+    return guarded([&]() -> rt_status {
+        if (!h || !tiling) return h ? h->fail(RT_E_INVAL, "null tiling") : RT_E_INVAL;
+        if (!h->uploaded) return h->fail(RT_E_STATE, "download before upload");
+        cudaSetDevice(h->cfg.device);
+        const int n = h->n;
+        rt_status s = launch_split(true, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0],
+                                   h->stream, &h->err);
+        if (s != RT_OK) return s;
+        cudaError_t e = cudaMemcpyAsync(tiling, h->d_tiling.p, (size_t)n * n * 4, cudaMemcpyDeviceToHost, h->stream);
+        if (e != cudaSuccess) return h->cuda_fail(e, "download");
+        return rt_synchronize(h);
+    });
 }
 
 rt_status rt_device_tiling(rt_tiler* h, int32_t** d_tiling) {
-    if (!h || !d_tiling) return h ? h->fail(RT_E_INVAL, "null pointer") : RT_E_INVAL;
-    if (!h->uploaded) return h->fail(RT_E_STATE, "device tiling before upload");
-    cudaSetDevice(h->cfg.device);
-    rt_status s = launch_split(true, h->elem, h->kind, h->ncol, h->n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0],
-                               h->stream, &h->err);
-    if (s != RT_OK) return s;
-    *d_tiling = static_cast<int32_t*>(h->d_tiling.p);
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!h || !d_tiling) return h ? h->fail(RT_E_INVAL, "null pointer") : RT_E_INVAL;
+        if (!h->uploaded) return h->fail(RT_E_STATE, "device tiling before upload");
+        cudaSetDevice(h->cfg.device);
+        rt_status s = launch_split(true, h->elem, h->kind, h->ncol, h->n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0],
+                                   h->stream, &h->err);
+        if (s != RT_OK) return s;
+        *d_tiling = static_cast<int32_t*>(h->d_tiling.p);
+        return RT_OK;
+    });
 }
 
 rt_status rt_synchronize(rt_tiler* h) {
-    if (!h) return RT_E_INVAL;
-    cudaSetDevice(h->cfg.device);
-    cudaError_t e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) return h->cuda_fail(e, "stream synchronize");
-    if (h->uploaded) {
-        e = cudaMemcpy(h->h_err.p, h->d_err.p, sizeof(int), cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) return h->cuda_fail(e, "error word readback");
-        const int code = *static_cast<int*>(h->h_err.p);
-        if (code & ERR_TIMEOUT) return h->fail(RT_E_TIMEOUT, "a bounded wait between CTAs timed out; walk aborted");
-        if (code) return h->fail(RT_E_CUDA, "device error word " + std::to_string(code));
-    }
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        cudaSetDevice(h->cfg.device);
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return h->cuda_fail(e, "stream synchronize");
+        if (h->uploaded) {
+            e = cudaMemcpy(h->h_err.p, h->d_err.p, sizeof(int), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) return h->cuda_fail(e, "error word readback");
+            const int code = *static_cast<int*>(h->h_err.p);
+            if (code & ERR_TIMEOUT) return h->fail(RT_E_TIMEOUT, "a bounded wait between CTAs timed out; walk aborted");
+            if (code) return h->fail(RT_E_CUDA, "device error word " + std::to_string(code));
+        }
+        return RT_OK;
+    });
 }
 
 // Stages the TinyMT parameter table on the device (all ids the walk uses).
@@ -732,34 +755,42 @@ static rt_status run_schedule(rt_tiler* h, const int64_t* steps, const int64_t* 
 }
 
 rt_status rt_run(rt_tiler* h, int64_t steps, int64_t seed) {
-    if (!h) return RT_E_INVAL;
-    return run_schedule(h, &steps, &seed, 1, true);
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        return run_schedule(h, &steps, &seed, 1, true);
+    });
 }
 
 rt_status rt_walk(rt_tiler* h, int32_t* tiling, int32_t n, int64_t steps, int64_t seed) {
-    if (!h) return RT_E_INVAL;
-    rt_status s = rt_upload(h, tiling, n);
-    if (s == RT_OK) s = run_schedule(h, &steps, &seed, 1, true);
-    if (s == RT_OK) s = rt_download(h, tiling);
-    return s;
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        rt_status s = rt_upload(h, tiling, n);
+        if (s == RT_OK) s = run_schedule(h, &steps, &seed, 1, true);
+        if (s == RT_OK) s = rt_download(h, tiling);
+        return s;
+    });
 }
 
 rt_status rt_walk_epochs(rt_tiler* h, int32_t* tiling, int32_t n, const int64_t* steps, const int64_t* seeds,
                          int32_t k) {
-    if (!h) return RT_E_INVAL;
-    if (h->kind != 0) return h->fail(RT_E_INVAL, "epoch walks exist for dominoes only (DominoTiler.h:76)");
-    if (k < 0 || (k > 0 && (!steps || !seeds))) return h->fail(RT_E_INVAL, "bad epoch arrays");
-    rt_status s = rt_upload(h, tiling, n);
-    if (s == RT_OK && k > 0) s = run_schedule(h, steps, seeds, k, false);
-    if (s == RT_OK) s = rt_download(h, tiling);
-    return s;
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        if (h->kind != 0) return h->fail(RT_E_INVAL, "epoch walks exist for dominoes only (DominoTiler.h:76)");
+        if (k < 0 || (k > 0 && (!steps || !seeds))) return h->fail(RT_E_INVAL, "bad epoch arrays");
+        rt_status s = rt_upload(h, tiling, n);
+        if (s == RT_OK && k > 0) s = run_schedule(h, steps, seeds, k, false);
+        if (s == RT_OK) s = rt_download(h, tiling);
+        return s;
+    });
 }
 
 rt_status rt_last_run_info(rt_tiler* h, int64_t* phases, int64_t* launches) {
-    if (!h) return RT_E_INVAL;
-    if (phases) *phases = h->last_phases;
-    if (launches) *launches = h->last_launches;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        if (phases) *phases = h->last_phases;
+        if (launches) *launches = h->last_launches;
+        return RT_OK;
+    });
 }
 
 // Coupling from the past: the reference's Examples/AztecDiamondCftpEx.cpp:42-68
@@ -778,80 +809,82 @@ rt_status rt_last_run_info(rt_tiler* h, int64_t* phases, int64_t* launches) {
 rt_status rt_cftp(rt_tiler* h, const int32_t* tmax, const int32_t* tmin, int32_t n, int64_t first_steps,
                   int32_t schedule, int64_t master_seed, int32_t max_trials, int32_t* out_tiling,
                   rt_cftp_stats* stats) {
-    if (!h) return RT_E_INVAL;
-    if (h->family != FAM_DOMINO_HB && h->family != FAM_LOZENGE8 && h->family != FAM_QLOZENGE8)
-        return h->fail(RT_E_INVAL,
-                       "CFTP needs a monotone kernel: the domino heat bath (RT_KERNEL_CFTP, dominokernelCFTP.cl) "
-                       "or a lozenge kernel");
-    // (bit-plane mode: both admitted families use heat-bath rules, monotone under shared bits)
-    if (!tmax || !tmin || first_steps <= 0 || max_trials <= 0 ||
-        (schedule != RT_CFTP_DOUBLING && schedule != RT_CFTP_REFERENCE))
-        return h->fail(RT_E_INVAL, "bad CFTP arguments");
-    rt_status s = rt_upload(h, tmax, n);
-    if (s != RT_OK) return s;
-    const size_t tb = (size_t)n * n * 4;
-    if (!h->d_tiling2.reserve(tb) || !h->d_count.reserve(8) || !h->h_count.reserve(8))
-        return h->fail(RT_E_NOMEM, "CFTP buffers");
-    cudaError_t e = cudaMemcpyAsync(h->d_tiling2.p, tmin, tb, cudaMemcpyHostToDevice, h->stream);
-    if (e != cudaSuccess) return h->cuda_fail(e, "upload of the minimal tiling");
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    std::mt19937 mt(master_seed);
-    std::vector<int64_t> steps{first_steps}, seeds{(int64_t)mt()};
-    rt_cftp_stats st{};
-    double ms_total = 0;
-    h->nlat = 2;
-    for (int trial = 0; trial < max_trials; ++trial) {
-        // Restart both chains at the far end of the current schedule.
-        s = launch_split(false, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0],
-                         h->stream, &h->err);
-        if (s == RT_OK)
-            s = launch_split(false, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling2.p), h->d_arr[1],
-                             h->stream, &h->err);
-        if (s != RT_OK) break;
-        cudaEventRecord(e0, h->stream);
-        s = run_schedule(h, steps.data(), seeds.data(), (int)steps.size(), false);
-        if (s != RT_OK) break;
-        cudaEventRecord(e1, h->stream);
-        s = launch_count_diff(h->d_arr[0][0], h->d_arr[1][0], h->per_arr_al * h->ncol,
-                              static_cast<unsigned long long*>(h->d_count.p), h->stream, &h->err);
-        if (s != RT_OK) break;
-        e = cudaMemcpyAsync(h->h_count.p, h->d_count.p, 8, cudaMemcpyDeviceToHost, h->stream);
-        if (e != cudaSuccess) {
-            s = h->cuda_fail(e, "coalescence readback");
-            break;
-        }
-        s = rt_synchronize(h);
-        if (s != RT_OK) break;
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        ms_total += ms;
-        st.trials = trial + 1;
-        st.total_steps = 0;
-        for (int64_t x : steps) st.total_steps += x;
-        if (*static_cast<unsigned long long*>(h->h_count.p) == 0) {
-            st.coalesced = 1;
-            break;
-        }
-        // Extend further into the past: the reference example prepends
-        // 2 * steps[last] (Examples/AztecDiamondCftpEx.cpp:67); the doubling
-        // schedule prepends the current total.
-        const int64_t add = schedule == RT_CFTP_REFERENCE ? 2 * steps.back() : st.total_steps;
-        steps.insert(steps.begin(), add);
-        seeds.insert(seeds.begin(), (int64_t)mt());
-    }
-    h->nlat = 1;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    st.device_ms = ms_total;
-    if (stats) *stats = st;
-    if (s != RT_OK) return s;
-    if (out_tiling) {
-        s = rt_download(h, out_tiling);  // lattice 0 = the chain started from the maximal tiling
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        if (h->family != FAM_DOMINO_HB && h->family != FAM_LOZENGE8 && h->family != FAM_QLOZENGE8)
+            return h->fail(RT_E_INVAL,
+                           "CFTP needs a monotone kernel: the domino heat bath (RT_KERNEL_CFTP, dominokernelCFTP.cl) "
+                           "or a lozenge kernel");
+        // (bit-plane mode: both admitted families use heat-bath rules, monotone under shared bits)
+        if (!tmax || !tmin || first_steps <= 0 || max_trials <= 0 ||
+            (schedule != RT_CFTP_DOUBLING && schedule != RT_CFTP_REFERENCE))
+            return h->fail(RT_E_INVAL, "bad CFTP arguments");
+        rt_status s = rt_upload(h, tmax, n);
         if (s != RT_OK) return s;
-    }
-    return RT_OK;
+        const size_t tb = (size_t)n * n * 4;
+        if (!h->d_tiling2.reserve(tb) || !h->d_count.reserve(8) || !h->h_count.reserve(8))
+            return h->fail(RT_E_NOMEM, "CFTP buffers");
+        cudaError_t e = cudaMemcpyAsync(h->d_tiling2.p, tmin, tb, cudaMemcpyHostToDevice, h->stream);
+        if (e != cudaSuccess) return h->cuda_fail(e, "upload of the minimal tiling");
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        std::mt19937 mt(master_seed);
+        std::vector<int64_t> steps{first_steps}, seeds{(int64_t)mt()};
+        rt_cftp_stats st{};
+        double ms_total = 0;
+        h->nlat = 2;
+        for (int trial = 0; trial < max_trials; ++trial) {
+            // Restart both chains at the far end of the current schedule.
+            s = launch_split(false, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling.p), h->d_arr[0],
+                             h->stream, &h->err);
+            if (s == RT_OK)
+                s = launch_split(false, h->elem, h->kind, h->ncol, n, static_cast<int32_t*>(h->d_tiling2.p), h->d_arr[1],
+                                 h->stream, &h->err);
+            if (s != RT_OK) break;
+            cudaEventRecord(e0, h->stream);
+            s = run_schedule(h, steps.data(), seeds.data(), (int)steps.size(), false);
+            if (s != RT_OK) break;
+            cudaEventRecord(e1, h->stream);
+            s = launch_count_diff(h->d_arr[0][0], h->d_arr[1][0], h->per_arr_al * h->ncol,
+                                  static_cast<unsigned long long*>(h->d_count.p), h->stream, &h->err);
+            if (s != RT_OK) break;
+            e = cudaMemcpyAsync(h->h_count.p, h->d_count.p, 8, cudaMemcpyDeviceToHost, h->stream);
+            if (e != cudaSuccess) {
+                s = h->cuda_fail(e, "coalescence readback");
+                break;
+            }
+            s = rt_synchronize(h);
+            if (s != RT_OK) break;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms_total += ms;
+            st.trials = trial + 1;
+            st.total_steps = 0;
+            for (int64_t x : steps) st.total_steps += x;
+            if (*static_cast<unsigned long long*>(h->h_count.p) == 0) {
+                st.coalesced = 1;
+                break;
+            }
+            // Extend further into the past: the reference example prepends
+            // 2 * steps[last] (Examples/AztecDiamondCftpEx.cpp:67); the doubling
+            // schedule prepends the current total.
+            const int64_t add = schedule == RT_CFTP_REFERENCE ? 2 * steps.back() : st.total_steps;
+            steps.insert(steps.begin(), add);
+            seeds.insert(seeds.begin(), (int64_t)mt());
+        }
+        h->nlat = 1;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        st.device_ms = ms_total;
+        if (stats) *stats = st;
+        if (s != RT_OK) return s;
+        if (out_tiling) {
+            s = rt_download(h, out_tiling);  // lattice 0 = the chain started from the maximal tiling
+            if (s != RT_OK) return s;
+        }
+        return RT_OK;
+    });
 }
 
 }  // extern "C"

@@ -29,6 +29,9 @@
 
 #include "../../include/rt_b200_extremal.h"
 #include "rt_internal.h"
+#include "rt_guard.h"
+
+using rtb::guarded;
 
 namespace rtb {
 namespace {
@@ -516,11 +519,15 @@ rt_status extremal_run(int32_t model, const int32_t* d, int64_t dlen, int32_t de
 extern "C" rt_status rt_extremal_tilings(int32_t model, const int32_t* d, int64_t dlen, int32_t device, int32_t* tmin,
                                          int32_t* tmax, int32_t* hmin, int32_t* hmax, int64_t len,
                                          rt_extremal_stats* stats) {
-    return extremal_run(model, d, dlen, device, tmin, tmax, hmin, hmax, len, stats, false);
+    return guarded([&]() -> rt_status {
+        return extremal_run(model, d, dlen, device, tmin, tmax, hmin, hmax, len, stats, false);
+    });
 }
 
 extern "C" rt_status rt_extremal_tilings_device(int32_t model, const int32_t* d, int64_t dlen, int32_t device,
                                                 int32_t* d_tmin, int32_t* d_tmax, int32_t* d_hmin, int32_t* d_hmax,
                                                 int64_t len, rt_extremal_stats* stats) {
-    return extremal_run(model, d, dlen, device, d_tmin, d_tmax, d_hmin, d_hmax, len, stats, true);
+    return guarded([&]() -> rt_status {
+        return extremal_run(model, d, dlen, device, d_tmin, d_tmax, d_hmin, d_hmax, len, stats, true);
+    });
 }

@@ -20,6 +20,9 @@
 
 #include "../../include/rt_b200_height.h"
 #include "rt_internal.h"
+#include "rt_guard.h"
+
+using rtb::guarded;
 
 namespace rtb {
 
@@ -215,152 +218,164 @@ dim3 finish_grid(int n) { return dim3((unsigned)std::max(1, std::min(16, (n + 25
 extern "C" {
 
 rt_status rt_hplan_create(int32_t model, const int32_t* d, int64_t dlen, int32_t device, rt_hplan** out) {
-    if (!out) return RT_E_INVAL;
-    *out = nullptr;
-    if (model != RT_DOMINO && model != RT_LOZENGE) {
-        g_hplan_create_error = "height plans exist for dominoes and lozenges";
-        return RT_E_INVAL;
-    }
-    int n = 0;
-    std::vector<uint8_t> kind, edges;
-    if (!lipschitz_graph(model, d, dlen, &n, &kind, &edges)) {
-        g_hplan_create_error = "not a domain of this model";
-        return RT_E_INVAL;
-    }
-    const int right = model == RT_DOMINO ? 2 : 0;  // direction (0, +1)
-    const int down = model == RT_DOMINO ? 0 : 5;   // direction (+1, 0)
-    std::vector<int> lo(n, n), hi(n, -1), conn(n, -1);
-    int64_t verts = 0;
-    int first = -1, last = -1, i0 = -1, j0 = -1;
-    for (int i = 0; i < n; ++i) {
-        for (int j = 0; j < n; ++j) {
-            const int k = kind[(size_t)i * n + j];
-            if (!k) continue;
-            lo[i] = std::min(lo[i], j);
-            hi[i] = std::max(hi[i], j);
-            ++verts;
-            if (k == 2 && i0 < 0) i0 = i, j0 = j;
+    return guarded([&]() -> rt_status {
+        if (!out) return RT_E_INVAL;
+        *out = nullptr;
+        if (model != RT_DOMINO && model != RT_LOZENGE) {
+            g_hplan_create_error = "height plans exist for dominoes and lozenges";
+            return RT_E_INVAL;
         }
-        if (hi[i] < 0) continue;
-        for (int j = lo[i]; j < hi[i]; ++j)
-            if (!kind[(size_t)i * n + j] || !(edges[(size_t)i * n + j] & (1u << right))) {
-                g_hplan_create_error = "vertex row " + std::to_string(i) + " is not one run of domain vertices";
-                return RT_E_INVAL;
+        int n = 0;
+        std::vector<uint8_t> kind, edges;
+        if (!lipschitz_graph(model, d, dlen, &n, &kind, &edges)) {
+            g_hplan_create_error = "not a domain of this model";
+            return RT_E_INVAL;
+        }
+        const int right = model == RT_DOMINO ? 2 : 0;  // direction (0, +1)
+        const int down = model == RT_DOMINO ? 0 : 5;   // direction (+1, 0)
+        std::vector<int> lo(n, n), hi(n, -1), conn(n, -1);
+        int64_t verts = 0;
+        int first = -1, last = -1, i0 = -1, j0 = -1;
+        for (int i = 0; i < n; ++i) {
+            for (int j = 0; j < n; ++j) {
+                const int k = kind[(size_t)i * n + j];
+                if (!k) continue;
+                lo[i] = std::min(lo[i], j);
+                hi[i] = std::max(hi[i], j);
+                ++verts;
+                if (k == 2 && i0 < 0) i0 = i, j0 = j;
             }
-        if (first < 0) {
-            first = i;
-        } else {
-            if (last != i - 1) {
-                g_hplan_create_error = "rows without domain vertices between domain rows";
-                return RT_E_INVAL;
-            }
-            for (int c = std::max(lo[i], lo[i - 1]); c <= std::min(hi[i], hi[i - 1]); ++c)
-                if (edges[(size_t)(i - 1) * n + c] & (1u << down)) {
-                    conn[i] = c;
-                    break;
+            if (hi[i] < 0) continue;
+            for (int j = lo[i]; j < hi[i]; ++j)
+                if (!kind[(size_t)i * n + j] || !(edges[(size_t)i * n + j] & (1u << right))) {
+                    g_hplan_create_error = "vertex row " + std::to_string(i) + " is not one run of domain vertices";
+                    return RT_E_INVAL;
                 }
-            if (conn[i] < 0) {
-                g_hplan_create_error = "vertex rows " + std::to_string(i - 1) + " and " + std::to_string(i) +
-                                       " share no in-domain edge";
-                return RT_E_INVAL;
+            if (first < 0) {
+                first = i;
+            } else {
+                if (last != i - 1) {
+                    g_hplan_create_error = "rows without domain vertices between domain rows";
+                    return RT_E_INVAL;
+                }
+                for (int c = std::max(lo[i], lo[i - 1]); c <= std::min(hi[i], hi[i - 1]); ++c)
+                    if (edges[(size_t)(i - 1) * n + c] & (1u << down)) {
+                        conn[i] = c;
+                        break;
+                    }
+                if (conn[i] < 0) {
+                    g_hplan_create_error = "vertex rows " + std::to_string(i - 1) + " and " + std::to_string(i) +
+                                           " share no in-domain edge";
+                    return RT_E_INVAL;
+                }
             }
+            last = i;
         }
-        last = i;
-    }
-    if (i0 < 0) {
-        g_hplan_create_error = "domain has no boundary vertex";
-        return RT_E_INVAL;
-    }
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
-        g_hplan_create_error = "no CUDA device with that ordinal";
-        return RT_E_NODEVICE;
-    }
-    cudaSetDevice(device);
-    rt_hplan* p = new rt_hplan();
-    p->model = model;
-    p->device = device;
-    p->n = n;
-    p->i0 = i0;
-    p->j0 = j0;
-    p->vertices = verts;
-    bool ok = cudaMalloc(&p->d_lo, n * sizeof(int)) == cudaSuccess &&
-              cudaMalloc(&p->d_hi, n * sizeof(int)) == cudaSuccess &&
-              cudaMalloc(&p->d_conn, n * sizeof(int)) == cudaSuccess &&
-              cudaMalloc(&p->d_R, n * sizeof(int32_t)) == cudaSuccess &&
-              cudaMalloc(&p->d_P, (size_t)n * n * sizeof(int32_t)) == cudaSuccess &&
-              cudaMalloc(&p->d_err, sizeof(double)) == cudaSuccess;
-    if (!ok) return create_fail(p, RT_E_NOMEM, "height plan buffers");
-    ok = cudaMemcpy(p->d_lo, lo.data(), n * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(p->d_hi, hi.data(), n * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(p->d_conn, conn.data(), n * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
-    if (!ok) return create_fail(p, RT_E_CUDA, "height plan upload");
-    *out = p;
-    return RT_OK;
+        if (i0 < 0) {
+            g_hplan_create_error = "domain has no boundary vertex";
+            return RT_E_INVAL;
+        }
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+            g_hplan_create_error = "no CUDA device with that ordinal";
+            return RT_E_NODEVICE;
+        }
+        cudaSetDevice(device);
+        rt_hplan* p = new rt_hplan();
+        p->model = model;
+        p->device = device;
+        p->n = n;
+        p->i0 = i0;
+        p->j0 = j0;
+        p->vertices = verts;
+        bool ok = cudaMalloc(&p->d_lo, n * sizeof(int)) == cudaSuccess &&
+                  cudaMalloc(&p->d_hi, n * sizeof(int)) == cudaSuccess &&
+                  cudaMalloc(&p->d_conn, n * sizeof(int)) == cudaSuccess &&
+                  cudaMalloc(&p->d_R, n * sizeof(int32_t)) == cudaSuccess &&
+                  cudaMalloc(&p->d_P, (size_t)n * n * sizeof(int32_t)) == cudaSuccess &&
+                  cudaMalloc(&p->d_err, sizeof(double)) == cudaSuccess;
+        if (!ok) return create_fail(p, RT_E_NOMEM, "height plan buffers");
+        ok = cudaMemcpy(p->d_lo, lo.data(), n * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(p->d_hi, hi.data(), n * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(p->d_conn, conn.data(), n * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+        if (!ok) return create_fail(p, RT_E_CUDA, "height plan upload");
+        *out = p;
+        return RT_OK;
+    });
 }
 
 rt_status rt_hplan_destroy(rt_hplan* p) {
-    if (!p) return RT_E_INVAL;
-    cudaSetDevice(p->device);
-    cudaFree(p->d_lo);
-    cudaFree(p->d_hi);
-    cudaFree(p->d_conn);
-    cudaFree(p->d_R);
-    cudaFree(p->d_P);
-    cudaFree(p->d_err);
-    delete p;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!p) return RT_E_INVAL;
+        cudaSetDevice(p->device);
+        cudaFree(p->d_lo);
+        cudaFree(p->d_hi);
+        cudaFree(p->d_conn);
+        cudaFree(p->d_R);
+        cudaFree(p->d_P);
+        cudaFree(p->d_err);
+        delete p;
+        return RT_OK;
+    });
 }
 
 rt_status rt_hplan_info(rt_hplan* p, int32_t* n, int64_t* vertices) {
-    if (!p) return RT_E_INVAL;
-    if (n) *n = p->n;
-    if (vertices) *vertices = p->vertices;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!p) return RT_E_INVAL;
+        if (n) *n = p->n;
+        if (vertices) *vertices = p->vertices;
+        return RT_OK;
+    });
 }
 
 const char* rt_hplan_last_error(rt_hplan* p) { return p ? p->err.c_str() : g_hplan_create_error.c_str(); }
 
 rt_status rt_hplan_heights(rt_hplan* p, const int32_t* d_tiling, int32_t* d_heights, void* stream) {
-    if (!p || !d_tiling || !d_heights) return p ? p->fail(RT_E_INVAL, "null pointer") : RT_E_INVAL;
-    cudaSetDevice(p->device);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    rt_status st = scan_rows(p, d_tiling, d_heights, s);
-    if (st != RT_OK) return st;
-    finish<FIN_WRITE><<<finish_grid(p->n), 256, 0, s>>>(p->n, p->d_lo, p->d_hi, p->d_R, d_heights, nullptr, nullptr,
-                                                        nullptr);
-    cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? RT_OK : p->fail(RT_E_CUDA, std::string("height launch: ") + cudaGetErrorString(e));
+    return guarded([&]() -> rt_status {
+        if (!p || !d_tiling || !d_heights) return p ? p->fail(RT_E_INVAL, "null pointer") : RT_E_INVAL;
+        cudaSetDevice(p->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        rt_status st = scan_rows(p, d_tiling, d_heights, s);
+        if (st != RT_OK) return st;
+        finish<FIN_WRITE><<<finish_grid(p->n), 256, 0, s>>>(p->n, p->d_lo, p->d_hi, p->d_R, d_heights, nullptr, nullptr,
+                                                            nullptr);
+        cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? RT_OK : p->fail(RT_E_CUDA, std::string("height launch: ") + cudaGetErrorString(e));
+    });
 }
 
 rt_status rt_hplan_accumulate(rt_hplan* p, const int32_t* d_tiling, int64_t* d_sum, void* stream) {
-    if (!p || !d_tiling || !d_sum) return p ? p->fail(RT_E_INVAL, "null pointer") : RT_E_INVAL;
-    cudaSetDevice(p->device);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    rt_status st = scan_rows(p, d_tiling, p->d_P, s);
-    if (st != RT_OK) return st;
-    finish<FIN_SUM><<<finish_grid(p->n), 256, 0, s>>>(p->n, p->d_lo, p->d_hi, p->d_R, p->d_P, d_sum, nullptr, nullptr);
-    cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? RT_OK : p->fail(RT_E_CUDA, std::string("height launch: ") + cudaGetErrorString(e));
+    return guarded([&]() -> rt_status {
+        if (!p || !d_tiling || !d_sum) return p ? p->fail(RT_E_INVAL, "null pointer") : RT_E_INVAL;
+        cudaSetDevice(p->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        rt_status st = scan_rows(p, d_tiling, p->d_P, s);
+        if (st != RT_OK) return st;
+        finish<FIN_SUM><<<finish_grid(p->n), 256, 0, s>>>(p->n, p->d_lo, p->d_hi, p->d_R, p->d_P, d_sum, nullptr, nullptr);
+        cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? RT_OK : p->fail(RT_E_CUDA, std::string("height launch: ") + cudaGetErrorString(e));
+    });
 }
 
 rt_status rt_hplan_error(rt_hplan* p, const int32_t* d_tiling, const float* d_ref, double* mean_abs, void* stream) {
-    if (!p || !d_tiling || !d_ref || !mean_abs) return p ? p->fail(RT_E_INVAL, "null pointer") : RT_E_INVAL;
-    cudaSetDevice(p->device);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemsetAsync(p->d_err, 0, sizeof(double), s);
-    if (e != cudaSuccess) return p->fail(RT_E_CUDA, std::string("memset: ") + cudaGetErrorString(e));
-    rt_status st = scan_rows(p, d_tiling, p->d_P, s);
-    if (st != RT_OK) return st;
-    finish<FIN_ERROR><<<finish_grid(p->n), 256, 0, s>>>(p->n, p->d_lo, p->d_hi, p->d_R, p->d_P, nullptr, d_ref,
-                                                        p->d_err);
-    double sum = 0.0;
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&sum, p->d_err, sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return p->fail(RT_E_CUDA, std::string("height error: ") + cudaGetErrorString(e));
-    *mean_abs = p->vertices > 0 ? sum / (double)p->vertices : 0.0;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!p || !d_tiling || !d_ref || !mean_abs) return p ? p->fail(RT_E_INVAL, "null pointer") : RT_E_INVAL;
+        cudaSetDevice(p->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        cudaError_t e = cudaMemsetAsync(p->d_err, 0, sizeof(double), s);
+        if (e != cudaSuccess) return p->fail(RT_E_CUDA, std::string("memset: ") + cudaGetErrorString(e));
+        rt_status st = scan_rows(p, d_tiling, p->d_P, s);
+        if (st != RT_OK) return st;
+        finish<FIN_ERROR><<<finish_grid(p->n), 256, 0, s>>>(p->n, p->d_lo, p->d_hi, p->d_R, p->d_P, nullptr, d_ref,
+                                                            p->d_err);
+        double sum = 0.0;
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&sum, p->d_err, sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return p->fail(RT_E_CUDA, std::string("height error: ") + cudaGetErrorString(e));
+        *mean_abs = p->vertices > 0 ? sum / (double)p->vertices : 0.0;
+        return RT_OK;
+    });
 }
 
 }  // extern "C"

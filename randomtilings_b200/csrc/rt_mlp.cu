@@ -21,6 +21,9 @@
 
 #include "../../include/rt_b200_mlp.h"
 #include "rt_device.cuh"
+#include "rt_guard.h"
+
+using rtb::guarded;
 
 namespace rtb {
 namespace mlp {
@@ -611,127 +614,143 @@ rt_status sync(rt_mlp* m) {
 extern "C" {
 
 rt_status rt_mlp_create(int32_t device, uint64_t seed, rt_mlp** out) {
-    if (!out) return RT_E_INVAL;
-    *out = nullptr;
-    if (cudaSetDevice(device) != cudaSuccess) return RT_E_NODEVICE;
-    rt_mlp* m = new rt_mlp();
-    m->device = device;
-    bool ok = cudaStreamCreateWithFlags(&m->s, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaMalloc(&m->P, NPARAM * 4) == cudaSuccess && cudaMalloc(&m->G, NPARAM * 4) == cudaSuccess &&
-              cudaMalloc(&m->M1, NPARAM * 4) == cudaSuccess && cudaMalloc(&m->M2, NPARAM * 4) == cudaSuccess &&
-              cudaMalloc(&m->w1, H * H * 2) == cudaSuccess && cudaMalloc(&m->w2, H * H * 2) == cudaSuccess &&
-              cudaMalloc(&m->loss, 4) == cudaSuccess && cudaMalloc(&m->err, sizeof(int)) == cudaSuccess &&
-              cudaMemset(m->err, 0, sizeof(int)) == cudaSuccess;
-    if (!ok) {
-        rt_mlp_destroy(m);
-        return RT_E_NOMEM;
-    }
-    // Initialisation: weights uniform in +-1/sqrt(fan_in) from Philox(seed), biases 0.
-    std::vector<float> p(NPARAM, 0.0f);
-    auto fill = [&](int off, int count, int fan_in) {
-        const float a = 1.0f / std::sqrt((float)fan_in);
-        for (int i = 0; i < count; ++i) {
-            const uint4 w = rtb::philox4((uint32_t)(off + i), 0x494e4954u, 0, 0, (uint32_t)seed, (uint32_t)(seed >> 32));
-            p[off + i] = a * (2.0f * ((float)(w.x >> 8) * (1.0f / 16777216.0f)) - 1.0f);
+    return guarded([&]() -> rt_status {
+        if (!out) return RT_E_INVAL;
+        *out = nullptr;
+        if (cudaSetDevice(device) != cudaSuccess) return RT_E_NODEVICE;
+        rt_mlp* m = new rt_mlp();
+        m->device = device;
+        bool ok = cudaStreamCreateWithFlags(&m->s, cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaMalloc(&m->P, NPARAM * 4) == cudaSuccess && cudaMalloc(&m->G, NPARAM * 4) == cudaSuccess &&
+                  cudaMalloc(&m->M1, NPARAM * 4) == cudaSuccess && cudaMalloc(&m->M2, NPARAM * 4) == cudaSuccess &&
+                  cudaMalloc(&m->w1, H * H * 2) == cudaSuccess && cudaMalloc(&m->w2, H * H * 2) == cudaSuccess &&
+                  cudaMalloc(&m->loss, 4) == cudaSuccess && cudaMalloc(&m->err, sizeof(int)) == cudaSuccess &&
+                  cudaMemset(m->err, 0, sizeof(int)) == cudaSuccess;
+        if (!ok) {
+            rt_mlp_destroy(m);
+            return RT_E_NOMEM;
         }
-    };
-    fill(OW0, H * IN, IN);
-    fill(OW1, H * H, H);
-    fill(OW2, H * H, H);
-    fill(OW3, H, H);
-    *out = m;
-    return rt_mlp_set_params(m, p.data());
+        // Initialisation: weights uniform in +-1/sqrt(fan_in) from Philox(seed), biases 0.
+        std::vector<float> p(NPARAM, 0.0f);
+        auto fill = [&](int off, int count, int fan_in) {
+            const float a = 1.0f / std::sqrt((float)fan_in);
+            for (int i = 0; i < count; ++i) {
+                const uint4 w = rtb::philox4((uint32_t)(off + i), 0x494e4954u, 0, 0, (uint32_t)seed, (uint32_t)(seed >> 32));
+                p[off + i] = a * (2.0f * ((float)(w.x >> 8) * (1.0f / 16777216.0f)) - 1.0f);
+            }
+        };
+        fill(OW0, H * IN, IN);
+        fill(OW1, H * H, H);
+        fill(OW2, H * H, H);
+        fill(OW3, H, H);
+        *out = m;
+        return rt_mlp_set_params(m, p.data());
+    });
 }
 
 rt_status rt_mlp_destroy(rt_mlp* m) {
-    if (!m) return RT_E_INVAL;
-    cudaSetDevice(m->device);
-    if (m->s) cudaStreamSynchronize(m->s);
-    free_ws(m);
-    void* ps[] = {m->P, m->G, m->M1, m->M2, m->w1, m->w2, m->loss, m->X, m->T, m->err};
-    for (void* p : ps)
-        if (p) cudaFree(p);
-    if (m->s) cudaStreamDestroy(m->s);
-    delete m;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!m) return RT_E_INVAL;
+        cudaSetDevice(m->device);
+        if (m->s) cudaStreamSynchronize(m->s);
+        free_ws(m);
+        void* ps[] = {m->P, m->G, m->M1, m->M2, m->w1, m->w2, m->loss, m->X, m->T, m->err};
+        for (void* p : ps)
+            if (p) cudaFree(p);
+        if (m->s) cudaStreamDestroy(m->s);
+        delete m;
+        return RT_OK;
+    });
 }
 
 rt_status rt_mlp_get_params(rt_mlp* m, float* params) {
-    if (!m || !params) return RT_E_INVAL;
-    cudaSetDevice(m->device);
-    if (cudaMemcpyAsync(params, m->P, NPARAM * 4, cudaMemcpyDeviceToHost, m->s) != cudaSuccess) return RT_E_CUDA;
-    return sync(m);
+    return guarded([&]() -> rt_status {
+        if (!m || !params) return RT_E_INVAL;
+        cudaSetDevice(m->device);
+        if (cudaMemcpyAsync(params, m->P, NPARAM * 4, cudaMemcpyDeviceToHost, m->s) != cudaSuccess) return RT_E_CUDA;
+        return sync(m);
+    });
 }
 
 rt_status rt_mlp_set_params(rt_mlp* m, const float* params) {
-    if (!m || !params) return RT_E_INVAL;
-    cudaSetDevice(m->device);
-    cudaMemcpyAsync(m->P, params, NPARAM * 4, cudaMemcpyHostToDevice, m->s);
-    cudaMemsetAsync(m->M1, 0, NPARAM * 4, m->s);
-    cudaMemsetAsync(m->M2, 0, NPARAM * 4, m->s);
-    m->adam_t = 0;
-    to_bf16<<<(H * H + 255) / 256, 256, 0, m->s>>>(m->P, m->w1, m->w2);
-    return sync(m);
+    return guarded([&]() -> rt_status {
+        if (!m || !params) return RT_E_INVAL;
+        cudaSetDevice(m->device);
+        cudaMemcpyAsync(m->P, params, NPARAM * 4, cudaMemcpyHostToDevice, m->s);
+        cudaMemsetAsync(m->M1, 0, NPARAM * 4, m->s);
+        cudaMemsetAsync(m->M2, 0, NPARAM * 4, m->s);
+        m->adam_t = 0;
+        to_bf16<<<(H * H + 255) / 256, 256, 0, m->s>>>(m->P, m->w1, m->w2);
+        return sync(m);
+    });
 }
 
 rt_status rt_mlp_predict(rt_mlp* m, const float* x, int64_t n, float* y) {
-    if (!m || !x || !y || n < 0) return RT_E_INVAL;
-    cudaSetDevice(m->device);
-    const int64_t chunk = 1 << 18;
-    for (int64_t r0 = 0; r0 < n; r0 += chunk) {
-        const int rn = (int)std::min<int64_t>(chunk, n - r0);
-        if (!reserve(m, rn)) return RT_E_NOMEM;
-        cudaMemcpyAsync(m->x, x + r0 * IN, (size_t)rn * IN * 4, cudaMemcpyHostToDevice, m->s);
-        forward(m, rn, false);
-        cudaMemcpyAsync(y + r0, m->y, (size_t)rn * 4, cudaMemcpyDeviceToHost, m->s);
-        rt_status st = sync(m);
-        if (st != RT_OK) return st;
-    }
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!m || !x || !y || n < 0) return RT_E_INVAL;
+        cudaSetDevice(m->device);
+        const int64_t chunk = 1 << 18;
+        for (int64_t r0 = 0; r0 < n; r0 += chunk) {
+            const int rn = (int)std::min<int64_t>(chunk, n - r0);
+            if (!reserve(m, rn)) return RT_E_NOMEM;
+            cudaMemcpyAsync(m->x, x + r0 * IN, (size_t)rn * IN * 4, cudaMemcpyHostToDevice, m->s);
+            forward(m, rn, false);
+            cudaMemcpyAsync(y + r0, m->y, (size_t)rn * 4, cudaMemcpyDeviceToHost, m->s);
+            rt_status st = sync(m);
+            if (st != RT_OK) return st;
+        }
+        return RT_OK;
+    });
 }
 
 rt_status rt_mlp_loss_grad(rt_mlp* m, const float* x, const float* target, int64_t n, float* loss, float* grad) {
-    if (!m || !x || !target || n <= 0 || n > (1 << 22)) return RT_E_INVAL;
-    cudaSetDevice(m->device);
-    if (!reserve(m, n)) return RT_E_NOMEM;
-    cudaMemcpyAsync(m->x, x, (size_t)n * IN * 4, cudaMemcpyHostToDevice, m->s);
-    cudaMemcpyAsync(m->t, target, (size_t)n * 4, cudaMemcpyHostToDevice, m->s);
-    forward(m, (int)n, true);
-    backward(m, (int)n);
-    if (loss) cudaMemcpyAsync(loss, m->loss, 4, cudaMemcpyDeviceToHost, m->s);
-    if (grad) cudaMemcpyAsync(grad, m->G, NPARAM * 4, cudaMemcpyDeviceToHost, m->s);
-    return sync(m);
+    return guarded([&]() -> rt_status {
+        if (!m || !x || !target || n <= 0 || n > (1 << 22)) return RT_E_INVAL;
+        cudaSetDevice(m->device);
+        if (!reserve(m, n)) return RT_E_NOMEM;
+        cudaMemcpyAsync(m->x, x, (size_t)n * IN * 4, cudaMemcpyHostToDevice, m->s);
+        cudaMemcpyAsync(m->t, target, (size_t)n * 4, cudaMemcpyHostToDevice, m->s);
+        forward(m, (int)n, true);
+        backward(m, (int)n);
+        if (loss) cudaMemcpyAsync(loss, m->loss, 4, cudaMemcpyDeviceToHost, m->s);
+        if (grad) cudaMemcpyAsync(grad, m->G, NPARAM * 4, cudaMemcpyDeviceToHost, m->s);
+        return sync(m);
+    });
 }
 
 rt_status rt_mlp_set_data(rt_mlp* m, const float* x, const float* target, int64_t n) {
-    if (!m || !x || !target || n <= 0) return RT_E_INVAL;
-    cudaSetDevice(m->device);
-    if (m->X) cudaFree(m->X);
-    if (m->T) cudaFree(m->T);
-    m->X = m->T = nullptr;
-    if (cudaMalloc(&m->X, (size_t)n * IN * 4) != cudaSuccess || cudaMalloc(&m->T, (size_t)n * 4) != cudaSuccess)
-        return RT_E_NOMEM;
-    cudaMemcpyAsync(m->X, x, (size_t)n * IN * 4, cudaMemcpyHostToDevice, m->s);
-    cudaMemcpyAsync(m->T, target, (size_t)n * 4, cudaMemcpyHostToDevice, m->s);
-    m->rows = n;
-    return sync(m);
+    return guarded([&]() -> rt_status {
+        if (!m || !x || !target || n <= 0) return RT_E_INVAL;
+        cudaSetDevice(m->device);
+        if (m->X) cudaFree(m->X);
+        if (m->T) cudaFree(m->T);
+        m->X = m->T = nullptr;
+        if (cudaMalloc(&m->X, (size_t)n * IN * 4) != cudaSuccess || cudaMalloc(&m->T, (size_t)n * 4) != cudaSuccess)
+            return RT_E_NOMEM;
+        cudaMemcpyAsync(m->X, x, (size_t)n * IN * 4, cudaMemcpyHostToDevice, m->s);
+        cudaMemcpyAsync(m->T, target, (size_t)n * 4, cudaMemcpyHostToDevice, m->s);
+        m->rows = n;
+        return sync(m);
+    });
 }
 
 rt_status rt_mlp_train(rt_mlp* m, int64_t steps, int32_t batch, float lr, uint64_t seed, float* loss) {
-    if (!m || steps < 0 || batch <= 0 || batch > (1 << 22) || !m->X) return RT_E_INVAL;
-    cudaSetDevice(m->device);
-    if (!reserve(m, batch)) return RT_E_NOMEM;
-    for (int64_t k = 0; k < steps; ++k) {
-        gather_batch<<<(batch + 255) / 256, 256, 0, m->s>>>(m->X, m->T, m->rows, batch, seed, m->adam_t, m->x, m->t);
-        forward(m, batch, true);
-        backward(m, batch);
-        ++m->adam_t;
-        const float b1t = std::pow(0.9f, (float)m->adam_t), b2t = std::pow(0.999f, (float)m->adam_t);
-        adam<<<(NPARAM + 255) / 256, 256, 0, m->s>>>(m->P, m->G, m->M1, m->M2, NPARAM, lr, b1t, b2t);
-        to_bf16<<<(H * H + 255) / 256, 256, 0, m->s>>>(m->P, m->w1, m->w2);
-    }
-    if (loss) cudaMemcpyAsync(loss, m->loss, 4, cudaMemcpyDeviceToHost, m->s);
-    return sync(m);
+    return guarded([&]() -> rt_status {
+        if (!m || steps < 0 || batch <= 0 || batch > (1 << 22) || !m->X) return RT_E_INVAL;
+        cudaSetDevice(m->device);
+        if (!reserve(m, batch)) return RT_E_NOMEM;
+        for (int64_t k = 0; k < steps; ++k) {
+            gather_batch<<<(batch + 255) / 256, 256, 0, m->s>>>(m->X, m->T, m->rows, batch, seed, m->adam_t, m->x, m->t);
+            forward(m, batch, true);
+            backward(m, batch);
+            ++m->adam_t;
+            const float b1t = std::pow(0.9f, (float)m->adam_t), b2t = std::pow(0.999f, (float)m->adam_t);
+            adam<<<(NPARAM + 255) / 256, 256, 0, m->s>>>(m->P, m->G, m->M1, m->M2, NPARAM, lr, b1t, b2t);
+            to_bf16<<<(H * H + 255) / 256, 256, 0, m->s>>>(m->P, m->w1, m->w2);
+        }
+        if (loss) cudaMemcpyAsync(loss, m->loss, 4, cudaMemcpyDeviceToHost, m->s);
+        return sync(m);
+    });
 }
 
 }  // extern "C"

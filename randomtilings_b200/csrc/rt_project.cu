@@ -17,6 +17,9 @@
 
 #include "../../include/rt_b200_project.h"
 #include "rt_internal.h"
+#include "rt_guard.h"
+
+using rtb::guarded;
 
 namespace rtb {
 
@@ -110,84 +113,86 @@ struct DevMem {
 extern "C" rt_status rt_project_heights(int32_t model, const int32_t* d, int64_t dlen, const int32_t* hmin,
                                         const int32_t* hmax, const float* target, int32_t* out, int64_t hlen,
                                         int32_t device, rt_project_stats* stats) {
-    if ((model != RT_DOMINO && model != RT_LOZENGE) || !d || !hmin || !hmax || !target || !out) return RT_E_INVAL;
-    int n = 0;
-    std::vector<uint8_t> kind, edges;
-    if (!lipschitz_graph(model, d, dlen, &n, &kind, &edges) || (int64_t)n * n != hlen) return RT_E_INVAL;
-    for (int64_t v = 0; v < hlen; ++v)
-        if (kind[v] && (hmin[v] == INT_MAX || hmax[v] == INT_MAX || hmin[v] > hmax[v] ||
-                        ((int64_t)hmax[v] - hmin[v]) % (model == RT_DOMINO ? 4 : 3) != 0))
-            return RT_E_INVAL;  // not a pair of height functions of this domain
-    if (cudaSetDevice(device) != cudaSuccess) return RT_E_NODEVICE;
-    const size_t N2 = (size_t)hlen;
-    DevMem dk, de, dlo, dhi, dt, dh, dc;
-    if (!dk.alloc(N2) || !de.alloc(N2) || !dlo.alloc(N2 * 4) || !dhi.alloc(N2 * 4) || !dt.alloc(N2 * 4) ||
-        !dh.alloc(N2 * 4) || !dc.alloc(16))
-        return RT_E_NOMEM;
-    cudaStream_t s;
-    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return RT_E_CUDA;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaMemcpyAsync(dk.p, kind.data(), N2, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(de.p, edges.data(), N2, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dlo.p, hmin, N2 * 4, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dhi.p, hmax, N2 * 4, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dt.p, target, N2 * 4, cudaMemcpyHostToDevice, s);
-    const int threads = 256;
-    const unsigned blocks = (unsigned)((N2 + threads - 1) / threads);
-    const bool dom = model == RT_DOMINO;
-    auto* K = static_cast<const uint8_t*>(dk.p);
-    auto* E = static_cast<const uint8_t*>(de.p);
-    auto* H = static_cast<int32_t*>(dh.p);
-    auto* C = static_cast<unsigned long long*>(dc.p);
-    cudaEventRecord(e0, s);
-    if (dom)
-        project_init<true><<<blocks, threads, 0, s>>>(K, (const int32_t*)dlo.p, (const int32_t*)dhi.p,
-                                                      (const float*)dt.p, H, n);
-    else
-        project_init<false><<<blocks, threads, 0, s>>>(K, (const int32_t*)dlo.p, (const int32_t*)dhi.p,
-                                                       (const float*)dt.p, H, n);
-    int64_t passes = 0, lowered = 0;
-    unsigned long long cnt[2] = {0, 0};
-    // Passes in chunks of 16 with one readback of the change counter per chunk;
-    // every pass is a monotone step, so extra passes after convergence are no-ops.
-    const int64_t cap = (int64_t)hlen + 32;  // Bellman-Ford bound: no more passes than vertices
-    for (;;) {
-        cudaMemsetAsync(C, 0, 8, s);
-        for (int k = 0; k < 16; ++k) {
-            if (dom)
-                project_relax<true><<<blocks, threads, 0, s>>>(K, E, H, n, C);
-            else
-                project_relax<false><<<blocks, threads, 0, s>>>(K, E, H, n, C);
+    return guarded([&]() -> rt_status {
+        if ((model != RT_DOMINO && model != RT_LOZENGE) || !d || !hmin || !hmax || !target || !out) return RT_E_INVAL;
+        int n = 0;
+        std::vector<uint8_t> kind, edges;
+        if (!lipschitz_graph(model, d, dlen, &n, &kind, &edges) || (int64_t)n * n != hlen) return RT_E_INVAL;
+        for (int64_t v = 0; v < hlen; ++v)
+            if (kind[v] && (hmin[v] == INT_MAX || hmax[v] == INT_MAX || hmin[v] > hmax[v] ||
+                            ((int64_t)hmax[v] - hmin[v]) % (model == RT_DOMINO ? 4 : 3) != 0))
+                return RT_E_INVAL;  // not a pair of height functions of this domain
+        if (cudaSetDevice(device) != cudaSuccess) return RT_E_NODEVICE;
+        const size_t N2 = (size_t)hlen;
+        DevMem dk, de, dlo, dhi, dt, dh, dc;
+        if (!dk.alloc(N2) || !de.alloc(N2) || !dlo.alloc(N2 * 4) || !dhi.alloc(N2 * 4) || !dt.alloc(N2 * 4) ||
+            !dh.alloc(N2 * 4) || !dc.alloc(16))
+            return RT_E_NOMEM;
+        cudaStream_t s;
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return RT_E_CUDA;
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaMemcpyAsync(dk.p, kind.data(), N2, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(de.p, edges.data(), N2, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(dlo.p, hmin, N2 * 4, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(dhi.p, hmax, N2 * 4, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(dt.p, target, N2 * 4, cudaMemcpyHostToDevice, s);
+        const int threads = 256;
+        const unsigned blocks = (unsigned)((N2 + threads - 1) / threads);
+        const bool dom = model == RT_DOMINO;
+        auto* K = static_cast<const uint8_t*>(dk.p);
+        auto* E = static_cast<const uint8_t*>(de.p);
+        auto* H = static_cast<int32_t*>(dh.p);
+        auto* C = static_cast<unsigned long long*>(dc.p);
+        cudaEventRecord(e0, s);
+        if (dom)
+            project_init<true><<<blocks, threads, 0, s>>>(K, (const int32_t*)dlo.p, (const int32_t*)dhi.p,
+                                                          (const float*)dt.p, H, n);
+        else
+            project_init<false><<<blocks, threads, 0, s>>>(K, (const int32_t*)dlo.p, (const int32_t*)dhi.p,
+                                                           (const float*)dt.p, H, n);
+        int64_t passes = 0, lowered = 0;
+        unsigned long long cnt[2] = {0, 0};
+        // Passes in chunks of 16 with one readback of the change counter per chunk;
+        // every pass is a monotone step, so extra passes after convergence are no-ops.
+        const int64_t cap = (int64_t)hlen + 32;  // Bellman-Ford bound: no more passes than vertices
+        for (;;) {
+            cudaMemsetAsync(C, 0, 8, s);
+            for (int k = 0; k < 16; ++k) {
+                if (dom)
+                    project_relax<true><<<blocks, threads, 0, s>>>(K, E, H, n, C);
+                else
+                    project_relax<false><<<blocks, threads, 0, s>>>(K, E, H, n, C);
+            }
+            passes += 16;
+            cudaError_t ce = cudaMemcpyAsync(cnt, C, 8, cudaMemcpyDeviceToHost, s);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+            if (ce != cudaSuccess) {
+                cudaStreamDestroy(s);
+                return RT_E_CUDA;
+            }
+            lowered += (int64_t)cnt[0];
+            if (cnt[0] == 0 || passes > cap) break;
         }
-        passes += 16;
-        cudaError_t ce = cudaMemcpyAsync(cnt, C, 8, cudaMemcpyDeviceToHost, s);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
-        if (ce != cudaSuccess) {
-            cudaStreamDestroy(s);
-            return RT_E_CUDA;
+        cudaMemsetAsync(C + 1, 0, 8, s);
+        project_finish<<<blocks, threads, 0, s>>>(K, (const int32_t*)dlo.p, H, n, C + 1);
+        cudaEventRecord(e1, s);
+        cudaMemcpyAsync(out, H, N2 * 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&cnt[1], C + 1, 8, cudaMemcpyDeviceToHost, s);
+        cudaError_t ce = cudaStreamSynchronize(s);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaStreamDestroy(s);
+        if (ce != cudaSuccess) return RT_E_CUDA;
+        if (stats) {
+            stats->passes = passes;
+            stats->lowered = lowered;
+            stats->raised = (int64_t)cnt[1];
+            stats->device_ms = ms;
         }
-        lowered += (int64_t)cnt[0];
-        if (cnt[0] == 0 || passes > cap) break;
-    }
-    cudaMemsetAsync(C + 1, 0, 8, s);
-    project_finish<<<blocks, threads, 0, s>>>(K, (const int32_t*)dlo.p, H, n, C + 1);
-    cudaEventRecord(e1, s);
-    cudaMemcpyAsync(out, H, N2 * 4, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&cnt[1], C + 1, 8, cudaMemcpyDeviceToHost, s);
-    cudaError_t ce = cudaStreamSynchronize(s);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaStreamDestroy(s);
-    if (ce != cudaSuccess) return RT_E_CUDA;
-    if (stats) {
-        stats->passes = passes;
-        stats->lowered = lowered;
-        stats->raised = (int64_t)cnt[1];
-        stats->device_ms = ms;
-    }
-    return RT_OK;
+        return RT_OK;
+    });
 }

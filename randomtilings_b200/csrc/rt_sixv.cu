@@ -26,6 +26,9 @@
 #include "../../include/rt_b200_sixv.h"
 #include "rt_device.cuh"
 #include "rt_internal.h"
+#include "rt_guard.h"
+
+using rtb::guarded;
 
 namespace rtb {
 
@@ -436,174 +439,194 @@ bool valid_n(int n) { return n >= 1 && n <= 32000; }
 extern "C" {
 
 rt_status rt_sixv_create(int32_t device, rt_sixv** out) {
-    if (!out) return RT_E_INVAL;
-    *out = nullptr;
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return RT_E_NODEVICE;
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) return RT_E_NODEVICE;
-    cudaSetDevice(device);
-    rt_sixv* h = new rt_sixv();
-    h->device = device;
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        delete h;
-        return RT_E_CUDA;
-    }
-    sixv_thresholds(h->w, h->thr, &h->monotone);
-    *out = h;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!out) return RT_E_INVAL;
+        *out = nullptr;
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return RT_E_NODEVICE;
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) return RT_E_NODEVICE;
+        cudaSetDevice(device);
+        rt_sixv* h = new rt_sixv();
+        h->device = device;
+        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete h;
+            return RT_E_CUDA;
+        }
+        sixv_thresholds(h->w, h->thr, &h->monotone);
+        *out = h;
+        return RT_OK;
+    });
 }
 
 rt_status rt_sixv_destroy(rt_sixv* h) {
-    if (!h) return RT_E_INVAL;
-    cudaSetDevice(h->device);
-    cudaStreamSynchronize(h->stream);
-    delete h;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        cudaSetDevice(h->device);
+        cudaStreamSynchronize(h->stream);
+        delete h;
+        return RT_OK;
+    });
 }
 
 const char* rt_sixv_last_error(rt_sixv* h) { return h ? h->err.c_str() : ""; }
 
 rt_status rt_sixv_set_weights(rt_sixv* h, const double w[6]) {
-    if (!h || !w) return RT_E_INVAL;
-    for (int t = 0; t < 6; ++t)
-        if (!(w[t] > 0) || !std::isfinite(w[t])) return h->fail(RT_E_INVAL, "vertex weights must be finite and > 0");
-    std::memcpy(h->w, w, sizeof h->w);
-    sixv_thresholds(h->w, h->thr, &h->monotone);
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!h || !w) return RT_E_INVAL;
+        for (int t = 0; t < 6; ++t)
+            if (!(w[t] > 0) || !std::isfinite(w[t])) return h->fail(RT_E_INVAL, "vertex weights must be finite and > 0");
+        std::memcpy(h->w, w, sizeof h->w);
+        sixv_thresholds(h->w, h->thr, &h->monotone);
+        return RT_OK;
+    });
 }
 
 rt_status rt_sixv_thresholds(rt_sixv* h, uint32_t thr[16], int32_t* monotone) {
-    if (!h) return RT_E_INVAL;
-    if (thr) std::memcpy(thr, h->thr, sizeof h->thr);
-    if (monotone) *monotone = h->monotone ? 1 : 0;
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        if (thr) std::memcpy(thr, h->thr, sizeof h->thr);
+        if (monotone) *monotone = h->monotone ? 1 : 0;
+        return RT_OK;
+    });
 }
 
 rt_status rt_sixv_dwbc_heights(int32_t n, int32_t* hmin, int32_t* hmax) {
-    if (!valid_n(n)) return RT_E_INVAL;
-    for (int i = 0; i <= n; ++i)
-        for (int j = 0; j <= n; ++j) {
-            const size_t at = (size_t)i * (n + 1) + j;
-            if (hmin) hmin[at] = std::abs(i - j);
-            if (hmax) hmax[at] = std::min(i + j, 2 * n - i - j);
-        }
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!valid_n(n)) return RT_E_INVAL;
+        for (int i = 0; i <= n; ++i)
+            for (int j = 0; j <= n; ++j) {
+                const size_t at = (size_t)i * (n + 1) + j;
+                if (hmin) hmin[at] = std::abs(i - j);
+                if (hmax) hmax[at] = std::min(i + j, 2 * n - i - j);
+            }
+        return RT_OK;
+    });
 }
 
 rt_status rt_sixv_check(const int32_t* heights, int32_t n) {
-    if (!heights || !valid_n(n)) return RT_E_INVAL;
-    const int S = n + 1;
-    auto H = [&](int i, int j) { return heights[(size_t)i * S + j]; };
-    for (int k = 0; k <= n; ++k)
-        if (H(0, k) != k || H(k, 0) != k || H(n, k) != n - k || H(k, n) != n - k) return RT_E_INVAL;
-    for (int i = 0; i <= n; ++i)
-        for (int j = 0; j <= n; ++j) {
-            if (i < n && std::abs(H(i + 1, j) - H(i, j)) != 1) return RT_E_INVAL;
-            if (j < n && std::abs(H(i, j + 1) - H(i, j)) != 1) return RT_E_INVAL;
-        }
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!heights || !valid_n(n)) return RT_E_INVAL;
+        const int S = n + 1;
+        auto H = [&](int i, int j) { return heights[(size_t)i * S + j]; };
+        for (int k = 0; k <= n; ++k)
+            if (H(0, k) != k || H(k, 0) != k || H(n, k) != n - k || H(k, n) != n - k) return RT_E_INVAL;
+        for (int i = 0; i <= n; ++i)
+            for (int j = 0; j <= n; ++j) {
+                if (i < n && std::abs(H(i + 1, j) - H(i, j)) != 1) return RT_E_INVAL;
+                if (j < n && std::abs(H(i, j + 1) - H(i, j)) != 1) return RT_E_INVAL;
+            }
+        return RT_OK;
+    });
 }
 
 rt_status rt_sixv_to_asm(const int32_t* heights, int32_t n, int32_t* asm_out) {
-    if (!asm_out || rt_sixv_check(heights, n) != RT_OK) return RT_E_INVAL;
-    const int S = n + 1;
-    for (int i = 1; i <= n; ++i)
-        for (int j = 1; j <= n; ++j) {
-            const int a = heights[(size_t)(i - 1) * S + j - 1], b = heights[(size_t)(i - 1) * S + j];
-            const int c = heights[(size_t)i * S + j - 1], d = heights[(size_t)i * S + j];
-            asm_out[(size_t)(i - 1) * n + (j - 1)] = (b + c - a - d) / 2;
-        }
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!asm_out || rt_sixv_check(heights, n) != RT_OK) return RT_E_INVAL;
+        const int S = n + 1;
+        for (int i = 1; i <= n; ++i)
+            for (int j = 1; j <= n; ++j) {
+                const int a = heights[(size_t)(i - 1) * S + j - 1], b = heights[(size_t)(i - 1) * S + j];
+                const int c = heights[(size_t)i * S + j - 1], d = heights[(size_t)i * S + j];
+                asm_out[(size_t)(i - 1) * n + (j - 1)] = (b + c - a - d) / 2;
+            }
+        return RT_OK;
+    });
 }
 
 rt_status rt_sixv_vertex_types(const int32_t* heights, int32_t n, int32_t* types) {
-    if (!types || rt_sixv_check(heights, n) != RT_OK) return RT_E_INVAL;
-    const int S = n + 1;
-    for (int i = 1; i <= n; ++i)
-        for (int j = 1; j <= n; ++j)
-            types[(size_t)(i - 1) * n + (j - 1)] =
-                vertex_type(heights[(size_t)(i - 1) * S + j - 1], heights[(size_t)(i - 1) * S + j],
-                            heights[(size_t)i * S + j - 1], heights[(size_t)i * S + j]);
-    return RT_OK;
+    return guarded([&]() -> rt_status {
+        if (!types || rt_sixv_check(heights, n) != RT_OK) return RT_E_INVAL;
+        const int S = n + 1;
+        for (int i = 1; i <= n; ++i)
+            for (int j = 1; j <= n; ++j)
+                types[(size_t)(i - 1) * n + (j - 1)] =
+                    vertex_type(heights[(size_t)(i - 1) * S + j - 1], heights[(size_t)(i - 1) * S + j],
+                                heights[(size_t)i * S + j - 1], heights[(size_t)i * S + j]);
+        return RT_OK;
+    });
 }
 
 rt_status rt_sixv_walk(rt_sixv* h, int32_t* heights, int32_t n, int64_t sweeps, uint64_t key, uint32_t chain) {
-    if (!h) return RT_E_INVAL;
-    if (!heights || !valid_n(n) || sweeps < 0) return h->fail(RT_E_INVAL, "bad arguments");
-    if (sweeps > kMaxColourSteps / 4) return h->fail(RT_E_INVAL, "more than 2^38 sweeps in one call");
-    if (rt_sixv_check(heights, n) != RT_OK)
-        return h->fail(RT_E_INVAL, "not a domain-wall height function of this size");
-    cudaSetDevice(h->device);
-    if (!h->reserve(n)) return h->fail(RT_E_NOMEM, "cudaMalloc six-vertex lattice");
-    rt_status s = upload(h, heights, n, 0);
-    if (s == RT_OK) s = run_epoch(h, n, 1, sweeps, key, chain);
-    if (s == RT_OK) s = download(h, heights, n, 0);
-    return s;
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        if (!heights || !valid_n(n) || sweeps < 0) return h->fail(RT_E_INVAL, "bad arguments");
+        if (sweeps > kMaxColourSteps / 4) return h->fail(RT_E_INVAL, "more than 2^38 sweeps in one call");
+        if (rt_sixv_check(heights, n) != RT_OK)
+            return h->fail(RT_E_INVAL, "not a domain-wall height function of this size");
+        cudaSetDevice(h->device);
+        if (!h->reserve(n)) return h->fail(RT_E_NOMEM, "cudaMalloc six-vertex lattice");
+        rt_status s = upload(h, heights, n, 0);
+        if (s == RT_OK) s = run_epoch(h, n, 1, sweeps, key, chain);
+        if (s == RT_OK) s = download(h, heights, n, 0);
+        return s;
+    });
 }
 
 rt_status rt_sixv_cftp(rt_sixv* h, int32_t n, int64_t first_sweeps, int64_t master_seed, int32_t max_trials,
                        int32_t* out_heights, rt_cftp_stats* stats) {
-    if (!h) return RT_E_INVAL;
-    if (!valid_n(n) || first_sweeps <= 0 || max_trials <= 0) return h->fail(RT_E_INVAL, "bad CFTP arguments");
-    if (first_sweeps > kMaxColourSteps / 4) return h->fail(RT_E_INVAL, "more than 2^38 sweeps in one call");
-    if (!h->monotone) return h->fail(RT_E_INVAL, "these weights give a heat bath that is not monotone: no CFTP");
-    cudaSetDevice(h->device);
-    if (!h->reserve(n)) return h->fail(RT_E_NOMEM, "cudaMalloc six-vertex lattices");
-    std::vector<int32_t> hmin((size_t)(n + 1) * (n + 1)), hmax(hmin.size());
-    rt_sixv_dwbc_heights(n, hmin.data(), hmax.data());
-    std::mt19937 mt((std::mt19937::result_type)master_seed);
-    std::vector<int64_t> sweeps{first_sweeps};
-    std::vector<uint64_t> keys{(uint64_t)mt()};
-    rt_cftp_stats st{};
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    rt_status s = RT_OK;
-    double ms_total = 0;
-    for (int trial = 0; trial < max_trials && s == RT_OK; ++trial) {
-        s = upload(h, hmax.data(), n, 0);
-        if (s == RT_OK) s = upload(h, hmin.data(), n, 1);
-        if (s != RT_OK) break;
-        cudaEventRecord(e0, h->stream);
-        for (size_t e = 0; e < sweeps.size() && s == RT_OK; ++e) s = run_epoch(h, n, 2, sweeps[e], keys[e], 0);
-        if (s != RT_OK) break;
-        cudaEventRecord(e1, h->stream);
-        s = launch_count_diff(h->d_h[0], h->d_h[1], h->cap, h->d_count, h->stream, &h->err);
-        if (s != RT_OK) break;
-        unsigned long long diff = 0;
-        cudaError_t ce = cudaMemcpyAsync(&diff, h->d_count, sizeof diff, cudaMemcpyDeviceToHost, h->stream);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
-        if (ce != cudaSuccess) {
-            s = h->cuda_fail(ce, "coalescence readback");
-            break;
+    return guarded([&]() -> rt_status {
+        if (!h) return RT_E_INVAL;
+        if (!valid_n(n) || first_sweeps <= 0 || max_trials <= 0) return h->fail(RT_E_INVAL, "bad CFTP arguments");
+        if (first_sweeps > kMaxColourSteps / 4) return h->fail(RT_E_INVAL, "more than 2^38 sweeps in one call");
+        if (!h->monotone) return h->fail(RT_E_INVAL, "these weights give a heat bath that is not monotone: no CFTP");
+        cudaSetDevice(h->device);
+        if (!h->reserve(n)) return h->fail(RT_E_NOMEM, "cudaMalloc six-vertex lattices");
+        std::vector<int32_t> hmin((size_t)(n + 1) * (n + 1)), hmax(hmin.size());
+        rt_sixv_dwbc_heights(n, hmin.data(), hmax.data());
+        std::mt19937 mt((std::mt19937::result_type)master_seed);
+        std::vector<int64_t> sweeps{first_sweeps};
+        std::vector<uint64_t> keys{(uint64_t)mt()};
+        rt_cftp_stats st{};
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        rt_status s = RT_OK;
+        double ms_total = 0;
+        for (int trial = 0; trial < max_trials && s == RT_OK; ++trial) {
+            s = upload(h, hmax.data(), n, 0);
+            if (s == RT_OK) s = upload(h, hmin.data(), n, 1);
+            if (s != RT_OK) break;
+            cudaEventRecord(e0, h->stream);
+            for (size_t e = 0; e < sweeps.size() && s == RT_OK; ++e) s = run_epoch(h, n, 2, sweeps[e], keys[e], 0);
+            if (s != RT_OK) break;
+            cudaEventRecord(e1, h->stream);
+            s = launch_count_diff(h->d_h[0], h->d_h[1], h->cap, h->d_count, h->stream, &h->err);
+            if (s != RT_OK) break;
+            unsigned long long diff = 0;
+            cudaError_t ce = cudaMemcpyAsync(&diff, h->d_count, sizeof diff, cudaMemcpyDeviceToHost, h->stream);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
+            if (ce != cudaSuccess) {
+                s = h->cuda_fail(ce, "coalescence readback");
+                break;
+            }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms_total += ms;
+            st.trials = trial + 1;
+            int64_t total = 0;
+            for (int64_t x : sweeps) total += x;
+            st.total_steps = 4 * total;
+            if (diff == 0) {
+                st.coalesced = 1;
+                break;
+            }
+            if (trial + 1 < max_trials && total > kMaxColourSteps / 8) {
+                // the next trial would run 2 total sweeps
+                s = h->fail(RT_E_INVAL, "CFTP schedule beyond 2^38 sweeps without coalescence");
+                break;
+            }
+            sweeps.insert(sweeps.begin(), total);
+            keys.insert(keys.begin(), (uint64_t)mt());
         }
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        ms_total += ms;
-        st.trials = trial + 1;
-        int64_t total = 0;
-        for (int64_t x : sweeps) total += x;
-        st.total_steps = 4 * total;
-        if (diff == 0) {
-            st.coalesced = 1;
-            break;
-        }
-        if (trial + 1 < max_trials && total > kMaxColourSteps / 8) {
-            // the next trial would run 2 total sweeps
-            s = h->fail(RT_E_INVAL, "CFTP schedule beyond 2^38 sweeps without coalescence");
-            break;
-        }
-        sweeps.insert(sweeps.begin(), total);
-        keys.insert(keys.begin(), (uint64_t)mt());
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    st.device_ms = ms_total;
-    if (stats) *stats = st;
-    if (s != RT_OK) return s;
-    if (out_heights) return download(h, out_heights, n, 0);
-    return RT_OK;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        st.device_ms = ms_total;
+        if (stats) *stats = st;
+        if (s != RT_OK) return s;
+        if (out_heights) return download(h, out_heights, n, 0);
+        return RT_OK;
+    });
 }
 
 }  // extern "C"
