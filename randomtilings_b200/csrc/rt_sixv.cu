@@ -10,10 +10,10 @@
 // b = 0..3, takes the four output words of one Philox4x32-10 call as their
 // draws, and applies the heat bath: a face whose four edge neighbours share
 // the height m becomes m+1 when its draw is below the threshold of its
-// diagonal pattern, else m-1.  Faces of one class share
-// no neighbour (edge or diagonal), so a launch is race-free and the result is
-// independent of the order of the threads.  Coupled CFTP chains are two
-// lattices of the same launch fed the same draws.
+// diagonal pattern, else m-1.  Faces of one class share no neighbour (edge
+// or diagonal), so a launch is race-free and the result is independent of the
+// order of the threads.  Coupled CFTP chains are two lattices of the same
+// launch fed the same draws.
 #include <cuda_runtime.h>
 
 #include <algorithm>
