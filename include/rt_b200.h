@@ -130,7 +130,8 @@ rt_status rt_set_lozenge_weights(rt_tiler* h, int32_t period, const double* w0, 
  * src/TriangleDimer/TriangleDimerTiler.cpp:86-483.  `tiling` (N*N int32,
  * host) is updated in place; synchronous, like the reference.  A call (and
  * each rt_walk_epochs / rt_run / CFTP trial, all epochs together) takes at
- * most 2^40 steps; more is RT_E_INVAL, with the tiling left as it was. */
+ * most 2^40 steps; more is RT_E_INVAL, with the tiling left as it was.
+ * Tiling sides above 32767 are RT_E_INVAL (the kernels' indices are 32-bit). */
 rt_status rt_walk(rt_tiler* h, int32_t* tiling, int32_t n, int64_t steps, int64_t seed);
 
 /* Replaces DominoTiler::Walk(tiling&, vector<long> steps, vector<long> seeds)

@@ -54,7 +54,8 @@ rt_status rt_batch_create(int32_t device, rt_batch** out);
 rt_status rt_batch_destroy(rt_batch* b);
 /* Copies an N x N host tiling into the batch; *index (optional) receives the
  * chain's index.  Chains are added before the first rt_batch_run
- * (RT_E_STATE after it); adding one invalidates the plan. */
+ * (RT_E_STATE after it); adding one invalidates the plan.  N above 32767 is
+ * RT_E_INVAL. */
 rt_status rt_batch_add(rt_batch* b, const rt_chain* c, const int32_t* tiling, int32_t n, int64_t* index);
 /* autotune = 1 (default): time the candidate plans at the first run;
  * autotune = 0: use `cluster` CTAs per cluster and `block` threads per CTA

@@ -991,6 +991,7 @@ rt_status rt_batch_add(rt_batch* b, const rt_chain* c, const int32_t* tiling, in
         ch.ncol = ncol_of(f);
         ch.elem = elem_of(f);
         ch.n = n;
+        if (n > kMaxTilingSide) return b->fail(RT_E_INVAL, "tiling side above 32767");
         if (ch.kind == 0 && (n < 6 || n % 2)) return b->fail(RT_E_INVAL, "domino tiling side must be even and >= 6");
         if ((ch.kind == 1 || ch.kind == 2) && (n < 9 || n % 3))
             return b->fail(RT_E_INVAL, "tiling side must be a multiple of 3 and >= 9");

@@ -464,6 +464,7 @@ rt_status rt_load_rng_params(rt_tiler* h, const char* path, int64_t n) {
 }
 
 static rt_status check_size(rt_tiler* h, int n) {
+    if (n > kMaxTilingSide) return h->fail(RT_E_INVAL, "tiling side above 32767");
     if (h->kind == 0 && (n < 6 || n % 2 != 0)) return h->fail(RT_E_INVAL, "domino tiling side must be even and >= 6");
     if (h->kind == 3 && (n < 8 || n % 2 != 0))
         return h->fail(RT_E_INVAL, "triangle-dimer tiling side must be even and >= 8");

@@ -27,6 +27,10 @@ enum Family : int {
 // size computed from a count can wrap.
 constexpr int64_t kMaxColourSteps = int64_t(1) << 40;
 
+// The largest tiling side a walk accepts: the kernels index a lattice with
+// 32-bit integers, and a side of 32,767 keeps every index below 2^31.
+constexpr int kMaxTilingSide = 32767;
+
 struct WalkPlan {
     int items = 0;
     int block = 0;

@@ -90,3 +90,17 @@ def test_batch_refuses_more_than_2_35_sweeps(rt, sweeps):
         b.set_sweeps_per_launch(sweeps)
     _refused(ei)
     b.close()
+
+
+def test_walk_refuses_a_tiling_side_above_32767(rt):
+    """The side is checked before the tiling is read, so a short buffer
+    suffices; 32,769 is a multiple of 3, as a lozenge side must be."""
+    from randomtilings_b200 import _capi
+
+    buf = np.zeros(16, dtype=np.int32)
+    tl = rt.LozengeTiler()
+    st = tl._lib.rt_walk(tl._h, buf.ctypes.data, 32769, 10, 1)
+    assert st == _capi.RT_E_INVAL
+    assert "32767" in tl._lib.rt_last_error(tl._h).decode()
+    assert not buf.any()
+    tl.close()
