@@ -720,13 +720,24 @@ rt_status rt_mlp_loss_grad(rt_mlp* m, const float* x, const float* target, int64
 
 rt_status rt_mlp_set_data(rt_mlp* m, const float* x, const float* target, int64_t n) {
     return guarded([&]() -> rt_status {
-        if (!m || !x || !target || n <= 0) return RT_E_INVAL;
+        // At most 2^40 rows, so that no byte count below can wrap.
+        if (!m || !x || !target || n <= 0 || n > ((int64_t)1 << 40)) return RT_E_INVAL;
         cudaSetDevice(m->device);
         if (m->X) cudaFree(m->X);
         if (m->T) cudaFree(m->T);
         m->X = m->T = nullptr;
-        if (cudaMalloc(&m->X, (size_t)n * IN * 4) != cudaSuccess || cudaMalloc(&m->T, (size_t)n * 4) != cudaSuccess)
+        m->rows = 0;
+        // Both buffers or neither: training checks for both.
+        float *X = nullptr, *T = nullptr;
+        const bool okx = cudaMalloc(&X, (size_t)n * IN * 4) == cudaSuccess;
+        const bool okt = okx && cudaMalloc(&T, (size_t)n * 4) == cudaSuccess;
+        if (!okt) {
+            if (okx) cudaFree(X);
+            cudaGetLastError();
             return RT_E_NOMEM;
+        }
+        m->X = X;
+        m->T = T;
         cudaMemcpyAsync(m->X, x, (size_t)n * IN * 4, cudaMemcpyHostToDevice, m->s);
         cudaMemcpyAsync(m->T, target, (size_t)n * 4, cudaMemcpyHostToDevice, m->s);
         m->rows = n;
@@ -736,7 +747,7 @@ rt_status rt_mlp_set_data(rt_mlp* m, const float* x, const float* target, int64_
 
 rt_status rt_mlp_train(rt_mlp* m, int64_t steps, int32_t batch, float lr, uint64_t seed, float* loss) {
     return guarded([&]() -> rt_status {
-        if (!m || steps < 0 || batch <= 0 || batch > (1 << 22) || !m->X) return RT_E_INVAL;
+        if (!m || steps < 0 || batch <= 0 || batch > (1 << 22) || !m->X || !m->T || m->rows <= 0) return RT_E_INVAL;
         cudaSetDevice(m->device);
         if (!reserve(m, batch)) return RT_E_NOMEM;
         for (int64_t k = 0; k < steps; ++k) {

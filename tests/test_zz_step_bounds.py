@@ -2,10 +2,13 @@
 2^35 batched sweeps; 2^38 six-vertex sweeps) are refused with RT_E_INVAL
 before any schedule is sized from them, up to the largest int64, and the
 caller's data stays as it was.  Without the bound, a count near 2^62 made the
-phase list's byte size wrap to a few bytes.  Collected last so that a
-failure here cannot hide other tests.
+phase list's byte size wrap to a few bytes.  The MLP's dataset row count is bounded
+the same way (2^40).  Collected last so that a failure here cannot hide
+other tests.
 """
 from __future__ import annotations
+
+import ctypes
 
 import numpy as np
 import pytest
@@ -104,3 +107,18 @@ def test_walk_refuses_a_tiling_side_above_32767(rt):
     assert "32767" in tl._lib.rt_last_error(tl._h).decode()
     assert not buf.any()
     tl.close()
+
+
+def test_mlp_refuses_a_dataset_above_2_40_rows(rt):
+    """A row count whose byte size would wrap is refused, and a handle
+    without data refuses to train (it would have nothing to sample)."""
+    from randomtilings_b200 import _capi
+    from randomtilings_b200.mlp import CoordinateMLP
+
+    m = CoordinateMLP()
+    x = np.zeros((4, _capi.RT_MLP_IN), dtype=np.float32)
+    t = np.zeros(4, dtype=np.float32)
+    assert m._lib.rt_mlp_set_data(m._h, x.ctypes.data, t.ctypes.data, 1 << 62) == _capi.RT_E_INVAL
+    loss = ctypes.c_float()
+    assert m._lib.rt_mlp_train(m._h, 1, 16, 1e-3, 0, ctypes.byref(loss)) == _capi.RT_E_INVAL
+    m.close()
