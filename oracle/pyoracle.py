@@ -28,7 +28,7 @@ _P, _I32, _I64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
 def build_oracle() -> str:
     """Builds the C restatement if it is missing (gcc only)."""
     if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < max(
-        os.path.getmtime(os.path.join(HERE, f)) for f in ("rt_oracle.c", "rt_oracle.h")
+        os.path.getmtime(os.path.join(HERE, f)) for f in ("rt_oracle.c", "rt_oracle.h", "sixv_oracle.c")
     ):
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
     return ORACLE_SO
@@ -75,6 +75,8 @@ def oracle() -> ctypes.CDLL:
         lib.orc_sixv_vertex_type.argtypes = [ctypes.c_int] * 4
         lib.orc_sixv_thresholds.argtypes = [_P, _P]
         lib.orc_sixv_walk.argtypes = [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_uint32, _P]
+        lib.orc_sixv_step_rows.argtypes = [_P, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64, ctypes.c_uint32, _P,
+                                           ctypes.c_int, ctypes.c_int]
         lib.orc_tinymt_init.argtypes = [_P, ctypes.c_uint32]
         lib.orc_tinymt_bits12.argtypes = [_P]
         lib.orc_tinymt_bits12.restype = ctypes.c_uint32
@@ -369,6 +371,16 @@ def sixv_walk(h, sweeps, keys, chain: int = 0, w=SIXV_UNIFORM) -> np.ndarray:
     _check(oracle().orc_sixv_walk(a.ctypes.data, n, st.ctypes.data, ke.ctypes.data, st.size, chain, ww.ctypes.data),
            "orc_sixv_walk")
     return a
+
+
+def sixv_step_rows(a: np.ndarray, s: int, key: int, lo: int, hi: int, chain: int = 0, w=SIXV_UNIFORM) -> None:
+    """Colour step s (epoch key `key`) on the face rows [lo, hi) of the
+    heights a ((n+1)^2 int32, contiguous), in place."""
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    n = int(round(a.size ** 0.5)) - 1
+    ww = np.ascontiguousarray(w, dtype=np.float64)
+    _check(oracle().orc_sixv_step_rows(a.ctypes.data, n, s, key & (2**64 - 1), chain, ww.ctypes.data, lo, hi),
+           "orc_sixv_step_rows")
 
 
 def sixv_cftp(n: int, first_sweeps: int, master_seed: int, max_trials: int = 30, w=SIXV_UNIFORM, chain: int = 0):

@@ -136,6 +136,11 @@ int orc_sixv_vertex_type(int a, int b, int c, int d);
 void orc_sixv_thresholds(const double w[6], uint32_t thr[16]);
 int orc_sixv_walk(int32_t* h, int n, const int64_t* sweeps, const int64_t* keys, int k, uint32_t chain,
                   const double w[6]);
+/* Colour step s of an epoch keyed by `key`, on the face rows [lo, hi) only:
+ * what one band of the CUDA band kernel computes (the tests rebuild its
+ * halo exchange from it). */
+int orc_sixv_step_rows(int32_t* h, int n, int64_t s, uint64_t key, uint32_t chain, const double w[6], int lo,
+                       int hi);
 
 #ifdef __cplusplus
 }

@@ -74,11 +74,17 @@ void orc_sixv_thresholds(const double w[6], uint32_t thr[16]) {
     }
 }
 
-static void sixv_step(int32_t* h, int n, int64_t s, uint64_t key, uint32_t chain, const uint32_t thr[16]) {
+/* Colour step s on the face rows i in [lo, hi) only (the whole step is
+ * lo = 1, hi = n). */
+static void sixv_step_range(int32_t* h, int n, int64_t s, uint64_t key, uint32_t chain, const uint32_t thr[16],
+                            int lo, int hi) {
     const int N1 = n + 1, Q = (N1 + 7) / 8;
     const int pi = (int)((s & 3) >> 1), pj = (int)(s & 1);
     const uint32_t k2[2] = {(uint32_t)key, (uint32_t)(key >> 32)};
-    for (int i = pi == 0 ? 2 : 1; i <= n - 1; i += 2)
+    int first = pi == 0 ? 2 : 1;
+    if (lo > first) first += ((lo - first + 1) / 2) * 2;
+    if (hi > n) hi = n;
+    for (int i = first; i < hi; i += 2)
         for (int q = 0; q < Q; ++q) {
             const uint32_t ctr[4] = {(uint32_t)(i * Q + q), (uint32_t)s, (uint32_t)((uint64_t)s >> 32), chain};
             uint32_t out[4];
@@ -93,6 +99,21 @@ static void sixv_step(int32_t* h, int n, int64_t s, uint64_t key, uint32_t chain
                 *f = (out[b] >> 9) < thr[p] ? m + 1 : m - 1;
             }
         }
+}
+
+static void sixv_step(int32_t* h, int n, int64_t s, uint64_t key, uint32_t chain, const uint32_t thr[16]) {
+    sixv_step_range(h, n, s, key, chain, thr, 1, n);
+}
+
+int orc_sixv_step_rows(int32_t* h, int n, int64_t s, uint64_t key, uint32_t chain, const double w[6], int lo,
+                       int hi) {
+    if (n < 1 || !h || !w || s < 0) return ORC_EINVAL;
+    for (int t = 0; t < 6; ++t)
+        if (!(w[t] > 0) || !isfinite(w[t])) return ORC_EINVAL;
+    uint32_t thr[16];
+    orc_sixv_thresholds(w, thr);
+    sixv_step_range(h, n, s, key, chain, thr, lo, hi);
+    return ORC_OK;
 }
 
 int orc_sixv_walk(int32_t* h, int n, const int64_t* sweeps, const int64_t* keys, int k, uint32_t chain,
