@@ -664,17 +664,20 @@ rt_status rt_load_matrix(const char* filename, int32_t* out, int64_t cap, int64_
         std::vector<int32_t> v;
         char c;
         bool inside = false;
-        int64_t cur = 0;
+        // Digits accumulate modulo 2^64 (defined for any length); the value
+        // kept is the low 32 bits, the wrap-around the reference's int
+        // accumulator (common.cpp:149-155) shows in practice.
+        uint64_t cur = 0;
         while (in.get(c)) {
             if (c >= '0' && c <= '9') {
-                cur = inside ? cur * 10 + (c - '0') : (c - '0');
+                cur = inside ? cur * 10 + (uint64_t)(c - '0') : (uint64_t)(c - '0');
                 inside = true;
             } else if (inside) {
-                v.push_back((int32_t)cur);
+                v.push_back((int32_t)(uint32_t)cur);
                 inside = false;
             }
         }
-        if (inside) v.push_back((int32_t)cur);
+        if (inside) v.push_back((int32_t)(uint32_t)cur);
         if (len) *len = (int64_t)v.size();
         if (!out) return RT_OK;
         if (cap < (int64_t)v.size()) return RT_E_INVAL;

@@ -96,3 +96,19 @@ def test_load_matrix_round_trip(tmp_path):
     p = tmp_path / "m.txt"
     rt.RectTriangleTiler.SaveMatrix(t, str(p))
     assert np.array_equal(rt.RectTriangleTiler.LoadMatrix(str(p)), t)
+
+
+def test_load_matrix_long_digit_runs_wrap_like_the_reference(tmp_path):
+    """LoadMatrix (common.cpp:141-161) reads every run of digits as one
+    number ('-' and other characters only separate) into an int that wraps;
+    runs of any length are read, keeping the value modulo 2^32 as int32."""
+    from randomtilings_b200 import builders
+
+    runs = ["7", "-12", "4294967297", "99999999999999999999999999", "2147483648", "0012"]
+    p = tmp_path / "m.txt"
+    p.write_text(" ".join(runs) + "\n")
+    want = []
+    for r in runs:
+        v = int(r.lstrip("-")) % 2**32
+        want.append(v - 2**32 if v >= 2**31 else v)
+    assert builders.load_matrix(p).tolist() == want
