@@ -443,7 +443,8 @@ rt_status rt_load_rng_params(rt_tiler* h, const char* path, int64_t n) {
         std::ifstream in(path);
         if (!in) return h->fail(RT_E_PARAMS, std::string("cannot open parameter file ") + path);
         std::vector<uint32_t> t;
-        t.reserve((size_t)(3 * n));
+        // The file, not n, bounds the table: reserve at most 2^21 entries ahead.
+        t.reserve((size_t)std::min<int64_t>(n, (int64_t)1 << 21) * 3);
         std::string line;
         int64_t got = 0;
         while (got < n && std::getline(in, line)) {
