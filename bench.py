@@ -470,8 +470,8 @@ def measure_sixv(args, device: int) -> dict:
 
 
 def measure_cftp_small(args, rank: int, world: int, dist) -> dict:
-    """Coupling from the past in the default run (the configs[2] run at order
-    500 and 32 seeds is --workload cftp): an Aztec diamond of order
+    """Coupling from the past in the default run (the 32-seed run at order
+    500 is --workload cftp): an Aztec diamond of order
     args.cftp_small_order, bit-plane heat bath, coupled maximal and minimal
     chains in one launch, doubling from 1,024 colour steps, master seeds
     0..args.cftp_small_seeds-1 dealt to the ranks."""
