@@ -511,11 +511,20 @@ rt_status rt_sixv_check(const int32_t* heights, int32_t n) {
         auto H = [&](int i, int j) { return heights[(size_t)i * S + j]; };
         for (int k = 0; k <= n; ++k)
             if (H(0, k) != k || H(k, 0) != k || H(n, k) != n - k || H(k, n) != n - k) return RT_E_INVAL;
-        for (int i = 0; i <= n; ++i)
-            for (int j = 0; j <= n; ++j) {
-                if (i < n && std::abs(H(i + 1, j) - H(i, j)) != 1) return RT_E_INVAL;
-                if (j < n && std::abs(H(i, j + 1) - H(i, j)) != 1) return RT_E_INVAL;
-            }
+        // Every edge joins heights that differ by exactly 1: a row at a time,
+        // branch-free.  Differences are taken modulo 2^32 (defined for any
+        // input; d is +-1 iff d + 1 is 0 or 2).  That accepts exactly what
+        // the exact test accepts: every face is within n / 2 edges of the
+        // boundary, whose heights are 0..n, so heights that pass every edge
+        // stay within [-n, 2n] and no difference wraps.
+        for (int i = 0; i <= n; ++i) {
+            const uint32_t* r = reinterpret_cast<const uint32_t*>(heights) + (size_t)i * S;
+            uint32_t bad = 0;
+            for (int j = 0; j < n; ++j) bad |= (r[j + 1] - r[j] + 1u) & ~2u;
+            if (i < n)
+                for (int j = 0; j <= n; ++j) bad |= (r[j + S] - r[j] + 1u) & ~2u;
+            if (bad) return RT_E_INVAL;
+        }
         return RT_OK;
     });
 }
