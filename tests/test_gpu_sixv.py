@@ -100,3 +100,19 @@ def test_bench_walk_matches_restatement(rt):
     tl.Walk(h, 400, 2)
     tl.close()
     assert np.array_equal(h, po.sixv_walk(start, 400, 2))
+
+
+@pytest.mark.parametrize("n", [7, 24, 65])
+def test_walks_match_the_committed_vectors(rt, n):
+    """The CUDA walk against tests/golden/sixv.npz directly (the vectors the
+    restatement is held to), from both extremes, uniform and weighted."""
+    from conftest import golden
+
+    z = golden("sixv")
+    for w, wname in ((po.SIXV_UNIFORM, "uniform"), (WEIGHTED, "weighted")):
+        tl = rt.SixVertexTiler(weights=w)
+        for sname, start in (("min", rt.SixVertexTiler.MinHeights(n)), ("max", rt.SixVertexTiler.MaxHeights(n))):
+            h = start.copy()
+            tl.Walk(h, 40, 0x5EED + n, n % 3)
+            assert np.array_equal(h, z[f"walk/{n}/{sname}/{wname}"]), (sname, wname)
+        tl.close()
