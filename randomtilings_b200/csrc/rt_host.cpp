@@ -175,7 +175,10 @@ Vec dom_height_to_tiling(const Vec& hf, const Vec& d, int n) {
                 dom_edge_faces(i, j, nb, f);
                 if (!dom_face(d, m, f[0], f[1]) && !dom_face(d, m, f[2], f[3])) continue;
                 const int64_t diff = (int64_t)hf[i2 * n + j2] - hf[i * n + j];
-                t[i * n + j] += kDomBit[nb] * (int32_t)std::llabs(diff / 2);
+                // modulo 2^32, so that heights that are no height function
+                // (any int32 input) still give a defined result
+                int32_t& tv = t[(size_t)i * n + j];
+                tv = (int32_t)((uint32_t)tv + (uint32_t)kDomBit[nb] * (uint32_t)std::llabs(diff / 2));
             }
         }
     return t;
