@@ -350,7 +350,15 @@ rt_status rt_domino_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d, 
             dlen = (int64_t)dom.size();
         }
         if (dlen < (int64_t)m * m) return RT_E_INVAL;
-        auto D = [&](int i, int j) { return d[(size_t)i * m + j]; };
+        // The reference indexes d[i M + j +- 1] and d[(i +- 1) M + j] as flat
+        // offsets (DominoTiler.cpp:571-592): a column step past the edge reads
+        // the next row's first cell, and the row after the last one lies past
+        // the array.  The same flat reads here, with offsets past the array
+        // reading as empty (the builders' padded domains never reach them).
+        auto D = [&](int i, int j) {
+            const int64_t k = (int64_t)i * m + j;
+            return k >= 0 && k < (int64_t)m * m ? d[k] : 0;
+        };
         Sink o(filename);
         o << kSvgOpen << "height=\"500\" width=\"500\" viewBox=\"0 0 " << m << " " << m << "\">\n";
         o << "<defs>\n";
@@ -595,9 +603,13 @@ rt_status rt_tridimer_dimer_svg(const int32_t* t, int64_t tlen, const int32_t* d
             dlen = len;
         }
         const int m = side_of(dlen / 2);
+        // The domain of an n x n tiling is m x 2m with 2m = n; the loops below
+        // read the tiling up to row and column 2m - 3.
+        if (2 * (int64_t)m > n) return RT_E_INVAL;
         // The reference also reads one cell before the domain and one row past it.
         Vec pad((size_t)2 * m * (m + 2) + 2, 0);
-        for (int64_t k = 0; k < dlen; ++k) pad[(size_t)k + 2 * m + 1] = d[k];
+        const int64_t cells = std::min<int64_t>(dlen, (int64_t)2 * m * m);
+        for (int64_t k = 0; k < cells; ++k) pad[(size_t)k + 2 * m + 1] = d[k];
         auto D = [&](int i, int j) { return pad[(size_t)(i * 2 * m + j) + 2 * m + 1]; };
         Sink o(filename);
         tri_header(o, m);

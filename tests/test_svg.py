@@ -112,3 +112,28 @@ def test_load_matrix_long_digit_runs_wrap_like_the_reference(tmp_path):
         v = int(r.lstrip("-")) % 2**32
         want.append(v - 2**32 if v >= 2**31 else v)
     assert builders.load_matrix(p).tolist() == want
+
+
+def test_dimer_writers_on_inputs_the_builders_never_make(tmp_path):
+    """A domino domain with cells in its last row (the reference's writer
+    reads one row past the array there; the builders' padded domains never
+    do), and triangle-dimer domains that do not belong to the tiling: a
+    larger one is refused, and one whose length is not 2 m^2 is read only as
+    far as its m x 2m cells."""
+    import ctypes
+
+    from randomtilings_b200 import _capi
+
+    lib = _capi.load()
+    path = str(tmp_path / "x.svg").encode()
+    t = np.asarray(rt.DominoTiler.MaxTiling(rt.DominoTiler.AztecDiamond(3)), dtype=np.int32)
+    m = int(round(t.size ** 0.5)) - 1
+    d = np.ones(m * m, dtype=np.int32)
+    assert lib.rt_domino_dimer_svg(t.ctypes.data, t.size, d.ctypes.data, d.size, path) == _capi.RT_OK
+
+    tt = np.asarray(rt.TriangleDimerTiler.IceCreamCone(6, 1), dtype=np.int32)
+    n = int(round(tt.size ** 0.5))
+    big = np.ones(2 * (n // 2 + 1) ** 2, dtype=np.int32)
+    assert lib.rt_tridimer_dimer_svg(tt.ctypes.data, tt.size, big.ctypes.data, big.size, path) == _capi.RT_E_INVAL
+    ragged = np.ones(2 * (n // 2 + 1) ** 2 - 1, dtype=np.int32)  # the longest length that still reads as m = n / 2
+    assert lib.rt_tridimer_dimer_svg(tt.ctypes.data, tt.size, ragged.ctypes.data, ragged.size, path) == _capi.RT_OK
